@@ -1,0 +1,348 @@
+"""Benchmark: F[rho] + dF/drho evaluations per second at 128^3 on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision fp64|mixed]
+
+Workload (one "step" = one full F + dF/drho evaluation, functionals::total of
+the reference): the 128^3 DDFT state of the LJ-fluid configuration --
+periodic 128^3 grid, dx = 0.125 sigma, kT = 0.8, single species White-Bear-II
+FMT with the WCA hard-sphere diameter of a cut LJ (sigma = eps = 1,
+r_c = 2.5, QF weights), mean density 0.35 with seeded 1% white noise.  Inputs
+are synthetic (seeded); no dataset is involved.
+
+Timing: inputs resident in HBM, W untimed warm-up steps, then K steps, each
+bracketed by CUDA events on the engine's stream with an L2 flush (a write of
+a 256 MiB buffer, outside the events) between steps; barrier + synchronize
+on both sides; the max over ranks.  Each rank evaluates its own replica
+(one grid does not shard), so `value` = N * K / max time.
+
+`e2e` repeats the metric through the public host API (cdft_total via
+classicaldft_b200.Engine.total_host) with pinned host buffers: H2D of rho,
+D2H of the force and the scalars inside the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+SHAPE = (128, 128, 128)
+DX = 0.125
+KT = 0.8
+RHO_BAR = 0.35
+SEED = 20261204
+METRIC = "F+dF/drho evals/s at 128^3"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+
+def workload_profile():
+    rng = np.random.default_rng(SEED)
+    return RHO_BAR * (1.0 + 0.01 * rng.uniform(-1.0, 1.0, SHAPE[0] * SHAPE[1] * SHAPE[2]))
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+def algorithmic_bytes(info, S=1, M=1, has_vext=False):
+    """Compulsory HBM bytes of one evaluation of this pipeline: one read and one
+    write of every array each stage touches (each FFT counted as one read of its
+    input and one write of its output), FP64 I/O for rho, V_ext and the force."""
+    N, Nk = info["N"], info["Nk"]
+    C, D = info["channels"], info["deriv_channels"]
+    s = 4 if info["precision"] == 1 else 8
+    Br, Bc, Bio = N * s, 2 * Nk * s, 8 * N
+    b = 0
+    if info["precision"] == 1:
+        b += S * Bio + S * Br            # rho -> fp32 copy
+    b += S * Br + S * Bc                 # r2c rho
+    b += S * Bc + M * 8 * Nk + C * Bc    # forward channels (+ MF weight, FP64 real)
+    b += C * (Bc + Br)                   # c2r channels
+    b += C * Br + S * Bio * (2 if has_vext else 1) + D * Br + S * Bio   # pointwise
+    b += D * (Br + Bc)                   # r2c derivatives
+    b += D * Bc + S * Bc                 # back-convolution
+    b += S * (Bc + Br)                   # c2r force
+    b += S * Br + 2 * S * Bio            # epilogue
+    return b
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def setup_dist(args):
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as d
+        backend = "nccl" if (args.impl == "ours" and torch.cuda.is_available()) else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        d.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        dist = d
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return ws, rank, local, dist
+
+
+def run_reference(args, ws, rank, dist):
+    """--impl reference: the CPU restatement of the reference path (the oracle)
+    on all host cores, same workload, bounded sample per step."""
+    if rank != 0:
+        return
+    from oracle import fmt as ofmt
+    from oracle import potentials as opot
+    from oracle.functional import Model, Species, make_weights, total
+    from oracle.grid import Grid, WORKERS
+    lj = opot.make_lennard_jones(1.0, 1.0, 2.5)
+    d = opot.hard_sphere_diameter(lj, KT, opot.WCA)
+    g = Grid(dx=DX, box_size=tuple(n * DX for n in SHAPE), shape=SHAPE)
+    model = Model(g, [Species("LJ", d)], [opot.Interaction(0, 0, lj)], KT)
+    w = make_weights(ofmt.FMTModel("WhiteBearII"), model)
+    rho = workload_profile()
+    for _ in range(args.warmup):
+        total(model, [rho], w, [0.0])
+    budget = 150.0
+    t0 = time.perf_counter()
+    done = 0
+    for _ in range(args.steps):
+        total(model, [rho], w, [0.0])
+        done += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    el = time.perf_counter() - t0
+    v = done / el
+    line = {"metric": METRIC, "value": v, "unit": "evals/s", "n_gpus": ws, "steps": done, "warmup": args.warmup,
+            "ms_per_step": 1e3 * el / done, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": "128^3 LJ-fluid DDFT state, WhiteBearII + cut LJ (QF), 1 species",
+                       "grid": list(SHAPE), "dx": DX, "kT": KT},
+            "cpu_baseline": {"value": v, "unit": "evals/s", "cores": WORKERS, "kind": "port",
+                             "sample": f"{done} evaluations of the 128^3 workload (NumPy/SciPy FP64 oracle)"},
+            "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(seconds=12.0):
+    """The oracle on the host cores, bounded to ~`seconds` of work."""
+    from oracle import fmt as ofmt
+    from oracle import potentials as opot
+    from oracle.functional import Model, Species, make_weights, total
+    from oracle.grid import Grid, WORKERS
+    lj = opot.make_lennard_jones(1.0, 1.0, 2.5)
+    d = opot.hard_sphere_diameter(lj, KT, opot.WCA)
+    g = Grid(dx=DX, box_size=tuple(n * DX for n in SHAPE), shape=SHAPE)
+    model = Model(g, [Species("LJ", d)], [opot.Interaction(0, 0, lj)], KT)
+    w = make_weights(ofmt.FMTModel("WhiteBearII"), model)
+    rho = workload_profile()
+    total(model, [rho], w, [0.0])  # warm-up
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        ref = total(model, [rho], w, [0.0])
+        n += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    el = time.perf_counter() - t0
+    return {"value": n / el, "unit": "evals/s", "cores": WORKERS, "kind": "port",
+            "sample": f"{n} evaluations of the 128^3 workload (NumPy/SciPy FP64 oracle, scipy.fft workers={WORKERS})"}, ref
+
+
+def run_ours(args, ws, rank, local, dist):
+    import torch
+    import classicaldft_b200 as cd
+    dev = torch.device("cuda", local)
+    precision = cd.MIXED if args.precision == "mixed" else cd.FP64
+    lj = cd.make_lennard_jones(1.0, 1.0, 2.5)
+    d = lj.hard_sphere_diameter(KT, cd.WEEKS_CHANDLER_ANDERSEN)
+    g = cd.Grid(dx=DX, box_size=tuple(n * DX for n in SHAPE), shape=SHAPE)
+    model = cd.Model(g, [cd.Species("LJ", d)], [cd.Interaction(0, 0, lj)], KT)
+    eng = cd.Engine(cd.WhiteBearII(), model, precision)
+    rho_h = workload_profile()
+    rho = torch.tensor(rho_h, dtype=torch.float64, device=dev)
+    force = torch.empty_like(rho)
+    scal = torch.zeros(10, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+
+    def step():
+        eng.total_device(rho.data_ptr(), None, [0.0], force.data_ptr(), scal.data_ptr(), sp)
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            step()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    with torch.cuda.stream(stream):
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            starts[i].record(stream)
+            step()
+            ends[i].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    times = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    t_ms = float(np.sum(times))
+    if dist:
+        tt = torch.tensor([t_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = ws * args.steps / (t_ms * 1e-3)
+    ms_step = t_ms / args.steps
+
+    # e2e through the host API with pinned buffers
+    rho_pin = torch.tensor(rho_h, dtype=torch.float64).pin_memory()
+    f_pin = torch.empty_like(rho_pin).pin_memory()
+    sc_pin = torch.empty(10, dtype=torch.float64).pin_memory()
+    L = cd.lib()
+    import ctypes
+    mu = (ctypes.c_double * 1)(0.0)
+
+    def e2e_step():
+        st = L.cdft_total(eng.handle, rho_pin.data_ptr(), None, mu, f_pin.data_ptr(),
+                          ctypes.cast(sc_pin.data_ptr(), ctypes.POINTER(ctypes.c_double)))
+        if st != 0:
+            raise RuntimeError(L.cdft_last_error().decode())
+
+    for _ in range(3):
+        e2e_step()
+    n_e2e = max(10, min(args.steps, 200))
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        e2e_step()
+    el = time.perf_counter() - t0
+    if dist:
+        tt = torch.tensor([el], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        el = float(tt.item())
+    e2e_val = ws * n_e2e / el
+
+    info = eng.info
+    nbytes = algorithmic_bytes(info, S=1, M=1)
+    peak, peak_kind = hbm_peak()
+    achieved = nbytes / (ms_step * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 FFT / f64 Phi+sums" if precision == cd.MIXED else "f64",
+        "data": "synthetic",
+        "config": {"workload": "128^3 LJ-fluid DDFT state, WhiteBearII + cut LJ (QF), 1 species",
+                   "grid": list(SHAPE), "dx": DX, "kT": KT, "rho_bar": RHO_BAR, "noise": "1% uniform, seeded",
+                   "hs_diameter": d, "precision": args.precision, "parallelism": f"replicas x{ws}",
+                   "l2": "flushed between timed steps (256 MiB write outside the events)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "scope": "one full evaluation (25 cuFFT transforms + 5 engine kernels)",
+                     "algorithmic_bytes": nbytes, "peak_source": peak_kind},
+        "e2e": {"value": e2e_val, "unit": "evals/s", "h2d_bytes_per_step": 8 * info["N"],
+                "d2h_bytes_per_step": 8 * info["N"] + 80},
+        "clocks": clocks,
+        "gpu_launches": int(info["kernels_per_eval"]) * args.steps + (args.steps if precision == cd.MIXED else 0),
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cb, _ = cpu_baseline_sample(args.cpu_seconds)
+        line["cpu_baseline"] = cb
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    ws, rank, local, dist = setup_dist(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank, dist)
+        else:
+            run_ours(args, ws, rank, local, dist)
+    finally:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,14 @@
+"""classicaldft_b200: the classicalDFT F[rho] / dF/drho hot path on NVIDIA B200.
+
+The compute path is libcdft_b200.so (hand-written sm_100a CUDA kernels, cuFFT
+for the batched R2C/C2R plans) behind the C ABI of include/cdft_b200.h.
+This package is the Python host API over that ABI, mirroring the reference
+library's functional interface.
+"""
+from ._lib import FP64, MIXED, EngineError, lib  # noqa: F401
+from .functionals import (BARKER_HENDERSON, WEEKS_CHANDLER_ANDERSEN, Engine, EsFMT, FMTModel, Functional,  # noqa: F401
+                          Grid, Interaction, Model, Potential, Result, Rosenfeld, RSLT, Species, Weights,
+                          WhiteBearI, WhiteBearII, interaction_weight, make_grid, make_lennard_jones,
+                          make_ten_wolde_frenkel, make_wang_ramirez_dobnikar_frenkel, make_weights, total)
+
+__version__ = "0.1.0"

@@ -1,0 +1,104 @@
+"""ctypes binding of the engine's C ABI (include/cdft_b200.h).
+
+The shared library is built in-tree (``python -m classicaldft_b200.build``)
+and loaded from this package's directory.  There is no fallback: if the
+library is missing, importing the host API raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcdft_b200.so")
+
+CDFT_OK = 0
+CDFT_ERR_INVALID = -1
+CDFT_ERR_RUNTIME = -2
+CDFT_ERR_CUDA = -3
+CDFT_ERR_CUFFT = -4
+SCALAR_COUNT = 10
+
+MODEL_IDS = {"Rosenfeld": 0, "RSLT": 1, "WhiteBearI": 2, "WhiteBearII": 3, "esFMT": 4}
+FP64 = 0
+MIXED = 1
+POT_LJ, POT_TWF, POT_WRDF = 0, 1, 2
+SPLIT_WCA, SPLIT_BH = 0, 1
+WEIGHT_SCHEMES = {"InterpolationZero": 0, "InterpolationLinearE": 1, "InterpolationLinearF": 2,
+                  "InterpolationQuadraticF": 3, "GaussE": 4, "GaussF": 5}
+
+c_double_p = ctypes.POINTER(ctypes.c_double)
+c_long3 = ctypes.c_long * 3
+
+
+class CPotential(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("sigma", ctypes.c_double), ("epsilon", ctypes.c_double),
+                ("r_cutoff", ctypes.c_double), ("alpha", ctypes.c_double)]
+
+
+class CInteraction(ctypes.Structure):
+    _fields_ = [("species_i", ctypes.c_int), ("species_j", ctypes.c_int), ("weight_real", c_double_p),
+                ("a_vdw", ctypes.c_double)]
+
+
+class EngineError(RuntimeError):
+    """A failed C-ABI call; ``code`` is the CDFT_ERR_* status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libcdft_b200.so once; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"classicaldft_b200: CUDA library not built ({LIB_PATH} missing); "
+                          "run `python -m classicaldft_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    L.cdft_last_error.restype = ctypes.c_char_p
+    L.cdft_version.restype = ctypes.c_char_p
+    vp = ctypes.c_void_p
+    sigs = {
+        "cdft_potential_info": [ctypes.POINTER(CPotential), c_double_p],
+        "cdft_potential_attractive": [ctypes.POINTER(CPotential), ctypes.c_int, c_double_p, ctypes.c_long, c_double_p],
+        "cdft_hard_sphere_diameter": [ctypes.POINTER(CPotential), ctypes.c_double, ctypes.c_int, c_double_p],
+        "cdft_vdw_integral": [ctypes.POINTER(CPotential), ctypes.c_double, ctypes.c_int, c_double_p],
+        "cdft_interaction_weight": [c_long3, ctypes.c_double, ctypes.POINTER(CPotential), ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_double, c_double_p, c_double_p],
+        "cdft_create": [ctypes.POINTER(vp), c_long3, ctypes.c_double, ctypes.c_int, c_double_p, ctypes.c_int,
+                        ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.POINTER(CInteraction), ctypes.c_int],
+        "cdft_destroy": [vp],
+        "cdft_engine_info": [vp, ctypes.POINTER(ctypes.c_longlong)],
+        "cdft_engine_a_vdw": [vp, ctypes.c_int, c_double_p],
+        "cdft_total": [vp, vp, vp, c_double_p, vp, c_double_p],
+        "cdft_total_device": [vp, vp, vp, c_double_p, vp, vp, vp],
+    }
+    for name, args in sigs.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def check(status: int):
+    if status != CDFT_OK:
+        msg = lib().cdft_last_error().decode(errors="replace")
+        if status == CDFT_ERR_INVALID:
+            raise ValueError(msg)
+        raise EngineError(status, msg)
+
+
+def declared_symbols():
+    """Names of every function declared in include/cdft_b200.h."""
+    import re
+    hdr = os.path.join(os.path.dirname(HERE), "include", "cdft_b200.h")
+    with open(hdr) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"CDFT_API\s+[\w\s\*]+?\b(cdft_\w+)\s*\(", text)))

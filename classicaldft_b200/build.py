@@ -1,0 +1,75 @@
+"""Build the engine's shared library in-tree for sm_100a.
+
+    python -m classicaldft_b200.build            # -> classicaldft_b200/libcdft_b200.so
+
+nvcc compiles every source with -gencode arch=compute_100a,code=sm_100a and
+links cuFFT; objects go to classicaldft_b200/_build/.  A source is rebuilt
+only when it (or a header) is newer than its object.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libcdft_b200.so")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA_HOME, "bin", "nvcc") if os.path.exists(os.path.join(CUDA_HOME, "bin", "nvcc")) else "nvcc"
+
+SOURCES = ["engine.cu", "capi.cu", "physics.cpp"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+         "--expt-relaxed-constexpr", "-I", CSRC, "-I", os.path.join(ROOT, "include")]
+
+
+def _headers():
+    out = []
+    for d in (CSRC, os.path.join(ROOT, "include")):
+        for f in os.listdir(d):
+            if f.endswith((".cuh", ".hpp", ".h")):
+                out.append(os.path.join(d, f))
+    return out
+
+
+def _stale(obj, deps):
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(verbose: bool = False, extra=None) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    headers = _headers()
+    objs = []
+    for src in SOURCES:
+        path = os.path.join(CSRC, src)
+        obj = os.path.join(BUILD, src + ".o")
+        objs.append(obj)
+        if not _stale(obj, [path] + headers):
+            continue
+        cmd = [NVCC] + ARCH + FLAGS + (extra or []) + ["-c", path, "-o", obj]
+        if src.endswith(".cpp"):
+            cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-I", CSRC, "-I",
+                   os.path.join(ROOT, "include"), "-I", os.path.join(CUDA_HOME, "include"), "-c", path, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    if _stale(LIB, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + [
+            "-L", os.path.join(CUDA_HOME, "lib64"), "-lcufft", "-lcudart",
+            "-Xlinker", "-rpath," + os.path.join(CUDA_HOME, "lib64")]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose="-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,210 @@
+// The extern "C" boundary (include/cdft_b200.h).  Every entry point catches
+// all C++ exceptions and turns them into a status code plus a thread-local
+// message, so nothing unwinds across the C ABI.
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cdft_b200.h"
+#include "engine.cuh"
+#include "physics.hpp"
+
+struct cdft_engine {
+  cdft::Engine* impl;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    return CDFT_OK;
+  } catch (const cdft::Error& e) {
+    return fail(e.code(), e.what());
+  } catch (const std::invalid_argument& e) {
+    return fail(CDFT_ERR_INVALID, e.what());
+  } catch (const std::bad_alloc& e) {
+    return fail(CDFT_ERR_RUNTIME, std::string("allocation failed: ") + e.what());
+  } catch (const std::exception& e) {
+    return fail(CDFT_ERR_RUNTIME, e.what());
+  } catch (...) {
+    return fail(CDFT_ERR_RUNTIME, "unknown error");
+  }
+}
+
+cdft::Potential to_potential(const cdft_potential* pot) {
+  if (!pot) throw std::invalid_argument("potential is NULL");
+  if (!(pot->sigma > 0.0)) throw std::invalid_argument("potential sigma must be positive");
+  if (pot->type == CDFT_POT_WRDF && !(pot->r_cutoff > pot->sigma))
+    throw std::invalid_argument("WRDF potential needs r_cutoff > sigma");
+  return cdft::make_potential(pot->type, pot->sigma, pot->epsilon, pot->r_cutoff, pot->alpha);
+}
+
+void check_split(int split) {
+  if (split != CDFT_SPLIT_WCA && split != CDFT_SPLIT_BH) throw std::invalid_argument("unknown split scheme");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cdft_last_error(void) { return g_last_error.c_str(); }
+
+const char* cdft_version(void) { return "classicaldft_b200 0.1.0 (sm_100a)"; }
+
+int cdft_potential_info(const cdft_potential* pot, double out[4]) {
+  return guarded([&] {
+    if (!out) throw std::invalid_argument("out is NULL");
+    cdft::Potential p = to_potential(pot);
+    out[0] = p.epsilon_shift;
+    out[1] = p.r_min;
+    out[2] = p.v_min;
+    out[3] = p.r_zero;
+  });
+}
+
+int cdft_potential_attractive(const cdft_potential* pot, int split, const double* r, long n, double* out) {
+  return guarded([&] {
+    check_split(split);
+    if (n < 0 || (n > 0 && (!r || !out))) throw std::invalid_argument("bad radius buffers");
+    cdft::Potential p = to_potential(pot);
+    for (long i = 0; i < n; ++i) out[i] = cdft::attractive(p, r[i], split);
+  });
+}
+
+int cdft_hard_sphere_diameter(const cdft_potential* pot, double kT, int split, double* diameter) {
+  return guarded([&] {
+    check_split(split);
+    if (!(kT > 0.0) || !diameter) throw std::invalid_argument("kT must be positive and diameter non-NULL");
+    *diameter = cdft::hard_sphere_diameter(to_potential(pot), kT, split);
+  });
+}
+
+int cdft_vdw_integral(const cdft_potential* pot, double kT, int split, double* value) {
+  return guarded([&] {
+    check_split(split);
+    if (!(kT > 0.0) || !value) throw std::invalid_argument("kT must be positive and value non-NULL");
+    *value = cdft::vdw_integral(to_potential(pot), kT, split);
+  });
+}
+
+int cdft_interaction_weight(const long shape[3], double dx, const cdft_potential* pot, int split, int scheme,
+                            double kT, double* weight_out, double* a_vdw) {
+  return guarded([&] {
+    check_split(split);
+    if (!shape || shape[0] <= 0 || shape[1] <= 0 || shape[2] <= 0) throw std::invalid_argument("bad grid shape");
+    if (!(dx > 0.0) || !(kT > 0.0)) throw std::invalid_argument("dx and kT must be positive");
+    if (scheme < CDFT_WEIGHT_ZERO || scheme > CDFT_WEIGHT_GAUSS_F) throw std::invalid_argument("unknown weight scheme");
+    if (!weight_out) throw std::invalid_argument("weight_out is NULL");
+    double a = cdft::interaction_weight(shape, dx, to_potential(pot), split, scheme, kT, weight_out);
+    if (a_vdw) *a_vdw = a;
+  });
+}
+
+int cdft_create(cdft_engine** out, const long shape[3], double dx, int n_species, const double* diameters,
+                int fmt_model, double esfmt_A, double esfmt_B, int n_interactions,
+                const cdft_interaction* interactions, int precision) {
+  return guarded([&] {
+    if (!out) throw std::invalid_argument("out is NULL");
+    *out = nullptr;
+    if (!shape) throw std::invalid_argument("shape is NULL");
+    if (n_species < 1 || !diameters) throw std::invalid_argument("need at least one species diameter");
+    if (n_interactions < 0 || (n_interactions > 0 && !interactions))
+      throw std::invalid_argument("interactions is NULL");
+    cdft::EngineSpec spec;
+    for (int d = 0; d < 3; ++d) spec.shape[d] = shape[d];
+    spec.dx = dx;
+    spec.diameters.assign(diameters, diameters + n_species);
+    spec.model = fmt_model;
+    spec.esfmt_A = esfmt_A;
+    spec.esfmt_B = esfmt_B;
+    spec.precision = precision;
+    const long long N = (long long)shape[0] * shape[1] * shape[2];
+    if (shape[0] <= 0 || shape[1] <= 0 || shape[2] <= 0) throw std::invalid_argument("grid dimensions must be positive");
+    for (int m = 0; m < n_interactions; ++m) {
+      cdft::InteractionSpec is;
+      is.species_i = interactions[m].species_i;
+      is.species_j = interactions[m].species_j;
+      if (!interactions[m].weight_real) throw std::invalid_argument("interaction weight_real is NULL");
+      is.weight_real.assign(interactions[m].weight_real, interactions[m].weight_real + N);
+      is.a_vdw = interactions[m].a_vdw;
+      spec.interactions.push_back(std::move(is));
+    }
+    auto* e = new cdft_engine{nullptr};
+    try {
+      e->impl = new cdft::Engine(spec);
+    } catch (...) {
+      delete e;
+      throw;
+    }
+    *out = e;
+  });
+}
+
+int cdft_destroy(cdft_engine* engine) {
+  return guarded([&] {
+    if (!engine) return;
+    delete engine->impl;
+    delete engine;
+  });
+}
+
+int cdft_engine_info(const cdft_engine* engine, long long info[8]) {
+  return guarded([&] {
+    if (!engine || !info) throw std::invalid_argument("engine or info is NULL");
+    const cdft::Engine& e = *engine->impl;
+    info[0] = e.points();
+    info[1] = e.modes();
+    info[2] = e.species();
+    info[3] = e.params().n_chan;
+    info[4] = e.params().L.n_deriv;
+    info[5] = e.precision();
+    info[6] = e.kernels_per_eval();
+    info[7] = (long long)e.scratch_bytes();
+  });
+}
+
+int cdft_engine_a_vdw(const cdft_engine* engine, int m, double* a_vdw) {
+  return guarded([&] {
+    if (!engine || !a_vdw) throw std::invalid_argument("engine or a_vdw is NULL");
+    if (m < 0 || m >= engine->impl->params().M) throw std::invalid_argument("interaction index out of range");
+    *a_vdw = engine->impl->a_vdw(m);
+  });
+}
+
+int cdft_total(cdft_engine* engine, const double* rho, const double* vext, const double* mu, double* force,
+               double* scalars) {
+  return guarded([&] {
+    if (!engine || !rho || !mu) throw std::invalid_argument("engine, rho and mu are required");
+    cdft::Engine& e = *engine->impl;
+    const size_t bytes = sizeof(double) * e.species() * e.points();
+    cudaStream_t st = e.stream();
+    CDFT_CUDA(cudaMemcpyAsync(e.host_rho(), rho, bytes, cudaMemcpyHostToDevice, st));
+    if (vext) CDFT_CUDA(cudaMemcpyAsync(e.host_vext(), vext, bytes, cudaMemcpyHostToDevice, st));
+    e.evaluate(e.host_rho(), vext ? e.host_vext() : nullptr, mu, e.host_force(), e.host_scalars(), st);
+    if (force) CDFT_CUDA(cudaMemcpyAsync(force, e.host_force(), bytes, cudaMemcpyDeviceToHost, st));
+    double tmp[CDFT_SCALAR_COUNT];
+    CDFT_CUDA(cudaMemcpyAsync(tmp, e.host_scalars(), sizeof(tmp), cudaMemcpyDeviceToHost, st));
+    CDFT_CUDA(cudaStreamSynchronize(st));
+    if (scalars) std::memcpy(scalars, tmp, sizeof(tmp));
+  });
+}
+
+int cdft_total_device(cdft_engine* engine, const double* rho, const double* vext, const double* mu, double* force,
+                      double* scalars, void* stream) {
+  return guarded([&] {
+    if (!engine || !rho || !mu || !force || !scalars)
+      throw std::invalid_argument("engine, rho, mu, force and scalars are required");
+    engine->impl->evaluate(rho, vext, mu, force, scalars, static_cast<cudaStream_t>(stream));
+  });
+}
+
+}  // extern "C"

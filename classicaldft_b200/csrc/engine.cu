@@ -1,0 +1,295 @@
+// Engine construction (buffers, cuFFT plans, mean-field weights) and the
+// evaluation pipeline of one F[rho] + dF/drho call.
+#include "engine.cuh"
+#include "eval_kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace cdft {
+
+namespace {
+
+template <typename T>
+T* dalloc(size_t count, size_t& total) {
+  void* p = nullptr;
+  if (count == 0) return nullptr;
+  CDFT_CUDA(cudaMalloc(&p, count * sizeof(T)));
+  total += count * sizeof(T);
+  return static_cast<T*>(p);
+}
+
+template <typename K>
+int occupancy_grid(K kernel, int block, int sms, long long work) {
+  int per_sm = 0;
+  CDFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0));
+  per_sm = std::max(per_sm, 1);
+  long long want = (work + block - 1) / block;
+  long long g = std::min<long long>((long long)sms * per_sm, want);
+  return (int)std::max<long long>(g, 1);
+}
+
+__global__ void k_real_part(const double2* __restrict__ in, double* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = in[i].x;
+}
+
+__global__ void k_to_float(const double* __restrict__ in, float* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
+}  // namespace
+
+Engine::Engine(const EngineSpec& spec) {
+  for (int d = 0; d < 3; ++d)
+    if (spec.shape[d] <= 0) throw Error(-1, "Engine: grid dimensions must be positive");
+  if (!(spec.dx > 0.0)) throw Error(-1, "Engine: dx must be positive");
+  const int S = (int)spec.diameters.size();
+  if (S < 1 || S > kMaxSpecies) throw Error(-1, "Engine: number of species must be in [1, 4]");
+  for (double d : spec.diameters)
+    if (!(d > 0.0)) throw Error(-1, "Engine: hard-sphere diameters must be positive");
+  if (spec.model < kRosenfeld || spec.model > kEsFMT) throw Error(-1, "Engine: unknown FMT model id");
+  if ((int)spec.interactions.size() > kMaxInteractions) throw Error(-1, "Engine: too many interactions (max 8)");
+  if (spec.precision != kFP64 && spec.precision != kMixed) throw Error(-1, "Engine: unknown precision mode");
+  precision_ = spec.precision;
+  CDFT_CUDA(cudaGetDevice(&device_));
+
+  EvalParams& p = p_;
+  p.nx = (int)spec.shape[0];
+  p.ny = (int)spec.shape[1];
+  p.nz = (int)spec.shape[2];
+  p.nzh = p.nz / 2 + 1;
+  p.N = (long long)p.nx * p.ny * p.nz;
+  p.Nk = (long long)p.nx * p.ny * p.nzh;
+  p.dx = spec.dx;
+  p.dv = spec.dx * spec.dx * spec.dx;
+  p.inv_n = 1.0 / (double)p.N;
+  p.dkx = 2.0 * kPi / ((double)p.nx * spec.dx);
+  p.dky = 2.0 * kPi / ((double)p.ny * spec.dx);
+  p.dkz = 2.0 * kPi / ((double)p.nz * spec.dx);
+  p.S = S;
+  for (int s = 0; s < kMaxSpecies; ++s) {
+    const double R = s < S ? 0.5 * spec.diameters[s] : 0.5;
+    p.R[s] = R;
+    p.inv4piR[s] = 1.0 / (4.0 * kPi * R);
+    p.inv4piR2[s] = 1.0 / (4.0 * kPi * R * R);
+  }
+  p.model = spec.model;
+  p.A = spec.esfmt_A;
+  p.B = spec.esfmt_B;
+  const bool tensor = (p.model == kWhiteBearI || p.model == kWhiteBearII || p.model == kEsFMT);
+  p.L = ChannelLayout::make(S > 1, tensor);
+  p.M = (int)spec.interactions.size();
+  int ch = p.L.n_fmt;
+  for (int m = 0; m < p.M; ++m) {
+    const auto& it = spec.interactions[m];
+    if (it.species_i < 0 || it.species_i >= S || it.species_j < 0 || it.species_j >= S)
+      throw Error(-1, "Engine: interaction species index out of range");
+    if ((long long)it.weight_real.size() != p.N)
+      throw Error(-1, "Engine: interaction weight must have N = nx*ny*nz entries");
+    p.mf_i[m] = it.species_i;
+    p.mf_j[m] = it.species_j;
+    p.mf_chan_j[m] = ch++;
+    p.mf_chan_i[m] = (it.species_i != it.species_j) ? ch++ : -1;
+  }
+  p.n_chan = ch;
+  p.n_terms = 4 + S;
+
+  int sms = 0;
+  CDFT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+  const bool mixed = precision_ == kMixed;
+  const size_t cs = mixed ? sizeof(float2) : sizeof(double2);
+  const size_t rs = mixed ? sizeof(float) : sizeof(double);
+  size_t tot = 0;
+  rho_k_ = dalloc<char>(cs * S * p.Nk, tot);
+  chan_k_ = dalloc<char>(cs * p.n_chan * p.Nk, tot);
+  chan_r_ = dalloc<char>(rs * p.n_chan * p.N, tot);
+  deriv_r_ = dalloc<char>(rs * p.L.n_deriv * p.N, tot);
+  deriv_k_ = dalloc<char>(cs * p.L.n_deriv * p.Nk, tot);
+  force_k_ = dalloc<char>(cs * S * p.Nk, tot);
+  hs_r_ = dalloc<char>(rs * S * p.N, tot);
+  if (mixed) rho_lo_ = dalloc<char>(sizeof(float) * S * p.N, tot);
+  mf_w_ = dalloc<double>((size_t)std::max(p.M, 1) * p.Nk, tot);
+
+  // grid sizes from occupancy (148 SMs on B200)
+  const bool multi = S > 1;
+  auto pick = [&](auto kern, long long work) { return occupancy_grid(kern, 256, sms, work); };
+  if (!mixed) {
+    if (!multi && !tensor) { grid_pw_ = pick(k_pointwise<false, false, double>, p.N); grid_k_ = pick(k_forward<false, false, double2>, p.Nk); }
+    if (!multi && tensor) { grid_pw_ = pick(k_pointwise<false, true, double>, p.N); grid_k_ = pick(k_forward<false, true, double2>, p.Nk); }
+    if (multi && !tensor) { grid_pw_ = pick(k_pointwise<true, false, double>, p.N); grid_k_ = pick(k_forward<true, false, double2>, p.Nk); }
+    if (multi && tensor) { grid_pw_ = pick(k_pointwise<true, true, double>, p.N); grid_k_ = pick(k_forward<true, true, double2>, p.Nk); }
+  } else {
+    if (!multi && !tensor) { grid_pw_ = pick(k_pointwise<false, false, float>, p.N); grid_k_ = pick(k_forward<false, false, float2>, p.Nk); }
+    if (!multi && tensor) { grid_pw_ = pick(k_pointwise<false, true, float>, p.N); grid_k_ = pick(k_forward<false, true, float2>, p.Nk); }
+    if (multi && !tensor) { grid_pw_ = pick(k_pointwise<true, false, float>, p.N); grid_k_ = pick(k_forward<true, false, float2>, p.Nk); }
+    if (multi && tensor) { grid_pw_ = pick(k_pointwise<true, true, float>, p.N); grid_k_ = pick(k_forward<true, true, float2>, p.Nk); }
+  }
+  partials_ = dalloc<double>((size_t)grid_pw_ * p.n_terms, tot);
+
+  build_plans();
+  upload_mean_field(spec);
+  scratch_bytes_ = tot;
+
+  CDFT_CUDA(cudaMalloc(&h_rho_, sizeof(double) * S * p.N));
+  CDFT_CUDA(cudaMalloc(&h_vext_, sizeof(double) * S * p.N));
+  CDFT_CUDA(cudaMalloc(&h_force_, sizeof(double) * S * p.N));
+  CDFT_CUDA(cudaMalloc(&h_scalars_, sizeof(double) * kScalarCount));
+  CDFT_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+}
+
+Engine::~Engine() {
+  if (plans_made_) {
+    cufftDestroy(plan_rho_);
+    cufftDestroy(plan_chan_);
+    cufftDestroy(plan_deriv_);
+    cufftDestroy(plan_force_);
+  }
+  for (void* q : {rho_k_, chan_k_, chan_r_, deriv_r_, deriv_k_, force_k_, hs_r_, rho_lo_, (void*)mf_w_,
+                  (void*)partials_, fft_work_, (void*)h_rho_, (void*)h_vext_, (void*)h_force_, (void*)h_scalars_})
+    if (q) cudaFree(q);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::build_plans() {
+  const EvalParams& p = p_;
+  const bool mixed = precision_ == kMixed;
+  long long n[3] = {p.nx, p.ny, p.nz};
+  size_t ws[4] = {0, 0, 0, 0};
+  cufftHandle* hs[4] = {&plan_rho_, &plan_chan_, &plan_deriv_, &plan_force_};
+  const int batch[4] = {p.S, p.n_chan, p.L.n_deriv, p.S};
+  const cufftType fwd = mixed ? CUFFT_R2C : CUFFT_D2Z;
+  const cufftType inv = mixed ? CUFFT_C2R : CUFFT_Z2D;
+  const cufftType type[4] = {fwd, inv, fwd, inv};
+  for (int i = 0; i < 4; ++i) {
+    CDFT_CUFFT(cufftCreate(hs[i]));
+    CDFT_CUFFT(cufftSetAutoAllocation(*hs[i], 0));
+    const bool r2c = (i == 0 || i == 2);
+    CDFT_CUFFT(cufftMakePlanMany64(*hs[i], 3, n, nullptr, 1, r2c ? p.N : p.Nk, nullptr, 1, r2c ? p.Nk : p.N,
+                                   type[i], batch[i], &ws[i]));
+  }
+  plans_made_ = true;
+  const size_t wmax = std::max(std::max(ws[0], ws[1]), std::max(ws[2], ws[3]));
+  if (wmax > 0) {
+    CDFT_CUDA(cudaMalloc(&fft_work_, wmax));
+    scratch_bytes_ += wmax;
+  }
+  for (int i = 0; i < 4; ++i) CDFT_CUFFT(cufftSetWorkArea(*hs[i], fft_work_));
+}
+
+void Engine::upload_mean_field(const EngineSpec& spec) {
+  const EvalParams& p = p_;
+  a_vdw_.clear();
+  if (p.M == 0) return;
+  // FFT the real-space weights once (mean_field.hpp:194) with a temporary
+  // FP64 plan; keep the real part (the weight is real and even).
+  double* wr = nullptr;
+  double2* wk = nullptr;
+  CDFT_CUDA(cudaMalloc(&wr, sizeof(double) * p.N));
+  CDFT_CUDA(cudaMalloc(&wk, sizeof(double2) * p.Nk));
+  cufftHandle plan = 0;
+  try {
+    CDFT_CUFFT(cufftPlan3d(&plan, p.nx, p.ny, p.nz, CUFFT_D2Z));
+    for (int m = 0; m < p.M; ++m) {
+      CDFT_CUDA(cudaMemcpy(wr, spec.interactions[m].weight_real.data(), sizeof(double) * p.N, cudaMemcpyHostToDevice));
+      CDFT_CUFFT(cufftExecD2Z(plan, wr, wk));
+      k_real_part<<<256, 256>>>(wk, mf_w_ + m * p.Nk, p.Nk);
+      CDFT_CUDA(cudaGetLastError());
+      a_vdw_.push_back(spec.interactions[m].a_vdw);
+    }
+    CDFT_CUDA(cudaDeviceSynchronize());
+  } catch (...) {
+    if (plan) cufftDestroy(plan);
+    cudaFree(wr);
+    cudaFree(wk);
+    throw;
+  }
+  cufftDestroy(plan);
+  cudaFree(wr);
+  cudaFree(wk);
+}
+
+template <typename R, typename C2>
+void Engine::run(const double* rho, const double* vext, const double* mu, double* force, double* scalars,
+                 cudaStream_t stream) {
+  const EvalParams& p = p_;
+  const bool multi = p.L.multi;
+  const bool tensor = p.L.tensor;
+  constexpr bool mixed = sizeof(R) == sizeof(float);
+  for (cufftHandle h : {plan_rho_, plan_chan_, plan_deriv_, plan_force_}) CDFT_CUFFT(cufftSetStream(h, stream));
+
+  C2* rho_k = static_cast<C2*>(rho_k_);
+  C2* chan_k = static_cast<C2*>(chan_k_);
+  R* chan_r = static_cast<R*>(chan_r_);
+  R* deriv_r = static_cast<R*>(deriv_r_);
+  C2* deriv_k = static_cast<C2*>(deriv_k_);
+  C2* force_k = static_cast<C2*>(force_k_);
+  R* hs_r = static_cast<R*>(hs_r_);
+
+  // 1. rho_k = r2c(rho)
+  if constexpr (mixed) {
+    k_to_float<<<grid_pw_, 256, 0, stream>>>(rho, static_cast<float*>(rho_lo_), p.S * p.N);
+    CDFT_CUFFT(cufftExecR2C(plan_rho_, static_cast<float*>(rho_lo_), reinterpret_cast<cufftComplex*>(rho_k)));
+  } else {
+    CDFT_CUFFT(cufftExecD2Z(plan_rho_, const_cast<double*>(rho), reinterpret_cast<cufftDoubleComplex*>(rho_k)));
+  }
+  // 2. weighted-density channels in k-space
+  if (!multi && !tensor) k_forward<false, false, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
+  if (!multi && tensor) k_forward<false, true, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
+  if (multi && !tensor) k_forward<true, false, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
+  if (multi && tensor) k_forward<true, true, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
+  CDFT_CUDA(cudaGetLastError());
+  // 3. n_alpha(r)
+  if constexpr (mixed)
+    CDFT_CUFFT(cufftExecC2R(plan_chan_, reinterpret_cast<cufftComplex*>(chan_k), reinterpret_cast<float*>(chan_r)));
+  else
+    CDFT_CUFFT(cufftExecZ2D(plan_chan_, reinterpret_cast<cufftDoubleComplex*>(chan_k), reinterpret_cast<double*>(chan_r)));
+  // 4. pointwise Phi / dPhi + local terms + reductions
+  PointwiseArgs a;
+  a.rho = rho;
+  a.vext = vext;
+  for (int s = 0; s < kMaxSpecies; ++s) a.mu[s] = s < p.S ? mu[s] : 0.0;
+  a.force = force;
+  a.partials = partials_;
+  if (!multi && !tensor) k_pointwise<false, false, R><<<grid_pw_, 256, 0, stream>>>(p, chan_r, deriv_r, a);
+  if (!multi && tensor) k_pointwise<false, true, R><<<grid_pw_, 256, 0, stream>>>(p, chan_r, deriv_r, a);
+  if (multi && !tensor) k_pointwise<true, false, R><<<grid_pw_, 256, 0, stream>>>(p, chan_r, deriv_r, a);
+  if (multi && tensor) k_pointwise<true, true, R><<<grid_pw_, 256, 0, stream>>>(p, chan_r, deriv_r, a);
+  CDFT_CUDA(cudaGetLastError());
+  // 5. D_k = r2c(dPhi channels)
+  if constexpr (mixed)
+    CDFT_CUFFT(cufftExecR2C(plan_deriv_, reinterpret_cast<float*>(deriv_r), reinterpret_cast<cufftComplex*>(deriv_k)));
+  else
+    CDFT_CUFFT(cufftExecD2Z(plan_deriv_, reinterpret_cast<double*>(deriv_r), reinterpret_cast<cufftDoubleComplex*>(deriv_k)));
+  // 6. back-convolution
+  if (!multi && !tensor) k_backward<false, false, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
+  if (!multi && tensor) k_backward<false, true, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
+  if (multi && !tensor) k_backward<true, false, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
+  if (multi && tensor) k_backward<true, true, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
+  CDFT_CUDA(cudaGetLastError());
+  // 7. force += c2r(F_k) dV
+  if constexpr (mixed)
+    CDFT_CUFFT(cufftExecC2R(plan_force_, reinterpret_cast<cufftComplex*>(force_k), reinterpret_cast<float*>(hs_r)));
+  else
+    CDFT_CUFFT(cufftExecZ2D(plan_force_, reinterpret_cast<cufftDoubleComplex*>(force_k), reinterpret_cast<double*>(hs_r)));
+  k_epilogue<R><<<grid_pw_, 256, 0, stream>>>(p.S * p.N, p.dv, hs_r, force);
+  CDFT_CUDA(cudaGetLastError());
+  // 8. scalars
+  MuArgs ma;
+  for (int s = 0; s < kMaxSpecies; ++s) ma.mu[s] = a.mu[s];
+  k_reduce_final<<<1, 32 * (4 + kMaxSpecies), 0, stream>>>(partials_, grid_pw_, p, ma, scalars);
+  CDFT_CUDA(cudaGetLastError());
+}
+
+void Engine::evaluate(const double* rho, const double* vext, const double* mu, double* force, double* scalars,
+                      cudaStream_t stream) {
+  if (!rho || !force || !scalars || !mu) throw Error(-1, "evaluate: rho, mu, force and scalars are required");
+  if (precision_ == kMixed)
+    run<float, float2>(rho, vext, mu, force, scalars, stream);
+  else
+    run<double, double2>(rho, vext, mu, force, scalars, stream);
+}
+
+}  // namespace cdft

@@ -1,0 +1,107 @@
+// The evaluation engine: one grid, its species, FMT model and mean-field
+// interactions, with every buffer, cuFFT plan and weight resident in HBM.
+//
+// An Engine is what the reference's (Model, Weights) pair becomes on the GPU
+// (include/dft/functionals/functionals.hpp:19-33): built once, immutable
+// afterwards, evaluated many times.  It is not thread-safe: one stream per
+// engine, as FFTW plans are per-object in the reference.
+#pragma once
+
+#include <cufft.h>
+
+#include <string>
+#include <vector>
+
+#include "cdft_common.cuh"
+
+namespace cdft {
+
+enum Precision : int { kFP64 = 0, kMixed = 1 };
+
+struct InteractionSpec {
+  int species_i = 0, species_j = 0;
+  std::vector<double> weight_real;  // N doubles: cell weight * dV / N (mean_field.hpp:188)
+  double a_vdw = 0.0;
+};
+
+struct EngineSpec {
+  long shape[3] = {0, 0, 0};
+  double dx = 0.0;
+  std::vector<double> diameters;
+  int model = kWhiteBearII;
+  double esfmt_A = 1.0, esfmt_B = 0.0;
+  std::vector<InteractionSpec> interactions;
+  int precision = kFP64;
+};
+
+class Engine {
+ public:
+  explicit Engine(const EngineSpec& spec);
+  ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  // Full evaluation on device data (functionals.hpp:64-95).
+  //   rho   : S*N doubles (device), species-major
+  //   vext  : S*N doubles (device) or null (no external field)
+  //   mu    : S chemical potentials (beta mu units), host
+  //   force : S*N doubles (device) receives dOmega/drho * dV, or null
+  //   scalars: kScalarCount doubles (device): F, Omega, F_id, F_ext, F_hs, F_mf, N_s
+  void evaluate(const double* rho, const double* vext, const double* mu, double* force, double* scalars,
+                cudaStream_t stream);
+
+  const EvalParams& params() const { return p_; }
+  int species() const { return p_.S; }
+  long long points() const { return p_.N; }
+  long long modes() const { return p_.Nk; }
+  int precision() const { return precision_; }
+  double a_vdw(int m) const { return a_vdw_[m]; }
+  int kernels_per_eval() const { return 5; }
+  // Scratch bytes held beyond inputs and outputs.
+  size_t scratch_bytes() const { return scratch_bytes_; }
+
+  // Staging buffers of the host-pointer API.
+  double* host_rho() { return h_rho_; }
+  double* host_vext() { return h_vext_; }
+  double* host_force() { return h_force_; }
+  double* host_scalars() { return h_scalars_; }
+  cudaStream_t stream() const { return stream_; }
+
+ private:
+  void build_plans();
+  void upload_mean_field(const EngineSpec& spec);
+  template <typename R, typename C2>
+  void run(const double* rho, const double* vext, const double* mu, double* force, double* scalars,
+           cudaStream_t stream);
+
+  EvalParams p_{};
+  int precision_ = kFP64;
+  int device_ = 0;
+  int grid_k_ = 0, grid_pw_ = 0;
+  std::vector<double> a_vdw_;
+
+  // FP64 pipeline buffers (the mixed pipeline views them as float storage).
+  void* rho_k_ = nullptr;     // S * Nk complex
+  void* chan_k_ = nullptr;    // C * Nk complex
+  void* chan_r_ = nullptr;    // C * N real
+  void* deriv_r_ = nullptr;   // D * N real
+  void* deriv_k_ = nullptr;   // D * Nk complex
+  void* force_k_ = nullptr;   // S * Nk complex
+  void* hs_r_ = nullptr;      // S * N real
+  void* rho_lo_ = nullptr;    // S * N float (mixed precision input copy)
+  double* mf_w_ = nullptr;    // M * Nk real (FP64)
+  double* partials_ = nullptr;
+  void* fft_work_ = nullptr;
+  size_t scratch_bytes_ = 0;
+
+  cufftHandle plan_rho_ = 0, plan_chan_ = 0, plan_deriv_ = 0, plan_force_ = 0;
+  bool plans_made_ = false;
+
+  double* h_rho_ = nullptr;   // device staging for host API
+  double* h_vext_ = nullptr;
+  double* h_force_ = nullptr;
+  double* h_scalars_ = nullptr;
+  cudaStream_t stream_ = nullptr;
+};
+
+}  // namespace cdft

@@ -1,0 +1,229 @@
+// Pointwise FMT free-energy density Phi(n_alpha) and its partial derivatives,
+// for all five models of include/dft/functionals/fmt/models.hpp.
+//
+// Everything is templated on the scalar type T: T = double gives the primal
+// evaluation of the reference (models.hpp:49-81); T = Dual carries a tangent
+// through the same arithmetic, which turns the hand-written adjoint dPhi into
+// its directional derivative (forward-over-reverse Hessian-vector product).
+//
+// The f-function derivatives are closed forms of the exact expressions the
+// reference differentiates with autodiff (models.hpp:59-61), including the
+// eta < 1e-6 Taylor branches (models.hpp:200, 250, 282, 290).
+#pragma once
+
+#include "cdft_common.cuh"
+
+namespace cdft {
+
+// ---------------------------------------------------------------- duals
+
+struct Dual {
+  double v, d;
+};
+__host__ __device__ inline Dual mk(double v, double d = 0.0) { return Dual{v, d}; }
+__host__ __device__ inline Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__host__ __device__ inline Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__host__ __device__ inline Dual operator-(Dual a) { return {-a.v, -a.d}; }
+__host__ __device__ inline Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__host__ __device__ inline Dual operator/(Dual a, Dual b) {
+  double q = a.v / b.v;
+  return {q, (a.d - q * b.d) / b.v};
+}
+__host__ __device__ inline Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
+__host__ __device__ inline Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
+__host__ __device__ inline Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
+__host__ __device__ inline Dual operator-(double a, Dual b) { return {a - b.v, -b.d}; }
+__host__ __device__ inline Dual operator*(Dual a, double b) { return {a.v * b, a.d * b}; }
+__host__ __device__ inline Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
+__host__ __device__ inline Dual operator/(Dual a, double b) { return {a.v / b, a.d / b}; }
+__host__ __device__ inline Dual operator/(double a, Dual b) {
+  double q = a / b.v;
+  return {q, -q * b.d / b.v};
+}
+__device__ inline Dual dlog(Dual a) { return {log(a.v), a.d / a.v}; }
+__device__ inline double dlog(double a) { return log(a); }
+__host__ __device__ inline double val(double a) { return a; }
+__host__ __device__ inline double val(Dual a) { return a.v; }
+__host__ __device__ inline double zero_like(double) { return 0.0; }
+__host__ __device__ inline Dual zero_like(Dual) { return Dual{0.0, 0.0}; }
+template <class T> __host__ __device__ inline T cst(double c) { return T(c); }
+template <> __host__ __device__ inline Dual cst<Dual>(double c) { return Dual{c, 0.0}; }
+
+// ------------------------------------------------------------- measures
+
+// Symmetric tensor stored as xx, xy, xz, yy, yz, zz (tensor_index order).
+template <class T>
+struct Measures {
+  T eta, n0, n1, n2;
+  T v0[3], v1[3];
+  T t[6];
+};
+
+template <class T>
+struct MeasureDerivs {
+  T d_eta, d_n0, d_n1, d_n2;
+  T d_v0[3], d_v1[3];
+  T d_t[6];  // dPhi/dT_ij for i <= j (the matrix is symmetric)
+};
+
+template <class T>
+struct FVals {
+  T f1, df1, f2, df2, f3, df3;
+};
+
+// f1, f2, f3 and their eta-derivatives for one model (models.hpp:153-324).
+template <class T>
+__device__ inline FVals<T> fmt_f(int model, T eta) {
+  FVals<T> r;
+  const double ev = val(eta);
+  T e = 1.0 - eta;
+  r.f1 = dlog(e);
+  r.df1 = -1.0 / e;
+  if (model == kWhiteBearII) {
+    if (ev < 1e-6) {
+      r.f2 = 1.0 + eta * (1.0 + eta * (10.0 / 9.0 + (7.0 / 6.0) * eta));
+      r.df2 = 1.0 + eta * (2.0 * (10.0 / 9.0) + 3.0 * (7.0 / 6.0) * eta);
+    } else {
+      T lg = dlog(e);
+      r.f2 = (1.0 / 3.0) + (4.0 / 3.0) / e + 2.0 / (3.0 * eta) * lg;
+      r.df2 = (4.0 / 3.0) / (e * e) - (2.0 / (3.0 * eta * eta)) * lg - 2.0 / (3.0 * eta * e);
+    }
+  } else {
+    r.f2 = 1.0 / e;
+    r.df2 = 1.0 / (e * e);
+  }
+  if (model == kRosenfeld || model == kEsFMT) {
+    r.f3 = 1.0 / (e * e);
+    r.df3 = 2.0 / (e * e * e);
+  } else if (model == kRSLT || model == kWhiteBearI) {
+    if (ev < 1e-6) {
+      if (model == kRSLT) {
+        r.f3 = 1.0 + (2.0 / 3.0) * eta + 0.5 * eta * eta;
+        r.df3 = (2.0 / 3.0) + eta;
+      } else {
+        r.f3 = 1.5 + eta * (8.0 / 3.0 + eta * (15.0 / 4.0 + (24.0 / 5.0) * eta));
+        r.df3 = 8.0 / 3.0 + eta * (2.0 * (15.0 / 4.0) + 3.0 * (24.0 / 5.0) * eta);
+      }
+    } else {
+      T h = eta * e * e;
+      T lg = dlog(e);
+      r.f3 = 1.0 / h + lg / (eta * eta);
+      r.df3 = -(e * (e - 2.0 * eta)) / (h * h) - 1.0 / (e * eta * eta) - 2.0 * lg / (eta * eta * eta);
+    }
+  } else {  // WhiteBearII
+    if (ev < 1e-6) {
+      r.f3 = 1.5 + (7.0 / 3.0) * eta + 3.25 * eta * eta + 4.2 * eta * eta * eta;
+      r.df3 = 7.0 / 3.0 + 6.5 * eta + 12.6 * eta * eta;
+    } else {
+      T g = 1.0 - 3.0 * eta + eta * eta;
+      T gp = -3.0 + 2.0 * eta;
+      T h = eta * e * e;
+      T hp = e * (e - 2.0 * eta);
+      T lg = dlog(e);
+      r.f3 = -(g / h) - lg / (eta * eta);
+      r.df3 = -(gp * h - g * hp) / (h * h) + 1.0 / (e * eta * eta) + 2.0 * lg / (eta * eta * eta);
+    }
+  }
+  return r;
+}
+
+// Phi and all partial derivatives at one point (models.hpp:22-81, 169-357).
+// Returns false (and leaves outputs untouched) where eta < 1e-30: the
+// reference skips those points (hard_sphere.hpp:199-200).
+template <class T>
+__device__ inline bool fmt_phi_dphi(int model, double A, double B, bool tensor, const Measures<T>& m, T& phi,
+                                    MeasureDerivs<T>& dm) {
+  if (val(m.eta) < 1e-30) return false;
+  constexpr double INV_24PI = 1.0 / (24.0 * kPi);
+  constexpr double INV_8PI = 1.0 / (8.0 * kPi);
+  constexpr double INV_4PI = 1.0 / (4.0 * kPi);
+  constexpr double INV_36PI = 1.0 / (36.0 * kPi);
+
+  // inner products (measures.hpp:34-44); T symmetric
+  const T* t = m.t;
+  T txx = t[0], txy = t[1], txz = t[2], tyy = t[3], tyz = t[4], tzz = t[5];
+  T dot01 = m.v0[0] * m.v1[0] + m.v0[1] * m.v1[1] + m.v0[2] * m.v1[2];
+  T dot11 = m.v1[0] * m.v1[0] + m.v1[1] * m.v1[1] + m.v1[2] * m.v1[2];
+  T tt[6];   // TT = T*T (symmetric)
+  T tv[3];   // T v1
+  T trT2 = zero_like(m.eta), trT3 = zero_like(m.eta), qf = zero_like(m.eta);
+  if (tensor) {
+    tt[0] = txx * txx + txy * txy + txz * txz;
+    tt[1] = txx * txy + txy * tyy + txz * tyz;
+    tt[2] = txx * txz + txy * tyz + txz * tzz;
+    tt[3] = txy * txy + tyy * tyy + tyz * tyz;
+    tt[4] = txy * txz + tyy * tyz + tyz * tzz;
+    tt[5] = txz * txz + tyz * tyz + tzz * tzz;
+    trT2 = tt[0] + tt[3] + tt[5];
+    trT3 = tt[0] * txx + tt[3] * tyy + tt[5] * tzz + 2.0 * (tt[1] * txy + tt[2] * txz + tt[4] * tyz);
+    tv[0] = txx * m.v1[0] + txy * m.v1[1] + txz * m.v1[2];
+    tv[1] = txy * m.v1[0] + tyy * m.v1[1] + tyz * m.v1[2];
+    tv[2] = txz * m.v1[0] + tyz * m.v1[1] + tzz * m.v1[2];
+    qf = m.v1[0] * tv[0] + m.v1[1] * tv[1] + m.v1[2] * tv[2];
+  }
+
+  // Phi3 and its partials
+  T p3, dp3_n2, dp3_v[3];
+  const T n2 = m.n2;
+  if (model == kRosenfeld) {
+    p3 = INV_24PI * (n2 * n2 * n2 - 3.0 * n2 * dot11);
+    dp3_n2 = INV_8PI * (n2 * n2 - dot11);
+    for (int a = 0; a < 3; ++a) dp3_v[a] = -INV_4PI * n2 * m.v1[a];
+  } else if (model == kRSLT) {
+    if (val(n2) < 1e-30) {
+      p3 = zero_like(n2);
+      dp3_n2 = zero_like(n2);
+      for (int a = 0; a < 3; ++a) dp3_v[a] = zero_like(n2);
+    } else {
+      T xi = dot11 / (n2 * n2);
+      if (val(xi) > 1.0) xi = cst<T>(1.0);  // std::min(xi, 1.0), models.hpp:210
+      T q = 1.0 - xi;
+      p3 = INV_36PI * n2 * n2 * n2 * q * q * q;
+      dp3_n2 = INV_36PI * 3.0 * n2 * n2 * q * q * (1.0 + xi);
+      for (int a = 0; a < 3; ++a) dp3_v[a] = INV_36PI * (-6.0) * n2 * q * q * m.v1[a];
+    }
+  } else if (model == kWhiteBearI || model == kWhiteBearII) {
+    p3 = INV_24PI * 3.0 * (n2 * trT2 - n2 * dot11 + qf - trT3);
+    dp3_n2 = INV_24PI * 3.0 * (trT2 - dot11);
+    for (int a = 0; a < 3; ++a) dp3_v[a] = INV_24PI * (-6.0 * n2 * m.v1[a] + 6.0 * tv[a]);
+  } else {  // esFMT(A, B)
+    T phi_a = n2 * n2 * n2 - 3.0 * n2 * dot11 + 3.0 * qf - trT3;
+    T phi_b = n2 * n2 * n2 - 3.0 * n2 * trT2 + 2.0 * trT3;
+    p3 = INV_24PI * (A * phi_a + B * phi_b);
+    dp3_n2 = INV_24PI * (A * (3.0 * n2 * n2 - 3.0 * dot11) + B * (3.0 * n2 * n2 - 3.0 * trT2));
+    for (int a = 0; a < 3; ++a) dp3_v[a] = INV_24PI * A * (-6.0 * n2 * m.v1[a] + 6.0 * tv[a]);
+  }
+
+  FVals<T> f = fmt_f<T>(model, m.eta);
+  T c2 = m.n1 * n2 - dot01;
+  phi = -m.n0 * f.f1 + c2 * f.f2 + p3 * f.f3;
+  dm.d_eta = -m.n0 * f.df1 + c2 * f.df2 + p3 * f.df3;
+  dm.d_n0 = -f.f1;
+  dm.d_n1 = n2 * f.f2;
+  dm.d_n2 = m.n1 * f.f2 + dp3_n2 * f.f3;
+  for (int a = 0; a < 3; ++a) {
+    dm.d_v0[a] = -m.v1[a] * f.f2;
+    dm.d_v1[a] = -m.v0[a] * f.f2 + dp3_v[a] * f.f3;
+  }
+  if (tensor) {
+    // dPhi3/dT_ij (models.hpp:39-45, 348-357); T and TT symmetric
+    for (int i = 0; i < 3; ++i) {
+      for (int j = i; j < 3; ++j) {
+        const int c = tensor_index(i, j);
+        T vv = m.v1[i] * m.v1[j];
+        T d;
+        if (model == kEsFMT) {
+          d = INV_8PI * A * (vv - tt[c]) + INV_4PI * B * (-n2 * t[c] + tt[c]);
+        } else {
+          d = INV_8PI * (vv + 2.0 * n2 * t[c] - 3.0 * tt[c]);
+        }
+        dm.d_t[c] = d * f.f3;
+      }
+    }
+  } else {
+    for (int c = 0; c < 6; ++c) dm.d_t[c] = zero_like(m.eta);
+  }
+  return true;
+}
+
+}  // namespace cdft

@@ -1,0 +1,344 @@
+"""Host-side mirror of the reference's functional API, backed by the GPU engine.
+
+Names, argument meaning and error behaviour follow the reference
+(include/dft/grid.hpp, types.hpp, physics/{potentials,interactions,model}.hpp,
+functionals/{functionals,functional,types}.hpp); every evaluation runs
+through the C ABI of libcdft_b200.so on the current CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+
+# ----------------------------------------------------------------- grid
+
+
+@dataclass(frozen=True)
+class Grid:
+    """grid.hpp:26-83: periodic uniform grid, z-fastest flat index."""
+
+    dx: float
+    box_size: tuple
+    shape: tuple
+
+    @property
+    def cell_volume(self) -> float:
+        return self.dx * self.dx * self.dx
+
+    @property
+    def total_points(self) -> int:
+        return int(self.shape[0] * self.shape[1] * self.shape[2])
+
+    def flat_index(self, ix, iy, iz):
+        return iz + self.shape[2] * (iy + self.shape[1] * ix)
+
+    def boundary_mask(self) -> np.ndarray:
+        """grid.hpp:67-82."""
+        nx, ny, nz = self.shape
+        m = np.zeros(self.shape, dtype=np.uint8)
+        m[[0, nx - 1], :, :] = 1
+        m[:, [0, ny - 1], :] = 1
+        m[:, :, [0, nz - 1]] = 1
+        return m.reshape(-1)
+
+
+def make_grid(dx: float, box) -> Grid:
+    """grid.hpp:87-108: raises ValueError (std::invalid_argument) on bad input."""
+    if dx <= 0.0:
+        raise ValueError(f"make_grid: dx must be positive, got {dx}")
+    shape = []
+    for b in box:
+        if b <= 0.0:
+            raise ValueError(f"make_grid: box dimension must be positive, got {b}")
+        n = b / dx
+        ni = int(round(n))
+        if abs(n - ni) > 1e-10:
+            raise ValueError(f"make_grid: box dimension {b} is not commensurate with dx={dx}")
+        shape.append(ni)
+    return Grid(dx=float(dx), box_size=tuple(float(b) for b in box), shape=tuple(shape))
+
+
+# ------------------------------------------------------------ potentials
+
+WEEKS_CHANDLER_ANDERSEN = "WeeksChandlerAndersen"
+BARKER_HENDERSON = "BarkerHenderson"
+_SPLIT = {WEEKS_CHANDLER_ANDERSEN: _lib.SPLIT_WCA, BARKER_HENDERSON: _lib.SPLIT_BH}
+
+
+@dataclass
+class Potential:
+    """potentials.hpp:248-307: LennardJones / TenWoldeFrenkel / WRDF."""
+
+    type: int
+    sigma: float
+    epsilon: float
+    r_cutoff: float
+    alpha: float = 50.0
+
+    def _c(self):
+        return _lib.CPotential(self.type, self.sigma, self.epsilon, self.r_cutoff, self.alpha)
+
+    def info(self):
+        out = (ctypes.c_double * 4)()
+        _lib.check(_lib.lib().cdft_potential_info(ctypes.byref(self._c()), out))
+        return {"epsilon_shift": out[0], "r_min": out[1], "v_min": out[2], "r_zero": out[3]}
+
+    def attractive(self, r, split=WEEKS_CHANDLER_ANDERSEN):
+        r = np.ascontiguousarray(np.atleast_1d(r), dtype=np.float64)
+        out = np.empty_like(r)
+        _lib.check(_lib.lib().cdft_potential_attractive(
+            ctypes.byref(self._c()), _SPLIT[split], r.ctypes.data_as(_lib.c_double_p), r.size,
+            out.ctypes.data_as(_lib.c_double_p)))
+        return out
+
+    def hard_sphere_diameter(self, kT, split=WEEKS_CHANDLER_ANDERSEN) -> float:
+        d = ctypes.c_double()
+        _lib.check(_lib.lib().cdft_hard_sphere_diameter(ctypes.byref(self._c()), kT, _SPLIT[split], ctypes.byref(d)))
+        return d.value
+
+    def vdw_integral(self, kT, split=WEEKS_CHANDLER_ANDERSEN) -> float:
+        d = ctypes.c_double()
+        _lib.check(_lib.lib().cdft_vdw_integral(ctypes.byref(self._c()), kT, _SPLIT[split], ctypes.byref(d)))
+        return d.value
+
+
+def make_lennard_jones(sigma, epsilon, r_cutoff=-1.0) -> Potential:
+    """potentials.hpp:311-325."""
+    return Potential(_lib.POT_LJ, sigma, epsilon, r_cutoff)
+
+
+def make_ten_wolde_frenkel(sigma, epsilon, r_cutoff=-1.0, alpha=50.0) -> Potential:
+    """potentials.hpp:327-346."""
+    return Potential(_lib.POT_TWF, sigma, epsilon, r_cutoff, alpha)
+
+
+def make_wang_ramirez_dobnikar_frenkel(sigma, epsilon, r_cutoff=3.0) -> Potential:
+    """potentials.hpp:348-368."""
+    return Potential(_lib.POT_WRDF, sigma, epsilon, r_cutoff)
+
+
+# -------------------------------------------------------- model / species
+
+
+@dataclass
+class Species:
+    """types.hpp:25-28."""
+
+    name: str
+    hard_sphere_diameter: float
+
+
+@dataclass
+class Interaction:
+    """interactions.hpp:23-30."""
+
+    species_i: int
+    species_j: int
+    potential: Potential
+    split: str = WEEKS_CHANDLER_ANDERSEN
+    weight_scheme: str = "InterpolationQuadraticF"
+
+
+@dataclass
+class Model:
+    """physics/model.hpp:15-20."""
+
+    grid: Grid
+    species: list
+    interactions: list = field(default_factory=list)
+    temperature: float = 1.0
+
+
+@dataclass(frozen=True)
+class FMTModel:
+    """fmt/models.hpp:363-419: Rosenfeld, RSLT, WhiteBearI, WhiteBearII, esFMT(A, B)."""
+
+    name: str
+    A: float = 1.0
+    B: float = 0.0
+
+    def __post_init__(self):
+        if self.name not in _lib.MODEL_IDS:
+            raise ValueError(f"Unknown FMT model: {self.name}")
+
+    @property
+    def needs_tensor(self) -> bool:
+        return self.name in ("WhiteBearI", "WhiteBearII", "esFMT")
+
+    @staticmethod
+    def from_name(name: str) -> "FMTModel":
+        return FMTModel(name)
+
+
+def Rosenfeld():
+    return FMTModel("Rosenfeld")
+
+
+def RSLT():
+    return FMTModel("RSLT")
+
+
+def WhiteBearI():
+    return FMTModel("WhiteBearI")
+
+
+def WhiteBearII():
+    return FMTModel("WhiteBearII")
+
+
+def EsFMT(A=1.0, B=0.0):
+    return FMTModel("esFMT", A, B)
+
+
+def interaction_weight(inter: Interaction, grid: Grid, kT: float):
+    """mean_field.hpp:146-196 up to the FFT: (real-space weight * dV/N, a_vdw)."""
+    out = np.empty(grid.total_points, dtype=np.float64)
+    a = ctypes.c_double()
+    _lib.check(_lib.lib().cdft_interaction_weight(
+        _lib.c_long3(*grid.shape), grid.dx, ctypes.byref(inter.potential._c()), _SPLIT[inter.split],
+        _lib.WEIGHT_SCHEMES[inter.weight_scheme], kT, out.ctypes.data_as(_lib.c_double_p), ctypes.byref(a)))
+    return out, a.value
+
+
+# ------------------------------------------------------------------ engine
+
+
+class Engine:
+    """An evaluation engine on the current CUDA device (owns a cdft_engine)."""
+
+    def __init__(self, fmt_model: FMTModel, model: Model, precision: int = _lib.FP64):
+        L = _lib.lib()
+        g = model.grid
+        diam = np.array([sp.hard_sphere_diameter for sp in model.species], dtype=np.float64)
+        self._keep = []
+        inters = (_lib.CInteraction * max(1, len(model.interactions)))()
+        self.a_vdw = []
+        for m, it in enumerate(model.interactions):
+            w, a = interaction_weight(it, g, model.temperature)
+            self._keep.append(w)
+            inters[m] = _lib.CInteraction(it.species_i, it.species_j, w.ctypes.data_as(_lib.c_double_p), a)
+            self.a_vdw.append(a)
+        h = ctypes.c_void_p()
+        _lib.check(L.cdft_create(ctypes.byref(h), _lib.c_long3(*g.shape), g.dx, len(model.species),
+                                 diam.ctypes.data_as(_lib.c_double_p), _lib.MODEL_IDS[fmt_model.name],
+                                 fmt_model.A, fmt_model.B, len(model.interactions), inters, precision))
+        self._keep = []
+        self.handle = h
+        self.S = len(model.species)
+        self.N = g.total_points
+        self.precision = precision
+        info = (ctypes.c_longlong * 8)()
+        _lib.check(L.cdft_engine_info(h, info))
+        self.info = {"N": info[0], "Nk": info[1], "S": info[2], "channels": info[3], "deriv_channels": info[4],
+                     "precision": info[5], "kernels_per_eval": info[6], "scratch_bytes": info[7]}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.lib().cdft_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def total_host(self, rho: np.ndarray, mu, vext=None, want_force=True):
+        """cdft_total on host arrays: rho (S, N) -> (scalars[10], force (S, N) or None)."""
+        rho = np.ascontiguousarray(rho, dtype=np.float64).reshape(self.S, self.N)
+        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), (self.S,)))
+        v = None if vext is None else np.ascontiguousarray(vext, dtype=np.float64).reshape(self.S, self.N)
+        force = np.empty((self.S, self.N)) if want_force else None
+        sc = np.empty(_lib.SCALAR_COUNT)
+        _lib.check(_lib.lib().cdft_total(self.handle, rho.ctypes.data, None if v is None else v.ctypes.data,
+                                         mu.ctypes.data_as(_lib.c_double_p),
+                                         None if force is None else force.ctypes.data,
+                                         sc.ctypes.data_as(_lib.c_double_p)))
+        return sc, force
+
+    def total_device(self, rho_ptr: int, vext_ptr, mu, force_ptr: int, scalars_ptr: int, stream: int = 0):
+        """cdft_total_device on device pointers (ints, e.g. torch.Tensor.data_ptr())."""
+        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), (self.S,)))
+        _lib.check(_lib.lib().cdft_total_device(self.handle, rho_ptr, vext_ptr or None,
+                                                mu.ctypes.data_as(_lib.c_double_p), force_ptr, scalars_ptr,
+                                                stream or None))
+
+
+@dataclass
+class Weights:
+    """functionals.hpp:19-23 with the grid weights resident on the GPU."""
+
+    fmt_model: FMTModel
+    engine: Engine
+
+    @property
+    def a_vdw(self):
+        return list(self.engine.a_vdw)
+
+
+def make_weights(fmt_model: FMTModel, model: Model, precision: int = _lib.FP64) -> Weights:
+    """functionals.hpp:27-33."""
+    return Weights(fmt_model, Engine(fmt_model, model, precision))
+
+
+@dataclass
+class Result:
+    """functionals/types.hpp:18-23 (plus the per-term parts and N_s)."""
+
+    free_energy: float
+    grand_potential: float
+    forces: list
+    parts: dict = field(default_factory=dict)
+
+
+def total(model: Model, rhos, weights: Weights, mus=None, vexts=None) -> Result:
+    """functionals.hpp:64-95: F = F_id + F_ext + F_hs + F_mf, Omega = F - sum mu N.
+
+    ``rhos`` is one profile per species (or an (S, N) array), ``mus`` the
+    beta*mu per species (default 0), ``vexts`` optional external fields.
+    """
+    S = len(model.species)
+    N = model.grid.total_points
+    rho = np.stack([np.asarray(r, dtype=np.float64).reshape(-1) for r in rhos]) if not isinstance(rhos, np.ndarray) \
+        else np.asarray(rhos, dtype=np.float64).reshape(S, N)
+    if rho.shape != (S, N):
+        raise ValueError(f"total: expected {S} profiles of {N} points")
+    mus = np.zeros(S) if mus is None else np.asarray(mus, dtype=np.float64)
+    v = None
+    if vexts is not None and any(x is not None for x in vexts):
+        v = np.stack([np.zeros(N) if x is None else np.asarray(x, dtype=np.float64).reshape(-1) for x in vexts])
+    sc, force = weights.engine.total_host(rho, mus, v)
+    parts = {"ideal": sc[2], "external": sc[3], "hard_sphere": sc[4], "mean_field": sc[5],
+             "N": [sc[6 + s] for s in range(S)]}
+    return Result(free_energy=float(sc[0]), grand_potential=float(sc[1]), forces=[force[s] for s in range(S)],
+                  parts=parts)
+
+
+class Functional:
+    """functional.hpp:22-107: model + GPU weights with the evaluate / callback facade."""
+
+    def __init__(self, fmt_model: FMTModel, model: Model, precision: int = _lib.FP64):
+        self.model = model
+        self.weights = make_weights(fmt_model, model, precision)
+
+    def evaluate(self, rho, chemical_potential=0.0) -> Result:
+        """functional.hpp:33-36 (single profile; V_ext is zero as in init::from_profile)."""
+        S = len(self.model.species)
+        rhos = [np.asarray(rho, dtype=np.float64).reshape(-1)]
+        rhos += [np.zeros(self.model.grid.total_points) for _ in range(1, S)]
+        return total(self.model, rhos, self.weights, [chemical_potential] + [0.0] * (S - 1))
+
+    def grand_potential(self, rho, chemical_potential) -> float:
+        return self.evaluate(rho, chemical_potential).grand_potential
+
+    def grand_potential_callback(self, chemical_potential):
+        """functional.hpp:62-73."""
+        def fn(densities):
+            r = total(self.model, densities, self.weights, [chemical_potential] * len(densities))
+            return r.grand_potential, r.forces
+        return fn

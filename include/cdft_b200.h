@@ -1,0 +1,160 @@
+/* classicalDFT B200 engine: the C ABI of the F[rho] / dF/drho hot path.
+ *
+ * This is the drop-in boundary behind the reference library's functional API
+ * (migduroli/classicalDFT v3.0.0).  The reference has no FFI of its own: its
+ * boundary is the C++ call
+ *     dft::functionals::total(const physics::Model&, const State&, const Weights&) -> Result
+ * (include/dft/functionals/functionals.hpp:64-95) plus the set-up calls that
+ * build Weights (functionals.hpp:27-33, fmt/weights.hpp:144-183,
+ * functionals/mean_field.hpp:146-219).  Each entry point below names the
+ * reference interface it replaces.
+ *
+ * Conventions (the reference's, functionals.hpp:55-63):
+ *   - fields are FP64, N = nx*ny*nz points, flat index iz + nz*(iy + ny*ix);
+ *     several species are passed species-major in one array of S*N doubles;
+ *   - forces are dOmega/drho * dV (not dOmega/drho);
+ *   - chemical potentials are beta*mu (dimensionless), one per species;
+ *   - the scalar block is [F, Omega, F_id, F_ext, F_hs, F_mf, N_0 .. N_{S-1}]
+ *     with N_s = sum(rho_s) dV, F = F_id + F_ext + F_hs + F_mf and
+ *     Omega = F - sum_s mu_s N_s (functionals.hpp:72-92).
+ *
+ * Every call returns CDFT_OK (0) or a negative status; cdft_last_error()
+ * gives the message of the calling thread's last failure.  The C++ host API
+ * (include/dft_b200/) rethrows them as std::invalid_argument /
+ * std::runtime_error, the reference's exception types.
+ *
+ * An engine is not thread-safe: use one engine per thread / stream.
+ */
+#ifndef CDFT_B200_H
+#define CDFT_B200_H
+
+#if defined(__GNUC__)
+#define CDFT_API __attribute__((visibility("default")))
+#else
+#define CDFT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CDFT_OK 0
+#define CDFT_ERR_INVALID (-1) /* std::invalid_argument in the reference */
+#define CDFT_ERR_RUNTIME (-2) /* std::runtime_error in the reference */
+#define CDFT_ERR_CUDA (-3)
+#define CDFT_ERR_CUFFT (-4)
+
+/* FMT models (fmt/models.hpp:153-359, FMTModel::from_name :398-410). */
+#define CDFT_ROSENFELD 0
+#define CDFT_RSLT 1
+#define CDFT_WHITEBEAR_I 2
+#define CDFT_WHITEBEAR_II 3
+#define CDFT_ESFMT 4
+
+/* Precision of the FFTs and k-space products; Phi, dPhi and all sums stay FP64. */
+#define CDFT_FP64 0
+#define CDFT_MIXED 1
+
+/* Potentials, split schemes and weight schemes
+ * (physics/potentials.hpp:18-21, 57-243; physics/interactions.hpp:11-18). */
+#define CDFT_POT_LENNARD_JONES 0
+#define CDFT_POT_TEN_WOLDE_FRENKEL 1
+#define CDFT_POT_WRDF 2
+#define CDFT_SPLIT_WCA 0
+#define CDFT_SPLIT_BH 1
+#define CDFT_WEIGHT_ZERO 0
+#define CDFT_WEIGHT_LINEAR_E 1
+#define CDFT_WEIGHT_LINEAR_F 2
+#define CDFT_WEIGHT_QUADRATIC_F 3
+#define CDFT_WEIGHT_GAUSS_E 4
+#define CDFT_WEIGHT_GAUSS_F 5
+
+#define CDFT_SCALAR_COUNT 10
+
+typedef struct cdft_engine cdft_engine;
+
+/* A pair potential as built by make_lennard_jones / make_ten_wolde_frenkel /
+ * make_wang_ramirez_dobnikar_frenkel (potentials.hpp:311-368). */
+typedef struct {
+  int type;
+  double sigma;
+  double epsilon;
+  double r_cutoff; /* <= 0: no cutoff (LJ, tWF) */
+  double alpha;    /* tWF only */
+} cdft_potential;
+
+/* One mean-field interaction (physics/interactions.hpp:23-30 after weight
+ * generation): the real-space weight array baked with dV/N, exactly the
+ * array the reference FFTs at mean_field.hpp:194. */
+typedef struct {
+  int species_i;
+  int species_j;
+  const double* weight_real; /* host, N doubles */
+  double a_vdw;
+} cdft_interaction;
+
+/* Message of this thread's last failed call ("" if none). */
+CDFT_API const char* cdft_last_error(void);
+
+/* Library version string. */
+CDFT_API const char* cdft_version(void);
+
+/* ---- set-up physics (host) ------------------------------------------- */
+
+/* Derived potential parameters: out = {epsilon_shift (WRDF: eps_eff), r_min,
+ * v_min, r_zero}.  Replaces make_lennard_jones & co (potentials.hpp:311-368). */
+CDFT_API int cdft_potential_info(const cdft_potential* pot, double out[4]);
+
+/* Attractive tail u_att(r) at n radii (potentials.hpp:97-107, 165-175, 228-236). */
+CDFT_API int cdft_potential_attractive(const cdft_potential* pot, int split, const double* r, long n, double* out);
+
+/* Barker-Henderson / WCA hard-sphere diameter (potentials.hpp:28-37). */
+CDFT_API int cdft_hard_sphere_diameter(const cdft_potential* pot, double kT, int split, double* diameter);
+
+/* (2 pi / kT) int r^2 u_att(r) dr (potentials.hpp:39-50). */
+CDFT_API int cdft_vdw_integral(const cdft_potential* pot, double kT, int split, double* value);
+
+/* Real-space mean-field weight w(r)/kT * dV/N on the grid and a_vdw = sum w dV
+ * (mean_field.hpp:146-196 up to its FFT).  weight_out: N doubles (host). */
+CDFT_API int cdft_interaction_weight(const long shape[3], double dx, const cdft_potential* pot, int split, int scheme,
+                            double kT, double* weight_out, double* a_vdw);
+
+/* ---- engine -------------------------------------------------------------- */
+
+/* Build an engine: grid, species diameters, FMT model (esFMT takes A, B) and
+ * interactions; uploads and transforms the mean-field weights once.
+ * Replaces make_weights(fmt_model, model) (functionals.hpp:27-33) together
+ * with the per-call FFTW plans of math/fourier.cpp:25-60.  Runs on the
+ * current CUDA device. */
+CDFT_API int cdft_create(cdft_engine** out, const long shape[3], double dx, int n_species, const double* diameters,
+                int fmt_model, double esfmt_A, double esfmt_B, int n_interactions,
+                const cdft_interaction* interactions, int precision);
+
+CDFT_API int cdft_destroy(cdft_engine* engine);
+
+/* Engine facts: info = {N, Nk, S, n_channels, n_deriv_channels, precision,
+ * kernels per evaluation, scratch bytes}. */
+CDFT_API int cdft_engine_info(const cdft_engine* engine, long long info[8]);
+
+/* a_vdw of interaction m as computed at set-up (InteractionWeight::a_vdw). */
+CDFT_API int cdft_engine_a_vdw(const cdft_engine* engine, int m, double* a_vdw);
+
+/* functionals::total (functionals.hpp:64-95) on HOST buffers:
+ *   rho    : S*N doubles            vext : S*N doubles or NULL (zero field)
+ *   mu     : S values (beta mu)     force: S*N doubles or NULL
+ *   scalars: CDFT_SCALAR_COUNT doubles or NULL
+ * Copies in, evaluates, copies out and synchronises. */
+CDFT_API int cdft_total(cdft_engine* engine, const double* rho, const double* vext, const double* mu, double* force,
+               double* scalars);
+
+/* functionals::total on DEVICE buffers, asynchronous on `stream`
+ * (cudaStream_t; NULL = the legacy default stream).  rho, vext, force and
+ * scalars are device pointers; mu is a host array read at call time. */
+CDFT_API int cdft_total_device(cdft_engine* engine, const double* rho, const double* vext, const double* mu, double* force,
+                      double* scalars, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CDFT_B200_H */
