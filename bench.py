@@ -211,64 +211,91 @@ def cpu_baseline_sample(seconds=12.0):
             "sample": f"{n} evaluations of the 128^3 workload (NumPy/SciPy FP64 oracle, scipy.fft workers={WORKERS})"}, ref
 
 
-def run_ours(args, ws, rank, local, dist):
-    import torch
-    import classicaldft_b200 as cd
-    dev = torch.device("cuda", local)
-    precision = cd.MIXED if args.precision == "mixed" else cd.FP64
+def _build_engine(cd, precision):
     lj = cd.make_lennard_jones(1.0, 1.0, 2.5)
     d = lj.hard_sphere_diameter(KT, cd.WEEKS_CHANDLER_ANDERSEN)
     g = cd.Grid(dx=DX, box_size=tuple(n * DX for n in SHAPE), shape=SHAPE)
     model = cd.Model(g, [cd.Species("LJ", d)], [cd.Interaction(0, 0, lj)], KT)
-    eng = cd.Engine(cd.WhiteBearII(), model, precision)
-    rho_h = workload_profile()
-    rho = torch.tensor(rho_h, dtype=torch.float64, device=dev)
-    force = torch.empty_like(rho)
-    scal = torch.zeros(10, dtype=torch.float64, device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    stream = torch.cuda.Stream(device=dev)
+    return cd.Engine(cd.WhiteBearII(), model, precision), d
+
+
+def _time_device(torch, eng, rho, force, scal, flush, stream, steps, warmup, sampler=None):
+    """Per-step CUDA-event timing on the engine's stream, L2 flushed between steps."""
     sp = stream.cuda_stream
 
     def step():
         eng.total_device(rho.data_ptr(), None, [0.0], force.data_ptr(), scal.data_ptr(), sp)
 
     with torch.cuda.stream(stream):
-        for _ in range(max(args.warmup, 3)):
+        for _ in range(max(warmup, 3)):
             step()
     torch.cuda.synchronize()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sampler.start()
-    time.sleep(0.3)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
     with torch.cuda.stream(stream):
-        for i in range(args.steps):
+        for i in range(steps):
             flush.fill_(float(i))
             starts[i].record(stream)
             step()
             ends[i].record(stream)
     torch.cuda.synchronize()
+    clocks = sampler.stop() if sampler else None
+    return float(np.sum([a.elapsed_time(b) for a, b in zip(starts, ends)])), clocks
+
+
+def run_ours(args, ws, rank, local, dist):
+    import ctypes
+    import torch
+    import classicaldft_b200 as cd
+    dev = torch.device("cuda", local)
+    precision = cd.MIXED if args.precision == "mixed" else cd.FP64
+    eng, d = _build_engine(cd, precision)
+    rho_h = workload_profile()
+    rho = torch.tensor(rho_h, dtype=torch.float64, device=dev)
+    force = torch.empty_like(rho)
+    scal = torch.zeros(10, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
     if dist:
         dist.barrier()
-    clocks = sampler.stop()
-    times = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    t_ms = float(np.sum(times))
+    torch.cuda.synchronize()
+    t_ms, clocks = _time_device(torch, eng, rho, force, scal, flush, stream, args.steps, args.warmup, sampler)
     if dist:
+        dist.barrier()
         tt = torch.tensor([t_ms], dtype=torch.float64, device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_ms = float(tt.item())
     value = ws * args.steps / (t_ms * 1e-3)
     ms_step = t_ms / args.steps
+    f_main = force.clone()
+    s_main = scal.clone()
+
+    # the other precision on the same input: throughput and the accuracy of mixed vs FP64
+    other = cd.FP64 if precision == cd.MIXED else cd.MIXED
+    eng2, _ = _build_engine(cd, other)
+    force2 = torch.empty_like(rho)
+    scal2 = torch.zeros(10, dtype=torch.float64, device=dev)
+    t2, _ = _time_device(torch, eng2, rho, force2, scal2, flush, stream, max(args.steps // 2, 10), args.warmup)
+    if dist:
+        tt = torch.tensor([t2], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t2 = float(tt.item())
+    n2 = max(args.steps // 2, 10)
+    f64, f32 = (force2, f_main) if precision == cd.MIXED else (f_main, force2)
+    s64, s32 = (scal2, s_main) if precision == cd.MIXED else (s_main, scal2)
+    dF = abs(float(s32[0]) - float(s64[0])) / abs(float(s64[0]))
+    dforce = float((f32 - f64).abs().max() / f64.abs().max())
+    eng2.close()
 
     # e2e through the host API with pinned buffers
     rho_pin = torch.tensor(rho_h, dtype=torch.float64).pin_memory()
     f_pin = torch.empty_like(rho_pin).pin_memory()
     sc_pin = torch.empty(10, dtype=torch.float64).pin_memory()
     L = cd.lib()
-    import ctypes
     mu = (ctypes.c_double * 1)(0.0)
 
     def e2e_step():
@@ -296,23 +323,26 @@ def run_ours(args, ws, rank, local, dist):
     nbytes = algorithmic_bytes(info, S=1, M=1)
     peak, peak_kind = hbm_peak()
     achieved = nbytes / (ms_step * 1e-3) / 1e9
+    names = {cd.MIXED: "mixed", cd.FP64: "fp64"}
     line = {
         "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": ws, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 FFT / f64 Phi+sums" if precision == cd.MIXED else "f64",
+        "vs_baseline": None, "dtype": "f32 FFT+k-space / f64 Phi+sums" if precision == cd.MIXED else "f64",
         "data": "synthetic",
         "config": {"workload": "128^3 LJ-fluid DDFT state, WhiteBearII + cut LJ (QF), 1 species",
                    "grid": list(SHAPE), "dx": DX, "kT": KT, "rho_bar": RHO_BAR, "noise": "1% uniform, seeded",
-                   "hs_diameter": d, "precision": args.precision, "parallelism": f"replicas x{ws}",
+                   "hs_diameter": d, "precision": names[precision], "parallelism": f"replicas x{ws}",
                    "l2": "flushed between timed steps (256 MiB write outside the events)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None,
-                     "scope": "one full evaluation (25 cuFFT transforms + 5 engine kernels)",
+                     "scope": "one full evaluation (cuFFT transforms + engine kernels)",
                      "algorithmic_bytes": nbytes, "peak_source": peak_kind},
+        names[other]: {"value": ws * n2 / (t2 * 1e-3), "ms_per_step": t2 / n2},
+        "mixed_vs_fp64": {"dF_over_F": dF, "max_dforce_over_max_force": dforce},
         "e2e": {"value": e2e_val, "unit": "evals/s", "h2d_bytes_per_step": 8 * info["N"],
                 "d2h_bytes_per_step": 8 * info["N"] + 80},
         "clocks": clocks,
-        "gpu_launches": int(info["kernels_per_eval"]) * args.steps + (args.steps if precision == cd.MIXED else 0),
+        "gpu_launches": int(info["kernels_per_eval"]) * args.steps,
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cb, _ = cpu_baseline_sample(args.cpu_seconds)
@@ -328,7 +358,7 @@ def main():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()

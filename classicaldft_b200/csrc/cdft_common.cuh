@@ -32,11 +32,15 @@ __host__ __device__ constexpr int tensor_index(int i, int j) {
 }
 
 // Forward (weighted-density) channel layout.
-//   one species  : eta, n2, v[3], T[6]                  (5 or 11 channels)
-//   mixtures     : eta, n2, n1, n0, v1[3], v0[3], T[6]  (10 or 16 channels)
-// followed by the mean-field convolution channels.  The derivative
-// (back-convolution) channels use the same order; for one species n1/n0 and
-// v0 are folded into n2 and v before the transform (hard_sphere.hpp:121,125).
+//   one species  : eta, n2, v[3], T[5]                  (5 or 10 channels)
+//   mixtures     : eta, n2, n1, n0, v1[3], v0[3], T[5]  (10 or 15 channels)
+// followed by the mean-field convolution channels.  Only five tensor
+// components are transformed (xx, xy, xz, yy, yz): the trace of the tensor
+// weight is the surface weight (A + 3B = w2 in weights.hpp:121-137), so
+// T_zz = n2 - T_xx - T_yy exactly, and in the back-convolution dPhi/dT_zz
+// folds into the n2, xx and yy channels.  The derivative channels use the
+// same order; for one species n1/n0 and v0 are folded into n2 and v before
+// the transform (hard_sphere.hpp:121,125).
 struct ChannelLayout {
   int multi = 0;       // species-summed n1, n0, v0 channels present
   int tensor = 0;      // tensor channels present
@@ -49,15 +53,17 @@ struct ChannelLayout {
     L.tensor = tensor;
     if (!multi) {
       L.eta = 0; L.n2 = 1; L.v1 = 2; L.t = 5;
-      L.n_fmt = tensor ? 11 : 5;
+      L.n_fmt = tensor ? 10 : 5;
     } else {
       L.eta = 0; L.n2 = 1; L.n1 = 2; L.n0 = 3; L.v1 = 4; L.v0 = 7; L.t = 10;
-      L.n_fmt = tensor ? 16 : 10;
+      L.n_fmt = tensor ? 15 : 10;
     }
     L.n_deriv = L.n_fmt;
     return L;
   }
 };
+
+constexpr int kMaxChannels = 15 + 2 * kMaxInteractions;
 
 struct EvalParams {
   int nx, ny, nz, nzh;

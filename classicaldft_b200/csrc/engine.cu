@@ -35,11 +35,6 @@ __global__ void k_real_part(const double2* __restrict__ in, double* __restrict__
     out[i] = in[i].x;
 }
 
-__global__ void k_to_float(const double* __restrict__ in, float* __restrict__ out, long long n) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    out[i] = (float)in[i];
-}
-
 }  // namespace
 
 Engine::Engine(const EngineSpec& spec) {
@@ -112,6 +107,8 @@ Engine::Engine(const EngineSpec& spec) {
   hs_r_ = dalloc<char>(rs * S * p.N, tot);
   if (mixed) rho_lo_ = dalloc<char>(sizeof(float) * S * p.N, tot);
   mf_w_ = dalloc<double>((size_t)std::max(p.M, 1) * p.Nk, tot);
+  mean_ = dalloc<double>(kMaxSpecies, tot);
+  dbar_ = dalloc<double>(kMaxChannels, tot);
 
   // grid sizes from occupancy (148 SMs on B200)
   const bool multi = S > 1;
@@ -148,6 +145,7 @@ Engine::~Engine() {
     cufftDestroy(plan_force_);
   }
   for (void* q : {rho_k_, chan_k_, chan_r_, deriv_r_, deriv_k_, force_k_, hs_r_, rho_lo_, (void*)mf_w_,
+                  (void*)mean_, (void*)dbar_,
                   (void*)partials_, fft_work_, (void*)h_rho_, (void*)h_vext_, (void*)h_force_, (void*)h_scalars_})
     if (q) cudaFree(q);
   if (stream_) cudaStreamDestroy(stream_);
@@ -228,9 +226,11 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   C2* force_k = static_cast<C2*>(force_k_);
   R* hs_r = static_cast<R*>(hs_r_);
 
-  // 1. rho_k = r2c(rho)
+  // 1. rho_k = r2c(rho); mixed precision transforms rho - mean in FP32
   if constexpr (mixed) {
-    k_to_float<<<grid_pw_, 256, 0, stream>>>(rho, static_cast<float*>(rho_lo_), p.S * p.N);
+    k_species_sums<<<grid_pw_, 256, 0, stream>>>(rho, p.N, p.S, partials_);
+    k_split_convert<<<grid_pw_, 256, 0, stream>>>(rho, p.N, p.S, partials_, grid_pw_,
+                                                  static_cast<float*>(rho_lo_), mean_);
     CDFT_CUFFT(cufftExecR2C(plan_rho_, static_cast<float*>(rho_lo_), reinterpret_cast<cufftComplex*>(rho_k)));
   } else {
     CDFT_CUFFT(cufftExecD2Z(plan_rho_, const_cast<double*>(rho), reinterpret_cast<cufftDoubleComplex*>(rho_k)));
@@ -253,6 +253,9 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   for (int s = 0; s < kMaxSpecies; ++s) a.mu[s] = s < p.S ? mu[s] : 0.0;
   a.force = force;
   a.partials = partials_;
+  a.mf_w = mf_w_;
+  a.mean = mean_;
+  a.dbar_out = dbar_;
   if (!multi && !tensor) k_pointwise<false, false, R><<<grid_pw_, 256, 0, stream>>>(p, chan_r, deriv_r, a);
   if (!multi && tensor) k_pointwise<false, true, R><<<grid_pw_, 256, 0, stream>>>(p, chan_r, deriv_r, a);
   if (multi && !tensor) k_pointwise<true, false, R><<<grid_pw_, 256, 0, stream>>>(p, chan_r, deriv_r, a);
@@ -274,7 +277,10 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
     CDFT_CUFFT(cufftExecC2R(plan_force_, reinterpret_cast<cufftComplex*>(force_k), reinterpret_cast<float*>(hs_r)));
   else
     CDFT_CUFFT(cufftExecZ2D(plan_force_, reinterpret_cast<cufftDoubleComplex*>(force_k), reinterpret_cast<double*>(hs_r)));
-  k_epilogue<R><<<grid_pw_, 256, 0, stream>>>(p.S * p.N, p.dv, hs_r, force);
+  if (!multi && !tensor) k_epilogue<false, false, R><<<grid_pw_, 256, 0, stream>>>(p, hs_r, dbar_, force);
+  if (!multi && tensor) k_epilogue<false, true, R><<<grid_pw_, 256, 0, stream>>>(p, hs_r, dbar_, force);
+  if (multi && !tensor) k_epilogue<true, false, R><<<grid_pw_, 256, 0, stream>>>(p, hs_r, dbar_, force);
+  if (multi && tensor) k_epilogue<true, true, R><<<grid_pw_, 256, 0, stream>>>(p, hs_r, dbar_, force);
   CDFT_CUDA(cudaGetLastError());
   // 8. scalars
   MuArgs ma;

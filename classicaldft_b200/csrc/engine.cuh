@@ -56,7 +56,7 @@ class Engine {
   long long modes() const { return p_.Nk; }
   int precision() const { return precision_; }
   double a_vdw(int m) const { return a_vdw_[m]; }
-  int kernels_per_eval() const { return 5; }
+  int kernels_per_eval() const { return precision_ == 1 ? 7 : 5; }
   // Scratch bytes held beyond inputs and outputs.
   size_t scratch_bytes() const { return scratch_bytes_; }
 
@@ -90,6 +90,8 @@ class Engine {
   void* hs_r_ = nullptr;      // S * N real
   void* rho_lo_ = nullptr;    // S * N float (mixed precision input copy)
   double* mf_w_ = nullptr;    // M * Nk real (FP64)
+  double* mean_ = nullptr;    // S species means (mixed precision)
+  double* dbar_ = nullptr;    // derivative-channel constants (mixed precision)
   double* partials_ = nullptr;
   void* fft_work_ = nullptr;
   size_t scratch_bytes_ = 0;

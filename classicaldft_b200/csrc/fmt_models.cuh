@@ -72,31 +72,42 @@ struct FVals {
 };
 
 // f1, f2, f3 and their eta-derivatives for one model (models.hpp:153-324).
+// log(1 - eta), 1/(1 - eta) and 1/eta are formed once; every other quotient
+// of the reference's expressions is rewritten with these reciprocals, which
+// keeps the FP64 division count at two per point.
 template <class T>
 __device__ inline FVals<T> fmt_f(int model, T eta) {
   FVals<T> r;
   const double ev = val(eta);
-  T e = 1.0 - eta;
-  r.f1 = dlog(e);
-  r.df1 = -1.0 / e;
+  const T e = 1.0 - eta;
+  const T ie = 1.0 / e;
+  const T ie2 = ie * ie;
+  const T lg = dlog(e);
+  r.f1 = lg;
+  r.df1 = -ie;
+  const bool taylor = ev < 1e-6;
+  T ih = cst<T>(0.0), ih2 = cst<T>(0.0);
+  if (!taylor && model != kRosenfeld && model != kEsFMT) {
+    ih = 1.0 / eta;
+    ih2 = ih * ih;
+  }
   if (model == kWhiteBearII) {
-    if (ev < 1e-6) {
+    if (taylor) {
       r.f2 = 1.0 + eta * (1.0 + eta * (10.0 / 9.0 + (7.0 / 6.0) * eta));
       r.df2 = 1.0 + eta * (2.0 * (10.0 / 9.0) + 3.0 * (7.0 / 6.0) * eta);
     } else {
-      T lg = dlog(e);
-      r.f2 = (1.0 / 3.0) + (4.0 / 3.0) / e + 2.0 / (3.0 * eta) * lg;
-      r.df2 = (4.0 / 3.0) / (e * e) - (2.0 / (3.0 * eta * eta)) * lg - 2.0 / (3.0 * eta * e);
+      r.f2 = (1.0 / 3.0) + (4.0 / 3.0) * ie + (2.0 / 3.0) * ih * lg;
+      r.df2 = (4.0 / 3.0) * ie2 - (2.0 / 3.0) * ih2 * lg - (2.0 / 3.0) * ih * ie;
     }
   } else {
-    r.f2 = 1.0 / e;
-    r.df2 = 1.0 / (e * e);
+    r.f2 = ie;
+    r.df2 = ie2;
   }
   if (model == kRosenfeld || model == kEsFMT) {
-    r.f3 = 1.0 / (e * e);
-    r.df3 = 2.0 / (e * e * e);
+    r.f3 = ie2;
+    r.df3 = 2.0 * ie2 * ie;
   } else if (model == kRSLT || model == kWhiteBearI) {
-    if (ev < 1e-6) {
+    if (taylor) {
       if (model == kRSLT) {
         r.f3 = 1.0 + (2.0 / 3.0) * eta + 0.5 * eta * eta;
         r.df3 = (2.0 / 3.0) + eta;
@@ -105,23 +116,20 @@ __device__ inline FVals<T> fmt_f(int model, T eta) {
         r.df3 = 8.0 / 3.0 + eta * (2.0 * (15.0 / 4.0) + 3.0 * (24.0 / 5.0) * eta);
       }
     } else {
-      T h = eta * e * e;
-      T lg = dlog(e);
-      r.f3 = 1.0 / h + lg / (eta * eta);
-      r.df3 = -(e * (e - 2.0 * eta)) / (h * h) - 1.0 / (e * eta * eta) - 2.0 * lg / (eta * eta * eta);
+      // f3 = 1/(eta e^2) + log(e)/eta^2
+      r.f3 = ih * ie2 + lg * ih2;
+      r.df3 = -(e - 2.0 * eta) * ih2 * ie2 * ie - ie * ih2 - 2.0 * lg * ih2 * ih;
     }
   } else {  // WhiteBearII
-    if (ev < 1e-6) {
+    if (taylor) {
       r.f3 = 1.5 + (7.0 / 3.0) * eta + 3.25 * eta * eta + 4.2 * eta * eta * eta;
       r.df3 = 7.0 / 3.0 + 6.5 * eta + 12.6 * eta * eta;
     } else {
-      T g = 1.0 - 3.0 * eta + eta * eta;
-      T gp = -3.0 + 2.0 * eta;
-      T h = eta * e * e;
-      T hp = e * (e - 2.0 * eta);
-      T lg = dlog(e);
-      r.f3 = -(g / h) - lg / (eta * eta);
-      r.df3 = -(gp * h - g * hp) / (h * h) + 1.0 / (e * eta * eta) + 2.0 * lg / (eta * eta * eta);
+      // f3 = -(1 - 3 eta + eta^2)/(eta e^2) - log(e)/eta^2
+      const T g = 1.0 - 3.0 * eta + eta * eta;
+      const T gp = -3.0 + 2.0 * eta;
+      r.f3 = -(g * ih * ie2) - lg * ih2;
+      r.df3 = -(gp * ih * ie2) + g * (e - 2.0 * eta) * ih2 * ie2 * ie + ie * ih2 + 2.0 * lg * ih2 * ih;
     }
   }
   return r;
