@@ -78,6 +78,7 @@ def lib():
         "cdft_engine_a_vdw": [vp, ctypes.c_int, c_double_p],
         "cdft_total": [vp, vp, vp, c_double_p, vp, c_double_p],
         "cdft_total_device": [vp, vp, vp, c_double_p, vp, vp, vp],
+        "cdft_engine_status": [vp, vp],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)

@@ -194,6 +194,7 @@ int cdft_total(cdft_engine* engine, const double* rho, const double* vext, const
     double tmp[CDFT_SCALAR_COUNT];
     CDFT_CUDA(cudaMemcpyAsync(tmp, e.host_scalars(), sizeof(tmp), cudaMemcpyDeviceToHost, st));
     CDFT_CUDA(cudaStreamSynchronize(st));
+    if (e.take_error(st)) throw cdft::Error(CDFT_ERR_RUNTIME, "evaluation aborted: a bounded device wait timed out");
     if (scalars) std::memcpy(scalars, tmp, sizeof(tmp));
   });
 }
@@ -204,6 +205,14 @@ int cdft_total_device(cdft_engine* engine, const double* rho, const double* vext
     if (!engine || !rho || !mu || !force || !scalars)
       throw std::invalid_argument("engine, rho, mu, force and scalars are required");
     engine->impl->evaluate(rho, vext, mu, force, scalars, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int cdft_engine_status(cdft_engine* engine, void* stream) {
+  return guarded([&] {
+    if (!engine) throw std::invalid_argument("engine is NULL");
+    if (engine->impl->take_error(static_cast<cudaStream_t>(stream)))
+      throw cdft::Error(CDFT_ERR_RUNTIME, "a bounded device wait timed out in an earlier call");
   });
 }
 

@@ -25,10 +25,14 @@ constexpr double kPi = 3.14159265358979323846;
 // FMT model ids (include/dft/functionals/fmt/models.hpp:153-359).
 enum ModelId : int { kRosenfeld = 0, kRSLT = 1, kWhiteBearI = 2, kWhiteBearII = 3, kEsFMT = 4 };
 
+__host__ __device__ constexpr bool model_has_tensor(int m) {
+  return m == kWhiteBearI || m == kWhiteBearII || m == kEsFMT;
+}
+
 // Tensor component order of the six stored channels (weights.hpp:46-50):
 // xx, xy, xz, yy, yz, zz.
 __host__ __device__ constexpr int tensor_index(int i, int j) {
-  return (i <= j) ? (i == 0 ? j : (i == 1 ? 2 + j : 5)) : tensor_index(j, i);
+  return (i > j) ? (j == 0 ? i : (j == 1 ? 2 + i : 5)) : (i == 0 ? j : (i == 1 ? 2 + j : 5));
 }
 
 // Forward (weighted-density) channel layout.

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 namespace cdft {
 
@@ -36,6 +37,31 @@ __global__ void k_real_part(const double2* __restrict__ in, double* __restrict__
 }
 
 }  // namespace
+
+// Calls f(model, multi, real-type) with compile-time constants matching this
+// engine's FMT model, species count and storage precision.
+template <class F>
+void Engine::with_kernels(bool mixed, F&& f) const {
+  auto by_model = [&](auto multi_c, auto r_c) {
+    switch (p_.model) {
+      case kRosenfeld: f(std::integral_constant<int, kRosenfeld>{}, multi_c, r_c); break;
+      case kRSLT: f(std::integral_constant<int, kRSLT>{}, multi_c, r_c); break;
+      case kWhiteBearI: f(std::integral_constant<int, kWhiteBearI>{}, multi_c, r_c); break;
+      case kWhiteBearII: f(std::integral_constant<int, kWhiteBearII>{}, multi_c, r_c); break;
+      default: f(std::integral_constant<int, kEsFMT>{}, multi_c, r_c); break;
+    }
+  };
+  auto by_multi = [&](auto r_c) {
+    if (p_.L.multi)
+      by_model(std::true_type{}, r_c);
+    else
+      by_model(std::false_type{}, r_c);
+  };
+  if (mixed)
+    by_multi(std::type_identity<float>{});
+  else
+    by_multi(std::type_identity<double>{});
+}
 
 Engine::Engine(const EngineSpec& spec) {
   for (int d = 0; d < 3; ++d)
@@ -111,20 +137,35 @@ Engine::Engine(const EngineSpec& spec) {
   dbar_ = dalloc<double>(kMaxChannels, tot);
 
   // grid sizes from occupancy (148 SMs on B200)
-  const bool multi = S > 1;
   auto pick = [&](auto kern, long long work) { return occupancy_grid(kern, 256, sms, work); };
-  if (!mixed) {
-    if (!multi && !tensor) { grid_pw_ = pick(k_pointwise<false, false, double>, p.N); grid_k_ = pick(k_forward<false, false, double2>, p.Nk); }
-    if (!multi && tensor) { grid_pw_ = pick(k_pointwise<false, true, double>, p.N); grid_k_ = pick(k_forward<false, true, double2>, p.Nk); }
-    if (multi && !tensor) { grid_pw_ = pick(k_pointwise<true, false, double>, p.N); grid_k_ = pick(k_forward<true, false, double2>, p.Nk); }
-    if (multi && tensor) { grid_pw_ = pick(k_pointwise<true, true, double>, p.N); grid_k_ = pick(k_forward<true, true, double2>, p.Nk); }
-  } else {
-    if (!multi && !tensor) { grid_pw_ = pick(k_pointwise<false, false, float>, p.N); grid_k_ = pick(k_forward<false, false, float2>, p.Nk); }
-    if (!multi && tensor) { grid_pw_ = pick(k_pointwise<false, true, float>, p.N); grid_k_ = pick(k_forward<false, true, float2>, p.Nk); }
-    if (multi && !tensor) { grid_pw_ = pick(k_pointwise<true, false, float>, p.N); grid_k_ = pick(k_forward<true, false, float2>, p.Nk); }
-    if (multi && tensor) { grid_pw_ = pick(k_pointwise<true, true, float>, p.N); grid_k_ = pick(k_forward<true, true, float2>, p.Nk); }
-  }
-  partials_ = dalloc<double>((size_t)grid_pw_ * p.n_terms, tot);
+  with_kernels(mixed, [&](auto model_c, auto multi_c, auto r_c) {
+    constexpr int MD = decltype(model_c)::value;
+    constexpr bool MU = decltype(multi_c)::value;
+    using RT = typename decltype(r_c)::type;
+    using C2 = std::conditional_t<sizeof(RT) == 4, float2, double2>;
+    constexpr bool TE = model_has_tensor(MD);
+    grid_pw_ = pick(k_pointwise<MD, MU, RT>, p.N);
+    grid_k_ = pick(k_forward<MU, TE, C2>, p.Nk);
+  });
+  // TMA-staged pointwise kernel: dynamic shared memory for the 3-stage ring
+  with_kernels(mixed, [&](auto model_c, auto multi_c, auto r_c) {
+    constexpr int MD = decltype(model_c)::value;
+    constexpr bool MU = decltype(multi_c)::value;
+    using RT = typename decltype(r_c)::type;
+    constexpr bool TE = model_has_tensor(MD);
+    tma_smem_ = (size_t)kTmaStages * tma_stage_bytes<MU, TE, RT>(S, false);
+    tma_smem_v_ = (size_t)kTmaStages * tma_stage_bytes<MU, TE, RT>(S, true);
+    CDFT_CUDA(cudaFuncSetAttribute(k_pointwise_tma<MD, MU, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)tma_smem_v_));
+    int per_sm = 0;
+    CDFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pointwise_tma<MD, MU, RT>, kTmaTile,
+                                                            tma_smem_v_));
+    grid_tma_ = sms * std::max(per_sm, 1);
+  });
+  grid_stream_ = (int)std::max<long long>(1, std::min<long long>((long long)sms * 8, (p.N + 255) / 256));
+  partials_ = dalloc<double>((size_t)std::max(std::max(grid_pw_, grid_tma_), grid_stream_) * p.n_terms, tot);
+  err_ = dalloc<int>(1, tot);
+  CDFT_CUDA(cudaMemset(err_, 0, sizeof(int)));
 
   build_plans();
   upload_mean_field(spec);
@@ -145,7 +186,7 @@ Engine::~Engine() {
     cufftDestroy(plan_force_);
   }
   for (void* q : {rho_k_, chan_k_, chan_r_, deriv_r_, deriv_k_, force_k_, hs_r_, rho_lo_, (void*)mf_w_,
-                  (void*)mean_, (void*)dbar_,
+                  (void*)mean_, (void*)dbar_, (void*)err_,
                   (void*)partials_, fft_work_, (void*)h_rho_, (void*)h_vext_, (void*)h_force_, (void*)h_scalars_})
     if (q) cudaFree(q);
   if (stream_) cudaStreamDestroy(stream_);
@@ -226,10 +267,15 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   C2* force_k = static_cast<C2*>(force_k_);
   R* hs_r = static_cast<R*>(hs_r_);
 
+  // cuFFT needs 16-byte aligned FP64 input: stage a misaligned rho
+  if (!mixed && ((uintptr_t)rho % 16 != 0)) {
+    CDFT_CUDA(cudaMemcpyAsync(h_rho_, rho, sizeof(double) * p.S * p.N, cudaMemcpyDeviceToDevice, stream));
+    rho = h_rho_;
+  }
   // 1. rho_k = r2c(rho); mixed precision transforms rho - mean in FP32
   if constexpr (mixed) {
-    k_species_sums<<<grid_pw_, 256, 0, stream>>>(rho, p.N, p.S, partials_);
-    k_split_convert<<<grid_pw_, 256, 0, stream>>>(rho, p.N, p.S, partials_, grid_pw_,
+    k_species_sums<<<grid_stream_, 256, 0, stream>>>(rho, p.N, p.S, partials_);
+    k_split_convert<<<grid_stream_, 256, 0, stream>>>(rho, p.N, p.S, partials_, grid_stream_,
                                                   static_cast<float*>(rho_lo_), mean_);
     CDFT_CUFFT(cufftExecR2C(plan_rho_, static_cast<float*>(rho_lo_), reinterpret_cast<cufftComplex*>(rho_k)));
   } else {
@@ -256,10 +302,22 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   a.mf_w = mf_w_;
   a.mean = mean_;
   a.dbar_out = dbar_;
-  if (!multi && !tensor) k_pointwise<false, false, R><<<grid_pw_, 256, 0, stream>>>(p, chan_r, deriv_r, a);
-  if (!multi && tensor) k_pointwise<false, true, R><<<grid_pw_, 256, 0, stream>>>(p, chan_r, deriv_r, a);
-  if (multi && !tensor) k_pointwise<true, false, R><<<grid_pw_, 256, 0, stream>>>(p, chan_r, deriv_r, a);
-  if (multi && tensor) k_pointwise<true, true, R><<<grid_pw_, 256, 0, stream>>>(p, chan_r, deriv_r, a);
+  // TMA ring when every segment start is 16-byte aligned (N % 4 == 0 and
+  // aligned base pointers); otherwise the register-prefetch variant.
+  const bool tma = (p.N % 4 == 0) && ((uintptr_t)rho % 16 == 0) && ((uintptr_t)vext % 16 == 0);
+  const int pw_blocks = tma ? grid_tma_ : grid_pw_;
+  with_kernels(mixed, [&](auto model_c, auto multi_c, auto r_c) {
+    constexpr int MD = decltype(model_c)::value;
+    constexpr bool MU = decltype(multi_c)::value;
+    using RT = typename decltype(r_c)::type;
+    if constexpr (std::is_same_v<RT, R>) {
+      if (tma)
+        k_pointwise_tma<MD, MU, RT><<<grid_tma_, kTmaTile, vext ? tma_smem_v_ : tma_smem_, stream>>>(
+            p, chan_r, deriv_r, a, err_);
+      else
+        k_pointwise<MD, MU, RT><<<grid_pw_, 256, 0, stream>>>(p, chan_r, deriv_r, a);
+    }
+  });
   CDFT_CUDA(cudaGetLastError());
   // 5. D_k = r2c(dPhi channels)
   if constexpr (mixed)
@@ -277,16 +335,24 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
     CDFT_CUFFT(cufftExecC2R(plan_force_, reinterpret_cast<cufftComplex*>(force_k), reinterpret_cast<float*>(hs_r)));
   else
     CDFT_CUFFT(cufftExecZ2D(plan_force_, reinterpret_cast<cufftDoubleComplex*>(force_k), reinterpret_cast<double*>(hs_r)));
-  if (!multi && !tensor) k_epilogue<false, false, R><<<grid_pw_, 256, 0, stream>>>(p, hs_r, dbar_, force);
-  if (!multi && tensor) k_epilogue<false, true, R><<<grid_pw_, 256, 0, stream>>>(p, hs_r, dbar_, force);
-  if (multi && !tensor) k_epilogue<true, false, R><<<grid_pw_, 256, 0, stream>>>(p, hs_r, dbar_, force);
-  if (multi && tensor) k_epilogue<true, true, R><<<grid_pw_, 256, 0, stream>>>(p, hs_r, dbar_, force);
+  if (!multi && !tensor) k_epilogue<false, false, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar_, force);
+  if (!multi && tensor) k_epilogue<false, true, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar_, force);
+  if (multi && !tensor) k_epilogue<true, false, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar_, force);
+  if (multi && tensor) k_epilogue<true, true, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar_, force);
   CDFT_CUDA(cudaGetLastError());
   // 8. scalars
   MuArgs ma;
   for (int s = 0; s < kMaxSpecies; ++s) ma.mu[s] = a.mu[s];
-  k_reduce_final<<<1, 32 * (4 + kMaxSpecies), 0, stream>>>(partials_, grid_pw_, p, ma, scalars);
+  k_reduce_final<<<1, 32 * (4 + kMaxSpecies), 0, stream>>>(partials_, pw_blocks, p, ma, err_, scalars);
   CDFT_CUDA(cudaGetLastError());
+}
+
+int Engine::take_error(cudaStream_t stream) {
+  int v = 0;
+  CDFT_CUDA(cudaMemcpyAsync(&v, err_, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CDFT_CUDA(cudaStreamSynchronize(stream));
+  if (v) CDFT_CUDA(cudaMemsetAsync(err_, 0, sizeof(int), stream));
+  return v;
 }
 
 void Engine::evaluate(const double* rho, const double* vext, const double* mu, double* force, double* scalars,

@@ -57,6 +57,8 @@ class Engine {
   int precision() const { return precision_; }
   double a_vdw(int m) const { return a_vdw_[m]; }
   int kernels_per_eval() const { return precision_ == 1 ? 7 : 5; }
+  // Reads and clears the device error word (synchronises the stream).
+  int take_error(cudaStream_t stream);
   // Scratch bytes held beyond inputs and outputs.
   size_t scratch_bytes() const { return scratch_bytes_; }
 
@@ -69,6 +71,8 @@ class Engine {
 
  private:
   void build_plans();
+  template <class F>
+  void with_kernels(bool mixed, F&& f) const;
   void upload_mean_field(const EngineSpec& spec);
   template <typename R, typename C2>
   void run(const double* rho, const double* vext, const double* mu, double* force, double* scalars,
@@ -93,6 +97,10 @@ class Engine {
   double* mean_ = nullptr;    // S species means (mixed precision)
   double* dbar_ = nullptr;    // derivative-channel constants (mixed precision)
   double* partials_ = nullptr;
+  int* err_ = nullptr;        // device error word (set by bounded waits that gave up)
+  int grid_tma_ = 0;
+  int grid_stream_ = 0;       // streaming kernels (sums, conversion, epilogue)
+  size_t tma_smem_ = 0, tma_smem_v_ = 0;
   void* fft_work_ = nullptr;
   size_t scratch_bytes_ = 0;
 

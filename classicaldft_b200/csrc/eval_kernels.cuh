@@ -24,8 +24,9 @@
 // real field there.  FFTW's rank>=2 c2r (and pocketfft's) compute the exact
 // inverse DFT of its Hermitian projection: on the self-conjugate planes
 // kz = 0 and kz = nz/2, X'(kx,ky) = (X(kx,ky) + conj(X(-kx,-ky)))/2.  The
-// kernels write X' explicitly, so the c2r input is exactly Hermitian and the
-// result does not depend on how a library treats non-Hermitian input.
+// kernels write X' (through the symmetrised weight of chan_weight_sym), so the
+// c2r input is Hermitian and the result does not depend on how a library
+// treats non-Hermitian input.
 //
 // Mixed precision (FP32 storage, R = float).  The FFTs see only fluctuations:
 // rho_s = c_s + delta_rho_s with c_s the exact FP64 mean, and each derivative
@@ -150,16 +151,34 @@ __device__ __forceinline__ void st2<float2>(float2* a, long long i, double2 v) {
   a[i] = make_float2((float)v.x, (float)v.y);
 }
 
+// Channel weight at kk, Hermitian-symmetrised on the self-conjugate planes:
+// W'(k) = (W(k) + conj(W(k_m)))/2 with k_m the stored mirror wavevector
+// (same |k|).  Since rho_k (and every derivative spectrum) is Hermitian,
+// W'(k) rho_k(k) equals the projection (X(k) + conj(X(k_m)))/2 of X = W rho_k
+// up to round-off, without reading the mirror mode.  For an odd channel
+// (W = i w) the coefficient of i is (w(k) - w(k_m))/2.
+template <bool MULTI, bool TENSOR>
+__device__ __forceinline__ double chan_weight_sym(int c, int s, const EvalParams& p, const double kk[3],
+                                                  const double km[3], bool proj, double inv_k2, const KW& w,
+                                                  bool& odd) {
+  double v = chan_weight<MULTI, TENSOR>(c, s, p, kk, inv_k2, w, odd);
+  if (proj) {
+    const double vm = chan_weight<MULTI, TENSOR>(c, s, p, km, inv_k2, w, odd);
+    v = odd ? 0.5 * (v - vm) : 0.5 * (v + vm);
+  }
+  return v;
+}
+
 // One forward channel value at wavevector kk from the species spectra r[].
 template <bool MULTI, bool TENSOR>
-__device__ __forceinline__ double2 fwd_value(int c, const EvalParams& p, const double kk[3], double inv_k2,
-                                             const KW* kw, const double2* r) {
+__device__ __forceinline__ double2 fwd_value(int c, const EvalParams& p, const double kk[3], const double km[3],
+                                             bool proj, double inv_k2, const KW* kw, const double2* r) {
   double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
   for (int s = 0; s < (MULTI ? kMaxSpecies : 1); ++s) {
     if (s < p.S) {
       bool odd;
-      const double w = chan_weight<MULTI, TENSOR>(c, s, p, kk, inv_k2, kw[s], odd);
+      const double w = chan_weight_sym<MULTI, TENSOR>(c, s, p, kk, km, proj, inv_k2, kw[s], odd);
       if (odd) {
         acc.x += -w * r[s].y;
         acc.y += w * r[s].x;
@@ -175,7 +194,6 @@ __device__ __forceinline__ double2 fwd_value(int c, const EvalParams& p, const d
 struct KIndex {
   int ix, iy, iz;
   bool proj;
-  long long midx;
 };
 
 __device__ __forceinline__ KIndex decode_k(const EvalParams& p, long long idx) {
@@ -185,13 +203,23 @@ __device__ __forceinline__ KIndex decode_k(const EvalParams& p, long long idx) {
   q.iy = (int)(t % p.ny);
   q.ix = (int)(t / p.ny);
   q.proj = (q.iz == 0) || (((p.nz & 1) == 0) && q.iz == p.nz / 2);
-  q.midx = 0;
-  if (q.proj) {
-    const int mx = (p.nx - q.ix) % p.nx;
-    const int my = (p.ny - q.iy) % p.ny;
-    q.midx = q.iz + (long long)p.nzh * (my + (long long)p.ny * mx);
-  }
   return q;
+}
+
+// k, 1/k^2 and (on the self-conjugate planes) the mirror wavevector.
+__device__ __forceinline__ void k_setup(const EvalParams& p, const KIndex& q, double kk[3], double km[3], double& k,
+                                        double& inv_k2) {
+  k_components(p, q.ix, q.iy, q.iz, kk);
+  const double k2 = kk[0] * kk[0] + kk[1] * kk[1] + kk[2] * kk[2];
+  k = sqrt(k2);
+  inv_k2 = (k > 1e-12) ? 1.0 / k2 : 0.0;
+  if (q.proj) {
+    k_components(p, (p.nx - q.ix) % p.nx, (p.ny - q.iy) % p.ny, q.iz, km);
+  } else {
+    km[0] = kk[0];
+    km[1] = kk[1];
+    km[2] = kk[2];
+  }
 }
 
 template <bool MULTI, bool TENSOR, typename C2>
@@ -202,11 +230,8 @@ __global__ void __launch_bounds__(256) k_forward(EvalParams p, const C2* __restr
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < Nk;
        idx += (long long)gridDim.x * blockDim.x) {
     const KIndex q = decode_k(p, idx);
-    double kk[3];
-    k_components(p, q.ix, q.iy, q.iz, kk);
-    const double k2 = kk[0] * kk[0] + kk[1] * kk[1] + kk[2] * kk[2];
-    const double k = sqrt(k2);
-    const double inv_k2 = (k > 1e-12) ? 1.0 / k2 : 0.0;
+    double kk[3], km[3], k, inv_k2;
+    k_setup(p, q, kk, km, k, inv_k2);
     KW kw[kMaxSpecies];
     double2 r[kMaxSpecies];
 #pragma unroll
@@ -216,58 +241,34 @@ __global__ void __launch_bounds__(256) k_forward(EvalParams p, const C2* __restr
         r[s] = ld2(rho_k, s * Nk + idx);
       }
     }
-    double km[3];
-    double2 rm[kMaxSpecies];
-    if (q.proj) {
-      const int mx = (p.nx - q.ix) % p.nx;
-      const int my = (p.ny - q.iy) % p.ny;
-      k_components(p, mx, my, q.iz, km);
 #pragma unroll
-      for (int s = 0; s < kMaxSpecies; ++s)
-        if (s < p.S) rm[s] = ld2(rho_k, s * Nk + q.midx);
-    }
-#pragma unroll
-    for (int c = 0; c < L::NFMT; ++c) {
-      double2 x = fwd_value<MULTI, TENSOR>(c, p, kk, inv_k2, kw, r);
-      if (q.proj) {
-        const double2 xm = fwd_value<MULTI, TENSOR>(c, p, km, inv_k2, kw, rm);
-        x.x = 0.5 * (x.x + xm.x);
-        x.y = 0.5 * (x.y - xm.y);
-      }
-      st2(chan, c * Nk + idx, x);
-    }
-    // mean-field convolution channels (mean_field.hpp:259, 275)
+    for (int c = 0; c < L::NFMT; ++c)
+      st2(chan, c * Nk + idx, fwd_value<MULTI, TENSOR>(c, p, kk, km, q.proj, inv_k2, kw, r));
+    // mean-field convolution channels (mean_field.hpp:259, 275); the weight is
+    // real and even, so it needs no symmetrisation
     for (int m = 0; m < p.M; ++m) {
       const double w = mf_w[m * Nk + idx];
-      const double wm = q.proj ? mf_w[m * Nk + q.midx] : w;
-      for (int side = 0; side < 2; ++side) {
-        const int ch = side == 0 ? p.mf_chan_j[m] : p.mf_chan_i[m];
-        if (ch < 0) continue;
-        const int sp = side == 0 ? p.mf_j[m] : p.mf_i[m];
-        const double2 rv = ld2(rho_k, sp * Nk + idx);
-        double2 x = make_double2(w * rv.x, w * rv.y);
-        if (q.proj) {
-          const double2 rmv = ld2(rho_k, sp * Nk + q.midx);
-          x.x = 0.5 * (x.x + wm * rmv.x);
-          x.y = 0.5 * (x.y - wm * rmv.y);
-        }
-        st2(chan, ch * Nk + idx, x);
+      const double2 rv = ld2(rho_k, p.mf_j[m] * Nk + idx);
+      st2(chan, p.mf_chan_j[m] * Nk + idx, make_double2(w * rv.x, w * rv.y));
+      if (p.mf_chan_i[m] >= 0) {
+        const double2 ri = ld2(rho_k, p.mf_i[m] * Nk + idx);
+        st2(chan, p.mf_chan_i[m] * Nk + idx, make_double2(w * ri.x, w * ri.y));
       }
     }
   }
 }
 
 // Back-convolution of species s at kk from the derivative spectra dk[]:
-// F_s = sum_c conj(W_cs) D_c (hard_sphere.hpp:117-134).
+// F_s = sum_c conj(W'_cs) D_c (hard_sphere.hpp:117-134).
 template <bool MULTI, bool TENSOR>
-__device__ __forceinline__ double2 bwd_value(int s, const EvalParams& p, const double kk[3], double inv_k2,
-                                             const KW& w, const double2* d) {
+__device__ __forceinline__ double2 bwd_value(int s, const EvalParams& p, const double kk[3], const double km[3],
+                                             bool proj, double inv_k2, const KW& w, const double2* d) {
   using L = Lay<MULTI, TENSOR>;
   double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
   for (int c = 0; c < L::NFMT; ++c) {
     bool odd;
-    const double wc = chan_weight<MULTI, TENSOR>(c, s, p, kk, inv_k2, w, odd);
+    const double wc = chan_weight_sym<MULTI, TENSOR>(c, s, p, kk, km, proj, inv_k2, w, odd);
     if (odd) {  // conj(i w) D = -i w D
       acc.x += wc * d[c].y;
       acc.y += -wc * d[c].x;
@@ -286,34 +287,16 @@ __global__ void __launch_bounds__(256) k_backward(EvalParams p, const C2* __rest
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < Nk;
        idx += (long long)gridDim.x * blockDim.x) {
     const KIndex q = decode_k(p, idx);
-    double kk[3];
-    k_components(p, q.ix, q.iy, q.iz, kk);
-    const double k2 = kk[0] * kk[0] + kk[1] * kk[1] + kk[2] * kk[2];
-    const double k = sqrt(k2);
-    const double inv_k2 = (k > 1e-12) ? 1.0 / k2 : 0.0;
+    double kk[3], km[3], k, inv_k2;
+    k_setup(p, q, kk, km, k, inv_k2);
     double2 d[L::NFMT];
 #pragma unroll
     for (int c = 0; c < L::NFMT; ++c) d[c] = ld2(dk, c * Nk + idx);
-    double km[3];
-    double2 dm[L::NFMT];
-    if (q.proj) {
-      const int mx = (p.nx - q.ix) % p.nx;
-      const int my = (p.ny - q.iy) % p.ny;
-      k_components(p, mx, my, q.iz, km);
-#pragma unroll
-      for (int c = 0; c < L::NFMT; ++c) dm[c] = ld2(dk, c * Nk + q.midx);
-    }
 #pragma unroll
     for (int s = 0; s < (MULTI ? kMaxSpecies : 1); ++s) {
       if (s < p.S) {
         const KW w = weight_kernels(k, p.R[s]);
-        double2 f = bwd_value<MULTI, TENSOR>(s, p, kk, inv_k2, w, d);
-        if (q.proj) {
-          const double2 fm = bwd_value<MULTI, TENSOR>(s, p, km, inv_k2, w, dm);
-          f.x = 0.5 * (f.x + fm.x);
-          f.y = 0.5 * (f.y - fm.y);
-        }
-        st2(fk, s * Nk + idx, f);
+        st2(fk, s * Nk + idx, bwd_value<MULTI, TENSOR>(s, p, kk, km, q.proj, inv_k2, w, d));
       }
     }
   }
@@ -453,111 +436,314 @@ __device__ __forceinline__ void assemble(const EvalParams& p, const double* n, M
   }
 }
 
-template <bool MULTI, bool TENSOR, typename RT>
+// Per-block constants of the mixed-precision split: channel offsets (the FP64
+// convolution of the species means) and the derivative-channel constants
+// dbar (dPhi of the uniform fluid at the means).  Thread 0 fills shared memory.
+template <int MODEL, bool MULTI>
+__device__ __forceinline__ void split_prologue(const EvalParams& p, const PointwiseArgs& a, double* s_off,
+                                               double* s_dbar) {
+  constexpr bool TENSOR = model_has_tensor(MODEL);
+  using L = Lay<MULTI, TENSOR>;
+  constexpr int NF = L::NFMT;
+  if (threadIdx.x == 0) {
+    for (int c = 0; c < p.n_chan; ++c) s_off[c] = 0.0;
+#pragma unroll
+    for (int c = 0; c < NF; ++c)
+      for (int s = 0; s < p.S; ++s) s_off[c] += a.mean[s] * chan_dc<MULTI, TENSOR>(c, s, p);
+    for (int m = 0; m < p.M; ++m) {
+      const double w0 = a.mf_w[m * p.Nk] * (double)p.N;
+      s_off[p.mf_chan_j[m]] = a.mean[p.mf_j[m]] * w0;
+      if (p.mf_chan_i[m] >= 0) s_off[p.mf_chan_i[m]] = a.mean[p.mf_i[m]] * w0;
+    }
+    Measures<double> m0;
+    assemble<MULTI, TENSOR>(p, s_off, m0);
+    double phi0;
+    MeasureDerivs<double> d0;
+    double D0[NF];
+    if (fmt_phi_dphi<MODEL, double>(p.A, p.B, m0, phi0, d0)) {
+      fold_derivs<MULTI, TENSOR>(p, d0, D0);
+    } else {
+#pragma unroll
+      for (int c = 0; c < NF; ++c) D0[c] = 0.0;
+    }
+#pragma unroll
+    for (int c = 0; c < NF; ++c) {
+      s_dbar[c] = D0[c];
+      if (blockIdx.x == 0) a.dbar_out[c] = D0[c];
+    }
+  }
+  __syncthreads();
+}
+
+// Everything computed at one grid point: Phi and the derivative channels, the
+// ideal-gas / external / mean-field local force, and the reduction terms.
+// cur[0..NF) are the FMT channel values, cur[NF..NF+n_mf_pre) the first
+// mean-field channels (others are read from `chan`).
+template <int MODEL, bool MULTI, typename RT, int NPRE>
+__device__ __forceinline__ void point_body(const EvalParams& p, const PointwiseArgs& a, const double* cur,
+                                           int n_mf_pre, const double* rs, const double* vs, long long idx,
+                                           const RT* __restrict__ chan, RT* __restrict__ deriv,
+                                           const double* s_off, const double* s_dbar, double* acc) {
+  constexpr bool TENSOR = model_has_tensor(MODEL);
+  using L = Lay<MULTI, TENSOR>;
+  constexpr bool SPLIT = sizeof(RT) == sizeof(float);
+  constexpr int NF = L::NFMT;
+  const long long N = p.N;
+  double n[NF];
+#pragma unroll
+  for (int c = 0; c < NF; ++c) n[c] = cur[c] + (SPLIT ? s_off[c] : 0.0);
+  Measures<double> m;
+  assemble<MULTI, TENSOR>(p, n, m);
+  double phi = 0.0;
+  MeasureDerivs<double> dm;
+  double D[NF];
+  if (fmt_phi_dphi<MODEL, double>(p.A, p.B, m, phi, dm)) {
+    fold_derivs<MULTI, TENSOR>(p, dm, D);
+  } else {
+    phi = 0.0;
+#pragma unroll
+    for (int c = 0; c < NF; ++c) D[c] = 0.0;
+  }
+  acc[kTermHS] += phi;
+#pragma unroll
+  for (int c = 0; c < NF; ++c) __stcs(deriv + c * N + idx, (RT)(SPLIT ? D[c] - s_dbar[c] : D[c]));
+  double f[kMaxSpecies];
+#pragma unroll
+  for (int s = 0; s < kMaxSpecies; ++s) {
+    if (s < p.S) {
+      const double r = rs[s];
+      const double v = vs[s];
+      const double lr = log(r < 1e-300 ? 1e-300 : r);
+      acc[kTermId] += r * (lr - 1.0);
+      acc[kTermExt] += r * v;
+      acc[kTermN0 + s] += r;
+      f[s] = (lr - a.mu[s]) * p.dv + v * p.dv;
+    }
+  }
+  for (int q = 0; q < p.M; ++q) {
+    const int i = p.mf_i[q], j = p.mf_j[q];
+    const int cjx = p.mf_chan_j[q];
+    const int cix = p.mf_chan_i[q];
+    double cj = 0.0, ci = 0.0;
+    bool hj = false, hi = false;
+#pragma unroll
+    for (int c = NF; c < NPRE; ++c) {
+      if (c == cjx && c - NF < n_mf_pre) { cj = cur[c]; hj = true; }
+      if (c == cix && c - NF < n_mf_pre) { ci = cur[c]; hi = true; }
+    }
+    if (!hj) cj = (double)chan[cjx * N + idx];
+    cj += SPLIT ? s_off[cjx] : 0.0;
+    double ri = 0.0;
+#pragma unroll
+    for (int s = 0; s < kMaxSpecies; ++s)
+      if (s == i) ri = rs[s];
+    acc[kTermMF] += 0.5 * ri * cj;
+    if (i == j) {
+#pragma unroll
+      for (int s = 0; s < kMaxSpecies; ++s)
+        if (s == i) f[s] += cj * p.dv;
+    } else {
+      if (!hi) ci = (double)chan[cix * N + idx];
+      ci += SPLIT ? s_off[cix] : 0.0;
+#pragma unroll
+      for (int s = 0; s < kMaxSpecies; ++s) {
+        if (s == i) f[s] += 0.5 * cj * p.dv;
+        if (s == j) f[s] += 0.5 * ci * p.dv;
+      }
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < kMaxSpecies; ++s)
+    if (s < p.S) __stcs(a.force + s * N + idx, f[s]);
+}
+
+// Plain variant (any N): each thread loads the next point's inputs before
+// working on the current one.
+template <int MODEL, bool MULTI, typename RT>
 __global__ void __launch_bounds__(256) k_pointwise(EvalParams p, const RT* __restrict__ chan, RT* __restrict__ deriv,
                                                    PointwiseArgs a) {
+  constexpr bool TENSOR = model_has_tensor(MODEL);
   using L = Lay<MULTI, TENSOR>;
   constexpr bool SPLIT = sizeof(RT) == sizeof(float);
   constexpr int NT = 4 + kMaxSpecies;
   constexpr int NF = L::NFMT;
+  constexpr int NPRE = NF + 2;
   __shared__ double s_off[kMaxChannels];
   __shared__ double s_dbar[NF];
-  if (SPLIT) {
-    if (threadIdx.x == 0) {
-      for (int c = 0; c < p.n_chan; ++c) s_off[c] = 0.0;
-#pragma unroll
-      for (int c = 0; c < NF; ++c)
-        for (int s = 0; s < p.S; ++s) s_off[c] += a.mean[s] * chan_dc<MULTI, TENSOR>(c, s, p);
-      for (int m = 0; m < p.M; ++m) {
-        const double w0 = a.mf_w[m * p.Nk] * (double)p.N;
-        s_off[p.mf_chan_j[m]] = a.mean[p.mf_j[m]] * w0;
-        if (p.mf_chan_i[m] >= 0) s_off[p.mf_chan_i[m]] = a.mean[p.mf_i[m]] * w0;
-      }
-      Measures<double> m0;
-      assemble<MULTI, TENSOR>(p, s_off, m0);
-      double phi0;
-      MeasureDerivs<double> d0;
-      double D0[NF];
-      if (fmt_phi_dphi<double>(p.model, p.A, p.B, TENSOR, m0, phi0, d0)) {
-        fold_derivs<MULTI, TENSOR>(p, d0, D0);
-      } else {
-#pragma unroll
-        for (int c = 0; c < NF; ++c) D0[c] = 0.0;
-      }
-#pragma unroll
-      for (int c = 0; c < NF; ++c) {
-        s_dbar[c] = D0[c];
-        if (blockIdx.x == 0) a.dbar_out[c] = D0[c];
-      }
-    }
-    __syncthreads();
-  }
+  if (SPLIT) split_prologue<MODEL, MULTI>(p, a, s_off, s_dbar);
   const long long N = p.N;
   double acc[NT];
 #pragma unroll
   for (int t = 0; t < NT; ++t) acc[t] = 0.0;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N;
-       idx += (long long)gridDim.x * blockDim.x) {
-    double n[NF];
+  const int n_mf_pre = (p.n_chan - NF) < 2 ? (p.n_chan - NF) : 2;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N; idx += stride) {
+    double cur[NPRE], rs[kMaxSpecies], vs[kMaxSpecies];
 #pragma unroll
-    for (int c = 0; c < NF; ++c) n[c] = (double)chan[c * N + idx] + (SPLIT ? s_off[c] : 0.0);
-    Measures<double> m;
-    assemble<MULTI, TENSOR>(p, n, m);
-    double phi = 0.0;
-    MeasureDerivs<double> dm;
-    double D[NF];
-    if (fmt_phi_dphi<double>(p.model, p.A, p.B, TENSOR, m, phi, dm)) {
-      fold_derivs<MULTI, TENSOR>(p, dm, D);
-    } else {
-      phi = 0.0;
-#pragma unroll
-      for (int c = 0; c < NF; ++c) D[c] = 0.0;
-    }
-    acc[kTermHS] += phi;
-#pragma unroll
-    for (int c = 0; c < NF; ++c) deriv[c * N + idx] = (RT)(SPLIT ? D[c] - s_dbar[c] : D[c]);
-    // ideal gas, external field, mean field (local parts of the force)
-    double f[kMaxSpecies];
-    double rs[kMaxSpecies];
+    for (int q = 0; q < NPRE; ++q)
+      if (q < NF || q - NF < n_mf_pre) cur[q] = (double)__ldcs(chan + q * N + idx);
 #pragma unroll
     for (int s = 0; s < kMaxSpecies; ++s) {
       if (s < p.S) {
-        const double r = a.rho[s * N + idx];
-        const double v = a.vext ? a.vext[s * N + idx] : 0.0;
-        const double lr = log(r < 1e-300 ? 1e-300 : r);
-        rs[s] = r;
-        acc[kTermId] += r * (lr - 1.0);
-        acc[kTermExt] += r * v;
-        acc[kTermN0 + s] += r;
-        f[s] = (lr - a.mu[s]) * p.dv + v * p.dv;
+        rs[s] = __ldcs(a.rho + s * N + idx);
+        vs[s] = a.vext ? __ldcs(a.vext + s * N + idx) : 0.0;
       }
     }
-    for (int q = 0; q < p.M; ++q) {
-      const int i = p.mf_i[q], j = p.mf_j[q];
-      const int cjx = p.mf_chan_j[q];
-      const double cj = (double)chan[cjx * N + idx] + (SPLIT ? s_off[cjx] : 0.0);
-      double ri = 0.0;
+    point_body<MODEL, MULTI, RT, NPRE>(p, a, cur, n_mf_pre, rs, vs, idx, chan, deriv, s_off, s_dbar, acc);
+  }
+  block_reduce_store<NT>(acc, p.n_terms, a.partials);
+}
+
+// ---- TMA-staged variant (N % 4 == 0) -----------------------------------
+//
+// Each CTA walks tiles of 256 points.  One elected thread streams every input
+// segment of a tile (channel values, rho, V_ext) from HBM into a 3-stage
+// shared-memory ring with cp.async.bulk (TMA bulk copies, no multicast),
+// signalled by an mbarrier with transaction counts; all 256 threads then read
+// their point from shared memory.  The FP64 work of a tile overlaps the
+// loads of the next two, independent of the register budget.
+
+__device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
+  return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// Bounded wait: gives up after `limit` polls, so a lost transaction can never
+// hang the GPU; the caller records the failure in the engine's error word.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit) {
+  for (long long it = 0; it < limit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+constexpr int kTmaTile = 256;
+constexpr int kTmaStages = 3;
+constexpr long long kWaitLimit = 1ll << 26;
+
+template <bool MULTI, bool TENSOR, typename RT>
+__host__ __device__ constexpr int tma_stage_bytes(int S, bool vext) {
+  return (Lay<MULTI, TENSOR>::NFMT + 2) * kTmaTile * (int)sizeof(RT) + S * kTmaTile * 8 * (vext ? 2 : 1);
+}
+
+template <int MODEL, bool MULTI, typename RT>
+__global__ void __launch_bounds__(kTmaTile) k_pointwise_tma(EvalParams p, const RT* __restrict__ chan,
+                                                            RT* __restrict__ deriv, PointwiseArgs a, int* err) {
+  constexpr bool TENSOR = model_has_tensor(MODEL);
+  using L = Lay<MULTI, TENSOR>;
+  constexpr bool SPLIT = sizeof(RT) == sizeof(float);
+  constexpr int NT = 4 + kMaxSpecies;
+  constexpr int NF = L::NFMT;
+  constexpr int NPRE = NF + 2;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bars[kTmaStages];
+  __shared__ double s_off[kMaxChannels];
+  __shared__ double s_dbar[NF];
+  __shared__ int s_fail;
+  const bool has_v = a.vext != nullptr;
+  const int S = p.S;
+  const int n_mf_pre = (p.n_chan - NF) < 2 ? (p.n_chan - NF) : 2;
+  const int n_in = NF + n_mf_pre;  // channel segments per tile
+  const int stage_bytes = NPRE * kTmaTile * (int)sizeof(RT) + S * kTmaTile * 8 * (has_v ? 2 : 1);
+  const long long N = p.N;
+  const long long ntiles = (N + kTmaTile - 1) / kTmaTile;
+  const long long mine = (blockIdx.x < ntiles) ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int st = 0; st < kTmaStages; ++st) mbar_init(&bars[st], 1);
+    s_fail = 0;
+    fence_mbar_init();
+  }
+  if (SPLIT) split_prologue<MODEL, MULTI>(p, a, s_off, s_dbar);
+  __syncthreads();
+
+  auto stage_ptr = [&](int st) { return smem + (size_t)st * stage_bytes; };
+  auto issue = [&](long long i) {  // local tile i -> stage i % kTmaStages
+    const int st = (int)(i % kTmaStages);
+    const long long tile = blockIdx.x + i * gridDim.x;
+    const long long start = tile * kTmaTile;
+    const long long cnt = (N - start) < kTmaTile ? (N - start) : kTmaTile;
+    const uint32_t cb = (uint32_t)(cnt * sizeof(RT));
+    const uint32_t db = (uint32_t)(cnt * 8);
+    unsigned char* base = stage_ptr(st);
+    mbar_arrive_expect_tx(&bars[st], cb * n_in + db * S * (has_v ? 2 : 1));
+    for (int q = 0; q < n_in; ++q)
+      bulk_copy_g2s(base + (size_t)q * kTmaTile * sizeof(RT), chan + q * N + start, cb, &bars[st]);
+    unsigned char* rb = base + (size_t)NPRE * kTmaTile * sizeof(RT);
+    for (int s = 0; s < S; ++s) bulk_copy_g2s(rb + (size_t)s * kTmaTile * 8, a.rho + s * N + start, db, &bars[st]);
+    if (has_v)
+      for (int s = 0; s < S; ++s)
+        bulk_copy_g2s(rb + (size_t)(S + s) * kTmaTile * 8, a.vext + s * N + start, db, &bars[st]);
+  };
+
+  if (tid == 0)
+    for (long long i = 0; i < mine && i < kTmaStages; ++i) issue(i);
+
+  double acc[NT];
 #pragma unroll
-      for (int s = 0; s < kMaxSpecies; ++s)
-        if (s == i) ri = rs[s];
-      acc[kTermMF] += 0.5 * ri * cj;
-      if (i == j) {
+  for (int t = 0; t < NT; ++t) acc[t] = 0.0;
+  long long done = 0;
+  for (long long i = 0; i < mine; ++i) {
+    const int st = (int)(i % kTmaStages);
+    const uint32_t par = (uint32_t)((i / kTmaStages) & 1);
+    if (!mbar_wait_bounded(&bars[st], par, kWaitLimit)) atomicExch(&s_fail, 1);
+    __syncthreads();
+    if (s_fail) break;
+    const long long tile = blockIdx.x + i * gridDim.x;
+    const long long idx = tile * kTmaTile + tid;
+    if (idx < N) {
+      const RT* cs = reinterpret_cast<const RT*>(stage_ptr(st));
+      const double* rb = reinterpret_cast<const double*>(stage_ptr(st) + (size_t)NPRE * kTmaTile * sizeof(RT));
+      double cur[NPRE], rs[kMaxSpecies], vs[kMaxSpecies];
 #pragma unroll
-        for (int s = 0; s < kMaxSpecies; ++s)
-          if (s == i) f[s] += cj * p.dv;
-      } else {
-        const int cix = p.mf_chan_i[q];
-        const double ci = (double)chan[cix * N + idx] + (SPLIT ? s_off[cix] : 0.0);
+      for (int q = 0; q < NPRE; ++q)
+        if (q < NF || q - NF < n_mf_pre) cur[q] = (double)cs[q * kTmaTile + tid];
 #pragma unroll
-        for (int s = 0; s < kMaxSpecies; ++s) {
-          if (s == i) f[s] += 0.5 * cj * p.dv;
-          if (s == j) f[s] += 0.5 * ci * p.dv;
+      for (int s = 0; s < kMaxSpecies; ++s) {
+        if (s < S) {
+          rs[s] = rb[s * kTmaTile + tid];
+          vs[s] = has_v ? rb[(S + s) * kTmaTile + tid] : 0.0;
         }
       }
+      point_body<MODEL, MULTI, RT, NPRE>(p, a, cur, n_mf_pre, rs, vs, idx, chan, deriv, s_off, s_dbar, acc);
     }
-#pragma unroll
-    for (int s = 0; s < kMaxSpecies; ++s)
-      if (s < p.S) a.force[s * N + idx] = f[s];
+    __syncthreads();  // every thread is done with stage st
+    done = i + 1;
+    if (tid == 0 && i + kTmaStages < mine) {
+      fence_proxy_async();
+      issue(i + kTmaStages);
+    }
+  }
+  if (s_fail) {
+    // drain the copies still in flight (bounded) before the CTA exits
+    if (tid == 0) {
+      *err = 1;
+      for (long long i = done; i < mine && i < done + kTmaStages; ++i)
+        mbar_wait_bounded(&bars[i % kTmaStages], (uint32_t)((i / kTmaStages) & 1), kWaitLimit);
+    }
+    __syncthreads();
   }
   block_reduce_store<NT>(acc, p.n_terms, a.partials);
 }
@@ -599,7 +785,7 @@ struct MuArgs {
 };
 
 __global__ void k_reduce_final(const double* __restrict__ partials, int nblocks, EvalParams p, MuArgs mu,
-                               double* __restrict__ out) {
+                               const int* __restrict__ err, double* __restrict__ out) {
   __shared__ double sh[4 + kMaxSpecies];
   const int warp = threadIdx.x >> 5;  // one warp per term
   const int n_terms = p.n_terms;
@@ -621,8 +807,9 @@ __global__ void k_reduce_final(const double* __restrict__ partials, int nblocks,
     if (p.M > 0) F += f_mf;
     double muN = 0.0;
     for (int s = 0; s < p.S; ++s) muN += mu.mu[s] * sh[kTermN0 + s] * dv;
-    out[0] = F;
-    out[1] = F - muN;
+    const bool bad = err && *err != 0;  // a bounded wait gave up: poison the result
+    out[0] = bad ? __longlong_as_double(0x7ff8000000000000ll) : F;
+    out[1] = bad ? __longlong_as_double(0x7ff8000000000000ll) : F - muN;
     out[2] = f_id;
     out[3] = f_ext;
     out[4] = f_hs;

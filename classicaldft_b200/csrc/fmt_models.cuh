@@ -75,8 +75,9 @@ struct FVals {
 // log(1 - eta), 1/(1 - eta) and 1/eta are formed once; every other quotient
 // of the reference's expressions is rewritten with these reciprocals, which
 // keeps the FP64 division count at two per point.
-template <class T>
-__device__ inline FVals<T> fmt_f(int model, T eta) {
+template <int MODEL, class T>
+__device__ __forceinline__ FVals<T> fmt_f(T eta) {
+  constexpr int model = MODEL;
   FVals<T> r;
   const double ev = val(eta);
   const T e = 1.0 - eta;
@@ -87,11 +88,11 @@ __device__ inline FVals<T> fmt_f(int model, T eta) {
   r.df1 = -ie;
   const bool taylor = ev < 1e-6;
   T ih = cst<T>(0.0), ih2 = cst<T>(0.0);
-  if (!taylor && model != kRosenfeld && model != kEsFMT) {
+  if (!taylor && model != kRosenfeld && model != kEsFMT) {  // 1/eta only where it is used
     ih = 1.0 / eta;
     ih2 = ih * ih;
   }
-  if (model == kWhiteBearII) {
+  if constexpr (model == kWhiteBearII) {
     if (taylor) {
       r.f2 = 1.0 + eta * (1.0 + eta * (10.0 / 9.0 + (7.0 / 6.0) * eta));
       r.df2 = 1.0 + eta * (2.0 * (10.0 / 9.0) + 3.0 * (7.0 / 6.0) * eta);
@@ -103,12 +104,12 @@ __device__ inline FVals<T> fmt_f(int model, T eta) {
     r.f2 = ie;
     r.df2 = ie2;
   }
-  if (model == kRosenfeld || model == kEsFMT) {
+  if constexpr (model == kRosenfeld || model == kEsFMT) {
     r.f3 = ie2;
     r.df3 = 2.0 * ie2 * ie;
-  } else if (model == kRSLT || model == kWhiteBearI) {
+  } else if constexpr (model == kRSLT || model == kWhiteBearI) {
     if (taylor) {
-      if (model == kRSLT) {
+      if constexpr (model == kRSLT) {
         r.f3 = 1.0 + (2.0 / 3.0) * eta + 0.5 * eta * eta;
         r.df3 = (2.0 / 3.0) + eta;
       } else {
@@ -138,9 +139,10 @@ __device__ inline FVals<T> fmt_f(int model, T eta) {
 // Phi and all partial derivatives at one point (models.hpp:22-81, 169-357).
 // Returns false (and leaves outputs untouched) where eta < 1e-30: the
 // reference skips those points (hard_sphere.hpp:199-200).
-template <class T>
-__device__ inline bool fmt_phi_dphi(int model, double A, double B, bool tensor, const Measures<T>& m, T& phi,
-                                    MeasureDerivs<T>& dm) {
+template <int MODEL, class T>
+__device__ __forceinline__ bool fmt_phi_dphi(double A, double B, const Measures<T>& m, T& phi, MeasureDerivs<T>& dm) {
+  constexpr int model = MODEL;
+  constexpr bool tensor = model_has_tensor(MODEL);
   if (val(m.eta) < 1e-30) return false;
   constexpr double INV_24PI = 1.0 / (24.0 * kPi);
   constexpr double INV_8PI = 1.0 / (8.0 * kPi);
@@ -148,14 +150,13 @@ __device__ inline bool fmt_phi_dphi(int model, double A, double B, bool tensor, 
   constexpr double INV_36PI = 1.0 / (36.0 * kPi);
 
   // inner products (measures.hpp:34-44); T symmetric
-  const T* t = m.t;
-  T txx = t[0], txy = t[1], txz = t[2], tyy = t[3], tyz = t[4], tzz = t[5];
+  const T txx = m.t[0], txy = m.t[1], txz = m.t[2], tyy = m.t[3], tyz = m.t[4], tzz = m.t[5];
   T dot01 = m.v0[0] * m.v1[0] + m.v0[1] * m.v1[1] + m.v0[2] * m.v1[2];
   T dot11 = m.v1[0] * m.v1[0] + m.v1[1] * m.v1[1] + m.v1[2] * m.v1[2];
   T tt[6];   // TT = T*T (symmetric)
   T tv[3];   // T v1
   T trT2 = zero_like(m.eta), trT3 = zero_like(m.eta), qf = zero_like(m.eta);
-  if (tensor) {
+  if constexpr (tensor) {
     tt[0] = txx * txx + txy * txy + txz * txz;
     tt[1] = txx * txy + txy * tyy + txz * tyz;
     tt[2] = txx * txz + txy * tyz + txz * tzz;
@@ -173,62 +174,72 @@ __device__ inline bool fmt_phi_dphi(int model, double A, double B, bool tensor, 
   // Phi3 and its partials
   T p3, dp3_n2, dp3_v[3];
   const T n2 = m.n2;
-  if (model == kRosenfeld) {
+  if constexpr (model == kRosenfeld) {
     p3 = INV_24PI * (n2 * n2 * n2 - 3.0 * n2 * dot11);
     dp3_n2 = INV_8PI * (n2 * n2 - dot11);
+#pragma unroll
     for (int a = 0; a < 3; ++a) dp3_v[a] = -INV_4PI * n2 * m.v1[a];
-  } else if (model == kRSLT) {
+  } else if constexpr (model == kRSLT) {
     if (val(n2) < 1e-30) {
       p3 = zero_like(n2);
       dp3_n2 = zero_like(n2);
-      for (int a = 0; a < 3; ++a) dp3_v[a] = zero_like(n2);
+  #pragma unroll
+    for (int a = 0; a < 3; ++a) dp3_v[a] = zero_like(n2);
     } else {
       T xi = dot11 / (n2 * n2);
       if (val(xi) > 1.0) xi = cst<T>(1.0);  // std::min(xi, 1.0), models.hpp:210
       T q = 1.0 - xi;
       p3 = INV_36PI * n2 * n2 * n2 * q * q * q;
       dp3_n2 = INV_36PI * 3.0 * n2 * n2 * q * q * (1.0 + xi);
-      for (int a = 0; a < 3; ++a) dp3_v[a] = INV_36PI * (-6.0) * n2 * q * q * m.v1[a];
+  #pragma unroll
+    for (int a = 0; a < 3; ++a) dp3_v[a] = INV_36PI * (-6.0) * n2 * q * q * m.v1[a];
     }
-  } else if (model == kWhiteBearI || model == kWhiteBearII) {
+  } else if constexpr (model == kWhiteBearI || model == kWhiteBearII) {
     p3 = INV_24PI * 3.0 * (n2 * trT2 - n2 * dot11 + qf - trT3);
     dp3_n2 = INV_24PI * 3.0 * (trT2 - dot11);
+#pragma unroll
     for (int a = 0; a < 3; ++a) dp3_v[a] = INV_24PI * (-6.0 * n2 * m.v1[a] + 6.0 * tv[a]);
   } else {  // esFMT(A, B)
     T phi_a = n2 * n2 * n2 - 3.0 * n2 * dot11 + 3.0 * qf - trT3;
     T phi_b = n2 * n2 * n2 - 3.0 * n2 * trT2 + 2.0 * trT3;
     p3 = INV_24PI * (A * phi_a + B * phi_b);
     dp3_n2 = INV_24PI * (A * (3.0 * n2 * n2 - 3.0 * dot11) + B * (3.0 * n2 * n2 - 3.0 * trT2));
+#pragma unroll
     for (int a = 0; a < 3; ++a) dp3_v[a] = INV_24PI * A * (-6.0 * n2 * m.v1[a] + 6.0 * tv[a]);
   }
 
-  FVals<T> f = fmt_f<T>(model, m.eta);
+  FVals<T> f = fmt_f<MODEL, T>(m.eta);
   T c2 = m.n1 * n2 - dot01;
   phi = -m.n0 * f.f1 + c2 * f.f2 + p3 * f.f3;
   dm.d_eta = -m.n0 * f.df1 + c2 * f.df2 + p3 * f.df3;
   dm.d_n0 = -f.f1;
   dm.d_n1 = n2 * f.f2;
   dm.d_n2 = m.n1 * f.f2 + dp3_n2 * f.f3;
+#pragma unroll
   for (int a = 0; a < 3; ++a) {
     dm.d_v0[a] = -m.v1[a] * f.f2;
     dm.d_v1[a] = -m.v0[a] * f.f2 + dp3_v[a] * f.f3;
   }
-  if (tensor) {
+  if constexpr (tensor) {
     // dPhi3/dT_ij (models.hpp:39-45, 348-357); T and TT symmetric
+#pragma unroll
     for (int i = 0; i < 3; ++i) {
-      for (int j = i; j < 3; ++j) {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        if (j < i) continue;
         const int c = tensor_index(i, j);
         T vv = m.v1[i] * m.v1[j];
         T d;
-        if (model == kEsFMT) {
-          d = INV_8PI * A * (vv - tt[c]) + INV_4PI * B * (-n2 * t[c] + tt[c]);
+        if constexpr (model == kEsFMT) {
+          d = INV_8PI * A * (vv - tt[c]) + INV_4PI * B * (-n2 * m.t[c] + tt[c]);
         } else {
-          d = INV_8PI * (vv + 2.0 * n2 * t[c] - 3.0 * tt[c]);
+          d = INV_8PI * (vv + 2.0 * n2 * m.t[c] - 3.0 * tt[c]);
         }
         dm.d_t[c] = d * f.f3;
       }
     }
   } else {
+#pragma unroll
     for (int c = 0; c < 6; ++c) dm.d_t[c] = zero_like(m.eta);
   }
   return true;

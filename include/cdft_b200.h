@@ -153,6 +153,12 @@ CDFT_API int cdft_total(cdft_engine* engine, const double* rho, const double* ve
 CDFT_API int cdft_total_device(cdft_engine* engine, const double* rho, const double* vext, const double* mu, double* force,
                       double* scalars, void* stream);
 
+/* Status of earlier asynchronous calls on `stream`: CDFT_ERR_RUNTIME if a
+ * bounded device-side wait gave up (the scalars of that call are NaN), else
+ * CDFT_OK.  Synchronises the stream and clears the flag.  No reference
+ * counterpart: the reference is synchronous CPU code. */
+CDFT_API int cdft_engine_status(cdft_engine* engine, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
