@@ -11,4 +11,8 @@ from .functionals import (BARKER_HENDERSON, WEEKS_CHANDLER_ANDERSEN, Engine, EsF
                           WhiteBearI, WhiteBearII, interaction_weight, make_grid, make_lennard_jones,
                           make_ten_wolde_frenkel, make_wang_ramirez_dobnikar_frenkel, make_weights, total)
 
+from .algorithms import (Bounded, EigenvalueResult, EigenvalueSolver, Fire, MinimizationResult, Minimizer,  # noqa: F401
+                         SaddleResult, Search, Simulation, StepConfig, Unbounded, hessian_times_vector,
+                         integrating_factor_step)
+
 __version__ = "0.1.0"

@@ -41,6 +41,44 @@ class CInteraction(ctypes.Structure):
                 ("a_vdw", ctypes.c_double)]
 
 
+class CFireParams(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("dt_max", ctypes.c_double), ("dt_min", ctypes.c_double),
+                ("alpha_start", ctypes.c_double), ("f_inc", ctypes.c_double), ("f_dec", ctypes.c_double),
+                ("f_alpha", ctypes.c_double), ("n_delay", ctypes.c_int), ("max_uphill", ctypes.c_int),
+                ("force_tolerance", ctypes.c_double), ("max_steps", ctypes.c_int)]
+
+
+class CMinimizerConfig(ctypes.Structure):
+    _fields_ = [("fire", CFireParams), ("mode", ctypes.c_int), ("parametrization", ctypes.c_int),
+                ("rho_min", ctypes.c_double), ("rho_max", ctypes.c_double), ("homogeneous_boundary", ctypes.c_int),
+                ("chemical_potential", ctypes.c_double), ("target_mass", ctypes.c_double),
+                ("boundary_mass", ctypes.c_double), ("use_monitor", ctypes.c_int), ("check_interval", ctypes.c_int)]
+
+
+class CMinimizerResult(ctypes.Structure):
+    _fields_ = [("free_energy", ctypes.c_double), ("grand_potential", ctypes.c_double),
+                ("rms_force", ctypes.c_double), ("iterations", ctypes.c_int), ("converged", ctypes.c_int),
+                ("uphill_error", ctypes.c_int)]
+
+
+class CDDFTConfig(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("diffusion_coefficient", ctypes.c_double),
+                ("min_density", ctypes.c_double), ("dt_max", ctypes.c_double), ("fp_tolerance", ctypes.c_double),
+                ("fp_max_iterations", ctypes.c_int)]
+
+
+class CEigenConfig(ctypes.Structure):
+    _fields_ = [("tolerance", ctypes.c_double), ("max_iterations", ctypes.c_int), ("hessian_eps", ctypes.c_double),
+                ("exact_hvp", ctypes.c_int), ("seed", ctypes.c_ulonglong)]
+
+
+class CSaddleConfig(ctypes.Structure):
+    _fields_ = [("fire", CFireParams), ("eigen", CEigenConfig), ("rho_min", ctypes.c_double),
+                ("omega_tolerance", ctypes.c_double), ("tolerance_start", ctypes.c_double),
+                ("tolerance_factor", ctypes.c_double), ("max_outer_iterations", ctypes.c_int),
+                ("eigenvalue_clear_count", ctypes.c_int)]
+
+
 class EngineError(RuntimeError):
     """A failed C-ABI call; ``code`` is the CDFT_ERR_* status."""
 
@@ -79,6 +117,18 @@ def lib():
         "cdft_total": [vp, vp, vp, c_double_p, vp, c_double_p],
         "cdft_total_device": [vp, vp, vp, c_double_p, vp, vp, vp],
         "cdft_engine_status": [vp, vp],
+        "cdft_minimize": [vp, ctypes.POINTER(CMinimizerConfig), vp, vp, vp, ctypes.c_double,
+                          ctypes.POINTER(CMinimizerResult), vp],
+        "cdft_ddft_step": [vp, ctypes.POINTER(CDDFTConfig), ctypes.c_double, vp, c_double_p,
+                           ctypes.POINTER(ctypes.c_int), vp],
+        "cdft_ddft_run": [vp, ctypes.POINTER(CDDFTConfig), ctypes.c_double, ctypes.c_int, vp, c_double_p, c_double_p,
+                          vp],
+        "cdft_hvp": [vp, vp, vp, ctypes.c_double, ctypes.c_int, vp, vp],
+        "cdft_hvp_fd": [vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, vp, vp],
+        "cdft_eigen_solve": [vp, ctypes.POINTER(CEigenConfig), vp, ctypes.c_double, vp, ctypes.c_int, c_double_p,
+                             ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), vp],
+        "cdft_saddle_find": [vp, ctypes.POINTER(CSaddleConfig), vp, ctypes.c_double, ctypes.c_double, vp,
+                             c_double_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), vp],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)

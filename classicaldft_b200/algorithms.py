@@ -1,0 +1,334 @@
+"""Host-side mirror of the reference's algorithms, running on the GPU engine.
+
+FIRE2 minimisation (fire.hpp, minimization.hpp), DDFT (dynamics.hpp) and the
+saddle-point search (saddle_point.hpp) keep the reference's names,
+parameters and defaults; their state lives in HBM and the steps run as
+device kernels of libcdft_b200.so.  Densities are exchanged as NumPy arrays
+(host) or torch CUDA tensors (device, no copy).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from .functionals import Model, Weights
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _dev(x):
+    """(tensor on the current CUDA device, was_host) for a numpy array or tensor."""
+    torch = _torch()
+    if isinstance(x, torch.Tensor):
+        if not x.is_cuda or x.dtype != torch.float64 or not x.is_contiguous():
+            raise ValueError("device vectors must be contiguous float64 CUDA tensors")
+        return x, False
+    return torch.tensor(np.ascontiguousarray(x, dtype=np.float64).reshape(-1), device="cuda"), True
+
+
+def _stream():
+    return _torch().cuda.current_stream().cuda_stream
+
+
+# ---------------------------------------------------------------- FIRE
+
+
+@dataclass
+class Fire:
+    """fire.hpp:33-44: FIRE2 parameters (same defaults)."""
+
+    dt: float = 1e-3
+    dt_max: float = 1e-2
+    dt_min: float = 1e-8
+    alpha_start: float = 0.1
+    f_inc: float = 1.1
+    f_dec: float = 0.5
+    f_alpha: float = 0.99
+    n_delay: int = 5
+    max_uphill: int = 20
+    force_tolerance: float = 0.1
+    max_steps: int = 10000
+
+    def c(self):
+        return _lib.CFireParams(self.dt, self.dt_max, self.dt_min, self.alpha_start, self.f_inc, self.f_dec,
+                                self.f_alpha, self.n_delay, self.max_uphill, self.force_tolerance, self.max_steps)
+
+
+@dataclass
+class Unbounded:
+    """minimization.hpp:27-29: rho = rho_min + x^2."""
+
+    rho_min: float = 1e-18
+
+
+@dataclass
+class Bounded:
+    """minimization.hpp:34-37: rho = rho_min + (rho_max - rho_min) x^2/(1+x^2)."""
+
+    rho_min: float = 1e-18
+    rho_max: float = 1.0
+
+
+@dataclass
+class MinimizationResult:
+    """minimization.hpp:114-121."""
+
+    densities: list
+    free_energy: float
+    grand_potential: float
+    rms_force: float
+    iterations: int
+    converged: bool
+
+
+@dataclass
+class Minimizer:
+    """minimization.hpp:123-147 on the device.
+
+    ``refine``: optional FP64 Weights of the same model; when given, the
+    minimiser switches to them (defect correction) once the energy monitor
+    falls below ``refine_switch`` x tolerance.
+    """
+
+    fire: Fire = field(default_factory=Fire)
+    param: object = field(default_factory=Unbounded)
+    use_homogeneous_boundary: bool = True
+    check_interval: int = 25
+    refine: Weights = None
+    refine_switch: float = 10.0
+
+    def _run(self, weights: Weights, rho, mode, mu, target_mass=0.0, boundary_mass=0.0, direction=None,
+             use_monitor=True):
+        torch = _torch()
+        d, host = _dev(rho)
+        if not host:
+            d = d.clone()
+        cfg = _lib.CMinimizerConfig()
+        cfg.fire = self.fire.c()
+        cfg.mode = mode
+        if isinstance(self.param, Bounded):
+            cfg.parametrization, cfg.rho_min, cfg.rho_max = 1, self.param.rho_min, self.param.rho_max
+        else:
+            cfg.parametrization, cfg.rho_min, cfg.rho_max = 0, self.param.rho_min, 1.0
+        cfg.homogeneous_boundary = 1 if self.use_homogeneous_boundary else 0
+        cfg.chemical_potential = mu
+        cfg.target_mass = target_mass
+        cfg.boundary_mass = boundary_mass
+        cfg.use_monitor = 1 if use_monitor else 0
+        cfg.check_interval = self.check_interval
+        res = _lib.CMinimizerResult()
+        dirp = None
+        if direction is not None:
+            dd, _ = _dev(direction)
+            dirp = dd.data_ptr()
+        ref = self.refine.engine.handle if self.refine is not None else None
+        st = _lib.lib().cdft_minimize(weights.engine.handle, ctypes.byref(cfg), d.data_ptr(), dirp, ref,
+                                      self.refine_switch, ctypes.byref(res), _stream())
+        torch.cuda.synchronize()
+        if st != _lib.CDFT_OK:
+            msg = _lib.lib().cdft_last_error().decode()
+            if res.uphill_error:
+                raise RuntimeError(msg)
+            _lib.check(st)
+        out = d.cpu().numpy() if host else d
+        return MinimizationResult([out], res.free_energy, res.grand_potential, res.rms_force, res.iterations,
+                                  bool(res.converged))
+
+    def grand_potential(self, model: Model, weights: Weights, initial_density, chemical_potential):
+        """minimization.hpp:280-354."""
+        return self._run(weights, initial_density, 0, chemical_potential)
+
+    def fixed_mass(self, model: Model, weights: Weights, initial_density, chemical_potential, target_mass):
+        """minimization.hpp:182-278."""
+        return self._run(weights, initial_density, 1, chemical_potential, target_mass=target_mass)
+
+
+# ---------------------------------------------------------------- DDFT
+
+
+@dataclass
+class StepConfig:
+    """dynamics.hpp:26-33."""
+
+    dt: float = 1e-4
+    diffusion_coefficient: float = 1.0
+    min_density: float = 1e-18
+    dt_max: float = 1.0
+    fp_tolerance: float = 1e-4
+    fp_max_iterations: int = 100
+
+    def c(self):
+        return _lib.CDDFTConfig(self.dt, self.diffusion_coefficient, self.min_density, self.dt_max,
+                                self.fp_tolerance, self.fp_max_iterations)
+
+
+def integrating_factor_step(density, weights: Weights, config: StepConfig, chemical_potential=0.0):
+    """dynamics.hpp:333-401: returns (density, energy, dt_used); config.dt is
+    divided by 10 on restarts, as in the reference."""
+    torch = _torch()
+    d, host = _dev(density)
+    if not host:
+        d = d.clone()
+    c = config.c()
+    e = ctypes.c_double()
+    it = ctypes.c_int()
+    _lib.check(_lib.lib().cdft_ddft_step(weights.engine.handle, ctypes.byref(c), chemical_potential, d.data_ptr(),
+                                         ctypes.byref(e), ctypes.byref(it), _stream()))
+    torch.cuda.synchronize()
+    config.dt = c.dt
+    return (d.cpu().numpy() if host else d), e.value, c.dt
+
+
+@dataclass
+class Simulation:
+    """dynamics.hpp:564-693 (integrating-factor DDFT with adaptive dt)."""
+
+    step: StepConfig = field(default_factory=StepConfig)
+    n_steps: int = 1000
+
+    def run(self, densities, weights: Weights, chemical_potential=0.0):
+        torch = _torch()
+        d, host = _dev(densities[0] if isinstance(densities, (list, tuple)) else densities)
+        if not host:
+            d = d.clone()
+        c = self.step.c()
+        times = np.zeros(self.n_steps + 1)
+        energies = np.zeros(self.n_steps + 1)
+        _lib.check(_lib.lib().cdft_ddft_run(weights.engine.handle, ctypes.byref(c), chemical_potential, self.n_steps,
+                                            d.data_ptr(), times.ctypes.data_as(_lib.c_double_p),
+                                            energies.ctypes.data_as(_lib.c_double_p), _stream()))
+        torch.cuda.synchronize()
+        return {"densities": [d.cpu().numpy() if host else d], "times": times, "energies": energies, "dt": c.dt}
+
+
+# ---------------------------------------------------------- saddle point
+
+
+def hessian_times_vector(weights: Weights, rho, v, chemical_potential=0.0, exact=True, eps=1e-6,
+                         fixed_boundary=False, force_at_rho=None):
+    """H v of Omega at rho: exact (forward-over-reverse) or the reference's
+    forward difference (saddle_point.hpp:30-39)."""
+    torch = _torch()
+    r, host = _dev(rho)
+    vv, _ = _dev(v)
+    hv = torch.empty_like(r)
+    b = 1 if fixed_boundary else 0
+    L = _lib.lib()
+    if exact:
+        _lib.check(L.cdft_hvp(weights.engine.handle, r.data_ptr(), vv.data_ptr(), chemical_potential, b,
+                              hv.data_ptr(), _stream()))
+    else:
+        if force_at_rho is None:
+            f0 = torch.empty_like(r)
+            sc = torch.empty(10, dtype=torch.float64, device=r.device)
+            weights.engine.total_device(r.data_ptr(), None, [chemical_potential], f0.data_ptr(), sc.data_ptr(),
+                                        _stream())
+            if fixed_boundary:
+                mask = torch.tensor(weights_mask(weights), device=r.device, dtype=torch.bool)
+                f0[mask] = 0.0
+        else:
+            f0, _ = _dev(force_at_rho)
+        _lib.check(L.cdft_hvp_fd(weights.engine.handle, r.data_ptr(), f0.data_ptr(), vv.data_ptr(),
+                                 chemical_potential, eps, b, hv.data_ptr(), _stream()))
+    torch.cuda.synchronize()
+    return hv.cpu().numpy() if host else hv
+
+
+def weights_mask(weights: Weights):
+    g = weights.engine.grid
+    return g.boundary_mask().astype(bool)
+
+
+@dataclass
+class EigenvalueResult:
+    """saddle_point.hpp:151-156."""
+
+    eigenvector: object
+    eigenvalue: float
+    iterations: int
+    converged: bool
+
+
+@dataclass
+class EigenvalueSolver:
+    """saddle_point.hpp:158-169 (``exact_hvp`` replaces the FD product)."""
+
+    tolerance: float = 1e-4
+    max_iterations: int = 300
+    hessian_eps: float = 1e-6
+    exact_hvp: bool = False
+    seed: int = 42
+
+    def c(self):
+        return _lib.CEigenConfig(self.tolerance, self.max_iterations, self.hessian_eps, 1 if self.exact_hvp else 0,
+                                 self.seed)
+
+    def solve(self, weights: Weights, rho, chemical_potential=0.0, initial_guess=None):
+        torch = _torch()
+        r, host = _dev(rho)
+        if initial_guess is not None:
+            vec, _ = _dev(initial_guess)
+            vec = vec.clone()
+        else:
+            vec = torch.empty_like(r)
+        ev = ctypes.c_double()
+        it = ctypes.c_int()
+        cv = ctypes.c_int()
+        c = self.c()
+        _lib.check(_lib.lib().cdft_eigen_solve(weights.engine.handle, ctypes.byref(c), r.data_ptr(),
+                                               chemical_potential, vec.data_ptr(), 1 if initial_guess is not None
+                                               else 0, ctypes.byref(ev), ctypes.byref(it), ctypes.byref(cv),
+                                               _stream()))
+        torch.cuda.synchronize()
+        return EigenvalueResult(vec.cpu().numpy() if host else vec, ev.value, it.value, bool(cv.value))
+
+
+@dataclass
+class SaddleResult:
+    """saddle_point.hpp:313-320."""
+
+    density: object
+    eigenvector: object
+    grand_potential: float
+    eigenvalue: float
+    outer_iterations: int
+    converged: bool
+
+
+@dataclass
+class Search:
+    """saddle_point.hpp:324-353 (same defaults)."""
+
+    fire: Fire = field(default_factory=lambda: Fire(dt=1e-3, dt_max=1.0, alpha_start=0.01, f_alpha=1.0,
+                                                    force_tolerance=1e-4, max_steps=100000))
+    eigenvalue: EigenvalueSolver = field(default_factory=lambda: EigenvalueSolver(1e-4, 300, 1e-6))
+    param: Unbounded = field(default_factory=lambda: Unbounded(1e-18))
+    omega_tolerance: float = 1e-5
+    tolerance_start: float = 1e-3
+    tolerance_factor: float = 10.0
+    max_outer_iterations: int = 20
+    eigenvalue_clear_count: int = 2
+
+    def find(self, model: Model, weights: Weights, initial_density, chemical_potential, target_mass):
+        torch = _torch()
+        r, host = _dev(initial_density)
+        r = r.clone()
+        ev = torch.empty_like(r)
+        cfg = _lib.CSaddleConfig(self.fire.c(), self.eigenvalue.c(), self.param.rho_min, self.omega_tolerance,
+                                 self.tolerance_start, self.tolerance_factor, self.max_outer_iterations,
+                                 self.eigenvalue_clear_count)
+        out = (ctypes.c_double * 2)()
+        it = ctypes.c_int()
+        cv = ctypes.c_int()
+        _lib.check(_lib.lib().cdft_saddle_find(weights.engine.handle, ctypes.byref(cfg), r.data_ptr(),
+                                               chemical_potential, target_mass, ev.data_ptr(), out,
+                                               ctypes.byref(it), ctypes.byref(cv), _stream()))
+        torch.cuda.synchronize()
+        conv = (lambda t: t.cpu().numpy()) if host else (lambda t: t)
+        return SaddleResult(conv(r), conv(ev), out[0], out[1], it.value, bool(cv.value))

@@ -6,11 +6,13 @@
 #include <vector>
 
 #include "../../include/cdft_b200.h"
+#include "drivers.cuh"
 #include "engine.cuh"
 #include "physics.hpp"
 
 struct cdft_engine {
   cdft::Engine* impl;
+  cdft::Drivers* drivers;  // created on first driver call
 };
 
 namespace {
@@ -138,7 +140,7 @@ int cdft_create(cdft_engine** out, const long shape[3], double dx, int n_species
       is.a_vdw = interactions[m].a_vdw;
       spec.interactions.push_back(std::move(is));
     }
-    auto* e = new cdft_engine{nullptr};
+    auto* e = new cdft_engine{nullptr, nullptr};
     try {
       e->impl = new cdft::Engine(spec);
     } catch (...) {
@@ -152,6 +154,7 @@ int cdft_create(cdft_engine** out, const long shape[3], double dx, int n_species
 int cdft_destroy(cdft_engine* engine) {
   return guarded([&] {
     if (!engine) return;
+    delete engine->drivers;
     delete engine->impl;
     delete engine;
   });
@@ -213,6 +216,201 @@ int cdft_engine_status(cdft_engine* engine, void* stream) {
     if (!engine) throw std::invalid_argument("engine is NULL");
     if (engine->impl->take_error(static_cast<cudaStream_t>(stream)))
       throw cdft::Error(CDFT_ERR_RUNTIME, "a bounded device wait timed out in an earlier call");
+  });
+}
+
+namespace {
+
+cdft::Drivers& drivers_of(cdft_engine* e) {
+  if (!e) throw std::invalid_argument("engine is NULL");
+  if (!e->drivers) e->drivers = new cdft::Drivers(*e->impl);
+  return *e->drivers;
+}
+
+cdft::FireParams to_fire(const cdft_fire_params& f) {
+  cdft::FireParams p;
+  p.dt = f.dt;
+  p.dt_max = f.dt_max;
+  p.dt_min = f.dt_min;
+  p.alpha_start = f.alpha_start;
+  p.f_inc = f.f_inc;
+  p.f_dec = f.f_dec;
+  p.f_alpha = f.f_alpha;
+  p.n_delay = f.n_delay;
+  p.max_uphill = f.max_uphill;
+  p.force_tolerance = f.force_tolerance;
+  p.max_steps = f.max_steps;
+  if (!(p.dt > 0.0) || p.max_steps < 0) throw std::invalid_argument("FIRE: dt must be positive, max_steps >= 0");
+  return p;
+}
+
+cdft::Drivers::EigenConfig to_eigen(const cdft_eigen_config& c) {
+  cdft::Drivers::EigenConfig e;
+  e.tolerance = c.tolerance;
+  e.max_iterations = c.max_iterations;
+  e.hessian_eps = c.hessian_eps;
+  e.exact_hvp = c.exact_hvp;
+  e.seed = c.seed;
+  return e;
+}
+
+}  // namespace
+
+int cdft_minimize(cdft_engine* engine, const cdft_minimizer_config* cfg, double* rho, const double* direction,
+                  cdft_engine* refine, double refine_switch, cdft_minimizer_result* result, void* stream) {
+  return guarded([&] {
+    if (!cfg || !rho || !result) throw std::invalid_argument("cfg, rho and result are required");
+    cdft::Drivers& d = drivers_of(engine);
+    cdft::FireConfig fc;
+    fc.fire = to_fire(cfg->fire);
+    fc.mode = cfg->mode;
+    if (fc.mode < CDFT_MIN_GRAND_POTENTIAL || fc.mode > CDFT_MIN_SADDLE) throw std::invalid_argument("unknown mode");
+    fc.param = cfg->parametrization;
+    fc.rho_min = cfg->rho_min;
+    fc.rho_max = cfg->rho_max;
+    fc.homogeneous_boundary = cfg->homogeneous_boundary != 0;
+    fc.mu = cfg->chemical_potential;
+    fc.target_mass = cfg->target_mass;
+    fc.boundary_mass = cfg->boundary_mass;
+    fc.use_monitor = cfg->use_monitor != 0;
+    fc.check_interval = cfg->check_interval > 0 ? cfg->check_interval : 25;
+    cdft::FireResult r = d.fire_minimize(fc, rho, direction, static_cast<cudaStream_t>(stream),
+                                         refine ? refine->impl : nullptr, refine_switch);
+    result->free_energy = r.free_energy;
+    result->grand_potential = r.grand_potential;
+    result->rms_force = r.rms_force;
+    result->iterations = r.iterations;
+    result->converged = r.converged ? 1 : 0;
+    result->uphill_error = r.uphill_error ? 1 : 0;
+    if (r.uphill_error) throw cdft::Error(CDFT_ERR_RUNTIME, "fire::step: exceeded max uphill steps");
+  });
+}
+
+namespace {
+cdft::Drivers::DDFTConfig to_ddft(const cdft_ddft_config& c, double mu) {
+  cdft::Drivers::DDFTConfig d;
+  d.dt = c.dt;
+  d.diffusion = c.diffusion_coefficient;
+  d.min_density = c.min_density;
+  d.dt_max = c.dt_max;
+  d.fp_tolerance = c.fp_tolerance;
+  d.fp_max_iterations = c.fp_max_iterations;
+  d.mu = mu;
+  if (!(d.dt > 0.0)) throw std::invalid_argument("DDFT: dt must be positive");
+  return d;
+}
+}  // namespace
+
+int cdft_ddft_step(cdft_engine* engine, cdft_ddft_config* cfg, double chemical_potential, double* rho,
+                   double* energy, int* fp_iterations, void* stream) {
+  return guarded([&] {
+    if (!cfg || !rho) throw std::invalid_argument("cfg and rho are required");
+    cdft::Drivers& d = drivers_of(engine);
+    cdft::Drivers::DDFTConfig dc = to_ddft(*cfg, chemical_potential);
+    const double e = d.ddft_step(dc, rho, static_cast<cudaStream_t>(stream), fp_iterations);
+    cfg->dt = dc.dt;
+    if (energy) *energy = e;
+  });
+}
+
+int cdft_ddft_run(cdft_engine* engine, cdft_ddft_config* cfg, double chemical_potential, int n_steps, double* rho,
+                  double* times, double* energies, void* stream) {
+  return guarded([&] {
+    if (!cfg || !rho || n_steps < 0) throw std::invalid_argument("cfg, rho and n_steps >= 0 are required");
+    cdft::Drivers& d = drivers_of(engine);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cdft::Drivers::DDFTConfig dc = to_ddft(*cfg, chemical_potential);
+    // Simulation::run (dynamics.hpp:597-649): initial energy, then steps with
+    // the adaptive time step.
+    double* fscratch = nullptr;
+    CDFT_CUDA(cudaMalloc(&fscratch, sizeof(double) * engine->impl->points()));
+    try {
+      const double e0 = d.force(rho, fscratch, chemical_potential, 0, st);
+      if (times) times[0] = 0.0;
+      if (energies) energies[0] = e0;
+      int successes = 0;
+      double time = 0.0;
+      for (int step = 1; step <= n_steps; ++step) {
+        const double dt_before = dc.dt;
+        const double e = d.ddft_step(dc, rho, st, nullptr);
+        const double dt_used = dc.dt;
+        time += dt_used;
+        if (dt_used < dt_before)
+          successes = 0;
+        else
+          ++successes;
+        if (successes >= 5 && dc.dt < dc.dt_max) {
+          dc.dt = std::min(2.0 * dc.dt, dc.dt_max);
+          successes = 0;
+        }
+        if (times) times[step] = time;
+        if (energies) energies[step] = e;
+      }
+    } catch (...) {
+      cudaFree(fscratch);
+      throw;
+    }
+    cudaFree(fscratch);
+    cfg->dt = dc.dt;
+  });
+}
+
+int cdft_hvp(cdft_engine* engine, const double* rho, const double* v, double chemical_potential, int boundary,
+             double* hv, void* stream) {
+  return guarded([&] {
+    if (!rho || !v || !hv) throw std::invalid_argument("rho, v and hv are required");
+    if (engine && engine->impl->species() != 1) {
+      double mu[4] = {chemical_potential, chemical_potential, chemical_potential, chemical_potential};
+      engine->impl->hvp(rho, v, mu, hv, static_cast<cudaStream_t>(stream));
+      return;
+    }
+    drivers_of(engine).hvp_exact(rho, v, hv, chemical_potential, boundary, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int cdft_hvp_fd(cdft_engine* engine, const double* rho, const double* force_at_rho, const double* v,
+                double chemical_potential, double eps, int boundary, double* hv, void* stream) {
+  return guarded([&] {
+    if (!rho || !force_at_rho || !v || !hv || !(eps > 0.0)) throw std::invalid_argument("bad HVP arguments");
+    drivers_of(engine).hvp_fd(rho, force_at_rho, v, hv, eps, chemical_potential, boundary,
+                              static_cast<cudaStream_t>(stream));
+  });
+}
+
+int cdft_eigen_solve(cdft_engine* engine, const cdft_eigen_config* cfg, const double* rho, double chemical_potential,
+                     double* vec, int use_guess, double* eigenvalue, int* iterations, int* converged, void* stream) {
+  return guarded([&] {
+    if (!cfg || !rho || !vec) throw std::invalid_argument("cfg, rho and vec are required");
+    cdft::Drivers::EigenResult r = drivers_of(engine).eigen_solve(to_eigen(*cfg), rho, chemical_potential, vec,
+                                                                  use_guess != 0, static_cast<cudaStream_t>(stream));
+    if (eigenvalue) *eigenvalue = r.eigenvalue;
+    if (iterations) *iterations = r.iterations;
+    if (converged) *converged = r.converged ? 1 : 0;
+  });
+}
+
+int cdft_saddle_find(cdft_engine* engine, const cdft_saddle_config* cfg, double* rho, double chemical_potential,
+                     double target_mass, double* eigvec, double out[2], int* outer_iterations, int* converged,
+                     void* stream) {
+  return guarded([&] {
+    if (!cfg || !rho || !eigvec) throw std::invalid_argument("cfg, rho and eigvec are required");
+    cdft::Drivers::SaddleConfig sc;
+    sc.fire = to_fire(cfg->fire);
+    sc.eigen = to_eigen(cfg->eigen);
+    sc.rho_min = cfg->rho_min;
+    sc.omega_tolerance = cfg->omega_tolerance;
+    sc.tolerance_start = cfg->tolerance_start;
+    sc.tolerance_factor = cfg->tolerance_factor;
+    sc.max_outer_iterations = cfg->max_outer_iterations;
+    sc.eigenvalue_clear_count = cfg->eigenvalue_clear_count;
+    cdft::Drivers::SaddleResult r = drivers_of(engine).saddle_find(sc, rho, chemical_potential, target_mass, eigvec,
+                                                                   static_cast<cudaStream_t>(stream));
+    if (out) {
+      out[0] = r.grand_potential;
+      out[1] = r.eigenvalue;
+    }
+    if (outer_iterations) *outer_iterations = r.outer_iterations;
+    if (converged) *converged = r.converged ? 1 : 0;
   });
 }
 

@@ -1,0 +1,956 @@
+// Device-resident drivers: FIRE2 minimisation, DDFT integrating-factor steps,
+// Hessian-vector products.  See drivers.cuh.
+#include "drivers.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+
+namespace cdft {
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kRedTerms = 4;
+
+__device__ __forceinline__ bool on_face(long long idx, int nx, int ny, int nz) {
+  const int iz = (int)(idx % nz);
+  const long long t = idx / nz;
+  const int iy = (int)(t % ny);
+  const int ix = (int)(t / ny);
+  return ix == 0 || ix == nx - 1 || iy == 0 || iy == ny - 1 || iz == 0 || iz == nz - 1;
+}
+
+// block sums of up to kRedTerms values -> partials[block][kRedTerms]
+__device__ __forceinline__ void block_sum_store(double (&a)[kRedTerms], double* __restrict__ partials) {
+  __shared__ double sh[32][kRedTerms];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int t = 0; t < kRedTerms; ++t) {
+    double v = a[t];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[warp][t] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kRedTerms) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sh[w][threadIdx.x];
+    partials[blockIdx.x * kRedTerms + threadIdx.x] = v;
+  }
+}
+
+// one warp: out[t] = sum_b partials[b][t]
+__global__ void k_finish_sums(const double* __restrict__ partials, int nblocks, double* __restrict__ out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (warp >= kRedTerms) return;
+  double v = 0.0;
+  for (int b = lane; b < nblocks; b += 32) v += partials[b * kRedTerms + warp];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if (lane == 0) out[warp] = v;
+}
+
+struct Vec {
+  double* x;
+  double* v;
+  double* f;
+  double* rho;
+  double* grad;
+  const double* dir;
+  long long N;
+  int nx, ny, nz;
+  double dv;
+  int param;
+  double rho_min, range;
+};
+
+__device__ __forceinline__ double to_density(const Vec& a, double x) {
+  if (a.param == kUnbounded) return a.rho_min + x * x;
+  const double x2 = x * x;
+  return a.rho_min + a.range * x2 / (1.0 + x2);
+}
+
+__device__ __forceinline__ double drho_dx(const Vec& a, double x) {
+  if (a.param == kUnbounded) return 2.0 * x;
+  const double x2 = x * x;
+  const double den = (1.0 + x2) * (1.0 + x2);
+  return 2.0 * a.range * x / den;
+}
+
+// minimization.hpp:63-78
+__global__ void k_from_density(Vec a, const double* __restrict__ rho) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
+    double d = rho[i] - a.rho_min;
+    double x;
+    if (a.param == kUnbounded) {
+      x = sqrt(d < 0.0 ? 0.0 : d);
+    } else {
+      const double hi = a.range * (1.0 - 1e-14);
+      d = d < 0.0 ? 0.0 : (d > hi ? hi : d);
+      x = sqrt(d / (a.range - d));
+    }
+    a.x[i] = x;
+    a.v[i] = 0.0;
+    a.rho[i] = to_density(a, x);
+  }
+}
+
+// sums: [sum rho, sum_interior rho]
+__global__ void k_density_sums(Vec a, double* __restrict__ partials) {
+  double s[kRedTerms] = {0, 0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
+    const double r = a.rho[i];
+    s[0] += r;
+    if (!on_face(i, a.nx, a.ny, a.nz)) s[1] += r;
+  }
+  block_sum_store(s, partials);
+}
+
+__global__ void k_power(Vec a, double* __restrict__ partials) {
+  double s[kRedTerms] = {0, 0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x)
+    s[0] += a.v[i] * a.f[i];
+  block_sum_store(s, partials);
+}
+
+// fire.hpp:95-121: the power test, dt/alpha adaptation and uphill count.
+__global__ void k_fire_control1(FireDevState* st, const double* __restrict__ sums, FireParams fp) {
+  if (threadIdx.x != 0 || !st->active) return;
+  const double power = sums[0];
+  st->dt_prev = st->dt;
+  st->backtrack = 0;
+  if (power > 0.0 || st->iteration == 0) {
+    st->n_positive++;
+    st->n_negative = 0;
+    if (st->n_positive > fp.n_delay) {
+      st->dt = fmin(st->dt * fp.f_inc, fp.dt_max);
+      st->alpha *= fp.f_alpha;
+    }
+  } else {
+    st->n_positive = 0;
+    st->n_negative++;
+    if (st->n_negative > fp.max_uphill) {
+      st->uphill_error = 1;
+      st->active = 0;
+      return;
+    }
+    st->backtrack = 1;
+    if (st->iteration > fp.n_delay) {
+      st->dt = fmax(st->dt * fp.f_dec, fp.dt_min);
+      st->alpha = fp.alpha_start;
+    }
+  }
+}
+
+// fire.hpp:110-126: backtrack (undo half a step with the old dt, kill v), then
+// v += dt f; sums |v|^2.
+__global__ void k_fire_vstep(Vec a, const FireDevState* __restrict__ st, double* __restrict__ partials) {
+  double s[kRedTerms] = {0, 0, 0, 0};
+  if (st->active) {
+    const double dt = st->dt, dtp = st->dt_prev;
+    const bool bt = st->backtrack;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N;
+         i += (long long)gridDim.x * blockDim.x) {
+      double v = a.v[i];
+      if (bt) {
+        a.x[i] -= 0.5 * dtp * v;
+        v = 0.0;
+      }
+      v += dt * a.f[i];
+      a.v[i] = v;
+      s[0] += v * v;
+    }
+  }
+  block_sum_store(s, partials);
+}
+
+struct FireAux {
+  double f2;  // |f|^2 of the forces driving this step
+};
+
+__global__ void k_fire_ratio(FireDevState* st, const double* __restrict__ sums, const FireAux* __restrict__ aux) {
+  if (threadIdx.x != 0 || !st->active) return;
+  const double v_norm = sqrt(sums[0]);
+  const double f_norm = sqrt(aux->f2);
+  st->ratio = (f_norm > 0.0) ? v_norm / f_norm : -1.0;
+}
+
+// fire.hpp:137-148 then the parametrisation: mixing, x += dt v, rho = rho(x).
+__global__ void k_fire_xstep(Vec a, const FireDevState* __restrict__ st) {
+  if (!st->active) return;
+  const double dt = st->dt, al = st->alpha, ratio = st->ratio;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
+    double v = a.v[i];
+    if (ratio >= 0.0) v = (1.0 - al) * v + al * ratio * a.f[i];
+    a.v[i] = v;
+    const double x = a.x[i] + dt * v;
+    a.x[i] = x;
+    a.rho[i] = to_density(a, x);
+  }
+}
+
+struct ComputeCfg {
+  int mode;
+  int homogeneous;
+  double target_mass;
+  double boundary_mass;
+  double n_face;
+};
+
+// Fixed-mass rescale factor (minimization.hpp:193-197, saddle_point.hpp:448-463).
+__global__ void k_scale_factor(FireDevState* st, const double* __restrict__ sums, ComputeCfg cc, double dv,
+                               int force_compute) {
+  if (threadIdx.x != 0) return;
+  if (!st->active && !force_compute) return;
+  double scale = 1.0;
+  if (cc.mode == kFixedMass) {
+    const double mass = sums[0] * dv;
+    if (mass > 0.0) scale = cc.target_mass / mass;
+  } else if (cc.mode == kSaddle) {
+    const double m_int = sums[1] * dv;
+    const double m_t = cc.target_mass - cc.boundary_mass;
+    if (m_int > 0.0 && m_t > 0.0) scale = m_t / m_int;
+  }
+  st->scale = scale;
+}
+
+__global__ void k_rescale(Vec a, const FireDevState* __restrict__ st, ComputeCfg cc, int force_compute) {
+  if ((!st->active && !force_compute) || cc.mode == kGrandPotential) return;
+  const double sc = st->scale;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
+    if (cc.mode == kFixedMass || !on_face(i, a.nx, a.ny, a.nz)) a.rho[i] *= sc;
+  }
+}
+
+// sums [sum_face grad, sum_interior grad*rho, sum_face rho, sum_face grad*rho]
+__global__ void k_post_sums(Vec a, double* __restrict__ partials) {
+  double s[kRedTerms] = {0, 0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
+    const double g = a.grad[i], r = a.rho[i];
+    if (on_face(i, a.nx, a.ny, a.nz)) {
+      s[0] += g;
+      s[2] += r;
+      s[3] += g * r;
+    } else {
+      s[1] += g * r;
+    }
+  }
+  block_sum_store(s, partials);
+}
+
+// The Lagrange multiplier (minimization.hpp:212-217, saddle_point.hpp:472-480).
+__global__ void k_post_control(FireDevState* st, const double* __restrict__ sums, ComputeCfg cc, double* bavg_out) {
+  if (threadIdx.x != 0) return;
+  const double bavg = (cc.n_face > 0.0) ? sums[0] / cc.n_face : 0.0;
+  *bavg_out = bavg;
+  double lam = 0.0;
+  if (cc.mode == kFixedMass) {
+    // <grad_b, rho> with grad_b the boundary-treated gradient
+    const double face = cc.homogeneous ? bavg * sums[2] : sums[3];
+    lam = (sums[1] + face) / cc.target_mass;
+  } else if (cc.mode == kSaddle) {
+    const double m_t = cc.target_mass - cc.boundary_mass;
+    lam = sums[1];
+    if (m_t > 0.0) lam /= m_t;
+  }
+  st->lambda = lam;
+}
+
+// Boundary treatment, Lagrange term and chain rule: f = -grad * drho/dx
+// (saddle: the projection follows).  sums [|f|^2, dir . f_alias].
+__global__ void k_post_apply(Vec a, const FireDevState* __restrict__ st, ComputeCfg cc,
+                             const double* __restrict__ bavg_p, double* __restrict__ partials) {
+  double s[kRedTerms] = {0, 0, 0, 0};
+  const double bavg = *bavg_p;
+  const double lam = st->lambda;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
+    double g = a.grad[i];
+    const bool face = on_face(i, a.nx, a.ny, a.nz);
+    if (cc.mode == kSaddle) {
+      g = face ? 0.0 : g - lam * a.dv;
+    } else {
+      if (cc.homogeneous && face) g = bavg;
+      if (cc.mode == kFixedMass) g -= lam * a.dv;
+    }
+    const double fa = g * drho_dx(a, a.x[i]);  // transform_force (minimization.hpp:82-99)
+    if (cc.mode == kSaddle) {
+      a.f[i] = fa;  // projected by k_project
+      s[1] += a.dir[i] * fa;
+    } else {
+      a.f[i] = -fa;
+      s[0] += fa * fa;
+    }
+  }
+  block_sum_store(s, partials);
+}
+
+// saddle_point.hpp:490-492: f_alias -= (dir . f_alias) dir; f = -f_alias.
+__global__ void k_project(Vec a, const double* __restrict__ sums_in, double* __restrict__ partials) {
+  double s[kRedTerms] = {0, 0, 0, 0};
+  const double proj = sums_in[1];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
+    const double fa = a.f[i] - proj * a.dir[i];
+    a.f[i] = -fa;
+    s[0] += fa * fa;
+  }
+  block_sum_store(s, partials);
+}
+
+// fire.hpp:150-162 and minimization.hpp:431-434: energy, rms force, the
+// convergence monitor and the iteration counter.
+__global__ void k_fire_finalize(FireDevState* st, const double* __restrict__ sums, const double* __restrict__ scal,
+                                FireAux* aux, FireParams fp, double n_dof, double volume, int use_monitor,
+                                int initial) {
+  if (threadIdx.x != 0) return;
+  if (!initial && !st->active) return;
+  const double f2 = sums[0];
+  aux->f2 = f2;
+  const double old_e = st->energy;
+  st->energy = scal[1];
+  st->free_energy = scal[0];
+  st->rms_force = sqrt(f2 / n_dof);
+  if (initial) {
+    st->converged = use_monitor ? 0 : (st->rms_force < fp.force_tolerance);
+    st->active = (!st->converged && fp.max_steps > 0) ? 1 : 0;
+    return;
+  }
+  st->iteration++;
+  if (use_monitor) {
+    st->vv = st->vv * 0.9 + 0.1 * (fabs(st->energy - old_e) / st->dt);
+    st->monitor = fabs(st->vv / volume);
+    st->converged = st->monitor < fp.force_tolerance;
+  } else {
+    st->converged = st->rms_force < fp.force_tolerance;
+  }
+  if (st->converged || st->iteration >= fp.max_steps) st->active = 0;
+}
+
+// ---------------------------------------------------------------- DDFT
+
+// dynamics.hpp:135-206: R = div(rho grad(force/dV)) - lap(rho).
+__global__ void k_ddft_rhs(const double* __restrict__ rho, const double* __restrict__ force, double* __restrict__ out,
+                           int nx, int ny, int nz, double dx, double inv_dv) {
+  const long long N = (long long)nx * ny * nz;
+  const double D = 0.5 / (dx * dx);
+  const double L = 1.0 / (dx * dx);
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += (long long)gridDim.x * blockDim.x) {
+    const int iz = (int)(p % nz);
+    const long long t = p / nz;
+    const int iy = (int)(t % ny);
+    const int ix = (int)(t / ny);
+    const long long nyz = (long long)ny * nz;
+    const long long ixp = ((ix + 1) % nx) * nyz, ixm = ((ix - 1 + nx) % nx) * nyz, ix0 = ix * nyz;
+    const long long iyp = ((iy + 1) % ny) * (long long)nz, iym = ((iy - 1 + ny) % ny) * (long long)nz,
+                    iy0 = iy * (long long)nz;
+    const int izp = (iz + 1) % nz, izm = (iz - 1 + nz) % nz;
+    const double d0 = rho[p];
+    const double x0 = force[p] * inv_dv;
+    const long long px = ixp + iy0 + iz, mx = ixm + iy0 + iz, py = ix0 + iyp + iz, my = ix0 + iym + iz,
+                    pz = ix0 + iy0 + izp, mz = ix0 + iy0 + izm;
+    const double g = D * ((rho[px] + d0) * (force[px] * inv_dv - x0) - (d0 + rho[mx]) * (x0 - force[mx] * inv_dv)) +
+                     D * ((rho[py] + d0) * (force[py] * inv_dv - x0) - (d0 + rho[my]) * (x0 - force[my] * inv_dv)) +
+                     D * ((rho[pz] + d0) * (force[pz] * inv_dv - x0) - (d0 + rho[mz]) * (x0 - force[mz] * inv_dv));
+    const double lap = L * (rho[px] + rho[mx] - 2.0 * d0) + L * (rho[py] + rho[my] - 2.0 * d0) +
+                       L * (rho[pz] + rho[mz] - 2.0 * d0);
+    out[p] = g - lap;
+  }
+}
+
+// dynamics.hpp:247-287: work = U0 rho0_k + U1 R0_k + U2 (R1_k - R0_k).
+__global__ void k_ddft_propagate(const double2* __restrict__ rho0k, const double2* __restrict__ r0k,
+                                 double2* __restrict__ r1k_work, const double* __restrict__ lam, int nx, int ny,
+                                 int nzh, double dt) {
+  const long long Nk = (long long)nx * ny * nzh;
+  for (long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x; pos < Nk;
+       pos += (long long)gridDim.x * blockDim.x) {
+    const int iz = (int)(pos % nzh);
+    const long long t = pos / nzh;
+    const int iy = (int)(t % ny);
+    const int ix = (int)(t / ny);
+    const double Lambda = lam[ix] + lam[nx + iy] + lam[nx + ny + iz];
+    const double ex = exp(lam[ix] * dt) * exp(lam[nx + iy] * dt) * exp(lam[nx + ny + iz] * dt);
+    const double U0 = ex;
+    const double U1 = (pos == 0) ? dt : (ex - 1.0) / Lambda;
+    const double U2 = (pos == 0) ? dt / 2.0 : (ex - 1.0 - dt * Lambda) / (Lambda * Lambda * dt);
+    const double2 a = rho0k[pos], b = r0k[pos], c = r1k_work[pos];
+    r1k_work[pos] = make_double2(U0 * a.x + U1 * b.x + U2 * (c.x - b.x), U0 * a.y + U1 * b.y + U2 * (c.y - b.y));
+  }
+}
+
+// d1_new = work / N; sums [max |d1 - d1_new|, min d1_new] via partial max/min.
+__global__ void k_ddft_update(const double* __restrict__ work, double* __restrict__ d1, long long N, double inv_n,
+                              double* __restrict__ partials) {
+  double mx = 0.0, mn = 1e300;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    const double nv = work[i] * inv_n;
+    const double dev = fabs(d1[i] - nv);
+    mx = dev > mx ? dev : mx;
+    mn = nv < mn ? nv : mn;
+    d1[i] = nv;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, o));
+  }
+  __shared__ double smx[32], smn[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    smx[warp] = mx;
+    smn[warp] = mn;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+      mx = fmax(mx, smx[w]);
+      mn = fmin(mn, smn[w]);
+    }
+    partials[blockIdx.x * 2 + 0] = fmax(mx, smx[0]);
+    partials[blockIdx.x * 2 + 1] = fmin(mn, smn[0]);
+  }
+}
+
+__global__ void k_maxmin_finish(const double* __restrict__ partials, int nb, double* __restrict__ out) {
+  if (threadIdx.x != 0) return;
+  double mx = 0.0, mn = 1e300;
+  for (int b = 0; b < nb; ++b) {
+    mx = fmax(mx, partials[2 * b]);
+    mn = fmin(mn, partials[2 * b + 1]);
+  }
+  out[0] = mx;
+  out[1] = mn;
+}
+
+// ------------------------------------------------------------------- HVP
+
+// hv = (f_eps - f0) / eps with the fixed boundary applied to both.
+__global__ void k_fd_hvp(const double* __restrict__ f_eps, const double* __restrict__ f0, double* __restrict__ hv,
+                         long long N, double inv_eps, int nx, int ny, int nz, int boundary) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    const bool zero = boundary && on_face(i, nx, ny, nz);
+    hv[i] = zero ? 0.0 : (f_eps[i] - f0[i]) * inv_eps;
+  }
+}
+
+__global__ void k_axpy_into(const double* __restrict__ x, double a, const double* __restrict__ y,
+                            double* __restrict__ out, long long N) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+    out[i] = y[i] + a * x[i];
+}
+
+__global__ void k_fixed_boundary(double* __restrict__ f, long long N, int nx, int ny, int nz) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+    if (on_face(i, nx, ny, nz)) f[i] = 0.0;
+}
+
+__global__ void k_dot(const double* __restrict__ a, const double* __restrict__ b, long long n,
+                      double* __restrict__ partials) {
+  double s[kRedTerms] = {0, 0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    s[0] += a[i] * b[i];
+  block_sum_store(s, partials);
+}
+
+__global__ void k_axpby(double a, const double* __restrict__ x, double b, double* __restrict__ y, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = a * x[i] + b * y[i];
+}
+
+// Seeded standard normal draws (splitmix64 counter hash + Box-Muller).
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+__global__ void k_randn(double* __restrict__ out, long long n, unsigned long long seed) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long a = mix64(seed * 0x100000001b3ull + 2 * i);
+    const unsigned long long b = mix64(seed * 0x100000001b3ull + 2 * i + 1);
+    const double u1 = ((a >> 11) + 1.0) * (1.0 / 9007199254740993.0);  // (0, 1]
+    const double u2 = (b >> 11) * (1.0 / 9007199254740992.0);
+    out[i] = sqrt(-2.0 * log(u1)) * cos(2.0 * 3.14159265358979323846 * u2);
+  }
+}
+
+// out = a*x + b*y + c*z (any of y, z may be null)
+__global__ void k_lincomb(double* __restrict__ out, double a, const double* __restrict__ x, double b,
+                          const double* __restrict__ y, double c, const double* __restrict__ z, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double v = a * x[i];
+    if (y) v += b * y[i];
+    if (z) v += c * z[i];
+    out[i] = v;
+  }
+}
+
+// dir = vec * drho/dx at x = x(rho) (saddle_point.hpp:424-426)
+__global__ void k_dir_alias(const double* __restrict__ vec, const double* __restrict__ rho, double* __restrict__ out,
+                            long long n, double rho_min) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double d = rho[i] - rho_min;
+    const double x = sqrt(d < 0.0 ? 0.0 : d);
+    out[i] = vec[i] * 2.0 * x;
+  }
+}
+
+__global__ void k_face_sum(const double* __restrict__ rho, long long n, int nx, int ny, int nz,
+                           double* __restrict__ partials) {
+  double s[kRedTerms] = {0, 0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    if (on_face(i, nx, ny, nz)) s[0] += rho[i];
+  block_sum_store(s, partials);
+}
+
+// Symmetric eigen-decomposition of a small matrix (cyclic Jacobi); returns
+// the eigenvector of the smallest eigenvalue (the reference takes column 0
+// of arma::eig_sym, saddle_point.hpp:251-254).
+void smallest_eigvec(int n, double A[3][3], double* vec, double* val) {
+  double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0;
+    for (int i = 0; i < n; ++i)
+      for (int j = i + 1; j < n; ++j) off += A[i][j] * A[i][j];
+    if (off < 1e-300) break;
+    for (int pq = 0; pq < n; ++pq)
+      for (int q = pq + 1; q < n; ++q) {
+        const int pp = pq;
+        if (std::abs(A[pp][q]) < 1e-300) continue;
+        const double theta = (A[q][q] - A[pp][pp]) / (2.0 * A[pp][q]);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::abs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < n; ++k) {
+          const double akp = A[k][pp], akq = A[k][q];
+          A[k][pp] = c * akp - s * akq;
+          A[k][q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double apk = A[pp][k], aqk = A[q][k];
+          A[pp][k] = c * apk - s * aqk;
+          A[q][k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double vkp = V[k][pp], vkq = V[k][q];
+          V[k][pp] = c * vkp - s * vkq;
+          V[k][q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  int m = 0;
+  for (int i = 1; i < n; ++i)
+    if (A[i][i] < A[m][m]) m = i;
+  for (int k = 0; k < n; ++k) vec[k] = V[k][m];
+  *val = A[m][m];
+}
+
+}  // namespace
+
+Drivers::Drivers(Engine& engine) : eng_(engine) {
+  if (engine.species() != 1) throw Error(-1, "drivers: the minimiser, DDFT and saddle drivers are single-species");
+  N_ = engine.points();
+  auto al = [&](double** p, size_t n) { CDFT_CUDA(cudaMalloc(p, sizeof(double) * n)); };
+  al(&x_, N_);
+  al(&v_, N_);
+  al(&f_, N_);
+  al(&grad_, N_);
+  al(&tmp_, N_);
+  al(&tmp2_, N_);
+  al(&scalars_, kScalarCount);
+  int sms = 0, dev = 0;
+  CDFT_CUDA(cudaGetDevice(&dev));
+  CDFT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  grid_ = (int)std::max<long long>(1, std::min<long long>((long long)sms * 8, (N_ + kBlock - 1) / kBlock));
+  al(&red_, (size_t)grid_ * kRedTerms + 64);
+  al(&red_out_, 64);
+  CDFT_CUDA(cudaMalloc(&st_, sizeof(FireDevState)));
+  CDFT_CUDA(cudaMallocHost(&st_host_, sizeof(FireDevState)));
+  CDFT_CUDA(cudaMallocHost(&host_pin_, sizeof(double) * 64));
+}
+
+Drivers::~Drivers() {
+  for (void* p : {(void*)x_, (void*)v_, (void*)f_, (void*)grad_, (void*)tmp_, (void*)tmp2_, (void*)scalars_,
+                  (void*)red_, (void*)red_out_, (void*)st_, ddft_k_, (void*)lam_, fft_work_, tan_})
+    if (p) cudaFree(p);
+  for (double* p : ev_)
+    if (p) cudaFree(p);
+  if (st_host_) cudaFreeHost(st_host_);
+  if (host_pin_) cudaFreeHost(host_pin_);
+  if (ddft_ready_) {
+    cufftDestroy(plan_r2c_);
+    cufftDestroy(plan_c2r_);
+  }
+}
+
+double Drivers::dot(const double* a, const double* b, long long n, cudaStream_t stream) {
+  k_dot<<<grid_, kBlock, 0, stream>>>(a, b, n, red_);
+  k_finish_sums<<<1, 32 * kRedTerms, 0, stream>>>(red_, grid_, red_out_);
+  CDFT_CUDA(cudaMemcpyAsync(host_pin_, red_out_, sizeof(double), cudaMemcpyDeviceToHost, stream));
+  CDFT_CUDA(cudaStreamSynchronize(stream));
+  return host_pin_[0];
+}
+
+void Drivers::axpby(double a, const double* x, double b, double* y, long long n, cudaStream_t stream) {
+  k_axpby<<<grid_, kBlock, 0, stream>>>(a, x, b, y, n);
+  CDFT_CUDA(cudaGetLastError());
+}
+
+double Drivers::force(const double* rho, double* f, double mu, int boundary, cudaStream_t stream) {
+  eng_.evaluate(rho, nullptr, &mu, f, scalars_, stream);
+  const EvalParams& p = eng_.params();
+  if (boundary) k_fixed_boundary<<<grid_, kBlock, 0, stream>>>(f, N_, p.nx, p.ny, p.nz);
+  CDFT_CUDA(cudaMemcpyAsync(host_pin_, scalars_, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+  CDFT_CUDA(cudaStreamSynchronize(stream));
+  return host_pin_[1];
+}
+
+void Drivers::hvp_fd(const double* rho, const double* force_at_rho, const double* v, double* hv, double eps,
+                     double mu, int boundary, cudaStream_t stream) {
+  const EvalParams& p = eng_.params();
+  k_axpy_into<<<grid_, kBlock, 0, stream>>>(v, eps, rho, tmp_, N_);  // rho + eps v
+  eng_.evaluate(tmp_, nullptr, &mu, tmp2_, scalars_, stream);
+  k_fd_hvp<<<grid_, kBlock, 0, stream>>>(tmp2_, force_at_rho, hv, N_, 1.0 / eps, p.nx, p.ny, p.nz, boundary);
+  CDFT_CUDA(cudaGetLastError());
+}
+
+void Drivers::hvp_exact(const double* rho, const double* v, double* hv, double mu, int boundary,
+                        cudaStream_t stream) {
+  eng_.hvp(rho, v, &mu, hv, stream);
+  const EvalParams& p = eng_.params();
+  if (boundary) k_fixed_boundary<<<grid_, kBlock, 0, stream>>>(hv, N_, p.nx, p.ny, p.nz);
+  CDFT_CUDA(cudaGetLastError());
+}
+
+FireResult Drivers::fire_minimize(const FireConfig& cfg, double* rho, const double* direction, cudaStream_t stream,
+                                  Engine* refine, double refine_switch) {
+  const EvalParams& p = eng_.params();
+  if (cfg.mode == kSaddle && !direction) throw Error(-1, "fire_minimize: saddle mode needs a direction");
+  if (cfg.mode == kFixedMass && !(cfg.target_mass > 0.0)) throw Error(-1, "fire_minimize: target mass must be > 0");
+  Vec a;
+  a.x = x_;
+  a.v = v_;
+  a.f = f_;
+  a.rho = rho;
+  a.grad = grad_;
+  a.dir = direction;
+  a.N = N_;
+  a.nx = p.nx;
+  a.ny = p.ny;
+  a.nz = p.nz;
+  a.dv = p.dv;
+  a.param = cfg.param;
+  a.rho_min = cfg.rho_min;
+  a.range = cfg.rho_max - cfg.rho_min;
+  ComputeCfg cc;
+  cc.mode = cfg.mode;
+  cc.homogeneous = cfg.homogeneous_boundary ? 1 : 0;
+  cc.target_mass = cfg.target_mass;
+  cc.boundary_mass = cfg.boundary_mass;
+  const long long inner = (long long)std::max(p.nx - 2, 0) * std::max(p.ny - 2, 0) * std::max(p.nz - 2, 0);
+  cc.n_face = (double)(N_ - inner);
+  const double volume = (double)N_ * p.dv;
+  // Minimizer::fixed_mass computes with mu = 0 (minimization.hpp:388); the
+  // other modes with the given chemical potential.
+  const double mu_compute = (cfg.mode == kFixedMass) ? 0.0 : cfg.mu;
+  double* bavg = red_out_ + 16;
+  FireAux* aux = reinterpret_cast<FireAux*>(red_out_ + 20);
+  const FireParams& fp = cfg.fire;
+  const int use_monitor = cfg.use_monitor ? 1 : 0;
+
+  Engine* eng = &eng_;
+  auto compute = [&](int initial) {
+    // rescale (fixed mass / saddle), evaluate, post-process into f
+    k_density_sums<<<grid_, kBlock, 0, stream>>>(a, red_);
+    k_finish_sums<<<1, 32 * kRedTerms, 0, stream>>>(red_, grid_, red_out_);
+    k_scale_factor<<<1, 32, 0, stream>>>(st_, red_out_, cc, p.dv, initial);
+    k_rescale<<<grid_, kBlock, 0, stream>>>(a, st_, cc, initial);
+    eng->evaluate(rho, nullptr, &mu_compute, grad_, scalars_, stream);
+    k_post_sums<<<grid_, kBlock, 0, stream>>>(a, red_);
+    k_finish_sums<<<1, 32 * kRedTerms, 0, stream>>>(red_, grid_, red_out_);
+    k_post_control<<<1, 32, 0, stream>>>(st_, red_out_, cc, bavg);
+    k_post_apply<<<grid_, kBlock, 0, stream>>>(a, st_, cc, bavg, red_);
+    k_finish_sums<<<1, 32 * kRedTerms, 0, stream>>>(red_, grid_, red_out_ + 4);
+    if (cfg.mode == kSaddle) {
+      k_project<<<grid_, kBlock, 0, stream>>>(a, red_out_ + 4, red_);
+      k_finish_sums<<<1, 32 * kRedTerms, 0, stream>>>(red_, grid_, red_out_ + 4);
+    }
+    k_fire_finalize<<<1, 32, 0, stream>>>(st_, red_out_ + 4, scalars_, aux, fp, (double)N_, volume, use_monitor,
+                                          initial);
+  };
+
+  // initialise (fire.hpp:60-84)
+  FireDevState s0;
+  std::memset(&s0, 0, sizeof(s0));
+  s0.dt = fp.dt;
+  s0.alpha = fp.alpha_start;
+  s0.vv = 1.0;
+  s0.scale = 1.0;
+  s0.active = 1;
+  CDFT_CUDA(cudaMemcpyAsync(st_, &s0, sizeof(s0), cudaMemcpyHostToDevice, stream));
+  k_from_density<<<grid_, kBlock, 0, stream>>>(a, rho);
+  compute(1);
+  CDFT_CUDA(cudaGetLastError());
+
+  bool refining = false;
+  int steps = 0;
+  for (;;) {
+    CDFT_CUDA(cudaMemcpyAsync(st_host_, st_, sizeof(FireDevState), cudaMemcpyDeviceToHost, stream));
+    CDFT_CUDA(cudaStreamSynchronize(stream));
+    if (!st_host_->active || steps >= fp.max_steps) break;
+    if (refine && !refining && cfg.use_monitor && st_host_->iteration > 0 &&
+        st_host_->monitor < refine_switch * fp.force_tolerance) {
+      eng = refine;  // FP64 defect correction from here on
+      refining = true;
+    }
+    const int chunk = std::max(1, std::min(cfg.check_interval, fp.max_steps - steps));
+    for (int k = 0; k < chunk; ++k) {
+      k_power<<<grid_, kBlock, 0, stream>>>(a, red_);
+      k_finish_sums<<<1, 32 * kRedTerms, 0, stream>>>(red_, grid_, red_out_);
+      k_fire_control1<<<1, 32, 0, stream>>>(st_, red_out_, fp);
+      k_fire_vstep<<<grid_, kBlock, 0, stream>>>(a, st_, red_);
+      k_finish_sums<<<1, 32 * kRedTerms, 0, stream>>>(red_, grid_, red_out_);
+      k_fire_ratio<<<1, 32, 0, stream>>>(st_, red_out_, aux);
+      k_fire_xstep<<<grid_, kBlock, 0, stream>>>(a, st_);
+      compute(0);
+    }
+    CDFT_CUDA(cudaGetLastError());
+    steps += chunk;
+  }
+  FireResult r;
+  r.iterations = st_host_->iteration;
+  r.converged = st_host_->converged != 0;
+  r.rms_force = st_host_->rms_force;
+  r.uphill_error = st_host_->uphill_error != 0;
+  if (r.uphill_error) return r;
+  // Final density (minimization.hpp:441-450, saddle_point.hpp:533-549): rho
+  // already holds rho(x) with the mass rescale of the last compute, which is
+  // exactly the reference's extraction from the final x.  The final total()
+  // uses the caller's chemical potential (fixed mass iterates with mu = 0).
+  eng->evaluate(rho, nullptr, &cfg.mu, grad_, scalars_, stream);
+  CDFT_CUDA(cudaMemcpyAsync(host_pin_, scalars_, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+  CDFT_CUDA(cudaStreamSynchronize(stream));
+  r.free_energy = host_pin_[0];
+  r.grand_potential = host_pin_[1];
+  return r;
+}
+
+void Drivers::ensure_ddft() {
+  if (ddft_ready_) return;
+  const EvalParams& p = eng_.params();
+  CDFT_CUDA(cudaMalloc(&ddft_k_, sizeof(double2) * 3 * p.Nk));
+  CDFT_CUDA(cudaMalloc(&lam_, sizeof(double) * (p.nx + p.ny + p.nzh)));
+  std::vector<double> lam(p.nx + p.ny + p.nzh);
+  const double Dx = 1.0 / (p.dx * p.dx);
+  for (int i = 0; i < p.nx; ++i) lam[i] = 2.0 * Dx * (std::cos(2.0 * kPi * i / p.nx) - 1.0);
+  for (int i = 0; i < p.ny; ++i) lam[p.nx + i] = 2.0 * Dx * (std::cos(2.0 * kPi * i / p.ny) - 1.0);
+  for (int i = 0; i < p.nzh; ++i) lam[p.nx + p.ny + i] = 2.0 * Dx * (std::cos(2.0 * kPi * i / p.nz) - 1.0);
+  CDFT_CUDA(cudaMemcpy(lam_, lam.data(), sizeof(double) * lam.size(), cudaMemcpyHostToDevice));
+  CDFT_CUFFT(cufftPlan3d(&plan_r2c_, p.nx, p.ny, p.nz, CUFFT_D2Z));
+  CDFT_CUFFT(cufftPlan3d(&plan_c2r_, p.nx, p.ny, p.nz, CUFFT_Z2D));
+  ddft_ready_ = true;
+}
+
+double Drivers::ddft_step(DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations) {
+  ensure_ddft();
+  const EvalParams& p = eng_.params();
+  CDFT_CUFFT(cufftSetStream(plan_r2c_, stream));
+  CDFT_CUFFT(cufftSetStream(plan_c2r_, stream));
+  double2* rho0k = static_cast<double2*>(ddft_k_);
+  double2* r0k = rho0k + p.Nk;
+  double2* work = r0k + p.Nk;
+  double* d1 = x_;       // the iterate
+  double* f1 = grad_;    // forces
+  double* rhs = tmp_;    // R(rho) in real space
+  const double mu = cfg.mu;
+  // compute(rho0), R0_k, rho0_k (dynamics.hpp:347-354)
+  eng_.evaluate(rho, nullptr, &mu, f1, scalars_, stream);
+  k_ddft_rhs<<<grid_, kBlock, 0, stream>>>(rho, f1, rhs, p.nx, p.ny, p.nz, p.dx, 1.0 / p.dv);
+  CDFT_CUFFT(cufftExecD2Z(plan_r2c_, rhs, r0k));
+  CDFT_CUFFT(cufftExecD2Z(plan_r2c_, rho, rho0k));
+  int total_it = 0;
+  for (int restarts = 0; restarts < 64; ++restarts) {
+    bool restart = false;
+    const double dt = cfg.dt;
+    CDFT_CUDA(cudaMemcpyAsync(d1, rho, sizeof(double) * N_, cudaMemcpyDeviceToDevice, stream));
+    double deviation = 1e30;
+    for (int it = 0; it < cfg.fp_max_iterations; ++it) {
+      ++total_it;
+      eng_.evaluate(d1, nullptr, &mu, f1, scalars_, stream);
+      k_ddft_rhs<<<grid_, kBlock, 0, stream>>>(d1, f1, rhs, p.nx, p.ny, p.nz, p.dx, 1.0 / p.dv);
+      CDFT_CUFFT(cufftExecD2Z(plan_r2c_, rhs, work));
+      k_ddft_propagate<<<grid_, kBlock, 0, stream>>>(rho0k, r0k, work, lam_, p.nx, p.ny, p.nzh, dt);
+      CDFT_CUFFT(cufftExecZ2D(plan_c2r_, work, tmp2_));
+      k_ddft_update<<<grid_, kBlock, 0, stream>>>(tmp2_, d1, N_, 1.0 / (double)N_, red_);
+      k_maxmin_finish<<<1, 32, 0, stream>>>(red_, grid_, red_out_);
+      CDFT_CUDA(cudaMemcpyAsync(host_pin_, red_out_, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+      CDFT_CUDA(cudaStreamSynchronize(stream));
+      const double old = deviation;
+      deviation = host_pin_[0];
+      if (host_pin_[1] < 0.0 || (it > 0 && deviation > old)) {
+        restart = true;
+        break;
+      }
+      if (deviation < cfg.fp_tolerance) break;
+    }
+    if (!restart && deviation > cfg.fp_tolerance) restart = true;
+    if (!restart) break;
+    cfg.dt /= 10.0;
+  }
+  if (fp_iterations) *fp_iterations = total_it;
+  // final compute (dynamics.hpp:394)
+  eng_.evaluate(d1, nullptr, &mu, f1, scalars_, stream);
+  CDFT_CUDA(cudaMemcpyAsync(rho, d1, sizeof(double) * N_, cudaMemcpyDeviceToDevice, stream));
+  CDFT_CUDA(cudaMemcpyAsync(host_pin_, scalars_, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+  CDFT_CUDA(cudaStreamSynchronize(stream));
+  return host_pin_[1];
+}
+
+}  // namespace cdft
+
+namespace cdft {
+
+Drivers::EigenResult Drivers::eigen_solve(const EigenConfig& cfg, const double* rho, double mu, double* vec,
+                                          bool use_guess, cudaStream_t stream) {
+  for (double*& p : ev_)
+    if (!p) CDFT_CUDA(cudaMalloc(&p, sizeof(double) * N_));
+  double* f0 = ev_[0];
+  double* hv = ev_[1];
+  double* q1 = ev_[2];
+  double* hq1 = ev_[3];
+  double* q2 = ev_[4];
+  double* hq2 = ev_[5];
+  double* praw = ev_[6];
+  double* vnew = ev_[7];
+  double* v = vec;
+  force(rho, f0, mu, 1, stream);
+  auto H = [&](const double* in, double* out) {
+    if (cfg.exact_hvp)
+      hvp_exact(rho, in, out, mu, 1, stream);
+    else
+      hvp_fd(rho, f0, in, out, cfg.hessian_eps, mu, 1, stream);
+  };
+  if (!use_guess) k_randn<<<grid_, kBlock, 0, stream>>>(v, N_, cfg.seed);
+  {
+    const double nv = std::sqrt(dot(v, v, N_, stream));
+    axpby(0.0, v, 1.0 / nv, v, N_, stream);
+  }
+  H(v, hv);
+  double lambda = dot(v, hv, N_, stream);
+  bool have_p = false;
+  EigenResult res;
+  int iter = 0;
+  for (; iter < cfg.max_iterations; ++iter) {
+    // residual = hv - lambda v (into q1)
+    k_lincomb<<<grid_, kBlock, 0, stream>>>(q1, 1.0, hv, -lambda, v, 0.0, nullptr, N_);
+    const double rn = std::sqrt(dot(q1, q1, N_, stream));
+    if (rn < cfg.tolerance) {
+      res.converged = true;
+      break;
+    }
+    const double rq = dot(q1, v, N_, stream);
+    axpby(-rq, v, 1.0, q1, N_, stream);
+    const double q1n = std::sqrt(dot(q1, q1, N_, stream));
+    if (q1n < 1e-30) break;
+    axpby(0.0, q1, 1.0 / q1n, q1, N_, stream);
+    H(q1, hq1);
+    int dim = 2;
+    if (have_p) {
+      const double a0 = dot(praw, v, N_, stream);
+      const double a1 = dot(praw, q1, N_, stream);
+      k_lincomb<<<grid_, kBlock, 0, stream>>>(q2, 1.0, praw, -a0, v, -a1, q1, N_);
+      const double q2n = std::sqrt(dot(q2, q2, N_, stream));
+      if (q2n > 1e-10) {
+        axpby(0.0, q2, 1.0 / q2n, q2, N_, stream);
+        H(q2, hq2);
+        dim = 3;
+      }
+    }
+    double Hm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    Hm[0][0] = dot(v, hv, N_, stream);
+    Hm[0][1] = Hm[1][0] = dot(v, hq1, N_, stream);
+    Hm[1][1] = dot(q1, hq1, N_, stream);
+    if (dim == 3) {
+      Hm[0][2] = Hm[2][0] = dot(v, hq2, N_, stream);
+      Hm[1][2] = Hm[2][1] = dot(q1, hq2, N_, stream);
+      Hm[2][2] = dot(q2, hq2, N_, stream);
+    }
+    double c[3] = {0, 0, 0}, ev = 0.0;
+    smallest_eigvec(dim, Hm, c, &ev);
+    k_lincomb<<<grid_, kBlock, 0, stream>>>(vnew, c[0], v, c[1], q1, dim == 3 ? c[2] : 0.0,
+                                            dim == 3 ? q2 : nullptr, N_);
+    k_lincomb<<<grid_, kBlock, 0, stream>>>(praw, 1.0, vnew, -1.0, v, 0.0, nullptr, N_);
+    have_p = true;
+    const double nn = std::sqrt(dot(vnew, vnew, N_, stream));
+    k_lincomb<<<grid_, kBlock, 0, stream>>>(v, 1.0 / nn, vnew, 0.0, nullptr, 0.0, nullptr, N_);
+    H(v, hv);
+    lambda = dot(v, hv, N_, stream);
+  }
+  res.eigenvalue = lambda;
+  res.iterations = iter;
+  return res;
+}
+
+Drivers::SaddleResult Drivers::saddle_find(const SaddleConfig& cfg, double* rho, double mu, double target_mass,
+                                           double* eigvec, cudaStream_t stream) {
+  const EvalParams& p = eng_.params();
+  double* dir = nullptr;
+  CDFT_CUDA(cudaMalloc(&dir, sizeof(double) * N_));
+  SaddleResult res;
+  double omega = 0.0;
+  double ftol = cfg.tolerance_start;
+  bool have_vec = false;
+  int outer = 0;
+  try {
+    for (; outer < cfg.max_outer_iterations; ++outer) {
+      const double omega_old = omega;
+      const bool guess = have_vec && outer >= cfg.eigenvalue_clear_count;
+      EigenConfig ec = cfg.eigen;
+      ec.seed = cfg.eigen.seed + (unsigned long long)outer;
+      EigenResult er = eigen_solve(ec, rho, mu, eigvec, guess, stream);
+      have_vec = true;
+      res.eigenvalue = er.eigenvalue;
+      // direction in parameter space, normalised (saddle_point.hpp:424-430)
+      k_dir_alias<<<grid_, kBlock, 0, stream>>>(eigvec, rho, dir, N_, cfg.rho_min);
+      const double dn = std::sqrt(dot(dir, dir, N_, stream));
+      if (dn > 1e-30) axpby(0.0, dir, 1.0 / dn, dir, N_, stream);
+      // boundary mass (saddle_point.hpp:432-443)
+      k_face_sum<<<grid_, kBlock, 0, stream>>>(rho, N_, p.nx, p.ny, p.nz, red_);
+      k_finish_sums<<<1, 32 * kRedTerms, 0, stream>>>(red_, grid_, red_out_);
+      CDFT_CUDA(cudaMemcpyAsync(host_pin_, red_out_, sizeof(double), cudaMemcpyDeviceToHost, stream));
+      CDFT_CUDA(cudaStreamSynchronize(stream));
+      const long long inner = (long long)std::max(p.nx - 2, 0) * std::max(p.ny - 2, 0) * std::max(p.nz - 2, 0);
+      const double n_face = (double)(N_ - inner);
+      const double avg = n_face > 0 ? host_pin_[0] / n_face : 0.0;
+      FireConfig fc;
+      fc.fire = cfg.fire;
+      fc.fire.force_tolerance = std::max(ftol, cfg.fire.force_tolerance);
+      ftol /= cfg.tolerance_factor;
+      fc.mode = kSaddle;
+      fc.param = kUnbounded;
+      fc.rho_min = cfg.rho_min;
+      fc.homogeneous_boundary = false;
+      fc.mu = mu;
+      fc.target_mass = target_mass;
+      fc.boundary_mass = avg * p.dv * n_face;
+      fc.use_monitor = false;
+      FireResult fr = fire_minimize(fc, rho, dir, stream);
+      if (fr.uphill_error) throw Error(-2, "fire::step: exceeded max uphill steps");
+      omega = fr.grand_potential;
+      if (outer > 0 && std::abs(omega - omega_old) < cfg.omega_tolerance) {
+        res.converged = true;
+        break;
+      }
+    }
+  } catch (...) {
+    cudaFree(dir);
+    throw;
+  }
+  cudaFree(dir);
+  res.grand_potential = omega;
+  res.outer_iterations = std::min(outer + 1, cfg.max_outer_iterations);
+  return res;
+}
+
+}  // namespace cdft

@@ -1,0 +1,177 @@
+// Device-resident drivers of the functional: FIRE2 minimisation (grand
+// potential, fixed mass, projected saddle mode), DDFT integrating-factor
+// steps, Hessian-vector products and the smallest-eigenpair solver.
+//
+// Every vector lives in HBM; per-step control decisions (the FIRE2 power test,
+// dt / alpha updates, convergence monitor) are taken by single-thread device
+// kernels from reduced scalars, so a FIRE step is a fixed kernel sequence that
+// never waits on the host.  The host reads the small control block only every
+// `check_interval` steps.
+#pragma once
+
+#include <cufft.h>
+
+#include <vector>
+
+#include "cdft_common.cuh"
+#include "engine.cuh"
+
+namespace cdft {
+
+// fire.hpp:33-44 (parameters)
+struct FireParams {
+  double dt = 1e-3, dt_max = 1e-2, dt_min = 1e-8;
+  double alpha_start = 0.1, f_inc = 1.1, f_dec = 0.5, f_alpha = 0.99;
+  int n_delay = 5, max_uphill = 20;
+  double force_tolerance = 0.1;
+  int max_steps = 10000;
+};
+
+enum FireMode : int { kGrandPotential = 0, kFixedMass = 1, kSaddle = 2 };
+enum ParamKind : int { kUnbounded = 0, kBounded = 1 };
+
+// Device-side FIRE2 state (fire.hpp:15-26 plus the minimiser's monitor).
+struct FireDevState {
+  double dt, alpha;
+  int n_positive, n_negative, iteration, converged;
+  int active;      // 1 while steps still change the state
+  int backtrack;   // this step backtracks (power <= 0)
+  int uphill_error;
+  double dt_prev;  // dt before this step's update (the backtrack uses it)
+  double energy, rms_force, vv, monitor;
+  double ratio;    // |v| / |f| of the mixing step
+  double scale;    // density rescale of the fixed-mass / saddle compute
+  double lambda;   // Lagrange multiplier of the fixed-mass / saddle compute
+  double free_energy;
+};
+
+struct FireConfig {
+  FireParams fire;
+  int mode = kGrandPotential;
+  int param = kUnbounded;
+  double rho_min = 1e-18, rho_max = 1.0;
+  bool homogeneous_boundary = true;
+  double mu = 0.0;
+  double target_mass = 0.0;     // fixed mass
+  double boundary_mass = 0.0;   // saddle: mass held by the boundary shell
+  int check_interval = 25;
+  bool use_monitor = true;      // Minimizer convergence (minimization.hpp:431-434) vs rms (fire.hpp:162)
+};
+
+struct FireResult {
+  double free_energy = 0.0, grand_potential = 0.0, rms_force = 0.0;
+  int iterations = 0;
+  bool converged = false;
+  bool uphill_error = false;
+};
+
+class Drivers {
+ public:
+  explicit Drivers(Engine& engine);
+  ~Drivers();
+  Drivers(const Drivers&) = delete;
+  Drivers& operator=(const Drivers&) = delete;
+
+  // Minimizer::grand_potential / fixed_mass (minimization.hpp:182-354) and the
+  // saddle FIRE of Search::find (saddle_point.hpp:445-530).  rho: N doubles on
+  // the device, replaced by the result.  `direction` (saddle mode, N doubles,
+  // device) is the unit eigen-direction in parameter space, or null.
+  // `refine` (optional) is an FP64 engine that takes over for the last
+  // `refine_steps` steps after the monitor first drops below
+  // `refine_switch` times the tolerance (mixed-precision defect correction).
+  FireResult fire_minimize(const FireConfig& cfg, double* rho, const double* direction, cudaStream_t stream,
+                           Engine* refine = nullptr, double refine_switch = 10.0);
+
+  // DDFT integrating-factor step (dynamics.hpp:333-401) for one species;
+  // returns the energy after the step and updates dt in place (dt/10 on
+  // restart).  rho: N doubles, device.
+  struct DDFTConfig {
+    double dt = 1e-4, diffusion = 1.0, min_density = 1e-18, dt_max = 1.0, fp_tolerance = 1e-4;
+    int fp_max_iterations = 100;
+    double mu = 0.0;
+  };
+  double ddft_step(DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations = nullptr);
+
+  // H v at rho (single species): exact forward-over-reverse (hvp_exact) or the
+  // reference's finite difference (F(rho + eps v) - F(rho)) / eps.
+  // `boundary` 1: fixed boundary (forces zeroed on the faces, saddle_point.hpp:382).
+  void hvp_fd(const double* rho, const double* force_at_rho, const double* v, double* hv, double eps, double mu,
+              int boundary, cudaStream_t stream);
+  void hvp_exact(const double* rho, const double* v, double* hv, double mu, int boundary, cudaStream_t stream);
+
+  // Plain force of one species with the boundary treatment (0 none, 1 fixed).
+  double force(const double* rho, double* f, double mu, int boundary, cudaStream_t stream);
+
+  // Device vector helpers (dot products etc.) used by the eigen solvers.
+  double dot(const double* a, const double* b, long long n, cudaStream_t stream);
+  void axpby(double a, const double* x, double b, double* y, long long n, cudaStream_t stream);  // y = a x + b y
+
+  // EigenvalueSolver::solve (saddle_point.hpp:171-276): smallest eigenpair of
+  // the Hessian of Omega at rho (fixed boundary on the forces), by the
+  // reference's 3-vector Rayleigh-Ritz iteration.  `vec` (device, N) holds
+  // the initial guess if `use_guess`, else a seeded normal vector is drawn;
+  // it receives the unit eigenvector.
+  struct EigenConfig {
+    double tolerance = 1e-4;
+    int max_iterations = 300;
+    double hessian_eps = 1e-6;
+    int exact_hvp = 0;
+    unsigned long long seed = 42;
+  };
+  struct EigenResult {
+    double eigenvalue = 0.0;
+    int iterations = 0;
+    bool converged = false;
+  };
+  EigenResult eigen_solve(const EigenConfig& cfg, const double* rho, double mu, double* vec, bool use_guess,
+                          cudaStream_t stream);
+
+  // Search::find (saddle_point.hpp:324-589): eigenvector following at fixed
+  // mass.  rho (device, N) is replaced by the saddle density, eigvec (device,
+  // N) receives the unstable direction.
+  struct SaddleConfig {
+    FireParams fire;
+    EigenConfig eigen;
+    double rho_min = 1e-18;
+    double omega_tolerance = 1e-5, tolerance_start = 1e-3, tolerance_factor = 10.0;
+    int max_outer_iterations = 20, eigenvalue_clear_count = 2;
+  };
+  struct SaddleResult {
+    double grand_potential = 0.0, eigenvalue = 0.0;
+    int outer_iterations = 0;
+    bool converged = false;
+  };
+  SaddleResult saddle_find(const SaddleConfig& cfg, double* rho, double mu, double target_mass, double* eigvec,
+                           cudaStream_t stream);
+
+  Engine& engine() { return eng_; }
+
+ private:
+  Engine& eng_;
+  long long N_ = 0;
+  double* x_ = nullptr;       // FIRE parameters
+  double* v_ = nullptr;       // FIRE velocity
+  double* f_ = nullptr;       // FIRE force (parameter space)
+  double* grad_ = nullptr;    // functional force from the engine
+  double* tmp_ = nullptr;     // scratch vector (HVP, DDFT)
+  double* tmp2_ = nullptr;
+  double* scalars_ = nullptr; // engine scalar block
+  double* red_ = nullptr;     // reduction partials
+  double* red_out_ = nullptr; // reduced values
+  FireDevState* st_ = nullptr;
+  FireDevState* st_host_ = nullptr;  // pinned
+  double* host_pin_ = nullptr;       // pinned scalars
+  int grid_ = 0;
+  // DDFT
+  void* ddft_k_ = nullptr;    // 3 * Nk complex (rho0_k, R0_k, R1_k / work)
+  double* lam_ = nullptr;     // nx + ny + nzh Laplacian eigenvalues
+  cufftHandle plan_r2c_ = 0, plan_c2r_ = 0;
+  void* fft_work_ = nullptr;
+  bool ddft_ready_ = false;
+  void ensure_ddft();
+  // eigen solver vectors
+  double* ev_[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  void* tan_ = nullptr;
+};
+
+}  // namespace cdft

@@ -186,7 +186,8 @@ Engine::~Engine() {
     cufftDestroy(plan_force_);
   }
   for (void* q : {rho_k_, chan_k_, chan_r_, deriv_r_, deriv_k_, force_k_, hs_r_, rho_lo_, (void*)mf_w_,
-                  (void*)mean_, (void*)dbar_, (void*)err_,
+                  (void*)mean_, (void*)dbar_, (void*)err_, tan_chan_, (void*)tan_mean_, (void*)tan_dbar_,
+                  (void*)tan_in_,
                   (void*)partials_, fft_work_, (void*)h_rho_, (void*)h_vext_, (void*)h_force_, (void*)h_scalars_})
     if (q) cudaFree(q);
   if (stream_) cudaStreamDestroy(stream_);
@@ -250,48 +251,84 @@ void Engine::upload_mean_field(const EngineSpec& spec) {
   cudaFree(wk);
 }
 
+// Stages 1-3: the weighted-density channels of the field `in` (S*N
+// doubles) in real space.  Mixed precision transforms in - mean in FP32 and
+// stores the species means in `mean_out`.
+template <typename R, typename C2>
+void Engine::forward_stage(const double* in, R* chan_out, double* mean_out, cudaStream_t stream) {
+  const EvalParams& p = p_;
+  constexpr bool mixed = sizeof(R) == sizeof(float);
+  C2* rho_k = static_cast<C2*>(rho_k_);
+  C2* chan_k = static_cast<C2*>(chan_k_);
+  if constexpr (mixed) {
+    k_species_sums<<<grid_stream_, 256, 0, stream>>>(in, p.N, p.S, partials_);
+    k_split_convert<<<grid_stream_, 256, 0, stream>>>(in, p.N, p.S, partials_, grid_stream_,
+                                                      static_cast<float*>(rho_lo_), mean_out);
+    CDFT_CUFFT(cufftExecR2C(plan_rho_, static_cast<float*>(rho_lo_), reinterpret_cast<cufftComplex*>(rho_k)));
+  } else {
+    CDFT_CUFFT(cufftExecD2Z(plan_rho_, const_cast<double*>(in), reinterpret_cast<cufftDoubleComplex*>(rho_k)));
+  }
+  const bool multi = p.L.multi, tensor = p.L.tensor;
+  if (!multi && !tensor) k_forward<false, false, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
+  if (!multi && tensor) k_forward<false, true, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
+  if (multi && !tensor) k_forward<true, false, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
+  if (multi && tensor) k_forward<true, true, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
+  CDFT_CUDA(cudaGetLastError());
+  if constexpr (mixed)
+    CDFT_CUFFT(cufftExecC2R(plan_chan_, reinterpret_cast<cufftComplex*>(chan_k), reinterpret_cast<float*>(chan_out)));
+  else
+    CDFT_CUFFT(cufftExecZ2D(plan_chan_, reinterpret_cast<cufftDoubleComplex*>(chan_k),
+                            reinterpret_cast<double*>(chan_out)));
+}
+
+// Stages 5-7: out += c2r(sum_c conj(W_c) r2c(deriv_c)) dV (+ the FP64
+// constants of the split derivative channels, `dbar`).
+template <typename R, typename C2>
+void Engine::backward_stage(R* deriv, const double* dbar, double* out, cudaStream_t stream) {
+  const EvalParams& p = p_;
+  constexpr bool mixed = sizeof(R) == sizeof(float);
+  C2* deriv_k = static_cast<C2*>(deriv_k_);
+  C2* force_k = static_cast<C2*>(force_k_);
+  R* hs_r = static_cast<R*>(hs_r_);
+  if constexpr (mixed)
+    CDFT_CUFFT(cufftExecR2C(plan_deriv_, reinterpret_cast<float*>(deriv), reinterpret_cast<cufftComplex*>(deriv_k)));
+  else
+    CDFT_CUFFT(cufftExecD2Z(plan_deriv_, reinterpret_cast<double*>(deriv),
+                            reinterpret_cast<cufftDoubleComplex*>(deriv_k)));
+  const bool multi = p.L.multi, tensor = p.L.tensor;
+  if (!multi && !tensor) k_backward<false, false, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
+  if (!multi && tensor) k_backward<false, true, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
+  if (multi && !tensor) k_backward<true, false, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
+  if (multi && tensor) k_backward<true, true, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
+  CDFT_CUDA(cudaGetLastError());
+  if constexpr (mixed)
+    CDFT_CUFFT(cufftExecC2R(plan_force_, reinterpret_cast<cufftComplex*>(force_k), reinterpret_cast<float*>(hs_r)));
+  else
+    CDFT_CUFFT(cufftExecZ2D(plan_force_, reinterpret_cast<cufftDoubleComplex*>(force_k),
+                            reinterpret_cast<double*>(hs_r)));
+  if (!multi && !tensor) k_epilogue<false, false, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar, out);
+  if (!multi && tensor) k_epilogue<false, true, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar, out);
+  if (multi && !tensor) k_epilogue<true, false, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar, out);
+  if (multi && tensor) k_epilogue<true, true, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar, out);
+  CDFT_CUDA(cudaGetLastError());
+}
+
 template <typename R, typename C2>
 void Engine::run(const double* rho, const double* vext, const double* mu, double* force, double* scalars,
                  cudaStream_t stream) {
   const EvalParams& p = p_;
-  const bool multi = p.L.multi;
-  const bool tensor = p.L.tensor;
   constexpr bool mixed = sizeof(R) == sizeof(float);
   for (cufftHandle h : {plan_rho_, plan_chan_, plan_deriv_, plan_force_}) CDFT_CUFFT(cufftSetStream(h, stream));
-
-  C2* rho_k = static_cast<C2*>(rho_k_);
-  C2* chan_k = static_cast<C2*>(chan_k_);
   R* chan_r = static_cast<R*>(chan_r_);
   R* deriv_r = static_cast<R*>(deriv_r_);
-  C2* deriv_k = static_cast<C2*>(deriv_k_);
-  C2* force_k = static_cast<C2*>(force_k_);
-  R* hs_r = static_cast<R*>(hs_r_);
 
   // cuFFT needs 16-byte aligned FP64 input: stage a misaligned rho
   if (!mixed && ((uintptr_t)rho % 16 != 0)) {
     CDFT_CUDA(cudaMemcpyAsync(h_rho_, rho, sizeof(double) * p.S * p.N, cudaMemcpyDeviceToDevice, stream));
     rho = h_rho_;
   }
-  // 1. rho_k = r2c(rho); mixed precision transforms rho - mean in FP32
-  if constexpr (mixed) {
-    k_species_sums<<<grid_stream_, 256, 0, stream>>>(rho, p.N, p.S, partials_);
-    k_split_convert<<<grid_stream_, 256, 0, stream>>>(rho, p.N, p.S, partials_, grid_stream_,
-                                                  static_cast<float*>(rho_lo_), mean_);
-    CDFT_CUFFT(cufftExecR2C(plan_rho_, static_cast<float*>(rho_lo_), reinterpret_cast<cufftComplex*>(rho_k)));
-  } else {
-    CDFT_CUFFT(cufftExecD2Z(plan_rho_, const_cast<double*>(rho), reinterpret_cast<cufftDoubleComplex*>(rho_k)));
-  }
-  // 2. weighted-density channels in k-space
-  if (!multi && !tensor) k_forward<false, false, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
-  if (!multi && tensor) k_forward<false, true, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
-  if (multi && !tensor) k_forward<true, false, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
-  if (multi && tensor) k_forward<true, true, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
-  CDFT_CUDA(cudaGetLastError());
-  // 3. n_alpha(r)
-  if constexpr (mixed)
-    CDFT_CUFFT(cufftExecC2R(plan_chan_, reinterpret_cast<cufftComplex*>(chan_k), reinterpret_cast<float*>(chan_r)));
-  else
-    CDFT_CUFFT(cufftExecZ2D(plan_chan_, reinterpret_cast<cufftDoubleComplex*>(chan_k), reinterpret_cast<double*>(chan_r)));
+  // 1-3. weighted densities
+  forward_stage<R, C2>(rho, chan_r, mean_, stream);
   // 4. pointwise Phi / dPhi + local terms + reductions
   PointwiseArgs a;
   a.rho = rho;
@@ -319,32 +356,67 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
     }
   });
   CDFT_CUDA(cudaGetLastError());
-  // 5. D_k = r2c(dPhi channels)
-  if constexpr (mixed)
-    CDFT_CUFFT(cufftExecR2C(plan_deriv_, reinterpret_cast<float*>(deriv_r), reinterpret_cast<cufftComplex*>(deriv_k)));
-  else
-    CDFT_CUFFT(cufftExecD2Z(plan_deriv_, reinterpret_cast<double*>(deriv_r), reinterpret_cast<cufftDoubleComplex*>(deriv_k)));
-  // 6. back-convolution
-  if (!multi && !tensor) k_backward<false, false, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
-  if (!multi && tensor) k_backward<false, true, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
-  if (multi && !tensor) k_backward<true, false, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
-  if (multi && tensor) k_backward<true, true, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
-  CDFT_CUDA(cudaGetLastError());
-  // 7. force += c2r(F_k) dV
-  if constexpr (mixed)
-    CDFT_CUFFT(cufftExecC2R(plan_force_, reinterpret_cast<cufftComplex*>(force_k), reinterpret_cast<float*>(hs_r)));
-  else
-    CDFT_CUFFT(cufftExecZ2D(plan_force_, reinterpret_cast<cufftDoubleComplex*>(force_k), reinterpret_cast<double*>(hs_r)));
-  if (!multi && !tensor) k_epilogue<false, false, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar_, force);
-  if (!multi && tensor) k_epilogue<false, true, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar_, force);
-  if (multi && !tensor) k_epilogue<true, false, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar_, force);
-  if (multi && tensor) k_epilogue<true, true, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar_, force);
-  CDFT_CUDA(cudaGetLastError());
+  // 5-7. back-convolution into the force
+  backward_stage<R, C2>(deriv_r, dbar_, force, stream);
   // 8. scalars
   MuArgs ma;
   for (int s = 0; s < kMaxSpecies; ++s) ma.mu[s] = a.mu[s];
   k_reduce_final<<<1, 32 * (4 + kMaxSpecies), 0, stream>>>(partials_, pw_blocks, p, ma, err_, scalars);
   CDFT_CUDA(cudaGetLastError());
+}
+
+// Exact Hessian-vector product (forward-over-reverse): hv = d(force)/d(rho) . v
+// = directional derivative of the force vector along v.  The tangent of the
+// weighted densities is the forward pipeline applied to v; the pointwise
+// kernel carries it through dPhi with dual numbers; the back-convolution is
+// linear.
+template <typename R, typename C2>
+void Engine::run_hvp(const double* rho, const double* v, const double* mu, double* hv, cudaStream_t stream) {
+  const EvalParams& p = p_;
+  constexpr bool mixed = sizeof(R) == sizeof(float);
+  for (cufftHandle h : {plan_rho_, plan_chan_, plan_deriv_, plan_force_}) CDFT_CUFFT(cufftSetStream(h, stream));
+  if (!tan_chan_) {
+    const size_t rs = mixed ? sizeof(float) : sizeof(double);
+    CDFT_CUDA(cudaMalloc(&tan_chan_, rs * p.n_chan * p.N));
+    CDFT_CUDA(cudaMalloc(&tan_mean_, sizeof(double) * kMaxSpecies));
+    CDFT_CUDA(cudaMalloc(&tan_dbar_, sizeof(double) * kMaxChannels));
+    CDFT_CUDA(cudaMalloc(&tan_in_, sizeof(double) * 2 * p.S * p.N));
+  }
+  double* rho_al = tan_in_;
+  double* v_al = tan_in_ + p.S * p.N;
+  CDFT_CUDA(cudaMemcpyAsync(rho_al, rho, sizeof(double) * p.S * p.N, cudaMemcpyDeviceToDevice, stream));
+  CDFT_CUDA(cudaMemcpyAsync(v_al, v, sizeof(double) * p.S * p.N, cudaMemcpyDeviceToDevice, stream));
+  R* chan_r = static_cast<R*>(chan_r_);
+  R* chan_t = static_cast<R*>(tan_chan_);
+  R* deriv_r = static_cast<R*>(deriv_r_);
+  forward_stage<R, C2>(rho_al, chan_r, mean_, stream);
+  forward_stage<R, C2>(v_al, chan_t, tan_mean_, stream);
+  HvpArgs a;
+  a.rho = rho_al;
+  a.v = v_al;
+  a.hv = hv;
+  a.mf_w = mf_w_;
+  a.mean = mean_;
+  a.tmean = tan_mean_;
+  a.tdbar_out = tan_dbar_;
+  with_kernels(mixed, [&](auto model_c, auto multi_c, auto r_c) {
+    constexpr int MD = decltype(model_c)::value;
+    constexpr bool MU = decltype(multi_c)::value;
+    using RT = typename decltype(r_c)::type;
+    if constexpr (std::is_same_v<RT, R>)
+      k_pointwise_hvp<MD, MU, RT><<<grid_stream_, 128, 0, stream>>>(p, chan_r, chan_t, deriv_r, a);
+  });
+  CDFT_CUDA(cudaGetLastError());
+  backward_stage<R, C2>(deriv_r, tan_dbar_, hv, stream);
+  (void)mu;
+}
+
+void Engine::hvp(const double* rho, const double* v, const double* mu, double* hv, cudaStream_t stream) {
+  if (!rho || !v || !hv) throw Error(-1, "hvp: rho, v and hv are required");
+  if (precision_ == kMixed)
+    run_hvp<float, float2>(rho, v, mu, hv, stream);
+  else
+    run_hvp<double, double2>(rho, v, mu, hv, stream);
 }
 
 int Engine::take_error(cudaStream_t stream) {

@@ -50,6 +50,10 @@ class Engine {
   void evaluate(const double* rho, const double* vext, const double* mu, double* force, double* scalars,
                 cudaStream_t stream);
 
+  // Hessian-vector product of Omega: hv = d(force)/d(rho) . v (S*N device
+  // doubles each); exact, by forward-over-reverse differentiation.
+  void hvp(const double* rho, const double* v, const double* mu, double* hv, cudaStream_t stream);
+
   const EvalParams& params() const { return p_; }
   int species() const { return p_.S; }
   long long points() const { return p_.N; }
@@ -77,6 +81,12 @@ class Engine {
   template <typename R, typename C2>
   void run(const double* rho, const double* vext, const double* mu, double* force, double* scalars,
            cudaStream_t stream);
+  template <typename R, typename C2>
+  void run_hvp(const double* rho, const double* v, const double* mu, double* hv, cudaStream_t stream);
+  template <typename R, typename C2>
+  void forward_stage(const double* in, R* chan_out, double* mean_out, cudaStream_t stream);
+  template <typename R, typename C2>
+  void backward_stage(R* deriv, const double* dbar, double* out, cudaStream_t stream);
 
   EvalParams p_{};
   int precision_ = kFP64;
@@ -98,6 +108,10 @@ class Engine {
   double* dbar_ = nullptr;    // derivative-channel constants (mixed precision)
   double* partials_ = nullptr;
   int* err_ = nullptr;        // device error word (set by bounded waits that gave up)
+  void* tan_chan_ = nullptr;  // tangent channels of the exact HVP (allocated on first use)
+  double* tan_mean_ = nullptr;
+  double* tan_dbar_ = nullptr;
+  double* tan_in_ = nullptr;  // aligned copies of rho and v
   int grid_tma_ = 0;
   int grid_stream_ = 0;       // streaming kernels (sums, conversion, epilogue)
   size_t tma_smem_ = 0, tma_smem_v_ = 0;

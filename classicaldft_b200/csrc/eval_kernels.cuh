@@ -379,10 +379,10 @@ struct PointwiseArgs {
 
 // Derivative-channel values at one point from dPhi (the folding of
 // hard_sphere.hpp:121,125,131 plus the T_zz trace folding).
-template <bool MULTI, bool TENSOR>
-__device__ __forceinline__ void fold_derivs(const EvalParams& p, const MeasureDerivs<double>& dm, double* D) {
+template <bool MULTI, bool TENSOR, class T = double>
+__device__ __forceinline__ void fold_derivs(const EvalParams& p, const MeasureDerivs<T>& dm, T* D) {
   using L = Lay<MULTI, TENSOR>;
-  const double dzz = TENSOR ? dm.d_t[5] : 0.0;
+  const T dzz = TENSOR ? dm.d_t[5] : cst<T>(0.0);
   D[L::ETA] = dm.d_eta;
   if (MULTI) {
     D[L::N2] = dm.d_n2 + dzz;
@@ -408,8 +408,8 @@ __device__ __forceinline__ void fold_derivs(const EvalParams& p, const MeasureDe
 }
 
 // Measures at one point from the channel values n[] (species-summed).
-template <bool MULTI, bool TENSOR>
-__device__ __forceinline__ void assemble(const EvalParams& p, const double* n, Measures<double>& m) {
+template <bool MULTI, bool TENSOR, class T = double>
+__device__ __forceinline__ void assemble(const EvalParams& p, const T* n, Measures<T>& m) {
   using L = Lay<MULTI, TENSOR>;
   m.eta = n[L::ETA];
   m.n2 = n[L::N2];
@@ -432,7 +432,7 @@ __device__ __forceinline__ void assemble(const EvalParams& p, const double* n, M
     m.t[5] = m.n2 - m.t[0] - m.t[3];
   } else {
 #pragma unroll
-    for (int c = 0; c < 6; ++c) m.t[c] = 0.0;
+    for (int c = 0; c < 6; ++c) m.t[c] = cst<T>(0.0);
   }
 }
 
@@ -746,6 +746,127 @@ __global__ void __launch_bounds__(kTmaTile) k_pointwise_tma(EvalParams p, const 
     __syncthreads();
   }
   block_reduce_store<NT>(acc, p.n_terms, a.partials);
+}
+
+// ---- exact Hessian-vector product ---------------------------------------
+
+struct HvpArgs {
+  const double* rho;   // S*N
+  const double* v;     // S*N direction
+  double* hv;          // S*N: local tangent terms written here
+  const double* mf_w;
+  const double* mean;  // species means of rho (mixed precision)
+  const double* tmean; // species means of v (mixed precision)
+  double* tdbar_out;   // tangent derivative-channel constants (mixed precision)
+};
+
+// Tangent of the pointwise stage along the tangent channels: dual numbers
+// through fmt_phi_dphi give the derivative channels' directional derivative
+// (forward over the hand-written reverse).  Local terms: the ideal gas
+// tangent v / rho dV (zero where the reference clamps rho to 1e-300,
+// ideal_gas.hpp:312) and the mean-field convolution of v.
+template <int MODEL, bool MULTI, typename RT>
+__global__ void __launch_bounds__(128) k_pointwise_hvp(EvalParams p, const RT* __restrict__ chan,
+                                                       const RT* __restrict__ tchan, RT* __restrict__ deriv,
+                                                       HvpArgs a) {
+  constexpr bool TENSOR = model_has_tensor(MODEL);
+  using L = Lay<MULTI, TENSOR>;
+  constexpr bool SPLIT = sizeof(RT) == sizeof(float);
+  constexpr int NF = L::NFMT;
+  __shared__ double s_off[kMaxChannels];
+  __shared__ double s_toff[kMaxChannels];
+  __shared__ double s_tdbar[NF];
+  if (SPLIT) {
+    if (threadIdx.x == 0) {
+      for (int c = 0; c < p.n_chan; ++c) s_off[c] = s_toff[c] = 0.0;
+#pragma unroll
+      for (int c = 0; c < NF; ++c)
+        for (int s = 0; s < p.S; ++s) {
+          s_off[c] += a.mean[s] * chan_dc<MULTI, TENSOR>(c, s, p);
+          s_toff[c] += a.tmean[s] * chan_dc<MULTI, TENSOR>(c, s, p);
+        }
+      for (int m = 0; m < p.M; ++m) {
+        const double w0 = a.mf_w[m * p.Nk] * (double)p.N;
+        s_off[p.mf_chan_j[m]] = a.mean[p.mf_j[m]] * w0;
+        s_toff[p.mf_chan_j[m]] = a.tmean[p.mf_j[m]] * w0;
+        if (p.mf_chan_i[m] >= 0) {
+          s_off[p.mf_chan_i[m]] = a.mean[p.mf_i[m]] * w0;
+          s_toff[p.mf_chan_i[m]] = a.tmean[p.mf_i[m]] * w0;
+        }
+      }
+      Dual n0[NF];
+#pragma unroll
+      for (int c = 0; c < NF; ++c) n0[c] = Dual{s_off[c], s_toff[c]};
+      Measures<Dual> m0;
+      assemble<MULTI, TENSOR, Dual>(p, n0, m0);
+      Dual phi0;
+      MeasureDerivs<Dual> d0;
+      Dual D0[NF];
+      if (fmt_phi_dphi<MODEL, Dual>(p.A, p.B, m0, phi0, d0)) {
+        fold_derivs<MULTI, TENSOR, Dual>(p, d0, D0);
+      } else {
+#pragma unroll
+        for (int c = 0; c < NF; ++c) D0[c] = Dual{0.0, 0.0};
+      }
+#pragma unroll
+      for (int c = 0; c < NF; ++c) {
+        s_tdbar[c] = D0[c].d;
+        if (blockIdx.x == 0) a.tdbar_out[c] = D0[c].d;
+      }
+    }
+    __syncthreads();
+  }
+  const long long N = p.N;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N;
+       idx += (long long)gridDim.x * blockDim.x) {
+    Dual n[NF];
+#pragma unroll
+    for (int c = 0; c < NF; ++c)
+      n[c] = Dual{(double)chan[c * N + idx] + (SPLIT ? s_off[c] : 0.0),
+                  (double)tchan[c * N + idx] + (SPLIT ? s_toff[c] : 0.0)};
+    Measures<Dual> m;
+    assemble<MULTI, TENSOR, Dual>(p, n, m);
+    Dual phi;
+    MeasureDerivs<Dual> dm;
+    Dual D[NF];
+    if (fmt_phi_dphi<MODEL, Dual>(p.A, p.B, m, phi, dm)) {
+      fold_derivs<MULTI, TENSOR, Dual>(p, dm, D);
+    } else {
+#pragma unroll
+      for (int c = 0; c < NF; ++c) D[c] = Dual{0.0, 0.0};
+    }
+#pragma unroll
+    for (int c = 0; c < NF; ++c) deriv[c * N + idx] = (RT)(SPLIT ? D[c].d - s_tdbar[c] : D[c].d);
+    double h[kMaxSpecies];
+#pragma unroll
+    for (int s = 0; s < kMaxSpecies; ++s) {
+      if (s < p.S) {
+        const double r = a.rho[s * N + idx];
+        h[s] = (r < 1e-300 ? 0.0 : a.v[s * N + idx] / r) * p.dv;
+      }
+    }
+    for (int q = 0; q < p.M; ++q) {
+      const int i = p.mf_i[q], j = p.mf_j[q];
+      const int cjx = p.mf_chan_j[q];
+      const double tj = (double)tchan[cjx * N + idx] + (SPLIT ? s_toff[cjx] : 0.0);
+      if (i == j) {
+#pragma unroll
+        for (int s = 0; s < kMaxSpecies; ++s)
+          if (s == i) h[s] += tj * p.dv;
+      } else {
+        const int cix = p.mf_chan_i[q];
+        const double ti = (double)tchan[cix * N + idx] + (SPLIT ? s_toff[cix] : 0.0);
+#pragma unroll
+        for (int s = 0; s < kMaxSpecies; ++s) {
+          if (s == i) h[s] += 0.5 * tj * p.dv;
+          if (s == j) h[s] += 0.5 * ti * p.dv;
+        }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < kMaxSpecies; ++s)
+      if (s < p.S) a.hv[s * N + idx] = h[s];
+  }
 }
 
 // force_s += c2r(F_s) dV (+ the FP64 constant of the split derivative channels)

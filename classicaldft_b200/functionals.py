@@ -229,6 +229,7 @@ class Engine:
                                  fmt_model.A, fmt_model.B, len(model.interactions), inters, precision))
         self._keep = []
         self.handle = h
+        self.grid = g
         self.S = len(model.species)
         self.N = g.total_points
         self.precision = precision

@@ -153,6 +153,114 @@ CDFT_API int cdft_total(cdft_engine* engine, const double* rho, const double* ve
 CDFT_API int cdft_total_device(cdft_engine* engine, const double* rho, const double* vext, const double* mu, double* force,
                       double* scalars, void* stream);
 
+
+/* ---- drivers (device-resident; single species) --------------------------- */
+
+/* FIRE2 parameters, fire.hpp:33-44 (same names and defaults). */
+typedef struct {
+  double dt, dt_max, dt_min, alpha_start, f_inc, f_dec, f_alpha;
+  int n_delay, max_uphill;
+  double force_tolerance;
+  int max_steps;
+} cdft_fire_params;
+
+#define CDFT_MIN_GRAND_POTENTIAL 0
+#define CDFT_MIN_FIXED_MASS 1
+#define CDFT_MIN_SADDLE 2
+#define CDFT_PARAM_UNBOUNDED 0
+#define CDFT_PARAM_BOUNDED 1
+
+/* Minimizer configuration (minimization.hpp:27-39, 123-147). */
+typedef struct {
+  cdft_fire_params fire;
+  int mode;                 /* CDFT_MIN_* */
+  int parametrization;      /* CDFT_PARAM_* */
+  double rho_min, rho_max;  /* Unbounded{rho_min} / Bounded{rho_min, rho_max} */
+  int homogeneous_boundary; /* Minimizer::use_homogeneous_boundary */
+  double chemical_potential;
+  double target_mass;       /* fixed mass / saddle */
+  double boundary_mass;     /* saddle: mass of the boundary shell */
+  int use_monitor;          /* 1: the minimiser's energy monitor; 0: rms force (Fire::step) */
+  int check_interval;       /* device steps between host checks */
+} cdft_minimizer_config;
+
+typedef struct {
+  double free_energy, grand_potential, rms_force;
+  int iterations, converged, uphill_error;
+} cdft_minimizer_result;
+
+/* Minimizer::grand_potential / Minimizer::fixed_mass (minimization.hpp:182-354)
+ * and the projected FIRE of Search::find (saddle_point.hpp:445-530, mode
+ * CDFT_MIN_SADDLE with `direction`).  rho: N doubles on the device, replaced
+ * by the minimiser's final density.  `refine` (or NULL): an FP64 engine of
+ * the same model that takes over once the monitor drops below
+ * refine_switch * force_tolerance (mixed-precision defect correction).
+ * Returns CDFT_ERR_RUNTIME with "fire::step: exceeded max uphill steps" where
+ * the reference throws (fire.hpp:106-108). */
+CDFT_API int cdft_minimize(cdft_engine* engine, const cdft_minimizer_config* cfg, double* rho,
+                           const double* direction, cdft_engine* refine, double refine_switch,
+                           cdft_minimizer_result* result, void* stream);
+
+/* DDFT step configuration, dynamics.hpp:26-33. */
+typedef struct {
+  double dt, diffusion_coefficient, min_density, dt_max, fp_tolerance;
+  int fp_max_iterations;
+} cdft_ddft_config;
+
+/* integrating_factor_step (dynamics.hpp:333-401): one implicit step of rho
+ * (device, N); cfg->dt is divided by 10 on every restart, as in the
+ * reference.  energy: Omega after the step. */
+CDFT_API int cdft_ddft_step(cdft_engine* engine, cdft_ddft_config* cfg, double chemical_potential, double* rho,
+                            double* energy, int* fp_iterations, void* stream);
+
+/* Simulation::run (dynamics.hpp:583-693) without snapshots: n_steps steps
+ * with the adaptive dt (x2 after 5 successes, capped at dt_max).
+ * times / energies: n_steps + 1 host doubles each, or NULL. */
+CDFT_API int cdft_ddft_run(cdft_engine* engine, cdft_ddft_config* cfg, double chemical_potential, int n_steps,
+                           double* rho, double* times, double* energies, void* stream);
+
+/* Hessian-vector product hv = d(force)/d(rho) . v of Omega at rho (device
+ * vectors, N each); `boundary` 1 zeroes the faces (the fixed boundary of
+ * saddle_point.hpp:377-384).  Exact forward-over-reverse differentiation;
+ * replaces hessian_times_vector (saddle_point.hpp:30-39). */
+CDFT_API int cdft_hvp(cdft_engine* engine, const double* rho, const double* v, double chemical_potential,
+                      int boundary, double* hv, void* stream);
+
+/* The reference's finite-difference product (force(rho + eps v) - force_at_rho) / eps. */
+CDFT_API int cdft_hvp_fd(cdft_engine* engine, const double* rho, const double* force_at_rho, const double* v,
+                         double chemical_potential, double eps, int boundary, double* hv, void* stream);
+
+/* EigenvalueSolver (saddle_point.hpp:158-276). */
+typedef struct {
+  double tolerance;
+  int max_iterations;
+  double hessian_eps;
+  int exact_hvp;            /* 1: cdft_hvp, 0: finite differences as the reference */
+  unsigned long long seed;  /* random initial vector */
+} cdft_eigen_config;
+
+/* Smallest eigenpair of the Hessian at rho (fixed boundary).  vec (device,
+ * N): initial guess when use_guess, else drawn; receives the eigenvector. */
+CDFT_API int cdft_eigen_solve(cdft_engine* engine, const cdft_eigen_config* cfg, const double* rho,
+                              double chemical_potential, double* vec, int use_guess, double* eigenvalue,
+                              int* iterations, int* converged, void* stream);
+
+/* Search (saddle_point.hpp:324-353). */
+typedef struct {
+  cdft_fire_params fire;
+  cdft_eigen_config eigen;
+  double rho_min;
+  double omega_tolerance, tolerance_start, tolerance_factor;
+  int max_outer_iterations, eigenvalue_clear_count;
+} cdft_saddle_config;
+
+/* Search::find (saddle_point.hpp:367-589): eigenvector following at fixed
+ * mass from rho (device, N, replaced by the saddle density); eigvec (device,
+ * N) receives the unstable mode.  out = {grand_potential, eigenvalue}. */
+CDFT_API int cdft_saddle_find(cdft_engine* engine, const cdft_saddle_config* cfg, double* rho,
+                              double chemical_potential, double target_mass, double* eigvec, double out[2],
+                              int* outer_iterations, int* converged, void* stream);
+
 /* Status of earlier asynchronous calls on `stream`: CDFT_ERR_RUNTIME if a
  * bounded device-side wait gave up (the scalars of that call are NaN), else
  * CDFT_OK.  Synchronises the stream and clears the flag.  No reference
