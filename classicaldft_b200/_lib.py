@@ -117,6 +117,8 @@ def lib():
         "cdft_total": [vp, vp, vp, c_double_p, vp, c_double_p],
         "cdft_total_device": [vp, vp, vp, c_double_p, vp, vp, vp],
         "cdft_engine_status": [vp, vp],
+        "cdft_local_terms_noalloc": [vp, vp, c_double_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_double, vp, vp,
+                                     vp],
         "cdft_minimize": [vp, ctypes.POINTER(CMinimizerConfig), vp, vp, vp, ctypes.c_double,
                           ctypes.POINTER(CMinimizerResult), vp],
         "cdft_ddft_step": [vp, ctypes.POINTER(CDDFTConfig), ctypes.c_double, vp, c_double_p,

@@ -56,6 +56,10 @@ void check_split(int split) {
 
 }  // namespace
 
+namespace cdft {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace cdft
+
 extern "C" {
 
 const char* cdft_last_error(void) { return g_last_error.c_str(); }

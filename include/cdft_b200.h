@@ -261,6 +261,25 @@ CDFT_API int cdft_saddle_find(cdft_engine* engine, const cdft_saddle_config* cfg
                               double chemical_potential, double target_mass, double* eigvec, double out[2],
                               int* outer_iterations, int* converged, void* stream);
 
+/* ---- allocation-free entry point ------------------------------------------ */
+
+/* The ideal-gas and external-field terms (ideal_gas.hpp:18-37 and
+ * external_field.hpp:16-30) for callers that cannot allocate device memory:
+ * no engine, no cudaMalloc, no cuFFT.  No counterpart in the reference; it is
+ * the local-term part of the pointwise kernel behind cdft_total.
+ *   rho, vext (or NULL), force: n_species * n_points device doubles
+ *   mu: n_species host values (beta mu);  scalars: 2 + n_species device
+ *   doubles receiving [F_id, F_ext, N_0 .. N_{S-1}] (the entries 2, 3 and
+ *   6.. of cdft_total's scalar block).
+ * force = (ln max(rho, 1e-300) - mu + V) dV.  Scratch is a 28 KiB file-scope
+ * device array (592 x 6 partial sums) held by every GPU that loads the
+ * library; n_species is limited to 4 by it.  The first call on a device looks
+ * the array's address up (cudaGetSymbolAddress): make that first call before
+ * any stream capture.  All calls share the array: calls whose kernels overlap
+ * on the GPU race, so serialise them.  Asynchronous on `stream`. */
+CDFT_API int cdft_local_terms_noalloc(const double* rho, const double* vext, const double* mu, int n_species,
+                                      long long n_points, double dv, double* force, double* scalars, void* stream);
+
 /* Status of earlier asynchronous calls on `stream`: CDFT_ERR_RUNTIME if a
  * bounded device-side wait gave up (the scalars of that call are NaN), else
  * CDFT_OK.  Synchronises the stream and clears the flag.  No reference
