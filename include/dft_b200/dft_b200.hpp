@@ -1,0 +1,500 @@
+// C++ host API of the classicalDFT B200 engine: the reference's functional,
+// grid, minimiser, DDFT and saddle-point interfaces (namespaces and names of
+// include/dft/{grid,types}.hpp, functionals/{functionals,functional}.hpp,
+// algorithms/{fire,minimization,dynamics,saddle_point}.hpp) over the C ABI of
+// cdft_b200.h.  Fields are std::vector<double> in the reference's layout
+// (z fastest); device copies are made per call.  Errors are thrown as the
+// reference's exception types: std::invalid_argument / std::runtime_error.
+//
+// Header-only; link with -lcdft_b200 -lcudart.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../cdft_b200.h"
+
+namespace dft_b200 {
+
+inline void check(int status) {
+  if (status == CDFT_OK) return;
+  const std::string msg = cdft_last_error();
+  if (status == CDFT_ERR_INVALID) throw std::invalid_argument(msg);
+  throw std::runtime_error(msg);
+}
+
+inline void cuda_check(cudaError_t e) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e));
+}
+
+// A device copy of a host vector, freed on scope exit.
+class DeviceVector {
+ public:
+  explicit DeviceVector(std::size_t n) : n_(n) { cuda_check(cudaMalloc(&p_, sizeof(double) * (n ? n : 1))); }
+  explicit DeviceVector(const std::vector<double>& h) : DeviceVector(h.size()) { upload(h); }
+  ~DeviceVector() { cudaFree(p_); }
+  DeviceVector(const DeviceVector&) = delete;
+  DeviceVector& operator=(const DeviceVector&) = delete;
+  void upload(const std::vector<double>& h) {
+    cuda_check(cudaMemcpy(p_, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+  }
+  std::vector<double> download() const {
+    std::vector<double> h(n_);
+    cuda_check(cudaMemcpy(h.data(), p_, sizeof(double) * n_, cudaMemcpyDeviceToHost));
+    return h;
+  }
+  double* get() const { return p_; }
+
+ private:
+  double* p_ = nullptr;
+  std::size_t n_ = 0;
+};
+
+// ---------------------------------------------------------------- grid.hpp
+
+struct Grid {
+  double dx = 0.0;
+  std::array<double, 3> box_size{};
+  std::array<long, 3> shape{};
+  double cell_volume() const { return dx * dx * dx; }
+  long total_points() const { return shape[0] * shape[1] * shape[2]; }
+  long flat_index(long ix, long iy, long iz) const { return iz + shape[2] * (iy + shape[1] * ix); }
+  std::vector<unsigned char> boundary_mask() const {
+    std::vector<unsigned char> m(static_cast<std::size_t>(total_points()), 0);
+    for (long ix = 0; ix < shape[0]; ++ix)
+      for (long iy = 0; iy < shape[1]; ++iy)
+        for (long iz = 0; iz < shape[2]; ++iz)
+          if (ix == 0 || ix == shape[0] - 1 || iy == 0 || iy == shape[1] - 1 || iz == 0 || iz == shape[2] - 1)
+            m[static_cast<std::size_t>(flat_index(ix, iy, iz))] = 1;
+    return m;
+  }
+};
+
+// grid.hpp:87-108
+inline Grid make_grid(double dx, std::array<double, 3> box) {
+  if (dx <= 0.0) throw std::invalid_argument("make_grid: dx must be positive, got " + std::to_string(dx));
+  Grid g{dx, box, {}};
+  for (int d = 0; d < 3; ++d) {
+    if (box[d] <= 0.0) throw std::invalid_argument("make_grid: box dimension must be positive");
+    const double n = box[d] / dx;
+    const long ni = static_cast<long>(std::round(n));
+    if (std::abs(n - static_cast<double>(ni)) > 1e-10)
+      throw std::invalid_argument("make_grid: box dimension " + std::to_string(box[d]) +
+                                  " is not commensurate with dx=" + std::to_string(dx));
+    g.shape[d] = ni;
+  }
+  return g;
+}
+
+// ------------------------------------------------------------- physics
+
+namespace physics {
+
+enum class SplitScheme { WeeksChandlerAndersen = CDFT_SPLIT_WCA, BarkerHenderson = CDFT_SPLIT_BH };
+enum class WeightScheme {
+  InterpolationZero = CDFT_WEIGHT_ZERO,
+  InterpolationLinearE = CDFT_WEIGHT_LINEAR_E,
+  InterpolationLinearF = CDFT_WEIGHT_LINEAR_F,
+  InterpolationQuadraticF = CDFT_WEIGHT_QUADRATIC_F,
+  GaussE = CDFT_WEIGHT_GAUSS_E,
+  GaussF = CDFT_WEIGHT_GAUSS_F,
+};
+
+// potentials.hpp:248-307 (the variant's parameters)
+struct Potential {
+  cdft_potential p{CDFT_POT_LENNARD_JONES, 1.0, 1.0, -1.0, 50.0};
+  double attractive(double r, SplitScheme s = SplitScheme::WeeksChandlerAndersen) const {
+    double out = 0.0;
+    check(cdft_potential_attractive(&p, static_cast<int>(s), &r, 1, &out));
+    return out;
+  }
+  double hard_sphere_diameter(double kT, SplitScheme s = SplitScheme::WeeksChandlerAndersen) const {
+    double d = 0.0;
+    check(cdft_hard_sphere_diameter(&p, kT, static_cast<int>(s), &d));
+    return d;
+  }
+  double vdw_integral(double kT, SplitScheme s = SplitScheme::WeeksChandlerAndersen) const {
+    double v = 0.0;
+    check(cdft_vdw_integral(&p, kT, static_cast<int>(s), &v));
+    return v;
+  }
+};
+
+inline Potential make_lennard_jones(double sigma, double epsilon, double r_cutoff = -1.0) {
+  return Potential{{CDFT_POT_LENNARD_JONES, sigma, epsilon, r_cutoff, 50.0}};
+}
+inline Potential make_ten_wolde_frenkel(double sigma, double epsilon, double r_cutoff = -1.0, double alpha = 50.0) {
+  return Potential{{CDFT_POT_TEN_WOLDE_FRENKEL, sigma, epsilon, r_cutoff, alpha}};
+}
+inline Potential make_wang_ramirez_dobnikar_frenkel(double sigma, double epsilon, double r_cutoff = 3.0) {
+  return Potential{{CDFT_POT_WRDF, sigma, epsilon, r_cutoff, 50.0}};
+}
+
+// interactions.hpp:23-30
+struct Interaction {
+  int species_i = 0, species_j = 0;
+  Potential potential;
+  SplitScheme split = SplitScheme::WeeksChandlerAndersen;
+  WeightScheme weight_scheme = WeightScheme::InterpolationQuadraticF;
+};
+
+struct Species {
+  std::string name;
+  double hard_sphere_diameter = 1.0;
+};
+
+// model.hpp:15-20
+struct Model {
+  Grid grid;
+  std::vector<Species> species;
+  std::vector<Interaction> interactions;
+  double temperature = 1.0;
+};
+
+}  // namespace physics
+
+// ---------------------------------------------------------- functionals
+
+namespace functionals {
+
+// models.hpp:363-419 (as a tag plus esFMT's A, B)
+struct FMTModel {
+  int id = CDFT_WHITEBEAR_II;
+  double A = 1.0, B = 0.0;
+  static FMTModel Rosenfeld() { return {CDFT_ROSENFELD}; }
+  static FMTModel RSLT() { return {CDFT_RSLT}; }
+  static FMTModel WhiteBearI() { return {CDFT_WHITEBEAR_I}; }
+  static FMTModel WhiteBearII() { return {CDFT_WHITEBEAR_II}; }
+  static FMTModel EsFMT(double a = 1.0, double b = 0.0) { return {CDFT_ESFMT, a, b}; }
+};
+
+// functionals.hpp:19-23: the GPU-resident weights of one (FMT model, Model).
+class Weights {
+ public:
+  Weights(const FMTModel& fmt, const physics::Model& model, int precision = CDFT_FP64) : fmt_(fmt) {
+    const auto& g = model.grid;
+    std::vector<double> d;
+    for (const auto& sp : model.species) d.push_back(sp.hard_sphere_diameter);
+    std::vector<std::vector<double>> w;
+    w.reserve(model.interactions.size());
+    std::vector<cdft_interaction> inter;
+    for (const auto& it : model.interactions) {  // mean_field.hpp:146-196 (set-up, host)
+      w.emplace_back(static_cast<std::size_t>(g.total_points()));
+      double a = 0.0;
+      check(cdft_interaction_weight(g.shape.data(), g.dx, &it.potential.p, static_cast<int>(it.split),
+                                    static_cast<int>(it.weight_scheme), model.temperature, w.back().data(), &a));
+      inter.push_back({it.species_i, it.species_j, w.back().data(), a});
+      a_vdw_.push_back(a);
+    }
+    cdft_engine* e = nullptr;
+    check(cdft_create(&e, g.shape.data(), g.dx, static_cast<int>(d.size()), d.data(), fmt.id, fmt.A, fmt.B,
+                      static_cast<int>(inter.size()), inter.empty() ? nullptr : inter.data(), precision));
+    engine_.reset(e);
+  }
+  cdft_engine* engine() const { return engine_.get(); }
+  const std::vector<double>& a_vdw() const { return a_vdw_; }
+  const FMTModel& fmt_model() const { return fmt_; }
+
+ private:
+  struct Del {
+    void operator()(cdft_engine* e) const { cdft_destroy(e); }
+  };
+  FMTModel fmt_;
+  std::unique_ptr<cdft_engine, Del> engine_;
+  std::vector<double> a_vdw_;
+};
+
+inline Weights make_weights(const FMTModel& fmt, const physics::Model& model, int precision = CDFT_FP64) {
+  return Weights(fmt, model, precision);
+}
+
+// types.hpp:17-48 (one species' state)
+struct SpeciesState {
+  std::vector<double> values;          // density
+  std::vector<double> external_field;  // empty: no field
+  double chemical_potential = 0.0;     // beta mu
+};
+struct State {
+  std::vector<SpeciesState> species;
+  double temperature = 1.0;
+};
+
+// functionals/types.hpp:18-23
+struct Result {
+  double free_energy = 0.0;
+  double grand_potential = 0.0;
+  std::vector<std::vector<double>> forces;
+};
+
+// functionals.hpp:64-95
+inline Result total(const physics::Model& model, const State& state, const Weights& weights) {
+  const std::size_t S = state.species.size();
+  const std::size_t N = static_cast<std::size_t>(model.grid.total_points());
+  if (S != model.species.size()) throw std::invalid_argument("total: one SpeciesState per species");
+  std::vector<double> rho(S * N), vext, mu(S), force(S * N), sc(CDFT_SCALAR_COUNT);
+  bool field = false;
+  for (const auto& sp : state.species) field = field || !sp.external_field.empty();
+  if (field) vext.assign(S * N, 0.0);
+  for (std::size_t s = 0; s < S; ++s) {
+    const auto& sp = state.species[s];
+    if (sp.values.size() != N) throw std::invalid_argument("total: density has the wrong size");
+    std::memcpy(rho.data() + s * N, sp.values.data(), sizeof(double) * N);
+    if (!sp.external_field.empty()) {
+      if (sp.external_field.size() != N) throw std::invalid_argument("total: external field has the wrong size");
+      std::memcpy(vext.data() + s * N, sp.external_field.data(), sizeof(double) * N);
+    }
+    mu[s] = sp.chemical_potential;
+  }
+  check(cdft_total(weights.engine(), rho.data(), field ? vext.data() : nullptr, mu.data(), force.data(), sc.data()));
+  Result r;
+  r.free_energy = sc[0];
+  r.grand_potential = sc[1];
+  for (std::size_t s = 0; s < S; ++s) r.forces.emplace_back(force.begin() + s * N, force.begin() + (s + 1) * N);
+  return r;
+}
+
+using ForceCallback = std::function<std::pair<double, std::vector<std::vector<double>>>(
+    const std::vector<std::vector<double>>&)>;
+
+// functional.hpp:22-107
+struct Functional {
+  physics::Model model;
+  std::shared_ptr<Weights> weights;
+
+  Functional(const FMTModel& fmt, physics::Model m, int precision = CDFT_FP64)
+      : model(std::move(m)), weights(std::make_shared<Weights>(fmt, model, precision)) {}
+
+  Result evaluate(const State& state) const { return total(model, state, *weights); }
+
+  // functional.hpp:33-36: the external field is zero (init::from_profile)
+  Result evaluate(const std::vector<double>& rho, double chemical_potential) const {
+    State st;
+    st.temperature = model.temperature;
+    st.species.push_back({rho, {}, chemical_potential});
+    for (std::size_t s = 1; s < model.species.size(); ++s)
+      st.species.push_back({std::vector<double>(rho.size(), 0.0), {}, 0.0});
+    return total(model, st, *weights);
+  }
+
+  double grand_potential(const std::vector<double>& rho, double mu) const { return evaluate(rho, mu).grand_potential; }
+
+  // functional.hpp:62-73
+  ForceCallback grand_potential_callback(double chemical_potential) const {
+    auto self = *this;
+    return [self, chemical_potential](const std::vector<std::vector<double>>& dens) {
+      State st;
+      st.temperature = self.model.temperature;
+      for (const auto& d : dens) st.species.push_back({d, {}, chemical_potential});
+      auto r = total(self.model, st, *self.weights);
+      return std::make_pair(r.grand_potential, r.forces);
+    };
+  }
+};
+
+}  // namespace functionals
+
+// ----------------------------------------------------------- algorithms
+
+namespace algorithms {
+
+namespace fire {
+// fire.hpp:33-44
+struct Fire {
+  double dt = 1e-3, dt_max = 1e-2, dt_min = 1e-8, alpha_start = 0.1, f_inc = 1.1, f_dec = 0.5, f_alpha = 0.99;
+  int n_delay = 5, max_uphill = 20;
+  double force_tolerance = 0.1;
+  int max_steps = 10000;
+  cdft_fire_params c() const {
+    return {dt, dt_max, dt_min, alpha_start, f_inc, f_dec, f_alpha, n_delay, max_uphill, force_tolerance, max_steps};
+  }
+};
+}  // namespace fire
+
+namespace minimization {
+
+struct Unbounded {
+  double rho_min = 1e-18;
+};
+struct Bounded {
+  double rho_min = 1e-18, rho_max = 1.0;
+};
+
+// minimization.hpp:114-121
+struct Result {
+  std::vector<std::vector<double>> densities;
+  double free_energy = 0.0, grand_potential = 0.0, rms_force = 0.0;
+  int iterations = 0;
+  bool converged = false;
+};
+
+// minimization.hpp:123-147; runs on the device (cdft_minimize)
+struct Minimizer {
+  fire::Fire fire{};
+  bool bounded = false;
+  Unbounded unbounded{};
+  Bounded bounded_param{};
+  bool use_homogeneous_boundary = true;
+  int check_interval = 25;
+  const functionals::Weights* refine = nullptr;  // optional FP64 defect correction
+  double refine_switch = 10.0;
+
+  Result run(const functionals::Weights& w, const std::vector<double>& rho0, int mode, double mu, double mass) const {
+    cdft_minimizer_config cfg{};
+    cfg.fire = fire.c();
+    cfg.mode = mode;
+    cfg.parametrization = bounded ? CDFT_PARAM_BOUNDED : CDFT_PARAM_UNBOUNDED;
+    cfg.rho_min = bounded ? bounded_param.rho_min : unbounded.rho_min;
+    cfg.rho_max = bounded ? bounded_param.rho_max : 1.0;
+    cfg.homogeneous_boundary = use_homogeneous_boundary ? 1 : 0;
+    cfg.chemical_potential = mu;
+    cfg.target_mass = mass;
+    cfg.use_monitor = 1;
+    cfg.check_interval = check_interval;
+    DeviceVector d(rho0);
+    cdft_minimizer_result res{};
+    check(cdft_minimize(w.engine(), &cfg, d.get(), nullptr, refine ? refine->engine() : nullptr, refine_switch, &res,
+                        nullptr));
+    Result r;
+    r.densities.push_back(d.download());
+    r.free_energy = res.free_energy;
+    r.grand_potential = res.grand_potential;
+    r.rms_force = res.rms_force;
+    r.iterations = res.iterations;
+    r.converged = res.converged != 0;
+    return r;
+  }
+  // minimization.hpp:182-278
+  Result fixed_mass(const physics::Model&, const functionals::Weights& w, const std::vector<double>& rho0, double mu,
+                    double target_mass) const {
+    return run(w, rho0, CDFT_MIN_FIXED_MASS, mu, target_mass);
+  }
+  // minimization.hpp:280-354
+  Result grand_potential(const physics::Model&, const functionals::Weights& w, const std::vector<double>& rho0,
+                         double mu) const {
+    return run(w, rho0, CDFT_MIN_GRAND_POTENTIAL, mu, 0.0);
+  }
+};
+
+}  // namespace minimization
+
+namespace dynamics {
+
+// dynamics.hpp:26-33
+struct StepConfig {
+  double dt = 1e-4, diffusion_coefficient = 1.0, min_density = 1e-18, dt_max = 1.0, fp_tolerance = 1e-4;
+  int fp_max_iterations = 100;
+  cdft_ddft_config c() const { return {dt, diffusion_coefficient, min_density, dt_max, fp_tolerance, fp_max_iterations}; }
+};
+
+struct SimulationResult {
+  std::vector<std::vector<double>> densities;
+  std::vector<double> times, energies;
+  double mass_initial = 0.0, mass_final = 0.0;
+};
+
+// dynamics.hpp:564-693 (integrating-factor DDFT on the device)
+struct Simulation {
+  StepConfig step;
+  int n_steps = 1000;
+  SimulationResult run(std::vector<std::vector<double>> densities, const Grid& grid, const functionals::Weights& w,
+                       double chemical_potential) const {
+    SimulationResult r;
+    DeviceVector d(densities.at(0));
+    cdft_ddft_config c = step.c();
+    r.times.assign(static_cast<std::size_t>(n_steps) + 1, 0.0);
+    r.energies.assign(static_cast<std::size_t>(n_steps) + 1, 0.0);
+    double m0 = 0.0;
+    for (double v : densities[0]) m0 += v;
+    check(cdft_ddft_run(w.engine(), &c, chemical_potential, n_steps, d.get(), r.times.data(), r.energies.data(),
+                        nullptr));
+    r.densities.push_back(d.download());
+    double m1 = 0.0;
+    for (double v : r.densities[0]) m1 += v;
+    r.mass_initial = m0 * grid.cell_volume();
+    r.mass_final = m1 * grid.cell_volume();
+    return r;
+  }
+};
+
+}  // namespace dynamics
+
+namespace saddle_point {
+
+struct EigenvalueResult {
+  std::vector<double> eigenvector;
+  double eigenvalue = 0.0;
+  int iterations = 0;
+  bool converged = false;
+};
+
+// saddle_point.hpp:158-169 (exact_hvp replaces the finite difference)
+struct EigenvalueSolver {
+  double tolerance = 1e-4;
+  int max_iterations = 300;
+  double hessian_eps = 1e-6;
+  bool exact_hvp = false;
+  unsigned long long seed = 42;
+  cdft_eigen_config c() const { return {tolerance, max_iterations, hessian_eps, exact_hvp ? 1 : 0, seed}; }
+  EigenvalueResult solve(const functionals::Weights& w, const std::vector<double>& rho, double mu,
+                         const std::vector<double>& initial_guess = {}) const {
+    DeviceVector d(rho);
+    DeviceVector v(rho.size());
+    if (initial_guess.size() == rho.size()) v.upload(initial_guess);
+    cdft_eigen_config cfg = c();
+    EigenvalueResult r;
+    int it = 0, conv = 0;
+    check(cdft_eigen_solve(w.engine(), &cfg, d.get(), mu, v.get(), initial_guess.size() == rho.size() ? 1 : 0,
+                           &r.eigenvalue, &it, &conv, nullptr));
+    r.eigenvector = v.download();
+    r.iterations = it;
+    r.converged = conv != 0;
+    return r;
+  }
+};
+
+struct Result {
+  std::vector<double> density, eigenvector;
+  double grand_potential = 0.0, eigenvalue = 0.0;
+  int outer_iterations = 0;
+  bool converged = false;
+};
+
+// saddle_point.hpp:324-353 (same defaults)
+struct Search {
+  fire::Fire fire{1e-3, 1.0, 1e-8, 0.01, 1.1, 0.5, 1.0, 5, 20, 1e-4, 100000};
+  EigenvalueSolver eigenvalue{1e-4, 300, 1e-6};
+  minimization::Unbounded param{1e-18};
+  double omega_tolerance = 1e-5, tolerance_start = 1e-3, tolerance_factor = 10.0;
+  int max_outer_iterations = 20, eigenvalue_clear_count = 2;
+  Result find(const physics::Model&, const functionals::Weights& w, const std::vector<double>& rho0, double mu,
+              double target_mass) const {
+    cdft_saddle_config cfg{fire.c(),        eigenvalue.c(),   param.rho_min,        omega_tolerance,
+                           tolerance_start, tolerance_factor, max_outer_iterations, eigenvalue_clear_count};
+    DeviceVector d(rho0);
+    DeviceVector ev(rho0.size());
+    double out[2] = {0.0, 0.0};
+    int it = 0, conv = 0;
+    check(cdft_saddle_find(w.engine(), &cfg, d.get(), mu, target_mass, ev.get(), out, &it, &conv, nullptr));
+    Result r;
+    r.density = d.download();
+    r.eigenvector = ev.download();
+    r.grand_potential = out[0];
+    r.eigenvalue = out[1];
+    r.outer_iterations = it;
+    r.converged = conv != 0;
+    return r;
+  }
+};
+
+}  // namespace saddle_point
+}  // namespace algorithms
+}  // namespace dft_b200
