@@ -9,7 +9,8 @@ from ._lib import FP64, MIXED, EngineError, lib  # noqa: F401
 from .functionals import (BARKER_HENDERSON, WEEKS_CHANDLER_ANDERSEN, Engine, EsFMT, FMTModel, Functional,  # noqa: F401
                           Grid, Interaction, Model, Potential, Result, Rosenfeld, RSLT, Species, Weights,
                           WhiteBearI, WhiteBearII, interaction_weight, make_grid, make_lennard_jones,
-                          make_ten_wolde_frenkel, make_wang_ramirez_dobnikar_frenkel, make_weights, total)
+                          make_ten_wolde_frenkel, make_wang_ramirez_dobnikar_frenkel, make_weights, total,
+                          total_batch)
 
 from .algorithms import (Bounded, EigenvalueResult, EigenvalueSolver, Fire, MinimizationResult, Minimizer,  # noqa: F401
                          SaddleResult, Search, Simulation, StepConfig, Unbounded, hessian_times_vector,

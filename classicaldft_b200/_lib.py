@@ -111,6 +111,10 @@ def lib():
                                     ctypes.c_double, c_double_p, c_double_p],
         "cdft_create": [ctypes.POINTER(vp), c_long3, ctypes.c_double, ctypes.c_int, c_double_p, ctypes.c_int,
                         ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.POINTER(CInteraction), ctypes.c_int],
+        "cdft_create_batch": [ctypes.POINTER(vp), c_long3, ctypes.c_double, ctypes.c_int, c_double_p, ctypes.c_int,
+                              ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.POINTER(CInteraction),
+                              ctypes.c_int, ctypes.c_int],
+        "cdft_engine_batch": [vp, ctypes.POINTER(ctypes.c_int)],
         "cdft_destroy": [vp],
         "cdft_engine_info": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "cdft_engine_a_vdw": [vp, ctypes.c_int, c_double_p],
@@ -121,6 +125,8 @@ def lib():
                                      vp],
         "cdft_minimize": [vp, ctypes.POINTER(CMinimizerConfig), vp, vp, vp, ctypes.c_double,
                           ctypes.POINTER(CMinimizerResult), vp],
+        "cdft_minimize_batch": [vp, ctypes.POINTER(CMinimizerConfig), c_double_p, c_double_p, vp, vp,
+                                ctypes.c_double, ctypes.POINTER(CMinimizerResult), vp],
         "cdft_ddft_step": [vp, ctypes.POINTER(CDDFTConfig), ctypes.c_double, vp, c_double_p,
                            ctypes.POINTER(ctypes.c_int), vp],
         "cdft_ddft_run": [vp, ctypes.POINTER(CDDFTConfig), ctypes.c_double, ctypes.c_int, vp, c_double_p, c_double_p,

@@ -103,12 +103,7 @@ class Minimizer:
     refine: Weights = None
     refine_switch: float = 10.0
 
-    def _run(self, weights: Weights, rho, mode, mu, target_mass=0.0, boundary_mass=0.0, direction=None,
-             use_monitor=True):
-        torch = _torch()
-        d, host = _dev(rho)
-        if not host:
-            d = d.clone()
+    def _config(self, mode, mu, target_mass=0.0, boundary_mass=0.0, use_monitor=True):
         cfg = _lib.CMinimizerConfig()
         cfg.fire = self.fire.c()
         cfg.mode = mode
@@ -122,6 +117,15 @@ class Minimizer:
         cfg.boundary_mass = boundary_mass
         cfg.use_monitor = 1 if use_monitor else 0
         cfg.check_interval = self.check_interval
+        return cfg
+
+    def _run(self, weights: Weights, rho, mode, mu, target_mass=0.0, boundary_mass=0.0, direction=None,
+             use_monitor=True):
+        torch = _torch()
+        d, host = _dev(rho)
+        if not host:
+            d = d.clone()
+        cfg = self._config(mode, mu, target_mass, boundary_mass, use_monitor)
         res = _lib.CMinimizerResult()
         dirp = None
         if direction is not None:
@@ -147,6 +151,47 @@ class Minimizer:
     def fixed_mass(self, model: Model, weights: Weights, initial_density, chemical_potential, target_mass):
         """minimization.hpp:182-278."""
         return self._run(weights, initial_density, 1, chemical_potential, target_mass=target_mass)
+
+    def _run_batch(self, weights: Weights, rhos, mode, mus, masses=None):
+        torch = _torch()
+        e = weights.engine
+        B, N = e.batch, e.N
+        if isinstance(rhos, np.ndarray) or not hasattr(rhos, "data_ptr"):
+            d = torch.tensor(np.asarray(rhos, dtype=np.float64).reshape(B, N), device="cuda")
+            host = True
+        else:
+            d = rhos.reshape(B, N).to(torch.float64).contiguous().clone()
+            host = False
+        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mus, dtype=np.float64), (B,)))
+        mass = None if masses is None else np.ascontiguousarray(
+            np.broadcast_to(np.asarray(masses, dtype=np.float64), (B,)))
+        cfg = self._config(mode, 0.0)
+        res = (_lib.CMinimizerResult * B)()
+        ref = self.refine.engine.handle if self.refine is not None else None
+        _lib.check(_lib.lib().cdft_minimize_batch(
+            e.handle, ctypes.byref(cfg), mu.ctypes.data_as(_lib.c_double_p),
+            None if mass is None else mass.ctypes.data_as(_lib.c_double_p), d.data_ptr(), ref, self.refine_switch,
+            res, _stream()))
+        torch.cuda.synchronize()
+        out = d.cpu().numpy() if host else d
+        return [MinimizationResult([out[b]], r.free_energy, r.grand_potential, r.rms_force, r.iterations,
+                                   bool(r.converged)) for b, r in enumerate(res)], [bool(r.uphill_error) for r in res]
+
+    def grand_potential_batch(self, model: Model, weights: Weights, initial_densities, chemical_potentials):
+        """``grand_potential`` for every problem of a batched engine (make_weights(..., batch=B)):
+        initial_densities (B, N), chemical_potentials (B,).  Returns B results."""
+        res, uphill = self._run_batch(weights, initial_densities, 0, chemical_potentials)
+        if any(uphill):
+            raise RuntimeError(f"fire::step: exceeded max uphill steps (problems {np.flatnonzero(uphill).tolist()})")
+        return res
+
+    def fixed_mass_batch(self, model: Model, weights: Weights, initial_densities, chemical_potentials,
+                         target_masses):
+        """``fixed_mass`` for every problem of a batched engine; target_masses (B,)."""
+        res, uphill = self._run_batch(weights, initial_densities, 1, chemical_potentials, target_masses)
+        if any(uphill):
+            raise RuntimeError(f"fire::step: exceeded max uphill steps (problems {np.flatnonzero(uphill).tolist()})")
+        return res
 
 
 # ---------------------------------------------------------------- DDFT

@@ -115,9 +115,9 @@ int cdft_interaction_weight(const long shape[3], double dx, const cdft_potential
   });
 }
 
-int cdft_create(cdft_engine** out, const long shape[3], double dx, int n_species, const double* diameters,
-                int fmt_model, double esfmt_A, double esfmt_B, int n_interactions,
-                const cdft_interaction* interactions, int precision) {
+int cdft_create_batch(cdft_engine** out, const long shape[3], double dx, int n_species, const double* diameters,
+                      int fmt_model, double esfmt_A, double esfmt_B, int n_interactions,
+                      const cdft_interaction* interactions, int precision, int batch) {
   return guarded([&] {
     if (!out) throw std::invalid_argument("out is NULL");
     *out = nullptr;
@@ -133,6 +133,8 @@ int cdft_create(cdft_engine** out, const long shape[3], double dx, int n_species
     spec.esfmt_A = esfmt_A;
     spec.esfmt_B = esfmt_B;
     spec.precision = precision;
+    if (batch < 1 || batch > CDFT_MAX_BATCH) throw std::invalid_argument("batch must be in [1, 64]");
+    spec.batch = batch;
     const long long N = (long long)shape[0] * shape[1] * shape[2];
     if (shape[0] <= 0 || shape[1] <= 0 || shape[2] <= 0) throw std::invalid_argument("grid dimensions must be positive");
     for (int m = 0; m < n_interactions; ++m) {
@@ -152,6 +154,20 @@ int cdft_create(cdft_engine** out, const long shape[3], double dx, int n_species
       throw;
     }
     *out = e;
+  });
+}
+
+int cdft_create(cdft_engine** out, const long shape[3], double dx, int n_species, const double* diameters,
+                int fmt_model, double esfmt_A, double esfmt_B, int n_interactions,
+                const cdft_interaction* interactions, int precision) {
+  return cdft_create_batch(out, shape, dx, n_species, diameters, fmt_model, esfmt_A, esfmt_B, n_interactions,
+                           interactions, precision, 1);
+}
+
+int cdft_engine_batch(const cdft_engine* engine, int* batch) {
+  return guarded([&] {
+    if (!engine || !batch) throw std::invalid_argument("engine or batch is NULL");
+    *batch = engine->impl->batch();
   });
 }
 
@@ -192,17 +208,17 @@ int cdft_total(cdft_engine* engine, const double* rho, const double* vext, const
   return guarded([&] {
     if (!engine || !rho || !mu) throw std::invalid_argument("engine, rho and mu are required");
     cdft::Engine& e = *engine->impl;
-    const size_t bytes = sizeof(double) * e.species() * e.points();
+    const size_t bytes = sizeof(double) * e.batch() * e.species() * e.points();
     cudaStream_t st = e.stream();
     CDFT_CUDA(cudaMemcpyAsync(e.host_rho(), rho, bytes, cudaMemcpyHostToDevice, st));
     if (vext) CDFT_CUDA(cudaMemcpyAsync(e.host_vext(), vext, bytes, cudaMemcpyHostToDevice, st));
     e.evaluate(e.host_rho(), vext ? e.host_vext() : nullptr, mu, e.host_force(), e.host_scalars(), st);
     if (force) CDFT_CUDA(cudaMemcpyAsync(force, e.host_force(), bytes, cudaMemcpyDeviceToHost, st));
-    double tmp[CDFT_SCALAR_COUNT];
-    CDFT_CUDA(cudaMemcpyAsync(tmp, e.host_scalars(), sizeof(tmp), cudaMemcpyDeviceToHost, st));
+    std::vector<double> tmp((size_t)e.batch() * CDFT_SCALAR_COUNT);
+    CDFT_CUDA(cudaMemcpyAsync(tmp.data(), e.host_scalars(), sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost, st));
     CDFT_CUDA(cudaStreamSynchronize(st));
     if (e.take_error(st)) throw cdft::Error(CDFT_ERR_RUNTIME, "evaluation aborted: a bounded device wait timed out");
-    if (scalars) std::memcpy(scalars, tmp, sizeof(tmp));
+    if (scalars) std::memcpy(scalars, tmp.data(), sizeof(double) * tmp.size());
   });
 }
 
@@ -225,8 +241,9 @@ int cdft_engine_status(cdft_engine* engine, void* stream) {
 
 namespace {
 
-cdft::Drivers& drivers_of(cdft_engine* e) {
+cdft::Drivers& drivers_of(cdft_engine* e, bool batched = false) {
   if (!e) throw std::invalid_argument("engine is NULL");
+  if (!batched && e->impl->batch() != 1) throw std::invalid_argument("the drivers need an engine with batch 1");
   if (!e->drivers) e->drivers = new cdft::Drivers(*e->impl);
   return *e->drivers;
 }
@@ -260,33 +277,59 @@ cdft::Drivers::EigenConfig to_eigen(const cdft_eigen_config& c) {
 
 }  // namespace
 
+namespace {
+cdft::FireConfig to_fire_config(const cdft_minimizer_config* cfg) {
+  cdft::FireConfig fc;
+  fc.fire = to_fire(cfg->fire);
+  fc.mode = cfg->mode;
+  if (fc.mode < CDFT_MIN_GRAND_POTENTIAL || fc.mode > CDFT_MIN_SADDLE) throw std::invalid_argument("unknown mode");
+  fc.param = cfg->parametrization;
+  fc.rho_min = cfg->rho_min;
+  fc.rho_max = cfg->rho_max;
+  fc.homogeneous_boundary = cfg->homogeneous_boundary != 0;
+  fc.mu = cfg->chemical_potential;
+  fc.target_mass = cfg->target_mass;
+  fc.boundary_mass = cfg->boundary_mass;
+  fc.use_monitor = cfg->use_monitor != 0;
+  fc.check_interval = cfg->check_interval > 0 ? cfg->check_interval : 25;
+  return fc;
+}
+
+void to_result(const cdft::FireResult& r, cdft_minimizer_result* result) {
+  result->free_energy = r.free_energy;
+  result->grand_potential = r.grand_potential;
+  result->rms_force = r.rms_force;
+  result->iterations = r.iterations;
+  result->converged = r.converged ? 1 : 0;
+  result->uphill_error = r.uphill_error ? 1 : 0;
+}
+}  // namespace
+
 int cdft_minimize(cdft_engine* engine, const cdft_minimizer_config* cfg, double* rho, const double* direction,
                   cdft_engine* refine, double refine_switch, cdft_minimizer_result* result, void* stream) {
   return guarded([&] {
     if (!cfg || !rho || !result) throw std::invalid_argument("cfg, rho and result are required");
     cdft::Drivers& d = drivers_of(engine);
-    cdft::FireConfig fc;
-    fc.fire = to_fire(cfg->fire);
-    fc.mode = cfg->mode;
-    if (fc.mode < CDFT_MIN_GRAND_POTENTIAL || fc.mode > CDFT_MIN_SADDLE) throw std::invalid_argument("unknown mode");
-    fc.param = cfg->parametrization;
-    fc.rho_min = cfg->rho_min;
-    fc.rho_max = cfg->rho_max;
-    fc.homogeneous_boundary = cfg->homogeneous_boundary != 0;
-    fc.mu = cfg->chemical_potential;
-    fc.target_mass = cfg->target_mass;
-    fc.boundary_mass = cfg->boundary_mass;
-    fc.use_monitor = cfg->use_monitor != 0;
-    fc.check_interval = cfg->check_interval > 0 ? cfg->check_interval : 25;
+    if (refine && refine->impl->batch() != 1) throw std::invalid_argument("the refine engine needs batch 1");
+    cdft::FireConfig fc = to_fire_config(cfg);
     cdft::FireResult r = d.fire_minimize(fc, rho, direction, static_cast<cudaStream_t>(stream),
                                          refine ? refine->impl : nullptr, refine_switch);
-    result->free_energy = r.free_energy;
-    result->grand_potential = r.grand_potential;
-    result->rms_force = r.rms_force;
-    result->iterations = r.iterations;
-    result->converged = r.converged ? 1 : 0;
-    result->uphill_error = r.uphill_error ? 1 : 0;
+    to_result(r, result);
     if (r.uphill_error) throw cdft::Error(CDFT_ERR_RUNTIME, "fire::step: exceeded max uphill steps");
+  });
+}
+
+int cdft_minimize_batch(cdft_engine* engine, const cdft_minimizer_config* cfg, const double* mu,
+                        const double* target_mass, double* rho, cdft_engine* refine, double refine_switch,
+                        cdft_minimizer_result* results, void* stream) {
+  return guarded([&] {
+    if (!cfg || !mu || !rho || !results) throw std::invalid_argument("cfg, mu, rho and results are required");
+    cdft::Drivers& d = drivers_of(engine, true);
+    if (cfg->mode == CDFT_MIN_SADDLE) throw std::invalid_argument("cdft_minimize_batch: no saddle mode");
+    cdft::FireConfig fc = to_fire_config(cfg);
+    std::vector<cdft::FireResult> r = d.fire_minimize_batch(fc, mu, target_mass, rho, static_cast<cudaStream_t>(stream),
+                                                            refine ? refine->impl : nullptr, refine_switch);
+    for (size_t b = 0; b < r.size(); ++b) to_result(r[b], results + b);
   });
 }
 

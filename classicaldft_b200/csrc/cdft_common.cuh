@@ -20,6 +20,9 @@ namespace cdft {
 
 constexpr int kMaxSpecies = 4;
 constexpr int kMaxInteractions = 8;
+// Problems of one shape evaluated together by a batched engine (one set of
+// launches; the problem index is blockIdx.y, or blockIdx.x in k_reduce_final).
+constexpr int kMaxBatch = 64;
 constexpr double kPi = 3.14159265358979323846;
 
 // FMT model ids (include/dft/functionals/fmt/models.hpp:153-359).
@@ -87,6 +90,13 @@ struct EvalParams {
   int mf_chan_i[kMaxInteractions];  // channel holding w * rho_i (cross terms), else -1
   int n_chan;                       // FMT + mean-field channels
   int n_terms;                      // reduction terms
+  int batch;                        // problems evaluated together (1..kMaxBatch)
+};
+
+// Chemical potentials (beta mu) of every problem of a batch, passed to the
+// kernels that need them as a __grid_constant__ parameter.
+struct MuArgs {
+  double mu[kMaxBatch][kMaxSpecies];
 };
 
 // Reduction term order: F_hs, F_id, F_ext, F_mf, then N_s for each species.

@@ -13,6 +13,10 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr int kRedTerms = 4;
+constexpr int kOut = 8;  // reduced values per problem: two groups of kRedTerms
+
+// Batched drivers: vector kernels take the problem from blockIdx.y, the
+// single-thread control kernels from blockIdx.x (one block per problem).
 
 __device__ __forceinline__ bool on_face(long long idx, int nx, int ny, int nz) {
   const int iz = (int)(idx % nz);
@@ -22,7 +26,7 @@ __device__ __forceinline__ bool on_face(long long idx, int nx, int ny, int nz) {
   return ix == 0 || ix == nx - 1 || iy == 0 || iy == ny - 1 || iz == 0 || iz == nz - 1;
 }
 
-// block sums of up to kRedTerms values -> partials[block][kRedTerms]
+// block sums of up to kRedTerms values -> partials[problem][block][kRedTerms]
 __device__ __forceinline__ void block_sum_store(double (&a)[kRedTerms], double* __restrict__ partials) {
   __shared__ double sh[32][kRedTerms];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -37,13 +41,16 @@ __device__ __forceinline__ void block_sum_store(double (&a)[kRedTerms], double* 
   if (threadIdx.x < kRedTerms) {
     double v = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sh[w][threadIdx.x];
-    partials[blockIdx.x * kRedTerms + threadIdx.x] = v;
+    partials[((long long)blockIdx.y * gridDim.x + blockIdx.x) * kRedTerms + threadIdx.x] = v;
   }
 }
 
-// one warp: out[t] = sum_b partials[b][t]
+// out[t] = sum_b partials[b][t], one warp per term; block i reduces problem i
+// into out + i * kOut.
 __global__ void k_finish_sums(const double* __restrict__ partials, int nblocks, double* __restrict__ out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  partials += (long long)blockIdx.x * nblocks * kRedTerms;
+  out += blockIdx.x * kOut;
   if (warp >= kRedTerms) return;
   double v = 0.0;
   for (int b = lane; b < nblocks; b += 32) v += partials[b * kRedTerms + warp];
@@ -66,6 +73,18 @@ struct Vec {
   double rho_min, range;
 };
 
+// The vectors of problem blockIdx.y.
+__device__ __forceinline__ Vec slice(Vec a) {
+  const long long o = (long long)blockIdx.y * a.N;
+  a.x += o;
+  a.v += o;
+  a.f += o;
+  a.rho += o;
+  a.grad += o;
+  if (a.dir) a.dir += o;
+  return a;
+}
+
 __device__ __forceinline__ double to_density(const Vec& a, double x) {
   if (a.param == kUnbounded) return a.rho_min + x * x;
   const double x2 = x * x;
@@ -81,6 +100,8 @@ __device__ __forceinline__ double drho_dx(const Vec& a, double x) {
 
 // minimization.hpp:63-78
 __global__ void k_from_density(Vec a, const double* __restrict__ rho) {
+  a = slice(a);
+  rho += (long long)blockIdx.y * a.N;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
     double d = rho[i] - a.rho_min;
     double x;
@@ -99,6 +120,7 @@ __global__ void k_from_density(Vec a, const double* __restrict__ rho) {
 
 // sums: [sum rho, sum_interior rho]
 __global__ void k_density_sums(Vec a, double* __restrict__ partials) {
+  a = slice(a);
   double s[kRedTerms] = {0, 0, 0, 0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
     const double r = a.rho[i];
@@ -109,6 +131,7 @@ __global__ void k_density_sums(Vec a, double* __restrict__ partials) {
 }
 
 __global__ void k_power(Vec a, double* __restrict__ partials) {
+  a = slice(a);
   double s[kRedTerms] = {0, 0, 0, 0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x)
     s[0] += a.v[i] * a.f[i];
@@ -117,6 +140,8 @@ __global__ void k_power(Vec a, double* __restrict__ partials) {
 
 // fire.hpp:95-121: the power test, dt/alpha adaptation and uphill count.
 __global__ void k_fire_control1(FireDevState* st, const double* __restrict__ sums, FireParams fp) {
+  st += blockIdx.x;
+  sums += blockIdx.x * kOut;
   if (threadIdx.x != 0 || !st->active) return;
   const double power = sums[0];
   st->dt_prev = st->dt;
@@ -147,6 +172,8 @@ __global__ void k_fire_control1(FireDevState* st, const double* __restrict__ sum
 // fire.hpp:110-126: backtrack (undo half a step with the old dt, kill v), then
 // v += dt f; sums |v|^2.
 __global__ void k_fire_vstep(Vec a, const FireDevState* __restrict__ st, double* __restrict__ partials) {
+  a = slice(a);
+  st += blockIdx.y;
   double s[kRedTerms] = {0, 0, 0, 0};
   if (st->active) {
     const double dt = st->dt, dtp = st->dt_prev;
@@ -166,19 +193,19 @@ __global__ void k_fire_vstep(Vec a, const FireDevState* __restrict__ st, double*
   block_sum_store(s, partials);
 }
 
-struct FireAux {
-  double f2;  // |f|^2 of the forces driving this step
-};
-
-__global__ void k_fire_ratio(FireDevState* st, const double* __restrict__ sums, const FireAux* __restrict__ aux) {
+__global__ void k_fire_ratio(FireDevState* st, const double* __restrict__ sums) {
+  st += blockIdx.x;
+  sums += blockIdx.x * kOut;
   if (threadIdx.x != 0 || !st->active) return;
   const double v_norm = sqrt(sums[0]);
-  const double f_norm = sqrt(aux->f2);
+  const double f_norm = sqrt(st->f2);
   st->ratio = (f_norm > 0.0) ? v_norm / f_norm : -1.0;
 }
 
 // fire.hpp:137-148 then the parametrisation: mixing, x += dt v, rho = rho(x).
 __global__ void k_fire_xstep(Vec a, const FireDevState* __restrict__ st) {
+  a = slice(a);
+  st += blockIdx.y;
   if (!st->active) return;
   const double dt = st->dt, al = st->alpha, ratio = st->ratio;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
@@ -194,7 +221,6 @@ __global__ void k_fire_xstep(Vec a, const FireDevState* __restrict__ st) {
 struct ComputeCfg {
   int mode;
   int homogeneous;
-  double target_mass;
   double boundary_mass;
   double n_face;
 };
@@ -202,21 +228,25 @@ struct ComputeCfg {
 // Fixed-mass rescale factor (minimization.hpp:193-197, saddle_point.hpp:448-463).
 __global__ void k_scale_factor(FireDevState* st, const double* __restrict__ sums, ComputeCfg cc, double dv,
                                int force_compute) {
+  st += blockIdx.x;
+  sums += blockIdx.x * kOut;
   if (threadIdx.x != 0) return;
   if (!st->active && !force_compute) return;
   double scale = 1.0;
   if (cc.mode == kFixedMass) {
     const double mass = sums[0] * dv;
-    if (mass > 0.0) scale = cc.target_mass / mass;
+    if (mass > 0.0) scale = st->target_mass / mass;
   } else if (cc.mode == kSaddle) {
     const double m_int = sums[1] * dv;
-    const double m_t = cc.target_mass - cc.boundary_mass;
+    const double m_t = st->target_mass - cc.boundary_mass;
     if (m_int > 0.0 && m_t > 0.0) scale = m_t / m_int;
   }
   st->scale = scale;
 }
 
 __global__ void k_rescale(Vec a, const FireDevState* __restrict__ st, ComputeCfg cc, int force_compute) {
+  a = slice(a);
+  st += blockIdx.y;
   if ((!st->active && !force_compute) || cc.mode == kGrandPotential) return;
   const double sc = st->scale;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
@@ -226,6 +256,7 @@ __global__ void k_rescale(Vec a, const FireDevState* __restrict__ st, ComputeCfg
 
 // sums [sum_face grad, sum_interior grad*rho, sum_face rho, sum_face grad*rho]
 __global__ void k_post_sums(Vec a, double* __restrict__ partials) {
+  a = slice(a);
   double s[kRedTerms] = {0, 0, 0, 0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
     const double g = a.grad[i], r = a.rho[i];
@@ -241,17 +272,19 @@ __global__ void k_post_sums(Vec a, double* __restrict__ partials) {
 }
 
 // The Lagrange multiplier (minimization.hpp:212-217, saddle_point.hpp:472-480).
-__global__ void k_post_control(FireDevState* st, const double* __restrict__ sums, ComputeCfg cc, double* bavg_out) {
+__global__ void k_post_control(FireDevState* st, const double* __restrict__ sums, ComputeCfg cc) {
+  st += blockIdx.x;
+  sums += blockIdx.x * kOut;
   if (threadIdx.x != 0) return;
   const double bavg = (cc.n_face > 0.0) ? sums[0] / cc.n_face : 0.0;
-  *bavg_out = bavg;
+  st->bavg = bavg;
   double lam = 0.0;
   if (cc.mode == kFixedMass) {
     // <grad_b, rho> with grad_b the boundary-treated gradient
     const double face = cc.homogeneous ? bavg * sums[2] : sums[3];
-    lam = (sums[1] + face) / cc.target_mass;
+    lam = (sums[1] + face) / st->target_mass;
   } else if (cc.mode == kSaddle) {
-    const double m_t = cc.target_mass - cc.boundary_mass;
+    const double m_t = st->target_mass - cc.boundary_mass;
     lam = sums[1];
     if (m_t > 0.0) lam /= m_t;
   }
@@ -261,9 +294,11 @@ __global__ void k_post_control(FireDevState* st, const double* __restrict__ sums
 // Boundary treatment, Lagrange term and chain rule: f = -grad * drho/dx
 // (saddle: the projection follows).  sums [|f|^2, dir . f_alias].
 __global__ void k_post_apply(Vec a, const FireDevState* __restrict__ st, ComputeCfg cc,
-                             const double* __restrict__ bavg_p, double* __restrict__ partials) {
+                             double* __restrict__ partials) {
+  a = slice(a);
+  st += blockIdx.y;
   double s[kRedTerms] = {0, 0, 0, 0};
-  const double bavg = *bavg_p;
+  const double bavg = st->bavg;
   const double lam = st->lambda;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
     double g = a.grad[i];
@@ -288,6 +323,8 @@ __global__ void k_post_apply(Vec a, const FireDevState* __restrict__ st, Compute
 
 // saddle_point.hpp:490-492: f_alias -= (dir . f_alias) dir; f = -f_alias.
 __global__ void k_project(Vec a, const double* __restrict__ sums_in, double* __restrict__ partials) {
+  a = slice(a);
+  sums_in += blockIdx.y * kOut;
   double s[kRedTerms] = {0, 0, 0, 0};
   const double proj = sums_in[1];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
@@ -301,12 +338,14 @@ __global__ void k_project(Vec a, const double* __restrict__ sums_in, double* __r
 // fire.hpp:150-162 and minimization.hpp:431-434: energy, rms force, the
 // convergence monitor and the iteration counter.
 __global__ void k_fire_finalize(FireDevState* st, const double* __restrict__ sums, const double* __restrict__ scal,
-                                FireAux* aux, FireParams fp, double n_dof, double volume, int use_monitor,
-                                int initial) {
+                                FireParams fp, double n_dof, double volume, int use_monitor, int initial) {
+  st += blockIdx.x;
+  sums += blockIdx.x * kOut;
+  scal += blockIdx.x * kScalarCount;
   if (threadIdx.x != 0) return;
   if (!initial && !st->active) return;
   const double f2 = sums[0];
-  aux->f2 = f2;
+  st->f2 = f2;
   const double old_e = st->energy;
   st->energy = scal[1];
   st->free_energy = scal[0];
@@ -551,22 +590,26 @@ void smallest_eigvec(int n, double A[3][3], double* vec, double* val) {
 Drivers::Drivers(Engine& engine) : eng_(engine) {
   if (engine.species() != 1) throw Error(-1, "drivers: the minimiser, DDFT and saddle drivers are single-species");
   N_ = engine.points();
+  B_ = engine.batch();
+  const size_t BN = (size_t)B_ * N_;
   auto al = [&](double** p, size_t n) { CDFT_CUDA(cudaMalloc(p, sizeof(double) * n)); };
-  al(&x_, N_);
-  al(&v_, N_);
-  al(&f_, N_);
-  al(&grad_, N_);
+  al(&x_, BN);
+  al(&v_, BN);
+  al(&f_, BN);
+  al(&grad_, BN);
   al(&tmp_, N_);
   al(&tmp2_, N_);
-  al(&scalars_, kScalarCount);
+  al(&scalars_, (size_t)B_ * kScalarCount);
   int sms = 0, dev = 0;
   CDFT_CUDA(cudaGetDevice(&dev));
   CDFT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  grid_ = (int)std::max<long long>(1, std::min<long long>((long long)sms * 8, (N_ + kBlock - 1) / kBlock));
-  al(&red_, (size_t)grid_ * kRedTerms + 64);
-  al(&red_out_, 64);
-  CDFT_CUDA(cudaMalloc(&st_, sizeof(FireDevState)));
-  CDFT_CUDA(cudaMallocHost(&st_host_, sizeof(FireDevState)));
+  // about 8 CTAs per SM in total, shared by the B problems
+  const long long all = std::max<long long>(1, std::min<long long>((long long)sms * 8, ((long long)BN + kBlock - 1) / kBlock));
+  grid_ = (int)std::max<long long>(1, (all + B_ - 1) / B_);
+  al(&red_, (size_t)B_ * grid_ * kRedTerms + 64);
+  al(&red_out_, std::max<size_t>(64, (size_t)B_ * kOut));
+  CDFT_CUDA(cudaMalloc(&st_, sizeof(FireDevState) * B_));
+  CDFT_CUDA(cudaMallocHost(&st_host_, sizeof(FireDevState) * B_));
   CDFT_CUDA(cudaMallocHost(&host_pin_, sizeof(double) * 64));
 }
 
@@ -625,9 +668,37 @@ void Drivers::hvp_exact(const double* rho, const double* v, double* hv, double m
 
 FireResult Drivers::fire_minimize(const FireConfig& cfg, double* rho, const double* direction, cudaStream_t stream,
                                   Engine* refine, double refine_switch) {
-  const EvalParams& p = eng_.params();
+  if (B_ != 1) throw Error(-1, "fire_minimize: needs an engine with batch 1");
   if (cfg.mode == kSaddle && !direction) throw Error(-1, "fire_minimize: saddle mode needs a direction");
   if (cfg.mode == kFixedMass && !(cfg.target_mass > 0.0)) throw Error(-1, "fire_minimize: target mass must be > 0");
+  return fire_run(cfg, &cfg.mu, &cfg.target_mass, rho, direction, stream, refine, refine_switch)[0];
+}
+
+std::vector<FireResult> Drivers::fire_minimize_batch(const FireConfig& cfg, const double* mu, const double* mass,
+                                                     double* rho, cudaStream_t stream, Engine* refine,
+                                                     double refine_switch) {
+  if (cfg.mode == kSaddle) throw Error(-1, "fire_minimize_batch: the saddle mode is single-problem");
+  if (!mu) throw Error(-1, "fire_minimize_batch: mu is required");
+  std::vector<double> m(B_, 0.0);
+  if (cfg.mode == kFixedMass) {
+    if (!mass) throw Error(-1, "fire_minimize_batch: fixed mass needs a target mass per problem");
+    for (int b = 0; b < B_; ++b) {
+      if (!(mass[b] > 0.0)) throw Error(-1, "fire_minimize_batch: target masses must be > 0");
+      m[b] = mass[b];
+    }
+  }
+  if (refine && refine->batch() != B_) throw Error(-1, "fire_minimize_batch: the refine engine needs the same batch");
+  return fire_run(cfg, mu, m.data(), rho, nullptr, stream, refine, refine_switch);
+}
+
+// FIRE2 for the B problems of the engine: each step is a fixed sequence of
+// launches over all problems; every control decision is taken per problem
+// on the device (fire.hpp:86-165, minimization.hpp:182-354).
+std::vector<FireResult> Drivers::fire_run(const FireConfig& cfg, const double* mu, const double* mass, double* rho,
+                                          const double* direction, cudaStream_t stream, Engine* refine,
+                                          double refine_switch) {
+  const EvalParams& p = eng_.params();
+  const int B = B_;
   Vec a;
   a.x = x_;
   a.v = v_;
@@ -646,94 +717,113 @@ FireResult Drivers::fire_minimize(const FireConfig& cfg, double* rho, const doub
   ComputeCfg cc;
   cc.mode = cfg.mode;
   cc.homogeneous = cfg.homogeneous_boundary ? 1 : 0;
-  cc.target_mass = cfg.target_mass;
   cc.boundary_mass = cfg.boundary_mass;
   const long long inner = (long long)std::max(p.nx - 2, 0) * std::max(p.ny - 2, 0) * std::max(p.nz - 2, 0);
   cc.n_face = (double)(N_ - inner);
   const double volume = (double)N_ * p.dv;
   // Minimizer::fixed_mass computes with mu = 0 (minimization.hpp:388); the
   // other modes with the given chemical potential.
-  const double mu_compute = (cfg.mode == kFixedMass) ? 0.0 : cfg.mu;
-  double* bavg = red_out_ + 16;
-  FireAux* aux = reinterpret_cast<FireAux*>(red_out_ + 20);
+  std::vector<double> mu_compute(B), mu_final(B);
+  for (int b = 0; b < B; ++b) {
+    mu_final[b] = mu[b];
+    mu_compute[b] = (cfg.mode == kFixedMass) ? 0.0 : mu[b];
+  }
   const FireParams& fp = cfg.fire;
   const int use_monitor = cfg.use_monitor ? 1 : 0;
+  const dim3 gv(grid_, B);
+  const int rt = 32 * kRedTerms;
 
   Engine* eng = &eng_;
   auto compute = [&](int initial) {
     // rescale (fixed mass / saddle), evaluate, post-process into f
-    k_density_sums<<<grid_, kBlock, 0, stream>>>(a, red_);
-    k_finish_sums<<<1, 32 * kRedTerms, 0, stream>>>(red_, grid_, red_out_);
-    k_scale_factor<<<1, 32, 0, stream>>>(st_, red_out_, cc, p.dv, initial);
-    k_rescale<<<grid_, kBlock, 0, stream>>>(a, st_, cc, initial);
-    eng->evaluate(rho, nullptr, &mu_compute, grad_, scalars_, stream);
-    k_post_sums<<<grid_, kBlock, 0, stream>>>(a, red_);
-    k_finish_sums<<<1, 32 * kRedTerms, 0, stream>>>(red_, grid_, red_out_);
-    k_post_control<<<1, 32, 0, stream>>>(st_, red_out_, cc, bavg);
-    k_post_apply<<<grid_, kBlock, 0, stream>>>(a, st_, cc, bavg, red_);
-    k_finish_sums<<<1, 32 * kRedTerms, 0, stream>>>(red_, grid_, red_out_ + 4);
+    k_density_sums<<<gv, kBlock, 0, stream>>>(a, red_);
+    k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
+    k_scale_factor<<<B, 32, 0, stream>>>(st_, red_out_, cc, p.dv, initial);
+    k_rescale<<<gv, kBlock, 0, stream>>>(a, st_, cc, initial);
+    eng->evaluate(rho, nullptr, mu_compute.data(), grad_, scalars_, stream);
+    k_post_sums<<<gv, kBlock, 0, stream>>>(a, red_);
+    k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
+    k_post_control<<<B, 32, 0, stream>>>(st_, red_out_, cc);
+    k_post_apply<<<gv, kBlock, 0, stream>>>(a, st_, cc, red_);
+    k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_ + 4);
     if (cfg.mode == kSaddle) {
-      k_project<<<grid_, kBlock, 0, stream>>>(a, red_out_ + 4, red_);
-      k_finish_sums<<<1, 32 * kRedTerms, 0, stream>>>(red_, grid_, red_out_ + 4);
+      k_project<<<gv, kBlock, 0, stream>>>(a, red_out_ + 4, red_);
+      k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_ + 4);
     }
-    k_fire_finalize<<<1, 32, 0, stream>>>(st_, red_out_ + 4, scalars_, aux, fp, (double)N_, volume, use_monitor,
-                                          initial);
+    k_fire_finalize<<<B, 32, 0, stream>>>(st_, red_out_ + 4, scalars_, fp, (double)N_, volume, use_monitor, initial);
   };
 
   // initialise (fire.hpp:60-84)
-  FireDevState s0;
-  std::memset(&s0, 0, sizeof(s0));
-  s0.dt = fp.dt;
-  s0.alpha = fp.alpha_start;
-  s0.vv = 1.0;
-  s0.scale = 1.0;
-  s0.active = 1;
-  CDFT_CUDA(cudaMemcpyAsync(st_, &s0, sizeof(s0), cudaMemcpyHostToDevice, stream));
-  k_from_density<<<grid_, kBlock, 0, stream>>>(a, rho);
+  for (int b = 0; b < B; ++b) {
+    FireDevState& s0 = st_host_[b];
+    std::memset(&s0, 0, sizeof(s0));
+    s0.dt = fp.dt;
+    s0.alpha = fp.alpha_start;
+    s0.vv = 1.0;
+    s0.scale = 1.0;
+    s0.active = 1;
+    s0.target_mass = mass[b];
+  }
+  CDFT_CUDA(cudaMemcpyAsync(st_, st_host_, sizeof(FireDevState) * B, cudaMemcpyHostToDevice, stream));
+  k_from_density<<<gv, kBlock, 0, stream>>>(a, rho);
   compute(1);
   CDFT_CUDA(cudaGetLastError());
 
   bool refining = false;
   int steps = 0;
   for (;;) {
-    CDFT_CUDA(cudaMemcpyAsync(st_host_, st_, sizeof(FireDevState), cudaMemcpyDeviceToHost, stream));
+    CDFT_CUDA(cudaMemcpyAsync(st_host_, st_, sizeof(FireDevState) * B, cudaMemcpyDeviceToHost, stream));
     CDFT_CUDA(cudaStreamSynchronize(stream));
-    if (!st_host_->active || steps >= fp.max_steps) break;
-    if (refine && !refining && cfg.use_monitor && st_host_->iteration > 0 &&
-        st_host_->monitor < refine_switch * fp.force_tolerance) {
+    bool any_active = false, all_close = true;
+    for (int b = 0; b < B; ++b) {
+      const FireDevState& h = st_host_[b];
+      if (!h.active) continue;
+      any_active = true;
+      if (!(h.iteration > 0 && h.monitor < refine_switch * fp.force_tolerance)) all_close = false;
+    }
+    if (!any_active || steps >= fp.max_steps) break;
+    if (refine && !refining && cfg.use_monitor && all_close) {
       eng = refine;  // FP64 defect correction from here on
       refining = true;
     }
     const int chunk = std::max(1, std::min(cfg.check_interval, fp.max_steps - steps));
     for (int k = 0; k < chunk; ++k) {
-      k_power<<<grid_, kBlock, 0, stream>>>(a, red_);
-      k_finish_sums<<<1, 32 * kRedTerms, 0, stream>>>(red_, grid_, red_out_);
-      k_fire_control1<<<1, 32, 0, stream>>>(st_, red_out_, fp);
-      k_fire_vstep<<<grid_, kBlock, 0, stream>>>(a, st_, red_);
-      k_finish_sums<<<1, 32 * kRedTerms, 0, stream>>>(red_, grid_, red_out_);
-      k_fire_ratio<<<1, 32, 0, stream>>>(st_, red_out_, aux);
-      k_fire_xstep<<<grid_, kBlock, 0, stream>>>(a, st_);
+      k_power<<<gv, kBlock, 0, stream>>>(a, red_);
+      k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
+      k_fire_control1<<<B, 32, 0, stream>>>(st_, red_out_, fp);
+      k_fire_vstep<<<gv, kBlock, 0, stream>>>(a, st_, red_);
+      k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
+      k_fire_ratio<<<B, 32, 0, stream>>>(st_, red_out_);
+      k_fire_xstep<<<gv, kBlock, 0, stream>>>(a, st_);
       compute(0);
     }
     CDFT_CUDA(cudaGetLastError());
     steps += chunk;
   }
-  FireResult r;
-  r.iterations = st_host_->iteration;
-  r.converged = st_host_->converged != 0;
-  r.rms_force = st_host_->rms_force;
-  r.uphill_error = st_host_->uphill_error != 0;
-  if (r.uphill_error) return r;
+  std::vector<FireResult> out(B);
+  bool any_uphill = false;
+  for (int b = 0; b < B; ++b) {
+    FireResult& r = out[b];
+    r.iterations = st_host_[b].iteration;
+    r.converged = st_host_[b].converged != 0;
+    r.rms_force = st_host_[b].rms_force;
+    r.uphill_error = st_host_[b].uphill_error != 0;
+    any_uphill = any_uphill || r.uphill_error;
+  }
+  if (B == 1 && any_uphill) return out;
   // Final density (minimization.hpp:441-450, saddle_point.hpp:533-549): rho
   // already holds rho(x) with the mass rescale of the last compute, which is
   // exactly the reference's extraction from the final x.  The final total()
   // uses the caller's chemical potential (fixed mass iterates with mu = 0).
-  eng->evaluate(rho, nullptr, &cfg.mu, grad_, scalars_, stream);
-  CDFT_CUDA(cudaMemcpyAsync(host_pin_, scalars_, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+  eng->evaluate(rho, nullptr, mu_final.data(), grad_, scalars_, stream);
+  std::vector<double> sc((size_t)B * kScalarCount);
+  CDFT_CUDA(cudaMemcpyAsync(sc.data(), scalars_, sizeof(double) * sc.size(), cudaMemcpyDeviceToHost, stream));
   CDFT_CUDA(cudaStreamSynchronize(stream));
-  r.free_energy = host_pin_[0];
-  r.grand_potential = host_pin_[1];
-  return r;
+  for (int b = 0; b < B; ++b) {
+    out[b].free_energy = sc[(size_t)b * kScalarCount + 0];
+    out[b].grand_potential = sc[(size_t)b * kScalarCount + 1];
+  }
+  return out;
 }
 
 void Drivers::ensure_ddft() {

@@ -30,7 +30,8 @@ struct FireParams {
 enum FireMode : int { kGrandPotential = 0, kFixedMass = 1, kSaddle = 2 };
 enum ParamKind : int { kUnbounded = 0, kBounded = 1 };
 
-// Device-side FIRE2 state (fire.hpp:15-26 plus the minimiser's monitor).
+// Device-side FIRE2 state of one problem (fire.hpp:15-26 plus the
+// minimiser's monitor); a batched engine keeps one per problem.
 struct FireDevState {
   double dt, alpha;
   int n_positive, n_negative, iteration, converged;
@@ -43,6 +44,9 @@ struct FireDevState {
   double scale;    // density rescale of the fixed-mass / saddle compute
   double lambda;   // Lagrange multiplier of the fixed-mass / saddle compute
   double free_energy;
+  double target_mass;  // fixed mass / saddle target of this problem
+  double bavg;         // mean boundary force of the last compute
+  double f2;           // |f|^2 of the forces driving this step
 };
 
 struct FireConfig {
@@ -81,6 +85,17 @@ class Drivers {
   // `refine_switch` times the tolerance (mixed-precision defect correction).
   FireResult fire_minimize(const FireConfig& cfg, double* rho, const double* direction, cudaStream_t stream,
                            Engine* refine = nullptr, double refine_switch = 10.0);
+
+  // The same minimisation for every problem of a batched engine at once
+  // (grand potential or fixed mass; no saddle mode): problem b has chemical
+  // potential mu[b] and (fixed mass) target mass[b], host arrays of B values;
+  // rho holds B*N device doubles.  The FP64 `refine` engine (same batch)
+  // takes over once every active problem's monitor is below refine_switch
+  // times the tolerance.  Problems that converge stop changing while the
+  // others continue.  Uphill errors are reported per problem.
+  std::vector<FireResult> fire_minimize_batch(const FireConfig& cfg, const double* mu, const double* mass,
+                                              double* rho, cudaStream_t stream, Engine* refine = nullptr,
+                                              double refine_switch = 10.0);
 
   // DDFT integrating-factor step (dynamics.hpp:333-401) for one species;
   // returns the energy after the step and updates dt in place (dt/10 on
@@ -147,21 +162,26 @@ class Drivers {
   Engine& engine() { return eng_; }
 
  private:
+  std::vector<FireResult> fire_run(const FireConfig& cfg, const double* mu, const double* mass, double* rho,
+                                   const double* direction, cudaStream_t stream, Engine* refine,
+                                   double refine_switch);
+
   Engine& eng_;
   long long N_ = 0;
-  double* x_ = nullptr;       // FIRE parameters
-  double* v_ = nullptr;       // FIRE velocity
-  double* f_ = nullptr;       // FIRE force (parameter space)
-  double* grad_ = nullptr;    // functional force from the engine
+  int B_ = 1;                 // problems of the engine's batch
+  double* x_ = nullptr;       // FIRE parameters (B*N)
+  double* v_ = nullptr;       // FIRE velocity (B*N)
+  double* f_ = nullptr;       // FIRE force (parameter space, B*N)
+  double* grad_ = nullptr;    // functional force from the engine (B*N)
   double* tmp_ = nullptr;     // scratch vector (HVP, DDFT)
   double* tmp2_ = nullptr;
-  double* scalars_ = nullptr; // engine scalar block
-  double* red_ = nullptr;     // reduction partials
-  double* red_out_ = nullptr; // reduced values
-  FireDevState* st_ = nullptr;
-  FireDevState* st_host_ = nullptr;  // pinned
+  double* scalars_ = nullptr; // engine scalar blocks (B)
+  double* red_ = nullptr;     // reduction partials [B][grid_][4]
+  double* red_out_ = nullptr; // reduced values [B][8]
+  FireDevState* st_ = nullptr;       // [B]
+  FireDevState* st_host_ = nullptr;  // pinned [B]
   double* host_pin_ = nullptr;       // pinned scalars
-  int grid_ = 0;
+  int grid_ = 0;              // CTAs per problem of the vector kernels
   // DDFT
   void* ddft_k_ = nullptr;    // 3 * Nk complex (rho0_k, R0_k, R1_k / work)
   double* lam_ = nullptr;     // nx + ny + nzh Laplacian eigenvalues

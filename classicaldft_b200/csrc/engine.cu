@@ -74,6 +74,7 @@ Engine::Engine(const EngineSpec& spec) {
   if (spec.model < kRosenfeld || spec.model > kEsFMT) throw Error(-1, "Engine: unknown FMT model id");
   if ((int)spec.interactions.size() > kMaxInteractions) throw Error(-1, "Engine: too many interactions (max 8)");
   if (spec.precision != kFP64 && spec.precision != kMixed) throw Error(-1, "Engine: unknown precision mode");
+  if (spec.batch < 1 || spec.batch > kMaxBatch) throw Error(-1, "Engine: batch must be in [1, 64]");
   precision_ = spec.precision;
   CDFT_CUDA(cudaGetDevice(&device_));
 
@@ -117,6 +118,8 @@ Engine::Engine(const EngineSpec& spec) {
   }
   p.n_chan = ch;
   p.n_terms = 4 + S;
+  p.batch = spec.batch;
+  const int B = p.batch;
 
   int sms = 0;
   CDFT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
@@ -124,20 +127,24 @@ Engine::Engine(const EngineSpec& spec) {
   const size_t cs = mixed ? sizeof(float2) : sizeof(double2);
   const size_t rs = mixed ? sizeof(float) : sizeof(double);
   size_t tot = 0;
-  rho_k_ = dalloc<char>(cs * S * p.Nk, tot);
-  chan_k_ = dalloc<char>(cs * p.n_chan * p.Nk, tot);
-  chan_r_ = dalloc<char>(rs * p.n_chan * p.N, tot);
-  deriv_r_ = dalloc<char>(rs * p.L.n_deriv * p.N, tot);
-  deriv_k_ = dalloc<char>(cs * p.L.n_deriv * p.Nk, tot);
-  force_k_ = dalloc<char>(cs * S * p.Nk, tot);
-  hs_r_ = dalloc<char>(rs * S * p.N, tot);
-  if (mixed) rho_lo_ = dalloc<char>(sizeof(float) * S * p.N, tot);
+  rho_k_ = dalloc<char>(cs * B * S * p.Nk, tot);
+  chan_k_ = dalloc<char>(cs * B * p.n_chan * p.Nk, tot);
+  chan_r_ = dalloc<char>(rs * B * p.n_chan * p.N, tot);
+  deriv_r_ = dalloc<char>(rs * B * p.L.n_deriv * p.N, tot);
+  deriv_k_ = dalloc<char>(cs * B * p.L.n_deriv * p.Nk, tot);
+  force_k_ = dalloc<char>(cs * B * S * p.Nk, tot);
+  hs_r_ = dalloc<char>(rs * B * S * p.N, tot);
+  if (mixed) rho_lo_ = dalloc<char>(sizeof(float) * B * S * p.N, tot);
   mf_w_ = dalloc<double>((size_t)std::max(p.M, 1) * p.Nk, tot);
-  mean_ = dalloc<double>(kMaxSpecies, tot);
-  dbar_ = dalloc<double>(kMaxChannels, tot);
+  mean_ = dalloc<double>((size_t)B * kMaxSpecies, tot);
+  dbar_ = dalloc<double>((size_t)B * kMaxChannels, tot);
 
-  // grid sizes from occupancy (148 SMs on B200)
-  auto pick = [&](auto kern, long long work) { return occupancy_grid(kern, 256, sms, work); };
+  // grid sizes from occupancy (148 SMs on B200), shared by the B problems:
+  // about one wave of CTAs per launch in total
+  auto per_problem = [&](long long g) { return (int)std::max<long long>(1, (g + B - 1) / B); };
+  auto pick = [&](auto kern, long long work) {
+    return per_problem(occupancy_grid(kern, 256, sms, work * B));
+  };
   with_kernels(mixed, [&](auto model_c, auto multi_c, auto r_c) {
     constexpr int MD = decltype(model_c)::value;
     constexpr bool MU = decltype(multi_c)::value;
@@ -160,10 +167,10 @@ Engine::Engine(const EngineSpec& spec) {
     int per_sm = 0;
     CDFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pointwise_tma<MD, MU, RT>, kTmaTile,
                                                             tma_smem_v_));
-    grid_tma_ = sms * std::max(per_sm, 1);
+    grid_tma_ = per_problem((long long)sms * std::max(per_sm, 1));
   });
-  grid_stream_ = (int)std::max<long long>(1, std::min<long long>((long long)sms * 8, (p.N + 255) / 256));
-  partials_ = dalloc<double>((size_t)std::max(std::max(grid_pw_, grid_tma_), grid_stream_) * p.n_terms, tot);
+  grid_stream_ = per_problem(std::max<long long>(1, std::min<long long>((long long)sms * 8, (p.N * B + 255) / 256)));
+  partials_ = dalloc<double>((size_t)B * std::max(std::max(grid_pw_, grid_tma_), grid_stream_) * p.n_terms, tot);
   err_ = dalloc<int>(1, tot);
   CDFT_CUDA(cudaMemset(err_, 0, sizeof(int)));
 
@@ -171,10 +178,10 @@ Engine::Engine(const EngineSpec& spec) {
   upload_mean_field(spec);
   scratch_bytes_ = tot;
 
-  CDFT_CUDA(cudaMalloc(&h_rho_, sizeof(double) * S * p.N));
-  CDFT_CUDA(cudaMalloc(&h_vext_, sizeof(double) * S * p.N));
-  CDFT_CUDA(cudaMalloc(&h_force_, sizeof(double) * S * p.N));
-  CDFT_CUDA(cudaMalloc(&h_scalars_, sizeof(double) * kScalarCount));
+  CDFT_CUDA(cudaMalloc(&h_rho_, sizeof(double) * B * S * p.N));
+  CDFT_CUDA(cudaMalloc(&h_vext_, sizeof(double) * B * S * p.N));
+  CDFT_CUDA(cudaMalloc(&h_force_, sizeof(double) * B * S * p.N));
+  CDFT_CUDA(cudaMalloc(&h_scalars_, sizeof(double) * B * kScalarCount));
   CDFT_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
 }
 
@@ -199,7 +206,7 @@ void Engine::build_plans() {
   long long n[3] = {p.nx, p.ny, p.nz};
   size_t ws[4] = {0, 0, 0, 0};
   cufftHandle* hs[4] = {&plan_rho_, &plan_chan_, &plan_deriv_, &plan_force_};
-  const int batch[4] = {p.S, p.n_chan, p.L.n_deriv, p.S};
+  const int batch[4] = {p.batch * p.S, p.batch * p.n_chan, p.batch * p.L.n_deriv, p.batch * p.S};
   const cufftType fwd = mixed ? CUFFT_R2C : CUFFT_D2Z;
   const cufftType inv = mixed ? CUFFT_C2R : CUFFT_Z2D;
   const cufftType type[4] = {fwd, inv, fwd, inv};
@@ -261,18 +268,20 @@ void Engine::forward_stage(const double* in, R* chan_out, double* mean_out, cuda
   C2* rho_k = static_cast<C2*>(rho_k_);
   C2* chan_k = static_cast<C2*>(chan_k_);
   if constexpr (mixed) {
-    k_species_sums<<<grid_stream_, 256, 0, stream>>>(in, p.N, p.S, partials_);
-    k_split_convert<<<grid_stream_, 256, 0, stream>>>(in, p.N, p.S, partials_, grid_stream_,
-                                                      static_cast<float*>(rho_lo_), mean_out);
+    const dim3 gs(grid_stream_, p.batch);
+    k_species_sums<<<gs, 256, 0, stream>>>(in, p.N, p.S, partials_);
+    k_split_convert<<<gs, 256, 0, stream>>>(in, p.N, p.S, partials_, grid_stream_, static_cast<float*>(rho_lo_),
+                                            mean_out);
     CDFT_CUFFT(cufftExecR2C(plan_rho_, static_cast<float*>(rho_lo_), reinterpret_cast<cufftComplex*>(rho_k)));
   } else {
     CDFT_CUFFT(cufftExecD2Z(plan_rho_, const_cast<double*>(in), reinterpret_cast<cufftDoubleComplex*>(rho_k)));
   }
   const bool multi = p.L.multi, tensor = p.L.tensor;
-  if (!multi && !tensor) k_forward<false, false, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
-  if (!multi && tensor) k_forward<false, true, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
-  if (multi && !tensor) k_forward<true, false, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
-  if (multi && tensor) k_forward<true, true, C2><<<grid_k_, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
+  const dim3 gk(grid_k_, p.batch);
+  if (!multi && !tensor) k_forward<false, false, C2><<<gk, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
+  if (!multi && tensor) k_forward<false, true, C2><<<gk, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
+  if (multi && !tensor) k_forward<true, false, C2><<<gk, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
+  if (multi && tensor) k_forward<true, true, C2><<<gk, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
   CDFT_CUDA(cudaGetLastError());
   if constexpr (mixed)
     CDFT_CUFFT(cufftExecC2R(plan_chan_, reinterpret_cast<cufftComplex*>(chan_k), reinterpret_cast<float*>(chan_out)));
@@ -281,10 +290,10 @@ void Engine::forward_stage(const double* in, R* chan_out, double* mean_out, cuda
                             reinterpret_cast<double*>(chan_out)));
 }
 
-// Stages 5-7: out += c2r(sum_c conj(W_c) r2c(deriv_c)) dV (+ the FP64
-// constants of the split derivative channels, `dbar`).
+// Stages 5-7: out += c2r(sum_c conj(W_c) r2c(deriv_c)) dV - mu dV (+ the
+// FP64 constants of the split derivative channels, `dbar`).
 template <typename R, typename C2>
-void Engine::backward_stage(R* deriv, const double* dbar, double* out, cudaStream_t stream) {
+void Engine::backward_stage(R* deriv, const double* dbar, double* out, const MuArgs& mu, cudaStream_t stream) {
   const EvalParams& p = p_;
   constexpr bool mixed = sizeof(R) == sizeof(float);
   C2* deriv_k = static_cast<C2*>(deriv_k_);
@@ -296,20 +305,21 @@ void Engine::backward_stage(R* deriv, const double* dbar, double* out, cudaStrea
     CDFT_CUFFT(cufftExecD2Z(plan_deriv_, reinterpret_cast<double*>(deriv),
                             reinterpret_cast<cufftDoubleComplex*>(deriv_k)));
   const bool multi = p.L.multi, tensor = p.L.tensor;
-  if (!multi && !tensor) k_backward<false, false, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
-  if (!multi && tensor) k_backward<false, true, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
-  if (multi && !tensor) k_backward<true, false, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
-  if (multi && tensor) k_backward<true, true, C2><<<grid_k_, 256, 0, stream>>>(p, deriv_k, force_k);
+  const dim3 gk(grid_k_, p.batch), gs(grid_stream_, p.batch);
+  if (!multi && !tensor) k_backward<false, false, C2><<<gk, 256, 0, stream>>>(p, deriv_k, force_k);
+  if (!multi && tensor) k_backward<false, true, C2><<<gk, 256, 0, stream>>>(p, deriv_k, force_k);
+  if (multi && !tensor) k_backward<true, false, C2><<<gk, 256, 0, stream>>>(p, deriv_k, force_k);
+  if (multi && tensor) k_backward<true, true, C2><<<gk, 256, 0, stream>>>(p, deriv_k, force_k);
   CDFT_CUDA(cudaGetLastError());
   if constexpr (mixed)
     CDFT_CUFFT(cufftExecC2R(plan_force_, reinterpret_cast<cufftComplex*>(force_k), reinterpret_cast<float*>(hs_r)));
   else
     CDFT_CUFFT(cufftExecZ2D(plan_force_, reinterpret_cast<cufftDoubleComplex*>(force_k),
                             reinterpret_cast<double*>(hs_r)));
-  if (!multi && !tensor) k_epilogue<false, false, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar, out);
-  if (!multi && tensor) k_epilogue<false, true, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar, out);
-  if (multi && !tensor) k_epilogue<true, false, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar, out);
-  if (multi && tensor) k_epilogue<true, true, R><<<grid_stream_, 256, 0, stream>>>(p, hs_r, dbar, out);
+  if (!multi && !tensor) k_epilogue<false, false, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu);
+  if (!multi && tensor) k_epilogue<false, true, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu);
+  if (multi && !tensor) k_epilogue<true, false, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu);
+  if (multi && tensor) k_epilogue<true, true, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu);
   CDFT_CUDA(cudaGetLastError());
 }
 
@@ -324,7 +334,7 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
 
   // cuFFT needs 16-byte aligned FP64 input: stage a misaligned rho
   if (!mixed && ((uintptr_t)rho % 16 != 0)) {
-    CDFT_CUDA(cudaMemcpyAsync(h_rho_, rho, sizeof(double) * p.S * p.N, cudaMemcpyDeviceToDevice, stream));
+    CDFT_CUDA(cudaMemcpyAsync(h_rho_, rho, sizeof(double) * p.batch * p.S * p.N, cudaMemcpyDeviceToDevice, stream));
     rho = h_rho_;
   }
   // 1-3. weighted densities
@@ -333,7 +343,6 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   PointwiseArgs a;
   a.rho = rho;
   a.vext = vext;
-  for (int s = 0; s < kMaxSpecies; ++s) a.mu[s] = s < p.S ? mu[s] : 0.0;
   a.force = force;
   a.partials = partials_;
   a.mf_w = mf_w_;
@@ -343,25 +352,27 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   // aligned base pointers); otherwise the register-prefetch variant.
   const bool tma = (p.N % 4 == 0) && ((uintptr_t)rho % 16 == 0) && ((uintptr_t)vext % 16 == 0);
   const int pw_blocks = tma ? grid_tma_ : grid_pw_;
+  const dim3 gt(grid_tma_, p.batch), gp(grid_pw_, p.batch);
   with_kernels(mixed, [&](auto model_c, auto multi_c, auto r_c) {
     constexpr int MD = decltype(model_c)::value;
     constexpr bool MU = decltype(multi_c)::value;
     using RT = typename decltype(r_c)::type;
     if constexpr (std::is_same_v<RT, R>) {
       if (tma)
-        k_pointwise_tma<MD, MU, RT><<<grid_tma_, kTmaTile, vext ? tma_smem_v_ : tma_smem_, stream>>>(
-            p, chan_r, deriv_r, a, err_);
+        k_pointwise_tma<MD, MU, RT><<<gt, kTmaTile, vext ? tma_smem_v_ : tma_smem_, stream>>>(p, chan_r, deriv_r,
+                                                                                             a, err_);
       else
-        k_pointwise<MD, MU, RT><<<grid_pw_, 256, 0, stream>>>(p, chan_r, deriv_r, a);
+        k_pointwise<MD, MU, RT><<<gp, 256, 0, stream>>>(p, chan_r, deriv_r, a);
     }
   });
   CDFT_CUDA(cudaGetLastError());
   // 5-7. back-convolution into the force
-  backward_stage<R, C2>(deriv_r, dbar_, force, stream);
-  // 8. scalars
   MuArgs ma;
-  for (int s = 0; s < kMaxSpecies; ++s) ma.mu[s] = a.mu[s];
-  k_reduce_final<<<1, 32 * (4 + kMaxSpecies), 0, stream>>>(partials_, pw_blocks, p, ma, err_, scalars);
+  for (int b = 0; b < kMaxBatch; ++b)
+    for (int s = 0; s < kMaxSpecies; ++s) ma.mu[b][s] = (b < p.batch && s < p.S) ? mu[b * p.S + s] : 0.0;
+  backward_stage<R, C2>(deriv_r, dbar_, force, ma, stream);
+  // 8. scalars, one block per problem
+  k_reduce_final<<<p.batch, 32 * (4 + kMaxSpecies), 0, stream>>>(partials_, pw_blocks, p, ma, err_, scalars);
   CDFT_CUDA(cudaGetLastError());
 }
 
@@ -374,6 +385,7 @@ template <typename R, typename C2>
 void Engine::run_hvp(const double* rho, const double* v, const double* mu, double* hv, cudaStream_t stream) {
   const EvalParams& p = p_;
   constexpr bool mixed = sizeof(R) == sizeof(float);
+  if (p.batch != 1) throw Error(-1, "hvp: needs an engine with batch 1");
   for (cufftHandle h : {plan_rho_, plan_chan_, plan_deriv_, plan_force_}) CDFT_CUFFT(cufftSetStream(h, stream));
   if (!tan_chan_) {
     const size_t rs = mixed ? sizeof(float) : sizeof(double);
@@ -407,7 +419,8 @@ void Engine::run_hvp(const double* rho, const double* v, const double* mu, doubl
       k_pointwise_hvp<MD, MU, RT><<<grid_stream_, 128, 0, stream>>>(p, chan_r, chan_t, deriv_r, a);
   });
   CDFT_CUDA(cudaGetLastError());
-  backward_stage<R, C2>(deriv_r, tan_dbar_, hv, stream);
+  MuArgs zero{};  // the Hessian does not depend on mu
+  backward_stage<R, C2>(deriv_r, tan_dbar_, hv, zero, stream);
   (void)mu;
 }
 

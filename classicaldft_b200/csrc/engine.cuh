@@ -32,6 +32,7 @@ struct EngineSpec {
   double esfmt_A = 1.0, esfmt_B = 0.0;
   std::vector<InteractionSpec> interactions;
   int precision = kFP64;
+  int batch = 1;  // problems of this shape evaluated together (1..kMaxBatch)
 };
 
 class Engine {
@@ -41,21 +42,23 @@ class Engine {
   Engine(const Engine&) = delete;
   Engine& operator=(const Engine&) = delete;
 
-  // Full evaluation on device data (functionals.hpp:64-95).
-  //   rho   : S*N doubles (device), species-major
-  //   vext  : S*N doubles (device) or null (no external field)
-  //   mu    : S chemical potentials (beta mu units), host
-  //   force : S*N doubles (device) receives dOmega/drho * dV, or null
-  //   scalars: kScalarCount doubles (device): F, Omega, F_id, F_ext, F_hs, F_mf, N_s
+  // Full evaluation on device data (functionals.hpp:64-95).  A batched
+  // engine evaluates B problems: every array holds B problems back to back.
+  //   rho   : B*S*N doubles (device), problem-major then species-major
+  //   vext  : B*S*N doubles (device) or null (no external field)
+  //   mu    : B*S chemical potentials (beta mu units), host
+  //   force : B*S*N doubles (device) receives dOmega/drho * dV
+  //   scalars: B*kScalarCount doubles (device): F, Omega, F_id, F_ext, F_hs, F_mf, N_s
   void evaluate(const double* rho, const double* vext, const double* mu, double* force, double* scalars,
                 cudaStream_t stream);
 
   // Hessian-vector product of Omega: hv = d(force)/d(rho) . v (S*N device
-  // doubles each); exact, by forward-over-reverse differentiation.
+  // doubles each); exact, by forward-over-reverse differentiation.  Batch 1 only.
   void hvp(const double* rho, const double* v, const double* mu, double* hv, cudaStream_t stream);
 
   const EvalParams& params() const { return p_; }
   int species() const { return p_.S; }
+  int batch() const { return p_.batch; }
   long long points() const { return p_.N; }
   long long modes() const { return p_.Nk; }
   int precision() const { return precision_; }
@@ -86,7 +89,7 @@ class Engine {
   template <typename R, typename C2>
   void forward_stage(const double* in, R* chan_out, double* mean_out, cudaStream_t stream);
   template <typename R, typename C2>
-  void backward_stage(R* deriv, const double* dbar, double* out, cudaStream_t stream);
+  void backward_stage(R* deriv, const double* dbar, double* out, const MuArgs& mu, cudaStream_t stream);
 
   EvalParams p_{};
   int precision_ = kFP64;
@@ -95,17 +98,18 @@ class Engine {
   std::vector<double> a_vdw_;
 
   // FP64 pipeline buffers (the mixed pipeline views them as float storage).
-  void* rho_k_ = nullptr;     // S * Nk complex
-  void* chan_k_ = nullptr;    // C * Nk complex
-  void* chan_r_ = nullptr;    // C * N real
-  void* deriv_r_ = nullptr;   // D * N real
-  void* deriv_k_ = nullptr;   // D * Nk complex
-  void* force_k_ = nullptr;   // S * Nk complex
-  void* hs_r_ = nullptr;      // S * N real
-  void* rho_lo_ = nullptr;    // S * N float (mixed precision input copy)
-  double* mf_w_ = nullptr;    // M * Nk real (FP64)
-  double* mean_ = nullptr;    // S species means (mixed precision)
-  double* dbar_ = nullptr;    // derivative-channel constants (mixed precision)
+  // Every per-problem buffer holds B problems back to back.
+  void* rho_k_ = nullptr;     // B * S * Nk complex
+  void* chan_k_ = nullptr;    // B * C * Nk complex
+  void* chan_r_ = nullptr;    // B * C * N real
+  void* deriv_r_ = nullptr;   // B * D * N real
+  void* deriv_k_ = nullptr;   // B * D * Nk complex
+  void* force_k_ = nullptr;   // B * S * Nk complex
+  void* hs_r_ = nullptr;      // B * S * N real
+  void* rho_lo_ = nullptr;    // B * S * N float (mixed precision input copy)
+  double* mf_w_ = nullptr;    // M * Nk real (FP64), shared by the batch
+  double* mean_ = nullptr;    // B * kMaxSpecies species means (mixed precision)
+  double* dbar_ = nullptr;    // B * kMaxChannels derivative-channel constants (mixed precision)
   double* partials_ = nullptr;
   int* err_ = nullptr;        // device error word (set by bounded waits that gave up)
   void* tan_chan_ = nullptr;  // tangent channels of the exact HVP (allocated on first use)
@@ -114,6 +118,7 @@ class Engine {
   double* tan_in_ = nullptr;  // aligned copies of rho and v
   int grid_tma_ = 0;
   int grid_stream_ = 0;       // streaming kernels (sums, conversion, epilogue)
+  // grid_* are CTAs per problem: a launch has grid_* x B CTAs
   size_t tma_smem_ = 0, tma_smem_v_ = 0;
   void* fft_work_ = nullptr;
   size_t scratch_bytes_ = 0;

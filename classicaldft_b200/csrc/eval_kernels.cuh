@@ -28,6 +28,11 @@
 // c2r input is Hermitian and the result does not depend on how a library
 // treats non-Hermitian input.
 //
+// Batched engines.  B problems of one shape are stored back to back
+// ([B][channel][N] in real space, [B][channel][Nk] in k-space, so cuFFT
+// transforms all B x channels in one plan); every kernel takes its problem
+// index from blockIdx.y and offsets its pointers by it.
+//
 // Mixed precision (FP32 storage, R = float).  The FFTs see only fluctuations:
 // rho_s = c_s + delta_rho_s with c_s the exact FP64 mean, and each derivative
 // channel D_c = dbar_c + delta_D_c with dbar_c = dPhi/dn_c of the uniform
@@ -227,6 +232,8 @@ __global__ void __launch_bounds__(256) k_forward(EvalParams p, const C2* __restr
                                                  const double* __restrict__ mf_w, C2* __restrict__ chan) {
   using L = Lay<MULTI, TENSOR>;
   const long long Nk = p.Nk;
+  rho_k += (long long)blockIdx.y * p.S * Nk;
+  chan += (long long)blockIdx.y * p.n_chan * Nk;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < Nk;
        idx += (long long)gridDim.x * blockDim.x) {
     const KIndex q = decode_k(p, idx);
@@ -284,6 +291,8 @@ template <bool MULTI, bool TENSOR, typename C2>
 __global__ void __launch_bounds__(256) k_backward(EvalParams p, const C2* __restrict__ dk, C2* __restrict__ fk) {
   using L = Lay<MULTI, TENSOR>;
   const long long Nk = p.Nk;
+  dk += (long long)blockIdx.y * p.L.n_deriv * Nk;
+  fk += (long long)blockIdx.y * p.S * Nk;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < Nk;
        idx += (long long)gridDim.x * blockDim.x) {
     const KIndex q = decode_k(p, idx);
@@ -338,6 +347,8 @@ __device__ __forceinline__ double warp_sum_partials(const double* __restrict__ p
 // Mixed precision, step 1: per-block sums of each species' density.
 __global__ void __launch_bounds__(256) k_species_sums(const double* __restrict__ rho, long long N, int S,
                                                       double* __restrict__ partials) {
+  rho += (long long)blockIdx.y * S * N;
+  partials += (long long)blockIdx.y * gridDim.x * S;
   double acc[kMaxSpecies] = {0.0, 0.0, 0.0, 0.0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
 #pragma unroll
@@ -350,6 +361,10 @@ __global__ void __launch_bounds__(256) k_species_sums(const double* __restrict__
 __global__ void __launch_bounds__(256) k_split_convert(const double* __restrict__ rho, long long N, int S,
                                                        const double* __restrict__ partials, int nblocks,
                                                        float* __restrict__ out, double* __restrict__ mean_out) {
+  rho += (long long)blockIdx.y * S * N;
+  out += (long long)blockIdx.y * S * N;
+  partials += (long long)blockIdx.y * nblocks * S;
+  mean_out += blockIdx.y * kMaxSpecies;
   __shared__ double sm[kMaxSpecies];
   const int warp = threadIdx.x >> 5;
   if (warp < S) {
@@ -367,15 +382,26 @@ __global__ void __launch_bounds__(256) k_split_convert(const double* __restrict_
 // ------------------------------------------------------------ pointwise
 
 struct PointwiseArgs {
-  const double* rho;      // S*N
-  const double* vext;     // S*N or null
-  double mu[kMaxSpecies];
-  double* force;          // S*N: local terms written here
-  double* partials;       // gridDim.x * n_terms
+  const double* rho;      // B*S*N
+  const double* vext;     // B*S*N or null
+  double* force;          // B*S*N: local terms (without -mu dV) written here
+  double* partials;       // B * gridDim.x * n_terms
   const double* mf_w;     // M*Nk (k = 0 entries give the mean-field DC weights)
-  const double* mean;     // S species means (mixed precision) or null
-  double* dbar_out;       // derivative-channel constants (mixed precision) or null
+  const double* mean;     // B*kMaxSpecies species means (mixed precision) or null
+  double* dbar_out;       // B*kMaxChannels derivative-channel constants (mixed precision) or null
 };
+
+// The arguments of problem b of a batch.
+__device__ __forceinline__ PointwiseArgs batch_slice(const EvalParams& p, PointwiseArgs a, int b) {
+  const long long o = (long long)b * p.S * p.N;
+  a.rho += o;
+  if (a.vext) a.vext += o;
+  a.force += o;
+  a.partials += (long long)b * gridDim.x * p.n_terms;
+  if (a.mean) a.mean += b * kMaxSpecies;
+  if (a.dbar_out) a.dbar_out += b * kMaxChannels;
+  return a;
+}
 
 // Derivative-channel values at one point from dPhi (the folding of
 // hard_sphere.hpp:121,125,131 plus the T_zz trace folding).
@@ -517,7 +543,7 @@ __device__ __forceinline__ void point_body(const EvalParams& p, const PointwiseA
       acc[kTermId] += r * (lr - 1.0);
       acc[kTermExt] += r * v;
       acc[kTermN0 + s] += r;
-      f[s] = (lr - a.mu[s]) * p.dv + v * p.dv;
+      f[s] = lr * p.dv + v * p.dv;  // -mu dV is added by k_epilogue
     }
   }
   for (int q = 0; q < p.M; ++q) {
@@ -561,13 +587,16 @@ __device__ __forceinline__ void point_body(const EvalParams& p, const PointwiseA
 // working on the current one.
 template <int MODEL, bool MULTI, typename RT>
 __global__ void __launch_bounds__(256) k_pointwise(EvalParams p, const RT* __restrict__ chan, RT* __restrict__ deriv,
-                                                   PointwiseArgs a) {
+                                                   PointwiseArgs a_all) {
   constexpr bool TENSOR = model_has_tensor(MODEL);
   using L = Lay<MULTI, TENSOR>;
   constexpr bool SPLIT = sizeof(RT) == sizeof(float);
   constexpr int NT = 4 + kMaxSpecies;
   constexpr int NF = L::NFMT;
   constexpr int NPRE = NF + 2;
+  const PointwiseArgs a = batch_slice(p, a_all, blockIdx.y);
+  chan += (long long)blockIdx.y * p.n_chan * p.N;
+  deriv += (long long)blockIdx.y * p.L.n_deriv * p.N;
   __shared__ double s_off[kMaxChannels];
   __shared__ double s_dbar[NF];
   if (SPLIT) split_prologue<MODEL, MULTI>(p, a, s_off, s_dbar);
@@ -650,7 +679,8 @@ __host__ __device__ constexpr int tma_stage_bytes(int S, bool vext) {
 
 template <int MODEL, bool MULTI, typename RT>
 __global__ void __launch_bounds__(kTmaTile) k_pointwise_tma(EvalParams p, const RT* __restrict__ chan,
-                                                            RT* __restrict__ deriv, PointwiseArgs a, int* err) {
+                                                            RT* __restrict__ deriv, PointwiseArgs a_all,
+                                                            int* err) {
   constexpr bool TENSOR = model_has_tensor(MODEL);
   using L = Lay<MULTI, TENSOR>;
   constexpr bool SPLIT = sizeof(RT) == sizeof(float);
@@ -662,6 +692,9 @@ __global__ void __launch_bounds__(kTmaTile) k_pointwise_tma(EvalParams p, const 
   __shared__ double s_off[kMaxChannels];
   __shared__ double s_dbar[NF];
   __shared__ int s_fail;
+  const PointwiseArgs a = batch_slice(p, a_all, blockIdx.y);
+  chan += (long long)blockIdx.y * p.n_chan * p.N;
+  deriv += (long long)blockIdx.y * p.L.n_deriv * p.N;
   const bool has_v = a.vext != nullptr;
   const int S = p.S;
   const int n_mf_pre = (p.n_chan - NF) < 2 ? (p.n_chan - NF) : 2;
@@ -869,44 +902,45 @@ __global__ void __launch_bounds__(128) k_pointwise_hvp(EvalParams p, const RT* _
   }
 }
 
-// force_s += c2r(F_s) dV (+ the FP64 constant of the split derivative channels)
-// (hard_sphere.hpp:250-253)
+// force_s += c2r(F_s) dV - mu_s dV (+ the FP64 constant of the split
+// derivative channels) (hard_sphere.hpp:250-253, ideal_gas.hpp:33).
 template <bool MULTI, bool TENSOR, typename RT>
 __global__ void __launch_bounds__(256) k_epilogue(EvalParams p, const RT* __restrict__ hs, const double* __restrict__ dbar,
-                                                  double* __restrict__ force) {
+                                                  double* __restrict__ force, const __grid_constant__ MuArgs mu) {
   using L = Lay<MULTI, TENSOR>;
   constexpr bool SPLIT = sizeof(RT) == sizeof(float);
+  const int b = blockIdx.y;
+  const long long N = p.N;
+  hs += (long long)b * p.S * N;
+  force += (long long)b * p.S * N;
+  dbar += b * kMaxChannels;
   __shared__ double s_const[kMaxSpecies];
-  if (SPLIT) {
-    if (threadIdx.x < p.S) {
-      const int s = threadIdx.x;
-      double v = 0.0;
+  if (threadIdx.x < p.S) {
+    const int s = threadIdx.x;
+    double v = 0.0;
+    if (SPLIT) {
 #pragma unroll
       for (int c = 0; c < L::NFMT; ++c) v += chan_dc<MULTI, TENSOR>(c, s, p) * dbar[c];
-      s_const[s] = v * p.dv;
     }
-    __syncthreads();
+    s_const[s] = v * p.dv - mu.mu[b][s] * p.dv;
   }
-  const long long N = p.N;
+  __syncthreads();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
 #pragma unroll
     for (int s = 0; s < kMaxSpecies; ++s) {
-      if (s < p.S) {
-        double v = force[s * N + i] + (double)hs[s * N + i] * p.dv;
-        if (SPLIT) v += s_const[s];
-        force[s * N + i] = v;
-      }
+      if (s < p.S) force[s * N + i] = force[s * N + i] + (double)hs[s * N + i] * p.dv + s_const[s];
     }
 }
 
-// Deterministic second reduction stage; writes the scalar block
-// [F, Omega, F_id, F_ext, F_hs, F_mf, N_0 .. N_{S-1}] (functionals.hpp:72-92).
-struct MuArgs {
-  double mu[kMaxSpecies];
-};
-
-__global__ void k_reduce_final(const double* __restrict__ partials, int nblocks, EvalParams p, MuArgs mu,
-                               const int* __restrict__ err, double* __restrict__ out) {
+// Deterministic second reduction stage, one block per problem; writes the
+// scalar block [F, Omega, F_id, F_ext, F_hs, F_mf, N_0 .. N_{S-1}]
+// (functionals.hpp:72-92) of problem blockIdx.x.
+__global__ void k_reduce_final(const double* __restrict__ partials, int nblocks, EvalParams p,
+                               const __grid_constant__ MuArgs mu, const int* __restrict__ err,
+                               double* __restrict__ out) {
+  const int b = blockIdx.x;
+  partials += (long long)b * nblocks * p.n_terms;
+  out += b * kScalarCount;
   __shared__ double sh[4 + kMaxSpecies];
   const int warp = threadIdx.x >> 5;  // one warp per term
   const int n_terms = p.n_terms;
@@ -927,7 +961,7 @@ __global__ void k_reduce_final(const double* __restrict__ partials, int nblocks,
     F += f_hs;
     if (p.M > 0) F += f_mf;
     double muN = 0.0;
-    for (int s = 0; s < p.S; ++s) muN += mu.mu[s] * sh[kTermN0 + s] * dv;
+    for (int s = 0; s < p.S; ++s) muN += mu.mu[b][s] * sh[kTermN0 + s] * dv;
     const bool bad = err && *err != 0;  // a bounded wait gave up: poison the result
     out[0] = bad ? __longlong_as_double(0x7ff8000000000000ll) : F;
     out[1] = bad ? __longlong_as_double(0x7ff8000000000000ll) : F - muN;

@@ -209,9 +209,13 @@ def interaction_weight(inter: Interaction, grid: Grid, kT: float):
 
 
 class Engine:
-    """An evaluation engine on the current CUDA device (owns a cdft_engine)."""
+    """An evaluation engine on the current CUDA device (owns a cdft_engine).
 
-    def __init__(self, fmt_model: FMTModel, model: Model, precision: int = _lib.FP64):
+    ``batch`` > 1 builds a batched engine: every call evaluates ``batch``
+    problems of this model at once (arrays carry a leading batch axis).
+    """
+
+    def __init__(self, fmt_model: FMTModel, model: Model, precision: int = _lib.FP64, batch: int = 1):
         L = _lib.lib()
         g = model.grid
         diam = np.array([sp.hard_sphere_diameter for sp in model.species], dtype=np.float64)
@@ -224,15 +228,19 @@ class Engine:
             inters[m] = _lib.CInteraction(it.species_i, it.species_j, w.ctypes.data_as(_lib.c_double_p), a)
             self.a_vdw.append(a)
         h = ctypes.c_void_p()
-        _lib.check(L.cdft_create(ctypes.byref(h), _lib.c_long3(*g.shape), g.dx, len(model.species),
-                                 diam.ctypes.data_as(_lib.c_double_p), _lib.MODEL_IDS[fmt_model.name],
-                                 fmt_model.A, fmt_model.B, len(model.interactions), inters, precision))
+        _lib.check(L.cdft_create_batch(ctypes.byref(h), _lib.c_long3(*g.shape), g.dx, len(model.species),
+                                       diam.ctypes.data_as(_lib.c_double_p), _lib.MODEL_IDS[fmt_model.name],
+                                       fmt_model.A, fmt_model.B, len(model.interactions), inters, precision,
+                                       int(batch)))
         self._keep = []
         self.handle = h
         self.grid = g
         self.S = len(model.species)
         self.N = g.total_points
         self.precision = precision
+        b = ctypes.c_int()
+        _lib.check(L.cdft_engine_batch(h, ctypes.byref(b)))
+        self.batch = b.value
         info = (ctypes.c_longlong * 8)()
         _lib.check(L.cdft_engine_info(h, info))
         self.info = {"N": info[0], "Nk": info[1], "S": info[2], "channels": info[3], "deriv_channels": info[4],
@@ -250,12 +258,17 @@ class Engine:
             pass
 
     def total_host(self, rho: np.ndarray, mu, vext=None, want_force=True):
-        """cdft_total on host arrays: rho (S, N) -> (scalars[10], force (S, N) or None)."""
-        rho = np.ascontiguousarray(rho, dtype=np.float64).reshape(self.S, self.N)
-        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), (self.S,)))
-        v = None if vext is None else np.ascontiguousarray(vext, dtype=np.float64).reshape(self.S, self.N)
-        force = np.empty((self.S, self.N)) if want_force else None
-        sc = np.empty(_lib.SCALAR_COUNT)
+        """cdft_total on host arrays: rho (S, N) -> (scalars[10], force (S, N) or None).
+
+        A batched engine takes rho (B, S, N) and mu (B, S) (or broadcastable)
+        and returns scalars (B, 10) and force (B, S, N).
+        """
+        lead = (self.S,) if self.batch == 1 else (self.batch, self.S)
+        rho = np.ascontiguousarray(rho, dtype=np.float64).reshape(*lead, self.N)
+        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), lead))
+        v = None if vext is None else np.ascontiguousarray(vext, dtype=np.float64).reshape(*lead, self.N)
+        force = np.empty((*lead, self.N)) if want_force else None
+        sc = np.empty(_lib.SCALAR_COUNT if self.batch == 1 else (self.batch, _lib.SCALAR_COUNT))
         _lib.check(_lib.lib().cdft_total(self.handle, rho.ctypes.data, None if v is None else v.ctypes.data,
                                          mu.ctypes.data_as(_lib.c_double_p),
                                          None if force is None else force.ctypes.data,
@@ -264,7 +277,8 @@ class Engine:
 
     def total_device(self, rho_ptr: int, vext_ptr, mu, force_ptr: int, scalars_ptr: int, stream: int = 0):
         """cdft_total_device on device pointers (ints, e.g. torch.Tensor.data_ptr())."""
-        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), (self.S,)))
+        lead = (self.S,) if self.batch == 1 else (self.batch, self.S)
+        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), lead))
         _lib.check(_lib.lib().cdft_total_device(self.handle, rho_ptr, vext_ptr or None,
                                                 mu.ctypes.data_as(_lib.c_double_p), force_ptr, scalars_ptr,
                                                 stream or None))
@@ -282,9 +296,9 @@ class Weights:
         return list(self.engine.a_vdw)
 
 
-def make_weights(fmt_model: FMTModel, model: Model, precision: int = _lib.FP64) -> Weights:
-    """functionals.hpp:27-33."""
-    return Weights(fmt_model, Engine(fmt_model, model, precision))
+def make_weights(fmt_model: FMTModel, model: Model, precision: int = _lib.FP64, batch: int = 1) -> Weights:
+    """functionals.hpp:27-33 (``batch`` > 1: a batched engine, see ``total_batch``)."""
+    return Weights(fmt_model, Engine(fmt_model, model, precision, batch))
 
 
 @dataclass
@@ -318,6 +332,29 @@ def total(model: Model, rhos, weights: Weights, mus=None, vexts=None) -> Result:
              "N": [sc[6 + s] for s in range(S)]}
     return Result(free_energy=float(sc[0]), grand_potential=float(sc[1]), forces=[force[s] for s in range(S)],
                   parts=parts)
+
+
+def total_batch(model: Model, rhos, weights: Weights, mus=None, vexts=None) -> list:
+    """``total`` for every problem of a batched engine in one call.
+
+    ``rhos``: (B, S, N) (or (B, N) for one species); ``mus``: (B, S) or
+    broadcastable; ``vexts``: None or like ``rhos``.  Returns B Results.
+    """
+    e = weights.engine
+    S, N, B = len(model.species), model.grid.total_points, e.batch
+    rho = np.asarray(rhos, dtype=np.float64).reshape(B, S, N)
+    mus = np.zeros((B, S)) if mus is None else np.asarray(mus, dtype=np.float64)
+    if mus.ndim == 1 and S == 1 and mus.shape[0] == B:
+        mus = mus[:, None]  # one beta*mu per problem
+    v = None if vexts is None else np.asarray(vexts, dtype=np.float64).reshape(B, S, N)
+    sc, force = e.total_host(rho, np.broadcast_to(mus, (B, S)), v)
+    out = []
+    for b in range(B):
+        parts = {"ideal": sc[b, 2], "external": sc[b, 3], "hard_sphere": sc[b, 4], "mean_field": sc[b, 5],
+                 "N": [sc[b, 6 + s] for s in range(S)]}
+        out.append(Result(free_energy=float(sc[b, 0]), grand_potential=float(sc[b, 1]),
+                          forces=[force[b, s] for s in range(S)], parts=parts))
+    return out
 
 
 class Functional:

@@ -130,6 +130,22 @@ CDFT_API int cdft_create(cdft_engine** out, const long shape[3], double dx, int 
                 int fmt_model, double esfmt_A, double esfmt_B, int n_interactions,
                 const cdft_interaction* interactions, int precision);
 
+/* Batched engine: `batch` problems of this grid, species, FMT model and
+ * interactions (one mean-field weight set) evaluated together by one set of
+ * launches.  cdft_total and cdft_total_device then take every array for all
+ * problems back to back: rho, vext and force batch*S*N doubles (problem-
+ * major), mu batch*S values and scalars batch*CDFT_SCALAR_COUNT doubles.
+ * This is the eval_many of a parameter sweep; problems of different grids
+ * use one engine per grid.  No reference counterpart (the reference
+ * evaluates one state per call).  The drivers and cdft_hvp need batch 1. */
+#define CDFT_MAX_BATCH 64
+CDFT_API int cdft_create_batch(cdft_engine** out, const long shape[3], double dx, int n_species,
+                               const double* diameters, int fmt_model, double esfmt_A, double esfmt_B,
+                               int n_interactions, const cdft_interaction* interactions, int precision, int batch);
+
+/* Number of problems an engine evaluates per call. */
+CDFT_API int cdft_engine_batch(const cdft_engine* engine, int* batch);
+
 CDFT_API int cdft_destroy(cdft_engine* engine);
 
 /* Engine facts: info = {N, Nk, S, n_channels, n_deriv_channels, precision,
@@ -200,6 +216,20 @@ typedef struct {
 CDFT_API int cdft_minimize(cdft_engine* engine, const cdft_minimizer_config* cfg, double* rho,
                            const double* direction, cdft_engine* refine, double refine_switch,
                            cdft_minimizer_result* result, void* stream);
+
+/* Minimizer::grand_potential / fixed_mass for every problem of a batched
+ * engine (cdft_create_batch) at once.  rho: batch*N device doubles, replaced
+ * by the results; mu: batch host values (beta mu); target_mass: batch host
+ * values (fixed mass) or NULL; results: batch entries.  cfg->mode is
+ * CDFT_MIN_GRAND_POTENTIAL or CDFT_MIN_FIXED_MASS; cfg->chemical_potential
+ * and cfg->target_mass are not used.  Converged problems stop changing while
+ * the others continue; an uphill error of one problem is reported in its
+ * result (uphill_error = 1) without stopping the others.  `refine`: a
+ * batched FP64 engine with the same batch, or NULL.  No reference
+ * counterpart: the reference minimises one state per call. */
+CDFT_API int cdft_minimize_batch(cdft_engine* engine, const cdft_minimizer_config* cfg, const double* mu,
+                                 const double* target_mass, double* rho, cdft_engine* refine, double refine_switch,
+                                 cdft_minimizer_result* results, void* stream);
 
 /* DDFT step configuration, dynamics.hpp:26-33. */
 typedef struct {

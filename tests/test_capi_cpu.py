@@ -87,3 +87,15 @@ def test_engine_creation_fails_loudly_without_a_gpu():
     with pytest.raises(cd.EngineError) as exc:
         cd.make_weights(cd.WhiteBearII(), model)
     assert exc.value.code in (_lib.CDFT_ERR_CUDA, _lib.CDFT_ERR_RUNTIME)
+
+
+def test_batched_engine_size_is_validated_before_any_device_call():
+    import ctypes
+    L = _lib.lib()
+    d = (ctypes.c_double * 1)(1.0)
+    for bad in (0, 65):
+        h = ctypes.c_void_p()
+        st = L.cdft_create_batch(ctypes.byref(h), _lib.c_long3(8, 8, 8), 0.1, 1, d, 3, 1.0, 0.0, 0, None, 0, bad)
+        assert st == _lib.CDFT_ERR_INVALID
+        assert b"batch" in L.cdft_last_error()
+        assert not h.value
