@@ -15,5 +15,7 @@ from .functionals import (BARKER_HENDERSON, WEEKS_CHANDLER_ANDERSEN, Engine, EsF
 from .algorithms import (Bounded, EigenvalueResult, EigenvalueSolver, Fire, MinimizationResult, Minimizer,  # noqa: F401
                          SaddleResult, Search, Simulation, StepConfig, Unbounded, hessian_times_vector,
                          integrating_factor_step)
+from .bulk import (BulkThermodynamics, Coexistence, PhaseSearch, Spinodal, density_from_chemical_potential,  # noqa: F401
+                   densities_from_chemical_potentials, make_bulk_thermodynamics, make_bulk_weights)
 
 __version__ = "0.1.0"

@@ -72,6 +72,16 @@ class CEigenConfig(ctypes.Structure):
                 ("exact_hvp", ctypes.c_int), ("seed", ctypes.c_ulonglong)]
 
 
+class CBulkInteraction(ctypes.Structure):
+    _fields_ = [("species_i", ctypes.c_int), ("species_j", ctypes.c_int), ("a_vdw", ctypes.c_double)]
+
+
+class CBulkModel(ctypes.Structure):
+    _fields_ = [("n_species", ctypes.c_int), ("diameters", ctypes.c_double * 4), ("fmt_model", ctypes.c_int),
+                ("esfmt_A", ctypes.c_double), ("esfmt_B", ctypes.c_double), ("n_interactions", ctypes.c_int),
+                ("interactions", CBulkInteraction * 8)]
+
+
 class CSaddleConfig(ctypes.Structure):
     _fields_ = [("fire", CFireParams), ("eigen", CEigenConfig), ("rho_min", ctypes.c_double),
                 ("omega_tolerance", ctypes.c_double), ("tolerance_start", ctypes.c_double),
@@ -116,6 +126,16 @@ def lib():
                               ctypes.c_int, ctypes.c_int],
         "cdft_engine_batch": [vp, ctypes.POINTER(ctypes.c_int)],
         "cdft_destroy": [vp],
+        "cdft_engine_bulk_model": [vp, ctypes.POINTER(CBulkModel)],
+        "cdft_bulk_free_energy_density": [ctypes.POINTER(CBulkModel), c_double_p, c_double_p],
+        "cdft_bulk_chemical_potentials": [ctypes.POINTER(CBulkModel), c_double_p, c_double_p],
+        "cdft_bulk_pressure": [ctypes.POINTER(CBulkModel), c_double_p, c_double_p],
+        "cdft_bulk_density_from_mu": [ctypes.POINTER(CBulkModel), ctypes.c_int, c_double_p, c_double_p, ctypes.c_int,
+                                      ctypes.c_double, c_double_p, ctypes.POINTER(ctypes.c_int)],
+        "cdft_bulk_spinodal": [ctypes.POINTER(CBulkModel), ctypes.c_double, ctypes.c_double, c_double_p,
+                               ctypes.POINTER(ctypes.c_int)],
+        "cdft_bulk_coexistence": [ctypes.POINTER(CBulkModel), ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                  ctypes.c_double, c_double_p, ctypes.POINTER(ctypes.c_int)],
         "cdft_engine_info": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "cdft_engine_a_vdw": [vp, ctypes.c_int, c_double_p],
         "cdft_total": [vp, vp, vp, c_double_p, vp, c_double_p],

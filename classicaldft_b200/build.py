@@ -21,7 +21,7 @@ LIB = os.path.join(HERE, "libcdft_b200.so")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc") if os.path.exists(os.path.join(CUDA_HOME, "bin", "nvcc")) else "nvcc"
 
-SOURCES = ["engine.cu", "drivers.cu", "capi.cu", "noalloc.cu", "physics.cpp"]
+SOURCES = ["engine.cu", "drivers.cu", "capi.cu", "noalloc.cu", "bulk.cu", "physics.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++20", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I", CSRC, "-I", os.path.join(ROOT, "include")]
@@ -46,7 +46,7 @@ def _stale(obj, deps):
 def build(verbose: bool = False, extra=None) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = _headers()
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src + ".o")
@@ -59,7 +59,12 @@ def build(verbose: bool = False, extra=None) -> str:
                    os.path.join(ROOT, "include"), "-I", os.path.join(CUDA_HOME, "include"), "-c", path, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
+    # translation units compile in parallel
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(subprocess.run, c, check=True) for c in cmds]:
+            f.result()
     if _stale(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + [
             "-L", os.path.join(CUDA_HOME, "lib64"), "-lcufft", "-lcudart",

@@ -171,6 +171,21 @@ int cdft_engine_batch(const cdft_engine* engine, int* batch) {
   });
 }
 
+int cdft_engine_bulk_model(const cdft_engine* engine, cdft_bulk_model* out) {
+  return guarded([&] {
+    if (!engine || !out) throw std::invalid_argument("engine or out is NULL");
+    const cdft::EvalParams& p = engine->impl->params();
+    *out = cdft_bulk_model{};
+    out->n_species = p.S;
+    for (int s = 0; s < p.S; ++s) out->diameters[s] = 2.0 * p.R[s];
+    out->fmt_model = p.model;
+    out->esfmt_A = p.A;
+    out->esfmt_B = p.B;
+    out->n_interactions = p.M;
+    for (int m = 0; m < p.M; ++m) out->interactions[m] = {p.mf_i[m], p.mf_j[m], engine->impl->a_vdw(m)};
+  });
+}
+
 int cdft_destroy(cdft_engine* engine) {
   return guarded([&] {
     if (!engine) return;

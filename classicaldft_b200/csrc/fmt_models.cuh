@@ -40,8 +40,8 @@ __host__ __device__ inline Dual operator/(double a, Dual b) {
   double q = a / b.v;
   return {q, -q * b.d / b.v};
 }
-__device__ inline Dual dlog(Dual a) { return {log(a.v), a.d / a.v}; }
-__device__ inline double dlog(double a) { return log(a); }
+__host__ __device__ inline Dual dlog(Dual a) { return {log(a.v), a.d / a.v}; }
+__host__ __device__ inline double dlog(double a) { return log(a); }
 __host__ __device__ inline double val(double a) { return a; }
 __host__ __device__ inline double val(Dual a) { return a.v; }
 __host__ __device__ inline double zero_like(double) { return 0.0; }
@@ -76,7 +76,7 @@ struct FVals {
 // of the reference's expressions is rewritten with these reciprocals, which
 // keeps the FP64 division count at two per point.
 template <int MODEL, class T>
-__device__ __forceinline__ FVals<T> fmt_f(T eta) {
+__host__ __device__ __forceinline__ FVals<T> fmt_f(T eta) {
   constexpr int model = MODEL;
   FVals<T> r;
   const double ev = val(eta);
@@ -140,7 +140,7 @@ __device__ __forceinline__ FVals<T> fmt_f(T eta) {
 // Returns false (and leaves outputs untouched) where eta < 1e-30: the
 // reference skips those points (hard_sphere.hpp:199-200).
 template <int MODEL, class T>
-__device__ __forceinline__ bool fmt_phi_dphi(double A, double B, const Measures<T>& m, T& phi, MeasureDerivs<T>& dm) {
+__host__ __device__ __forceinline__ bool fmt_phi_dphi(double A, double B, const Measures<T>& m, T& phi, MeasureDerivs<T>& dm) {
   constexpr int model = MODEL;
   constexpr bool tensor = model_has_tensor(MODEL);
   if (val(m.eta) < 1e-30) return false;

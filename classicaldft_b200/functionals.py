@@ -374,6 +374,11 @@ class Functional:
     def grand_potential(self, rho, chemical_potential) -> float:
         return self.evaluate(rho, chemical_potential).grand_potential
 
+    def bulk(self):
+        """functional.hpp:48-50: the uniform fluid with the grid a_vdw."""
+        from .bulk import make_bulk_thermodynamics
+        return make_bulk_thermodynamics(self.model.species, self.weights)
+
     def grand_potential_callback(self, chemical_potential):
         """functional.hpp:62-73."""
         def fn(densities):

@@ -51,6 +51,9 @@ extern "C" {
 #define CDFT_WHITEBEAR_II 3
 #define CDFT_ESFMT 4
 
+#define CDFT_MAX_SPECIES 4
+#define CDFT_MAX_INTERACTIONS 8
+
 /* Precision of the FFTs and k-space products; Phi, dPhi and all sums stay FP64. */
 #define CDFT_FP64 0
 #define CDFT_MIXED 1
@@ -290,6 +293,57 @@ typedef struct {
 CDFT_API int cdft_saddle_find(cdft_engine* engine, const cdft_saddle_config* cfg, double* rho,
                               double chemical_potential, double target_mass, double* eigvec, double out[2],
                               int* outer_iterations, int* converged, void* stream);
+
+/* ---- bulk thermodynamics (host) ------------------------------------------ */
+
+/* The uniform fluid of a functional: species diameters, FMT model and the
+ * mean-field a_vdw of each interaction (BulkThermodynamics,
+ * functionals/bulk/thermodynamics.hpp:201-206). */
+typedef struct {
+  int species_i;
+  int species_j;
+  double a_vdw;
+} cdft_bulk_interaction;
+
+typedef struct {
+  int n_species;
+  double diameters[CDFT_MAX_SPECIES];
+  int fmt_model;
+  double esfmt_A, esfmt_B;
+  int n_interactions;
+  cdft_bulk_interaction interactions[CDFT_MAX_INTERACTIONS];
+} cdft_bulk_model;
+
+/* Functional::bulk() (functional.hpp:48-50): the engine's model with the grid
+ * a_vdw of its mean-field weights. */
+CDFT_API int cdft_engine_bulk_model(const cdft_engine* engine, cdft_bulk_model* out);
+
+/* f(rho) = ideal + hard-sphere + mean-field free energy density (kT units),
+ * rho: n_species densities (thermodynamics.hpp:208-218). */
+CDFT_API int cdft_bulk_free_energy_density(const cdft_bulk_model* model, const double* rho, double* f);
+
+/* beta mu_s for every species (thermodynamics.hpp:220-244). */
+CDFT_API int cdft_bulk_chemical_potentials(const cdft_bulk_model* model, const double* rho, double* mu);
+
+/* beta P = sum rho_s mu_s - f (thermodynamics.hpp:246-253); Omega/V = -P. */
+CDFT_API int cdft_bulk_pressure(const cdft_bulk_model* model, const double* rho, double* p);
+
+/* density_from_chemical_potential (coexistence.hpp:35-49) for n targets at
+ * once (one species): Newton from guess[i]; found[i] = 0 where the reference
+ * returns nullopt (rho[i] is then NaN). */
+CDFT_API int cdft_bulk_density_from_mu(const cdft_bulk_model* model, int n, const double* mu, const double* guess,
+                                       int max_iterations, double tolerance, double* rho, int* found);
+
+/* PhaseSearch::find_spinodal (coexistence.hpp:77-113): out = {rho_low,
+ * rho_high}; found = 0 where the reference returns nullopt. */
+CDFT_API int cdft_bulk_spinodal(const cdft_bulk_model* model, double rho_max, double rho_scan_step, double out[2],
+                                int* found);
+
+/* PhaseSearch::find_coexistence (coexistence.hpp:115-191): out = {rho_vapor,
+ * rho_liquid}; max_iterations / tolerance are the Newton settings of the
+ * PhaseSearch (the reference's defaults: 200, 1e-10). */
+CDFT_API int cdft_bulk_coexistence(const cdft_bulk_model* model, double rho_max, double rho_scan_step,
+                                   int max_iterations, double tolerance, double out[2], int* found);
 
 /* ---- allocation-free entry point ------------------------------------------ */
 

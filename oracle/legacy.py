@@ -149,3 +149,104 @@ def compute_a_vdw_qf(sigma, eps, rcut, kT, dx):
                 a, b, c = sorted((abs(ix), abs(iy), abs(iz)), reverse=True)
                 total += g * generate_weight_qf(sigma, eps, rcut, a, b, c, dx)
     return total / (dx * dx * dx) / kT
+
+
+# ------------------------------------------------- legacy phase solvers
+# legacy/classicaldft.hpp:799-907 (DFT_Coex.cpp of the original code): the
+# spinodal by golden-section search on P(rho), mu inversion by bisection and
+# the coexistence by bracketing P_v - P_l.  The reference cross-checks its
+# PhaseSearch against these to 1e-6 (tests/integration/functionals/bulk/coexistence.cpp).
+
+
+def legacy_find_spinodal(pressure, xmax, dx, tol=1e-8):
+    x = 2 * dx
+    p0 = pressure(dx)
+    p = pressure(2 * dx)
+    dp = p - p0
+    if dp < 0:
+        raise RuntimeError("Could not get started in findSpinodal")
+    while dp > 0 and x < xmax - dx:
+        dp = -p
+        x += dx
+        p = pressure(x)
+        dp += p
+    if x >= xmax - dx:
+        raise RuntimeError("Xmax exceeded in findSpinodal (max)")
+    r = (3.0 - math.sqrt(5.0)) / 2.0
+
+    def golden(a, b, maximum):
+        u = a + r * (b - a)
+        v = b - r * (b - a)
+        fu, fv = pressure(u), pressure(v)
+        while True:
+            if (fu > fv) if maximum else (fu < fv):
+                b, v, fv = v, u, fu
+                u = a + r * (b - a)
+                fu = pressure(u)
+            else:
+                a, u, fu = u, v, fv
+                v = b - r * (b - a)
+                fv = pressure(v)
+            if not (b - a > tol):
+                return (a + b) / 2
+
+    xs1 = golden(x - 2 * dx, x, True)
+    x = xs1
+    p = pressure(x)
+    while True:
+        dp = -p
+        x += dx
+        p = pressure(x)
+        dp += p
+        if not (dp < 0 and x < xmax - dx):
+            break
+    if x >= xmax - dx:
+        raise RuntimeError("Xmax exceeded in findSpinodal (min)")
+    xs2 = golden(x - 2 * dx, x, False)
+    return xs1, xs2
+
+
+def legacy_find_density_from_mu(chem, mu, xmin, xmax, tol=1e-8):
+    mu1, mu2 = chem(xmin), chem(xmax)
+    if mu1 > mu2:
+        xmin, xmax, mu1, mu2 = xmax, xmin, mu2, mu1
+    if mu2 < mu or mu1 > mu:
+        raise RuntimeError("find_density_from_mu: target mu out of range")
+    while True:
+        x = (xmin + xmax) / 2
+        mux = chem(x)
+        if mux > mu:
+            xmax, mu2 = x, mux
+        else:
+            xmin, mu1 = x, mux
+        if not (mu2 - mu1 > tol):
+            return (xmin + xmax) / 2
+
+
+def legacy_find_coex(pressure, chem, xmax, dx, tol=1e-8):
+    xs1, xs2 = legacy_find_spinodal(pressure, xmax, dx, tol)
+    xvap = xs1
+    xliq = legacy_find_density_from_mu(chem, chem(xvap), xs2, xmax - dx, tol)
+    dp1 = pressure(xvap) - pressure(xliq)
+    while True:
+        dp2 = dp1
+        xvap /= 1.1
+        xliq = legacy_find_density_from_mu(chem, chem(xvap), xs2, xmax - dx, tol)
+        dp1 = pressure(xvap) - pressure(xliq)
+        if not (xvap > 1e-40 and ((dp1 < 0) == (dp2 < 0))):
+            break
+    if xvap < 1e-40:
+        raise RuntimeError("findCoex bracket failed")
+    y1, y2 = xvap, xvap * 1.1
+    while True:
+        y = (y1 + y2) / 2
+        xliq = legacy_find_density_from_mu(chem, chem(y), xs2, xmax - dx, tol)
+        dp = pressure(y) - pressure(xliq)
+        if (dp < 0) == (dp1 < 0):
+            y1, dp1 = y, dp
+        else:
+            y2, dp2 = y, dp
+        if not (abs(y2 - y1) > xvap * tol):
+            break
+    rv = (y1 + y2) / 2
+    return rv, legacy_find_density_from_mu(chem, chem(rv), xs2, xmax - dx, tol)
