@@ -59,26 +59,38 @@ def hbm_peak():
         return FALLBACK_HBM, "fallback"
 
 
-def algorithmic_bytes(info, S=1, M=1, has_vext=False):
-    """Compulsory HBM bytes of one evaluation of this pipeline: one read and one
-    write of every array each stage touches (each FFT counted as one read of its
-    input and one write of its output), FP64 I/O for rho, V_ext and the force."""
+def stage_bytes(info, S=1, M=1, has_vext=False):
+    """Compulsory HBM bytes of each stage of one evaluation: one read and one
+    write of every array the stage touches (each FFT counted as one read of its
+    input and one write of its output), FP64 I/O for rho, V_ext and the force.
+    Keys follow the engine's stage order (Engine.STAGES)."""
     N, Nk = info["N"], info["Nk"]
     C, D = info["channels"], info["deriv_channels"]
     s = 4 if info["precision"] == 1 else 8
     Br, Bc, Bio = N * s, 2 * Nk * s, 8 * N
-    b = 0
-    if info["precision"] == 1:
-        b += S * Bio + S * Br            # rho -> fp32 copy
-    b += S * Br + S * Bc                 # r2c rho
-    b += S * Bc + M * 8 * Nk + C * Bc    # forward channels (+ MF weight, FP64 real)
-    b += C * (Bc + Br)                   # c2r channels
-    b += C * Br + S * Bio * (2 if has_vext else 1) + D * Br + S * Bio   # pointwise
-    b += D * (Br + Bc)                   # r2c derivatives
-    b += D * Bc + S * Bc                 # back-convolution
-    b += S * (Bc + Br)                   # c2r force
-    b += S * Br + 2 * S * Bio            # epilogue
-    return b
+    return {
+        "split": (S * Bio + S * Br) if info["precision"] == 1 else 0,   # rho -> fp32 fluctuation
+        "r2c_rho": S * Br + S * Bc,
+        "k_forward": S * Bc + M * 8 * Nk + C * Bc,                     # (+ MF weight, FP64 real)
+        "c2r_channels": C * (Bc + Br),
+        "pointwise": C * Br + S * Bio * (2 if has_vext else 1) + D * Br + S * Bio,
+        "r2c_derivatives": D * (Br + Bc),
+        "k_backward": D * Bc + S * Bc,
+        "c2r_force": S * (Bc + Br),
+        "epilogue": S * Br + 2 * S * Bio,
+        "reduce": 0,
+    }
+
+
+def algorithmic_bytes(info, S=1, M=1, has_vext=False):
+    """Compulsory HBM bytes of one evaluation (the sum over its stages)."""
+    return sum(stage_bytes(info, S, M, has_vext).values())
+
+
+# DRAM bytes per evaluation measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum over every launch of one evaluation, 128^3 mixed); the
+# launch list is summarised in profiles/eval_128cubed_mixed_launches.md.
+MEASURED_TRAFFIC = {"mixed": 1131.5e6}
 
 
 class ClockSampler:
@@ -246,6 +258,78 @@ def _time_device(torch, eng, rho, force, scal, flush, stream, steps, warmup, sam
     return float(np.sum([a.elapsed_time(b) for a, b in zip(starts, ends)])), clocks
 
 
+def stage_breakdown(torch, eng, rho, force, scal, flush, stream, n, peak):
+    """Live per-stage durations (CUDA events between the stages, on the
+    evaluation's stream) and the HBM roofline fraction of each stage."""
+    eng.stage_timing(True)
+    eng.stage_times()
+    with torch.cuda.stream(stream):
+        for i in range(n):
+            flush.fill_(float(i))
+            eng.total_device(rho.data_ptr(), None, [0.0], force.data_ptr(), scal.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    ms, count = eng.stage_times()
+    eng.stage_timing(False)
+    sb = stage_bytes(eng.info)
+    out = {}
+    for k, v in ms.items():
+        t = v / max(count, 1)
+        gbs = sb[k] / (t * 1e-3) / 1e9 if t > 0 and sb[k] else None
+        out[k] = {"ms": t, "algorithmic_bytes": sb[k], "achieved_gbs": gbs,
+                  "frac": (gbs / peak) if gbs else None,
+                  "kind": "cuFFT" if k.startswith(("r2c", "c2r")) else "engine kernel"}
+    return out
+
+
+SWEEP_SHAPES = (48, 64, 96)
+SWEEP_BATCH = 16
+
+
+def sweep_throughput(torch, cd, dev, precision, flush, stream, steps):
+    """Batched evaluation of 16 problems of each grid of the parameter sweep
+    (48^3, 64^3, 96^3 at dx = 0.1, kT = 1, WhiteBearII + cut LJ), as problem
+    evaluations per second, against the same problems one engine call each."""
+    lj = cd.make_lennard_jones(1.0, 1.0, 2.5)
+    d = lj.hard_sphere_diameter(1.0, cd.WEEKS_CHANDLER_ANDERSEN)
+    rng = np.random.default_rng(SEED + 4)
+    out = {}
+    for n in SWEEP_SHAPES:
+        g = cd.Grid(dx=0.1, box_size=(0.1 * n,) * 3, shape=(n, n, n))
+        model = cd.Model(g, [cd.Species("LJ", d)], [cd.Interaction(0, 0, lj)], 1.0)
+        N = g.total_points
+        rho = torch.tensor(0.6 * (1.0 + 0.01 * rng.uniform(-1.0, 1.0, (SWEEP_BATCH, N))), device=dev)
+        mus = list(np.linspace(-1.0, 2.0, SWEEP_BATCH))
+        res = {}
+        for B in (SWEEP_BATCH, 1):
+            eng = cd.Engine(cd.WhiteBearII(), model, precision, batch=B)
+            f = torch.empty((B, N), dtype=torch.float64, device=dev)
+            sc = torch.empty((B, 10), dtype=torch.float64, device=dev)
+            calls = SWEEP_BATCH // B
+
+            def step():
+                for c in range(calls):
+                    eng.total_device(rho[c * B].data_ptr(), None, mus[c * B:(c + 1) * B], f.data_ptr(), sc.data_ptr(),
+                                     stream.cuda_stream)
+            with torch.cuda.stream(stream):
+                for _ in range(3):
+                    step()
+            torch.cuda.synchronize()
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+            with torch.cuda.stream(stream):
+                for i in range(steps):
+                    flush.fill_(float(i))
+                    evs[i][0].record(stream)
+                    step()
+                    evs[i][1].record(stream)
+            torch.cuda.synchronize()
+            t = sum(a.elapsed_time(b) for a, b in evs) / steps
+            res[B] = SWEEP_BATCH / (t * 1e-3)
+            eng.close()
+        out[f"{n}^3"] = {"batched_problem_evals_per_s": res[SWEEP_BATCH], "one_by_one_problem_evals_per_s": res[1],
+                         "speedup": res[SWEEP_BATCH] / res[1]}
+    return out
+
+
 def run_ours(args, ws, rank, local, dist):
     import ctypes
     import torch
@@ -324,6 +408,10 @@ def run_ours(args, ws, rank, local, dist):
     peak, peak_kind = hbm_peak()
     achieved = nbytes / (ms_step * 1e-3) / 1e9
     names = {cd.MIXED: "mixed", cd.FP64: "fp64"}
+    stages = stage_breakdown(torch, eng, rho, force, scal, flush, stream, max(10, min(args.steps, 100)), peak)
+    mine = {k: v for k, v in stages.items() if v["kind"] == "engine kernel" and v["algorithmic_bytes"]}
+    top = max(mine, key=lambda k: mine[k]["ms"])
+    sweep = None if args.no_sweep else sweep_throughput(torch, cd, dev, precision, flush, stream, 20)
     line = {
         "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": ws, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -334,9 +422,13 @@ def run_ours(args, ws, rank, local, dist):
                    "hs_diameter": d, "precision": names[precision], "parallelism": f"replicas x{ws}",
                    "l2": "flushed between timed steps (256 MiB write outside the events)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": MEASURED_TRAFFIC.get(names[precision]),
                      "scope": "one full evaluation (cuFFT transforms + engine kernels)",
-                     "algorithmic_bytes": nbytes, "peak_source": peak_kind},
+                     "algorithmic_bytes": nbytes, "peak_source": peak_kind,
+                     "traffic_source": "ncu dram bytes over one evaluation's launches (profiles/)",
+                     "dominant_engine_kernel": {"stage": top, **mine[top]}},
+        "stages": stages,
+        "sweep": sweep,
         names[other]: {"value": ws * n2 / (t2 * 1e-3), "ms_per_step": t2 / n2},
         "mixed_vs_fp64": {"dF_over_F": dF, "max_dforce_over_max_force": dforce},
         "e2e": {"value": e2e_val, "unit": "evals/s", "h2d_bytes_per_step": 8 * info["N"],
@@ -361,6 +453,7 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-sweep", action="store_true", help="skip the batched 48/64/96^3 sweep measurement")
     args = ap.parse_args()
     ws, rank, local, dist = setup_dist(args)
     try:

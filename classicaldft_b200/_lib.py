@@ -141,6 +141,8 @@ def lib():
         "cdft_total": [vp, vp, vp, c_double_p, vp, c_double_p],
         "cdft_total_device": [vp, vp, vp, c_double_p, vp, vp, vp],
         "cdft_engine_status": [vp, vp],
+        "cdft_engine_stage_timing": [vp, ctypes.c_int],
+        "cdft_engine_stage_times": [vp, c_double_p, ctypes.POINTER(ctypes.c_longlong)],
         "cdft_local_terms_noalloc": [vp, vp, c_double_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_double, vp, vp,
                                      vp],
         "cdft_minimize": [vp, ctypes.POINTER(CMinimizerConfig), vp, vp, vp, ctypes.c_double,

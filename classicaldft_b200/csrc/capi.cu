@@ -246,6 +246,22 @@ int cdft_total_device(cdft_engine* engine, const double* rho, const double* vext
   });
 }
 
+int cdft_engine_stage_timing(cdft_engine* engine, int on) {
+  return guarded([&] {
+    if (!engine) throw std::invalid_argument("engine is NULL");
+    engine->impl->set_stage_timing(on != 0);
+  });
+}
+
+int cdft_engine_stage_times(cdft_engine* engine, double ms[CDFT_STAGE_COUNT], long long* evaluations) {
+  return guarded([&] {
+    if (!engine || !ms) throw std::invalid_argument("engine and ms are required");
+    static_assert(CDFT_STAGE_COUNT == cdft::Engine::kStages, "stage count");
+    const long long n = engine->impl->take_stage_times(ms);
+    if (evaluations) *evaluations = n;
+  });
+}
+
 int cdft_engine_status(cdft_engine* engine, void* stream) {
   return guarded([&] {
     if (!engine) throw std::invalid_argument("engine is NULL");

@@ -198,6 +198,28 @@ Engine::~Engine() {
                   (void*)partials_, fft_work_, (void*)h_rho_, (void*)h_vext_, (void*)h_force_, (void*)h_scalars_})
     if (q) cudaFree(q);
   if (stream_) cudaStreamDestroy(stream_);
+  for (cudaEvent_t e : stage_ev_)
+    if (e) cudaEventDestroy(e);
+}
+
+void Engine::set_stage_timing(bool on) {
+  if (on && !stage_ev_[0])
+    for (cudaEvent_t& e : stage_ev_) CDFT_CUDA(cudaEventCreate(&e));
+  timing_ = on;
+}
+
+void Engine::mark(int i, cudaStream_t stream) {
+  if (timing_run_) CDFT_CUDA(cudaEventRecord(stage_ev_[i], stream));
+}
+
+long long Engine::take_stage_times(double* ms) {
+  for (int i = 0; i < kStages; ++i) {
+    ms[i] = stage_ms_[i];
+    stage_ms_[i] = 0.0;
+  }
+  const long long n = stage_count_;
+  stage_count_ = 0;
+  return n;
 }
 
 void Engine::build_plans() {
@@ -272,10 +294,13 @@ void Engine::forward_stage(const double* in, R* chan_out, double* mean_out, cuda
     k_species_sums<<<gs, 256, 0, stream>>>(in, p.N, p.S, partials_);
     k_split_convert<<<gs, 256, 0, stream>>>(in, p.N, p.S, partials_, grid_stream_, static_cast<float*>(rho_lo_),
                                             mean_out);
+    mark(1, stream);
     CDFT_CUFFT(cufftExecR2C(plan_rho_, static_cast<float*>(rho_lo_), reinterpret_cast<cufftComplex*>(rho_k)));
   } else {
+    mark(1, stream);
     CDFT_CUFFT(cufftExecD2Z(plan_rho_, const_cast<double*>(in), reinterpret_cast<cufftDoubleComplex*>(rho_k)));
   }
+  mark(2, stream);
   const bool multi = p.L.multi, tensor = p.L.tensor;
   const dim3 gk(grid_k_, p.batch);
   if (!multi && !tensor) k_forward<false, false, C2><<<gk, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
@@ -283,11 +308,13 @@ void Engine::forward_stage(const double* in, R* chan_out, double* mean_out, cuda
   if (multi && !tensor) k_forward<true, false, C2><<<gk, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
   if (multi && tensor) k_forward<true, true, C2><<<gk, 256, 0, stream>>>(p, rho_k, mf_w_, chan_k);
   CDFT_CUDA(cudaGetLastError());
+  mark(3, stream);
   if constexpr (mixed)
     CDFT_CUFFT(cufftExecC2R(plan_chan_, reinterpret_cast<cufftComplex*>(chan_k), reinterpret_cast<float*>(chan_out)));
   else
     CDFT_CUFFT(cufftExecZ2D(plan_chan_, reinterpret_cast<cufftDoubleComplex*>(chan_k),
                             reinterpret_cast<double*>(chan_out)));
+  mark(4, stream);
 }
 
 // Stages 5-7: out += c2r(sum_c conj(W_c) r2c(deriv_c)) dV - mu dV (+ the
@@ -304,6 +331,7 @@ void Engine::backward_stage(R* deriv, const double* dbar, double* out, const MuA
   else
     CDFT_CUFFT(cufftExecD2Z(plan_deriv_, reinterpret_cast<double*>(deriv),
                             reinterpret_cast<cufftDoubleComplex*>(deriv_k)));
+  mark(6, stream);
   const bool multi = p.L.multi, tensor = p.L.tensor;
   const dim3 gk(grid_k_, p.batch), gs(grid_stream_, p.batch);
   if (!multi && !tensor) k_backward<false, false, C2><<<gk, 256, 0, stream>>>(p, deriv_k, force_k);
@@ -311,16 +339,19 @@ void Engine::backward_stage(R* deriv, const double* dbar, double* out, const MuA
   if (multi && !tensor) k_backward<true, false, C2><<<gk, 256, 0, stream>>>(p, deriv_k, force_k);
   if (multi && tensor) k_backward<true, true, C2><<<gk, 256, 0, stream>>>(p, deriv_k, force_k);
   CDFT_CUDA(cudaGetLastError());
+  mark(7, stream);
   if constexpr (mixed)
     CDFT_CUFFT(cufftExecC2R(plan_force_, reinterpret_cast<cufftComplex*>(force_k), reinterpret_cast<float*>(hs_r)));
   else
     CDFT_CUFFT(cufftExecZ2D(plan_force_, reinterpret_cast<cufftDoubleComplex*>(force_k),
                             reinterpret_cast<double*>(hs_r)));
+  mark(8, stream);
   if (!multi && !tensor) k_epilogue<false, false, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu);
   if (!multi && tensor) k_epilogue<false, true, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu);
   if (multi && !tensor) k_epilogue<true, false, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu);
   if (multi && tensor) k_epilogue<true, true, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu);
   CDFT_CUDA(cudaGetLastError());
+  mark(9, stream);
 }
 
 template <typename R, typename C2>
@@ -337,6 +368,8 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
     CDFT_CUDA(cudaMemcpyAsync(h_rho_, rho, sizeof(double) * p.batch * p.S * p.N, cudaMemcpyDeviceToDevice, stream));
     rho = h_rho_;
   }
+  timing_run_ = timing_;
+  mark(0, stream);
   // 1-3. weighted densities
   forward_stage<R, C2>(rho, chan_r, mean_, stream);
   // 4. pointwise Phi / dPhi + local terms + reductions
@@ -366,6 +399,7 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
     }
   });
   CDFT_CUDA(cudaGetLastError());
+  mark(5, stream);
   // 5-7. back-convolution into the force
   MuArgs ma;
   for (int b = 0; b < kMaxBatch; ++b)
@@ -374,6 +408,17 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   // 8. scalars, one block per problem
   k_reduce_final<<<p.batch, 32 * (4 + kMaxSpecies), 0, stream>>>(partials_, pw_blocks, p, ma, err_, scalars);
   CDFT_CUDA(cudaGetLastError());
+  mark(10, stream);
+  if (timing_run_) {
+    timing_run_ = false;
+    CDFT_CUDA(cudaEventSynchronize(stage_ev_[kStages]));
+    for (int i = 0; i < kStages; ++i) {
+      float ms = 0.0f;
+      CDFT_CUDA(cudaEventElapsedTime(&ms, stage_ev_[i], stage_ev_[i + 1]));
+      stage_ms_[i] += ms;
+    }
+    ++stage_count_;
+  }
 }
 
 // Exact Hessian-vector product (forward-over-reverse): hv = d(force)/d(rho) . v

@@ -66,6 +66,18 @@ class Engine {
   int kernels_per_eval() const { return precision_ == 1 ? 7 : 5; }
   // Reads and clears the device error word (synchronises the stream).
   int take_error(cudaStream_t stream);
+
+  // Stage timing: when on, every evaluate() records CUDA events between its
+  // stages on its stream and synchronises at the end to accumulate the
+  // durations (kStages of them, in pipeline order):
+  //   0 split / FP32 conversion (mixed), 1 r2c rho, 2 k_forward, 3 c2r channels,
+  //   4 pointwise, 5 r2c derivatives, 6 k_backward, 7 c2r force, 8 epilogue,
+  //   9 final reduction.
+  static constexpr int kStages = 10;
+  void set_stage_timing(bool on);
+  // Accumulated milliseconds per stage and the number of timed evaluations;
+  // clears the accumulators.
+  long long take_stage_times(double* ms);
   // Scratch bytes held beyond inputs and outputs.
   size_t scratch_bytes() const { return scratch_bytes_; }
 
@@ -125,6 +137,12 @@ class Engine {
 
   cufftHandle plan_rho_ = 0, plan_chan_ = 0, plan_deriv_ = 0, plan_force_ = 0;
   bool plans_made_ = false;
+
+  void mark(int i, cudaStream_t stream);
+  bool timing_ = false, timing_run_ = false;
+  cudaEvent_t stage_ev_[kStages + 1] = {};
+  double stage_ms_[kStages] = {};
+  long long stage_count_ = 0;
 
   double* h_rho_ = nullptr;   // device staging for host API
   double* h_vext_ = nullptr;

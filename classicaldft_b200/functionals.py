@@ -257,6 +257,14 @@ class Engine:
         except Exception:
             pass
 
+    def _mu(self, mu):
+        """beta*mu as a contiguous (S,) or (B, S) array; B values for one species broadcast per problem."""
+        lead = (self.S,) if self.batch == 1 else (self.batch, self.S)
+        m = np.asarray(mu, dtype=np.float64)
+        if self.batch > 1 and self.S == 1 and m.ndim == 1 and m.size == self.batch:
+            m = m[:, None]
+        return np.ascontiguousarray(np.broadcast_to(m, lead))
+
     def total_host(self, rho: np.ndarray, mu, vext=None, want_force=True):
         """cdft_total on host arrays: rho (S, N) -> (scalars[10], force (S, N) or None).
 
@@ -265,7 +273,7 @@ class Engine:
         """
         lead = (self.S,) if self.batch == 1 else (self.batch, self.S)
         rho = np.ascontiguousarray(rho, dtype=np.float64).reshape(*lead, self.N)
-        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), lead))
+        mu = self._mu(mu)
         v = None if vext is None else np.ascontiguousarray(vext, dtype=np.float64).reshape(*lead, self.N)
         force = np.empty((*lead, self.N)) if want_force else None
         sc = np.empty(_lib.SCALAR_COUNT if self.batch == 1 else (self.batch, _lib.SCALAR_COUNT))
@@ -275,10 +283,23 @@ class Engine:
                                          sc.ctypes.data_as(_lib.c_double_p)))
         return sc, force
 
+    STAGES = ("split", "r2c_rho", "k_forward", "c2r_channels", "pointwise", "r2c_derivatives", "k_backward",
+              "c2r_force", "epilogue", "reduce")
+
+    def stage_timing(self, on: bool = True):
+        """Record CUDA events between the evaluation stages (synchronises each evaluation)."""
+        _lib.check(_lib.lib().cdft_engine_stage_timing(self.handle, 1 if on else 0))
+
+    def stage_times(self):
+        """({stage: accumulated ms}, evaluations) since the last call."""
+        ms = (ctypes.c_double * len(self.STAGES))()
+        n = ctypes.c_longlong()
+        _lib.check(_lib.lib().cdft_engine_stage_times(self.handle, ms, ctypes.byref(n)))
+        return dict(zip(self.STAGES, list(ms))), n.value
+
     def total_device(self, rho_ptr: int, vext_ptr, mu, force_ptr: int, scalars_ptr: int, stream: int = 0):
         """cdft_total_device on device pointers (ints, e.g. torch.Tensor.data_ptr())."""
-        lead = (self.S,) if self.batch == 1 else (self.batch, self.S)
-        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), lead))
+        mu = self._mu(mu)
         _lib.check(_lib.lib().cdft_total_device(self.handle, rho_ptr, vext_ptr or None,
                                                 mu.ctypes.data_as(_lib.c_double_p), force_ptr, scalars_ptr,
                                                 stream or None))

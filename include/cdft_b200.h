@@ -364,6 +364,20 @@ CDFT_API int cdft_bulk_coexistence(const cdft_bulk_model* model, double rho_max,
 CDFT_API int cdft_local_terms_noalloc(const double* rho, const double* vext, const double* mu, int n_species,
                                       long long n_points, double dv, double* force, double* scalars, void* stream);
 
+/* Stage timing (a measurement hook; no reference counterpart).  With `on`,
+ * every evaluation records CUDA events between its stages on its own stream
+ * and synchronises at its end to accumulate the stage durations; off by
+ * default (then evaluations are fully asynchronous).  The stages, in order:
+ * 0 split / FP32 conversion (mixed), 1 r2c rho, 2 k_forward, 3 c2r channels,
+ * 4 pointwise, 5 r2c derivatives, 6 k_backward, 7 c2r force, 8 epilogue,
+ * 9 final reduction. */
+#define CDFT_STAGE_COUNT 10
+CDFT_API int cdft_engine_stage_timing(cdft_engine* engine, int on);
+
+/* Accumulated milliseconds per stage since the last call, and the number of
+ * timed evaluations; clears the accumulators. */
+CDFT_API int cdft_engine_stage_times(cdft_engine* engine, double ms[CDFT_STAGE_COUNT], long long* evaluations);
+
 /* Status of earlier asynchronous calls on `stream`: CDFT_ERR_RUNTIME if a
  * bounded device-side wait gave up (the scalars of that call are NaN), else
  * CDFT_OK.  Synchronises the stream and clears the flag.  No reference

@@ -185,3 +185,23 @@ def test_tma_and_plain_pointwise_paths_agree():
     assert np.max(np.abs(f1 - f2)) <= 1e-13 * np.max(np.abs(f1))
     r = pr.ref([rho], [0.3])
     assert rel_err(s1[0], r.free_energy) <= F_TOL
+
+
+def test_stage_timing_hook_records_every_stage_and_changes_nothing():
+    pr = Problem((32, 32, 32), 0.2, [1.0], "WhiteBearII", inters=[(0, 0) + LJ], kT=0.8, precision=cd.MIXED)
+    rho = profile(pr.N, (32, 32, 32), 13, 0.35, 0.1)
+    e = pr.weights.engine
+    plain = pr.gpu([rho], [0.2])
+    e.stage_timing(True)
+    e.stage_times()
+    timed = [pr.gpu([rho], [0.2]) for _ in range(3)]
+    ms, n = e.stage_times()
+    e.stage_timing(False)
+    assert n == 3
+    assert set(ms) == set(cd.Engine.STAGES)
+    assert all(v >= 0.0 for v in ms.values())
+    assert ms["pointwise"] > 0.0 and ms["c2r_channels"] > 0.0 and ms["split"] > 0.0
+    for t in timed:
+        assert t.free_energy == plain.free_energy
+        assert np.array_equal(t.forces[0], plain.forces[0])
+    assert e.stage_times()[1] == 0
