@@ -10,9 +10,10 @@ r_c = 2.5, QF weights), mean density 0.35 with seeded 1% white noise.  Inputs
 are synthetic (seeded); no dataset is involved.
 
 Timing: inputs resident in HBM, W untimed warm-up steps, then K steps, each
-bracketed by CUDA events on the engine's stream with an L2 flush (a write of
-a 256 MiB buffer, outside the events) between steps; barrier + synchronize
-on both sides; the max over ranks.  Each rank evaluates its own replica
+bracketed by CUDA events on the engine's stream with an L2 flush between
+steps, outside the events: a write of a 256 MiB buffer, then a read of a
+second one, so that no dirty line of the flush is written back inside the
+timed region; barrier + synchronize on both sides; the max over ranks.  Each rank evaluates its own replica
 (one grid does not shard), so `value` = N * K / max time.
 
 `e2e` repeats the metric through the public host API (cdft_total via
@@ -59,21 +60,35 @@ def hbm_peak():
         return FALLBACK_HBM, "fallback"
 
 
-def stage_bytes(info, S=1, M=1, has_vext=False):
+def stage_bytes(info, S=1, M=1, has_vext=False, fused=False):
     """Compulsory HBM bytes of each stage of one evaluation: one read and one
     write of every array the stage touches (each FFT counted as one read of its
     input and one write of its output), FP64 I/O for rho, V_ext and the force.
-    Keys follow the engine's stage order (Engine.STAGES)."""
+    Keys follow the engine's stage order (Engine.stage_names)."""
     N, Nk = info["N"], info["Nk"]
     C, D = info["channels"], info["deriv_channels"]
     s = 4 if info["precision"] == 1 else 8
     Br, Bc, Bio = N * s, 2 * Nk * s, 8 * N
+    pointwise = C * Br + S * Bio * (2 if has_vext else 1) + D * Br + S * Bio
+    if fused:
+        return {
+            "species_mean": S * Bio,
+            "plane_fwd_rho": S * Bio + S * Bc,
+            "col_fwd": S * Bc + M * 8 * Nk + C * Bc,
+            "plane_inv_channels": C * (Bc + Br),
+            "pointwise": pointwise,
+            "plane_fwd_derivatives": D * (Br + Bc),
+            "col_bwd": D * Bc + S * Bc,
+            "plane_inv_epilogue": S * Bc + 2 * S * Bio,
+            "-8": 0,
+            "-9": 0,
+        }
     return {
         "split": (S * Bio + S * Br) if info["precision"] == 1 else 0,   # rho -> fp32 fluctuation
         "r2c_rho": S * Br + S * Bc,
         "k_forward": S * Bc + M * 8 * Nk + C * Bc,                     # (+ MF weight, FP64 real)
         "c2r_channels": C * (Bc + Br),
-        "pointwise": C * Br + S * Bio * (2 if has_vext else 1) + D * Br + S * Bio,
+        "pointwise": pointwise,
         "r2c_derivatives": D * (Br + Bc),
         "k_backward": D * Bc + S * Bc,
         "c2r_force": S * (Bc + Br),
@@ -82,9 +97,25 @@ def stage_bytes(info, S=1, M=1, has_vext=False):
     }
 
 
-def algorithmic_bytes(info, S=1, M=1, has_vext=False):
+def algorithmic_bytes(info, S=1, M=1, has_vext=False, fused=False):
     """Compulsory HBM bytes of one evaluation (the sum over its stages)."""
-    return sum(stage_bytes(info, S, M, has_vext).values())
+    return sum(stage_bytes(info, S, M, has_vext, fused).values())
+
+
+class L2Flush:
+    """Between timed steps: write a 256 MiB buffer (more than the 126 MB L2),
+    then read another, leaving L2 clean and cold."""
+
+    def __init__(self, torch, dev):
+        n = 256 * 1024 * 1024 // 4
+        self.w = torch.empty(n, dtype=torch.float32, device=dev)
+        self.r = torch.ones(n, dtype=torch.float32, device=dev)
+        self.acc = torch.empty((), dtype=torch.float32, device=dev)
+        self.torch = torch
+
+    def __call__(self, i):
+        self.w.fill_(float(i))
+        self.torch.sum(self.r, 0, out=self.acc)
 
 
 # DRAM bytes per evaluation measured by ncu (dram__bytes_read.sum +
@@ -249,7 +280,7 @@ def _time_device(torch, eng, rho, force, scal, flush, stream, steps, warmup, sam
         time.sleep(0.3)
     with torch.cuda.stream(stream):
         for i in range(steps):
-            flush.fill_(float(i))
+            flush(i)
             starts[i].record(stream)
             step()
             ends[i].record(stream)
@@ -265,12 +296,12 @@ def stage_breakdown(torch, eng, rho, force, scal, flush, stream, n, peak):
     eng.stage_times()
     with torch.cuda.stream(stream):
         for i in range(n):
-            flush.fill_(float(i))
+            flush(i)
             eng.total_device(rho.data_ptr(), None, [0.0], force.data_ptr(), scal.data_ptr(), stream.cuda_stream)
     torch.cuda.synchronize()
     ms, count = eng.stage_times()
     eng.stage_timing(False)
-    sb = stage_bytes(eng.info)
+    sb = stage_bytes(eng.info, fused=eng.transforms == "fused")
     out = {}
     for k, v in ms.items():
         t = v / max(count, 1)
@@ -317,7 +348,7 @@ def sweep_throughput(torch, cd, dev, precision, flush, stream, steps):
             evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
             with torch.cuda.stream(stream):
                 for i in range(steps):
-                    flush.fill_(float(i))
+                    flush(i)
                     evs[i][0].record(stream)
                     step()
                     evs[i][1].record(stream)
@@ -341,7 +372,7 @@ def run_ours(args, ws, rank, local, dist):
     rho = torch.tensor(rho_h, dtype=torch.float64, device=dev)
     force = torch.empty_like(rho)
     scal = torch.zeros(10, dtype=torch.float64, device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    flush = L2Flush(torch, dev)
     stream = torch.cuda.Stream(device=dev)
     sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
     if dist:
@@ -404,7 +435,7 @@ def run_ours(args, ws, rank, local, dist):
     e2e_val = ws * n_e2e / el
 
     info = eng.info
-    nbytes = algorithmic_bytes(info, S=1, M=1)
+    nbytes = algorithmic_bytes(info, S=1, M=1, fused=eng.transforms == "fused")
     peak, peak_kind = hbm_peak()
     achieved = nbytes / (ms_step * 1e-3) / 1e9
     names = {cd.MIXED: "mixed", cd.FP64: "fp64"}
@@ -420,7 +451,8 @@ def run_ours(args, ws, rank, local, dist):
         "config": {"workload": "128^3 LJ-fluid DDFT state, WhiteBearII + cut LJ (QF), 1 species",
                    "grid": list(SHAPE), "dx": DX, "kT": KT, "rho_bar": RHO_BAR, "noise": "1% uniform, seeded",
                    "hs_diameter": d, "precision": names[precision], "parallelism": f"replicas x{ws}",
-                   "l2": "flushed between timed steps (256 MiB write outside the events)"},
+                   "l2": "flushed between timed steps (256 MiB write + 256 MiB read, outside the events)",
+                   "transforms": eng.transforms},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": MEASURED_TRAFFIC.get(names[precision]),
                      "scope": "one full evaluation (cuFFT transforms + engine kernels)",

@@ -22,6 +22,7 @@ SCALAR_COUNT = 10
 MODEL_IDS = {"Rosenfeld": 0, "RSLT": 1, "WhiteBearI": 2, "WhiteBearII": 3, "esFMT": 4}
 FP64 = 0
 MIXED = 1
+TRANSFORMS_CUFFT, TRANSFORMS_FUSED = 0, 1
 POT_LJ, POT_TWF, POT_WRDF = 0, 1, 2
 SPLIT_WCA, SPLIT_BH = 0, 1
 WEIGHT_SCHEMES = {"InterpolationZero": 0, "InterpolationLinearE": 1, "InterpolationLinearF": 2,
@@ -141,6 +142,8 @@ def lib():
         "cdft_total": [vp, vp, vp, c_double_p, vp, c_double_p],
         "cdft_total_device": [vp, vp, vp, c_double_p, vp, vp, vp],
         "cdft_engine_status": [vp, vp],
+        "cdft_engine_set_transforms": [vp, ctypes.c_int],
+        "cdft_engine_transforms": [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
         "cdft_engine_stage_timing": [vp, ctypes.c_int],
         "cdft_engine_stage_times": [vp, c_double_p, ctypes.POINTER(ctypes.c_longlong)],
         "cdft_local_terms_noalloc": [vp, vp, c_double_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_double, vp, vp,

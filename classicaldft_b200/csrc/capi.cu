@@ -262,6 +262,23 @@ int cdft_engine_stage_times(cdft_engine* engine, double ms[CDFT_STAGE_COUNT], lo
   });
 }
 
+int cdft_engine_set_transforms(cdft_engine* engine, int transforms) {
+  return guarded([&] {
+    if (!engine) throw std::invalid_argument("engine is NULL");
+    if (transforms != CDFT_TRANSFORMS_CUFFT && transforms != CDFT_TRANSFORMS_FUSED)
+      throw std::invalid_argument("unknown transform implementation");
+    engine->impl->set_fused(transforms == CDFT_TRANSFORMS_FUSED);
+  });
+}
+
+int cdft_engine_transforms(const cdft_engine* engine, int* transforms, int* fused_available) {
+  return guarded([&] {
+    if (!engine) throw std::invalid_argument("engine is NULL");
+    if (transforms) *transforms = engine->impl->fused() ? CDFT_TRANSFORMS_FUSED : CDFT_TRANSFORMS_CUFFT;
+    if (fused_available) *fused_available = engine->impl->fusable() ? 1 : 0;
+  });
+}
+
 int cdft_engine_status(cdft_engine* engine, void* stream) {
   return guarded([&] {
     if (!engine) throw std::invalid_argument("engine is NULL");

@@ -21,7 +21,7 @@ namespace cdft {
 constexpr int kMaxSpecies = 4;
 constexpr int kMaxInteractions = 8;
 // Problems of one shape evaluated together by a batched engine (one set of
-// launches; the problem index is blockIdx.y, or blockIdx.x in k_reduce_final).
+// launches; the problem index is blockIdx.y).
 constexpr int kMaxBatch = 64;
 constexpr double kPi = 3.14159265358979323846;
 
@@ -97,6 +97,15 @@ struct EvalParams {
 // kernels that need them as a __grid_constant__ parameter.
 struct MuArgs {
   double mu[kMaxBatch][kMaxSpecies];
+};
+
+// Inputs of the final reduction folded into k_epilogue (scalars == null
+// skips it).
+struct FinalArgs {
+  const double* partials;  // B * nblocks * n_terms (the pointwise kernel's)
+  int nblocks;
+  const int* err;
+  double* scalars;         // B * kScalarCount
 };
 
 // Reduction term order: F_hs, F_id, F_ext, F_mf, then N_s for each species.

@@ -2,6 +2,7 @@
 // evaluation pipeline of one F[rho] + dF/drho call.
 #include "engine.cuh"
 #include "eval_kernels.cuh"
+#include "fft_kernels.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -173,9 +174,12 @@ Engine::Engine(const EngineSpec& spec) {
   partials_ = dalloc<double>((size_t)B * std::max(std::max(grid_pw_, grid_tma_), grid_stream_) * p.n_terms, tot);
   err_ = dalloc<int>(1, tot);
   CDFT_CUDA(cudaMemset(err_, 0, sizeof(int)));
+  sync_ = dalloc<unsigned>((size_t)B, tot);
+  CDFT_CUDA(cudaMemset(sync_, 0, sizeof(unsigned) * B));
 
   build_plans();
   upload_mean_field(spec);
+  setup_fused();
   scratch_bytes_ = tot;
 
   CDFT_CUDA(cudaMalloc(&h_rho_, sizeof(double) * B * S * p.N));
@@ -193,9 +197,9 @@ Engine::~Engine() {
     cufftDestroy(plan_force_);
   }
   for (void* q : {rho_k_, chan_k_, chan_r_, deriv_r_, deriv_k_, force_k_, hs_r_, rho_lo_, (void*)mf_w_,
-                  (void*)mean_, (void*)dbar_, (void*)err_, tan_chan_, (void*)tan_mean_, (void*)tan_dbar_,
+                  (void*)mean_, (void*)dbar_, (void*)err_, (void*)sync_, tan_chan_, (void*)tan_mean_, (void*)tan_dbar_,
                   (void*)tan_in_,
-                  (void*)partials_, fft_work_, (void*)h_rho_, (void*)h_vext_, (void*)h_force_, (void*)h_scalars_})
+                  (void*)partials_, fft_work_, tw_, (void*)h_rho_, (void*)h_vext_, (void*)h_force_, (void*)h_scalars_})
     if (q) cudaFree(q);
   if (stream_) cudaStreamDestroy(stream_);
   for (cudaEvent_t e : stage_ev_)
@@ -203,16 +207,35 @@ Engine::~Engine() {
 }
 
 void Engine::set_stage_timing(bool on) {
-  if (on && !stage_ev_[0])
+  if (on && stage_ev_.empty()) {
+    stage_ev_.assign((size_t)kTimingRing * (kStages + 1), nullptr);
     for (cudaEvent_t& e : stage_ev_) CDFT_CUDA(cudaEventCreate(&e));
+  }
+  if (!on) harvest_stage_times();
   timing_ = on;
 }
 
 void Engine::mark(int i, cudaStream_t stream) {
-  if (timing_run_) CDFT_CUDA(cudaEventRecord(stage_ev_[i], stream));
+  if (timing_run_) CDFT_CUDA(cudaEventRecord(stage_ev_[(size_t)ring_used_ * (kStages + 1) + i], stream));
+}
+
+// Waits for the recorded sets and adds their stage durations.
+void Engine::harvest_stage_times() {
+  for (int r = 0; r < ring_used_; ++r) {
+    cudaEvent_t* ev = &stage_ev_[(size_t)r * (kStages + 1)];
+    CDFT_CUDA(cudaEventSynchronize(ev[kStages]));
+    for (int i = 0; i < kStages; ++i) {
+      float ms = 0.0f;
+      CDFT_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+      stage_ms_[i] += ms;
+    }
+    ++stage_count_;
+  }
+  ring_used_ = 0;
 }
 
 long long Engine::take_stage_times(double* ms) {
+  harvest_stage_times();
   for (int i = 0; i < kStages; ++i) {
     ms[i] = stage_ms_[i];
     stage_ms_[i] = 0.0;
@@ -220,6 +243,82 @@ long long Engine::take_stage_times(double* ms) {
   const long long n = stage_count_;
   stage_count_ = 0;
   return n;
+}
+
+// The fused transform path (fft_kernels.cuh) serves mixed-precision engines
+// on power-of-two grids whose (y, z) plane fits in shared memory with two
+// CTAs per SM; everything else (and the HVP) uses the cuFFT plans.
+void Engine::setup_fused() {
+  const EvalParams& p = p_;
+  auto pow2 = [](int n) { return n >= 2 && (n & (n - 1)) == 0; };
+  fusable_ = false;
+  if (precision_ != kMixed || !pow2(p.nx) || !pow2(p.ny) || !pow2(p.nz) || p.nz < 4 || p.nx > 256 || p.ny > 256 ||
+      p.nz > 256)
+    return;
+  const size_t kSmemCap = 110 * 1024;
+  plane_smem_ = plane_smem_bytes(p.ny, p.nz);
+  if (plane_smem_ > kSmemCap) return;
+  const int nbuf_f = p.S + p.n_chan, nbuf_b = p.L.n_deriv;
+  int tq = 16;
+  while (tq >= 1 && (col_smem_bytes(p.nx, tq, nbuf_f) > kSmemCap || col_smem_bytes(p.nx, tq, nbuf_b) > kSmemCap))
+    tq /= 2;
+  if (tq < 1) return;
+  tq_ = tq;
+  colf_smem_ = col_smem_bytes(p.nx, tq, nbuf_f);
+  colb_smem_ = col_smem_bytes(p.nx, tq, nbuf_b);
+  col_tiles_ = (int)(((long long)p.ny * p.nzh + tq - 1) / tq);
+  // twiddle tables, FP64-rounded
+  std::vector<fft::cpx> tw;
+  auto table = [&](int M) {
+    for (int n = 0; n < M; ++n) {
+      const double a = -2.0 * kPi * (double)n / (double)M;
+      tw.push_back({(float)std::cos(a), (float)std::sin(a)});
+    }
+  };
+  table(p.nx);
+  table(p.ny);
+  table(p.nz / 2);
+  table(p.nz);
+  CDFT_CUDA(cudaMalloc(&tw_, sizeof(fft::cpx) * tw.size()));
+  CDFT_CUDA(cudaMemcpy(tw_, tw.data(), sizeof(fft::cpx) * tw.size(), cudaMemcpyHostToDevice));
+  const fft::cpx* t = static_cast<const fft::cpx*>(tw_);
+  tables_ = FftTables{t, t + p.nx, t + p.nx + p.ny, t + p.nx + p.ny + p.nz / 2};
+  auto allow = [](auto kern, size_t bytes) {
+    CDFT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  };
+  allow(k_plane_fwd<double>, plane_smem_);
+  allow(k_plane_fwd<float>, plane_smem_);
+  allow(k_plane_inv, plane_smem_);
+  const bool multi = p.L.multi, tensor = p.L.tensor;
+  if (!multi && !tensor) {
+    allow(k_col_fwd<false, false>, colf_smem_);
+    allow(k_col_bwd<false, false>, colb_smem_);
+    allow(k_plane_inv_epi<false, false>, plane_smem_);
+  }
+  if (!multi && tensor) {
+    allow(k_col_fwd<false, true>, colf_smem_);
+    allow(k_col_bwd<false, true>, colb_smem_);
+    allow(k_plane_inv_epi<false, true>, plane_smem_);
+  }
+  if (multi && !tensor) {
+    allow(k_col_fwd<true, false>, colf_smem_);
+    allow(k_col_bwd<true, false>, colb_smem_);
+    allow(k_plane_inv_epi<true, false>, plane_smem_);
+  }
+  if (multi && tensor) {
+    allow(k_col_fwd<true, true>, colf_smem_);
+    allow(k_col_bwd<true, true>, colb_smem_);
+    allow(k_plane_inv_epi<true, true>, plane_smem_);
+  }
+  fusable_ = true;
+  fused_ = true;
+}
+
+void Engine::set_fused(bool on) {
+  if (on && !fusable_)
+    throw Error(-1, "fused transforms need a mixed-precision engine on a power-of-two grid whose (y, z) plane "
+                    "fits in shared memory");
+  fused_ = on;
 }
 
 void Engine::build_plans() {
@@ -291,9 +390,8 @@ void Engine::forward_stage(const double* in, R* chan_out, double* mean_out, cuda
   C2* chan_k = static_cast<C2*>(chan_k_);
   if constexpr (mixed) {
     const dim3 gs(grid_stream_, p.batch);
-    k_species_sums<<<gs, 256, 0, stream>>>(in, p.N, p.S, partials_);
-    k_split_convert<<<gs, 256, 0, stream>>>(in, p.N, p.S, partials_, grid_stream_, static_cast<float*>(rho_lo_),
-                                            mean_out);
+    k_species_mean<<<gs, 256, 0, stream>>>(in, p.N, p.S, partials_, sync_, mean_out);
+    k_split_convert<<<gs, 256, 0, stream>>>(in, p.N, p.S, static_cast<float*>(rho_lo_), mean_out);
     mark(1, stream);
     CDFT_CUFFT(cufftExecR2C(plan_rho_, static_cast<float*>(rho_lo_), reinterpret_cast<cufftComplex*>(rho_k)));
   } else {
@@ -320,7 +418,8 @@ void Engine::forward_stage(const double* in, R* chan_out, double* mean_out, cuda
 // Stages 5-7: out += c2r(sum_c conj(W_c) r2c(deriv_c)) dV - mu dV (+ the
 // FP64 constants of the split derivative channels, `dbar`).
 template <typename R, typename C2>
-void Engine::backward_stage(R* deriv, const double* dbar, double* out, const MuArgs& mu, cudaStream_t stream) {
+void Engine::backward_stage(R* deriv, const double* dbar, double* out, const MuArgs& mu, const FinalArgs& fin,
+                            cudaStream_t stream) {
   const EvalParams& p = p_;
   constexpr bool mixed = sizeof(R) == sizeof(float);
   C2* deriv_k = static_cast<C2*>(deriv_k_);
@@ -346,11 +445,71 @@ void Engine::backward_stage(R* deriv, const double* dbar, double* out, const MuA
     CDFT_CUFFT(cufftExecZ2D(plan_force_, reinterpret_cast<cufftDoubleComplex*>(force_k),
                             reinterpret_cast<double*>(hs_r)));
   mark(8, stream);
-  if (!multi && !tensor) k_epilogue<false, false, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu);
-  if (!multi && tensor) k_epilogue<false, true, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu);
-  if (multi && !tensor) k_epilogue<true, false, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu);
-  if (multi && tensor) k_epilogue<true, true, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu);
+  if (!multi && !tensor) k_epilogue<false, false, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu, fin);
+  if (!multi && tensor) k_epilogue<false, true, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu, fin);
+  if (multi && !tensor) k_epilogue<true, false, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu, fin);
+  if (multi && tensor) k_epilogue<true, true, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu, fin);
   CDFT_CUDA(cudaGetLastError());
+  mark(9, stream);
+}
+
+// Fused transform path, stages 1-3: species means, plane pass of rho, column
+// pass with the channel products, inverse plane pass of every channel.
+void Engine::fused_forward(const double* rho, cudaStream_t stream) {
+  const EvalParams& p = p_;
+  const dim3 gs(grid_stream_, p.batch);
+  k_species_mean<<<gs, 256, 0, stream>>>(rho, p.N, p.S, partials_, sync_, mean_);
+  mark(1, stream);
+  fft::cpx* prho = static_cast<fft::cpx*>(rho_k_);
+  fft::cpx* q = static_cast<fft::cpx*>(chan_k_);
+  k_plane_fwd<double><<<dim3(p.nx, p.S, p.batch), kPlaneThreads, plane_smem_, stream>>>(p, rho, p.S, mean_, prho,
+                                                                                        tables_);
+  mark(2, stream);
+  const dim3 gc(col_tiles_, p.batch);
+  const bool multi = p.L.multi, tensor = p.L.tensor;
+  if (!multi && !tensor)
+    k_col_fwd<false, false><<<gc, kColThreads, colf_smem_, stream>>>(p, prho, mf_w_, q, tq_, tables_);
+  if (!multi && tensor)
+    k_col_fwd<false, true><<<gc, kColThreads, colf_smem_, stream>>>(p, prho, mf_w_, q, tq_, tables_);
+  if (multi && !tensor)
+    k_col_fwd<true, false><<<gc, kColThreads, colf_smem_, stream>>>(p, prho, mf_w_, q, tq_, tables_);
+  if (multi && tensor)
+    k_col_fwd<true, true><<<gc, kColThreads, colf_smem_, stream>>>(p, prho, mf_w_, q, tq_, tables_);
+  mark(3, stream);
+  k_plane_inv<<<dim3(p.nx, p.n_chan, p.batch), kPlaneThreads, plane_smem_, stream>>>(
+      p, q, p.n_chan, static_cast<float*>(chan_r_), tables_);
+  CDFT_CUDA(cudaGetLastError());
+  mark(4, stream);
+}
+
+// Fused transform path, stages 5-8: plane pass of every derivative channel,
+// column pass with the back-convolution, inverse plane pass with the
+// epilogue and the scalars.
+void Engine::fused_backward(double* force, const MuArgs& mu, const FinalArgs& fin, cudaStream_t stream) {
+  const EvalParams& p = p_;
+  fft::cpx* pd = static_cast<fft::cpx*>(deriv_k_);
+  fft::cpx* pf = static_cast<fft::cpx*>(force_k_);
+  k_plane_fwd<float><<<dim3(p.nx, p.L.n_deriv, p.batch), kPlaneThreads, plane_smem_, stream>>>(
+      p, static_cast<const float*>(deriv_r_), p.L.n_deriv, nullptr, pd, tables_);
+  mark(6, stream);
+  const dim3 gc(col_tiles_, p.batch);
+  const dim3 gpl(p.nx, p.S, p.batch);
+  const bool multi = p.L.multi, tensor = p.L.tensor;
+  if (!multi && !tensor) k_col_bwd<false, false><<<gc, kColThreads, colb_smem_, stream>>>(p, pd, pf, tq_, tables_);
+  if (!multi && tensor) k_col_bwd<false, true><<<gc, kColThreads, colb_smem_, stream>>>(p, pd, pf, tq_, tables_);
+  if (multi && !tensor) k_col_bwd<true, false><<<gc, kColThreads, colb_smem_, stream>>>(p, pd, pf, tq_, tables_);
+  if (multi && tensor) k_col_bwd<true, true><<<gc, kColThreads, colb_smem_, stream>>>(p, pd, pf, tq_, tables_);
+  mark(7, stream);
+  if (!multi && !tensor)
+    k_plane_inv_epi<false, false><<<gpl, kPlaneThreads, plane_smem_, stream>>>(p, pf, dbar_, force, mu, fin, tables_);
+  if (!multi && tensor)
+    k_plane_inv_epi<false, true><<<gpl, kPlaneThreads, plane_smem_, stream>>>(p, pf, dbar_, force, mu, fin, tables_);
+  if (multi && !tensor)
+    k_plane_inv_epi<true, false><<<gpl, kPlaneThreads, plane_smem_, stream>>>(p, pf, dbar_, force, mu, fin, tables_);
+  if (multi && tensor)
+    k_plane_inv_epi<true, true><<<gpl, kPlaneThreads, plane_smem_, stream>>>(p, pf, dbar_, force, mu, fin, tables_);
+  CDFT_CUDA(cudaGetLastError());
+  mark(8, stream);
   mark(9, stream);
 }
 
@@ -369,9 +528,14 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
     rho = h_rho_;
   }
   timing_run_ = timing_;
+  if (timing_run_ && ring_used_ == kTimingRing) harvest_stage_times();
   mark(0, stream);
+  const bool fused = mixed && fused_;
   // 1-3. weighted densities
-  forward_stage<R, C2>(rho, chan_r, mean_, stream);
+  if (fused)
+    fused_forward(rho, stream);
+  else
+    forward_stage<R, C2>(rho, chan_r, mean_, stream);
   // 4. pointwise Phi / dPhi + local terms + reductions
   PointwiseArgs a;
   a.rho = rho;
@@ -404,20 +568,16 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   MuArgs ma;
   for (int b = 0; b < kMaxBatch; ++b)
     for (int s = 0; s < kMaxSpecies; ++s) ma.mu[b][s] = (b < p.batch && s < p.S) ? mu[b * p.S + s] : 0.0;
-  backward_stage<R, C2>(deriv_r, dbar_, force, ma, stream);
-  // 8. scalars, one block per problem
-  k_reduce_final<<<p.batch, 32 * (4 + kMaxSpecies), 0, stream>>>(partials_, pw_blocks, p, ma, err_, scalars);
-  CDFT_CUDA(cudaGetLastError());
+  // 8. scalars: block 0 of each problem's epilogue reduces the partials
+  FinalArgs fin{partials_, pw_blocks, err_, scalars};
+  if (fused)
+    fused_backward(force, ma, fin, stream);
+  else
+    backward_stage<R, C2>(deriv_r, dbar_, force, ma, fin, stream);
   mark(10, stream);
   if (timing_run_) {
     timing_run_ = false;
-    CDFT_CUDA(cudaEventSynchronize(stage_ev_[kStages]));
-    for (int i = 0; i < kStages; ++i) {
-      float ms = 0.0f;
-      CDFT_CUDA(cudaEventElapsedTime(&ms, stage_ev_[i], stage_ev_[i + 1]));
-      stage_ms_[i] += ms;
-    }
-    ++stage_count_;
+    ++ring_used_;
   }
 }
 
@@ -465,7 +625,7 @@ void Engine::run_hvp(const double* rho, const double* v, const double* mu, doubl
   });
   CDFT_CUDA(cudaGetLastError());
   MuArgs zero{};  // the Hessian does not depend on mu
-  backward_stage<R, C2>(deriv_r, tan_dbar_, hv, zero, stream);
+  backward_stage<R, C2>(deriv_r, tan_dbar_, hv, zero, FinalArgs{nullptr, 0, nullptr, nullptr}, stream);
   (void)mu;
 }
 

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "cdft_common.cuh"
+#include "fft_core.cuh"
 
 namespace cdft {
 
@@ -62,18 +63,27 @@ class Engine {
   long long points() const { return p_.N; }
   long long modes() const { return p_.Nk; }
   int precision() const { return precision_; }
+  // Transform path: the fused plane/column kernels (mixed precision on
+  // power-of-two grids whose (y, z) plane fits in shared memory; on by
+  // default there) or cuFFT plans with separate k-space kernels.
+  bool fusable() const { return fusable_; }
+  bool fused() const { return fused_; }
+  void set_fused(bool on);
   double a_vdw(int m) const { return a_vdw_[m]; }
-  int kernels_per_eval() const { return precision_ == 1 ? 7 : 5; }
+  int kernels_per_eval() const { return precision_ == 1 ? (fused_ ? 8 : 6) : 4; }
   // Reads and clears the device error word (synchronises the stream).
   int take_error(cudaStream_t stream);
 
   // Stage timing: when on, every evaluate() records CUDA events between its
-  // stages on its stream and synchronises at the end to accumulate the
-  // durations (kStages of them, in pipeline order):
+  // stages on its stream (one set of a ring of kTimingRing sets per
+  // evaluation, so timed evaluations still queue back to back); the ring is
+  // harvested when full and by take_stage_times.  Durations (kStages of
+  // them, in pipeline order):
   //   0 split / FP32 conversion (mixed), 1 r2c rho, 2 k_forward, 3 c2r channels,
-  //   4 pointwise, 5 r2c derivatives, 6 k_backward, 7 c2r force, 8 epilogue,
-  //   9 final reduction.
+  //   4 pointwise, 5 r2c derivatives, 6 k_backward, 7 c2r force, 8 epilogue
+  //   (with the final reduction), 9 (empty: the reduction is folded into 8).
   static constexpr int kStages = 10;
+  static constexpr int kTimingRing = 64;
   void set_stage_timing(bool on);
   // Accumulated milliseconds per stage and the number of timed evaluations;
   // clears the accumulators.
@@ -93,6 +103,9 @@ class Engine {
   template <class F>
   void with_kernels(bool mixed, F&& f) const;
   void upload_mean_field(const EngineSpec& spec);
+  void setup_fused();
+  void fused_forward(const double* rho, cudaStream_t stream);
+  void fused_backward(double* force, const MuArgs& mu, const FinalArgs& fin, cudaStream_t stream);
   template <typename R, typename C2>
   void run(const double* rho, const double* vext, const double* mu, double* force, double* scalars,
            cudaStream_t stream);
@@ -101,7 +114,8 @@ class Engine {
   template <typename R, typename C2>
   void forward_stage(const double* in, R* chan_out, double* mean_out, cudaStream_t stream);
   template <typename R, typename C2>
-  void backward_stage(R* deriv, const double* dbar, double* out, const MuArgs& mu, cudaStream_t stream);
+  void backward_stage(R* deriv, const double* dbar, double* out, const MuArgs& mu, const FinalArgs& fin,
+                      cudaStream_t stream);
 
   EvalParams p_{};
   int precision_ = kFP64;
@@ -124,6 +138,7 @@ class Engine {
   double* dbar_ = nullptr;    // B * kMaxChannels derivative-channel constants (mixed precision)
   double* partials_ = nullptr;
   int* err_ = nullptr;        // device error word (set by bounded waits that gave up)
+  unsigned* sync_ = nullptr;  // B last-block counters of k_species_mean (zero between launches)
   void* tan_chan_ = nullptr;  // tangent channels of the exact HVP (allocated on first use)
   double* tan_mean_ = nullptr;
   double* tan_dbar_ = nullptr;
@@ -135,12 +150,21 @@ class Engine {
   void* fft_work_ = nullptr;
   size_t scratch_bytes_ = 0;
 
+  // fused transform path
+  bool fusable_ = false, fused_ = false;
+  int tq_ = 0, col_tiles_ = 0;
+  size_t plane_smem_ = 0, colf_smem_ = 0, colb_smem_ = 0;
+  void* tw_ = nullptr;
+  FftTables tables_{};
+
   cufftHandle plan_rho_ = 0, plan_chan_ = 0, plan_deriv_ = 0, plan_force_ = 0;
   bool plans_made_ = false;
 
   void mark(int i, cudaStream_t stream);
+  void harvest_stage_times();
   bool timing_ = false, timing_run_ = false;
-  cudaEvent_t stage_ev_[kStages + 1] = {};
+  std::vector<cudaEvent_t> stage_ev_;  // kTimingRing sets of kStages + 1
+  int ring_used_ = 0;                  // sets recorded and not yet harvested
   double stage_ms_[kStages] = {};
   long long stage_count_ = 0;
 

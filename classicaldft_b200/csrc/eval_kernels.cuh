@@ -12,7 +12,7 @@
 //   D_k = r2c(dPhi channels)                 convolution.hpp:31-49     cuFFT (batched)
 //   F_s(k) = sum_c conj(W_cs(k)) D_c(k)      hard_sphere.hpp:103-136   k_backward
 //   force_s += c2r(F_s) dV                   hard_sphere.hpp:250-253   cuFFT + k_epilogue
-//   F, Omega                                 functionals.hpp:64-95     k_reduce_final
+//   F, Omega                                 functionals.hpp:64-95     k_epilogue (block 0)
 //
 // W_cs(k) is generated analytically from |k| (weights.hpp:91-137) instead of
 // being read from stored tables, and the k-space products of all channels
@@ -344,35 +344,66 @@ __device__ __forceinline__ double warp_sum_partials(const double* __restrict__ p
   return __shfl_sync(0xffffffffu, v, 0);
 }
 
-// Mixed precision, step 1: per-block sums of each species' density.
-__global__ void __launch_bounds__(256) k_species_sums(const double* __restrict__ rho, long long N, int S,
-                                                      double* __restrict__ partials) {
+// Sum of `n` partials written by other blocks of the running grid (L2 loads,
+// fixed order; the caller has fenced).
+__device__ __forceinline__ double warp_sum_partials_cg(const double* partials, int n, int stride, int off) {
+  const int lane = threadIdx.x & 31;
+  double v = 0.0;
+  for (int b = lane; b < n; b += 32) v += __ldcg(partials + b * (long long)stride + off);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return __shfl_sync(0xffffffffu, v, 0);
+}
+
+// True in the one block of problem blockIdx.y that finishes last: every
+// block has stored (and fenced) its partials by then.  The counter returns
+// to zero for the next launch.
+__device__ __forceinline__ bool last_block_done(unsigned* counter) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned prev = atomicAdd(counter, 1u);
+    last = (prev == gridDim.x - 1);
+    if (last) *counter = 0u;
+  }
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// Mixed precision, step 1: each species' mean density.  Per-block sums, then
+// the last block to finish sums the partials (fixed order) into mean_out.
+__global__ void __launch_bounds__(256) k_species_mean(const double* __restrict__ rho, long long N, int S,
+                                                      double* __restrict__ partials, unsigned* __restrict__ counters,
+                                                      double* __restrict__ mean_out) {
   rho += (long long)blockIdx.y * S * N;
   partials += (long long)blockIdx.y * gridDim.x * S;
+  mean_out += blockIdx.y * kMaxSpecies;
   double acc[kMaxSpecies] = {0.0, 0.0, 0.0, 0.0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
 #pragma unroll
     for (int s = 0; s < kMaxSpecies; ++s)
       if (s < S) acc[s] += rho[s * N + i];
   block_reduce_store<kMaxSpecies>(acc, S, partials);
+  if (last_block_done(counters + blockIdx.y)) {
+    const int warp = threadIdx.x >> 5;
+    if (warp < S) {
+      const double v = warp_sum_partials_cg(partials, gridDim.x, S, warp);
+      if ((threadIdx.x & 31) == 0) mean_out[warp] = v / (double)N;
+    }
+  }
 }
 
-// Mixed precision, step 2: delta_rho = rho - mean in FP32; block 0 stores the means.
+// Mixed precision, step 2: delta_rho = rho - mean in FP32.
 __global__ void __launch_bounds__(256) k_split_convert(const double* __restrict__ rho, long long N, int S,
-                                                       const double* __restrict__ partials, int nblocks,
-                                                       float* __restrict__ out, double* __restrict__ mean_out) {
+                                                       float* __restrict__ out, const double* __restrict__ mean) {
   rho += (long long)blockIdx.y * S * N;
   out += (long long)blockIdx.y * S * N;
-  partials += (long long)blockIdx.y * nblocks * S;
-  mean_out += blockIdx.y * kMaxSpecies;
+  mean += blockIdx.y * kMaxSpecies;
   __shared__ double sm[kMaxSpecies];
-  const int warp = threadIdx.x >> 5;
-  if (warp < S) {
-    const double v = warp_sum_partials(partials, nblocks, S, warp);
-    if ((threadIdx.x & 31) == 0) sm[warp] = v / (double)N;
-  }
+  if (threadIdx.x < S) sm[threadIdx.x] = mean[threadIdx.x];
   __syncthreads();
-  if (blockIdx.x == 0 && threadIdx.x < S) mean_out[threadIdx.x] = sm[threadIdx.x];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
 #pragma unroll
     for (int s = 0; s < kMaxSpecies; ++s)
@@ -902,15 +933,58 @@ __global__ void __launch_bounds__(128) k_pointwise_hvp(EvalParams p, const RT* _
   }
 }
 
+// Final reduction of one problem: the pointwise kernel's partials into the
+// scalar block [F, Omega, F_id, F_ext, F_hs, F_mf, N_0 .. N_{S-1}]
+// (functionals.hpp:72-92), fixed summation order, one warp per term.
+__device__ __forceinline__ void reduce_final(const double* __restrict__ partials, int nblocks, const EvalParams& p,
+                                             const double* mu, const int* __restrict__ err, double* __restrict__ out) {
+  __shared__ double sh[4 + kMaxSpecies];
+  const int warp = threadIdx.x >> 5;
+  const int n_terms = p.n_terms;
+  if (warp < n_terms) {
+    const double v = warp_sum_partials(partials, nblocks, n_terms, warp);
+    if ((threadIdx.x & 31) == 0) sh[warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double dv = p.dv;
+    const double f_id = sh[kTermId] * dv;
+    const double f_ext = sh[kTermExt] * dv;
+    const double f_hs = sh[kTermHS] * dv;
+    const double f_mf = sh[kTermMF] * dv;
+    double F = 0.0;
+    F += f_id;
+    F += f_ext;
+    F += f_hs;
+    if (p.M > 0) F += f_mf;
+    double muN = 0.0;
+    for (int s = 0; s < p.S; ++s) muN += mu[s] * sh[kTermN0 + s] * dv;
+    const bool bad = err && *err != 0;  // a bounded wait gave up: poison the result
+    out[0] = bad ? __longlong_as_double(0x7ff8000000000000ll) : F;
+    out[1] = bad ? __longlong_as_double(0x7ff8000000000000ll) : F - muN;
+    out[2] = f_id;
+    out[3] = f_ext;
+    out[4] = f_hs;
+    out[5] = f_mf;
+    for (int s = 0; s < p.S; ++s) out[6 + s] = sh[kTermN0 + s] * dv;
+  }
+}
+
 // force_s += c2r(F_s) dV - mu_s dV (+ the FP64 constant of the split
-// derivative channels) (hard_sphere.hpp:250-253, ideal_gas.hpp:33).
+// derivative channels) (hard_sphere.hpp:250-253, ideal_gas.hpp:33).  Block 0
+// of each problem also finishes the scalars (the pointwise kernel, which
+// wrote the partials, completed before this launch).
 template <bool MULTI, bool TENSOR, typename RT>
 __global__ void __launch_bounds__(256) k_epilogue(EvalParams p, const RT* __restrict__ hs, const double* __restrict__ dbar,
-                                                  double* __restrict__ force, const __grid_constant__ MuArgs mu) {
+                                                  double* __restrict__ force, const __grid_constant__ MuArgs mu,
+                                                  FinalArgs fin) {
   using L = Lay<MULTI, TENSOR>;
   constexpr bool SPLIT = sizeof(RT) == sizeof(float);
   const int b = blockIdx.y;
   const long long N = p.N;
+  if (blockIdx.x == 0 && fin.scalars)
+    reduce_final(fin.partials + (long long)b * fin.nblocks * p.n_terms, fin.nblocks, p, mu.mu[b], fin.err,
+                 fin.scalars + b * kScalarCount);
   hs += (long long)b * p.S * N;
   force += (long long)b * p.S * N;
   dbar += b * kMaxChannels;
@@ -930,47 +1004,6 @@ __global__ void __launch_bounds__(256) k_epilogue(EvalParams p, const RT* __rest
     for (int s = 0; s < kMaxSpecies; ++s) {
       if (s < p.S) force[s * N + i] = force[s * N + i] + (double)hs[s * N + i] * p.dv + s_const[s];
     }
-}
-
-// Deterministic second reduction stage, one block per problem; writes the
-// scalar block [F, Omega, F_id, F_ext, F_hs, F_mf, N_0 .. N_{S-1}]
-// (functionals.hpp:72-92) of problem blockIdx.x.
-__global__ void k_reduce_final(const double* __restrict__ partials, int nblocks, EvalParams p,
-                               const __grid_constant__ MuArgs mu, const int* __restrict__ err,
-                               double* __restrict__ out) {
-  const int b = blockIdx.x;
-  partials += (long long)b * nblocks * p.n_terms;
-  out += b * kScalarCount;
-  __shared__ double sh[4 + kMaxSpecies];
-  const int warp = threadIdx.x >> 5;  // one warp per term
-  const int n_terms = p.n_terms;
-  if (warp < n_terms) {
-    const double v = warp_sum_partials(partials, nblocks, n_terms, warp);
-    if ((threadIdx.x & 31) == 0) sh[warp] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const double dv = p.dv;
-    const double f_id = sh[kTermId] * dv;
-    const double f_ext = sh[kTermExt] * dv;
-    const double f_hs = sh[kTermHS] * dv;
-    const double f_mf = sh[kTermMF] * dv;
-    double F = 0.0;
-    F += f_id;
-    F += f_ext;
-    F += f_hs;
-    if (p.M > 0) F += f_mf;
-    double muN = 0.0;
-    for (int s = 0; s < p.S; ++s) muN += mu.mu[b][s] * sh[kTermN0 + s] * dv;
-    const bool bad = err && *err != 0;  // a bounded wait gave up: poison the result
-    out[0] = bad ? __longlong_as_double(0x7ff8000000000000ll) : F;
-    out[1] = bad ? __longlong_as_double(0x7ff8000000000000ll) : F - muN;
-    out[2] = f_id;
-    out[3] = f_ext;
-    out[4] = f_hs;
-    out[5] = f_mf;
-    for (int s = 0; s < p.S; ++s) out[6 + s] = sh[kTermN0 + s] * dv;
-  }
 }
 
 }  // namespace cdft

@@ -285,6 +285,28 @@ class Engine:
 
     STAGES = ("split", "r2c_rho", "k_forward", "c2r_channels", "pointwise", "r2c_derivatives", "k_backward",
               "c2r_force", "epilogue", "reduce")
+    STAGES_FUSED = ("species_mean", "plane_fwd_rho", "col_fwd", "plane_inv_channels", "pointwise",
+                    "plane_fwd_derivatives", "col_bwd", "plane_inv_epilogue", "-8", "-9")
+
+    @property
+    def transforms(self) -> str:
+        """"fused" (hand-written plane/column FFT kernels) or "cufft"."""
+        t, a = ctypes.c_int(), ctypes.c_int()
+        _lib.check(_lib.lib().cdft_engine_transforms(self.handle, ctypes.byref(t), ctypes.byref(a)))
+        return "fused" if t.value == _lib.TRANSFORMS_FUSED else "cufft"
+
+    @property
+    def fused_available(self) -> bool:
+        t, a = ctypes.c_int(), ctypes.c_int()
+        _lib.check(_lib.lib().cdft_engine_transforms(self.handle, ctypes.byref(t), ctypes.byref(a)))
+        return bool(a.value)
+
+    def set_transforms(self, which: str):
+        """Select "fused" (where available) or "cufft"; ValueError if fused is unavailable."""
+        if which not in ("fused", "cufft"):
+            raise ValueError("transforms: 'fused' or 'cufft'")
+        _lib.check(_lib.lib().cdft_engine_set_transforms(
+            self.handle, _lib.TRANSFORMS_FUSED if which == "fused" else _lib.TRANSFORMS_CUFFT))
 
     def stage_timing(self, on: bool = True):
         """Record CUDA events between the evaluation stages (synchronises each evaluation)."""
@@ -295,7 +317,8 @@ class Engine:
         ms = (ctypes.c_double * len(self.STAGES))()
         n = ctypes.c_longlong()
         _lib.check(_lib.lib().cdft_engine_stage_times(self.handle, ms, ctypes.byref(n)))
-        return dict(zip(self.STAGES, list(ms))), n.value
+        names = self.STAGES_FUSED if self.transforms == "fused" else self.STAGES
+        return dict(zip(names, list(ms))), n.value
 
     def total_device(self, rho_ptr: int, vext_ptr, mu, force_ptr: int, scalars_ptr: int, stream: int = 0):
         """cdft_total_device on device pointers (ints, e.g. torch.Tensor.data_ptr())."""

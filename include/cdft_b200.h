@@ -366,17 +366,32 @@ CDFT_API int cdft_local_terms_noalloc(const double* rho, const double* vext, con
 
 /* Stage timing (a measurement hook; no reference counterpart).  With `on`,
  * every evaluation records CUDA events between its stages on its own stream
- * and synchronises at its end to accumulate the stage durations; off by
- * default (then evaluations are fully asynchronous).  The stages, in order:
+ * (a ring of 64 event sets: evaluations still queue back to back; the host
+ * waits only when the ring is full); off by default.  The stages, in order:
  * 0 split / FP32 conversion (mixed), 1 r2c rho, 2 k_forward, 3 c2r channels,
- * 4 pointwise, 5 r2c derivatives, 6 k_backward, 7 c2r force, 8 epilogue,
- * 9 final reduction. */
+ * 4 pointwise, 5 r2c derivatives, 6 k_backward, 7 c2r force, 8 epilogue
+ * (which also finishes the scalars), 9 reserved (empty). */
 #define CDFT_STAGE_COUNT 10
 CDFT_API int cdft_engine_stage_timing(cdft_engine* engine, int on);
 
 /* Accumulated milliseconds per stage since the last call, and the number of
  * timed evaluations; clears the accumulators. */
 CDFT_API int cdft_engine_stage_times(cdft_engine* engine, double ms[CDFT_STAGE_COUNT], long long* evaluations);
+
+/* Transform implementation of an engine (no reference counterpart; the
+ * reference uses FFTW).  CDFT_TRANSFORMS_FUSED: hand-written plane / column
+ * FFT kernels with the k-space stages fused into the column pass, available
+ * for mixed-precision engines on power-of-two grids (each dimension 2..256,
+ * nz >= 4) whose (y, z) plane fits in shared memory, and the default there.
+ * CDFT_TRANSFORMS_CUFFT: cuFFT plans with separate k-space kernels (every
+ * other engine, and the exact HVP always).  Selecting FUSED where it is not
+ * available is CDFT_ERR_INVALID. */
+#define CDFT_TRANSFORMS_CUFFT 0
+#define CDFT_TRANSFORMS_FUSED 1
+CDFT_API int cdft_engine_set_transforms(cdft_engine* engine, int transforms);
+
+/* The current transform implementation and whether FUSED is available. */
+CDFT_API int cdft_engine_transforms(const cdft_engine* engine, int* transforms, int* fused_available);
 
 /* Status of earlier asynchronous calls on `stream`: CDFT_ERR_RUNTIME if a
  * bounded device-side wait gave up (the scalars of that call are NaN), else

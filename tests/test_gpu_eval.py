@@ -187,20 +187,23 @@ def test_tma_and_plain_pointwise_paths_agree():
     assert rel_err(s1[0], r.free_energy) <= F_TOL
 
 
-def test_stage_timing_hook_records_every_stage_and_changes_nothing():
+@pytest.mark.parametrize("transforms", ["cufft", "fused"])
+def test_stage_timing_hook_records_every_stage_and_changes_nothing(transforms):
     pr = Problem((32, 32, 32), 0.2, [1.0], "WhiteBearII", inters=[(0, 0) + LJ], kT=0.8, precision=cd.MIXED)
     rho = profile(pr.N, (32, 32, 32), 13, 0.35, 0.1)
     e = pr.weights.engine
+    e.set_transforms(transforms)
     plain = pr.gpu([rho], [0.2])
     e.stage_timing(True)
     e.stage_times()
-    timed = [pr.gpu([rho], [0.2]) for _ in range(3)]
+    timed = [pr.gpu([rho], [0.2]) for _ in range(70)]  # more than the 64-set event ring
     ms, n = e.stage_times()
     e.stage_timing(False)
-    assert n == 3
-    assert set(ms) == set(cd.Engine.STAGES)
+    assert n == 70
+    names = cd.Engine.STAGES if transforms == "cufft" else cd.Engine.STAGES_FUSED
+    assert set(ms) == set(names)
     assert all(v >= 0.0 for v in ms.values())
-    assert ms["pointwise"] > 0.0 and ms["c2r_channels"] > 0.0 and ms["split"] > 0.0
+    assert all(ms[k] > 0.0 for k in names[:8])
     for t in timed:
         assert t.free_energy == plain.free_energy
         assert np.array_equal(t.forces[0], plain.forces[0])

@@ -1,0 +1,104 @@
+"""The fused transform path (hand-written plane / column FFT kernels with the
+k-space stages in the column pass) against the FP64 oracle and against the
+cuFFT path of the same engine.
+
+Tolerances are those of the mixed-precision specification (both paths run
+their transforms in FP32): near-uniform states |dF|/|F| <= 1e-9 and forces
+1e-6 of their max; 10%-noise states |dF|/|F| <= 1e-6 and forces 1e-4.  On
+top, the fused path's error may exceed the cuFFT path's by at most a factor
+of 10 (same arithmetic precision; radix-4 stages and the R2C post-processing
+round more often than cuFFT's kernels) unless it is below 5% of the
+tolerance.
+"""
+import numpy as np
+import pytest
+
+import classicaldft_b200 as cd
+from tests.parity import Problem, force_err, rel_err, smooth_noise
+
+pytestmark = pytest.mark.gpu
+LJ = (1.0, 1.0, 2.5)
+
+
+def both_paths(pr, rhos, mus, vexts=None):
+    e = pr.weights.engine
+    assert e.transforms == "fused"
+    fused = pr.gpu(rhos, mus, vexts)
+    e.set_transforms("cufft")
+    cufft = pr.gpu(rhos, mus, vexts)
+    e.set_transforms("fused")
+    return fused, cufft
+
+
+def test_path_selection():
+    g32 = Problem((32, 32, 32), 0.2, [1.0], "WhiteBearII", precision=cd.MIXED)
+    assert g32.weights.engine.fused_available and g32.weights.engine.transforms == "fused"
+    g64 = Problem((16, 16, 16), 0.2, [1.0], "WhiteBearII", precision=cd.FP64)
+    assert not g64.weights.engine.fused_available and g64.weights.engine.transforms == "cufft"
+    odd = Problem((24, 24, 24), 0.2, [1.0], "WhiteBearII", precision=cd.MIXED)
+    assert not odd.weights.engine.fused_available and odd.weights.engine.transforms == "cufft"
+    with pytest.raises(ValueError):
+        odd.weights.engine.set_transforms("fused")
+    assert g32.weights.engine.info["kernels_per_eval"] == 8
+
+
+CASES = [
+    ((32, 32, 32), 0.2, [1.0], "WhiteBearII", [(0, 0) + LJ]),
+    ((64, 64, 64), 0.1, [1.0], "RSLT", []),
+    ((16, 32, 64), 0.2, [1.0], "WhiteBearI", [(0, 0) + LJ]),
+    ((64, 16, 8), 0.2, [1.0], "Rosenfeld", [(0, 0) + LJ]),
+    ((32, 16, 32), 0.2, [1.0, 0.6], "esFMT", [(0, 0) + LJ, (0, 1, 1.0, 0.8, 2.5), (1, 1, 0.8, 0.5, 2.0)]),
+    ((16, 16, 32), 0.2, [1.0, 0.7], "Rosenfeld", [(0, 1, 1.0, 0.8, 2.5)]),
+]
+
+
+@pytest.mark.parametrize("shape,dx,diam,model,inters", CASES)
+def test_fused_matches_oracle_and_cufft_path(shape, dx, diam, model, inters):
+    pr = Problem(shape, dx, diam, model, A=1.0, B=0.1, inters=inters, kT=0.9, precision=cd.MIXED)
+    rng = np.random.default_rng(sum(shape))
+    S = len(diam)
+    for amp, f_tol, force_tol in ((0.01, 1e-9, 1e-6), (0.1, 1e-6, 1e-4)):
+        rhos = [0.3 / S * (1.0 + amp * smooth_noise(shape, rng)) for _ in range(S)]
+        vexts = [0.2 * smooth_noise(shape, rng) for _ in range(S)]
+        mus = list(rng.uniform(-1.0, 1.0, S))
+        fused, cufft = both_paths(pr, rhos, mus, vexts)
+        ref = pr.ref(rhos, mus, vexts)
+        ef = rel_err(fused.free_energy, ref.free_energy)
+        ec = rel_err(cufft.free_energy, ref.free_energy)
+        assert ef <= f_tol
+        assert rel_err(fused.grand_potential, ref.grand_potential) <= f_tol
+        pf, pc = force_err(fused.forces, ref.forces), force_err(cufft.forces, ref.forces)
+        assert pf <= force_tol
+        assert pf <= max(10.0 * pc, 0.05 * force_tol)
+        assert ef <= max(10.0 * ec, 0.05 * f_tol)
+
+
+def test_fused_batch_and_unaligned_buffers():
+    import torch
+    shape = (32, 32, 32)
+    pr = Problem(shape, 0.2, [1.0], "WhiteBearII", inters=[(0, 0) + LJ], kT=0.8, precision=cd.MIXED)
+    rng = np.random.default_rng(11)
+    B = 3
+    rho = np.stack([0.35 * (1.0 + 0.05 * smooth_noise(shape, rng)) for _ in range(B)])
+    mus = [0.1, -0.4, 0.9]
+    wb = cd.make_weights(pr.fmt, pr.model, cd.MIXED, batch=B)
+    assert wb.engine.transforms == "fused"
+    res = cd.total_batch(pr.model, rho, wb, mus)
+    for b in range(B):
+        one = pr.gpu([rho[b]], [mus[b]])
+        assert rel_err(res[b].free_energy, one.free_energy) <= 1e-13
+        assert force_err(res[b].forces, one.forces) <= 1e-12
+    # rho, vext and force only 8-byte aligned on the device API
+    N = pr.N
+    e = pr.weights.engine
+    v = 0.3 * smooth_noise(shape, rng)
+    buf = torch.zeros(3 * N + 3, dtype=torch.float64, device="cuda")
+    buf[1:N + 1] = torch.tensor(rho[0])
+    buf[N + 2:2 * N + 2] = torch.tensor(v)
+    sc = torch.empty(10, dtype=torch.float64, device="cuda")
+    e.total_device(buf[1:].data_ptr(), buf[N + 2:].data_ptr(), [mus[0]], buf[2 * N + 3:].data_ptr(), sc.data_ptr(),
+                   0)
+    torch.cuda.synchronize()
+    ref = pr.gpu([rho[0]], [mus[0]], [v])
+    assert rel_err(float(sc[0]), ref.free_energy) <= 1e-13
+    assert force_err([buf[2 * N + 3:].cpu().numpy()], ref.forces) <= 1e-12
