@@ -2,7 +2,7 @@
 // evaluation pipeline of one F[rho] + dF/drho call.
 #include "engine.cuh"
 #include "eval_kernels.cuh"
-#include "fft_kernels.cuh"
+#include "fused.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -199,7 +199,7 @@ Engine::~Engine() {
   for (void* q : {rho_k_, chan_k_, chan_r_, deriv_r_, deriv_k_, force_k_, hs_r_, rho_lo_, (void*)mf_w_,
                   (void*)mean_, (void*)dbar_, (void*)err_, (void*)sync_, tan_chan_, (void*)tan_mean_, (void*)tan_dbar_,
                   (void*)tan_in_,
-                  (void*)partials_, fft_work_, tw_, (void*)h_rho_, (void*)h_vext_, (void*)h_force_, (void*)h_scalars_})
+                  (void*)partials_, fft_work_, tw_, (void*)wtab_, (void*)h_rho_, (void*)h_vext_, (void*)h_force_, (void*)h_scalars_})
     if (q) cudaFree(q);
   if (stream_) cudaStreamDestroy(stream_);
   for (cudaEvent_t e : stage_ev_)
@@ -245,28 +245,13 @@ long long Engine::take_stage_times(double* ms) {
   return n;
 }
 
-// The fused transform path (fft_kernels.cuh) serves mixed-precision engines
-// on power-of-two grids whose (y, z) plane fits in shared memory with two
-// CTAs per SM; everything else (and the HVP) uses the cuFFT plans.
+// The fused transform path (fused.cu) serves mixed-precision engines on the
+// grids it has specialisations for; everything else (and the HVP) uses the
+// cuFFT plans.
 void Engine::setup_fused() {
   const EvalParams& p = p_;
-  auto pow2 = [](int n) { return n >= 2 && (n & (n - 1)) == 0; };
   fusable_ = false;
-  if (precision_ != kMixed || !pow2(p.nx) || !pow2(p.ny) || !pow2(p.nz) || p.nz < 4 || p.nx > 256 || p.ny > 256 ||
-      p.nz > 256)
-    return;
-  const size_t kSmemCap = 110 * 1024;
-  plane_smem_ = plane_smem_bytes(p.ny, p.nz);
-  if (plane_smem_ > kSmemCap) return;
-  const int nbuf_f = p.S + p.n_chan, nbuf_b = p.L.n_deriv;
-  int tq = 16;
-  while (tq >= 1 && (col_smem_bytes(p.nx, tq, nbuf_f) > kSmemCap || col_smem_bytes(p.nx, tq, nbuf_b) > kSmemCap))
-    tq /= 2;
-  if (tq < 1) return;
-  tq_ = tq;
-  colf_smem_ = col_smem_bytes(p.nx, tq, nbuf_f);
-  colb_smem_ = col_smem_bytes(p.nx, tq, nbuf_b);
-  col_tiles_ = (int)(((long long)p.ny * p.nzh + tq - 1) / tq);
+  if (precision_ != kMixed || !fused_plan(p, &plan_)) return;
   // twiddle tables, FP64-rounded
   std::vector<fft::cpx> tw;
   auto table = [&](int M) {
@@ -283,33 +268,9 @@ void Engine::setup_fused() {
   CDFT_CUDA(cudaMemcpy(tw_, tw.data(), sizeof(fft::cpx) * tw.size(), cudaMemcpyHostToDevice));
   const fft::cpx* t = static_cast<const fft::cpx*>(tw_);
   tables_ = FftTables{t, t + p.nx, t + p.nx + p.ny, t + p.nx + p.ny + p.nz / 2};
-  auto allow = [](auto kern, size_t bytes) {
-    CDFT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  };
-  allow(k_plane_fwd<double>, plane_smem_);
-  allow(k_plane_fwd<float>, plane_smem_);
-  allow(k_plane_inv, plane_smem_);
-  const bool multi = p.L.multi, tensor = p.L.tensor;
-  if (!multi && !tensor) {
-    allow(k_col_fwd<false, false>, colf_smem_);
-    allow(k_col_bwd<false, false>, colb_smem_);
-    allow(k_plane_inv_epi<false, false>, plane_smem_);
-  }
-  if (!multi && tensor) {
-    allow(k_col_fwd<false, true>, colf_smem_);
-    allow(k_col_bwd<false, true>, colb_smem_);
-    allow(k_plane_inv_epi<false, true>, plane_smem_);
-  }
-  if (multi && !tensor) {
-    allow(k_col_fwd<true, false>, colf_smem_);
-    allow(k_col_bwd<true, false>, colb_smem_);
-    allow(k_plane_inv_epi<true, false>, plane_smem_);
-  }
-  if (multi && tensor) {
-    allow(k_col_fwd<true, true>, colf_smem_);
-    allow(k_col_bwd<true, true>, colb_smem_);
-    allow(k_plane_inv_epi<true, true>, plane_smem_);
-  }
+  CDFT_CUDA(cudaMalloc(&wtab_, sizeof(float) * fused_weight_table_floats(p)));
+  fused_build_weights(p, wtab_, nullptr);
+  CDFT_CUDA(cudaDeviceSynchronize());
   fusable_ = true;
   fused_ = true;
 }
@@ -462,23 +423,11 @@ void Engine::fused_forward(const double* rho, cudaStream_t stream) {
   mark(1, stream);
   fft::cpx* prho = static_cast<fft::cpx*>(rho_k_);
   fft::cpx* q = static_cast<fft::cpx*>(chan_k_);
-  k_plane_fwd<double><<<dim3(p.nx, p.S, p.batch), kPlaneThreads, plane_smem_, stream>>>(p, rho, p.S, mean_, prho,
-                                                                                        tables_);
+  fused_plane_fwd_rho(plan_, p, rho, mean_, prho, tables_, stream);
   mark(2, stream);
-  const dim3 gc(col_tiles_, p.batch);
-  const bool multi = p.L.multi, tensor = p.L.tensor;
-  if (!multi && !tensor)
-    k_col_fwd<false, false><<<gc, kColThreads, colf_smem_, stream>>>(p, prho, mf_w_, q, tq_, tables_);
-  if (!multi && tensor)
-    k_col_fwd<false, true><<<gc, kColThreads, colf_smem_, stream>>>(p, prho, mf_w_, q, tq_, tables_);
-  if (multi && !tensor)
-    k_col_fwd<true, false><<<gc, kColThreads, colf_smem_, stream>>>(p, prho, mf_w_, q, tq_, tables_);
-  if (multi && tensor)
-    k_col_fwd<true, true><<<gc, kColThreads, colf_smem_, stream>>>(p, prho, mf_w_, q, tq_, tables_);
+  fused_col_fwd(plan_, p, prho, mf_w_, wtab_, q, tables_, stream);
   mark(3, stream);
-  k_plane_inv<<<dim3(p.nx, p.n_chan, p.batch), kPlaneThreads, plane_smem_, stream>>>(
-      p, q, p.n_chan, static_cast<float*>(chan_r_), tables_);
-  CDFT_CUDA(cudaGetLastError());
+  fused_plane_inv(plan_, p, q, static_cast<float*>(chan_r_), tables_, stream);
   mark(4, stream);
 }
 
@@ -489,26 +438,11 @@ void Engine::fused_backward(double* force, const MuArgs& mu, const FinalArgs& fi
   const EvalParams& p = p_;
   fft::cpx* pd = static_cast<fft::cpx*>(deriv_k_);
   fft::cpx* pf = static_cast<fft::cpx*>(force_k_);
-  k_plane_fwd<float><<<dim3(p.nx, p.L.n_deriv, p.batch), kPlaneThreads, plane_smem_, stream>>>(
-      p, static_cast<const float*>(deriv_r_), p.L.n_deriv, nullptr, pd, tables_);
+  fused_plane_fwd_deriv(plan_, p, static_cast<const float*>(deriv_r_), pd, tables_, stream);
   mark(6, stream);
-  const dim3 gc(col_tiles_, p.batch);
-  const dim3 gpl(p.nx, p.S, p.batch);
-  const bool multi = p.L.multi, tensor = p.L.tensor;
-  if (!multi && !tensor) k_col_bwd<false, false><<<gc, kColThreads, colb_smem_, stream>>>(p, pd, pf, tq_, tables_);
-  if (!multi && tensor) k_col_bwd<false, true><<<gc, kColThreads, colb_smem_, stream>>>(p, pd, pf, tq_, tables_);
-  if (multi && !tensor) k_col_bwd<true, false><<<gc, kColThreads, colb_smem_, stream>>>(p, pd, pf, tq_, tables_);
-  if (multi && tensor) k_col_bwd<true, true><<<gc, kColThreads, colb_smem_, stream>>>(p, pd, pf, tq_, tables_);
+  fused_col_bwd(plan_, p, pd, wtab_, pf, tables_, stream);
   mark(7, stream);
-  if (!multi && !tensor)
-    k_plane_inv_epi<false, false><<<gpl, kPlaneThreads, plane_smem_, stream>>>(p, pf, dbar_, force, mu, fin, tables_);
-  if (!multi && tensor)
-    k_plane_inv_epi<false, true><<<gpl, kPlaneThreads, plane_smem_, stream>>>(p, pf, dbar_, force, mu, fin, tables_);
-  if (multi && !tensor)
-    k_plane_inv_epi<true, false><<<gpl, kPlaneThreads, plane_smem_, stream>>>(p, pf, dbar_, force, mu, fin, tables_);
-  if (multi && tensor)
-    k_plane_inv_epi<true, true><<<gpl, kPlaneThreads, plane_smem_, stream>>>(p, pf, dbar_, force, mu, fin, tables_);
-  CDFT_CUDA(cudaGetLastError());
+  fused_plane_inv_epi(plan_, p, pf, dbar_, force, mu, fin, tables_, stream);
   mark(8, stream);
   mark(9, stream);
 }

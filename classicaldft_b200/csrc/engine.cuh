@@ -14,6 +14,7 @@
 
 #include "cdft_common.cuh"
 #include "fft_core.cuh"
+#include "fused.cuh"
 
 namespace cdft {
 
@@ -63,8 +64,8 @@ class Engine {
   long long points() const { return p_.N; }
   long long modes() const { return p_.Nk; }
   int precision() const { return precision_; }
-  // Transform path: the fused plane/column kernels (mixed precision on
-  // power-of-two grids whose (y, z) plane fits in shared memory; on by
+  // Transform path: the fused plane/column kernels (mixed precision on the
+  // grids fused.cu specialises: nx and ny, nz in {16, 32, 64, 128}; on by
   // default there) or cuFFT plans with separate k-space kernels.
   bool fusable() const { return fusable_; }
   bool fused() const { return fused_; }
@@ -152,9 +153,9 @@ class Engine {
 
   // fused transform path
   bool fusable_ = false, fused_ = false;
-  int tq_ = 0, col_tiles_ = 0;
-  size_t plane_smem_ = 0, colf_smem_ = 0, colb_smem_ = 0;
+  FusedPlan plan_{};
   void* tw_ = nullptr;
+  float* wtab_ = nullptr;  // column-pass weight table ([1 + 5 S][Nk] floats)
   FftTables tables_{};
 
   cufftHandle plan_rho_ = 0, plan_chan_ = 0, plan_deriv_ = 0, plan_force_ = 0;

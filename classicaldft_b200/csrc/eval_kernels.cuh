@@ -344,15 +344,36 @@ __device__ __forceinline__ double warp_sum_partials(const double* __restrict__ p
   return __shfl_sync(0xffffffffu, v, 0);
 }
 
-// Sum of `n` partials written by other blocks of the running grid (L2 loads,
-// fixed order; the caller has fenced).
-__device__ __forceinline__ double warp_sum_partials_cg(const double* partials, int n, int stride, int off) {
-  const int lane = threadIdx.x & 31;
+// Sum of `n` partials by the whole block (every thread takes a strided
+// share, then a fixed-order tree), so the latency is that of a few loads
+// rather than n / 32 dependent ones; the result goes to every thread.  CG:
+// L2 loads, for partials written by other blocks of the running grid (the
+// caller has fenced).  Call from every thread of the block.
+template <bool CG>
+__device__ __forceinline__ double block_sum_partials(const double* partials, int n, int stride, int off) {
+  __shared__ double sh[32];
+  __shared__ double total;
   double v = 0.0;
-  for (int b = lane; b < n; b += 32) v += __ldcg(partials + b * (long long)stride + off);
+  for (int b = threadIdx.x; b < n; b += blockDim.x) {
+    const double* q = partials + b * (long long)stride + off;
+    v += CG ? __ldcg(q) : *q;
+  }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  return __shfl_sync(0xffffffffu, v, 0);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    double u = lane < nw ? sh[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) u += __shfl_down_sync(0xffffffffu, u, o);
+    if (lane == 0) total = u;
+  }
+  __syncthreads();
+  const double r = total;
+  __syncthreads();  // sh / total free for the next call
+  return r;
 }
 
 // True in the one block of problem blockIdx.y that finishes last: every
@@ -374,7 +395,7 @@ __device__ __forceinline__ bool last_block_done(unsigned* counter) {
 
 // Mixed precision, step 1: each species' mean density.  Per-block sums, then
 // the last block to finish sums the partials (fixed order) into mean_out.
-__global__ void __launch_bounds__(256) k_species_mean(const double* __restrict__ rho, long long N, int S,
+static __global__ void __launch_bounds__(256) k_species_mean(const double* __restrict__ rho, long long N, int S,
                                                       double* __restrict__ partials, unsigned* __restrict__ counters,
                                                       double* __restrict__ mean_out) {
   rho += (long long)blockIdx.y * S * N;
@@ -387,16 +408,15 @@ __global__ void __launch_bounds__(256) k_species_mean(const double* __restrict__
       if (s < S) acc[s] += rho[s * N + i];
   block_reduce_store<kMaxSpecies>(acc, S, partials);
   if (last_block_done(counters + blockIdx.y)) {
-    const int warp = threadIdx.x >> 5;
-    if (warp < S) {
-      const double v = warp_sum_partials_cg(partials, gridDim.x, S, warp);
-      if ((threadIdx.x & 31) == 0) mean_out[warp] = v / (double)N;
+    for (int s = 0; s < S; ++s) {
+      const double v = block_sum_partials<true>(partials, gridDim.x, S, s);
+      if (threadIdx.x == 0) mean_out[s] = v / (double)N;
     }
   }
 }
 
 // Mixed precision, step 2: delta_rho = rho - mean in FP32.
-__global__ void __launch_bounds__(256) k_split_convert(const double* __restrict__ rho, long long N, int S,
+static __global__ void __launch_bounds__(256) k_split_convert(const double* __restrict__ rho, long long N, int S,
                                                        float* __restrict__ out, const double* __restrict__ mean) {
   rho += (long long)blockIdx.y * S * N;
   out += (long long)blockIdx.y * S * N;
@@ -935,15 +955,14 @@ __global__ void __launch_bounds__(128) k_pointwise_hvp(EvalParams p, const RT* _
 
 // Final reduction of one problem: the pointwise kernel's partials into the
 // scalar block [F, Omega, F_id, F_ext, F_hs, F_mf, N_0 .. N_{S-1}]
-// (functionals.hpp:72-92), fixed summation order, one warp per term.
+// (functionals.hpp:72-92), fixed summation order, the whole block per term.
 __device__ __forceinline__ void reduce_final(const double* __restrict__ partials, int nblocks, const EvalParams& p,
                                              const double* mu, const int* __restrict__ err, double* __restrict__ out) {
   __shared__ double sh[4 + kMaxSpecies];
-  const int warp = threadIdx.x >> 5;
   const int n_terms = p.n_terms;
-  if (warp < n_terms) {
-    const double v = warp_sum_partials(partials, nblocks, n_terms, warp);
-    if ((threadIdx.x & 31) == 0) sh[warp] = v;
+  for (int t = 0; t < n_terms; ++t) {
+    const double v = block_sum_partials<false>(partials, nblocks, n_terms, t);
+    if (threadIdx.x == 0) sh[t] = v;
   }
   __syncthreads();
   if (threadIdx.x == 0) {

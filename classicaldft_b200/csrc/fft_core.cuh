@@ -1,7 +1,8 @@
 // In-place power-of-two FFT building blocks for the fused transform path
-// (fft_kernels.cuh): radix-4 stages (one radix-2 stage when log2 M is odd),
-// decimation in frequency (natural order in, digit-reversed order out) and in
-// time (digit-reversed in, natural out), plus the real<->half-complex
+// (fft_kernels.cuh): radix-16 stages, then one radix-8, -4 or -2 stage for
+// the rest (128 = 16 x 8, 64 = 16 x 4, 32 = 16 x 2), each butterfly an
+// in-register DFT; decimation in frequency (natural order in, digit-reversed
+// order out) and in time (digit-reversed in, natural out), plus the real<->half-complex
 // pre/post-processing of a length-2M real transform done as a length-M
 // complex one.  Conventions are cuFFT's (and FFTW's): forward exp(-2 pi i
 // n k / M), inverse exp(+2 pi i n k / M), no normalisation.
@@ -13,10 +14,14 @@
 // arithmetic against numpy.
 #pragma once
 
+#include <utility>
+
 #ifdef __CUDACC__
 #define CDFT_HD __host__ __device__ __forceinline__
+#define CDFT_UNROLL _Pragma("unroll")
 #else
 #define CDFT_HD inline
+#define CDFT_UNROLL
 #endif
 
 namespace cdft {
@@ -34,25 +39,25 @@ CDFT_HD cpx mul_i(cpx a) { return {-a.y, a.x}; }   // i a
 CDFT_HD cpx mul_mi(cpx a) { return {a.y, -a.x}; }  // -i a
 CDFT_HD cpx scale(cpx a, float s) { return {a.x * s, a.y * s}; }
 
-CDFT_HD int ilog2(int n) {
+CDFT_HD constexpr int ilog2(int n) {
   int l = 0;
   while ((1 << l) < n) ++l;
   return l;
 }
 
-// Radix plan of a length-M transform (M = 2^m): stage s has radix 2 for s = 0
-// when m is odd, else 4.  Number of stages and radix of stage s.
-CDFT_HD int n_stages(int M) {
+// Radix plan of a length-M transform (M = 2^m): radix 16 for the first
+// m / 4 stages, then 2^(m mod 4) for a last stage when m mod 4 != 0.
+CDFT_HD constexpr int n_stages(int M) {
   const int m = ilog2(M);
-  return (m + 1) / 2;
+  return m / 4 + ((m % 4) ? 1 : 0);
 }
-CDFT_HD int stage_radix(int M, int s) {
+CDFT_HD constexpr int stage_radix(int M, int s) {
   const int m = ilog2(M);
-  return (s == 0 && (m & 1)) ? 2 : 4;
+  return (s < m / 4) ? 16 : (1 << (m % 4));
 }
 
 // Sub-transform length of DIF stage s (L_0 = M).
-CDFT_HD int dif_length(int M, int s) {
+CDFT_HD constexpr int dif_length(int M, int s) {
   int L = M;
   for (int q = 0; q < s; ++q) L /= stage_radix(M, q);
   return L;
@@ -61,7 +66,7 @@ CDFT_HD int dif_length(int M, int s) {
 // After all DIF stages, slot p holds X[k] with k = dif_order(M, p): the digits
 // of p (most significant first, radices in stage order) become the digits of
 // k (least significant first).
-CDFT_HD int dif_order(int M, int p) {
+CDFT_HD constexpr int dif_order(int M, int p) {
   int k = 0, mult = 1, L = M;
   const int ns = n_stages(M);
   for (int s = 0; s < ns; ++s) {
@@ -78,7 +83,7 @@ CDFT_HD int dif_order(int M, int p) {
 
 // Inverse of dif_order: the slot that holds frequency (or, for DIT input,
 // sample) k.
-CDFT_HD int dif_slot(int M, int k) {
+CDFT_HD constexpr int dif_slot(int M, int k) {
   int p = 0, L = M;
   const int ns = n_stages(M);
   for (int s = 0; s < ns; ++s) {
@@ -98,61 +103,108 @@ CDFT_HD cpx twiddle(const cpx* tw, int M, int L, int e) {
   return INV ? conj(w) : w;
 }
 
-// Radix-4 DFT in registers with exp(-/+ 2 pi i q t / 4).
-template <bool INV>
-CDFT_HD void dft4(cpx& a0, cpx& a1, cpx& a2, cpx& a3) {
-  const cpx t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, t3 = a1 - a3;
-  a0 = t0 + t2;
-  a2 = t0 - t2;
-  a1 = INV ? t1 + mul_i(t3) : t1 + mul_mi(t3);
-  a3 = INV ? t1 + mul_mi(t3) : t1 + mul_i(t3);
+// exp(-/+ 2 pi i t / R) for R dividing 16, as constants: cos and sin of
+// 2 pi t / 16 for t = 0 .. 15.
+CDFT_HD constexpr float c16(int t) {
+  constexpr float c[16] = {1.0f, 0.92387953251128674f, 0.70710678118654752f, 0.38268343236508977f,
+                           0.0f, -0.38268343236508977f, -0.70710678118654752f, -0.92387953251128674f,
+                           -1.0f, -0.92387953251128674f, -0.70710678118654752f, -0.38268343236508977f,
+                           0.0f, 0.38268343236508977f, 0.70710678118654752f, 0.92387953251128674f};
+  return c[t & 15];
 }
+CDFT_HD constexpr float s16(int t) { return c16(t + 12); }  // sin(x) = cos(x - pi/2)
 
-// One DIF butterfly: stage with sub-transform length L and radix r, item w in
-// [0, M / r).  Natural order in, dif_order out after the last stage.
-template <bool INV>
-CDFT_HD void dif_item(cpx* x, int stride, int M, int L, int r, int w, const cpx* tw) {
-  const int span = L / r;
-  const int j = w % span;
-  const int base = (w / span) * L + j;
-  if (r == 4) {
-    cpx a0 = x[base * stride], a1 = x[(base + span) * stride], a2 = x[(base + 2 * span) * stride],
-        a3 = x[(base + 3 * span) * stride];
-    dft4<INV>(a0, a1, a2, a3);
-    x[base * stride] = a0;
-    x[(base + span) * stride] = cmul(a1, twiddle<INV>(tw, M, L, j));
-    x[(base + 2 * span) * stride] = cmul(a2, twiddle<INV>(tw, M, L, 2 * j));
-    x[(base + 3 * span) * stride] = cmul(a3, twiddle<INV>(tw, M, L, 3 * j));
+// a * exp(-/+ 2 pi i t / R), exact for the trivial angles.
+template <int R, int T, bool INV>
+CDFT_HD cpx rot(cpx a) {
+  constexpr int t16 = (T * (16 / R)) & 15;
+  if constexpr (t16 == 0) {
+    return a;
+  } else if constexpr (t16 == 4) {
+    return INV ? mul_i(a) : mul_mi(a);
+  } else if constexpr (t16 == 8) {
+    return {-a.x, -a.y};
+  } else if constexpr (t16 == 12) {
+    return INV ? mul_mi(a) : mul_i(a);
   } else {
-    const cpx a0 = x[base * stride], a1 = x[(base + span) * stride];
-    x[base * stride] = a0 + a1;
-    x[(base + span) * stride] = cmul(a0 - a1, twiddle<INV>(tw, M, L, j));
+    constexpr float c = c16(t16), sn = INV ? s16(t16) : -s16(t16);
+    return {a.x * c - a.y * sn, a.x * sn + a.y * c};
   }
 }
 
-// One DIT butterfly, the mirror of dif_item.  Stages run in the reverse order
-// (the DIF plan's stage 0 last), so dif_order input becomes natural output;
-// the inverse DIT after the forward DIF is M times the identity.
-template <bool INV>
-CDFT_HD void dit_item(cpx* x, int stride, int M, int L, int r, int w, const cpx* tw) {
-  const int span = L / r;
+// In-register DFT of a[0..R), natural order in and out (radix-2 decimation
+// in time, recursively), R in {1, 2, 4, 8, 16}.
+template <int R, bool INV>
+CDFT_HD void dft(cpx* a) {
+  if constexpr (R == 2) {
+    const cpx t = a[0];
+    a[0] = t + a[1];
+    a[1] = t - a[1];
+  } else if constexpr (R > 2) {
+    cpx e[R / 2], o[R / 2];
+CDFT_UNROLL
+    for (int i = 0; i < R / 2; ++i) {
+      e[i] = a[2 * i];
+      o[i] = a[2 * i + 1];
+    }
+    dft<R / 2, INV>(e);
+    dft<R / 2, INV>(o);
+    [&]<int... T>(std::integer_sequence<int, T...>) {
+      ((a[T] = e[T] + rot<R, T, INV>(o[T]), a[T + R / 2] = e[T] - rot<R, T, INV>(o[T])), ...);
+    }(std::make_integer_sequence<int, R / 2>{});
+  }
+}
+
+// One DIF butterfly: stage with sub-transform length L and radix R, item w in
+// [0, M / R).  Natural order in, dif_order out after the last stage.
+template <int R, bool INV>
+CDFT_HD void dif_item_r(cpx* x, int stride, int M, int L, int w, const cpx* tw) {
+  const int span = L / R;
   const int j = w % span;
   const int base = (w / span) * L + j;
-  if (r == 4) {
-    cpx a0 = x[base * stride];
-    cpx a1 = cmul(x[(base + span) * stride], twiddle<INV>(tw, M, L, j));
-    cpx a2 = cmul(x[(base + 2 * span) * stride], twiddle<INV>(tw, M, L, 2 * j));
-    cpx a3 = cmul(x[(base + 3 * span) * stride], twiddle<INV>(tw, M, L, 3 * j));
-    dft4<INV>(a0, a1, a2, a3);
-    x[base * stride] = a0;
-    x[(base + span) * stride] = a1;
-    x[(base + 2 * span) * stride] = a2;
-    x[(base + 3 * span) * stride] = a3;
-  } else {
-    const cpx a0 = x[base * stride];
-    const cpx a1 = cmul(x[(base + span) * stride], twiddle<INV>(tw, M, L, j));
-    x[base * stride] = a0 + a1;
-    x[(base + span) * stride] = a0 - a1;
+  cpx a[R];
+CDFT_UNROLL
+  for (int q = 0; q < R; ++q) a[q] = x[(base + q * span) * stride];
+  dft<R, INV>(a);
+  x[base * stride] = a[0];
+CDFT_UNROLL
+  for (int t = 1; t < R; ++t) x[(base + t * span) * stride] = cmul(a[t], twiddle<INV>(tw, M, L, j * t));
+}
+
+// One DIT butterfly, the mirror of dif_item_r.  Stages run in the reverse
+// order (the DIF plan's stage 0 last), so dif_order input becomes natural
+// output; the inverse DIT after the forward DIF is M times the identity.
+template <int R, bool INV>
+CDFT_HD void dit_item_r(cpx* x, int stride, int M, int L, int w, const cpx* tw) {
+  const int span = L / R;
+  const int j = w % span;
+  const int base = (w / span) * L + j;
+  cpx a[R];
+  a[0] = x[base * stride];
+CDFT_UNROLL
+  for (int q = 1; q < R; ++q) a[q] = cmul(x[(base + q * span) * stride], twiddle<INV>(tw, M, L, j * q));
+  dft<R, INV>(a);
+CDFT_UNROLL
+  for (int t = 0; t < R; ++t) x[(base + t * span) * stride] = a[t];
+}
+
+// Runtime-radix forms (the host test drives every stage through these).
+template <bool INV>
+inline void dif_item(cpx* x, int stride, int M, int L, int r, int w, const cpx* tw) {
+  switch (r) {
+    case 16: dif_item_r<16, INV>(x, stride, M, L, w, tw); break;
+    case 8: dif_item_r<8, INV>(x, stride, M, L, w, tw); break;
+    case 4: dif_item_r<4, INV>(x, stride, M, L, w, tw); break;
+    default: dif_item_r<2, INV>(x, stride, M, L, w, tw); break;
+  }
+}
+template <bool INV>
+inline void dit_item(cpx* x, int stride, int M, int L, int r, int w, const cpx* tw) {
+  switch (r) {
+    case 16: dit_item_r<16, INV>(x, stride, M, L, w, tw); break;
+    case 8: dit_item_r<8, INV>(x, stride, M, L, w, tw); break;
+    case 4: dit_item_r<4, INV>(x, stride, M, L, w, tw); break;
+    default: dit_item_r<2, INV>(x, stride, M, L, w, tw); break;
   }
 }
 

@@ -1,0 +1,38 @@
+// Launchers of the fused transform path (fused.cu, kernels in
+// fft_kernels.cuh).  Specialisations exist for nx in {16, 32, 64, 128} and
+// (ny, nz) in {16, 32, 64, 128}^2; fused_plan reports whether an engine's grid
+// and channel count have one.
+#pragma once
+
+#include "cdft_common.cuh"
+#include "fft_core.cuh"
+
+namespace cdft {
+
+struct FusedPlan {
+  size_t plane_smem = 0, colf_smem = 0, colb_smem = 0;
+  int col_tiles = 0;  // column-pass CTAs per problem
+};
+
+// True (and `plan` filled, the kernels' shared-memory limits raised) when the
+// fused path serves this engine.
+bool fused_plan(const EvalParams& p, FusedPlan* plan);
+
+void fused_plane_fwd_rho(const FusedPlan& f, const EvalParams& p, const double* rho, const double* mean,
+                         fft::cpx* prho, const FftTables& T, cudaStream_t st);
+// The column pass reads the FMT weights from a table built once per engine.
+long long fused_weight_table_floats(const EvalParams& p);
+void fused_build_weights(const EvalParams& p, float* wtab, cudaStream_t st);
+
+void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho, const double* mf_w,
+                   const float* wtab, fft::cpx* q, const FftTables& T, cudaStream_t st);
+void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q, float* chan_r, const FftTables& T,
+                     cudaStream_t st);
+void fused_plane_fwd_deriv(const FusedPlan& f, const EvalParams& p, const float* deriv_r, fft::cpx* pd,
+                           const FftTables& T, cudaStream_t st);
+void fused_col_bwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* pd, const float* wtab, fft::cpx* pf,
+                   const FftTables& T, cudaStream_t st);
+void fused_plane_inv_epi(const FusedPlan& f, const EvalParams& p, const fft::cpx* pf, const double* dbar,
+                         double* force, const MuArgs& mu, const FinalArgs& fin, const FftTables& T, cudaStream_t st);
+
+}  // namespace cdft

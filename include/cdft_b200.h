@@ -381,8 +381,9 @@ CDFT_API int cdft_engine_stage_times(cdft_engine* engine, double ms[CDFT_STAGE_C
 /* Transform implementation of an engine (no reference counterpart; the
  * reference uses FFTW).  CDFT_TRANSFORMS_FUSED: hand-written plane / column
  * FFT kernels with the k-space stages fused into the column pass, available
- * for mixed-precision engines on power-of-two grids (each dimension 2..256,
- * nz >= 4) whose (y, z) plane fits in shared memory, and the default there.
+ * for mixed-precision engines whose nx, ny and nz are each one of 16, 32, 64
+ * or 128 (and whose channel tiles fit in shared memory), and the default
+ * there.
  * CDFT_TRANSFORMS_CUFFT: cuFFT plans with separate k-space kernels (every
  * other engine, and the exact HVP always).  Selecting FUSED where it is not
  * available is CDFT_ERR_INVALID. */

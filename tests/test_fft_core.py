@@ -18,7 +18,7 @@ TOL = 2e-6
 @pytest.fixture(scope="module")
 def lib(tmp_path_factory):
     out = str(tmp_path_factory.mktemp("fftcore") / "libfftcore.so")
-    subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-Wall", "-Wextra", "-Werror",
+    subprocess.run(["g++", "-O2", "-std=c++20", "-shared", "-fPIC", "-Wall", "-Wextra", "-Werror",
                     "-I", os.path.join(ROOT, "classicaldft_b200", "csrc"),
                     os.path.join(ROOT, "tests", "cpp", "fft_core_check.cpp"), "-o", out], check=True)
     L = ctypes.CDLL(out)

@@ -35,7 +35,7 @@ def test_path_selection():
     assert g32.weights.engine.fused_available and g32.weights.engine.transforms == "fused"
     g64 = Problem((16, 16, 16), 0.2, [1.0], "WhiteBearII", precision=cd.FP64)
     assert not g64.weights.engine.fused_available and g64.weights.engine.transforms == "cufft"
-    odd = Problem((24, 24, 24), 0.2, [1.0], "WhiteBearII", precision=cd.MIXED)
+    odd = Problem((24, 24, 24), 0.2, [1.0], "WhiteBearII", precision=cd.MIXED)  # no specialisation
     assert not odd.weights.engine.fused_available and odd.weights.engine.transforms == "cufft"
     with pytest.raises(ValueError):
         odd.weights.engine.set_transforms("fused")
@@ -46,7 +46,7 @@ CASES = [
     ((32, 32, 32), 0.2, [1.0], "WhiteBearII", [(0, 0) + LJ]),
     ((64, 64, 64), 0.1, [1.0], "RSLT", []),
     ((16, 32, 64), 0.2, [1.0], "WhiteBearI", [(0, 0) + LJ]),
-    ((64, 16, 8), 0.2, [1.0], "Rosenfeld", [(0, 0) + LJ]),
+    ((64, 16, 16), 0.2, [1.0], "Rosenfeld", [(0, 0) + LJ]),
     ((32, 16, 32), 0.2, [1.0, 0.6], "esFMT", [(0, 0) + LJ, (0, 1, 1.0, 0.8, 2.5), (1, 1, 0.8, 0.5, 2.0)]),
     ((16, 16, 32), 0.2, [1.0, 0.7], "Rosenfeld", [(0, 1, 1.0, 0.8, 2.5)]),
 ]
