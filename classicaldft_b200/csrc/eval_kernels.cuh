@@ -402,10 +402,23 @@ static __global__ void __launch_bounds__(256) k_species_mean(const double* __res
   partials += (long long)blockIdx.y * gridDim.x * S;
   mean_out += blockIdx.y * kMaxSpecies;
   double acc[kMaxSpecies] = {0.0, 0.0, 0.0, 0.0};
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long first = blockIdx.x * (long long)blockDim.x + threadIdx.x;
 #pragma unroll
-    for (int s = 0; s < kMaxSpecies; ++s)
-      if (s < S) acc[s] += rho[s * N + i];
+  for (int s = 0; s < kMaxSpecies; ++s) {
+    if (s >= S) break;
+    const double* r = rho + s * N;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    long long i = first;
+    for (; i + 3 * stride < N; i += 4 * stride) {  // four independent loads in flight
+      a0 += r[i];
+      a1 += r[i + stride];
+      a2 += r[i + 2 * stride];
+      a3 += r[i + 3 * stride];
+    }
+    for (; i < N; i += stride) a0 += r[i];
+    acc[s] = (a0 + a1) + (a2 + a3);
+  }
   block_reduce_store<kMaxSpecies>(acc, S, partials);
   if (last_block_done(counters + blockIdx.y)) {
     for (int s = 0; s < S; ++s) {

@@ -32,9 +32,9 @@
 
 namespace cdft {
 
-constexpr int kPlaneThreads = 256;
+constexpr int kPlaneThreads = 256;     // plane passes over many sequences
+constexpr int kPlaneThreadsWide = 512;  // plane passes with one sequence per plane (rho, force)
 constexpr int kColThreads = 256;
-constexpr int kColTile = 512;  // elements (complex) of one column-pass tile: nx x tq
 
 template <int I, int N, class F>
 __device__ __forceinline__ void static_for(F&& f) {
@@ -76,21 +76,24 @@ __device__ __forceinline__ void fft_seqs(fft::cpx* base, const fft::cpx* tw) {
   });
 }
 
-// All stages along x of `ntiles` column tiles (tile t at buf + t * TILE,
-// TQ columns of M rows, row stride TQ).
-template <int M, bool INV, bool DIT, int NT, int TQ, int TILE>
-__device__ __forceinline__ void fft_tiles(fft::cpx* buf, int ntiles, const fft::cpx* tw) {
+// All stages along x of `ntiles` column tiles (tile t at buf + t * (M << ltq),
+// 2^ltq columns of M rows, row stride 2^ltq).  Powers of two throughout, so
+// the item decomposition is shifts and masks.
+template <int M, bool INV, bool DIT, int NT>
+__device__ __forceinline__ void fft_tiles(fft::cpx* buf, int ntiles, int ltq, const fft::cpx* tw) {
   constexpr int NS = fft::n_stages(M);
+  constexpr int LM = fft::ilog2(M);
+  const int tq = 1 << ltq;
   static_for<0, NS>([&](auto kc) {
     constexpr int k = decltype(kc)::value;
     constexpr int ST = DIT ? NS - 1 - k : k;
-    constexpr int PER = M / fft::stage_radix(M, ST);
-    constexpr int PER_TILE = TQ * PER;
-    const int items = ntiles * PER_TILE;
+    constexpr int LPER = LM - fft::ilog2(fft::stage_radix(M, ST));
+    const int lpt = ltq + LPER;  // log2 of the items per tile
+    const int items = ntiles << lpt;
     for (int t = threadIdx.x; t < items; t += NT) {
-      const int tile = t / PER_TILE, r = t % PER_TILE;
-      const int q = r % TQ, w = r / TQ;
-      stage_item<M, ST, INV, DIT>(buf + tile * TILE + q, TQ, w, tw);
+      const int tile = t >> lpt, r = t & ((1 << lpt) - 1);
+      const int q = r & (tq - 1), w = r >> ltq;
+      stage_item<M, ST, INV, DIT>(buf + ((size_t)tile << (LM + ltq)) + q, tq, w, tw);
     }
     __syncthreads();
   });
@@ -98,7 +101,7 @@ __device__ __forceinline__ void fft_tiles(fft::cpx* buf, int ntiles, const fft::
 
 // ------------------------------------------------------------ plane pass
 
-template <int NY, int NZ>
+template <int NY, int NZ, int NT>
 struct Plane {
   static constexpr int MZ = NZ / 2, LD = MZ + 1;
   static constexpr size_t kSmem =
@@ -117,32 +120,32 @@ struct Plane {
     t2 = tz + MZ;
     slot_y = reinterpret_cast<int*>(t2 + NZ);
     slot_z = slot_y + NY;
-    for (int i = threadIdx.x; i < NY; i += kPlaneThreads) {
+    for (int i = threadIdx.x; i < NY; i += NT) {
       ty[i] = T.ty[i];
       slot_y[i] = fft::dif_slot(NY, i);
     }
-    for (int i = threadIdx.x; i < MZ; i += kPlaneThreads) {
+    for (int i = threadIdx.x; i < MZ; i += NT) {
       tz[i] = T.tz[i];
       slot_z[i] = fft::dif_slot(MZ, i);
     }
-    for (int i = threadIdx.x; i < NZ; i += kPlaneThreads) t2[i] = T.t2[i];
+    for (int i = threadIdx.x; i < NZ; i += NT) t2[i] = T.t2[i];
   }
 
   // y transform of every column kz (DIF: natural in, slot_y order out)
   template <bool INV>
   __device__ __forceinline__ void y_dif() {
-    fft_seqs<NY, INV, false, kPlaneThreads, LD, 1, LD, false>(P, ty);
+    fft_seqs<NY, INV, false, NT, LD, 1, LD, false>(P, ty);
   }
 };
 
 // Forward plane pass: R2C along z, FFT along y, store natural order.
 // IN = double: rho with the species mean subtracted (the mixed-precision
 // split); IN = float: a derivative channel as is.
-template <int NY, int NZ, typename IN>
-__global__ void __launch_bounds__(kPlaneThreads, 3)
+template <int NY, int NZ, typename IN, int NT>
+__global__ void __launch_bounds__(NT, NT == kPlaneThreads ? 3 : 1)
     k_plane_fwd(EvalParams p, const IN* __restrict__ in, int nseq, const double* __restrict__ mean,
                 fft::cpx* __restrict__ out, FftTables T) {
-  using PL = Plane<NY, NZ>;
+  using PL = Plane<NY, NZ, NT>;
   constexpr int MZ = PL::MZ, LD = PL::LD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ix = blockIdx.x, sq = blockIdx.y, b = blockIdx.z;
@@ -151,7 +154,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 3)
   const IN* src = in + ((long long)b * nseq + sq) * p.N + (long long)ix * NY * NZ;
   const double c = mean ? mean[b * kMaxSpecies + sq] : 0.0;
   // pairs z[n] = x[2n] + i x[2n+1] into DIT input order
-  for (int t = threadIdx.x; t < NY * MZ; t += kPlaneThreads) {
+  for (int t = threadIdx.x; t < NY * MZ; t += NT) {
     const int iy = t / MZ, n = t % MZ;
     const IN* q = src + (long long)iy * NZ + 2 * n;  // the caller's buffer: scalar loads
     fft::cpx v;
@@ -164,16 +167,16 @@ __global__ void __launch_bounds__(kPlaneThreads, 3)
   __syncthreads();
   // z: DIT, slot order in, natural out; neighbouring threads take
   // neighbouring rows (row stride LD is odd: no bank conflicts)
-  fft_seqs<MZ, false, true, kPlaneThreads, NY, LD, 1, false>(s.P, s.tz);
+  fft_seqs<MZ, false, true, NT, NY, LD, 1, false>(s.P, s.tz);
   constexpr int PAIRS = MZ / 2 + 1;
-  for (int t = threadIdx.x; t < NY * PAIRS; t += kPlaneThreads) {
+  for (int t = threadIdx.x; t < NY * PAIRS; t += NT) {
     const int row = t / PAIRS, k = t % PAIRS;
     fft::r2c_post_item(s.P + row * LD, 1, MZ, k, s.t2);
   }
   __syncthreads();
   s.template y_dif<false>();
   fft::cpx* dst = out + ((long long)b * nseq + sq) * p.Nk + (long long)ix * NY * LD;
-  for (int t = threadIdx.x; t < NY * LD; t += kPlaneThreads) {
+  for (int t = threadIdx.x; t < NY * LD; t += NT) {
     const int ky = t / LD, kz = t % LD;
     dst[t] = s.P[s.slot_y[ky] * LD + kz];
   }
@@ -182,35 +185,36 @@ __global__ void __launch_bounds__(kPlaneThreads, 3)
 // Inverse plane pass shared part: load a natural-order plane, IFFT along y
 // (DIF), C2R pre-processing and IFFT along z (DIF).  Afterwards sample
 // (iy, 2n | 2n+1) is 2 * (Re | Im) of P[slot_y[iy] * LD + slot_z[n]].
-template <int NY, int NZ>
-__device__ __forceinline__ void plane_inverse_core(Plane<NY, NZ>& s, const fft::cpx* __restrict__ src) {
-  using PL = Plane<NY, NZ>;
+template <int NY, int NZ, int NT>
+__device__ __forceinline__ void plane_inverse_core(Plane<NY, NZ, NT>& s, const fft::cpx* __restrict__ src) {
+  using PL = Plane<NY, NZ, NT>;
   constexpr int MZ = PL::MZ, LD = PL::LD;
-  for (int t = threadIdx.x; t < NY * LD; t += kPlaneThreads) s.P[t] = src[t];
+  for (int t = threadIdx.x; t < NY * LD; t += NT) s.P[t] = src[t];
   __syncthreads();
   s.template y_dif<true>();
   constexpr int PAIRS = MZ / 2 + 1;
-  for (int t = threadIdx.x; t < NY * PAIRS; t += kPlaneThreads) {
+  for (int t = threadIdx.x; t < NY * PAIRS; t += NT) {
     const int row = t / PAIRS, k = t % PAIRS;
     fft::c2r_pre_item(s.P + row * LD, 1, MZ, k, s.t2);
   }
   __syncthreads();
-  fft_seqs<MZ, true, false, kPlaneThreads, NY, LD, 1, false>(s.P, s.tz);
+  fft_seqs<MZ, true, false, NT, NY, LD, 1, false>(s.P, s.tz);
 }
 
 // Inverse plane pass of the weighted-density channels -> real FP32 channels.
 template <int NY, int NZ>
 __global__ void __launch_bounds__(kPlaneThreads, 3)
     k_plane_inv(EvalParams p, const fft::cpx* __restrict__ in, int nseq, float* __restrict__ out, FftTables T) {
-  using PL = Plane<NY, NZ>;
+  constexpr int NT = kPlaneThreads;
+  using PL = Plane<NY, NZ, NT>;
   constexpr int MZ = PL::MZ, LD = PL::LD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ix = blockIdx.x, sq = blockIdx.y, b = blockIdx.z;
   PL s(smem_raw, T);
   __syncthreads();
-  plane_inverse_core<NY, NZ>(s, in + ((long long)b * nseq + sq) * p.Nk + (long long)ix * NY * LD);
+  plane_inverse_core<NY, NZ, NT>(s, in + ((long long)b * nseq + sq) * p.Nk + (long long)ix * NY * LD);
   float* dst = out + ((long long)b * nseq + sq) * p.N + (long long)ix * NY * NZ;  // engine buffer: 8-byte aligned
-  for (int t = threadIdx.x; t < NY * MZ; t += kPlaneThreads) {
+  for (int t = threadIdx.x; t < NY * MZ; t += NT) {
     const int iy = t / MZ, n = t % MZ;
     const fft::cpx v = s.P[s.slot_y[iy] * LD + s.slot_z[n]];
     *reinterpret_cast<float2*>(dst + (long long)iy * NZ + 2 * n) = make_float2(2.0f * v.x, 2.0f * v.y);
@@ -222,10 +226,11 @@ __global__ void __launch_bounds__(kPlaneThreads, 3)
 // 0, species 0 of each problem also reduces the pointwise partials into the
 // scalar block (the pointwise kernel completed before this launch).
 template <int NY, int NZ, bool MULTI, bool TENSOR>
-__global__ void __launch_bounds__(kPlaneThreads, 3)
+__global__ void __launch_bounds__(kPlaneThreadsWide, 1)
     k_plane_inv_epi(EvalParams p, const fft::cpx* __restrict__ in, const double* __restrict__ dbar,
                     double* __restrict__ force, const __grid_constant__ MuArgs mu, FinalArgs fin, FftTables T) {
-  using PL = Plane<NY, NZ>;
+  constexpr int NT = kPlaneThreadsWide;
+  using PL = Plane<NY, NZ, NT>;
   using L = Lay<MULTI, TENSOR>;
   constexpr int MZ = PL::MZ, LD = PL::LD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -243,10 +248,10 @@ __global__ void __launch_bounds__(kPlaneThreads, 3)
     s_const = v * p.dv - mu.mu[b][sp] * p.dv;
   }
   __syncthreads();
-  plane_inverse_core<NY, NZ>(s, in + ((long long)b * p.S + sp) * p.Nk + (long long)ix * NY * LD);
+  plane_inverse_core<NY, NZ, NT>(s, in + ((long long)b * p.S + sp) * p.Nk + (long long)ix * NY * LD);
   double* dst = force + ((long long)b * p.S + sp) * p.N + (long long)ix * NY * NZ;
   const double dv = p.dv, cst = s_const;
-  for (int t = threadIdx.x; t < NY * MZ; t += kPlaneThreads) {
+  for (int t = threadIdx.x; t < NY * MZ; t += NT) {
     const int iy = t / MZ, n = t % MZ;
     const fft::cpx v = s.P[s.slot_y[iy] * LD + s.slot_z[n]];
     double* f = dst + (long long)iy * NZ + 2 * n;  // the caller's buffer: 8-byte alignment suffices
@@ -257,19 +262,16 @@ __global__ void __launch_bounds__(kPlaneThreads, 3)
 
 // ----------------------------------------------------------- column pass
 
-template <int NX>
-struct Col {
-  static constexpr int TQ = kColTile / NX;  // columns per tile
-  static constexpr int TILE = kColTile;
-  static __host__ __device__ constexpr size_t smem(int nbuf) {
-    return sizeof(fft::cpx) * ((size_t)NX + (size_t)nbuf * TILE) + sizeof(int) * NX + 16;
-  }
-};
+// Shared memory of a column kernel: the x twiddles and row table, then nbuf
+// tiles of nx rows x 2^ltq columns.
+__host__ __device__ inline size_t col_smem(int nx, int ltq, int nbuf) {
+  return 16 * ((sizeof(fft::cpx) * nx + sizeof(int) * nx + 15) / 16) + sizeof(fft::cpx) * ((size_t)nbuf * nx << ltq);
+}
 
-// x transform of `ntiles` tiles (tile t at buf + t * TILE, row stride TQ).
+// x transform of `ntiles` tiles (tile t at buf + t * (NX << ltq), row stride 2^ltq).
 template <int NX, bool INV, bool DIT>
-__device__ __forceinline__ void col_x(fft::cpx* buf, int ntiles, const fft::cpx* tx) {
-  fft_tiles<NX, INV, DIT, kColThreads, Col<NX>::TQ, Col<NX>::TILE>(buf, ntiles, tx);
+__device__ __forceinline__ void col_x(fft::cpx* buf, int ntiles, int ltq, const fft::cpx* tx) {
+  fft_tiles<NX, INV, DIT, kColThreads>(buf, ntiles, ltq, tx);
 }
 
 // Weight table of the column pass, built once per engine (k_build_weights):
@@ -341,9 +343,10 @@ __device__ __forceinline__ KIndex col_kindex(const EvalParams& p, int kx, long l
 template <int NX, bool MULTI, bool TENSOR>
 __global__ void __launch_bounds__(kColThreads, 2)
     k_col_fwd(EvalParams p, const fft::cpx* __restrict__ prho, const double* __restrict__ mf_w,
-              const float* __restrict__ wtab, fft::cpx* __restrict__ q_out, FftTables T) {
+              const float* __restrict__ wtab, fft::cpx* __restrict__ q_out, int ltq, FftTables T) {
   using Ly = Lay<MULTI, TENSOR>;
-  constexpr int TQ = Col<NX>::TQ, TILE = Col<NX>::TILE;
+  constexpr int LNX = fft::ilog2(NX);
+  const int TQ = 1 << ltq, LT = LNX + ltq, TILE = 1 << LT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int S = p.S, C = p.n_chan;
   const long long plane = (long long)p.ny * p.nzh;
@@ -358,15 +361,15 @@ __global__ void __launch_bounds__(kColThreads, 2)
     kx_of_row[i] = fft::dif_order(NX, i);
   }
   for (int t = threadIdx.x; t < S * TILE; t += kColThreads) {
-    const int sp = t / TILE, e = t % TILE, ix = e / TQ, qq = e % TQ;
+    const int sp = t >> LT, e = t & (TILE - 1), ix = e >> ltq, qq = e & (TQ - 1);
     const long long q = q0 + qq;
     R[t] = (q < plane) ? prho[((long long)b * S + sp) * p.Nk + ix * plane + q] : fft::cpx{0.0f, 0.0f};
   }
   __syncthreads();
-  col_x<NX, false, false>(R, S, tx);
+  col_x<NX, false, false>(R, S, ltq, tx);
   // k-space products, one element per thread iteration (FP64 weights)
   for (int e = threadIdx.x; e < TILE; e += kColThreads) {
-    const int row = e / TQ, qq = e % TQ;
+    const int row = e >> ltq, qq = e & (TQ - 1);
     const long long q = q0 + qq;
     if (q >= plane) {
       for (int c = 0; c < C; ++c) Ch[(size_t)c * TILE + e] = fft::cpx{0.0f, 0.0f};
@@ -402,9 +405,9 @@ __global__ void __launch_bounds__(kColThreads, 2)
     }
   }
   __syncthreads();
-  col_x<NX, true, true>(Ch, C, tx);
+  col_x<NX, true, true>(Ch, C, ltq, tx);
   for (int t = threadIdx.x; t < C * TILE; t += kColThreads) {
-    const int c = t / TILE, e = t % TILE, ix = e / TQ, qq = e % TQ;
+    const int c = t >> LT, e = t & (TILE - 1), ix = e >> ltq, qq = e & (TQ - 1);
     const long long q = q0 + qq;
     if (q < plane) q_out[((long long)b * C + c) * p.Nk + ix * plane + q] = Ch[t];
   }
@@ -415,10 +418,11 @@ __global__ void __launch_bounds__(kColThreads, 2)
 template <int NX, bool MULTI, bool TENSOR>
 __global__ void __launch_bounds__(kColThreads, 2)
     k_col_bwd(EvalParams p, const fft::cpx* __restrict__ pd, const float* __restrict__ wtab, fft::cpx* __restrict__ pf,
-              FftTables T) {
+              int ltq, FftTables T) {
   using Ly = Lay<MULTI, TENSOR>;
   constexpr int NF = Ly::NFMT;
-  constexpr int TQ = Col<NX>::TQ, TILE = Col<NX>::TILE;
+  constexpr int LNX = fft::ilog2(NX);
+  const int TQ = 1 << ltq, LT = LNX + ltq, TILE = 1 << LT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int S = p.S;
   const long long plane = (long long)p.ny * p.nzh;
@@ -432,16 +436,16 @@ __global__ void __launch_bounds__(kColThreads, 2)
     kx_of_row[i] = fft::dif_order(NX, i);
   }
   for (int t = threadIdx.x; t < NF * TILE; t += kColThreads) {
-    const int c = t / TILE, e = t % TILE, ix = e / TQ, qq = e % TQ;
+    const int c = t >> LT, e = t & (TILE - 1), ix = e >> ltq, qq = e & (TQ - 1);
     const long long q = q0 + qq;
     Dt[t] = (q < plane) ? pd[((long long)b * NF + c) * p.Nk + ix * plane + q] : fft::cpx{0.0f, 0.0f};
   }
   __syncthreads();
-  col_x<NX, false, false>(Dt, NF, tx);
+  col_x<NX, false, false>(Dt, NF, ltq, tx);
   // species force spectra overwrite tiles 0 .. S-1 (each element is read in
   // full before it is written, and elements are independent)
   for (int e = threadIdx.x; e < TILE; e += kColThreads) {
-    const int row = e / TQ, qq = e % TQ;
+    const int row = e >> ltq, qq = e & (TQ - 1);
     const long long q = q0 + qq;
     if (q >= plane) continue;
     const KIndex ki = col_kindex(p, kx_of_row[row], q);
@@ -461,9 +465,9 @@ __global__ void __launch_bounds__(kColThreads, 2)
     }
   }
   __syncthreads();
-  col_x<NX, true, true>(Dt, S, tx);
+  col_x<NX, true, true>(Dt, S, ltq, tx);
   for (int t = threadIdx.x; t < S * TILE; t += kColThreads) {
-    const int sp = t / TILE, e = t % TILE, ix = e / TQ, qq = e % TQ;
+    const int sp = t >> LT, e = t & (TILE - 1), ix = e >> ltq, qq = e & (TQ - 1);
     const long long q = q0 + qq;
     if (q < plane) pf[((long long)b * S + sp) * p.Nk + ix * plane + q] = Dt[t];
   }

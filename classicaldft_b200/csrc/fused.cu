@@ -61,19 +61,22 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan) {
   FusedPlan f;
   bool ok = with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
-    f.plane_smem = Plane<NY, NZ>::kSmem;
+    f.plane_smem = Plane<NY, NZ, kPlaneThreads>::kSmem;
   });
-  ok = ok && with_len(p.nx, [&](auto xc) {
-    constexpr int NX = decltype(xc)::value;
-    f.colf_smem = Col<NX>::smem(p.S + p.n_chan);
-    f.colb_smem = Col<NX>::smem(p.L.n_deriv);
-    f.col_tiles = (int)(((long long)p.ny * p.nzh + Col<NX>::TQ - 1) / Col<NX>::TQ);
-  });
-  if (!ok || f.plane_smem > kSmemCap || f.colf_smem > kSmemCap || f.colb_smem > kSmemCap) return false;
+  ok = ok && with_len(p.nx, [](auto) {});
+  if (!ok || f.plane_smem > kSmemCap) return false;
+  // column tiles: the widest (at most 16 columns) whose buffers fit
+  f.ltq = 4;
+  while (f.ltq > 0 && (col_smem(p.nx, f.ltq, p.S + p.n_chan) > kSmemCap || col_smem(p.nx, f.ltq, p.L.n_deriv) > kSmemCap))
+    --f.ltq;
+  f.colf_smem = col_smem(p.nx, f.ltq, p.S + p.n_chan);
+  f.colb_smem = col_smem(p.nx, f.ltq, p.L.n_deriv);
+  if (f.colf_smem > kSmemCap || f.colb_smem > kSmemCap) return false;
+  f.col_tiles = (int)(((long long)p.ny * p.nzh + (1 << f.ltq) - 1) >> f.ltq);
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
-    allow_smem(k_plane_fwd<NY, NZ, double>, f.plane_smem);
-    allow_smem(k_plane_fwd<NY, NZ, float>, f.plane_smem);
+    allow_smem(k_plane_fwd<NY, NZ, double, kPlaneThreadsWide>, f.plane_smem);
+    allow_smem(k_plane_fwd<NY, NZ, float, kPlaneThreads>, f.plane_smem);
     allow_smem(k_plane_inv<NY, NZ>, f.plane_smem);
     with_layout(p, [&](auto mc, auto tc) {
       allow_smem(k_plane_inv_epi<NY, NZ, decltype(mc)::value, decltype(tc)::value>, f.plane_smem);
@@ -94,8 +97,8 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan) {
 void fused_plane_fwd_rho(const FusedPlan& f, const EvalParams& p, const double* rho, const double* mean,
                          fft::cpx* prho, const FftTables& T, cudaStream_t st) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
-    k_plane_fwd<decltype(yc)::value, decltype(zc)::value, double>
-        <<<dim3(p.nx, p.S, p.batch), kPlaneThreads, f.plane_smem, st>>>(p, rho, p.S, mean, prho, T);
+    k_plane_fwd<decltype(yc)::value, decltype(zc)::value, double, kPlaneThreadsWide>
+        <<<dim3(p.nx, p.S, p.batch), kPlaneThreadsWide, f.plane_smem, st>>>(p, rho, p.S, mean, prho, T);
   });
   CDFT_CUDA(cudaGetLastError());
 }
@@ -105,7 +108,7 @@ void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho
   with_len(p.nx, [&](auto xc) {
     with_layout(p, [&](auto mc, auto tc) {
       k_col_fwd<decltype(xc)::value, decltype(mc)::value, decltype(tc)::value>
-          <<<dim3(f.col_tiles, p.batch), kColThreads, f.colf_smem, st>>>(p, prho, mf_w, wtab, q, T);
+          <<<dim3(f.col_tiles, p.batch), kColThreads, f.colf_smem, st>>>(p, prho, mf_w, wtab, q, f.ltq, T);
     });
   });
   CDFT_CUDA(cudaGetLastError());
@@ -123,7 +126,7 @@ void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q,
 void fused_plane_fwd_deriv(const FusedPlan& f, const EvalParams& p, const float* deriv_r, fft::cpx* pd,
                            const FftTables& T, cudaStream_t st) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
-    k_plane_fwd<decltype(yc)::value, decltype(zc)::value, float>
+    k_plane_fwd<decltype(yc)::value, decltype(zc)::value, float, kPlaneThreads>
         <<<dim3(p.nx, p.L.n_deriv, p.batch), kPlaneThreads, f.plane_smem, st>>>(p, deriv_r, p.L.n_deriv, nullptr,
                                                                                  pd, T);
   });
@@ -135,7 +138,7 @@ void fused_col_bwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* pd, 
   with_len(p.nx, [&](auto xc) {
     with_layout(p, [&](auto mc, auto tc) {
       k_col_bwd<decltype(xc)::value, decltype(mc)::value, decltype(tc)::value>
-          <<<dim3(f.col_tiles, p.batch), kColThreads, f.colb_smem, st>>>(p, pd, wtab, pf, T);
+          <<<dim3(f.col_tiles, p.batch), kColThreads, f.colb_smem, st>>>(p, pd, wtab, pf, f.ltq, T);
     });
   });
   CDFT_CUDA(cudaGetLastError());
@@ -146,7 +149,7 @@ void fused_plane_inv_epi(const FusedPlan& f, const EvalParams& p, const fft::cpx
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     with_layout(p, [&](auto mc, auto tc) {
       k_plane_inv_epi<decltype(yc)::value, decltype(zc)::value, decltype(mc)::value, decltype(tc)::value>
-          <<<dim3(p.nx, p.S, p.batch), kPlaneThreads, f.plane_smem, st>>>(p, pf, dbar, force, mu, fin, T);
+          <<<dim3(p.nx, p.S, p.batch), kPlaneThreadsWide, f.plane_smem, st>>>(p, pf, dbar, force, mu, fin, T);
     });
   });
   CDFT_CUDA(cudaGetLastError());

@@ -11,6 +11,7 @@ namespace cdft {
 
 struct FusedPlan {
   size_t plane_smem = 0, colf_smem = 0, colb_smem = 0;
+  int ltq = 0;        // log2 of the columns per column-pass tile
   int col_tiles = 0;  // column-pass CTAs per problem
 };
 
