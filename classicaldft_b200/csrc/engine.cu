@@ -171,6 +171,9 @@ Engine::Engine(const EngineSpec& spec) {
     grid_tma_ = per_problem((long long)sms * std::max(per_sm, 1));
   });
   grid_stream_ = per_problem(std::max<long long>(1, std::min<long long>((long long)sms * 8, (p.N * B + 255) / 256)));
+  // the species mean: four blocks per SM in all (its last block sums the
+  // partials, so fewer blocks shorten that tail and the counter's contention)
+  grid_mean_ = per_problem(std::max<long long>(1, std::min<long long>((long long)sms * 4, (p.N * B + 255) / 256)));
   partials_ = dalloc<double>((size_t)B * std::max(std::max(grid_pw_, grid_tma_), grid_stream_) * p.n_terms, tot);
   err_ = dalloc<int>(1, tot);
   CDFT_CUDA(cudaMemset(err_, 0, sizeof(int)));
@@ -351,7 +354,7 @@ void Engine::forward_stage(const double* in, R* chan_out, double* mean_out, cuda
   C2* chan_k = static_cast<C2*>(chan_k_);
   if constexpr (mixed) {
     const dim3 gs(grid_stream_, p.batch);
-    k_species_mean<<<gs, 256, 0, stream>>>(in, p.N, p.S, partials_, sync_, mean_out);
+    k_species_mean<<<dim3(grid_mean_, p.batch), 256, 0, stream>>>(in, p.N, p.S, partials_, sync_, mean_out);
     k_split_convert<<<gs, 256, 0, stream>>>(in, p.N, p.S, static_cast<float*>(rho_lo_), mean_out);
     mark(1, stream);
     CDFT_CUFFT(cufftExecR2C(plan_rho_, static_cast<float*>(rho_lo_), reinterpret_cast<cufftComplex*>(rho_k)));
@@ -419,7 +422,7 @@ void Engine::backward_stage(R* deriv, const double* dbar, double* out, const MuA
 void Engine::fused_forward(const double* rho, cudaStream_t stream) {
   const EvalParams& p = p_;
   const dim3 gs(grid_stream_, p.batch);
-  k_species_mean<<<gs, 256, 0, stream>>>(rho, p.N, p.S, partials_, sync_, mean_);
+  k_species_mean<<<dim3(grid_mean_, p.batch), 256, 0, stream>>>(rho, p.N, p.S, partials_, sync_, mean_);
   mark(1, stream);
   fft::cpx* prho = static_cast<fft::cpx*>(rho_k_);
   fft::cpx* q = static_cast<fft::cpx*>(chan_k_);

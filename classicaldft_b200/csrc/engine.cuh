@@ -146,6 +146,7 @@ class Engine {
   double* tan_in_ = nullptr;  // aligned copies of rho and v
   int grid_tma_ = 0;
   int grid_stream_ = 0;       // streaming kernels (sums, conversion, epilogue)
+  int grid_mean_ = 0;         // k_species_mean
   // grid_* are CTAs per problem: a launch has grid_* x B CTAs
   size_t tma_smem_ = 0, tma_smem_v_ = 0;
   void* fft_work_ = nullptr;

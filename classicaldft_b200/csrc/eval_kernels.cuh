@@ -58,9 +58,12 @@ struct Lay {
   static constexpr int NFMT = MULTI ? (TENSOR ? 15 : 10) : (TENSOR ? 10 : 5);
 };
 
-struct KW {
-  double w3, w2, fv, A, B;
+// |k|-only factors of the FMT weights of one species at one wavevector.
+template <typename T>
+struct KWT {
+  T w3, w2, fv, A, B;
 };
+using KW = KWT<double>;
 
 // weights.hpp:91-137: |k|-only factors of the FMT weights of a sphere of radius R.
 __device__ inline KW weight_kernels(double k, double R) {
@@ -98,27 +101,29 @@ __host__ __device__ constexpr int tchan_j(int t) { return t < 3 ? t : t - 2; }
 // !odd, or i*W*rho_s if odd.  Mirrors weights.hpp:163-179 and the Rosenfeld
 // scalings of hard_sphere.hpp:80-85.  c is a compile-time constant at every
 // call site (fully unrolled loops), so the branches fold away.
-template <bool MULTI, bool TENSOR>
-__device__ __forceinline__ double chan_weight(int c, int s, const EvalParams& p, const double kk[3], double inv_k2,
-                                              const KW& w, bool& odd) {
+// T = double on the cuFFT path; T = float in the fused column pass (the
+// mixed path's FP32 k-space).
+template <bool MULTI, bool TENSOR, typename T = double>
+__device__ __forceinline__ T chan_weight(int c, int s, const EvalParams& p, const T kk[3], T inv_k2,
+                                         const KWT<T>& w, bool& odd) {
   using L = Lay<MULTI, TENSOR>;
-  const double in = p.inv_n;
+  const T in = (T)p.inv_n;
   odd = false;
   if (c == L::ETA) return w.w3 * in;
   if (c == L::N2) return w.w2 * in;
-  if (MULTI && c == L::N1) return (w.w2 * in) * p.inv4piR[s];
-  if (MULTI && c == L::N0) return (w.w2 * in) * p.inv4piR2[s];
+  if (MULTI && c == L::N1) return (w.w2 * in) * (T)p.inv4piR[s];
+  if (MULTI && c == L::N0) return (w.w2 * in) * (T)p.inv4piR2[s];
   if (c >= L::V1 && c < L::V1 + 3) {
     odd = true;
     return kk[c - L::V1] * w.fv * in;
   }
   if (MULTI && c >= L::V0 && c < L::V0 + 3) {
     odd = true;
-    return (kk[c - L::V0] * w.fv * in) * p.inv4piR[s];
+    return (kk[c - L::V0] * w.fv * in) * (T)p.inv4piR[s];
   }
   const int t = c - L::T;
   const int i = tchan_i(t), j = tchan_j(t);
-  const double d = (i == j) ? 1.0 : 0.0;
+  const T d = (i == j) ? T(1) : T(0);
   return (w.A * kk[i] * kk[j] * inv_k2 + w.B * d) * in;
 }
 
@@ -162,28 +167,28 @@ __device__ __forceinline__ void st2<float2>(float2* a, long long i, double2 v) {
 // W'(k) rho_k(k) equals the projection (X(k) + conj(X(k_m)))/2 of X = W rho_k
 // up to round-off, without reading the mirror mode.  For an odd channel
 // (W = i w) the coefficient of i is (w(k) - w(k_m))/2.
-template <bool MULTI, bool TENSOR>
-__device__ __forceinline__ double chan_weight_sym(int c, int s, const EvalParams& p, const double kk[3],
-                                                  const double km[3], bool proj, double inv_k2, const KW& w,
-                                                  bool& odd) {
-  double v = chan_weight<MULTI, TENSOR>(c, s, p, kk, inv_k2, w, odd);
+template <bool MULTI, bool TENSOR, typename T = double>
+__device__ __forceinline__ T chan_weight_sym(int c, int s, const EvalParams& p, const T kk[3], const T km[3],
+                                             bool proj, T inv_k2, const KWT<T>& w, bool& odd) {
+  T v = chan_weight<MULTI, TENSOR, T>(c, s, p, kk, inv_k2, w, odd);
   if (proj) {
-    const double vm = chan_weight<MULTI, TENSOR>(c, s, p, km, inv_k2, w, odd);
-    v = odd ? 0.5 * (v - vm) : 0.5 * (v + vm);
+    const T vm = chan_weight<MULTI, TENSOR, T>(c, s, p, km, inv_k2, w, odd);
+    v = odd ? T(0.5) * (v - vm) : T(0.5) * (v + vm);
   }
   return v;
 }
 
-// One forward channel value at wavevector kk from the species spectra r[].
-template <bool MULTI, bool TENSOR>
-__device__ __forceinline__ double2 fwd_value(int c, const EvalParams& p, const double kk[3], const double km[3],
-                                             bool proj, double inv_k2, const KW* kw, const double2* r) {
-  double2 acc = make_double2(0.0, 0.0);
+// One forward channel value at wavevector kk from the species spectra r[]
+// (V2 = double2 or float2, matching T).
+template <bool MULTI, bool TENSOR, typename T = double, typename V2 = double2>
+__device__ __forceinline__ V2 fwd_value(int c, const EvalParams& p, const T kk[3], const T km[3], bool proj,
+                                        T inv_k2, const KWT<T>* kw, const V2* r) {
+  V2 acc{};
 #pragma unroll
   for (int s = 0; s < (MULTI ? kMaxSpecies : 1); ++s) {
     if (s < p.S) {
       bool odd;
-      const double w = chan_weight_sym<MULTI, TENSOR>(c, s, p, kk, km, proj, inv_k2, kw[s], odd);
+      const T w = chan_weight_sym<MULTI, TENSOR, T>(c, s, p, kk, km, proj, inv_k2, kw[s], odd);
       if (odd) {
         acc.x += -w * r[s].y;
         acc.y += w * r[s].x;
@@ -267,15 +272,15 @@ __global__ void __launch_bounds__(256) k_forward(EvalParams p, const C2* __restr
 
 // Back-convolution of species s at kk from the derivative spectra dk[]:
 // F_s = sum_c conj(W'_cs) D_c (hard_sphere.hpp:117-134).
-template <bool MULTI, bool TENSOR>
-__device__ __forceinline__ double2 bwd_value(int s, const EvalParams& p, const double kk[3], const double km[3],
-                                             bool proj, double inv_k2, const KW& w, const double2* d) {
+template <bool MULTI, bool TENSOR, typename T = double, typename V2 = double2>
+__device__ __forceinline__ V2 bwd_value(int s, const EvalParams& p, const T kk[3], const T km[3], bool proj,
+                                        T inv_k2, const KWT<T>& w, const V2* d) {
   using L = Lay<MULTI, TENSOR>;
-  double2 acc = make_double2(0.0, 0.0);
+  V2 acc{};
 #pragma unroll
   for (int c = 0; c < L::NFMT; ++c) {
     bool odd;
-    const double wc = chan_weight_sym<MULTI, TENSOR>(c, s, p, kk, km, proj, inv_k2, w, odd);
+    const T wc = chan_weight_sym<MULTI, TENSOR, T>(c, s, p, kk, km, proj, inv_k2, w, odd);
     if (odd) {  // conj(i w) D = -i w D
       acc.x += wc * d[c].y;
       acc.y += -wc * d[c].x;
@@ -377,11 +382,12 @@ __device__ __forceinline__ double block_sum_partials(const double* partials, int
 }
 
 // True in the one block of problem blockIdx.y that finishes last: every
-// block has stored (and fenced) its partials by then.  The counter returns
-// to zero for the next launch.
-__device__ __forceinline__ bool last_block_done(unsigned* counter) {
+// block has stored (and fenced) its partials by then.  The threads below
+// `writers` stored this block's partials and fence them.  The counter
+// returns to zero for the next launch.
+__device__ __forceinline__ bool last_block_done(unsigned* counter, int writers) {
   __shared__ bool last;
-  __threadfence();
+  if (threadIdx.x < writers) __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned prev = atomicAdd(counter, 1u);
@@ -408,19 +414,17 @@ static __global__ void __launch_bounds__(256) k_species_mean(const double* __res
   for (int s = 0; s < kMaxSpecies; ++s) {
     if (s >= S) break;
     const double* r = rho + s * N;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     long long i = first;
-    for (; i + 3 * stride < N; i += 4 * stride) {  // four independent loads in flight
-      a0 += r[i];
-      a1 += r[i + stride];
-      a2 += r[i + 2 * stride];
-      a3 += r[i + 3 * stride];
+    for (; i + 7 * stride < N; i += 8 * stride) {  // eight independent loads in flight
+#pragma unroll
+      for (int u = 0; u < 8; ++u) a[u] += r[i + u * stride];
     }
-    for (; i < N; i += stride) a0 += r[i];
-    acc[s] = (a0 + a1) + (a2 + a3);
+    for (; i < N; i += stride) a[0] += r[i];
+    acc[s] = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
   }
   block_reduce_store<kMaxSpecies>(acc, S, partials);
-  if (last_block_done(counters + blockIdx.y)) {
+  if (last_block_done(counters + blockIdx.y, S)) {
     for (int s = 0; s < S; ++s) {
       const double v = block_sum_partials<true>(partials, gridDim.x, S, s);
       if (threadIdx.x == 0) mean_out[s] = v / (double)N;

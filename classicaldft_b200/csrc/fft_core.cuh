@@ -168,7 +168,8 @@ CDFT_UNROLL
   dft<R, INV>(a);
   x[base * stride] = a[0];
 CDFT_UNROLL
-  for (int t = 1; t < R; ++t) x[(base + t * span) * stride] = cmul(a[t], twiddle<INV>(tw, M, L, j * t));
+  for (int t = 1; t < R; ++t)  // the last stage (L == R) has j = 0: no twiddle
+    x[(base + t * span) * stride] = (L == R) ? a[t] : cmul(a[t], twiddle<INV>(tw, M, L, j * t));
 }
 
 // One DIT butterfly, the mirror of dif_item_r.  Stages run in the reverse
@@ -182,7 +183,8 @@ CDFT_HD void dit_item_r(cpx* x, int stride, int M, int L, int w, const cpx* tw) 
   cpx a[R];
   a[0] = x[base * stride];
 CDFT_UNROLL
-  for (int q = 1; q < R; ++q) a[q] = cmul(x[(base + q * span) * stride], twiddle<INV>(tw, M, L, j * q));
+  for (int q = 1; q < R; ++q)  // the first DIT stage (L == R) has j = 0: no twiddle
+    a[q] = (L == R) ? x[(base + q * span) * stride] : cmul(x[(base + q * span) * stride], twiddle<INV>(tw, M, L, j * q));
   dft<R, INV>(a);
 CDFT_UNROLL
   for (int t = 0; t < R; ++t) x[(base + t * span) * stride] = a[t];

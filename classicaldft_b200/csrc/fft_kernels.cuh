@@ -238,6 +238,12 @@ __global__ void __launch_bounds__(kPlaneThreadsWide, 1)
   if (ix == 0 && sp == 0 && fin.scalars)
     reduce_final(fin.partials + (long long)b * fin.nblocks * p.n_terms, fin.nblocks, p, mu.mu[b], fin.err,
                  fin.scalars + b * kScalarCount);
+  // the force plane is read at the end: start pulling it into L2 now
+  {
+    const char* fp = reinterpret_cast<const char*>(force + ((long long)b * p.S + sp) * p.N + (long long)ix * NY * NZ);
+    for (int off = threadIdx.x * 128; off < NY * NZ * 8; off += NT * 128)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(fp + off));
+  }
   PL s(smem_raw, T);
   __shared__ double s_const;
   if (threadIdx.x == 0) {
@@ -300,21 +306,26 @@ static __global__ void __launch_bounds__(256) k_build_weights(EvalParams p, floa
   }
 }
 
-// kk and the mirror wavevector km of an index (k_setup without |k|).
-__device__ __forceinline__ void k_vectors(const EvalParams& p, const KIndex& q, double kk[3], double km[3]) {
-  k_components(p, q.ix, q.iy, q.iz, kk);
+// kk and the mirror wavevector km of an index in FP32 (k_setup without |k|).
+__device__ __forceinline__ void k_vectors(const EvalParams& p, const KIndex& q, float kk[3], float km[3]) {
+  double d[3], m[3];
+  k_components(p, q.ix, q.iy, q.iz, d);
   if (q.proj) {
-    k_components(p, (p.nx - q.ix) % p.nx, (p.ny - q.iy) % p.ny, q.iz, km);
+    k_components(p, (p.nx - q.ix) % p.nx, (p.ny - q.iy) % p.ny, q.iz, m);
   } else {
-    km[0] = kk[0];
-    km[1] = kk[1];
-    km[2] = kk[2];
+    m[0] = d[0];
+    m[1] = d[1];
+    m[2] = d[2];
+  }
+  for (int a = 0; a < 3; ++a) {
+    kk[a] = (float)d[a];
+    km[a] = (float)m[a];
   }
 }
 
-__device__ __forceinline__ KW table_kw(const float* __restrict__ tab, long long Nk, int s, long long idx) {
+__device__ __forceinline__ KWT<float> table_kw(const float* __restrict__ tab, long long Nk, int s, long long idx) {
   const float* t = tab + (1 + 5LL * s) * Nk + idx;
-  KW w;
+  KWT<float> w;
   w.w3 = t[0];
   w.w2 = t[Nk];
   w.fv = t[2 * Nk];
@@ -323,8 +334,8 @@ __device__ __forceinline__ KW table_kw(const float* __restrict__ tab, long long 
   return w;
 }
 
-__device__ __forceinline__ double2 c2d(fft::cpx v) { return make_double2((double)v.x, (double)v.y); }
-__device__ __forceinline__ fft::cpx d2c(double2 v) { return {(float)v.x, (float)v.y}; }
+__device__ __forceinline__ float2 c2f(fft::cpx v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ fft::cpx f2c(float2 v) { return {v.x, v.y}; }
 
 // The wavevector indices of tile element (row, q): row holds frequency
 // kx_of_row[row] after the forward DIF; q is the in-plane index.
@@ -341,7 +352,7 @@ __device__ __forceinline__ KIndex col_kindex(const EvalParams& p, int kx, long l
 // channel (and mean-field convolution) in k-space, inverse x.  Tile: in-plane
 // indices q0 .. q0 + TQ - 1 of all NX planes.
 template <int NX, bool MULTI, bool TENSOR>
-__global__ void __launch_bounds__(kColThreads, 2)
+__global__ void __launch_bounds__(kColThreads, 3)
     k_col_fwd(EvalParams p, const fft::cpx* __restrict__ prho, const double* __restrict__ mf_w,
               const float* __restrict__ wtab, fft::cpx* __restrict__ q_out, int ltq, FftTables T) {
   using Ly = Lay<MULTI, TENSOR>;
@@ -377,30 +388,30 @@ __global__ void __launch_bounds__(kColThreads, 2)
     }
     const KIndex ki = col_kindex(p, kx_of_row[row], q);
     const long long kidx = (long long)ki.ix * plane + q;
-    double kk[3], km[3];
+    float kk[3], km[3];
     k_vectors(p, ki, kk, km);
-    const double inv_k2 = wtab[kidx];
-    KW kw[kMaxSpecies];
-    double2 r[kMaxSpecies];
+    const float inv_k2 = wtab[kidx];
+    KWT<float> kw[kMaxSpecies];
+    float2 r[kMaxSpecies];
 #pragma unroll
     for (int sp = 0; sp < kMaxSpecies; ++sp) {
       if (sp < S) {
         kw[sp] = table_kw(wtab, p.Nk, sp, kidx);
-        r[sp] = c2d(R[(size_t)sp * TILE + e]);
+        r[sp] = c2f(R[(size_t)sp * TILE + e]);
       }
     }
 #pragma unroll
     for (int c = 0; c < Ly::NFMT; ++c)
-      Ch[(size_t)c * TILE + e] = d2c(fwd_value<MULTI, TENSOR>(c, p, kk, km, ki.proj, inv_k2, kw, r));
+      Ch[(size_t)c * TILE + e] = f2c(fwd_value<MULTI, TENSOR, float, float2>(c, p, kk, km, ki.proj, inv_k2, kw, r));
     // mean-field convolutions (the weight is real and even); rho_k from the
     // tile, not the register array, so no dynamic register index
     for (int m = 0; m < p.M; ++m) {
-      const double w = mf_w[m * p.Nk + kidx];
-      const double2 rv = c2d(R[(size_t)p.mf_j[m] * TILE + e]);
-      Ch[(size_t)p.mf_chan_j[m] * TILE + e] = d2c(make_double2(w * rv.x, w * rv.y));
+      const float w = (float)mf_w[m * p.Nk + kidx];
+      const float2 rv = c2f(R[(size_t)p.mf_j[m] * TILE + e]);
+      Ch[(size_t)p.mf_chan_j[m] * TILE + e] = fft::cpx{w * rv.x, w * rv.y};
       if (p.mf_chan_i[m] >= 0) {
-        const double2 ri = c2d(R[(size_t)p.mf_i[m] * TILE + e]);
-        Ch[(size_t)p.mf_chan_i[m] * TILE + e] = d2c(make_double2(w * ri.x, w * ri.y));
+        const float2 ri = c2f(R[(size_t)p.mf_i[m] * TILE + e]);
+        Ch[(size_t)p.mf_chan_i[m] * TILE + e] = fft::cpx{w * ri.x, w * ri.y};
       }
     }
   }
@@ -416,7 +427,7 @@ __global__ void __launch_bounds__(kColThreads, 2)
 // Column pass of the backward stage: every derivative channel along x, the
 // back-convolution F_s = sum_c conj(W'_cs) D_c, inverse x of F_s.
 template <int NX, bool MULTI, bool TENSOR>
-__global__ void __launch_bounds__(kColThreads, 2)
+__global__ void __launch_bounds__(kColThreads, 3)
     k_col_bwd(EvalParams p, const fft::cpx* __restrict__ pd, const float* __restrict__ wtab, fft::cpx* __restrict__ pf,
               int ltq, FftTables T) {
   using Ly = Lay<MULTI, TENSOR>;
@@ -450,17 +461,17 @@ __global__ void __launch_bounds__(kColThreads, 2)
     if (q >= plane) continue;
     const KIndex ki = col_kindex(p, kx_of_row[row], q);
     const long long kidx = (long long)ki.ix * plane + q;
-    double kk[3], km[3];
+    float kk[3], km[3];
     k_vectors(p, ki, kk, km);
-    const double inv_k2 = wtab[kidx];
-    double2 d[NF];
+    const float inv_k2 = wtab[kidx];
+    float2 d[NF];
 #pragma unroll
-    for (int c = 0; c < NF; ++c) d[c] = c2d(Dt[(size_t)c * TILE + e]);
+    for (int c = 0; c < NF; ++c) d[c] = c2f(Dt[(size_t)c * TILE + e]);
 #pragma unroll
     for (int sp = 0; sp < (MULTI ? kMaxSpecies : 1); ++sp) {
       if (sp < S) {
-        const KW w = table_kw(wtab, p.Nk, sp, kidx);
-        Dt[(size_t)sp * TILE + e] = d2c(bwd_value<MULTI, TENSOR>(sp, p, kk, km, ki.proj, inv_k2, w, d));
+        const KWT<float> w = table_kw(wtab, p.Nk, sp, kidx);
+        Dt[(size_t)sp * TILE + e] = f2c(bwd_value<MULTI, TENSOR, float, float2>(sp, p, kk, km, ki.proj, inv_k2, w, d));
       }
     }
   }

@@ -11,7 +11,8 @@ namespace cdft {
 
 namespace {
 
-constexpr size_t kSmemCap = 110 * 1024;  // two CTAs per SM
+constexpr size_t kSmemCap = 110 * 1024;     // plane kernels: two CTAs per SM at least
+constexpr size_t kColSmemCap = 74 * 1024;   // column kernels: three CTAs per SM
 
 template <int N>
 using IC = std::integral_constant<int, N>;
@@ -65,9 +66,11 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan) {
   });
   ok = ok && with_len(p.nx, [](auto) {});
   if (!ok || f.plane_smem > kSmemCap) return false;
-  // column tiles: the widest (at most 16 columns) whose buffers fit
+  // column tiles: the widest (at most 16 columns) whose buffers leave room
+  // for three CTAs per SM (one CTA's worth of buffers at the least)
   f.ltq = 4;
-  while (f.ltq > 0 && (col_smem(p.nx, f.ltq, p.S + p.n_chan) > kSmemCap || col_smem(p.nx, f.ltq, p.L.n_deriv) > kSmemCap))
+  while (f.ltq > 0 &&
+         (col_smem(p.nx, f.ltq, p.S + p.n_chan) > kColSmemCap || col_smem(p.nx, f.ltq, p.L.n_deriv) > kColSmemCap))
     --f.ltq;
   f.colf_smem = col_smem(p.nx, f.ltq, p.S + p.n_chan);
   f.colb_smem = col_smem(p.nx, f.ltq, p.L.n_deriv);
