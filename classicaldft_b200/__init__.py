@@ -12,9 +12,10 @@ from .functionals import (BARKER_HENDERSON, WEEKS_CHANDLER_ANDERSEN, Engine, EsF
                           make_ten_wolde_frenkel, make_wang_ramirez_dobnikar_frenkel, make_weights, total,
                           total_batch)
 
-from .algorithms import (Bounded, EigenvalueResult, EigenvalueSolver, Fire, MinimizationResult, Minimizer,  # noqa: F401
-                         SaddleResult, Search, Simulation, StepConfig, Unbounded, hessian_times_vector,
-                         integrating_factor_step)
+from .algorithms import (Bounded, EigenvalueResult, EigenvalueSolver, Fire, FixedMassConstraint,  # noqa: F401
+                         MinimizationResult, Minimizer, Picard, PicardResult, ReservoirBoundary, SaddleResult, Search,
+                         Simulation, Snapshot, StepConfig, Unbounded, crank_nicholson_step, fixed_mass_constraint,
+                         hessian_times_vector, integrating_factor_step, reservoir_boundary, split_operator_step)
 from .bulk import (BulkThermodynamics, Coexistence, PhaseSearch, Spinodal, density_from_chemical_potential,  # noqa: F401
                    densities_from_chemical_potentials, make_bulk_thermodynamics, make_bulk_weights)
 

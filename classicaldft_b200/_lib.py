@@ -68,6 +68,20 @@ class CDDFTConfig(ctypes.Structure):
                 ("fp_max_iterations", ctypes.c_int)]
 
 
+class CPicardConfig(ctypes.Structure):
+    _fields_ = [("mixing", ctypes.c_double), ("min_density", ctypes.c_double), ("tolerance", ctypes.c_double),
+                ("constraint_min_density", ctypes.c_double), ("max_iterations", ctypes.c_int),
+                ("check_interval", ctypes.c_int)]
+
+
+class CPicardResult(ctypes.Structure):
+    _fields_ = [("grand_potential", ctypes.c_double), ("residual", ctypes.c_double),
+                ("iterations", ctypes.c_int), ("converged", ctypes.c_int)]
+
+
+STOP_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_void_p)
+
+
 class CEigenConfig(ctypes.Structure):
     _fields_ = [("tolerance", ctypes.c_double), ("max_iterations", ctypes.c_int), ("hessian_eps", ctypes.c_double),
                 ("exact_hvp", ctypes.c_int), ("seed", ctypes.c_ulonglong)]
@@ -156,6 +170,15 @@ def lib():
                            ctypes.POINTER(ctypes.c_int), vp],
         "cdft_ddft_run": [vp, ctypes.POINTER(CDDFTConfig), ctypes.c_double, ctypes.c_int, vp, c_double_p, c_double_p,
                           vp],
+        "cdft_ddft_split_step": [vp, ctypes.POINTER(CDDFTConfig), ctypes.c_double, vp, c_double_p, vp],
+        "cdft_ddft_cn_step": [vp, ctypes.POINTER(CDDFTConfig), ctypes.c_double, vp, c_double_p,
+                              ctypes.POINTER(ctypes.c_int), vp],
+        "cdft_ddft_simulate": [vp, ctypes.POINTER(CDDFTConfig), ctypes.c_double, ctypes.c_int, vp, c_double_p,
+                               c_double_p, ctypes.c_int, c_double_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                               ctypes.POINTER(ctypes.c_int), vp, ctypes.c_double, STOP_FN, vp,
+                               ctypes.POINTER(ctypes.c_int), vp],
+        "cdft_picard": [vp, ctypes.POINTER(CPicardConfig), c_double_p, c_double_p, vp, vp,
+                        ctypes.POINTER(CPicardResult), vp],
         "cdft_hvp": [vp, vp, vp, ctypes.c_double, ctypes.c_int, vp, vp],
         "cdft_hvp_fd": [vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, vp, vp],
         "cdft_eigen_solve": [vp, ctypes.POINTER(CEigenConfig), vp, ctypes.c_double, vp, ctypes.c_int, c_double_p,

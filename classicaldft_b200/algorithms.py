@@ -194,6 +194,104 @@ class Minimizer:
         return res
 
 
+# ---------------------------------------------------------------- Picard
+
+
+@dataclass
+class FixedMassConstraint:
+    """fixed_mass_constraint (minimization.hpp:159-180): after every update
+    the excess over the background is rescaled to the target mass."""
+
+    target_masses: list
+    backgrounds: list
+    cell_volume: float
+    min_density: float = 1e-30
+
+
+def fixed_mass_constraint(target_masses, backgrounds, cell_volume, min_density=1e-30):
+    """minimization.hpp:159-180."""
+    return FixedMassConstraint(list(np.atleast_1d(np.asarray(target_masses, dtype=np.float64))), list(backgrounds),
+                               float(cell_volume), float(min_density))
+
+
+@dataclass
+class PicardResult:
+    """picard.hpp:23-29."""
+
+    densities: list
+    grand_potential: float
+    residual: float
+    iterations: int
+    converged: bool
+
+
+@dataclass
+class Picard:
+    """picard.hpp:31-42 on the device: rho <- max(rho exp(-mixing force / dV),
+    min_density) until the force RMS or the change of Omega falls below the
+    tolerance.  log_interval is kept for the interface and prints nothing;
+    check_interval is how many iterations run between host checks."""
+
+    mixing: float = 0.01
+    min_density: float = 1e-30
+    tolerance: float = 1e-6
+    max_iterations: int = 5000
+    log_interval: int = 500
+    check_interval: int = 25
+
+    def _c(self):
+        return _lib.CPicardConfig(self.mixing, self.min_density, self.tolerance, 1e-30, self.max_iterations,
+                                  self.check_interval)
+
+    def _solve(self, weights: Weights, rho, mus, constraint):
+        torch = _torch()
+        e = weights.engine
+        B, N = e.batch, e.N
+        if e.S != 1:
+            raise ValueError("Picard: single-species engines")
+        if isinstance(rho, np.ndarray) or not hasattr(rho, "data_ptr"):
+            d = torch.tensor(np.asarray(rho, dtype=np.float64).reshape(B, N), device="cuda")
+            host = True
+        else:
+            d = rho.reshape(B, N).to(torch.float64).contiguous().clone()
+            host = False
+        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mus, dtype=np.float64), (B,)))
+        mass = None
+        bg = None
+        cfg = self._c()
+        if constraint is not None:
+            if abs(constraint.cell_volume - e.grid.cell_volume) > 1e-12 * e.grid.cell_volume:
+                raise ValueError("fixed_mass_constraint: cell_volume differs from the grid's")
+            mass = np.ascontiguousarray(np.broadcast_to(np.asarray(constraint.target_masses, dtype=np.float64)
+                                                        .reshape(-1)[:B], (B,)))
+            if constraint.backgrounds is not None and len(constraint.backgrounds):
+                b = np.asarray([np.asarray(x, dtype=np.float64).reshape(-1) for x in constraint.backgrounds])
+                bg = torch.tensor(np.broadcast_to(b.reshape(-1, N), (B, N)).copy(), device="cuda")
+            cfg.constraint_min_density = constraint.min_density
+        res = (_lib.CPicardResult * B)()
+        _lib.check(_lib.lib().cdft_picard(
+            e.handle, ctypes.byref(cfg), mu.ctypes.data_as(_lib.c_double_p),
+            None if mass is None else mass.ctypes.data_as(_lib.c_double_p),
+            None if bg is None else bg.data_ptr(), d.data_ptr(), res, _stream()))
+        torch.cuda.synchronize()
+        out = d.cpu().numpy() if host else d
+        return [PicardResult([out[b]], r.grand_potential, r.residual, r.iterations, bool(r.converged))
+                for b, r in enumerate(res)]
+
+    def solve(self, densities, weights: Weights, chemical_potential=0.0, constraint: FixedMassConstraint = None):
+        """picard.hpp:63-124 for one state (engine batch 1)."""
+        if weights.engine.batch != 1:
+            raise ValueError("Picard.solve: an engine with batch 1 (solve_batch for more)")
+        rho = densities[0] if isinstance(densities, (list, tuple)) else densities
+        return self._solve(weights, rho, [chemical_potential], constraint)[0]
+
+    def solve_batch(self, densities, weights: Weights, chemical_potentials, constraint: FixedMassConstraint = None):
+        """``solve`` for every problem of a batched engine: densities (B, N),
+        chemical_potentials (B,); a constraint's target_masses (B,) and
+        backgrounds (B, N) or one background for all."""
+        return self._solve(weights, densities, chemical_potentials, constraint)
+
+
 # ---------------------------------------------------------------- DDFT
 
 
@@ -230,26 +328,138 @@ def integrating_factor_step(density, weights: Weights, config: StepConfig, chemi
     return (d.cpu().numpy() if host else d), e.value, c.dt
 
 
+def _ddft_single(fn, density, weights: Weights, config: StepConfig, chemical_potential, with_iterations):
+    torch = _torch()
+    d, host = _dev(density)
+    if not host:
+        d = d.clone()
+    c = config.c()
+    e = ctypes.c_double()
+    args = [weights.engine.handle, ctypes.byref(c), chemical_potential, d.data_ptr(), ctypes.byref(e)]
+    if with_iterations:
+        args.append(ctypes.byref(ctypes.c_int()))
+    _lib.check(fn(*args, _stream()))
+    torch.cuda.synchronize()
+    return (d.cpu().numpy() if host else d), e.value, config.dt
+
+
+def split_operator_step(density, weights: Weights, config: StepConfig, chemical_potential=0.0):
+    """dynamics.hpp:410-465 (Strang splitting: half diffusion, explicit
+    excess step, half diffusion); returns (density, energy, dt_used)."""
+    return _ddft_single(_lib.lib().cdft_ddft_split_step, density, weights, config, chemical_potential, False)
+
+
+def crank_nicholson_step(density, weights: Weights, config: StepConfig, chemical_potential=0.0):
+    """dynamics.hpp:472-538 (Crank-Nicolson fixed point); returns
+    (density, energy, dt_used)."""
+    return _ddft_single(_lib.lib().cdft_ddft_cn_step, density, weights, config, chemical_potential, True)
+
+
+@dataclass
+class ReservoirBoundary:
+    """reservoir_boundary (dynamics.hpp:551-557): the cells where mask is
+    true are reset to reservoir_density after every DDFT step."""
+
+    mask: np.ndarray
+    reservoir_density: float
+
+
+def reservoir_boundary(mask, reservoir_density):
+    """dynamics.hpp:551-557."""
+    return ReservoirBoundary(np.asarray(mask).reshape(-1).astype(bool), float(reservoir_density))
+
+
+@dataclass
+class Snapshot:
+    """dynamics.hpp:45-50."""
+
+    step: int
+    time: float
+    energy: float
+    densities: list
+
+
 @dataclass
 class Simulation:
-    """dynamics.hpp:564-693 (integrating-factor DDFT with adaptive dt)."""
+    """dynamics.hpp:564-693 (integrating-factor DDFT with adaptive dt).
+
+    The steps, the snapshots (copied to pinned host memory while the next
+    steps run), the reservoir boundary and the stop test run through one
+    call of the device driver.  ``times`` / ``energies`` of the result hold
+    the entries the reference records (step 0, every log_interval-th step
+    and the last one); ``all_times`` / ``all_energies`` hold every step.
+    ``stop_condition(step, time, energy) -> bool`` ends the run early.
+    """
 
     step: StepConfig = field(default_factory=StepConfig)
     n_steps: int = 1000
+    snapshot_interval: int = 100
+    log_interval: int = 50
+    energy_offset: float = 0.0
+    boundary: ReservoirBoundary = None
+    stop_condition: object = None
 
     def run(self, densities, weights: Weights, chemical_potential=0.0):
         torch = _torch()
         d, host = _dev(densities[0] if isinstance(densities, (list, tuple)) else densities)
         if not host:
             d = d.clone()
+        n = d.numel()
+        dv = weights.engine.grid.cell_volume
         c = self.step.c()
         times = np.zeros(self.n_steps + 1)
         energies = np.zeros(self.n_steps + 1)
-        _lib.check(_lib.lib().cdft_ddft_run(weights.engine.handle, ctypes.byref(c), chemical_potential, self.n_steps,
-                                            d.data_ptr(), times.ctypes.data_as(_lib.c_double_p),
-                                            energies.ctypes.data_as(_lib.c_double_p), _stream()))
+        cap = 0
+        if self.snapshot_interval > 0:
+            cap = 1 + self.n_steps // self.snapshot_interval
+        snaps = torch.empty((max(cap, 1), n), dtype=torch.float64).pin_memory() if cap else None
+        snap_steps = (ctypes.c_int * max(cap, 1))()
+        count = ctypes.c_int()
+        done = ctypes.c_int()
+        mask_dev = None
+        res_density = 0.0
+        if self.boundary is not None:
+            m = np.asarray(self.boundary.mask).reshape(-1)
+            if m.size != n:
+                raise ValueError("reservoir mask: one entry per grid point")
+            mask_dev = torch.tensor(m.astype(np.uint8), device="cuda")
+            res_density = self.boundary.reservoir_density
+        err = []
+
+        def _stop(step, time, energy, _user):
+            try:
+                return 1 if self.stop_condition(step, time, energy) else 0
+            except Exception as exc:  # surfaced after the run
+                err.append(exc)
+                return 1
+
+        cb = _lib.STOP_FN(_stop) if self.stop_condition is not None else _lib.STOP_FN()
+        if mask_dev is not None:
+            d.masked_fill_(mask_dev.bool(), res_density)  # the driver applies it too; the initial mass needs it
+        mass_initial = float(torch.sum(d).item()) * dv
+        _lib.check(_lib.lib().cdft_ddft_simulate(
+            weights.engine.handle, ctypes.byref(c), chemical_potential, self.n_steps, d.data_ptr(),
+            times.ctypes.data_as(_lib.c_double_p), energies.ctypes.data_as(_lib.c_double_p), self.snapshot_interval,
+            ctypes.cast(snaps.data_ptr(), _lib.c_double_p) if snaps is not None else None, snap_steps, cap,
+            ctypes.byref(count), mask_dev.data_ptr() if mask_dev is not None else None, res_density, cb, None,
+            ctypes.byref(done), _stream()))
         torch.cuda.synchronize()
-        return {"densities": [d.cpu().numpy() if host else d], "times": times, "energies": energies, "dt": c.dt}
+        if err:
+            raise err[0]
+        steps = done.value
+        snapshots = []
+        for k in range(count.value):
+            st = snap_steps[k]
+            rho_k = snaps[k].numpy().copy() if host else snaps[k].to(d.device)
+            snapshots.append(Snapshot(st, float(times[st]), float(energies[st]), [rho_k]))
+        idx = [0]
+        if self.log_interval > 0:
+            idx += [s for s in range(1, steps + 1) if s % self.log_interval == 0 or s == self.n_steps]
+        out = d.cpu().numpy() if host else d
+        return {"densities": [out], "times": [float(times[i]) for i in idx],
+                "energies": [float(energies[i]) for i in idx], "snapshots": snapshots,
+                "mass_initial": mass_initial, "mass_final": float(torch.sum(d).item()) * dv, "dt": c.dt,
+                "steps": steps, "all_times": times[:steps + 1], "all_energies": energies[:steps + 1]}
 
 
 # ---------------------------------------------------------- saddle point

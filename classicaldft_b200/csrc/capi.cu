@@ -413,40 +413,88 @@ int cdft_ddft_run(cdft_engine* engine, cdft_ddft_config* cfg, double chemical_po
   return guarded([&] {
     if (!cfg || !rho || n_steps < 0) throw std::invalid_argument("cfg, rho and n_steps >= 0 are required");
     cdft::Drivers& d = drivers_of(engine);
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     cdft::Drivers::DDFTConfig dc = to_ddft(*cfg, chemical_potential);
-    // Simulation::run (dynamics.hpp:597-649): initial energy, then steps with
-    // the adaptive time step.
-    double* fscratch = nullptr;
-    CDFT_CUDA(cudaMalloc(&fscratch, sizeof(double) * engine->impl->points()));
+    d.ddft_run(dc, n_steps, rho, times, energies, 0, nullptr, nullptr, nullptr, nullptr,
+               static_cast<cudaStream_t>(stream));
+    cfg->dt = dc.dt;
+  });
+}
+
+int cdft_ddft_split_step(cdft_engine* engine, const cdft_ddft_config* cfg, double chemical_potential, double* rho,
+                         double* energy, void* stream) {
+  return guarded([&] {
+    if (!cfg || !rho) throw std::invalid_argument("cfg and rho are required");
+    cdft::Drivers& d = drivers_of(engine);
+    const double e = d.ddft_split_step(to_ddft(*cfg, chemical_potential), rho, static_cast<cudaStream_t>(stream));
+    if (energy) *energy = e;
+  });
+}
+
+int cdft_ddft_cn_step(cdft_engine* engine, const cdft_ddft_config* cfg, double chemical_potential, double* rho,
+                      double* energy, int* fp_iterations, void* stream) {
+  return guarded([&] {
+    if (!cfg || !rho) throw std::invalid_argument("cfg and rho are required");
+    cdft::Drivers& d = drivers_of(engine);
+    const double e =
+        d.ddft_cn_step(to_ddft(*cfg, chemical_potential), rho, static_cast<cudaStream_t>(stream), fp_iterations);
+    if (energy) *energy = e;
+  });
+}
+
+int cdft_ddft_simulate(cdft_engine* engine, cdft_ddft_config* cfg, double chemical_potential, int n_steps,
+                       double* rho, double* times, double* energies, int snapshot_interval, double* snapshots,
+                       int* snapshot_steps, int snapshot_capacity, int* snapshot_count,
+                       const unsigned char* reservoir_mask, double reservoir_density, cdft_ddft_stop_fn stop,
+                       void* user, int* steps_done, void* stream) {
+  return guarded([&] {
+    if (!cfg || !rho || n_steps < 0) throw std::invalid_argument("cfg, rho and n_steps >= 0 are required");
+    if (snapshot_interval < 0 || snapshot_capacity < 0 || (snapshot_capacity > 0 && !snapshots))
+      throw std::invalid_argument("snapshots: interval >= 0, and a buffer for a positive capacity");
+    cdft::Drivers& d = drivers_of(engine);
+    cdft::Drivers::DDFTConfig dc = to_ddft(*cfg, chemical_potential);
+    cdft::Drivers::SnapshotSink sink;
+    sink.host = snapshots;
+    sink.steps = snapshot_steps;
+    sink.capacity = snapshot_capacity;
+    int done = 0;
     try {
-      const double e0 = d.force(rho, fscratch, chemical_potential, 0, st);
-      if (times) times[0] = 0.0;
-      if (energies) energies[0] = e0;
-      int successes = 0;
-      double time = 0.0;
-      for (int step = 1; step <= n_steps; ++step) {
-        const double dt_before = dc.dt;
-        const double e = d.ddft_step(dc, rho, st, nullptr);
-        const double dt_used = dc.dt;
-        time += dt_used;
-        if (dt_used < dt_before)
-          successes = 0;
-        else
-          ++successes;
-        if (successes >= 5 && dc.dt < dc.dt_max) {
-          dc.dt = std::min(2.0 * dc.dt, dc.dt_max);
-          successes = 0;
-        }
-        if (times) times[step] = time;
-        if (energies) energies[step] = e;
-      }
+      cdft::Drivers::Reservoir res;
+      res.mask = reservoir_mask;
+      res.density = reservoir_density;
+      done = d.ddft_run(dc, n_steps, rho, times, energies, snapshot_interval, &sink, stop, user, &res,
+                        static_cast<cudaStream_t>(stream));
     } catch (...) {
-      cudaFree(fscratch);
+      if (snapshot_count) *snapshot_count = sink.count;
       throw;
     }
-    cudaFree(fscratch);
     cfg->dt = dc.dt;
+    if (snapshot_count) *snapshot_count = sink.count;
+    if (steps_done) *steps_done = done;
+  });
+}
+
+int cdft_picard(cdft_engine* engine, const cdft_picard_config* cfg, const double* mu, const double* target_mass,
+                const double* background, double* rho, cdft_picard_result* results, void* stream) {
+  return guarded([&] {
+    if (!cfg || !mu || !rho || !results) throw std::invalid_argument("cfg, mu, rho and results are required");
+    if (!(cfg->mixing > 0.0) || cfg->max_iterations < 0)
+      throw std::invalid_argument("picard: mixing > 0 and max_iterations >= 0 are required");
+    cdft::Drivers& d = drivers_of(engine, true);
+    cdft::Drivers::PicardConfig pc;
+    pc.mixing = cfg->mixing;
+    pc.min_density = cfg->min_density;
+    pc.tolerance = cfg->tolerance;
+    pc.constraint_min_density = cfg->constraint_min_density;
+    pc.max_iterations = cfg->max_iterations;
+    pc.check_interval = cfg->check_interval > 0 ? cfg->check_interval : 25;
+    std::vector<cdft::Drivers::PicardResult> r =
+        d.picard(pc, mu, target_mass, background, rho, static_cast<cudaStream_t>(stream));
+    for (size_t b = 0; b < r.size(); ++b) {
+      results[b].grand_potential = r[b].grand_potential;
+      results[b].residual = r[b].residual;
+      results[b].iterations = r[b].iterations;
+      results[b].converged = r[b].converged ? 1 : 0;
+    }
   });
 }
 

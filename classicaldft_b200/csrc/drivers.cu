@@ -544,6 +544,178 @@ __global__ void k_face_sum(const double* __restrict__ rho, long long n, int nx, 
   block_sum_store(s, partials);
 }
 
+// --------------------------------------------------- split / CN DDFT steps
+
+// |k|^2 of half-spectrum index pos (dynamics.hpp:310-318: the wavevector of
+// grid.hpp with the Nyquist index positive).
+__device__ __forceinline__ double k_squared(long long pos, int nx, int ny, int nzh, int nz, double dx) {
+  const int iz = (int)(pos % nzh);
+  const long long t = pos / nzh;
+  const int iy = (int)(t % ny);
+  const int ix = (int)(t / ny);
+  const double kx = 2.0 * 3.14159265358979323846 / (nx * dx) * (double)(ix <= nx / 2 ? ix : ix - nx);
+  const double ky = 2.0 * 3.14159265358979323846 / (ny * dx) * (double)(iy <= ny / 2 ? iy : iy - ny);
+  const double kz = 2.0 * 3.14159265358979323846 / (nz * dx) * (double)iz;
+  return kx * kx + ky * ky + kz * kz;
+}
+
+// work *= sqrt(exp(-D k^2 dt)) (the half propagator of dynamics.hpp:426).
+__global__ void k_half_diffusion(double2* __restrict__ work, int nx, int ny, int nzh, int nz, double dx, double D,
+                                 double dt) {
+  const long long Nk = (long long)nx * ny * nzh;
+  for (long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x; pos < Nk;
+       pos += (long long)gridDim.x * blockDim.x) {
+    const double h = sqrt(exp(-D * k_squared(pos, nx, ny, nzh, nz, dx) * dt));
+    const double2 v = work[pos];
+    work[pos] = make_double2(v.x * h, v.y * h);
+  }
+}
+
+// out = max(in * scale + dt * add, min_density) (add may be null).
+__global__ void k_scale_clamp(const double* __restrict__ in, const double* __restrict__ add, double* __restrict__ out,
+                              long long N, double scale, double dt, double min_density) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    double v = in[i] * scale;
+    if (add) v += dt * add[i];
+    out[i] = v < min_density ? min_density : v;
+  }
+}
+
+// The Crank-Nicolson update of dynamics.hpp:518-521 in k-space:
+// wk = ((1 - a) rho0_k + dt/2 (R0_k + R1_k)) / (1 + a), a = D k^2 dt / 2.
+__global__ void k_cn_combine(const double2* __restrict__ rho0k, const double2* __restrict__ r0k,
+                             double2* __restrict__ r1k_work, int nx, int ny, int nzh, int nz, double dx, double D,
+                             double dt) {
+  const long long Nk = (long long)nx * ny * nzh;
+  for (long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x; pos < Nk;
+       pos += (long long)gridDim.x * blockDim.x) {
+    const double a = D * k_squared(pos, nx, ny, nzh, nz, dx) * dt * 0.5;
+    const double cm = 1.0 - a, cpi = 1.0 / (1.0 + a);
+    const double2 r0 = rho0k[pos], q0 = r0k[pos], q1 = r1k_work[pos];
+    r1k_work[pos] = make_double2((cm * r0.x + (dt * 0.5) * (q0.x + q1.x)) * cpi,
+                                 (cm * r0.y + (dt * 0.5) * (q0.y + q1.y)) * cpi);
+  }
+}
+
+// d1_new = max(work / N, min); partial max |d1_new - d1|; d1 = d1_new.
+__global__ void k_cn_update(const double* __restrict__ work, double* __restrict__ d1, long long N, double inv_n,
+                            double min_density, double* __restrict__ partials) {
+  double mx = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    double nv = work[i] * inv_n;
+    nv = nv < min_density ? min_density : nv;
+    const double dev = fabs(nv - d1[i]);
+    mx = dev > mx ? dev : mx;
+    d1[i] = nv;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+  __shared__ double smx[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) smx[warp] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) mx = fmax(mx, smx[w]);
+    partials[blockIdx.x * 2 + 0] = fmax(mx, smx[0]);
+    partials[blockIdx.x * 2 + 1] = 0.0;
+  }
+}
+
+__global__ void k_reservoir_fill(double* __restrict__ rho, const unsigned char* __restrict__ mask, long long N,
+                                 double value) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+    if (mask[i]) rho[i] = value;
+}
+
+// ------------------------------------------------------------------ Picard
+
+struct PicardDevState {
+  double omega, omega_prev, residual, target_mass, scale;
+  int iter, active, converged, apply;
+};
+
+// sums [sum f^2] of problem blockIdx.y
+__global__ void k_sum_sq(const double* __restrict__ f, long long N, double* __restrict__ partials) {
+  f += (long long)blockIdx.y * N;
+  double s[kRedTerms] = {0, 0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+    s[0] += f[i] * f[i];
+  block_sum_store(s, partials);
+}
+
+// picard.hpp:81-106: residual, the two convergence tests, Omega bookkeeping.
+__global__ void k_picard_control(PicardDevState* st, const double* __restrict__ sums, const double* __restrict__ scal,
+                                 double n_dof, double tol) {
+  st += blockIdx.x;
+  sums += blockIdx.x * kOut;
+  scal += blockIdx.x * kScalarCount;
+  if (threadIdx.x != 0 || !st->active) return;
+  st->omega = scal[1];
+  st->residual = sqrt(sums[0] / n_dof);
+  const bool force_conv = st->residual < tol;
+  const bool omega_conv = st->iter > 0 && fabs(st->omega - st->omega_prev) < tol;
+  if (force_conv || omega_conv) {
+    st->converged = 1;
+    st->active = 0;
+    return;
+  }
+  st->omega_prev = st->omega;
+}
+
+// picard.hpp:108-111: rho *= exp(-mixing f / dV), clamped at min_density.
+__global__ void k_picard_update(double* __restrict__ rho, const double* __restrict__ f,
+                                const PicardDevState* __restrict__ st, long long N, double mixing_over_dv,
+                                double min_density) {
+  st += blockIdx.y;
+  if (!st->active) return;
+  rho += (long long)blockIdx.y * N;
+  f += (long long)blockIdx.y * N;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    const double v = rho[i] * exp(-mixing_over_dv * f[i]);
+    rho[i] = v < min_density ? min_density : v;
+  }
+}
+
+// sums [sum (rho - background)] of problem blockIdx.y (background may be null)
+__global__ void k_excess_sum(const double* __restrict__ rho, const double* __restrict__ bg, long long N,
+                             double* __restrict__ partials) {
+  rho += (long long)blockIdx.y * N;
+  if (bg) bg += (long long)blockIdx.y * N;
+  double s[kRedTerms] = {0, 0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+    s[0] += rho[i] - (bg ? bg[i] : 0.0);
+  block_sum_store(s, partials);
+}
+
+// minimization.hpp:169-175: the mass rescale of the excess over the background.
+__global__ void k_picard_mass(PicardDevState* st, const double* __restrict__ sums, double dv) {
+  st += blockIdx.x;
+  sums += blockIdx.x * kOut;
+  if (threadIdx.x != 0) return;
+  const double mass = sums[0] * dv;
+  st->apply = (st->active && fabs(mass) > 1e-30) ? 1 : 0;
+  st->scale = st->apply ? st->target_mass / mass : 1.0;
+}
+
+__global__ void k_picard_rescale(double* __restrict__ rho, const double* __restrict__ bg,
+                                 const PicardDevState* __restrict__ st, long long N, double min_density) {
+  st += blockIdx.y;
+  if (!st->apply) return;
+  rho += (long long)blockIdx.y * N;
+  if (bg) bg += (long long)blockIdx.y * N;
+  const double sc = st->scale;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    const double b = bg ? bg[i] : 0.0;
+    const double v = b + sc * (rho[i] - b);
+    rho[i] = v < min_density ? min_density : v;
+  }
+}
+
+__global__ void k_picard_count(PicardDevState* st) {
+  st += blockIdx.x;
+  if (threadIdx.x == 0 && st->active) st->iter++;
+}
+
 // Symmetric eigen-decomposition of a small matrix (cyclic Jacobi); returns
 // the eigenvector of the smallest eigenvalue (the reference takes column 0
 // of arma::eig_sym, saddle_point.hpp:251-254).
@@ -620,6 +792,12 @@ Drivers::~Drivers() {
   for (double* p : ev_)
     if (p) cudaFree(p);
   if (st_host_) cudaFreeHost(st_host_);
+  for (int i = 0; i < 2; ++i) {
+    if (snap_stage_[i]) cudaFree(snap_stage_[i]);
+    if (snap_ready_[i]) cudaEventDestroy(snap_ready_[i]);
+    if (snap_done_[i]) cudaEventDestroy(snap_done_[i]);
+  }
+  if (copy_stream_) cudaStreamDestroy(copy_stream_);
   if (host_pin_) cudaFreeHost(host_pin_);
   if (ddft_ready_) {
     cufftDestroy(plan_r2c_);
@@ -1041,6 +1219,209 @@ Drivers::SaddleResult Drivers::saddle_find(const SaddleConfig& cfg, double* rho,
   res.grand_potential = omega;
   res.outer_iterations = std::min(outer + 1, cfg.max_outer_iterations);
   return res;
+}
+
+// ---------------------------------------------------- split / CN / run
+
+double Drivers::ddft_split_step(const DDFTConfig& cfg, double* rho, cudaStream_t stream) {
+  ensure_ddft();
+  const EvalParams& p = eng_.params();
+  CDFT_CUFFT(cufftSetStream(plan_r2c_, stream));
+  CDFT_CUFFT(cufftSetStream(plan_c2r_, stream));
+  double2* work = static_cast<double2*>(ddft_k_);
+  const double inv_n = 1.0 / (double)N_;
+  double* star = x_;   // rho*, then rho**
+  double* f = grad_;
+  double* rhs = tmp_;
+  // half diffusion (dynamics.hpp:423-437)
+  CDFT_CUFFT(cufftExecD2Z(plan_r2c_, rho, work));
+  k_half_diffusion<<<grid_, kBlock, 0, stream>>>(work, p.nx, p.ny, p.nzh, p.nz, p.dx, cfg.diffusion, cfg.dt);
+  CDFT_CUFFT(cufftExecZ2D(plan_c2r_, work, tmp2_));
+  k_scale_clamp<<<grid_, kBlock, 0, stream>>>(tmp2_, nullptr, star, N_, inv_n, 0.0, cfg.min_density);
+  // forward-Euler excess step (dynamics.hpp:439-443)
+  eng_.evaluate(star, nullptr, &cfg.mu, f, scalars_, stream);
+  k_ddft_rhs<<<grid_, kBlock, 0, stream>>>(star, f, rhs, p.nx, p.ny, p.nz, p.dx, 1.0 / p.dv);
+  k_scale_clamp<<<grid_, kBlock, 0, stream>>>(star, rhs, star, N_, 1.0, cfg.dt, cfg.min_density);
+  // half diffusion (dynamics.hpp:445-456)
+  CDFT_CUFFT(cufftExecD2Z(plan_r2c_, star, work));
+  k_half_diffusion<<<grid_, kBlock, 0, stream>>>(work, p.nx, p.ny, p.nzh, p.nz, p.dx, cfg.diffusion, cfg.dt);
+  CDFT_CUFFT(cufftExecZ2D(plan_c2r_, work, tmp2_));
+  k_scale_clamp<<<grid_, kBlock, 0, stream>>>(tmp2_, nullptr, rho, N_, inv_n, 0.0, cfg.min_density);
+  CDFT_CUDA(cudaGetLastError());
+  return force(rho, f, cfg.mu, 0, stream);  // the energy of the final state (dynamics.hpp:458)
+}
+
+double Drivers::ddft_cn_step(const DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations) {
+  ensure_ddft();
+  const EvalParams& p = eng_.params();
+  CDFT_CUFFT(cufftSetStream(plan_r2c_, stream));
+  CDFT_CUFFT(cufftSetStream(plan_c2r_, stream));
+  double2* rho0k = static_cast<double2*>(ddft_k_);
+  double2* r0k = rho0k + p.Nk;
+  double2* work = r0k + p.Nk;
+  double* d1 = x_;
+  double* f = grad_;
+  double* rhs = tmp_;
+  const double inv_n = 1.0 / (double)N_;
+  // rho0_k, R0_k (dynamics.hpp:491-500)
+  CDFT_CUFFT(cufftExecD2Z(plan_r2c_, rho, rho0k));
+  eng_.evaluate(rho, nullptr, &cfg.mu, f, scalars_, stream);
+  k_ddft_rhs<<<grid_, kBlock, 0, stream>>>(rho, f, rhs, p.nx, p.ny, p.nz, p.dx, 1.0 / p.dv);
+  CDFT_CUFFT(cufftExecD2Z(plan_r2c_, rhs, r0k));
+  CDFT_CUDA(cudaMemcpyAsync(d1, rho, sizeof(double) * N_, cudaMemcpyDeviceToDevice, stream));
+  int it = 0;
+  for (; it < cfg.fp_max_iterations; ++it) {  // dynamics.hpp:505-530
+    eng_.evaluate(d1, nullptr, &cfg.mu, f, scalars_, stream);
+    k_ddft_rhs<<<grid_, kBlock, 0, stream>>>(d1, f, rhs, p.nx, p.ny, p.nz, p.dx, 1.0 / p.dv);
+    CDFT_CUFFT(cufftExecD2Z(plan_r2c_, rhs, work));
+    k_cn_combine<<<grid_, kBlock, 0, stream>>>(rho0k, r0k, work, p.nx, p.ny, p.nzh, p.nz, p.dx, cfg.diffusion,
+                                               cfg.dt);
+    CDFT_CUFFT(cufftExecZ2D(plan_c2r_, work, tmp2_));
+    k_cn_update<<<grid_, kBlock, 0, stream>>>(tmp2_, d1, N_, inv_n, cfg.min_density, red_);
+    k_maxmin_finish<<<1, 32, 0, stream>>>(red_, grid_, red_out_);
+    CDFT_CUDA(cudaMemcpyAsync(host_pin_, red_out_, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    CDFT_CUDA(cudaStreamSynchronize(stream));
+    if (host_pin_[0] < cfg.fp_tolerance) {
+      ++it;
+      break;
+    }
+  }
+  if (fp_iterations) *fp_iterations = it;
+  CDFT_CUDA(cudaMemcpyAsync(rho, d1, sizeof(double) * N_, cudaMemcpyDeviceToDevice, stream));
+  return force(rho, f, cfg.mu, 0, stream);  // dynamics.hpp:532
+}
+
+int Drivers::ddft_run(DDFTConfig& cfg, int n_steps, double* rho, double* times, double* energies,
+                      int snapshot_interval, SnapshotSink* snaps, StopFn stop, void* user, const Reservoir* reservoir,
+                      cudaStream_t stream) {
+  const bool res = reservoir && reservoir->mask;
+  auto apply_boundary = [&]() {
+    if (res) k_reservoir_fill<<<grid_, kBlock, 0, stream>>>(rho, reservoir->mask, N_, reservoir->density);
+  };
+  const bool snapping = snaps && snaps->host && snapshot_interval > 0 && snaps->capacity > 0;
+  if (snapping && !copy_stream_) {
+    CDFT_CUDA(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+      CDFT_CUDA(cudaMalloc(&snap_stage_[i], sizeof(double) * N_));
+      CDFT_CUDA(cudaEventCreateWithFlags(&snap_ready_[i], cudaEventDisableTiming));
+      CDFT_CUDA(cudaEventCreateWithFlags(&snap_done_[i], cudaEventDisableTiming));
+    }
+  }
+  if (snaps) snaps->count = 0;
+  int issued = 0;
+  // the snapshot of the current density: a device copy into a staging
+  // buffer on the compute stream, then its D2H copy on the copy stream, so
+  // the next steps run while it drains
+  auto snapshot = [&](int step) {
+    if (!snapping || snaps->count >= snaps->capacity) return;
+    const int k = issued & 1;
+    if (issued >= 2) CDFT_CUDA(cudaStreamWaitEvent(stream, snap_done_[k], 0));
+    CDFT_CUDA(cudaMemcpyAsync(snap_stage_[k], rho, sizeof(double) * N_, cudaMemcpyDeviceToDevice, stream));
+    CDFT_CUDA(cudaEventRecord(snap_ready_[k], stream));
+    CDFT_CUDA(cudaStreamWaitEvent(copy_stream_, snap_ready_[k], 0));
+    CDFT_CUDA(cudaMemcpyAsync(snaps->host + (size_t)snaps->count * N_, snap_stage_[k], sizeof(double) * N_,
+                              cudaMemcpyDeviceToHost, copy_stream_));
+    CDFT_CUDA(cudaEventRecord(snap_done_[k], copy_stream_));
+    if (snaps->steps) snaps->steps[snaps->count] = step;
+    ++snaps->count;
+    ++issued;
+  };
+  // Simulation::run (dynamics.hpp:597-649): initial energy, then steps with
+  // the adaptive time step
+  apply_boundary();
+  const double e0 = force(rho, tmp2_, cfg.mu, 0, stream);
+  if (times) times[0] = 0.0;
+  if (energies) energies[0] = e0;
+  snapshot(0);
+  int successes = 0, step = 1;
+  double time = 0.0;
+  for (; step <= n_steps; ++step) {
+    const double dt_before = cfg.dt;
+    const double e = ddft_step(cfg, rho, stream, nullptr);
+    const double dt_used = cfg.dt;
+    time += dt_used;
+    apply_boundary();
+    if (dt_used < dt_before)
+      successes = 0;
+    else
+      ++successes;
+    if (successes >= 5 && cfg.dt < cfg.dt_max) {
+      cfg.dt = std::min(2.0 * cfg.dt, cfg.dt_max);
+      successes = 0;
+    }
+    if (times) times[step] = time;
+    if (energies) energies[step] = e;
+    if (snapshot_interval > 0 && step % snapshot_interval == 0) snapshot(step);
+    if (stop && stop(step, time, e, user)) {
+      ++step;
+      break;
+    }
+  }
+  if (snapping) CDFT_CUDA(cudaStreamSynchronize(copy_stream_));
+  return step - 1;
+}
+
+// ------------------------------------------------------------------ Picard
+
+std::vector<Drivers::PicardResult> Drivers::picard(const PicardConfig& cfg, const double* mu, const double* mass,
+                                                   const double* background, double* rho, cudaStream_t stream) {
+  const EvalParams& p = eng_.params();
+  const int B = B_;
+  if (!(cfg.mixing > 0.0) || cfg.max_iterations < 0) throw Error(-1, "picard: mixing > 0 and max_iterations >= 0");
+  std::vector<double> muv(mu, mu + B);
+  PicardDevState* st = reinterpret_cast<PicardDevState*>(st_);  // the FIRE state slots (larger) hold it
+  static_assert(sizeof(PicardDevState) <= sizeof(FireDevState), "state slot");
+  std::vector<PicardDevState> h(B);
+  for (int b = 0; b < B; ++b) {
+    h[b] = PicardDevState{};
+    h[b].active = 1;
+    h[b].scale = 1.0;
+    h[b].target_mass = mass ? mass[b] : 0.0;
+  }
+  CDFT_CUDA(cudaMemcpyAsync(st, h.data(), sizeof(PicardDevState) * B, cudaMemcpyHostToDevice, stream));
+  const dim3 gv(grid_, B);
+  const int rt = 32 * kRedTerms;
+  const double n_dof = (double)N_;
+  int steps = 0;
+  auto all_done = [&]() {
+    CDFT_CUDA(cudaMemcpyAsync(h.data(), st, sizeof(PicardDevState) * B, cudaMemcpyDeviceToHost, stream));
+    CDFT_CUDA(cudaStreamSynchronize(stream));
+    for (const auto& x : h)
+      if (x.active) return false;
+    return true;
+  };
+  while (steps < cfg.max_iterations && !all_done()) {
+    const int chunk = std::max(1, std::min(cfg.check_interval, cfg.max_iterations - steps));
+    for (int k = 0; k < chunk; ++k) {
+      eng_.evaluate(rho, nullptr, muv.data(), grad_, scalars_, stream);
+      k_sum_sq<<<gv, kBlock, 0, stream>>>(grad_, N_, red_);
+      k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
+      k_picard_control<<<B, 32, 0, stream>>>(st, red_out_, scalars_, n_dof, cfg.tolerance);
+      k_picard_update<<<gv, kBlock, 0, stream>>>(rho, grad_, st, N_, cfg.mixing / p.dv, cfg.min_density);
+      if (mass) {
+        k_excess_sum<<<gv, kBlock, 0, stream>>>(rho, background, N_, red_);
+        k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
+        k_picard_mass<<<B, 32, 0, stream>>>(st, red_out_, p.dv);
+        k_picard_rescale<<<gv, kBlock, 0, stream>>>(rho, background, st, N_, cfg.constraint_min_density);
+      }
+      k_picard_count<<<B, 32, 0, stream>>>(st);
+    }
+    CDFT_CUDA(cudaGetLastError());
+    steps += chunk;
+  }
+  all_done();  // the state after the last chunk
+  std::vector<PicardResult> out(B);
+  for (int b = 0; b < B; ++b) {
+    const PicardDevState& x = h[b];
+    out[b].grand_potential = x.omega;
+    out[b].residual = x.residual;
+    out[b].iterations = x.iter;
+    // picard.hpp:121: the converged flag after the loop, with omega_prev as
+    // the loop left it (equal to omega when max_iterations ran out)
+    out[b].converged = x.converged || x.residual < cfg.tolerance ||
+                       (x.iter > 0 && std::fabs(x.omega - x.omega_prev) < cfg.tolerance);
+  }
+  return out;
 }
 
 }  // namespace cdft

@@ -107,6 +107,55 @@ class Drivers {
   };
   double ddft_step(DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations = nullptr);
 
+  // split_operator_step (dynamics.hpp:410-465): half diffusion in k-space,
+  // forward-Euler excess step, half diffusion; returns the energy after it.
+  double ddft_split_step(const DDFTConfig& cfg, double* rho, cudaStream_t stream);
+  // crank_nicholson_step (dynamics.hpp:472-538), fixed-point iterated.
+  double ddft_cn_step(const DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations = nullptr);
+
+  // Simulation::run (dynamics.hpp:583-693) on the device: n_steps IF steps
+  // with the adaptive dt; times / energies (n_steps + 1 host doubles each, or
+  // null) get every step; every snapshot_interval steps (and at step 0) the
+  // density is copied to the snapshot sink (host memory; the copy overlaps
+  // the next step when that memory is page-locked); `stop` (or null) ends
+  // the run after the step for which it returns nonzero.  Returns the steps
+  // taken.
+  struct SnapshotSink {
+    double* host = nullptr;  // capacity * N doubles
+    int* steps = nullptr;    // capacity step numbers
+    int capacity = 0;
+    int count = 0;           // written by ddft_run
+  };
+  using StopFn = int (*)(int step, double time, double energy, void* user);
+  // reservoir_boundary (dynamics.hpp:551-557): cells with mask[i] != 0
+  // (device, N bytes) reset to `density` on the initial state and after
+  // every step.
+  struct Reservoir {
+    const unsigned char* mask = nullptr;
+    double density = 0.0;
+  };
+  // Returns the steps taken (n_steps unless stop ended the run).
+  int ddft_run(DDFTConfig& cfg, int n_steps, double* rho, double* times, double* energies, int snapshot_interval,
+               SnapshotSink* snaps, StopFn stop, void* user, const Reservoir* reservoir, cudaStream_t stream);
+
+  // Picard::solve (picard.hpp:63-124) for every problem of the engine's
+  // batch: rho *= exp(-mixing force / dV), clamped at min_density, until the
+  // rms force or the change of Omega is below the tolerance; with `mass`
+  // (B values, or null) the fixed-mass constraint of
+  // minimization.hpp:159-180 (relative to `background`, B*N device doubles,
+  // or zero) after every update.
+  struct PicardConfig {
+    double mixing = 0.01, min_density = 1e-30, tolerance = 1e-6, constraint_min_density = 1e-30;
+    int max_iterations = 5000, check_interval = 25;
+  };
+  struct PicardResult {
+    double grand_potential = 0.0, residual = 0.0;
+    int iterations = 0;
+    bool converged = false;
+  };
+  std::vector<PicardResult> picard(const PicardConfig& cfg, const double* mu, const double* mass,
+                                   const double* background, double* rho, cudaStream_t stream);
+
   // H v at rho (single species): exact forward-over-reverse (hvp_exact) or the
   // reference's finite difference (F(rho + eps v) - F(rho)) / eps.
   // `boundary` 1: fixed boundary (forces zeroed on the faces, saddle_point.hpp:382).
@@ -186,6 +235,9 @@ class Drivers {
   void* ddft_k_ = nullptr;    // 3 * Nk complex (rho0_k, R0_k, R1_k / work)
   double* lam_ = nullptr;     // nx + ny + nzh Laplacian eigenvalues
   cufftHandle plan_r2c_ = 0, plan_c2r_ = 0;
+  cudaStream_t copy_stream_ = nullptr;          // snapshot D2H copies
+  double* snap_stage_[2] = {nullptr, nullptr};  // device staging of two snapshots in flight
+  cudaEvent_t snap_ready_[2] = {}, snap_done_[2] = {};
   void* fft_work_ = nullptr;
   bool ddft_ready_ = false;
   void ensure_ddft();

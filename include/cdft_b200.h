@@ -252,6 +252,65 @@ CDFT_API int cdft_ddft_step(cdft_engine* engine, cdft_ddft_config* cfg, double c
 CDFT_API int cdft_ddft_run(cdft_engine* engine, cdft_ddft_config* cfg, double chemical_potential, int n_steps,
                            double* rho, double* times, double* energies, void* stream);
 
+/* split_operator_step (dynamics.hpp:410-465): Strang splitting, half a
+ * diffusion step exp(-D k^2 dt / 2) in k-space, an explicit excess step,
+ * half a diffusion step; every stage clamped at min_density.  rho (device, N)
+ * is advanced in place; energy: Omega after the step.  cfg->dt is not
+ * changed. */
+CDFT_API int cdft_ddft_split_step(cdft_engine* engine, const cdft_ddft_config* cfg, double chemical_potential,
+                                  double* rho, double* energy, void* stream);
+
+/* crank_nicholson_step (dynamics.hpp:472-538): the fixed-point iteration
+ * of the Crank-Nicolson update with continuous k^2; fp_iterations: the
+ * iterations taken (or NULL). */
+CDFT_API int cdft_ddft_cn_step(cdft_engine* engine, const cdft_ddft_config* cfg, double chemical_potential,
+                               double* rho, double* energy, int* fp_iterations, void* stream);
+
+/* Return non-zero from the stop callback to end a simulation after `step`. */
+typedef int (*cdft_ddft_stop_fn)(int step, double time, double energy, void* user);
+
+/* Simulation::run (dynamics.hpp:583-693) with snapshots: as cdft_ddft_run,
+ * plus the density at step 0 and every snapshot_interval steps copied to
+ * snapshots (host, snapshot_capacity * N doubles; pinned memory lets the
+ * copies overlap the next steps) with their step numbers in snapshot_steps
+ * (host, snapshot_capacity ints, or NULL); snapshots beyond the capacity
+ * are dropped.  reservoir_mask (device, N bytes, or NULL): the cells that
+ * reservoir_boundary (dynamics.hpp:551-557) resets to reservoir_density on
+ * the initial state and after every step.  stop (or NULL) is called after
+ * every step with the step, the time and Omega.  steps_done /
+ * snapshot_count: the steps taken and the snapshots written. */
+CDFT_API int cdft_ddft_simulate(cdft_engine* engine, cdft_ddft_config* cfg, double chemical_potential, int n_steps,
+                                double* rho, double* times, double* energies, int snapshot_interval,
+                                double* snapshots, int* snapshot_steps, int snapshot_capacity, int* snapshot_count,
+                                const unsigned char* reservoir_mask, double reservoir_density,
+                                cdft_ddft_stop_fn stop, void* user, int* steps_done, void* stream);
+
+/* Picard parameters (picard.hpp:31-36; log_interval has no counterpart,
+ * check_interval is how many iterations run between host checks of the
+ * convergence flags; constraint_min_density is the min_density of
+ * fixed_mass_constraint, minimization.hpp:159-164). */
+typedef struct {
+  double mixing, min_density, tolerance, constraint_min_density;
+  int max_iterations, check_interval;
+} cdft_picard_config;
+
+typedef struct {
+  double grand_potential, residual;
+  int iterations, converged;
+} cdft_picard_result;
+
+/* Picard::solve (picard.hpp:63-124) for every problem of an engine (batch
+ * B >= 1): rho <- max(rho exp(-mixing force / dV), min_density) until the
+ * force RMS or the change of Omega falls below the tolerance.  mu: B host
+ * values; target_mass: B host values, or NULL for no constraint; with it,
+ * fixed_mass_constraint (minimization.hpp:159-180) rescales the excess over
+ * background (device, B * N, or NULL for zero) after every update.  rho:
+ * device, B * N.  results: B entries.  Converged problems stop changing
+ * while the others continue. */
+CDFT_API int cdft_picard(cdft_engine* engine, const cdft_picard_config* cfg, const double* mu,
+                         const double* target_mass, const double* background, double* rho,
+                         cdft_picard_result* results, void* stream);
+
 /* Hessian-vector product hv = d(force)/d(rho) . v of Omega at rho (device
  * vectors, N each); `boundary` 1 zeroes the faces (the fixed boundary of
  * saddle_point.hpp:377-384).  Exact forward-over-reverse differentiation;

@@ -1,6 +1,6 @@
 """FIRE2, density minimisation, DDFT and saddle-point search (oracle, test infrastructure only).
 
-Restates include/dft/algorithms/{fire,minimization,dynamics,saddle_point}.hpp.
+Restates include/dft/algorithms/{fire,minimization,dynamics,saddle_point,picard}.hpp.
 Vectors are flat FP64 NumPy arrays; multi-species state is a list of them.
 """
 from __future__ import annotations
@@ -569,3 +569,65 @@ class EigenvalueSolver:
             lam = float(np.dot(v, hv))
             it += 1
         return EigenvalueResult(v, lam, it, converged)
+
+
+# ================================================================= Picard
+
+
+def fixed_mass_constraint(target_masses, backgrounds, cell_volume, min_density=1e-30):
+    """minimization.hpp:159-180: rescale the excess over the background of
+    each species to its target mass (skipped when the mass is ~0)."""
+
+    def apply(densities):
+        out = [np.array(r, dtype=np.float64) for r in densities]
+        for s in range(min(len(out), len(target_masses))):
+            excess = out[s] - backgrounds[s]
+            mass = float(np.sum(excess)) * cell_volume
+            if abs(mass) > 1e-30:
+                out[s] = np.maximum(backgrounds[s] + (target_masses[s] / mass) * excess, min_density)
+        return out
+
+    return apply
+
+
+@dataclass
+class PicardResult:
+    """picard.hpp:23-29."""
+
+    densities: list
+    grand_potential: float
+    residual: float
+    iterations: int
+    converged: bool
+
+
+@dataclass
+class Picard:
+    """picard.hpp:31-124: log-space Picard iteration."""
+
+    mixing: float = 0.01
+    min_density: float = 1e-30
+    tolerance: float = 1e-6
+    max_iterations: int = 5000
+
+    def solve(self, densities, compute, cell_volume, constraint=None):
+        densities = [np.array(r, dtype=np.float64).reshape(-1) for r in densities]
+        residual = 0.0
+        omega = 0.0
+        omega_prev = float(np.finfo(np.float64).max)
+        it = 0
+        while it < self.max_iterations:
+            omega, forces = compute(densities)
+            sum_f2 = sum(float(np.dot(f, f)) for f in forces)
+            dof = float(sum(f.size for f in forces))
+            residual = math.sqrt(sum_f2 / dof)
+            if residual < self.tolerance or (it > 0 and abs(omega - omega_prev) < self.tolerance):
+                break
+            omega_prev = omega
+            densities = [np.maximum(r * np.exp(-self.mixing * f / cell_volume), self.min_density)
+                         for r, f in zip(densities, forces)]
+            if constraint is not None:
+                densities = constraint(densities)
+            it += 1
+        converged = residual < self.tolerance or (it > 0 and abs(omega - omega_prev) < self.tolerance)
+        return PicardResult(densities, omega, residual, it, converged)

@@ -143,3 +143,45 @@ def test_integrating_factor_ideal_gas_is_exact_diffusion():
     assert dt == 1e-3
     assert float(np.sum(d[0])) == pytest.approx(float(np.sum(rho0)), rel=1e-12)
     assert np.var(d[0]) < np.var(rho0)
+
+
+def test_picard_ideal_gas_converges_to_exp_mu():
+    """picard.hpp:63-124 on the ideal gas: force / dV = ln rho - mu, so
+    ln rho - mu shrinks by (1 - mixing) per iteration and the fixed point is
+    exp(mu)."""
+    mu = -1.2
+    dv = GRID8.cell_volume
+
+    def fn(dens):
+        e, f = ideal_forces(dens)
+        return e - mu * float(np.sum(dens[0])) * dv, [f[0] - mu * dv]
+
+    rho0 = gaussian_blob(0.2)
+    p = alg.Picard(mixing=0.2, tolerance=1e-9, max_iterations=2000)
+    r = p.solve([rho0], fn, dv)
+    # Omega stops changing (|dOmega| < tol, second order in the error) before
+    # the force RMS falls below the tolerance
+    assert r.converged and r.residual > 1e-9
+    assert np.max(np.abs(r.densities[0] - math.exp(mu))) < 1e-5
+    # the loop stops before updating: the residual belongs to the returned state
+    f = (np.log(r.densities[0]) - mu) * dv
+    assert math.sqrt(float(np.mean(f * f))) == pytest.approx(r.residual, rel=1e-9)
+    # one iteration by hand
+    r1 = alg.Picard(mixing=0.2, max_iterations=1).solve([rho0], fn, dv)
+    assert r1.iterations == 1
+    assert np.allclose(r1.densities[0], rho0 * np.exp(-0.2 * (np.log(rho0) - mu)), rtol=1e-14)
+    # max_iterations exhausted: omega_prev equals omega, so the reference reports converged
+    assert r1.converged
+
+
+def test_fixed_mass_constraint_rescales_the_excess():
+    """minimization.hpp:159-180."""
+    dv = GRID8.cell_volume
+    bg = np.full(512, 0.05)
+    rho = gaussian_blob(0.3)
+    target = 1.7
+    out = alg.fixed_mass_constraint([target], [bg], dv)([rho])
+    assert float(np.sum(out[0] - bg)) * dv == pytest.approx(target, rel=1e-13)
+    # a zero excess is left as it is
+    same = alg.fixed_mass_constraint([target], [bg], dv)([bg.copy()])
+    assert np.array_equal(same[0], bg)
