@@ -179,6 +179,12 @@ def lib():
                                ctypes.POINTER(ctypes.c_int), vp],
         "cdft_picard": [vp, ctypes.POINTER(CPicardConfig), c_double_p, c_double_p, vp, vp,
                         ctypes.POINTER(CPicardResult), vp],
+        "cdft_lattice_size": [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long)],
+        "cdft_build_lattice": [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_long), c_double_p, ctypes.c_long,
+                               c_double_p],
+        "cdft_lattice_export": [c_double_p, ctypes.c_long, ctypes.c_char_p, ctypes.c_int],
+        "cdft_gaussian_peaks": [ctypes.POINTER(ctypes.c_long), ctypes.c_double, c_double_p, ctypes.c_long,
+                                ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp],
         "cdft_hvp": [vp, vp, vp, ctypes.c_double, ctypes.c_int, vp, vp],
         "cdft_hvp_fd": [vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, vp, vp],
         "cdft_eigen_solve": [vp, ctypes.POINTER(CEigenConfig), vp, ctypes.c_double, vp, ctypes.c_int, c_double_p,

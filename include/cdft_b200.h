@@ -459,6 +459,48 @@ CDFT_API int cdft_engine_transforms(const cdft_engine* engine, int* transforms, 
  * counterpart: the reference is synchronous CPU code. */
 CDFT_API int cdft_engine_status(cdft_engine* engine, void* stream);
 
+/* ------------------------------------------------------------ lattices */
+
+/* Structure, Orientation and ExportFormat (types.hpp:52-71). */
+#define CDFT_BCC 0
+#define CDFT_FCC 1
+#define CDFT_HCP 2
+#define CDFT_ORIENT_001 0
+#define CDFT_ORIENT_010 1
+#define CDFT_ORIENT_100 2
+#define CDFT_ORIENT_110 3
+#define CDFT_ORIENT_101 4
+#define CDFT_ORIENT_011 5
+#define CDFT_ORIENT_111 6
+#define CDFT_EXPORT_XYZ 0
+#define CDFT_EXPORT_CSV 1
+
+/* The number of sites build_lattice makes: sites per unit cell x
+ * shape[0] x shape[1] x shape[2] (shape: 3 cell counts). */
+CDFT_API int cdft_lattice_size(int structure, int orientation, const long* shape, long* n_sites);
+
+/* build_lattice (crystal.cpp:205-245): site positions (host, row-major
+ * n_sites x 3, `capacity` >= n_sites) with unit nearest-neighbour distance,
+ * cells tiled x-fastest; dimensions (3 doubles, or NULL): the box edges.
+ * Invalid shapes and HCP along 110/101/011/111 are CDFT_ERR_INVALID, as the
+ * reference's std::invalid_argument. */
+CDFT_API int cdft_build_lattice(int structure, int orientation, const long* shape, double* positions, long capacity,
+                                double* dimensions);
+
+/* Lattice::export_to (crystal.cpp:257-279): XYZ ("Ar x y z" lines after the
+ * count and a comment line) or CSV (header "x,y,z"), default stream
+ * formatting.  A file that cannot be opened is CDFT_ERR_RUNTIME. */
+CDFT_API int cdft_lattice_export(const double* positions, long n_sites, const char* filename, int format);
+
+/* A crystal density profile on the grid (device, N doubles, z-fastest):
+ * rho = background + amplitude * sum_i exp(-alpha |r - R_i|^2) over the
+ * sites (host, n_sites x 3) at minimum-image distance, each peak cut where
+ * alpha |r - R_i|^2 > 40.  The box must be at least 2 sqrt(40 / alpha) on
+ * every axis.  No reference counterpart (a project-defined initialiser of
+ * solid profiles from build_lattice sites). */
+CDFT_API int cdft_gaussian_peaks(const long* shape, double dx, const double* sites, long n_sites, double alpha,
+                                 double amplitude, double background, double* rho, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
