@@ -42,6 +42,11 @@ class CInteraction(ctypes.Structure):
                 ("a_vdw", ctypes.c_double)]
 
 
+class CModelInteraction(ctypes.Structure):
+    _fields_ = [("species_i", ctypes.c_int), ("species_j", ctypes.c_int), ("potential", CPotential),
+                ("split", ctypes.c_int), ("scheme", ctypes.c_int)]
+
+
 class CFireParams(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_double), ("dt_max", ctypes.c_double), ("dt_min", ctypes.c_double),
                 ("alpha_start", ctypes.c_double), ("f_inc", ctypes.c_double), ("f_dec", ctypes.c_double),
@@ -139,6 +144,9 @@ def lib():
         "cdft_create_batch": [ctypes.POINTER(vp), c_long3, ctypes.c_double, ctypes.c_int, c_double_p, ctypes.c_int,
                               ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.POINTER(CInteraction),
                               ctypes.c_int, ctypes.c_int],
+        "cdft_create_model": [ctypes.POINTER(vp), c_long3, ctypes.c_double, ctypes.c_int, c_double_p, ctypes.c_int,
+                              ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.POINTER(CModelInteraction),
+                              ctypes.c_double, ctypes.c_int, ctypes.c_int],
         "cdft_engine_batch": [vp, ctypes.POINTER(ctypes.c_int)],
         "cdft_destroy": [vp],
         "cdft_engine_bulk_model": [vp, ctypes.POINTER(CBulkModel)],

@@ -115,28 +115,55 @@ int cdft_interaction_weight(const long shape[3], double dx, const cdft_potential
   });
 }
 
+}  // extern "C"
+
+namespace {
+
+// The grid / species / FMT part of an engine spec, validated.
+cdft::EngineSpec base_spec(const long shape[3], double dx, int n_species, const double* diameters, int fmt_model,
+                           double esfmt_A, double esfmt_B, int n_interactions, const void* interactions, int precision,
+                           int batch) {
+  if (!shape) throw std::invalid_argument("shape is NULL");
+  if (n_species < 1 || !diameters) throw std::invalid_argument("need at least one species diameter");
+  if (n_interactions < 0 || (n_interactions > 0 && !interactions)) throw std::invalid_argument("interactions is NULL");
+  if (batch < 1 || batch > CDFT_MAX_BATCH) throw std::invalid_argument("batch must be in [1, 64]");
+  if (shape[0] <= 0 || shape[1] <= 0 || shape[2] <= 0) throw std::invalid_argument("grid dimensions must be positive");
+  cdft::EngineSpec spec;
+  for (int d = 0; d < 3; ++d) spec.shape[d] = shape[d];
+  spec.dx = dx;
+  spec.diameters.assign(diameters, diameters + n_species);
+  spec.model = fmt_model;
+  spec.esfmt_A = esfmt_A;
+  spec.esfmt_B = esfmt_B;
+  spec.precision = precision;
+  spec.batch = batch;
+  return spec;
+}
+
+void make_engine(cdft_engine** out, const cdft::EngineSpec& spec) {
+  auto* e = new cdft_engine{nullptr, nullptr};
+  try {
+    e->impl = new cdft::Engine(spec);
+  } catch (...) {
+    delete e;
+    throw;
+  }
+  *out = e;
+}
+
+}  // namespace
+
+extern "C" {
+
 int cdft_create_batch(cdft_engine** out, const long shape[3], double dx, int n_species, const double* diameters,
                       int fmt_model, double esfmt_A, double esfmt_B, int n_interactions,
                       const cdft_interaction* interactions, int precision, int batch) {
   return guarded([&] {
     if (!out) throw std::invalid_argument("out is NULL");
     *out = nullptr;
-    if (!shape) throw std::invalid_argument("shape is NULL");
-    if (n_species < 1 || !diameters) throw std::invalid_argument("need at least one species diameter");
-    if (n_interactions < 0 || (n_interactions > 0 && !interactions))
-      throw std::invalid_argument("interactions is NULL");
-    cdft::EngineSpec spec;
-    for (int d = 0; d < 3; ++d) spec.shape[d] = shape[d];
-    spec.dx = dx;
-    spec.diameters.assign(diameters, diameters + n_species);
-    spec.model = fmt_model;
-    spec.esfmt_A = esfmt_A;
-    spec.esfmt_B = esfmt_B;
-    spec.precision = precision;
-    if (batch < 1 || batch > CDFT_MAX_BATCH) throw std::invalid_argument("batch must be in [1, 64]");
-    spec.batch = batch;
+    cdft::EngineSpec spec = base_spec(shape, dx, n_species, diameters, fmt_model, esfmt_A, esfmt_B, n_interactions,
+                                      interactions, precision, batch);
     const long long N = (long long)shape[0] * shape[1] * shape[2];
-    if (shape[0] <= 0 || shape[1] <= 0 || shape[2] <= 0) throw std::invalid_argument("grid dimensions must be positive");
     for (int m = 0; m < n_interactions; ++m) {
       cdft::InteractionSpec is;
       is.species_i = interactions[m].species_i;
@@ -146,14 +173,35 @@ int cdft_create_batch(cdft_engine** out, const long shape[3], double dx, int n_s
       is.a_vdw = interactions[m].a_vdw;
       spec.interactions.push_back(std::move(is));
     }
-    auto* e = new cdft_engine{nullptr, nullptr};
-    try {
-      e->impl = new cdft::Engine(spec);
-    } catch (...) {
-      delete e;
-      throw;
+    make_engine(out, spec);
+  });
+}
+
+int cdft_create_model(cdft_engine** out, const long shape[3], double dx, int n_species, const double* diameters,
+                      int fmt_model, double esfmt_A, double esfmt_B, int n_interactions,
+                      const cdft_model_interaction* interactions, double kT, int precision, int batch) {
+  return guarded([&] {
+    if (!out) throw std::invalid_argument("out is NULL");
+    *out = nullptr;
+    if (!(kT > 0.0)) throw std::invalid_argument("the temperature must be positive");
+    cdft::EngineSpec spec = base_spec(shape, dx, n_species, diameters, fmt_model, esfmt_A, esfmt_B, n_interactions,
+                                      interactions, precision, batch);
+    for (int m = 0; m < n_interactions; ++m) {
+      const cdft_model_interaction& mi = interactions[m];
+      check_split(mi.split);
+      if (mi.scheme < CDFT_WEIGHT_ZERO || mi.scheme > CDFT_WEIGHT_GAUSS_F)
+        throw std::invalid_argument("unknown weight scheme");
+      cdft::InteractionSpec is;
+      is.species_i = mi.species_i;
+      is.species_j = mi.species_j;
+      is.on_device = true;
+      is.potential = to_potential(&mi.potential);
+      is.split = mi.split;
+      is.scheme = mi.scheme;
+      is.kT = kT;
+      spec.interactions.push_back(std::move(is));
     }
-    *out = e;
+    make_engine(out, spec);
   });
 }
 

@@ -3,6 +3,7 @@
 #include "engine.cuh"
 #include "eval_kernels.cuh"
 #include "fused.cuh"
+#include "physics_fn.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -35,6 +36,53 @@ int occupancy_grid(K kernel, int block, int sms, long long work) {
 __global__ void k_real_part(const double2* __restrict__ in, double* __restrict__ out, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     out[i] = in[i].x;
+}
+
+// mean_field.hpp:146-196 up to its FFT, one thread per cell: the cell weight
+// at the cell's signed offset (zero beyond the cut-off plus half a cell
+// diagonal) times dV / N, and per block the sum of weight * dV.
+constexpr int kMfThreads = 256;
+
+__global__ void __launch_bounds__(kMfThreads) k_mf_weight(Potential pot, int split, int scheme, double kT, double dx,
+                                                          int nx, int ny, int nz, double* __restrict__ out,
+                                                          double* __restrict__ partials) {
+  const long long N = (long long)nx * ny * nz;
+  const double dv = dx * dx * dx;
+  const double inv_n = 1.0 / static_cast<double>(N);
+  double s = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    const long iz = (long)(i % nz);
+    const long long t = i / nz;
+    const long iy = (long)(t % ny);
+    const long ix = (long)(t / ny);
+    const long sx = phys::signed_offset(ix, nx), sy = phys::signed_offset(iy, ny), sz = phys::signed_offset(iz, nz);
+    if (phys::cell_skipped(pot, dx, sx, sy, sz)) {
+      out[i] = 0.0;
+      continue;
+    }
+    const double w = phys::cell_weight(pot, split, scheme, kT, dx, sx, sy, sz);
+    out[i] = w * dv * inv_n;
+    s += w * dv;
+  }
+  __shared__ double sh[kMfThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = 0.0;
+    for (int w = 0; w < kMfThreads / 32; ++w) b += sh[w];
+    partials[blockIdx.x] = b;
+  }
+}
+
+// a_vdw = the partials summed in a fixed order (deterministic).
+__global__ void k_sum_partials(const double* __restrict__ partials, int n, double* __restrict__ out) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += 32) s += partials[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) *out = s;
 }
 
 }  // namespace
@@ -110,8 +158,15 @@ Engine::Engine(const EngineSpec& spec) {
     const auto& it = spec.interactions[m];
     if (it.species_i < 0 || it.species_i >= S || it.species_j < 0 || it.species_j >= S)
       throw Error(-1, "Engine: interaction species index out of range");
-    if ((long long)it.weight_real.size() != p.N)
+    if (it.on_device) {
+      if (!(it.kT > 0.0)) throw Error(-1, "Engine: the temperature must be positive");
+      if (!(it.potential.sigma > 0.0)) throw Error(-1, "Engine: potential sigma must be positive");
+      if (it.scheme < kWeightZero || it.scheme > kWeightGaussF) throw Error(-1, "Engine: unknown weight scheme");
+      if (it.split != kWeeksChandlerAndersen && it.split != kBarkerHenderson)
+        throw Error(-1, "Engine: unknown split scheme");
+    } else if ((long long)it.weight_real.size() != p.N) {
       throw Error(-1, "Engine: interaction weight must have N = nx*ny*nz entries");
+    }
     p.mf_i[m] = it.species_i;
     p.mf_j[m] = it.species_j;
     p.mf_chan_j[m] = ch++;
@@ -319,28 +374,48 @@ void Engine::upload_mean_field(const EngineSpec& spec) {
   // FP64 plan; keep the real part (the weight is real and even).
   double* wr = nullptr;
   double2* wk = nullptr;
+  double* partials = nullptr;
+  int sms = 0, dev = 0;
+  CDFT_CUDA(cudaGetDevice(&dev));
+  CDFT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int mf_blocks = (int)std::max<long long>(
+      1, std::min<long long>((long long)sms * 8, ((long long)p.N + kMfThreads - 1) / kMfThreads));
   CDFT_CUDA(cudaMalloc(&wr, sizeof(double) * p.N));
   CDFT_CUDA(cudaMalloc(&wk, sizeof(double2) * p.Nk));
+  CDFT_CUDA(cudaMalloc(&partials, sizeof(double) * (mf_blocks + 1)));
   cufftHandle plan = 0;
   try {
     CDFT_CUFFT(cufftPlan3d(&plan, p.nx, p.ny, p.nz, CUFFT_D2Z));
     for (int m = 0; m < p.M; ++m) {
-      CDFT_CUDA(cudaMemcpy(wr, spec.interactions[m].weight_real.data(), sizeof(double) * p.N, cudaMemcpyHostToDevice));
+      const InteractionSpec& is = spec.interactions[m];
+      if (is.on_device) {
+        k_mf_weight<<<mf_blocks, kMfThreads>>>(is.potential, is.split, is.scheme, is.kT, p.dx, p.nx, p.ny, p.nz, wr,
+                                               partials);
+        k_sum_partials<<<1, 32>>>(partials, mf_blocks, partials + mf_blocks);
+        CDFT_CUDA(cudaGetLastError());
+        double a = 0.0;
+        CDFT_CUDA(cudaMemcpy(&a, partials + mf_blocks, sizeof(double), cudaMemcpyDeviceToHost));
+        a_vdw_.push_back(a);
+      } else {
+        CDFT_CUDA(cudaMemcpy(wr, is.weight_real.data(), sizeof(double) * p.N, cudaMemcpyHostToDevice));
+        a_vdw_.push_back(is.a_vdw);
+      }
       CDFT_CUFFT(cufftExecD2Z(plan, wr, wk));
       k_real_part<<<256, 256>>>(wk, mf_w_ + m * p.Nk, p.Nk);
       CDFT_CUDA(cudaGetLastError());
-      a_vdw_.push_back(spec.interactions[m].a_vdw);
     }
     CDFT_CUDA(cudaDeviceSynchronize());
   } catch (...) {
     if (plan) cufftDestroy(plan);
     cudaFree(wr);
     cudaFree(wk);
+    cudaFree(partials);
     throw;
   }
   cufftDestroy(plan);
   cudaFree(wr);
   cudaFree(wk);
+  cudaFree(partials);
 }
 
 // Stages 1-3: the weighted-density channels of the field `in` (S*N

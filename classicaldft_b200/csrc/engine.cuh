@@ -15,6 +15,7 @@
 #include "cdft_common.cuh"
 #include "fft_core.cuh"
 #include "fused.cuh"
+#include "physics.hpp"
 
 namespace cdft {
 
@@ -24,6 +25,12 @@ struct InteractionSpec {
   int species_i = 0, species_j = 0;
   std::vector<double> weight_real;  // N doubles: cell weight * dV / N (mean_field.hpp:188)
   double a_vdw = 0.0;
+  // on_device: weight_real and a_vdw are left empty and the engine builds
+  // them from the potential, split and weight scheme at temperature kT
+  bool on_device = false;
+  Potential potential;
+  int split = kWeeksChandlerAndersen, scheme = kWeightQuadraticF;
+  double kT = 1.0;
 };
 
 struct EngineSpec {

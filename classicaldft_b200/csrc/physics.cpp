@@ -5,6 +5,8 @@
 // the evaluation itself runs on the GPU.
 #include "physics.hpp"
 
+#include "physics_fn.cuh"
+
 #include <algorithm>
 #include <cmath>
 #include <stdexcept>
@@ -59,58 +61,12 @@ Potential make_potential(int type, double sigma, double epsilon, double r_cutoff
   return p;
 }
 
-// V(r) before shifting (potentials.hpp:71-75, 135-143, 199-206).
-double raw_potential(const Potential& p, double r) {
-  if (p.type == kLennardJones) {
-    double y = p.sigma / r;
-    double y6 = y * y * y * y * y * y;
-    return 4.0 * p.epsilon * (y6 * y6 - y6);
-  }
-  if (p.type == kTenWoldeFrenkel) {
-    if (r < p.sigma) return kMaxPotential;
-    double s = r / p.sigma;
-    double y = 1.0 / (s * s - 1.0);
-    double y3 = y * y * y;
-    return (4.0 * p.epsilon / (p.alpha * p.alpha)) * (y3 * y3 - p.alpha * y3);
-  }
-  // WRDF: epsilon_shift holds eps_eff
-  if (r >= p.r_cutoff) return 0.0;
-  double y = p.sigma / r;
-  double z = p.r_cutoff / r;
-  return p.epsilon_shift * (y * y - 1.0) * (z * z - 1.0) * (z * z - 1.0);
-}
-
-double split_point(const Potential& p, int split) {
-  if (p.type == kWRDF) return p.r_min;
-  return split == kBarkerHenderson ? p.r_zero : p.r_min;
-}
-
+// The potential pieces live in physics_fn.cuh, shared with the device.
+double raw_potential(const Potential& p, double r) { return phys::raw_potential(p, r); }
+double split_point(const Potential& p, int split) { return phys::split_point(p, split); }
 double hard_core(const Potential& p) { return p.type == kTenWoldeFrenkel ? p.sigma : 0.0; }
-
-// potentials.hpp:88-94, 157-163, 221-226
-double repulsive(const Potential& p, double r, int split) {
-  if (p.type == kWRDF) {
-    if (split == kBarkerHenderson) return (r < p.r_min) ? raw_potential(p, r) : 0.0;
-    return (r < p.r_min) ? raw_potential(p, r) - p.v_min : 0.0;
-  }
-  double v = raw_potential(p, r) - p.epsilon_shift;
-  if (split == kBarkerHenderson) return (r < p.r_zero) ? v : 0.0;
-  return (r < p.r_min) ? v - p.v_min : 0.0;
-}
-
-// potentials.hpp:97-107, 165-175, 228-236
-double attractive(const Potential& p, double r, int split) {
-  if (p.type == kWRDF) {
-    if (r >= p.r_cutoff) return 0.0;
-    if (split == kBarkerHenderson) return (r >= p.r_min) ? raw_potential(p, r) : 0.0;
-    return (r >= p.r_min) ? raw_potential(p, r) : p.v_min;
-  }
-  double rc = p.r_cutoff > 0.0 ? p.r_cutoff : 1e30;
-  if (r >= rc) return 0.0;
-  double v = raw_potential(p, r) - p.epsilon_shift;
-  if (split == kBarkerHenderson) return (r >= p.r_zero) ? v : 0.0;
-  return (r >= p.r_min) ? v : p.v_min;
-}
+double repulsive(const Potential& p, double r, int split) { return phys::repulsive(p, r, split); }
+double attractive(const Potential& p, double r, int split) { return phys::attractive(p, r, split); }
 
 // ------------------------------------------------------------ quadrature
 
@@ -216,37 +172,7 @@ double vdw_integral(const Potential& p, double kT, int split) {
 
 // mean_field.hpp:42-134
 double cell_weight(const Potential& p, int split, int scheme, double kT, double dx, long sx, long sy, long sz) {
-  if (scheme == kWeightZero) {
-    double r2 = static_cast<double>(sx * sx + sy * sy + sz * sz) * dx * dx;
-    return attractive(p, std::sqrt(r2), split) / kT;
-  }
-  if (scheme == kWeightQuadraticF) {
-    static constexpr double vv[] = {1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0};
-    static constexpr double pt[] = {-0.5, 0.0, 0.5};
-    double sum = 0.0;
-    for (int i = 0; i < 3; ++i)
-      for (int j = 0; j < 3; ++j)
-        for (int k = 0; k < 3; ++k) {
-          double rx = (static_cast<double>(sx) + pt[i]) * dx;
-          double ry = (static_cast<double>(sy) + pt[j]) * dx;
-          double rz = (static_cast<double>(sz) + pt[k]) * dx;
-          double r = std::sqrt(rx * rx + ry * ry + rz * rz);
-          sum += vv[i] * vv[j] * vv[k] * attractive(p, r, split) / kT;
-        }
-    return sum;
-  }
-  // linear (E/F) and the Gauss schemes share the 8-corner average
-  double sum = 0.0;
-  for (int di = 0; di <= 1; ++di)
-    for (int dj = 0; dj <= 1; ++dj)
-      for (int dk = 0; dk <= 1; ++dk) {
-        double x = (static_cast<double>(sx) - 0.5 + static_cast<double>(di)) * dx;
-        double y = (static_cast<double>(sy) - 0.5 + static_cast<double>(dj)) * dx;
-        double z = (static_cast<double>(sz) - 0.5 + static_cast<double>(dk)) * dx;
-        double r = std::sqrt(x * x + y * y + z * z);
-        sum += attractive(p, r, split) / kT;
-      }
-  return sum / 8.0;
+  return phys::cell_weight(p, split, scheme, kT, dx, sx, sy, sz);
 }
 
 // mean_field.hpp:146-196 (before the FFT, which the engine does on the GPU)
@@ -255,20 +181,15 @@ double interaction_weight(const long shape[3], double dx, const Potential& p, in
   const long nx = shape[0], ny = shape[1], nz = shape[2];
   const double dv = dx * dx * dx;
   const double inv_n = 1.0 / static_cast<double>(nx * ny * nz);
-  const double r_cutoff = p.r_cutoff;
-  const double margin = std::sqrt(3.0) * 0.5 * dx;
-  const double r_skip = r_cutoff + margin;
-  const double r_skip_sq = r_skip * r_skip;
   double weight_sum = 0.0;
   for (long ix = 0; ix < nx; ++ix) {
-    long sx = (ix <= nx / 2) ? ix : ix - nx;
+    const long sx = phys::signed_offset(ix, nx);
     for (long iy = 0; iy < ny; ++iy) {
-      long sy = (iy <= ny / 2) ? iy : iy - ny;
+      const long sy = phys::signed_offset(iy, ny);
       for (long iz = 0; iz < nz; ++iz) {
-        long sz = (iz <= nz / 2) ? iz : iz - nz;
+        const long sz = phys::signed_offset(iz, nz);
         const long idx = iz + nz * (iy + ny * ix);
-        double dist2 = static_cast<double>(sx * sx + sy * sy + sz * sz) * dx * dx;
-        if (r_cutoff > 0.0 && dist2 > r_skip_sq) {
+        if (phys::cell_skipped(p, dx, sx, sy, sz)) {
           out[idx] = 0.0;
           continue;
         }

@@ -213,26 +213,47 @@ class Engine:
 
     ``batch`` > 1 builds a batched engine: every call evaluates ``batch``
     problems of this model at once (arrays carry a leading batch axis).
+    ``weights_on``: "device" builds the mean-field cell weights on the GPU
+    (cdft_create_model); "host" runs the set-up loop of mean_field.hpp:146-196
+    on the CPU (cdft_interaction_weight) and uploads the result.
     """
 
-    def __init__(self, fmt_model: FMTModel, model: Model, precision: int = _lib.FP64, batch: int = 1):
+    def __init__(self, fmt_model: FMTModel, model: Model, precision: int = _lib.FP64, batch: int = 1,
+                 weights_on: str = "device"):
         L = _lib.lib()
         g = model.grid
         diam = np.array([sp.hard_sphere_diameter for sp in model.species], dtype=np.float64)
-        self._keep = []
-        inters = (_lib.CInteraction * max(1, len(model.interactions)))()
-        self.a_vdw = []
-        for m, it in enumerate(model.interactions):
-            w, a = interaction_weight(it, g, model.temperature)
-            self._keep.append(w)
-            inters[m] = _lib.CInteraction(it.species_i, it.species_j, w.ctypes.data_as(_lib.c_double_p), a)
-            self.a_vdw.append(a)
         h = ctypes.c_void_p()
-        _lib.check(L.cdft_create_batch(ctypes.byref(h), _lib.c_long3(*g.shape), g.dx, len(model.species),
-                                       diam.ctypes.data_as(_lib.c_double_p), _lib.MODEL_IDS[fmt_model.name],
-                                       fmt_model.A, fmt_model.B, len(model.interactions), inters, precision,
-                                       int(batch)))
-        self._keep = []
+        M = len(model.interactions)
+        if weights_on == "device":
+            inters = (_lib.CModelInteraction * max(1, M))()
+            for m, it in enumerate(model.interactions):
+                inters[m] = _lib.CModelInteraction(it.species_i, it.species_j, it.potential._c(), _SPLIT[it.split],
+                                                   _lib.WEIGHT_SCHEMES[it.weight_scheme])
+            _lib.check(L.cdft_create_model(ctypes.byref(h), _lib.c_long3(*g.shape), g.dx, len(model.species),
+                                           diam.ctypes.data_as(_lib.c_double_p), _lib.MODEL_IDS[fmt_model.name],
+                                           fmt_model.A, fmt_model.B, M, inters, model.temperature, precision,
+                                           int(batch)))
+            a = ctypes.c_double()
+            self.a_vdw = []
+            for m in range(M):
+                _lib.check(L.cdft_engine_a_vdw(h, m, ctypes.byref(a)))
+                self.a_vdw.append(a.value)
+        elif weights_on == "host":
+            keep = []
+            inters = (_lib.CInteraction * max(1, M))()
+            self.a_vdw = []
+            for m, it in enumerate(model.interactions):
+                w, a = interaction_weight(it, g, model.temperature)
+                keep.append(w)
+                inters[m] = _lib.CInteraction(it.species_i, it.species_j, w.ctypes.data_as(_lib.c_double_p), a)
+                self.a_vdw.append(a)
+            _lib.check(L.cdft_create_batch(ctypes.byref(h), _lib.c_long3(*g.shape), g.dx, len(model.species),
+                                           diam.ctypes.data_as(_lib.c_double_p), _lib.MODEL_IDS[fmt_model.name],
+                                           fmt_model.A, fmt_model.B, M, inters, precision, int(batch)))
+        else:
+            raise ValueError('weights_on: "device" or "host"')
+        self.weights_on = weights_on
         self.handle = h
         self.grid = g
         self.S = len(model.species)
@@ -340,9 +361,11 @@ class Weights:
         return list(self.engine.a_vdw)
 
 
-def make_weights(fmt_model: FMTModel, model: Model, precision: int = _lib.FP64, batch: int = 1) -> Weights:
-    """functionals.hpp:27-33 (``batch`` > 1: a batched engine, see ``total_batch``)."""
-    return Weights(fmt_model, Engine(fmt_model, model, precision, batch))
+def make_weights(fmt_model: FMTModel, model: Model, precision: int = _lib.FP64, batch: int = 1,
+                 weights_on: str = "device") -> Weights:
+    """functionals.hpp:27-33 (``batch`` > 1: a batched engine, see ``total_batch``;
+    ``weights_on``: where the mean-field cell weights are made, see ``Engine``)."""
+    return Weights(fmt_model, Engine(fmt_model, model, precision, batch, weights_on))
 
 
 @dataclass

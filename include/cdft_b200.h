@@ -99,6 +99,17 @@ typedef struct {
 /* Message of this thread's last failed call ("" if none). */
 CDFT_API const char* cdft_last_error(void);
 
+/* One mean-field interaction described by its potential (interactions.hpp:23-30
+ * before weight generation): cdft_create_model builds the real-space cell
+ * weights and a_vdw on the GPU from it. */
+typedef struct {
+  int species_i;
+  int species_j;
+  cdft_potential potential;
+  int split;  /* CDFT_SPLIT_* */
+  int scheme; /* CDFT_WEIGHT_* */
+} cdft_model_interaction;
+
 /* Library version string. */
 CDFT_API const char* cdft_version(void);
 
@@ -145,6 +156,18 @@ CDFT_API int cdft_create(cdft_engine** out, const long shape[3], double dx, int 
 CDFT_API int cdft_create_batch(cdft_engine** out, const long shape[3], double dx, int n_species,
                                const double* diameters, int fmt_model, double esfmt_A, double esfmt_B,
                                int n_interactions, const cdft_interaction* interactions, int precision, int batch);
+
+/* cdft_create_batch with the mean-field weights made on the GPU: for each
+ * interaction the cell weight of mean_field.hpp:42-134 (zero beyond the
+ * cut-off plus half a cell diagonal), times dV / N, at every grid offset
+ * (mean_field.hpp:146-196), then its FFT; a_vdw = sum of weight * dV
+ * (cdft_engine_a_vdw), summed in a fixed order.  The host set-up loop
+ * (cdft_interaction_weight) is not run.  kT > 0: the temperature the
+ * weights are divided by (model.hpp:20-26). */
+CDFT_API int cdft_create_model(cdft_engine** out, const long shape[3], double dx, int n_species,
+                               const double* diameters, int fmt_model, double esfmt_A, double esfmt_B,
+                               int n_interactions, const cdft_model_interaction* interactions, double kT,
+                               int precision, int batch);
 
 /* Number of problems an engine evaluates per call. */
 CDFT_API int cdft_engine_batch(const cdft_engine* engine, int* batch);
