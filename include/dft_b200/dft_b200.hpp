@@ -1,8 +1,9 @@
 // C++ host API of the classicalDFT B200 engine: the reference's functional,
-// grid, minimiser, DDFT and saddle-point interfaces (namespaces and names of
-// include/dft/{grid,types}.hpp, functionals/{functionals,functional}.hpp,
-// algorithms/{fire,minimization,dynamics,saddle_point}.hpp) over the C ABI of
-// cdft_b200.h.  Fields are std::vector<double> in the reference's layout
+// grid, minimiser, Picard, DDFT, saddle-point and lattice interfaces
+// (namespaces and names of include/dft/{grid,types}.hpp,
+// functionals/{functionals,functional}.hpp,
+// algorithms/{fire,minimization,picard,dynamics,saddle_point}.hpp,
+// src/crystal.cpp) over the C ABI of cdft_b200.h.  Fields are std::vector<double> in the reference's layout
 // (z fastest); device copies are made per call.  Errors are thrown as the
 // reference's exception types: std::invalid_argument / std::runtime_error.
 //
@@ -13,7 +14,9 @@
 
 #include <array>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
+#include <exception>
 #include <functional>
 #include <memory>
 #include <stdexcept>
@@ -184,21 +187,20 @@ class Weights {
     const auto& g = model.grid;
     std::vector<double> d;
     for (const auto& sp : model.species) d.push_back(sp.hard_sphere_diameter);
-    std::vector<std::vector<double>> w;
-    w.reserve(model.interactions.size());
-    std::vector<cdft_interaction> inter;
-    for (const auto& it : model.interactions) {  // mean_field.hpp:146-196 (set-up, host)
-      w.emplace_back(static_cast<std::size_t>(g.total_points()));
+    std::vector<cdft_model_interaction> inter;
+    for (const auto& it : model.interactions)  // mean_field.hpp:146-196, made on the GPU
+      inter.push_back({it.species_i, it.species_j, it.potential.p, static_cast<int>(it.split),
+                       static_cast<int>(it.weight_scheme)});
+    cdft_engine* e = nullptr;
+    check(cdft_create_model(&e, g.shape.data(), g.dx, static_cast<int>(d.size()), d.data(), fmt.id, fmt.A, fmt.B,
+                            static_cast<int>(inter.size()), inter.empty() ? nullptr : inter.data(),
+                            model.temperature, precision, 1));
+    engine_.reset(e);
+    for (int m = 0; m < static_cast<int>(inter.size()); ++m) {
       double a = 0.0;
-      check(cdft_interaction_weight(g.shape.data(), g.dx, &it.potential.p, static_cast<int>(it.split),
-                                    static_cast<int>(it.weight_scheme), model.temperature, w.back().data(), &a));
-      inter.push_back({it.species_i, it.species_j, w.back().data(), a});
+      check(cdft_engine_a_vdw(e, m, &a));
       a_vdw_.push_back(a);
     }
-    cdft_engine* e = nullptr;
-    check(cdft_create(&e, g.shape.data(), g.dx, static_cast<int>(d.size()), d.data(), fmt.id, fmt.A, fmt.B,
-                      static_cast<int>(inter.size()), inter.empty() ? nullptr : inter.data(), precision));
-    engine_.reset(e);
   }
   cdft_engine* engine() const { return engine_.get(); }
   const std::vector<double>& a_vdw() const { return a_vdw_; }
@@ -386,6 +388,68 @@ struct Minimizer {
 
 }  // namespace minimization
 
+namespace picard {
+
+// picard.hpp:23-29
+struct PicardResult {
+  std::vector<std::vector<double>> densities;
+  double grand_potential = 0.0, residual = 0.0;
+  int iterations = 0;
+  bool converged = false;
+};
+
+// minimization.hpp:159-180: the excess over the background rescaled to the
+// target mass after every update
+struct Constraint {
+  std::vector<double> target_masses;
+  std::vector<std::vector<double>> backgrounds;
+  double cell_volume = 0.0, min_density = 1e-30;
+};
+inline Constraint fixed_mass_constraint(std::vector<double> target_masses,
+                                        std::vector<std::vector<double>> backgrounds, double cell_volume,
+                                        double min_density = 1e-30) {
+  return Constraint{std::move(target_masses), std::move(backgrounds), cell_volume, min_density};
+}
+
+// picard.hpp:31-124 on the device (log_interval kept for the interface;
+// nothing is printed)
+struct Picard {
+  double mixing = 0.01, min_density = 1e-30, tolerance = 1e-6;
+  int max_iterations = 5000, log_interval = 500;
+  int check_interval = 25;
+
+  PicardResult solve(std::vector<std::vector<double>> densities, const functionals::Weights& w,
+                     double chemical_potential, const Constraint* constraint = nullptr) const {
+    const std::vector<double>& rho = densities.at(0);
+    DeviceVector d(rho);
+    cdft_picard_config cfg{mixing, min_density, tolerance, constraint ? constraint->min_density : 1e-30,
+                           max_iterations, check_interval};
+    cdft_picard_result res{};
+    std::unique_ptr<DeviceVector> bg;
+    double mass = 0.0;
+    if (constraint) {
+      if (constraint->target_masses.empty()) throw std::invalid_argument("fixed_mass_constraint: no target mass");
+      mass = constraint->target_masses[0];
+      if (!constraint->backgrounds.empty()) {
+        if (constraint->backgrounds[0].size() != rho.size())
+          throw std::invalid_argument("fixed_mass_constraint: background has the wrong size");
+        bg = std::make_unique<DeviceVector>(constraint->backgrounds[0]);
+      }
+    }
+    check(cdft_picard(w.engine(), &cfg, &chemical_potential, constraint ? &mass : nullptr, bg ? bg->get() : nullptr,
+                      d.get(), &res, nullptr));
+    PicardResult r;
+    r.densities.push_back(d.download());
+    r.grand_potential = res.grand_potential;
+    r.residual = res.residual;
+    r.iterations = res.iterations;
+    r.converged = res.converged != 0;
+    return r;
+  }
+};
+
+}  // namespace picard
+
 namespace dynamics {
 
 // dynamics.hpp:26-33
@@ -395,31 +459,169 @@ struct StepConfig {
   cdft_ddft_config c() const { return {dt, diffusion_coefficient, min_density, dt_max, fp_tolerance, fp_max_iterations}; }
 };
 
+// dynamics.hpp:36-40
+struct StepResult {
+  std::vector<std::vector<double>> densities;
+  double energy = 0.0;
+  double dt_used = 0.0;
+};
+
+namespace detail {
+template <class F>
+StepResult one_step(const std::vector<std::vector<double>>& densities, F&& call) {
+  DeviceVector d(densities.at(0));
+  StepResult r;
+  r.dt_used = call(d.get(), &r.energy);
+  r.densities.push_back(d.download());
+  return r;
+}
+}  // namespace detail
+
+// dynamics.hpp:333-401 (config.dt is divided by 10 on every restart)
+inline StepResult integrating_factor_step(const std::vector<std::vector<double>>& densities,
+                                          const functionals::Weights& w, StepConfig& config,
+                                          double chemical_potential = 0.0) {
+  return detail::one_step(densities, [&](double* d, double* e) {
+    cdft_ddft_config c = config.c();
+    check(cdft_ddft_step(w.engine(), &c, chemical_potential, d, e, nullptr, nullptr));
+    config.dt = c.dt;
+    return c.dt;
+  });
+}
+
+// dynamics.hpp:410-465
+inline StepResult split_operator_step(const std::vector<std::vector<double>>& densities,
+                                      const functionals::Weights& w, const StepConfig& config,
+                                      double chemical_potential = 0.0) {
+  return detail::one_step(densities, [&](double* d, double* e) {
+    const cdft_ddft_config c = config.c();
+    check(cdft_ddft_split_step(w.engine(), &c, chemical_potential, d, e, nullptr));
+    return c.dt;
+  });
+}
+
+// dynamics.hpp:472-538
+inline StepResult crank_nicholson_step(const std::vector<std::vector<double>>& densities,
+                                       const functionals::Weights& w, const StepConfig& config,
+                                       double chemical_potential = 0.0) {
+  return detail::one_step(densities, [&](double* d, double* e) {
+    const cdft_ddft_config c = config.c();
+    check(cdft_ddft_cn_step(w.engine(), &c, chemical_potential, d, e, nullptr, nullptr));
+    return c.dt;
+  });
+}
+
+// dynamics.hpp:45-50
+struct Snapshot {
+  int step = 0;
+  double time = 0.0, energy = 0.0;
+  std::vector<std::vector<double>> densities;
+};
+
+// dynamics.hpp:54-61
 struct SimulationResult {
   std::vector<std::vector<double>> densities;
   std::vector<double> times, energies;
+  std::vector<Snapshot> snapshots;
   double mass_initial = 0.0, mass_final = 0.0;
 };
 
-// dynamics.hpp:564-693 (integrating-factor DDFT on the device)
+// dynamics.hpp:551-557: the masked cells are reset to the reservoir density
+// after every step (an empty mask: periodic, canonical).
+struct BoundaryCondition {
+  std::vector<unsigned char> mask;
+  double reservoir_density = 0.0;
+  explicit operator bool() const { return !mask.empty(); }
+};
+inline BoundaryCondition reservoir_boundary(const std::vector<unsigned char>& mask, double reservoir_density) {
+  return BoundaryCondition{mask, reservoir_density};
+}
+
+using StopCondition = std::function<bool(int step, double time, double energy)>;
+
+// dynamics.hpp:564-693 (integrating-factor DDFT on the device; snapshots are
+// copied to pinned host memory while the following steps run).  times and
+// energies hold the entries the reference records (step 0, every
+// log_interval-th step and the last); nothing is printed.
 struct Simulation {
   StepConfig step;
   int n_steps = 1000;
+  int snapshot_interval = 100;
+  int log_interval = 50;
+  double energy_offset = 0.0;
+  BoundaryCondition boundary{};
+  StopCondition stop_condition{};
+
   SimulationResult run(std::vector<std::vector<double>> densities, const Grid& grid, const functionals::Weights& w,
                        double chemical_potential) const {
+    const std::size_t N = static_cast<std::size_t>(grid.total_points());
+    auto& rho0 = densities.at(0);
+    if (rho0.size() != N) throw std::invalid_argument("Simulation::run: density has the wrong size");
+    if (boundary) {
+      if (boundary.mask.size() != N) throw std::invalid_argument("reservoir mask: one entry per grid point");
+      for (std::size_t i = 0; i < N; ++i)
+        if (boundary.mask[i]) rho0[i] = boundary.reservoir_density;
+    }
     SimulationResult r;
-    DeviceVector d(densities.at(0));
-    cdft_ddft_config c = step.c();
-    r.times.assign(static_cast<std::size_t>(n_steps) + 1, 0.0);
-    r.energies.assign(static_cast<std::size_t>(n_steps) + 1, 0.0);
     double m0 = 0.0;
-    for (double v : densities[0]) m0 += v;
-    check(cdft_ddft_run(w.engine(), &c, chemical_potential, n_steps, d.get(), r.times.data(), r.energies.data(),
-                        nullptr));
+    for (double v : rho0) m0 += v;
+    r.mass_initial = m0 * grid.cell_volume();
+    DeviceVector d(rho0);
+    unsigned char* mask = nullptr;
+    if (boundary) {
+      cuda_check(cudaMalloc(&mask, N));
+      cuda_check(cudaMemcpy(mask, boundary.mask.data(), N, cudaMemcpyHostToDevice));
+    }
+    const int cap = snapshot_interval > 0 ? 1 + n_steps / snapshot_interval : 0;
+    double* snaps = nullptr;
+    std::vector<int> snap_steps(static_cast<std::size_t>(cap > 0 ? cap : 1));
+    if (cap > 0) {
+      const cudaError_t e = cudaMallocHost(&snaps, sizeof(double) * N * static_cast<std::size_t>(cap));
+      if (e != cudaSuccess) {
+        cudaFree(mask);
+        cuda_check(e);
+      }
+    }
+    std::vector<double> times(static_cast<std::size_t>(n_steps) + 1), energies(times.size());
+    struct Ctx {
+      const StopCondition* f;
+      std::exception_ptr err;
+    } ctx{&stop_condition, nullptr};
+    auto tramp = [](int s, double t, double e, void* user) -> int {
+      auto* c = static_cast<Ctx*>(user);
+      try {
+        return (*c->f)(s, t, e) ? 1 : 0;
+      } catch (...) {
+        c->err = std::current_exception();
+        return 1;
+      }
+    };
+    cdft_ddft_config c = step.c();
+    int count = 0, done = 0;
+    const int status = cdft_ddft_simulate(w.engine(), &c, chemical_potential, n_steps, d.get(), times.data(),
+                                          energies.data(), snapshot_interval, snaps, snap_steps.data(), cap, &count,
+                                          mask, boundary.reservoir_density, stop_condition ? +tramp : nullptr,
+                                          &ctx, &done, nullptr);
+    cudaFree(mask);
+    for (int k = 0; k < count; ++k) {
+      const int st = snap_steps[static_cast<std::size_t>(k)];
+      Snapshot sn{st, times[static_cast<std::size_t>(st)], energies[static_cast<std::size_t>(st)], {}};
+      sn.densities.emplace_back(snaps + static_cast<std::size_t>(k) * N, snaps + static_cast<std::size_t>(k + 1) * N);
+      r.snapshots.push_back(std::move(sn));
+    }
+    if (snaps) cudaFreeHost(snaps);
+    check(status);
+    if (ctx.err) std::rethrow_exception(ctx.err);
+    r.times.push_back(times[0]);
+    r.energies.push_back(energies[0]);
+    for (int s = 1; s <= done; ++s)
+      if (log_interval > 0 && (s % log_interval == 0 || s == n_steps)) {
+        r.times.push_back(times[static_cast<std::size_t>(s)]);
+        r.energies.push_back(energies[static_cast<std::size_t>(s)]);
+      }
     r.densities.push_back(d.download());
     double m1 = 0.0;
     for (double v : r.densities[0]) m1 += v;
-    r.mass_initial = m0 * grid.cell_volume();
     r.mass_final = m1 * grid.cell_volume();
     return r;
   }
@@ -497,4 +699,61 @@ struct Search {
 
 }  // namespace saddle_point
 }  // namespace algorithms
+
+// ---------------------------------------------------------------- crystal
+
+// types.hpp:52-71
+enum class Structure : std::uint8_t { BCC = CDFT_BCC, FCC = CDFT_FCC, HCP = CDFT_HCP };
+enum class Orientation : std::uint8_t {
+  _001 = CDFT_ORIENT_001,
+  _010 = CDFT_ORIENT_010,
+  _100 = CDFT_ORIENT_100,
+  _110 = CDFT_ORIENT_110,
+  _101 = CDFT_ORIENT_101,
+  _011 = CDFT_ORIENT_011,
+  _111 = CDFT_ORIENT_111
+};
+enum class ExportFormat : std::uint8_t { XYZ = CDFT_EXPORT_XYZ, CSV = CDFT_EXPORT_CSV };
+
+// types.hpp:73-83; positions are rows (x, y, z) with unit nearest-neighbour
+// distance
+static_assert(sizeof(std::array<double, 3>) == 3 * sizeof(double), "positions are passed as n x 3 doubles");
+struct Lattice {
+  Structure structure = Structure::FCC;
+  Orientation orientation = Orientation::_001;
+  std::vector<long> shape;
+  std::array<double, 3> dimensions{};
+  std::vector<std::array<double, 3>> positions;
+
+  // crystal.cpp:247-255
+  std::vector<std::array<double, 3>> scaled_positions(double dnn) const {
+    auto out = positions;
+    for (auto& p : out)
+      for (double& x : p) x *= dnn;
+    return out;
+  }
+  std::vector<std::array<double, 3>> scaled_positions(const std::array<double, 3>& box) const {
+    auto out = positions;
+    for (auto& p : out)
+      for (int d = 0; d < 3; ++d) p[d] *= box[d] / dimensions[d];
+    return out;
+  }
+  // crystal.cpp:257-279
+  void export_to(const std::string& filename, ExportFormat format = ExportFormat::XYZ) const {
+    check(cdft_lattice_export(positions.empty() ? nullptr : positions.data()->data(),
+                              static_cast<long>(positions.size()), filename.c_str(), static_cast<int>(format)));
+  }
+};
+
+// crystal.cpp:205-245
+inline Lattice build_lattice(Structure structure, Orientation orientation, const std::vector<long>& shape = {1, 1, 1}) {
+  if (shape.size() != 3) throw std::invalid_argument("Shape must have exactly 3 elements");
+  long n = 0;
+  check(cdft_lattice_size(static_cast<int>(structure), static_cast<int>(orientation), shape.data(), &n));
+  Lattice l{structure, orientation, shape, {}, std::vector<std::array<double, 3>>(static_cast<std::size_t>(n))};
+  check(cdft_build_lattice(static_cast<int>(structure), static_cast<int>(orientation), shape.data(),
+                           l.positions.data()->data(), n, l.dimensions.data()));
+  return l;
+}
+
 }  // namespace dft_b200

@@ -3,10 +3,15 @@
 // 16^3 grid (dx 0.25, kT 1, d 1, LJ sigma 1, epsilon 1, r_c 1.8), then
 //   1. functionals::total with an external field and Functional::evaluate,
 //   2. Minimizer::grand_potential (FIRE2 on the device),
-//   3. Simulation::run, three integrating-factor DDFT steps at fixed dt.
+//   3. Simulation::run, three integrating-factor DDFT steps at fixed dt,
+//   4. Picard::solve (30 iterations), split_operator_step and
+//      crank_nicholson_step, a Simulation with snapshots and a stop condition,
+//   5. build_lattice and Lattice::export_to.
 // Reads <dir>/rho.bin and <dir>/vext.bin (4096 doubles each); writes
-// <dir>/force.bin, <dir>/min_rho.bin, <dir>/ddft_rho.bin and prints the scalars
-// as key=value lines.  The test that runs it compares them with the oracle.
+// <dir>/force.bin, <dir>/min_rho.bin, <dir>/ddft_rho.bin, <dir>/picard_rho.bin,
+// <dir>/split_rho.bin, <dir>/cn_rho.bin, <dir>/snap2_rho.bin,
+// <dir>/lattice.xyz and prints the scalars as key=value lines.  The test that
+// runs it compares them with the oracle.
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -89,7 +94,39 @@ int main(int argc, char** argv) {
     std::printf("ddft_energy=%.17g\nddft_time=%.17g\nmass_initial=%.17g\nmass_final=%.17g\n", s.energies.back(),
                 s.times.back(), s.mass_initial, s.mass_final);
 
-    // 4. the reference's exception types
+    // 4. Picard, the split-operator and Crank-Nicolson steps, snapshots
+    d::algorithms::picard::Picard pc;
+    pc.mixing = 0.1;
+    pc.tolerance = 1e-14;
+    pc.max_iterations = 30;
+    const auto p = pc.solve({rho}, *func.weights, 1.5);
+    write_doubles(dir + "/picard_rho.bin", p.densities.at(0));
+    std::printf("picard_iterations=%d\npicard_omega=%.17g\n", p.iterations, p.grand_potential);
+    d::algorithms::dynamics::StepConfig sc;
+    sc.dt = 1e-3;
+    sc.fp_tolerance = 1e-11;
+    const auto so = d::algorithms::dynamics::split_operator_step({rho}, *func.weights, sc, 0.0);
+    write_doubles(dir + "/split_rho.bin", so.densities.at(0));
+    const auto cn = d::algorithms::dynamics::crank_nicholson_step({rho}, *func.weights, sc, 0.0);
+    write_doubles(dir + "/cn_rho.bin", cn.densities.at(0));
+    std::printf("split_energy=%.17g\ncn_energy=%.17g\n", so.energy, cn.energy);
+    d::algorithms::dynamics::Simulation sim2 = sim;
+    sim2.n_steps = 6;
+    sim2.snapshot_interval = 2;
+    sim2.log_interval = 0;
+    sim2.stop_condition = [](int step, double, double) { return step == 5; };
+    const auto s2 = sim2.run({rho}, model.grid, *func.weights, 0.0);
+    std::printf("snapshots=%d\nsnapshot_last_step=%d\nrecorded=%d\n", static_cast<int>(s2.snapshots.size()),
+                s2.snapshots.back().step, static_cast<int>(s2.times.size()));
+    write_doubles(dir + "/snap2_rho.bin", s2.snapshots.at(1).densities.at(0));
+
+    // 5. lattice
+    const auto lat = d::build_lattice(d::Structure::HCP, d::Orientation::_010, {2, 1, 2});
+    lat.export_to(dir + "/lattice.xyz", d::ExportFormat::XYZ);
+    std::printf("lattice_sites=%d\nlattice_dim_y=%.17g\n", static_cast<int>(lat.positions.size()),
+                lat.dimensions[1]);
+
+    // 6. the reference's exception types
     try {
       d::make_grid(0.3, {1.0, 1.0, 1.0});
       std::printf("grid_error=none\n");

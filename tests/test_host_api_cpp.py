@@ -3,7 +3,9 @@ tests/cpp is compiled with g++ against the header and libcdft_b200.so (CPU
 test), then run on the GPU and compared with the oracle: F and Omega to
 1e-12 relative and forces to 1e-11 of their max (the tolerances of the other
 FP64 parity tests), the converged FIRE2 density to 1e-8 in max-norm and three
-DDFT steps to 1e-10, as in the Python-API driver tests.
+DDFT steps to 1e-10, as in the Python-API driver tests; Picard after 30
+iterations to 1e-10, a split-operator step to 1e-11 and a Crank-Nicolson step
+to 1e-10; the lattice file equal to the oracle's text.
 """
 import os
 import subprocess
@@ -51,6 +53,7 @@ def test_cpp_host_api_matches_oracle(tmp_path):
     assert run.returncode == 0, run.stderr
     out = dict(line.split("=", 1) for line in run.stdout.split())
     val = {k: float(v) for k, v in out.items() if k not in ("grid_error", "size_error")}
+    from oracle import crystal as ocr
 
     # 1. total
     ref = pr.ref([rho], [0.7], [vext])
@@ -85,6 +88,35 @@ def test_cpp_host_api_matches_oracle(tmp_path):
     assert val["ddft_time"] == pytest.approx(s["times"][-1], rel=1e-15)
     assert val["mass_final"] == pytest.approx(val["mass_initial"], rel=1e-12)
 
-    # 4. exception mapping
+    # 4. Picard, split-operator and Crank-Nicolson steps, snapshots
+    def pfn(mu):
+        def f(dens):
+            r = pr.ref(dens, [mu])
+            return r.grand_potential, r.forces
+        return f
+    op = oalg.Picard(mixing=0.1, tolerance=1e-14, max_iterations=30).solve([rho], pfn(1.5), DX ** 3)
+    assert val["picard_iterations"] == op.iterations == 30
+    assert np.max(np.abs(np.fromfile(tmp_path / "picard_rho.bin") - op.densities[0])) <= 1e-10
+    assert rel_err(val["picard_omega"], op.grand_potential) <= 1e-11
+    grid = pr.omodel.grid
+    k2 = oalg.compute_k_squared(grid)
+    cfg = oalg.StepConfig(dt=1e-3, fp_tolerance=1e-11)
+    so, se, _ = oalg.split_operator_step([rho], grid, k2, oalg.diffusion_propagator(k2, 1.0, 1e-3), dfn, cfg)
+    assert np.max(np.abs(np.fromfile(tmp_path / "split_rho.bin") - so[0])) <= 1e-11
+    assert rel_err(val["split_energy"], se) <= 1e-11
+    co, ce, _ = oalg.crank_nicholson_step([rho], grid, k2, dfn, cfg)
+    assert np.max(np.abs(np.fromfile(tmp_path / "cn_rho.bin") - co[0])) <= 1e-10
+    assert rel_err(val["cn_energy"], ce) <= 1e-11
+    assert val["snapshots"] == 3 and val["snapshot_last_step"] == 4 and val["recorded"] == 1
+    s2 = oalg.Simulation(step=oalg.StepConfig(dt=2e-3, dt_max=2e-3, fp_tolerance=1e-10), n_steps=2).run(
+        [rho], grid, dfn)
+    assert np.max(np.abs(np.fromfile(tmp_path / "snap2_rho.bin") - s2["densities"][0])) <= 1e-10
+
+    # 5. lattice
+    pos, dims = ocr.build_lattice(ocr.HCP, ocr.O010, (2, 1, 2))
+    assert val["lattice_sites"] == len(pos) and val["lattice_dim_y"] == dims[1]
+    assert (tmp_path / "lattice.xyz").read_text() == ocr.export_text(pos, 0)
+
+    # 6. exception mapping
     assert out["grid_error"] == "invalid_argument"
     assert out["size_error"] == "invalid_argument"
