@@ -327,7 +327,7 @@ void Engine::setup_fused() {
   const fft::cpx* t = static_cast<const fft::cpx*>(tw_);
   tables_ = FftTables{t, t + p.nx, t + p.nx + p.ny, t + p.nx + p.ny + p.nz / 2};
   CDFT_CUDA(cudaMalloc(&wtab_, sizeof(float) * fused_weight_table_floats(p)));
-  fused_build_weights(p, wtab_, nullptr);
+  fused_build_weights(p, mf_w_, wtab_, nullptr);
   CDFT_CUDA(cudaDeviceSynchronize());
   fusable_ = true;
   fused_ = true;
@@ -503,7 +503,7 @@ void Engine::fused_forward(const double* rho, cudaStream_t stream) {
   fft::cpx* q = static_cast<fft::cpx*>(chan_k_);
   fused_plane_fwd_rho(plan_, p, rho, mean_, prho, tables_, stream);
   mark(2, stream);
-  fused_col_fwd(plan_, p, prho, mf_w_, wtab_, q, tables_, stream);
+  fused_col_fwd(plan_, p, prho, wtab_, q, tables_, stream);
   mark(3, stream);
   fused_plane_inv(plan_, p, q, static_cast<float*>(chan_r_), tables_, stream);
   mark(4, stream);

@@ -1,0 +1,901 @@
+// Kernels of the fused transform path on register-resident transforms
+// (fft_reg.cuh).  A length-N transform is two in-register DFTs (A and B
+// points) with one shared-memory exchange between them; a plane pass is a
+// y transform and a z transform (four exchanges at most, with the
+// half-complex steps on the y-spectrum), a column pass one x transform per
+// array.  The passes and their arrays are those of the stage-by-stage
+// kernels they replace:
+//
+//   k_rplane_fwd<double>  R2C z, FFT y of rho - mean          -> P_rho
+//   k_rcol_fwd            FFT x, channels W_c(k) rho_k, IFFT x -> Q_c
+//   k_rplane_inv          IFFT y, C2R z                        -> channels (real)
+//   (pointwise)
+//   k_rplane_fwd<float>   R2C z, FFT y of every derivative     -> P_d
+//   k_rcol_bwd            FFT x, F_s = sum_c conj(W_cs) D_c, IFFT x -> P_f
+//   k_rplane_inv<EPI>     IFFT y, C2R z, force += hs dV + const, scalars
+//
+// Every task loop maps consecutive threads to consecutive z (plane) or
+// in-plane column (column pass) indices, so global accesses are contiguous
+// and shared-memory accesses fall in distinct banks; values a task needs
+// after a barrier that also frees the buffer are held in registers.
+#pragma once
+
+#include <type_traits>
+
+#include "eval_kernels.cuh"
+#include "fft_reg.cuh"
+
+namespace cdft {
+namespace rk {
+
+using fft::cpx;
+
+template <int I, int N, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (I < N) {
+    f(std::integral_constant<int, I>{});
+    static_for<I + 1, N>(f);
+  }
+}
+
+// Smallest v >= x with v = 8 (mod 16): a row stride that puts rows y and
+// y + 1 of a half-warp's 64-bit accesses in different bank halves.
+__host__ __device__ constexpr int pad8(int x) { return x + ((8 - x % 16) + 16) % 16; }
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+// ------------------------------------------------------------ plane pass
+
+template <int NY, int NZ>
+struct RPlane {
+  static constexpr int M = NZ / 2, LD = M + 1;
+  using SY = fft::Split<NY>;
+  using SZ = fft::Split<M>;
+  static constexpr int AY = SY::A, BY = SY::B, AZ = SZ::A, BZ = SZ::B;
+  static constexpr int EY = M;               // y exchange: [n2][k1][kz]
+  static constexpr int ER = pad8(M);         // rows: [y][kz]
+  static constexpr int EZS = AZ + 1;         // z exchange: [y][n2][k1], n2 stride
+  static constexpr int EZ = pad8(BZ * EZS);  // z exchange row stride
+  static constexpr int BUF = cmax(NY * EY, cmax(NY * ER, NY * EZ));
+  static constexpr int NT = NY * M >= 8192 ? 512 : (NY * M >= 2048 ? 256 : 128);
+  static constexpr size_t kSmem = sizeof(cpx) * ((size_t)BUF + NY + M + NZ);
+  // tasks of each phase and the tasks a thread holds across a barrier
+  static constexpr int T_Y_SPEC = M * AY, T_Y_NAT = M * BY, T_Z_SPEC = NY * AZ, T_Z_NAT = NY * BZ;
+};
+
+template <int NY, int NZ, int NT>
+__device__ __forceinline__ void plane_tables(cpx* ty, cpx* tz, cpx* t2, const FftTables& T) {
+  for (int i = threadIdx.x; i < NY; i += NT) ty[i] = T.ty[i];
+  for (int i = threadIdx.x; i < NZ / 2; i += NT) tz[i] = T.tz[i];
+  for (int i = threadIdx.x; i < NZ; i += NT) t2[i] = T.t2[i];
+}
+
+// Forward plane pass of one real NY x NZ plane (IN = double: rho minus the
+// species mean, the mixed-precision split; IN = float: a derivative
+// channel) into its half spectrum (NY x (NZ/2 + 1), natural order).
+template <int NY, int NZ, typename IN>
+__global__ void __launch_bounds__(RPlane<NY, NZ>::NT)
+    k_rplane_fwd(EvalParams p, const IN* __restrict__ in, int nseq, const double* __restrict__ mean,
+                 cpx* __restrict__ out, FftTables T) {
+  using P = RPlane<NY, NZ>;
+  constexpr int M = P::M, LD = P::LD, AY = P::AY, BY = P::BY, AZ = P::AZ, BZ = P::BZ, NT = P::NT;
+  constexpr int EY = P::EY, ER = P::ER, EZS = P::EZS, EZ = P::EZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cpx* E = reinterpret_cast<cpx*>(smem_raw);
+  cpx* ty = E + P::BUF;
+  cpx* tz = ty + NY;
+  cpx* t2 = tz + M;
+  const int ix = blockIdx.x, sq = blockIdx.y, b = blockIdx.z;
+  plane_tables<NY, NZ, NT>(ty, tz, t2, T);
+  __syncthreads();
+  const IN* src = in + ((long long)b * nseq + sq) * p.N + (long long)ix * NY * NZ;
+  const double c = mean ? mean[b * kMaxSpecies + sq] : 0.0;
+  // z, first half: task (y, n2) takes the pairs n = BZ n1 + n2 of row y
+  for (int t = threadIdx.x; t < P::T_Z_NAT; t += NT) {
+    const int n2 = t % BZ, y = t / BZ;
+    cpx a[AZ];
+#pragma unroll
+    for (int n1 = 0; n1 < AZ; ++n1) {
+      const IN* q = src + (long long)y * NZ + 2 * (BZ * n1 + n2);  // the caller's buffer: scalar loads
+      if constexpr (sizeof(IN) == 8)
+        a[n1] = {(float)(q[0] - c), (float)(q[1] - c)};
+      else
+        a[n1] = {q[0], q[1]};
+    }
+    fft::nat_in<M, false>(a, n2, tz);
+#pragma unroll
+    for (int k1 = 0; k1 < AZ; ++k1) E[y * EZ + n2 * EZS + k1] = a[k1];
+  }
+  __syncthreads();
+  // z, second half: task (y, k1) -> Z_y[kz = k1 + AZ k2]
+  constexpr int H1 = cdiv(P::T_Z_SPEC, NT);
+  cpx h1[H1][BZ];
+#pragma unroll
+  for (int j = 0; j < H1; ++j) {
+    const int t = threadIdx.x + j * NT;
+    if (t < P::T_Z_SPEC) {
+      const int k1 = t % AZ, y = t / AZ;
+#pragma unroll
+      for (int n2 = 0; n2 < BZ; ++n2) h1[j][n2] = E[y * EZ + n2 * EZS + k1];
+      fft::nat_out<M, false>(h1[j]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < H1; ++j) {
+    const int t = threadIdx.x + j * NT;
+    if (t < P::T_Z_SPEC) {
+      const int k1 = t % AZ, y = t / AZ;
+#pragma unroll
+      for (int k2 = 0; k2 < BZ; ++k2) E[y * ER + k1 + AZ * k2] = h1[j][k2];
+    }
+  }
+  __syncthreads();
+  // y, first half: task (kz, n2) takes rows y = BY n1 + n2 of column kz
+  constexpr int H2 = cdiv(P::T_Y_NAT, NT);
+  cpx h2[H2][AY];
+#pragma unroll
+  for (int j = 0; j < H2; ++j) {
+    const int t = threadIdx.x + j * NT;
+    if (t < P::T_Y_NAT) {
+      const int kz = t % M, n2 = t / M;
+#pragma unroll
+      for (int n1 = 0; n1 < AY; ++n1) h2[j][n1] = E[(BY * n1 + n2) * ER + kz];
+      fft::nat_in<NY, false>(h2[j], n2, ty);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < H2; ++j) {
+    const int t = threadIdx.x + j * NT;
+    if (t < P::T_Y_NAT) {
+      const int kz = t % M, n2 = t / M;
+#pragma unroll
+      for (int k1 = 0; k1 < AY; ++k1) E[(n2 * AY + k1) * EY + kz] = h2[j][k1];
+    }
+  }
+  __syncthreads();
+  // y, second half: task (kz, k1) -> Z[ky = k1 + AY k2][kz]
+  constexpr int H3 = cdiv(P::T_Y_SPEC, NT);
+  cpx h3[H3][BY];
+#pragma unroll
+  for (int j = 0; j < H3; ++j) {
+    const int t = threadIdx.x + j * NT;
+    if (t < P::T_Y_SPEC) {
+      const int kz = t % M, k1 = t / M;
+#pragma unroll
+      for (int n2 = 0; n2 < BY; ++n2) h3[j][n2] = E[(n2 * AY + k1) * EY + kz];
+      fft::nat_out<NY, false>(h3[j]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < H3; ++j) {
+    const int t = threadIdx.x + j * NT;
+    if (t < P::T_Y_SPEC) {
+      const int kz = t % M, k1 = t / M;
+#pragma unroll
+      for (int k2 = 0; k2 < BY; ++k2) E[(k1 + AY * k2) * ER + kz] = h3[j][k2];
+    }
+  }
+  __syncthreads();
+  // half-complex post-processing on the y-spectrum, stored in natural order
+  cpx* dst = out + ((long long)b * nseq + sq) * p.Nk + (long long)ix * NY * LD;
+  for (int t = threadIdx.x; t < NY * M; t += NT) {
+    const int kz = t % M, ky = t / M, km = (NY - ky) & (NY - 1);
+    if (kz == 0) {
+      cpx x0, xM;
+      fft::r2c_post_2d_dc(E[ky * ER], E[km * ER], x0, xM);
+      dst[ky * LD] = x0;
+      dst[ky * LD + M] = xM;
+    } else {
+      dst[ky * LD + kz] = fft::r2c_post_2d(E[ky * ER + kz], E[km * ER + (M - kz)], t2[kz]);
+    }
+  }
+}
+
+// Inverse plane pass of one half spectrum (NY x (NZ/2 + 1), natural order):
+// the C2R of its Hermitian projection, unnormalised.  EPI = false: written
+// as a real FP32 channel.  EPI = true: the back-convolved force of species
+// blockIdx.y, added to the FP64 force with the epilogue constant
+// (force_s += hs dV - mu_s dV + the DC split term); the CTA of plane 0,
+// species 0 of each problem also reduces the pointwise partials into the
+// scalars (the pointwise kernel completed before this launch).
+template <int NY, int NZ, bool EPI, bool MULTI, bool TENSOR>
+__global__ void __launch_bounds__(RPlane<NY, NZ>::NT)
+    k_rplane_inv(EvalParams p, const cpx* __restrict__ in, int nseq, float* __restrict__ out_f,
+                 double* __restrict__ force, const double* __restrict__ dbar, const __grid_constant__ MuArgs mu,
+                 FinalArgs fin, FftTables T) {
+  using P = RPlane<NY, NZ>;
+  using L = Lay<MULTI, TENSOR>;
+  constexpr int M = P::M, LD = P::LD, AY = P::AY, BY = P::BY, AZ = P::AZ, BZ = P::BZ, NT = P::NT;
+  constexpr int EY = P::EY, ER = P::ER, EZS = P::EZS, EZ = P::EZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cpx* E = reinterpret_cast<cpx*>(smem_raw);
+  cpx* ty = E + P::BUF;
+  cpx* tz = ty + NY;
+  cpx* t2 = tz + M;
+  const int ix = blockIdx.x, sq = blockIdx.y, b = blockIdx.z;
+  __shared__ double s_const;
+  if constexpr (EPI) {
+    if (ix == 0 && sq == 0 && fin.scalars)
+      reduce_final(fin.partials + (long long)b * fin.nblocks * p.n_terms, fin.nblocks, p, mu.mu[b], fin.err,
+                   fin.scalars + b * kScalarCount);
+    // the force plane is read at the end: start pulling it into L2 now
+    const char* fp = reinterpret_cast<const char*>(force + ((long long)b * p.S + sq) * p.N + (long long)ix * NY * NZ);
+    for (int off = threadIdx.x * 128; off < NY * NZ * 8; off += NT * 128)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(fp + off));
+    if (threadIdx.x == 0) {
+      double v = 0.0;
+      const double* db = dbar + b * kMaxChannels;
+#pragma unroll
+      for (int c = 0; c < L::NFMT; ++c) v += chan_dc<MULTI, TENSOR>(c, sq, p) * db[c];
+      s_const = v * p.dv - mu.mu[b][sq] * p.dv;
+    }
+  }
+  plane_tables<NY, NZ, NT>(ty, tz, t2, T);
+  __syncthreads();
+  const cpx* src = in + ((long long)b * nseq + sq) * p.Nk + (long long)ix * NY * LD;
+  // y, first half: task (kz, k1) pre-processes X[ky = k1 + AY k2][kz] with
+  // its mirror and starts the inverse y transform
+  for (int t = threadIdx.x; t < P::T_Y_SPEC; t += NT) {
+    const int kz = t % M, k1 = t / M;
+    cpx bv[BY];
+#pragma unroll
+    for (int k2 = 0; k2 < BY; ++k2) {
+      const int ky = k1 + AY * k2, km = (NY - ky) & (NY - 1);
+      if (kz == 0)
+        bv[k2] = fft::c2r_pre_2d_dc(src[ky * LD], src[km * LD], src[ky * LD + M], src[km * LD + M]);
+      else
+        bv[k2] = fft::c2r_pre_2d(src[ky * LD + kz], src[km * LD + (M - kz)], t2[kz]);
+    }
+    fft::spec_in<NY, true>(bv, k1, ty);
+#pragma unroll
+    for (int n2 = 0; n2 < BY; ++n2) E[(n2 * AY + k1) * EY + kz] = bv[n2];
+  }
+  __syncthreads();
+  // y, second half: task (kz, n2) -> rows y = BY n1 + n2
+  constexpr int H1 = cdiv(P::T_Y_NAT, NT);
+  cpx h1[H1][AY];
+#pragma unroll
+  for (int j = 0; j < H1; ++j) {
+    const int t = threadIdx.x + j * NT;
+    if (t < P::T_Y_NAT) {
+      const int kz = t % M, n2 = t / M;
+#pragma unroll
+      for (int k1 = 0; k1 < AY; ++k1) h1[j][k1] = E[(n2 * AY + k1) * EY + kz];
+      fft::spec_out<NY, true>(h1[j]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < H1; ++j) {
+    const int t = threadIdx.x + j * NT;
+    if (t < P::T_Y_NAT) {
+      const int kz = t % M, n2 = t / M;
+#pragma unroll
+      for (int n1 = 0; n1 < AY; ++n1) E[(BY * n1 + n2) * ER + kz] = h1[j][n1];
+    }
+  }
+  __syncthreads();
+  // z, first half: task (y, k1) takes Z_y[kz = k1 + AZ k2]
+  constexpr int H2 = cdiv(P::T_Z_SPEC, NT);
+  cpx h2[H2][BZ];
+#pragma unroll
+  for (int j = 0; j < H2; ++j) {
+    const int t = threadIdx.x + j * NT;
+    if (t < P::T_Z_SPEC) {
+      const int k1 = t % AZ, y = t / AZ;
+#pragma unroll
+      for (int k2 = 0; k2 < BZ; ++k2) h2[j][k2] = E[y * ER + k1 + AZ * k2];
+      fft::spec_in<M, true>(h2[j], k1, tz);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < H2; ++j) {
+    const int t = threadIdx.x + j * NT;
+    if (t < P::T_Z_SPEC) {
+      const int k1 = t % AZ, y = t / AZ;
+#pragma unroll
+      for (int n2 = 0; n2 < BZ; ++n2) E[y * EZ + n2 * EZS + k1] = h2[j][n2];
+    }
+  }
+  __syncthreads();
+  // z, second half: task (y, n2) -> pairs n = BZ n1 + n2 of row y
+  const long long plane_off = ((long long)b * (EPI ? p.S : nseq) + sq) * p.N + (long long)ix * NY * NZ;
+  double cst = 0.0;
+  if constexpr (EPI) cst = s_const;
+  for (int t = threadIdx.x; t < P::T_Z_NAT; t += NT) {
+    const int n2 = t % BZ, y = t / BZ;
+    cpx a[AZ];
+#pragma unroll
+    for (int k1 = 0; k1 < AZ; ++k1) a[k1] = E[y * EZ + n2 * EZS + k1];
+    fft::spec_out<M, true>(a);
+#pragma unroll
+    for (int n1 = 0; n1 < AZ; ++n1) {
+      const int n = BZ * n1 + n2;
+      if constexpr (EPI) {
+        double* f = force + plane_off + (long long)y * NZ + 2 * n;  // the caller's buffer: 8-byte alignment
+        f[0] = f[0] + (double)(2.0f * a[n1].x) * p.dv + cst;
+        f[1] = f[1] + (double)(2.0f * a[n1].y) * p.dv + cst;
+      } else {
+        *reinterpret_cast<float2*>(out_f + plane_off + (long long)y * NZ + 2 * n) =
+            make_float2(2.0f * a[n1].x, 2.0f * a[n1].y);
+      }
+    }
+  }
+}
+
+// ----------------------------------------------------------- column pass
+
+// Fused-path weight table, built once per engine: per species the |k|
+// factors pre-scaled by 1/N, FP64-computed and rounded to FP32 -- w3, w2,
+// fv, A/k^2, B -- then the mean-field weights (real) in FP32.  Layout
+// [S][5][Nk] floats, then [M][Nk].
+__host__ __device__ inline long long rweight_table_floats(const EvalParams& p) { return (5LL * p.S + p.M) * p.Nk; }
+
+static __global__ void __launch_bounds__(256)
+    k_build_rweights(EvalParams p, const double* __restrict__ mf_w, float* __restrict__ tab) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < p.Nk;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const KIndex q = decode_k(p, idx);
+    double kk[3], km[3], k, inv_k2;
+    k_setup(p, q, kk, km, k, inv_k2);
+    for (int s = 0; s < p.S; ++s) {
+      const KW w = weight_kernels(k, p.R[s]);
+      float* t = tab + 5LL * s * p.Nk + idx;
+      t[0] = (float)(w.w3 * p.inv_n);
+      t[p.Nk] = (float)(w.w2 * p.inv_n);
+      t[2 * p.Nk] = (float)(w.fv * p.inv_n);
+      t[3 * p.Nk] = (float)(w.A * inv_k2 * p.inv_n);
+      t[4 * p.Nk] = (float)(w.B * p.inv_n);
+    }
+    for (int m = 0; m < p.M; ++m) tab[(5LL * p.S + m) * p.Nk + idx] = (float)mf_w[m * p.Nk + idx];
+  }
+}
+
+// The symmetrised k-space factors of one element.  On the self-conjugate
+// planes (kz = 0 and kz = nz/2: `proj` columns) the channel weights become
+// W'(k) = (W(k) + conj W(k_m)) / 2 with the mirror k_m = (-kx, -ky, kz),
+// except that a Nyquist x or y index is its own mirror.  With s_a = -1 for
+// a mirrored component and +1 for an unmirrored one (z always, Nyquist x or
+// y), an odd channel k_a keeps its weight iff s_a = -1 and a tensor cross
+// term k_a k_b iff s_a = s_b; every other weight is unchanged.
+struct RKv {
+  float k[3];   // the wavevector
+  float o[3];   // odd-channel masks
+  float cxy, cxz, cyz;  // tensor cross-term masks
+};
+
+__device__ __forceinline__ RKv rk_element(float kx, bool xnyq, float ky, bool ynyq, float kz, bool proj) {
+  RKv v;
+  v.k[0] = kx;
+  v.k[1] = ky;
+  v.k[2] = kz;
+  v.o[0] = (!proj || !xnyq) ? 1.0f : 0.0f;
+  v.o[1] = (!proj || !ynyq) ? 1.0f : 0.0f;
+  v.o[2] = proj ? 0.0f : 1.0f;
+  v.cxy = (!proj || xnyq == ynyq) ? 1.0f : 0.0f;
+  v.cxz = (!proj || xnyq) ? 1.0f : 0.0f;
+  v.cyz = (!proj || ynyq) ? 1.0f : 0.0f;
+  return v;
+}
+
+__device__ __forceinline__ float rk_cross(const RKv& v, int i, int j) {
+  if (i == j) return 1.0f;
+  if (i + j == 1) return v.cxy;
+  if (i + j == 2) return v.cxz;
+  return v.cyz;
+}
+
+// Weight of FMT channel c for species s (c uniform across the block): the
+// channel is w rho_s, or i w rho_s when `odd`.  weights.hpp:163-179 with the
+// Rosenfeld scalings of hard_sphere.hpp:80-85, as chan_weight.
+template <bool MULTI, bool TENSOR>
+__device__ __forceinline__ float rk_weight(int c, const float* __restrict__ ts, long long Nk, const RKv& v,
+                                           float i4r, float i4r2, bool& odd) {
+  using L = Lay<MULTI, TENSOR>;
+  odd = false;
+  if (c == L::ETA) return ts[0];
+  if (c == L::N2) return ts[Nk];
+  if (MULTI && c == L::N1) return ts[Nk] * i4r;
+  if (MULTI && c == L::N0) return ts[Nk] * i4r2;
+  if (c >= L::V1 && c < L::V1 + 3) {
+    odd = true;
+    const int a = c - L::V1;
+    return ts[2 * Nk] * (v.k[a] * v.o[a]);
+  }
+  if (MULTI && c >= L::V0 && c < L::V0 + 3) {
+    odd = true;
+    const int a = c - L::V0;
+    return (ts[2 * Nk] * (v.k[a] * v.o[a])) * i4r;
+  }
+  const int t = c - L::T;
+  const int i = tchan_i(t), j = tchan_j(t);
+  const float kij = v.k[i] * v.k[j] * rk_cross(v, i, j);
+  return (i == j) ? ts[3 * Nk] * kij + ts[4 * Nk] : ts[3 * Nk] * kij;
+}
+
+template <int NX>
+struct RCol {
+  using SX = fft::Split<NX>;
+  static constexpr int AX = SX::A, BX = SX::B;
+  static constexpr int NT = 256;
+};
+
+// Shared memory of a column kernel with TQ columns: the x twiddles, two
+// exchange buffers and `nkeep` natural-order spectra (rho_k of every species
+// forward, the force accumulators backward), each NX x TQ.
+__host__ __device__ inline size_t rcol_smem(int nx, int tq, int nkeep) {
+  return sizeof(cpx) * ((size_t)nx + (size_t)(2 + nkeep) * nx * tq);
+}
+
+// Per-column constants of in-plane index q.
+struct RColumn {
+  float ky, kz;
+  bool ynyq, proj, valid;
+};
+
+__device__ __forceinline__ RColumn rk_column(const EvalParams& p, long long q, float dky, float dkz) {
+  RColumn c;
+  const long long plane = (long long)p.ny * p.nzh;
+  c.valid = q < plane;
+  const int iy = c.valid ? (int)(q / p.nzh) : 0;
+  const int iz = c.valid ? (int)(q - (long long)iy * p.nzh) : 0;
+  c.ky = dky * (float)(iy <= p.ny / 2 ? iy : iy - p.ny);
+  c.kz = dkz * (float)iz;
+  c.ynyq = (p.ny % 2 == 0) && iy == p.ny / 2;
+  c.proj = (iz == 0) || (((p.nz & 1) == 0) && iz == p.nz / 2);
+  return c;
+}
+
+// Forward transform along x of one array's column tile: the natural-order
+// spectrum of tile column q, row kx, goes to spec[kx * TQ + q].
+template <int NX, int TQ>
+__device__ __forceinline__ void col_forward(const cpx* __restrict__ src, long long plane, long long q0, cpx* E,
+                                            cpx* spec, const cpx* tx) {
+  using C = RCol<NX>;
+  constexpr int AX = C::AX, BX = C::BX, NT = C::NT;
+#pragma unroll 1
+  for (int t = threadIdx.x; t < TQ * BX; t += NT) {
+    const int q = t % TQ, n2 = t / TQ;
+    const bool ok = q0 + q < plane;
+    cpx a[AX];
+#pragma unroll
+    for (int n1 = 0; n1 < AX; ++n1) a[n1] = ok ? src[(BX * n1 + n2) * plane + q0 + q] : cpx{0.0f, 0.0f};
+    fft::nat_in<NX, false>(a, n2, tx);
+#pragma unroll
+    for (int k1 = 0; k1 < AX; ++k1) E[(n2 * AX + k1) * TQ + q] = a[k1];
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int t = threadIdx.x; t < TQ * AX; t += NT) {
+    const int q = t % TQ, k1 = t / TQ;
+    cpx bv[BX];
+#pragma unroll
+    for (int n2 = 0; n2 < BX; ++n2) bv[n2] = E[(n2 * AX + k1) * TQ + q];
+    fft::nat_out<NX, false>(bv);
+#pragma unroll
+    for (int k2 = 0; k2 < BX; ++k2) spec[(k1 + AX * k2) * TQ + q] = bv[k2];
+  }
+}
+
+// Inverse transform along x of the natural-order spectrum whose values
+// kx = k1 + AX k2 (k2 < BX) of column q values(k1, q, bv) fills (called by
+// the thread that owns them in col_forward's second half), stored to dst
+// column q0 + q.
+template <int NX, int TQ, class V>
+__device__ __forceinline__ void col_inverse(V&& values, cpx* E, const cpx* tx, cpx* __restrict__ dst,
+                                            long long plane, long long q0) {
+  using C = RCol<NX>;
+  constexpr int AX = C::AX, BX = C::BX, NT = C::NT;
+#pragma unroll 1
+  for (int t = threadIdx.x; t < TQ * AX; t += NT) {
+    const int q = t % TQ, k1 = t / TQ;
+    cpx bv[BX];
+    values(k1, q, bv);
+    fft::spec_in<NX, true>(bv, k1, tx);
+#pragma unroll
+    for (int n2 = 0; n2 < BX; ++n2) E[(n2 * AX + k1) * TQ + q] = bv[n2];
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int t = threadIdx.x; t < TQ * BX; t += NT) {
+    const int q = t % TQ, n2 = t / TQ;
+    cpx a[AX];
+#pragma unroll
+    for (int k1 = 0; k1 < AX; ++k1) a[k1] = E[(n2 * AX + k1) * TQ + q];
+    fft::spec_out<NX, true>(a);
+    if (q0 + q < plane) {
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) dst[(BX * n1 + n2) * plane + q0 + q] = a[n1];
+    }
+  }
+}
+
+// Column pass of the forward stage: rho_k along x for every species, then
+// for every channel its k-space product and the inverse x transform.  Tile:
+// in-plane indices q0 .. q0 + TQ - 1 of all NX planes.  The two exchange
+// buffers alternate, so one barrier per transform suffices.
+template <int NX, int TQ, bool MULTI, bool TENSOR>
+__global__ void __launch_bounds__(256, 2)
+    k_rcol_fwd(EvalParams p, const cpx* __restrict__ prho, const float* __restrict__ wtab, cpx* __restrict__ q_out,
+               FftTables T) {
+  using L = Lay<MULTI, TENSOR>;
+  constexpr int NT = RCol<NX>::NT, TILE = NX * TQ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cpx* tx = reinterpret_cast<cpx*>(smem_raw);
+  cpx* Eb = tx + NX;
+  cpx* R = Eb + 2 * TILE;
+  const int S = p.S, C = p.n_chan;
+  const long long plane = (long long)p.ny * p.nzh, Nk = p.Nk;
+  const int b = blockIdx.y;
+  const long long q0 = (long long)blockIdx.x * TQ;
+  for (int i = threadIdx.x; i < NX; i += NT) tx[i] = T.tx[i];
+  __syncthreads();
+  int buf = 0;
+  for (int s = 0; s < S; ++s) {
+    col_forward<NX, TQ>(prho + ((long long)b * S + s) * Nk, plane, q0, Eb + buf * TILE, R + (size_t)s * TILE, tx);
+    buf ^= 1;
+  }
+  const float dkx = (float)p.dkx, dky = (float)p.dky, dkz = (float)p.dkz;
+  float i4r[kMaxSpecies], i4r2[kMaxSpecies];
+#pragma unroll
+  for (int s = 0; s < kMaxSpecies; ++s) {
+    i4r[s] = (float)p.inv4piR[s];
+    i4r2[s] = (float)p.inv4piR2[s];
+  }
+  for (int c = 0; c < C; ++c) {
+    // mean-field channel c: w * rho of species mf_sp (weight table mf_m)
+    int mf_m = -1, mf_sp = 0;
+    for (int m = 0; m < p.M; ++m) {
+      if (c == p.mf_chan_j[m]) mf_m = m, mf_sp = p.mf_j[m];
+      if (c == p.mf_chan_i[m]) mf_m = m, mf_sp = p.mf_i[m];
+    }
+    auto values = [&](int k1, int q, cpx* bv) {
+      const RColumn col = rk_column(p, q0 + q, dky, dkz);
+#pragma unroll
+      for (int k2 = 0; k2 < RCol<NX>::BX; ++k2) {
+        const int kx = k1 + RCol<NX>::AX * k2;
+        const long long kidx = (long long)kx * plane + q0 + q;
+        cpx acc{0.0f, 0.0f};
+        if (col.valid) {
+          if (mf_m >= 0) {
+            const float w = wtab[(5LL * S + mf_m) * Nk + kidx];
+            const cpx r = R[(size_t)mf_sp * TILE + kx * TQ + q];
+            acc = cpx{w * r.x, w * r.y};
+          } else {
+            const bool xnyq = (p.nx % 2 == 0) && kx == p.nx / 2;
+            const RKv v = rk_element(dkx * (float)(kx <= p.nx / 2 ? kx : kx - p.nx), xnyq, col.ky, col.ynyq, col.kz,
+                                     col.proj);
+#pragma unroll
+            for (int s = 0; s < (MULTI ? kMaxSpecies : 1); ++s) {
+              if (s < S) {
+                bool odd;
+                const float w = rk_weight<MULTI, TENSOR>(c, wtab + 5LL * s * Nk + kidx, Nk, v, i4r[s], i4r2[s], odd);
+                const cpx r = R[(size_t)s * TILE + kx * TQ + q];
+                if (odd) {
+                  acc.x -= w * r.y;
+                  acc.y += w * r.x;
+                } else {
+                  acc.x += w * r.x;
+                  acc.y += w * r.y;
+                }
+              }
+            }
+          }
+        }
+        bv[k2] = acc;
+      }
+    };
+    col_inverse<NX, TQ>(values, Eb + buf * TILE, tx, q_out + ((long long)b * C + c) * Nk, plane, q0);
+    buf ^= 1;
+  }
+}
+
+// Column pass of the backward stage: every derivative channel along x, the
+// back-convolution F_s = sum_c conj(W'_cs) D_c accumulated per element by
+// the thread that owns it, then the inverse x transform of each F_s.
+template <int NX, int TQ, bool MULTI, bool TENSOR>
+__global__ void __launch_bounds__(256, 2)
+    k_rcol_bwd(EvalParams p, const cpx* __restrict__ pd, const float* __restrict__ wtab, cpx* __restrict__ pf,
+               FftTables T) {
+  using L = Lay<MULTI, TENSOR>;
+  constexpr int NF = L::NFMT, NT = RCol<NX>::NT, TILE = NX * TQ;
+  constexpr int AX = RCol<NX>::AX, BX = RCol<NX>::BX;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cpx* tx = reinterpret_cast<cpx*>(smem_raw);
+  cpx* Eb = tx + NX;
+  cpx* F = Eb + 2 * TILE;  // S natural-order force spectra
+  const int S = p.S;
+  const long long plane = (long long)p.ny * p.nzh, Nk = p.Nk;
+  const int b = blockIdx.y;
+  const long long q0 = (long long)blockIdx.x * TQ;
+  for (int i = threadIdx.x; i < NX; i += NT) tx[i] = T.tx[i];
+  const float dkx = (float)p.dkx, dky = (float)p.dky, dkz = (float)p.dkz;
+  float i4r[kMaxSpecies], i4r2[kMaxSpecies];
+#pragma unroll
+  for (int s = 0; s < kMaxSpecies; ++s) {
+    i4r[s] = (float)p.inv4piR[s];
+    i4r2[s] = (float)p.inv4piR2[s];
+  }
+  __syncthreads();
+  int buf = 0;
+  for (int c = 0; c < NF; ++c) {
+    cpx* E = Eb + buf * TILE;
+    const cpx* src = pd + ((long long)b * NF + c) * Nk;
+#pragma unroll 1
+    for (int t = threadIdx.x; t < TQ * BX; t += NT) {
+      const int q = t % TQ, n2 = t / TQ;
+      const bool ok = q0 + q < plane;
+      cpx a[AX];
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) a[n1] = ok ? src[(BX * n1 + n2) * plane + q0 + q] : cpx{0.0f, 0.0f};
+      fft::nat_in<NX, false>(a, n2, tx);
+#pragma unroll
+      for (int k1 = 0; k1 < AX; ++k1) E[(n2 * AX + k1) * TQ + q] = a[k1];
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int t = threadIdx.x; t < TQ * AX; t += NT) {
+      const int q = t % TQ, k1 = t / TQ;
+      cpx d[BX];
+#pragma unroll
+      for (int n2 = 0; n2 < BX; ++n2) d[n2] = E[(n2 * AX + k1) * TQ + q];
+      fft::nat_out<NX, false>(d);
+      const RColumn col = rk_column(p, q0 + q, dky, dkz);
+#pragma unroll
+      for (int k2 = 0; k2 < BX; ++k2) {
+        const int kx = k1 + AX * k2;
+        const long long kidx = (long long)kx * plane + q0 + q;
+        const bool xnyq = (p.nx % 2 == 0) && kx == p.nx / 2;
+        const RKv v =
+            rk_element(dkx * (float)(kx <= p.nx / 2 ? kx : kx - p.nx), xnyq, col.ky, col.ynyq, col.kz, col.proj);
+#pragma unroll
+        for (int s = 0; s < (MULTI ? kMaxSpecies : 1); ++s) {
+          if (s < S) {
+            cpx add{0.0f, 0.0f};
+            if (col.valid) {
+              bool odd;
+              const float w = rk_weight<MULTI, TENSOR>(c, wtab + 5LL * s * Nk + kidx, Nk, v, i4r[s], i4r2[s], odd);
+              // conj(i w) D = -i w D for an odd channel
+              add = odd ? cpx{w * d[k2].y, -w * d[k2].x} : cpx{w * d[k2].x, w * d[k2].y};
+            }
+            cpx& f = F[(size_t)s * TILE + kx * TQ + q];
+            f = (c == 0) ? add : f + add;
+          }
+        }
+      }
+    }
+    buf ^= 1;
+  }
+  for (int s = 0; s < S; ++s) {
+    auto values = [&](int k1, int q, cpx* bv) {
+#pragma unroll
+      for (int k2 = 0; k2 < BX; ++k2) bv[k2] = F[(size_t)s * TILE + (k1 + AX * k2) * TQ + q];
+    };
+    col_inverse<NX, TQ>(values, Eb + buf * TILE, tx, pf + ((long long)b * S + s) * Nk, plane, q0);
+    buf ^= 1;
+  }
+}
+
+// ------------------------------------------- single-species column passes
+
+// One species: the thread of spectrum task (q, k1) keeps its BX elements'
+// |k| factors and rho_k (forward) or force accumulators (backward) in
+// registers for the whole pass, and the FMT channel loop is unrolled at
+// compile time, so each k-space product is a few multiplies.  One spectrum
+// task per thread (NT = TQ * AX); the first TQ * BX threads also run the
+// natural-order half of each transform.
+template <int NX, int TQ>
+struct RCol1 {
+  using SX = fft::Split<NX>;
+  static constexpr int AX = SX::A, BX = SX::B;
+  static constexpr int NT = TQ * AX;
+  static constexpr int TILE = NX * TQ;
+};
+
+__host__ __device__ inline size_t rcol1_smem(int nx, int tq) { return sizeof(cpx) * ((size_t)nx + 2ull * nx * tq); }
+
+// The |k| factors of a task's elements (zero for columns past the plane).
+template <int BX>
+struct RTab {
+  float w3[BX], w2[BX], fv[BX], a[BX], b[BX];
+};
+
+template <int NX, int TQ>
+__device__ __forceinline__ RTab<RCol1<NX, TQ>::BX> rk_task_table(const float* __restrict__ wtab, long long Nk,
+                                                                   long long plane, long long col0, int k1,
+                                                                   bool valid) {
+  constexpr int AX = RCol1<NX, TQ>::AX, BX = RCol1<NX, TQ>::BX;
+  RTab<BX> t;
+#pragma unroll
+  for (int k2 = 0; k2 < BX; ++k2) {
+    const long long kidx = (long long)(k1 + AX * k2) * plane + col0;
+    t.w3[k2] = valid ? wtab[kidx] : 0.0f;
+    t.w2[k2] = valid ? wtab[Nk + kidx] : 0.0f;
+    t.fv[k2] = valid ? wtab[2 * Nk + kidx] : 0.0f;
+    t.a[k2] = valid ? wtab[3 * Nk + kidx] : 0.0f;
+    t.b[k2] = valid ? wtab[4 * Nk + kidx] : 0.0f;
+  }
+  return t;
+}
+
+// Weight of FMT channel C (single species) at element k2 of a task; odd:
+// the channel is i w rho.
+template <bool TENSOR, int C, int BX>
+__device__ __forceinline__ float rk_weight1(const RTab<BX>& t, int k2, const RKv& v, bool& odd) {
+  using L = Lay<false, TENSOR>;
+  odd = false;
+  if constexpr (C == L::ETA) {
+    return t.w3[k2];
+  } else if constexpr (C == L::N2) {
+    return t.w2[k2];
+  } else if constexpr (C >= L::V1 && C < L::V1 + 3) {
+    odd = true;
+    constexpr int A = C - L::V1;
+    return t.fv[k2] * (v.k[A] * v.o[A]);
+  } else {
+    constexpr int TT = C - L::T;
+    constexpr int I = tchan_i(TT), J = tchan_j(TT);
+    if constexpr (I == J) {
+      return t.a[k2] * (v.k[I] * v.k[J]) + t.b[k2];
+    } else {
+      const float m = (I + J == 1) ? v.cxy : ((I + J == 2) ? v.cxz : v.cyz);
+      return t.a[k2] * (v.k[I] * v.k[J] * m);
+    }
+  }
+}
+
+template <int NX>
+__device__ __forceinline__ RKv rk_task_element(const EvalParams& p, int kx, float dkx, const RColumn& col) {
+  const bool xnyq = (p.nx % 2 == 0) && kx == p.nx / 2;
+  return rk_element(dkx * (float)(kx <= p.nx / 2 ? kx : kx - p.nx), xnyq, col.ky, col.ynyq, col.kz, col.proj);
+}
+
+// Inverse x transform of the task values bv (this thread's spectrum task)
+// through exchange buffer E; the natural-order half stores column q0 + q of
+// dst.  The caller alternates E between two buffers.
+template <int NX, int TQ>
+__device__ __forceinline__ void col1_inverse(cpx (&bv)[RCol1<NX, TQ>::BX], int q, int k1, cpx* E, const cpx* tx,
+                                             cpx* __restrict__ dst, long long plane, long long q0) {
+  using C = RCol1<NX, TQ>;
+  constexpr int AX = C::AX, BX = C::BX;
+  fft::spec_in<NX, true>(bv, k1, tx);
+#pragma unroll
+  for (int n2 = 0; n2 < BX; ++n2) E[(n2 * AX + k1) * TQ + q] = bv[n2];
+  __syncthreads();
+  const int t = threadIdx.x;
+  if (t < TQ * BX) {
+    const int qn = t % TQ, n2 = t / TQ;
+    cpx a[AX];
+#pragma unroll
+    for (int kk = 0; kk < AX; ++kk) a[kk] = E[(n2 * AX + kk) * TQ + qn];
+    fft::spec_out<NX, true>(a);
+    if (q0 + qn < plane) {
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) dst[(BX * n1 + n2) * plane + q0 + qn] = a[n1];
+    }
+  }
+}
+
+// Forward x transform of one array's column tile into this thread's task
+// values (natural-order spectrum elements k1 + AX k2 of column q).
+template <int NX, int TQ>
+__device__ __forceinline__ void col1_forward(const cpx* __restrict__ src, long long plane, long long q0, int q, int k1,
+                                             cpx* E, const cpx* tx, cpx (&out)[RCol1<NX, TQ>::BX]) {
+  using C = RCol1<NX, TQ>;
+  constexpr int AX = C::AX, BX = C::BX;
+  const int t = threadIdx.x;
+  if (t < TQ * BX) {
+    const int qn = t % TQ, n2 = t / TQ;
+    const bool ok = q0 + qn < plane;
+    cpx a[AX];
+#pragma unroll
+    for (int n1 = 0; n1 < AX; ++n1) a[n1] = ok ? src[(BX * n1 + n2) * plane + q0 + qn] : cpx{0.0f, 0.0f};
+    fft::nat_in<NX, false>(a, n2, tx);
+#pragma unroll
+    for (int kk = 0; kk < AX; ++kk) E[(n2 * AX + kk) * TQ + qn] = a[kk];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int n2 = 0; n2 < BX; ++n2) out[n2] = E[(n2 * AX + k1) * TQ + q];
+  fft::nat_out<NX, false>(out);
+}
+
+template <int NX, int TQ, bool TENSOR>
+__global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
+    k_rcol_fwd1(EvalParams p, const cpx* __restrict__ prho, const float* __restrict__ wtab, cpx* __restrict__ q_out,
+                FftTables T) {
+  using L = Lay<false, TENSOR>;
+  using C = RCol1<NX, TQ>;
+  constexpr int AX = C::AX, BX = C::BX, NT = C::NT, TILE = C::TILE;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cpx* tx = reinterpret_cast<cpx*>(smem_raw);
+  cpx* Eb = tx + NX;
+  const int NCH = p.n_chan;
+  const long long plane = (long long)p.ny * p.nzh, Nk = p.Nk;
+  const int b = blockIdx.y;
+  const long long q0 = (long long)blockIdx.x * TQ;
+  const int q = threadIdx.x % TQ, k1 = threadIdx.x / TQ;
+  for (int i = threadIdx.x; i < NX; i += NT) tx[i] = T.tx[i];
+  const RColumn col = rk_column(p, q0 + q, (float)p.dky, (float)p.dkz);
+  const RTab<BX> tab = rk_task_table<NX, TQ>(wtab, Nk, plane, q0 + q, k1, col.valid);
+  const float dkx = (float)p.dkx;
+  __syncthreads();
+  cpx r[BX];
+  col1_forward<NX, TQ>(prho + (long long)b * Nk, plane, q0, q, k1, Eb, tx, r);
+  int buf = 1;
+  cpx* out = q_out + (long long)b * NCH * Nk;
+  static_for<0, L::NFMT>([&](auto cc) {
+    constexpr int CH = decltype(cc)::value;
+    cpx bv[BX];
+#pragma unroll
+    for (int k2 = 0; k2 < BX; ++k2) {
+      const RKv v = rk_task_element<NX>(p, k1 + AX * k2, dkx, col);
+      bool odd;
+      const float w = rk_weight1<TENSOR, CH, BX>(tab, k2, v, odd);
+      bv[k2] = odd ? cpx{-w * r[k2].y, w * r[k2].x} : cpx{w * r[k2].x, w * r[k2].y};
+    }
+    col1_inverse<NX, TQ>(bv, q, k1, Eb + buf * TILE, tx, out + (long long)CH * Nk, plane, q0);
+    buf ^= 1;
+  });
+  // mean-field channels: w(k) rho_k with the real weight from the table
+  for (int m = 0; m < p.M; ++m) {
+    cpx bv[BX];
+#pragma unroll
+    for (int k2 = 0; k2 < BX; ++k2) {
+      const long long kidx = (long long)(k1 + AX * k2) * plane + q0 + q;
+      const float w = col.valid ? wtab[(5LL + m) * Nk + kidx] : 0.0f;
+      bv[k2] = cpx{w * r[k2].x, w * r[k2].y};
+    }
+    col1_inverse<NX, TQ>(bv, q, k1, Eb + buf * TILE, tx, out + (long long)p.mf_chan_j[m] * Nk, plane, q0);
+    buf ^= 1;
+  }
+}
+
+template <int NX, int TQ, bool TENSOR>
+__global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
+    k_rcol_bwd1(EvalParams p, const cpx* __restrict__ pd, const float* __restrict__ wtab, cpx* __restrict__ pf,
+                FftTables T) {
+  using L = Lay<false, TENSOR>;
+  using C = RCol1<NX, TQ>;
+  constexpr int AX = C::AX, BX = C::BX, NT = C::NT, TILE = C::TILE, NF = L::NFMT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cpx* tx = reinterpret_cast<cpx*>(smem_raw);
+  cpx* Eb = tx + NX;
+  const long long plane = (long long)p.ny * p.nzh, Nk = p.Nk;
+  const int b = blockIdx.y;
+  const long long q0 = (long long)blockIdx.x * TQ;
+  const int q = threadIdx.x % TQ, k1 = threadIdx.x / TQ;
+  for (int i = threadIdx.x; i < NX; i += NT) tx[i] = T.tx[i];
+  const RColumn col = rk_column(p, q0 + q, (float)p.dky, (float)p.dkz);
+  const RTab<BX> tab = rk_task_table<NX, TQ>(wtab, Nk, plane, q0 + q, k1, col.valid);
+  const float dkx = (float)p.dkx;
+  __syncthreads();
+  cpx f[BX];
+#pragma unroll
+  for (int k2 = 0; k2 < BX; ++k2) f[k2] = cpx{0.0f, 0.0f};
+  int buf = 0;
+  const cpx* src = pd + (long long)b * NF * Nk;
+  static_for<0, NF>([&](auto cc) {
+    constexpr int CH = decltype(cc)::value;
+    cpx d[BX];
+    col1_forward<NX, TQ>(src + (long long)CH * Nk, plane, q0, q, k1, Eb + buf * TILE, tx, d);
+#pragma unroll
+    for (int k2 = 0; k2 < BX; ++k2) {
+      const RKv v = rk_task_element<NX>(p, k1 + AX * k2, dkx, col);
+      bool odd;
+      const float w = rk_weight1<TENSOR, CH, BX>(tab, k2, v, odd);
+      // conj(i w) D = -i w D for an odd channel
+      f[k2] = odd ? cpx{f[k2].x + w * d[k2].y, f[k2].y - w * d[k2].x}
+                  : cpx{f[k2].x + w * d[k2].x, f[k2].y + w * d[k2].y};
+    }
+    buf ^= 1;
+  });
+  col1_inverse<NX, TQ>(f, q, k1, Eb + buf * TILE, tx, pf + (long long)b * Nk, plane, q0);
+}
+
+}  // namespace rk
+}  // namespace cdft

@@ -1,18 +1,17 @@
 // Instantiations and launchers of the fused transform path (the kernels are
-// in fft_kernels.cuh): dispatch from runtime grid sizes and channel layout to
-// the size-specialised kernels.
+// in fft_reg_kernels.cuh): dispatch from runtime grid sizes and channel
+// layout to the size-specialised kernels.
 #include "fused.cuh"
 
 #include <type_traits>
 
-#include "fft_kernels.cuh"
+#include "fft_reg_kernels.cuh"
 
 namespace cdft {
 
 namespace {
 
-constexpr size_t kSmemCap = 110 * 1024;     // plane kernels: two CTAs per SM at least
-constexpr size_t kColSmemCap = 74 * 1024;   // column kernels: three CTAs per SM
+constexpr size_t kSmemCap = 110 * 1024;  // two CTAs per SM at least
 
 template <int N>
 using IC = std::integral_constant<int, N>;
@@ -51,6 +50,15 @@ void with_layout(const EvalParams& p, F&& f) {
   }
 }
 
+// f(IC<tq>) for the column tile width of the plan.
+template <class F>
+void with_tq(int tq, F&& f) {
+  if (tq == 32)
+    f(IC<32>{});
+  else
+    f(IC<16>{});
+}
+
 template <class K>
 void allow_smem(K kern, size_t bytes) {
   CDFT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -62,35 +70,48 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan) {
   FusedPlan f;
   bool ok = with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
-    f.plane_smem = Plane<NY, NZ, kPlaneThreads>::kSmem;
+    f.plane_smem = rk::RPlane<NY, NZ>::kSmem;
   });
   ok = ok && with_len(p.nx, [](auto) {});
   if (!ok || f.plane_smem > kSmemCap) return false;
-  // column tiles: the widest (at most 16 columns) whose buffers leave room
-  // for three CTAs per SM (one CTA's worth of buffers at the least)
-  f.ltq = 4;
-  while (f.ltq > 0 &&
-         (col_smem(p.nx, f.ltq, p.S + p.n_chan) > kColSmemCap || col_smem(p.nx, f.ltq, p.L.n_deriv) > kColSmemCap))
-    --f.ltq;
-  f.colf_smem = col_smem(p.nx, f.ltq, p.S + p.n_chan);
-  f.colb_smem = col_smem(p.nx, f.ltq, p.L.n_deriv);
-  if (f.colf_smem > kSmemCap || f.colb_smem > kSmemCap) return false;
-  f.col_tiles = (int)(((long long)p.ny * p.nzh + (1 << f.ltq) - 1) >> f.ltq);
+  // column tiles: one species keeps its spectra in registers (16 columns
+  // a tile); several keep them in shared memory (32 columns unless their
+  // spectra need narrower tiles)
+  if (p.S == 1) {
+    f.tq = 16;
+    f.colf_smem = rk::rcol1_smem(p.nx, f.tq);
+  } else {
+    f.tq = 32;
+    if (rk::rcol_smem(p.nx, f.tq, p.S) > kSmemCap) f.tq = 16;
+    f.colf_smem = rk::rcol_smem(p.nx, f.tq, p.S);
+  }
+  f.colb_smem = f.colf_smem;
+  if (f.colf_smem > kSmemCap) return false;
+  f.col_tiles = (int)(((long long)p.ny * p.nzh + f.tq - 1) / f.tq);
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
-    allow_smem(k_plane_fwd<NY, NZ, double, kPlaneThreadsWide>, f.plane_smem);
-    allow_smem(k_plane_fwd<NY, NZ, float, kPlaneThreads>, f.plane_smem);
-    allow_smem(k_plane_inv<NY, NZ>, f.plane_smem);
+    allow_smem(rk::k_rplane_fwd<NY, NZ, double>, f.plane_smem);
+    allow_smem(rk::k_rplane_fwd<NY, NZ, float>, f.plane_smem);
     with_layout(p, [&](auto mc, auto tc) {
-      allow_smem(k_plane_inv_epi<NY, NZ, decltype(mc)::value, decltype(tc)::value>, f.plane_smem);
+      constexpr bool MU = decltype(mc)::value, TE = decltype(tc)::value;
+      allow_smem(rk::k_rplane_inv<NY, NZ, false, MU, TE>, f.plane_smem);
+      allow_smem(rk::k_rplane_inv<NY, NZ, true, MU, TE>, f.plane_smem);
     });
   });
   with_len(p.nx, [&](auto xc) {
     constexpr int NX = decltype(xc)::value;
-    with_layout(p, [&](auto mc, auto tc) {
-      constexpr bool MU = decltype(mc)::value, TE = decltype(tc)::value;
-      allow_smem(k_col_fwd<NX, MU, TE>, f.colf_smem);
-      allow_smem(k_col_bwd<NX, MU, TE>, f.colb_smem);
+    with_tq(f.tq, [&](auto qc) {
+      constexpr int TQ = decltype(qc)::value;
+      with_layout(p, [&](auto mc, auto tc) {
+        constexpr bool MU = decltype(mc)::value, TE = decltype(tc)::value;
+        if constexpr (MU) {
+          allow_smem(rk::k_rcol_fwd<NX, TQ, MU, TE>, f.colf_smem);
+          allow_smem(rk::k_rcol_bwd<NX, TQ, MU, TE>, f.colb_smem);
+        } else {
+          allow_smem(rk::k_rcol_fwd1<NX, TQ, TE>, f.colf_smem);
+          allow_smem(rk::k_rcol_bwd1<NX, TQ, TE>, f.colb_smem);
+        }
+      });
     });
   });
   *plan = f;
@@ -100,18 +121,27 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan) {
 void fused_plane_fwd_rho(const FusedPlan& f, const EvalParams& p, const double* rho, const double* mean,
                          fft::cpx* prho, const FftTables& T, cudaStream_t st) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
-    k_plane_fwd<decltype(yc)::value, decltype(zc)::value, double, kPlaneThreadsWide>
-        <<<dim3(p.nx, p.S, p.batch), kPlaneThreadsWide, f.plane_smem, st>>>(p, rho, p.S, mean, prho, T);
+    constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
+    rk::k_rplane_fwd<NY, NZ, double>
+        <<<dim3(p.nx, p.S, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(p, rho, p.S, mean, prho, T);
   });
   CDFT_CUDA(cudaGetLastError());
 }
 
-void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho, const double* mf_w,
-                   const float* wtab, fft::cpx* q, const FftTables& T, cudaStream_t st) {
+void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho, const float* wtab, fft::cpx* q,
+                   const FftTables& T, cudaStream_t st) {
   with_len(p.nx, [&](auto xc) {
-    with_layout(p, [&](auto mc, auto tc) {
-      k_col_fwd<decltype(xc)::value, decltype(mc)::value, decltype(tc)::value>
-          <<<dim3(f.col_tiles, p.batch), kColThreads, f.colf_smem, st>>>(p, prho, mf_w, wtab, q, f.ltq, T);
+    with_tq(f.tq, [&](auto qc) {
+      with_layout(p, [&](auto mc, auto tc) {
+        constexpr int NX = decltype(xc)::value, TQ = decltype(qc)::value;
+        constexpr bool MU = decltype(mc)::value, TE = decltype(tc)::value;
+        if constexpr (MU)
+          rk::k_rcol_fwd<NX, TQ, MU, TE>
+              <<<dim3(f.col_tiles, p.batch), rk::RCol<NX>::NT, f.colf_smem, st>>>(p, prho, wtab, q, T);
+        else
+          rk::k_rcol_fwd1<NX, TQ, TE>
+              <<<dim3(f.col_tiles, p.batch), rk::RCol1<NX, TQ>::NT, f.colf_smem, st>>>(p, prho, wtab, q, T);
+      });
     });
   });
   CDFT_CUDA(cudaGetLastError());
@@ -120,8 +150,12 @@ void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho
 void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q, float* chan_r, const FftTables& T,
                      cudaStream_t st) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
-    k_plane_inv<decltype(yc)::value, decltype(zc)::value>
-        <<<dim3(p.nx, p.n_chan, p.batch), kPlaneThreads, f.plane_smem, st>>>(p, q, p.n_chan, chan_r, T);
+    constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
+    with_layout(p, [&](auto mc, auto tc) {
+      rk::k_rplane_inv<NY, NZ, false, decltype(mc)::value, decltype(tc)::value>
+          <<<dim3(p.nx, p.n_chan, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(
+              p, q, p.n_chan, chan_r, nullptr, nullptr, MuArgs{}, FinalArgs{nullptr, 0, nullptr, nullptr}, T);
+    });
   });
   CDFT_CUDA(cudaGetLastError());
 }
@@ -129,9 +163,9 @@ void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q,
 void fused_plane_fwd_deriv(const FusedPlan& f, const EvalParams& p, const float* deriv_r, fft::cpx* pd,
                            const FftTables& T, cudaStream_t st) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
-    k_plane_fwd<decltype(yc)::value, decltype(zc)::value, float, kPlaneThreads>
-        <<<dim3(p.nx, p.L.n_deriv, p.batch), kPlaneThreads, f.plane_smem, st>>>(p, deriv_r, p.L.n_deriv, nullptr,
-                                                                                 pd, T);
+    constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
+    rk::k_rplane_fwd<NY, NZ, float><<<dim3(p.nx, p.L.n_deriv, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(
+        p, deriv_r, p.L.n_deriv, nullptr, pd, T);
   });
   CDFT_CUDA(cudaGetLastError());
 }
@@ -139,9 +173,17 @@ void fused_plane_fwd_deriv(const FusedPlan& f, const EvalParams& p, const float*
 void fused_col_bwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* pd, const float* wtab, fft::cpx* pf,
                    const FftTables& T, cudaStream_t st) {
   with_len(p.nx, [&](auto xc) {
-    with_layout(p, [&](auto mc, auto tc) {
-      k_col_bwd<decltype(xc)::value, decltype(mc)::value, decltype(tc)::value>
-          <<<dim3(f.col_tiles, p.batch), kColThreads, f.colb_smem, st>>>(p, pd, wtab, pf, f.ltq, T);
+    with_tq(f.tq, [&](auto qc) {
+      with_layout(p, [&](auto mc, auto tc) {
+        constexpr int NX = decltype(xc)::value, TQ = decltype(qc)::value;
+        constexpr bool MU = decltype(mc)::value, TE = decltype(tc)::value;
+        if constexpr (MU)
+          rk::k_rcol_bwd<NX, TQ, MU, TE>
+              <<<dim3(f.col_tiles, p.batch), rk::RCol<NX>::NT, f.colb_smem, st>>>(p, pd, wtab, pf, T);
+        else
+          rk::k_rcol_bwd1<NX, TQ, TE>
+              <<<dim3(f.col_tiles, p.batch), rk::RCol1<NX, TQ>::NT, f.colb_smem, st>>>(p, pd, wtab, pf, T);
+      });
     });
   });
   CDFT_CUDA(cudaGetLastError());
@@ -150,18 +192,20 @@ void fused_col_bwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* pd, 
 void fused_plane_inv_epi(const FusedPlan& f, const EvalParams& p, const fft::cpx* pf, const double* dbar,
                          double* force, const MuArgs& mu, const FinalArgs& fin, const FftTables& T, cudaStream_t st) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
+    constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
     with_layout(p, [&](auto mc, auto tc) {
-      k_plane_inv_epi<decltype(yc)::value, decltype(zc)::value, decltype(mc)::value, decltype(tc)::value>
-          <<<dim3(p.nx, p.S, p.batch), kPlaneThreadsWide, f.plane_smem, st>>>(p, pf, dbar, force, mu, fin, T);
+      rk::k_rplane_inv<NY, NZ, true, decltype(mc)::value, decltype(tc)::value>
+          <<<dim3(p.nx, p.S, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(p, pf, p.S, nullptr, force, dbar,
+                                                                                   mu, fin, T);
     });
   });
   CDFT_CUDA(cudaGetLastError());
 }
 
-long long fused_weight_table_floats(const EvalParams& p) { return weight_table_floats(p); }
+long long fused_weight_table_floats(const EvalParams& p) { return rk::rweight_table_floats(p); }
 
-void fused_build_weights(const EvalParams& p, float* wtab, cudaStream_t st) {
-  k_build_weights<<<592, 256, 0, st>>>(p, wtab);
+void fused_build_weights(const EvalParams& p, const double* mf_w, float* wtab, cudaStream_t st) {
+  rk::k_build_rweights<<<592, 256, 0, st>>>(p, mf_w, wtab);
   CDFT_CUDA(cudaGetLastError());
 }
 

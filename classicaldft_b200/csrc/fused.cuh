@@ -1,5 +1,5 @@
 // Launchers of the fused transform path (fused.cu, kernels in
-// fft_kernels.cuh).  Specialisations exist for nx in {16, 32, 64, 128} and
+// fft_reg_kernels.cuh).  Specialisations exist for nx in {16, 32, 64, 128} and
 // (ny, nz) in {16, 32, 64, 128}^2; fused_plan reports whether an engine's grid
 // and channel count have one.
 #pragma once
@@ -11,7 +11,7 @@ namespace cdft {
 
 struct FusedPlan {
   size_t plane_smem = 0, colf_smem = 0, colb_smem = 0;
-  int ltq = 0;        // log2 of the columns per column-pass tile
+  int tq = 0;         // columns per column-pass tile
   int col_tiles = 0;  // column-pass CTAs per problem
 };
 
@@ -21,12 +21,13 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan);
 
 void fused_plane_fwd_rho(const FusedPlan& f, const EvalParams& p, const double* rho, const double* mean,
                          fft::cpx* prho, const FftTables& T, cudaStream_t st);
-// The column pass reads the FMT weights from a table built once per engine.
+// The column pass reads the FMT and mean-field weights from a table built
+// once per engine (after the mean-field weights).
 long long fused_weight_table_floats(const EvalParams& p);
-void fused_build_weights(const EvalParams& p, float* wtab, cudaStream_t st);
+void fused_build_weights(const EvalParams& p, const double* mf_w, float* wtab, cudaStream_t st);
 
-void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho, const double* mf_w,
-                   const float* wtab, fft::cpx* q, const FftTables& T, cudaStream_t st);
+void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho, const float* wtab, fft::cpx* q,
+                   const FftTables& T, cudaStream_t st);
 void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q, float* chan_r, const FftTables& T,
                      cudaStream_t st);
 void fused_plane_fwd_deriv(const FusedPlan& f, const EvalParams& p, const float* deriv_r, fft::cpx* pd,

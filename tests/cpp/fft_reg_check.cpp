@@ -1,0 +1,165 @@
+// Host build of the register-resident transform steps
+// (classicaldft_b200/csrc/fft_reg.cuh) for the CPU tests: every task of a
+// GPU pass runs here in a sequential loop, with the exchange between the two
+// halves of a transform done through an explicit array exactly as the
+// kernels index their shared-memory buffers.  C linkage for ctypes; double
+// on the interface, float inside.
+#include <cmath>
+#include <vector>
+
+#include "fft_reg.cuh"
+
+using cdft::fft::cpx;
+namespace F = cdft::fft;
+
+namespace {
+
+std::vector<cpx> table(int M) {  // exp(-2 pi i n / M), rounded from FP64
+  std::vector<cpx> t(M);
+  for (int n = 0; n < M; ++n) {
+    const double a = -2.0 * 3.14159265358979323846 * n / M;
+    t[n] = {(float)std::cos(a), (float)std::sin(a)};
+  }
+  return t;
+}
+
+// One transform of the sequence x[0..N) (element e at x[e * stride]) in
+// either ordering; out is natural order, written back in place.
+template <int N, bool INV>
+void transform(cpx* x, int stride, bool spectrum_in, const cpx* tw) {
+  using S = F::Split<N>;
+  constexpr int A = S::A, B = S::B;
+  std::vector<cpx> ex((size_t)N);  // ex[n2 * A + k1], as the kernels' exchange
+  if (!spectrum_in) {
+    for (int n2 = 0; n2 < B; ++n2) {
+      cpx a[A];
+      for (int n1 = 0; n1 < A; ++n1) a[n1] = x[(B * n1 + n2) * stride];
+      F::nat_in<N, INV>(a, n2, tw);
+      for (int k1 = 0; k1 < A; ++k1) ex[n2 * A + k1] = a[k1];
+    }
+    for (int k1 = 0; k1 < A; ++k1) {
+      cpx b[B];
+      for (int n2 = 0; n2 < B; ++n2) b[n2] = ex[n2 * A + k1];
+      F::nat_out<N, INV>(b);
+      for (int k2 = 0; k2 < B; ++k2) x[(k1 + A * k2) * stride] = b[k2];
+    }
+  } else {
+    for (int k1 = 0; k1 < A; ++k1) {
+      cpx b[B];
+      for (int k2 = 0; k2 < B; ++k2) b[k2] = x[(k1 + A * k2) * stride];
+      F::spec_in<N, INV>(b, k1, tw);
+      for (int n2 = 0; n2 < B; ++n2) ex[n2 * A + k1] = b[n2];
+    }
+    for (int n2 = 0; n2 < B; ++n2) {
+      cpx a[A];
+      for (int k1 = 0; k1 < A; ++k1) a[k1] = ex[n2 * A + k1];
+      F::spec_out<N, INV>(a);
+      for (int n1 = 0; n1 < A; ++n1) x[(B * n1 + n2) * stride] = a[n1];
+    }
+  }
+}
+
+template <bool INV>
+void transform_rt(int N, cpx* x, int stride, bool spectrum_in, const cpx* tw) {
+  switch (N) {
+    case 1: break;  // a length-1 transform is the identity
+    case 2: transform<2, INV>(x, stride, spectrum_in, tw); break;
+    case 4: transform<4, INV>(x, stride, spectrum_in, tw); break;
+    case 8: transform<8, INV>(x, stride, spectrum_in, tw); break;
+    case 16: transform<16, INV>(x, stride, spectrum_in, tw); break;
+    case 32: transform<32, INV>(x, stride, spectrum_in, tw); break;
+    case 64: transform<64, INV>(x, stride, spectrum_in, tw); break;
+    case 128: transform<128, INV>(x, stride, spectrum_in, tw); break;
+    default: transform<256, INV>(x, stride, spectrum_in, tw); break;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int fr_split_a(int N) {
+  switch (N) {
+    case 2: return F::Split<2>::A;
+    case 4: return F::Split<4>::A;
+    case 8: return F::Split<8>::A;
+    case 16: return F::Split<16>::A;
+    case 32: return F::Split<32>::A;
+    case 64: return F::Split<64>::A;
+    case 128: return F::Split<128>::A;
+    default: return F::Split<256>::A;
+  }
+}
+
+// One complex transform: spectrum_in selects the ordering, inv the sign.
+void fr_transform(int N, int spectrum_in, int inv, double* re, double* im) {
+  std::vector<cpx> x(N);
+  for (int i = 0; i < N; ++i) x[i] = {(float)re[i], (float)im[i]};
+  const auto tw = table(N);
+  if (inv)
+    transform_rt<true>(N, x.data(), 1, spectrum_in != 0, tw.data());
+  else
+    transform_rt<false>(N, x.data(), 1, spectrum_in != 0, tw.data());
+  for (int i = 0; i < N; ++i) {
+    re[i] = x[i].x;
+    im[i] = x[i].y;
+  }
+}
+
+// The forward plane pass: z transforms of the pairs x[2n] + i x[2n+1] of
+// every row, y transforms of the M packed columns, post-processing on the
+// y-spectrum.  real: ny*nz; out: ny*(nz/2+1).
+void fr_plane_forward(int ny, int nz, const double* real, double* out_re, double* out_im) {
+  const int M = nz / 2, ld = M + 1;
+  std::vector<cpx> Z((size_t)ny * M);
+  for (int y = 0; y < ny; ++y)
+    for (int n = 0; n < M; ++n)
+      Z[(size_t)y * M + n] = {(float)real[(size_t)y * nz + 2 * n], (float)real[(size_t)y * nz + 2 * n + 1]};
+  const auto twz = table(M), tw2 = table(nz), twy = table(ny);
+  for (int y = 0; y < ny; ++y) transform_rt<false>(M, &Z[(size_t)y * M], 1, false, twz.data());
+  for (int kz = 0; kz < M; ++kz) transform_rt<false>(ny, &Z[kz], M, false, twy.data());
+  for (int ky = 0; ky < ny; ++ky) {
+    const int km = (ny - ky) % ny;
+    for (int kz = 0; kz < M; ++kz) {
+      cpx x0, xM;
+      if (kz == 0) {
+        F::r2c_post_2d_dc(Z[(size_t)ky * M], Z[(size_t)km * M], x0, xM);
+        out_re[(size_t)ky * ld] = x0.x;
+        out_im[(size_t)ky * ld] = x0.y;
+        out_re[(size_t)ky * ld + M] = xM.x;
+        out_im[(size_t)ky * ld + M] = xM.y;
+      } else {
+        const cpx v = F::r2c_post_2d(Z[(size_t)ky * M + kz], Z[(size_t)km * M + (M - kz)], tw2[kz]);
+        out_re[(size_t)ky * ld + kz] = v.x;
+        out_im[(size_t)ky * ld + kz] = v.y;
+      }
+    }
+  }
+}
+
+// The inverse plane pass (unnormalised C2R of the Hermitian projection):
+// pre-processing on the y-spectrum, inverse y transforms of the M packed
+// columns, inverse z transforms of the rows, samples doubled.
+void fr_plane_inverse(int ny, int nz, const double* in_re, const double* in_im, double* real) {
+  const int M = nz / 2, ld = M + 1;
+  auto X = [&](int ky, int kz) {
+    return cpx{(float)in_re[(size_t)ky * ld + kz], (float)in_im[(size_t)ky * ld + kz]};
+  };
+  const auto twz = table(M), tw2 = table(nz), twy = table(ny);
+  std::vector<cpx> Z((size_t)ny * M);
+  for (int ky = 0; ky < ny; ++ky) {
+    const int km = (ny - ky) % ny;
+    for (int kz = 0; kz < M; ++kz)
+      Z[(size_t)ky * M + kz] = kz == 0 ? F::c2r_pre_2d_dc(X(ky, 0), X(km, 0), X(ky, M), X(km, M))
+                                       : F::c2r_pre_2d(X(ky, kz), X(km, M - kz), tw2[kz]);
+  }
+  for (int kz = 0; kz < M; ++kz) transform_rt<true>(ny, &Z[kz], M, true, twy.data());
+  for (int y = 0; y < ny; ++y) transform_rt<true>(M, &Z[(size_t)y * M], 1, true, twz.data());
+  for (int y = 0; y < ny; ++y)
+    for (int n = 0; n < M; ++n) {
+      real[(size_t)y * nz + 2 * n] = 2.0 * Z[(size_t)y * M + n].x;
+      real[(size_t)y * nz + 2 * n + 1] = 2.0 * Z[(size_t)y * M + n].y;
+    }
+}
+
+}  // extern "C"
