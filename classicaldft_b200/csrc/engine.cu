@@ -501,11 +501,11 @@ void Engine::fused_forward(const double* rho, cudaStream_t stream) {
   mark(1, stream);
   fft::cpx* prho = static_cast<fft::cpx*>(rho_k_);
   fft::cpx* q = static_cast<fft::cpx*>(chan_k_);
-  fused_plane_fwd_rho(plan_, p, rho, mean_, prho, tables_, stream);
+  fused_plane_fwd_rho(plan_, p, rho, mean_, prho, err_, tables_, stream);
   mark(2, stream);
   fused_col_fwd(plan_, p, prho, wtab_, q, tables_, stream);
   mark(3, stream);
-  fused_plane_inv(plan_, p, q, static_cast<float*>(chan_r_), tables_, stream);
+  fused_plane_inv(plan_, p, q, static_cast<float*>(chan_r_), err_, tables_, stream);
   mark(4, stream);
 }
 
@@ -516,11 +516,11 @@ void Engine::fused_backward(double* force, const MuArgs& mu, const FinalArgs& fi
   const EvalParams& p = p_;
   fft::cpx* pd = static_cast<fft::cpx*>(deriv_k_);
   fft::cpx* pf = static_cast<fft::cpx*>(force_k_);
-  fused_plane_fwd_deriv(plan_, p, static_cast<const float*>(deriv_r_), pd, tables_, stream);
+  fused_plane_fwd_deriv(plan_, p, static_cast<const float*>(deriv_r_), pd, err_, tables_, stream);
   mark(6, stream);
   fused_col_bwd(plan_, p, pd, wtab_, pf, tables_, stream);
   mark(7, stream);
-  fused_plane_inv_epi(plan_, p, pf, dbar_, force, mu, fin, tables_, stream);
+  fused_plane_inv_epi(plan_, p, pf, dbar_, force, mu, fin, err_, tables_, stream);
   mark(8, stream);
   mark(9, stream);
 }

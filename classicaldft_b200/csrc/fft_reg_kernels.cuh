@@ -70,13 +70,37 @@ __device__ __forceinline__ void plane_tables(cpx* ty, cpx* tz, cpx* t2, const Ff
   for (int i = threadIdx.x; i < NZ; i += NT) t2[i] = T.t2[i];
 }
 
+// One bulk copy (TMA, no multicast) of `bytes` (a multiple of 16, both
+// addresses 16-byte aligned) from global memory into shared dst, waited for
+// by every thread with a bound.  False, with *err set, when the wait gave
+// up: the block then waits once more (bounded) so a late copy lands before
+// it exits, and returns without using the data.
+__device__ __forceinline__ bool bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar, int* err) {
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_arrive_expect_tx(bar, bytes);
+    bulk_copy_g2s(dst, src, bytes, bar);
+  }
+  const bool ok = mbar_wait_bounded(bar, 0, kWaitLimit);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0 && err) atomicExch(err, 1);
+    mbar_wait_bounded(bar, 0, kWaitLimit);
+    return false;
+  }
+  return true;
+}
+
 // Forward plane pass of one real NY x NZ plane (IN = double: rho minus the
 // species mean, the mixed-precision split; IN = float: a derivative
 // channel) into its half spectrum (NY x (NZ/2 + 1), natural order).
 template <int NY, int NZ, typename IN>
 __global__ void __launch_bounds__(RPlane<NY, NZ>::NT)
     k_rplane_fwd(EvalParams p, const IN* __restrict__ in, int nseq, const double* __restrict__ mean,
-                 cpx* __restrict__ out, FftTables T) {
+                 cpx* __restrict__ out, int* err, FftTables T) {
   using P = RPlane<NY, NZ>;
   constexpr int M = P::M, LD = P::LD, AY = P::AY, BY = P::BY, AZ = P::AZ, BZ = P::BZ, NT = P::NT;
   constexpr int EY = P::EY, ER = P::ER, EZS = P::EZS, EZ = P::EZ;
@@ -89,22 +113,49 @@ __global__ void __launch_bounds__(RPlane<NY, NZ>::NT)
   plane_tables<NY, NZ, NT>(ty, tz, t2, T);
   __syncthreads();
   const IN* src = in + ((long long)b * nseq + sq) * p.N + (long long)ix * NY * NZ;
-  const double c = mean ? mean[b * kMaxSpecies + sq] : 0.0;
-  // z, first half: task (y, n2) takes the pairs n = BZ n1 + n2 of row y
-  for (int t = threadIdx.x; t < P::T_Z_NAT; t += NT) {
-    const int n2 = t % BZ, y = t / BZ;
-    cpx a[AZ];
+  if constexpr (sizeof(IN) == 8) {
+    // rho (FP64): task (y, n2) takes the pairs n = BZ n1 + n2 of row y
+    // straight from global memory, minus the species mean
+    const double c = mean ? mean[b * kMaxSpecies + sq] : 0.0;
+    for (int t = threadIdx.x; t < P::T_Z_NAT; t += NT) {
+      const int n2 = t % BZ, y = t / BZ;
+      cpx a[AZ];
 #pragma unroll
-    for (int n1 = 0; n1 < AZ; ++n1) {
-      const IN* q = src + (long long)y * NZ + 2 * (BZ * n1 + n2);  // the caller's buffer: scalar loads
-      if constexpr (sizeof(IN) == 8)
+      for (int n1 = 0; n1 < AZ; ++n1) {
+        const IN* q = src + (long long)y * NZ + 2 * (BZ * n1 + n2);  // the caller's buffer: scalar loads
         a[n1] = {(float)(q[0] - c), (float)(q[1] - c)};
-      else
-        a[n1] = {q[0], q[1]};
-    }
-    fft::nat_in<M, false>(a, n2, tz);
+      }
+      fft::nat_in<M, false>(a, n2, tz);
 #pragma unroll
-    for (int k1 = 0; k1 < AZ; ++k1) E[y * EZ + n2 * EZS + k1] = a[k1];
+      for (int k1 = 0; k1 < AZ; ++k1) E[y * EZ + n2 * EZS + k1] = a[k1];
+    }
+  } else {
+    // a derivative channel (FP32, the engine's buffer): the plane arrives in
+    // shared memory by one bulk copy; its pairs are E[y * M + n]
+    __shared__ __align__(8) uint64_t bar;
+    if (!bulk_load(E, src, sizeof(float) * NY * NZ, &bar, err)) return;
+    constexpr int H0 = cdiv(P::T_Z_NAT, NT);
+    cpx h0[H0][AZ];
+#pragma unroll
+    for (int j = 0; j < H0; ++j) {
+      const int t = threadIdx.x + j * NT;
+      if (t < P::T_Z_NAT) {
+        const int n2 = t % BZ, y = t / BZ;
+#pragma unroll
+        for (int n1 = 0; n1 < AZ; ++n1) h0[j][n1] = E[y * M + BZ * n1 + n2];
+        fft::nat_in<M, false>(h0[j], n2, tz);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < H0; ++j) {
+      const int t = threadIdx.x + j * NT;
+      if (t < P::T_Z_NAT) {
+        const int n2 = t % BZ, y = t / BZ;
+#pragma unroll
+        for (int k1 = 0; k1 < AZ; ++k1) E[y * EZ + n2 * EZS + k1] = h0[j][k1];
+      }
+    }
   }
   __syncthreads();
   // z, second half: task (y, k1) -> Z_y[kz = k1 + AZ k2]
@@ -205,7 +256,7 @@ template <int NY, int NZ, bool EPI, bool MULTI, bool TENSOR>
 __global__ void __launch_bounds__(RPlane<NY, NZ>::NT)
     k_rplane_inv(EvalParams p, const cpx* __restrict__ in, int nseq, float* __restrict__ out_f,
                  double* __restrict__ force, const double* __restrict__ dbar, const __grid_constant__ MuArgs mu,
-                 FinalArgs fin, FftTables T) {
+                 FinalArgs fin, int* err, FftTables T) {
   using P = RPlane<NY, NZ>;
   using L = Lay<MULTI, TENSOR>;
   constexpr int M = P::M, LD = P::LD, AY = P::AY, BY = P::BY, AZ = P::AZ, BZ = P::BZ, NT = P::NT;
@@ -236,22 +287,39 @@ __global__ void __launch_bounds__(RPlane<NY, NZ>::NT)
   plane_tables<NY, NZ, NT>(ty, tz, t2, T);
   __syncthreads();
   const cpx* src = in + ((long long)b * nseq + sq) * p.Nk + (long long)ix * NY * LD;
+  // the half spectrum arrives in shared memory by one bulk copy: X[ky][kz]
+  // at E[ky * LD + kz]
+  __shared__ __align__(8) uint64_t bar;
+  if (!bulk_load(E, src, sizeof(cpx) * NY * LD, &bar, err)) return;
   // y, first half: task (kz, k1) pre-processes X[ky = k1 + AY k2][kz] with
   // its mirror and starts the inverse y transform
-  for (int t = threadIdx.x; t < P::T_Y_SPEC; t += NT) {
-    const int kz = t % M, k1 = t / M;
-    cpx bv[BY];
+  constexpr int H0 = cdiv(P::T_Y_SPEC, NT);
+  cpx h0[H0][BY];
 #pragma unroll
-    for (int k2 = 0; k2 < BY; ++k2) {
-      const int ky = k1 + AY * k2, km = (NY - ky) & (NY - 1);
-      if (kz == 0)
-        bv[k2] = fft::c2r_pre_2d_dc(src[ky * LD], src[km * LD], src[ky * LD + M], src[km * LD + M]);
-      else
-        bv[k2] = fft::c2r_pre_2d(src[ky * LD + kz], src[km * LD + (M - kz)], t2[kz]);
+  for (int j = 0; j < H0; ++j) {
+    const int t = threadIdx.x + j * NT;
+    if (t < P::T_Y_SPEC) {
+      const int kz = t % M, k1 = t / M;
+#pragma unroll
+      for (int k2 = 0; k2 < BY; ++k2) {
+        const int ky = k1 + AY * k2, km = (NY - ky) & (NY - 1);
+        if (kz == 0)
+          h0[j][k2] = fft::c2r_pre_2d_dc(E[ky * LD], E[km * LD], E[ky * LD + M], E[km * LD + M]);
+        else
+          h0[j][k2] = fft::c2r_pre_2d(E[ky * LD + kz], E[km * LD + (M - kz)], t2[kz]);
+      }
+      fft::spec_in<NY, true>(h0[j], k1, ty);
     }
-    fft::spec_in<NY, true>(bv, k1, ty);
+  }
+  __syncthreads();
 #pragma unroll
-    for (int n2 = 0; n2 < BY; ++n2) E[(n2 * AY + k1) * EY + kz] = bv[n2];
+  for (int j = 0; j < H0; ++j) {
+    const int t = threadIdx.x + j * NT;
+    if (t < P::T_Y_SPEC) {
+      const int kz = t % M, k1 = t / M;
+#pragma unroll
+      for (int n2 = 0; n2 < BY; ++n2) E[(n2 * AY + k1) * EY + kz] = h0[j][n2];
+    }
   }
   __syncthreads();
   // y, second half: task (kz, n2) -> rows y = BY n1 + n2

@@ -119,11 +119,11 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan) {
 }
 
 void fused_plane_fwd_rho(const FusedPlan& f, const EvalParams& p, const double* rho, const double* mean,
-                         fft::cpx* prho, const FftTables& T, cudaStream_t st) {
+                         fft::cpx* prho, int* err, const FftTables& T, cudaStream_t st) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
     rk::k_rplane_fwd<NY, NZ, double>
-        <<<dim3(p.nx, p.S, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(p, rho, p.S, mean, prho, T);
+        <<<dim3(p.nx, p.S, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(p, rho, p.S, mean, prho, err, T);
   });
   CDFT_CUDA(cudaGetLastError());
 }
@@ -147,25 +147,25 @@ void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho
   CDFT_CUDA(cudaGetLastError());
 }
 
-void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q, float* chan_r, const FftTables& T,
-                     cudaStream_t st) {
+void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q, float* chan_r, int* err,
+                     const FftTables& T, cudaStream_t st) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
     with_layout(p, [&](auto mc, auto tc) {
       rk::k_rplane_inv<NY, NZ, false, decltype(mc)::value, decltype(tc)::value>
           <<<dim3(p.nx, p.n_chan, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(
-              p, q, p.n_chan, chan_r, nullptr, nullptr, MuArgs{}, FinalArgs{nullptr, 0, nullptr, nullptr}, T);
+              p, q, p.n_chan, chan_r, nullptr, nullptr, MuArgs{}, FinalArgs{nullptr, 0, nullptr, nullptr}, err, T);
     });
   });
   CDFT_CUDA(cudaGetLastError());
 }
 
-void fused_plane_fwd_deriv(const FusedPlan& f, const EvalParams& p, const float* deriv_r, fft::cpx* pd,
+void fused_plane_fwd_deriv(const FusedPlan& f, const EvalParams& p, const float* deriv_r, fft::cpx* pd, int* err,
                            const FftTables& T, cudaStream_t st) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
     rk::k_rplane_fwd<NY, NZ, float><<<dim3(p.nx, p.L.n_deriv, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(
-        p, deriv_r, p.L.n_deriv, nullptr, pd, T);
+        p, deriv_r, p.L.n_deriv, nullptr, pd, err, T);
   });
   CDFT_CUDA(cudaGetLastError());
 }
@@ -190,13 +190,14 @@ void fused_col_bwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* pd, 
 }
 
 void fused_plane_inv_epi(const FusedPlan& f, const EvalParams& p, const fft::cpx* pf, const double* dbar,
-                         double* force, const MuArgs& mu, const FinalArgs& fin, const FftTables& T, cudaStream_t st) {
+                         double* force, const MuArgs& mu, const FinalArgs& fin, int* err, const FftTables& T,
+                         cudaStream_t st) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
     with_layout(p, [&](auto mc, auto tc) {
       rk::k_rplane_inv<NY, NZ, true, decltype(mc)::value, decltype(tc)::value>
           <<<dim3(p.nx, p.S, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(p, pf, p.S, nullptr, force, dbar,
-                                                                                   mu, fin, T);
+                                                                                   mu, fin, err, T);
     });
   });
   CDFT_CUDA(cudaGetLastError());

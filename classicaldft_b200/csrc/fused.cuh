@@ -19,8 +19,10 @@ struct FusedPlan {
 // fused path serves this engine.
 bool fused_plan(const EvalParams& p, FusedPlan* plan);
 
+// err: the engine's error word, set when a bounded wait of a bulk copy
+// gives up (cdft_engine_status reports it).
 void fused_plane_fwd_rho(const FusedPlan& f, const EvalParams& p, const double* rho, const double* mean,
-                         fft::cpx* prho, const FftTables& T, cudaStream_t st);
+                         fft::cpx* prho, int* err, const FftTables& T, cudaStream_t st);
 // The column pass reads the FMT and mean-field weights from a table built
 // once per engine (after the mean-field weights).
 long long fused_weight_table_floats(const EvalParams& p);
@@ -28,13 +30,14 @@ void fused_build_weights(const EvalParams& p, const double* mf_w, float* wtab, c
 
 void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho, const float* wtab, fft::cpx* q,
                    const FftTables& T, cudaStream_t st);
-void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q, float* chan_r, const FftTables& T,
-                     cudaStream_t st);
-void fused_plane_fwd_deriv(const FusedPlan& f, const EvalParams& p, const float* deriv_r, fft::cpx* pd,
+void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q, float* chan_r, int* err,
+                     const FftTables& T, cudaStream_t st);
+void fused_plane_fwd_deriv(const FusedPlan& f, const EvalParams& p, const float* deriv_r, fft::cpx* pd, int* err,
                            const FftTables& T, cudaStream_t st);
 void fused_col_bwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* pd, const float* wtab, fft::cpx* pf,
                    const FftTables& T, cudaStream_t st);
 void fused_plane_inv_epi(const FusedPlan& f, const EvalParams& p, const fft::cpx* pf, const double* dbar,
-                         double* force, const MuArgs& mu, const FinalArgs& fin, const FftTables& T, cudaStream_t st);
+                         double* force, const MuArgs& mu, const FinalArgs& fin, int* err, const FftTables& T,
+                         cudaStream_t st);
 
 }  // namespace cdft
