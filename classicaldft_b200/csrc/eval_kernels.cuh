@@ -693,12 +693,14 @@ __global__ void __launch_bounds__(256) k_pointwise(EvalParams p, const RT* __res
 
 // ---- TMA-staged variant (N % 4 == 0) -----------------------------------
 //
-// Each CTA walks tiles of 256 points.  One elected thread streams every input
-// segment of a tile (channel values, rho, V_ext) from HBM into a 3-stage
-// shared-memory ring with cp.async.bulk (TMA bulk copies, no multicast),
-// signalled by an mbarrier with transaction counts; all 256 threads then read
-// their point from shared memory.  The FP64 work of a tile overlaps the
-// loads of the next two, independent of the register budget.
+// Each CTA walks tiles of 256 points.  Every input segment of a tile
+// (channel values, rho, V_ext) streams from HBM into a 3-stage shared-memory
+// ring with cp.async.bulk (TMA bulk copies, no multicast), signalled by an
+// mbarrier with transaction counts; each thread then reads its point from
+// shared memory.  There is no block-wide barrier per tile: each warp counts
+// itself out of a stage when it has read it, and the last warp out issues
+// the stage's next fill, so warps run ahead of one another by up to the
+// ring depth and the FP64 work of a tile overlaps the loads of the next two.
 
 __device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
   return (uint32_t)__cvta_generic_to_shared(ptr);
@@ -760,6 +762,8 @@ __global__ void __launch_bounds__(kTmaTile) k_pointwise_tma(EvalParams p, const 
   __shared__ double s_off[kMaxChannels];
   __shared__ double s_dbar[NF];
   __shared__ int s_fail;
+  __shared__ int s_out[kTmaStages];             // warps done with the stage's current fill
+  __shared__ long long s_issued[kTmaStages];    // last local tile issued into the stage
   const PointwiseArgs a = batch_slice(p, a_all, blockIdx.y);
   chan += (long long)blockIdx.y * p.n_chan * p.N;
   deriv += (long long)blockIdx.y * p.L.n_deriv * p.N;
@@ -773,7 +777,11 @@ __global__ void __launch_bounds__(kTmaTile) k_pointwise_tma(EvalParams p, const 
   const long long mine = (blockIdx.x < ntiles) ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const int tid = threadIdx.x;
   if (tid == 0) {
-    for (int st = 0; st < kTmaStages; ++st) mbar_init(&bars[st], 1);
+    for (int st = 0; st < kTmaStages; ++st) {
+      mbar_init(&bars[st], 1);
+      s_out[st] = 0;
+      s_issued[st] = -1;
+    }
     s_fail = 0;
     fence_mbar_init();
   }
@@ -789,6 +797,7 @@ __global__ void __launch_bounds__(kTmaTile) k_pointwise_tma(EvalParams p, const 
     const uint32_t cb = (uint32_t)(cnt * sizeof(RT));
     const uint32_t db = (uint32_t)(cnt * 8);
     unsigned char* base = stage_ptr(st);
+    s_issued[st] = i;
     mbar_arrive_expect_tx(&bars[st], cb * n_in + db * S * (has_v ? 2 : 1));
     for (int q = 0; q < n_in; ++q)
       bulk_copy_g2s(base + (size_t)q * kTmaTile * sizeof(RT), chan + q * N + start, cb, &bars[st]);
@@ -805,13 +814,17 @@ __global__ void __launch_bounds__(kTmaTile) k_pointwise_tma(EvalParams p, const 
   double acc[NT];
 #pragma unroll
   for (int t = 0; t < NT; ++t) acc[t] = 0.0;
-  long long done = 0;
+  constexpr int kWarps = kTmaTile / 32;
+  const int lane = tid & 31;
+  volatile int* fail = &s_fail;
   for (long long i = 0; i < mine; ++i) {
     const int st = (int)(i % kTmaStages);
     const uint32_t par = (uint32_t)((i / kTmaStages) & 1);
-    if (!mbar_wait_bounded(&bars[st], par, kWaitLimit)) atomicExch(&s_fail, 1);
-    __syncthreads();
-    if (s_fail) break;
+    if (*fail) break;
+    if (!mbar_wait_bounded(&bars[st], par, kWaitLimit)) {
+      *fail = 1;
+      break;
+    }
     const long long tile = blockIdx.x + i * gridDim.x;
     const long long idx = tile * kTmaTile + tid;
     if (idx < N) {
@@ -830,19 +843,27 @@ __global__ void __launch_bounds__(kTmaTile) k_pointwise_tma(EvalParams p, const 
       }
       point_body<MODEL, MULTI, RT, NPRE>(p, a, cur, n_mf_pre, rs, vs, idx, chan, deriv, s_off, s_dbar, acc);
     }
-    __syncthreads();  // every thread is done with stage st
-    done = i + 1;
-    if (tid == 0 && i + kTmaStages < mine) {
-      fence_proxy_async();
-      issue(i + kTmaStages);
+    // this warp is done reading stage st; the last warp out refills it
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence_block();
+      if (atomicAdd(&s_out[st], 1) == kWarps - 1) {
+        s_out[st] = 0;
+        if (i + kTmaStages < mine) {
+          fence_proxy_async();
+          issue(i + kTmaStages);
+        }
+      }
     }
   }
+  __syncthreads();
   if (s_fail) {
     // drain the copies still in flight (bounded) before the CTA exits
     if (tid == 0) {
       *err = 1;
-      for (long long i = done; i < mine && i < done + kTmaStages; ++i)
-        mbar_wait_bounded(&bars[i % kTmaStages], (uint32_t)((i / kTmaStages) & 1), kWaitLimit);
+      for (int st = 0; st < kTmaStages; ++st)
+        if (s_issued[st] >= 0)
+          mbar_wait_bounded(&bars[st], (uint32_t)((s_issued[st] / kTmaStages) & 1), kWaitLimit);
     }
     __syncthreads();
   }
