@@ -764,7 +764,8 @@ struct RCol1 {
   static constexpr int TILE = NX * TQ;
 };
 
-__host__ __device__ inline size_t rcol1_smem(int nx, int tq) { return sizeof(cpx) * ((size_t)nx + 2ull * nx * tq); }
+// tx, two exchange buffers and (backward) two load buffers of NX x TQ.
+__host__ __device__ inline size_t rcol1_smem(int nx, int tq) { return sizeof(cpx) * ((size_t)nx + 4ull * nx * tq); }
 
 // The |k| factors of a task's elements (zero for columns past the plane).
 template <int BX>
@@ -790,36 +791,52 @@ __device__ __forceinline__ RTab<RCol1<NX, TQ>::BX> rk_task_table(const float* __
   return t;
 }
 
-// Weight of FMT channel C (single species) at element k2 of a task; odd:
-// the channel is i w rho.
-template <bool TENSOR, int C, int BX>
-__device__ __forceinline__ float rk_weight1(const RTab<BX>& t, int k2, const RKv& v, bool& odd) {
-  using L = Lay<false, TENSOR>;
-  odd = false;
-  if constexpr (C == L::ETA) {
-    return t.w3[k2];
-  } else if constexpr (C == L::N2) {
-    return t.w2[k2];
-  } else if constexpr (C >= L::V1 && C < L::V1 + 3) {
-    odd = true;
-    constexpr int A = C - L::V1;
-    return t.fv[k2] * (v.k[A] * v.o[A]);
-  } else {
-    constexpr int TT = C - L::T;
-    constexpr int I = tchan_i(TT), J = tchan_j(TT);
-    if constexpr (I == J) {
-      return t.a[k2] * (v.k[I] * v.k[J]) + t.b[k2];
-    } else {
-      const float m = (I + J == 1) ? v.cxy : ((I + J == 2) ? v.cxz : v.cyz);
-      return t.a[k2] * (v.k[I] * v.k[J] * m);
-    }
-  }
-}
-
 template <int NX>
 __device__ __forceinline__ RKv rk_task_element(const EvalParams& p, int kx, float dkx, const RColumn& col) {
   const bool xnyq = (p.nx % 2 == 0) && kx == p.nx / 2;
   return rk_element(dkx * (float)(kx <= p.nx / 2 ? kx : kx - p.nx), xnyq, col.ky, col.ynyq, col.kz, col.proj);
+}
+
+// Weights of FMT channel c (one species; c uniform across the block) at the
+// BX elements of a task, as rk_weight1; returns `odd` (the channel is
+// i w rho).  One switch per channel and task keeps a single copy of the
+// transform code in the channel loop.
+template <bool TENSOR, int NX, int TQ>
+__device__ __forceinline__ bool rk_task_weights(int c, const RTab<RCol1<NX, TQ>::BX>& t, const EvalParams& p,
+                                                int k1, float dkx, const RColumn& col,
+                                                float (&w)[RCol1<NX, TQ>::BX]) {
+  using L = Lay<false, TENSOR>;
+  constexpr int AX = RCol1<NX, TQ>::AX, BX = RCol1<NX, TQ>::BX;
+  if (c == L::ETA) {
+#pragma unroll
+    for (int k2 = 0; k2 < BX; ++k2) w[k2] = t.w3[k2];
+    return false;
+  }
+  if (c == L::N2) {
+#pragma unroll
+    for (int k2 = 0; k2 < BX; ++k2) w[k2] = t.w2[k2];
+    return false;
+  }
+  if (c < L::V1 + 3) {
+    const int a = c - L::V1;
+#pragma unroll
+    for (int k2 = 0; k2 < BX; ++k2) {
+      const RKv v = rk_task_element<NX>(p, k1 + AX * k2, dkx, col);
+      const float ka = a == 0 ? v.k[0] * v.o[0] : (a == 1 ? v.k[1] * v.o[1] : v.k[2] * v.o[2]);
+      w[k2] = t.fv[k2] * ka;
+    }
+    return true;
+  }
+  const int tt = c - L::T, i = tchan_i(tt), j = tchan_j(tt);
+#pragma unroll
+  for (int k2 = 0; k2 < BX; ++k2) {
+    const RKv v = rk_task_element<NX>(p, k1 + AX * k2, dkx, col);
+    const float ki = i == 0 ? v.k[0] : v.k[1];
+    const float kj = j == 0 ? v.k[0] : (j == 1 ? v.k[1] : v.k[2]);
+    const float m = (i == j) ? 1.0f : ((i + j == 1) ? v.cxy : ((i + j == 2) ? v.cxz : v.cyz));
+    w[k2] = t.a[k2] * (ki * kj * m) + ((i == j) ? t.b[k2] : 0.0f);
+  }
+  return false;
 }
 
 // Inverse x transform of the task values bv (this thread's spectrum task)
@@ -896,19 +913,17 @@ __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
   col1_forward<NX, TQ>(prho + (long long)b * Nk, plane, q0, q, k1, Eb, tx, r);
   int buf = 1;
   cpx* out = q_out + (long long)b * NCH * Nk;
-  static_for<0, L::NFMT>([&](auto cc) {
-    constexpr int CH = decltype(cc)::value;
+#pragma unroll 1
+  for (int ch = 0; ch < L::NFMT; ++ch) {
+    float w[BX];
+    const bool odd = rk_task_weights<TENSOR, NX, TQ>(ch, tab, p, k1, dkx, col, w);
     cpx bv[BX];
 #pragma unroll
-    for (int k2 = 0; k2 < BX; ++k2) {
-      const RKv v = rk_task_element<NX>(p, k1 + AX * k2, dkx, col);
-      bool odd;
-      const float w = rk_weight1<TENSOR, CH, BX>(tab, k2, v, odd);
-      bv[k2] = odd ? cpx{-w * r[k2].y, w * r[k2].x} : cpx{w * r[k2].x, w * r[k2].y};
-    }
-    col1_inverse<NX, TQ>(bv, q, k1, Eb + buf * TILE, tx, out + (long long)CH * Nk, plane, q0);
+    for (int k2 = 0; k2 < BX; ++k2)
+      bv[k2] = odd ? cpx{-w[k2] * r[k2].y, w[k2] * r[k2].x} : cpx{w[k2] * r[k2].x, w[k2] * r[k2].y};
+    col1_inverse<NX, TQ>(bv, q, k1, Eb + buf * TILE, tx, out + (long long)ch * Nk, plane, q0);
     buf ^= 1;
-  });
+  }
   // mean-field channels: w(k) rho_k with the real weight from the table
   for (int m = 0; m < p.M; ++m) {
     cpx bv[BX];
@@ -923,6 +938,18 @@ __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
   }
 }
 
+// Per-thread asynchronous 8-byte copies global -> shared (cp.async, the
+// LSU's path; no TMA), committed and waited for in groups.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Backward: each natural-order task's column values of the next derivative
+// channel stream into a second load buffer (cp.async; every thread reads
+// back only what it copied itself) while the current channel is
+// transformed.
 template <int NX, int TQ, bool TENSOR>
 __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
     k_rcol_bwd1(EvalParams p, const cpx* __restrict__ pd, const float* __restrict__ wtab, cpx* __restrict__ pf,
@@ -933,11 +960,30 @@ __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cpx* tx = reinterpret_cast<cpx*>(smem_raw);
   cpx* Eb = tx + NX;
+  cpx* Lb = Eb + 2 * TILE;
   const long long plane = (long long)p.ny * p.nzh, Nk = p.Nk;
   const int b = blockIdx.y;
   const long long q0 = (long long)blockIdx.x * TQ;
-  const int q = threadIdx.x % TQ, k1 = threadIdx.x / TQ;
-  for (int i = threadIdx.x; i < NX; i += NT) tx[i] = T.tx[i];
+  const int t = threadIdx.x;
+  const int q = t % TQ, k1 = t / TQ;
+  const bool nat = t < TQ * BX;
+  const int qn = t % TQ, n2 = t / TQ;
+  const bool ok = q0 + qn < plane;
+  const cpx* src = pd + (long long)b * NF * Nk;
+  auto prefetch = [&](int ch) {
+    if (nat && ok) {
+      cpx* dst = Lb + (ch & 1) * TILE;
+      const cpx* s0 = src + (long long)ch * Nk + q0 + qn;
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) {
+        const int x = BX * n1 + n2;
+        cp_async8(dst + x * TQ + qn, s0 + (long long)x * plane);
+      }
+    }
+    cp_async_commit();
+  };
+  prefetch(0);
+  for (int i = t; i < NX; i += NT) tx[i] = T.tx[i];
   const RColumn col = rk_column(p, q0 + q, (float)p.dky, (float)p.dkz);
   const RTab<BX> tab = rk_task_table<NX, TQ>(wtab, Nk, plane, q0 + q, k1, col.valid);
   const float dkx = (float)p.dkx;
@@ -946,22 +992,38 @@ __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
 #pragma unroll
   for (int k2 = 0; k2 < BX; ++k2) f[k2] = cpx{0.0f, 0.0f};
   int buf = 0;
-  const cpx* src = pd + (long long)b * NF * Nk;
-  static_for<0, NF>([&](auto cc) {
-    constexpr int CH = decltype(cc)::value;
-    cpx d[BX];
-    col1_forward<NX, TQ>(src + (long long)CH * Nk, plane, q0, q, k1, Eb + buf * TILE, tx, d);
+#pragma unroll 1
+  for (int ch = 0; ch < NF; ++ch) {
+    if (ch + 1 < NF)
+      prefetch(ch + 1);
+    else
+      cp_async_commit();  // an empty group keeps the wait count uniform
+    cpx* E = Eb + buf * TILE;
+    if (nat) {
+      cp_async_wait_one();  // channel ch has landed
+      const cpx* Lt = Lb + (ch & 1) * TILE;
+      cpx a[AX];
 #pragma unroll
-    for (int k2 = 0; k2 < BX; ++k2) {
-      const RKv v = rk_task_element<NX>(p, k1 + AX * k2, dkx, col);
-      bool odd;
-      const float w = rk_weight1<TENSOR, CH, BX>(tab, k2, v, odd);
-      // conj(i w) D = -i w D for an odd channel
-      f[k2] = odd ? cpx{f[k2].x + w * d[k2].y, f[k2].y - w * d[k2].x}
-                  : cpx{f[k2].x + w * d[k2].x, f[k2].y + w * d[k2].y};
+      for (int n1 = 0; n1 < AX; ++n1) a[n1] = ok ? Lt[(BX * n1 + n2) * TQ + qn] : cpx{0.0f, 0.0f};
+      fft::nat_in<NX, false>(a, n2, tx);
+#pragma unroll
+      for (int kk = 0; kk < AX; ++kk) E[(n2 * AX + kk) * TQ + qn] = a[kk];
     }
+    __syncthreads();
+    cpx d[BX];
+#pragma unroll
+    for (int j = 0; j < BX; ++j) d[j] = E[(j * AX + k1) * TQ + q];
+    fft::nat_out<NX, false>(d);
+    float w[BX];
+    const bool odd = rk_task_weights<TENSOR, NX, TQ>(ch, tab, p, k1, dkx, col, w);
+    // conj(i w) D = -i w D for an odd channel
+#pragma unroll
+    for (int k2 = 0; k2 < BX; ++k2)
+      f[k2] = odd ? cpx{f[k2].x + w[k2] * d[k2].y, f[k2].y - w[k2] * d[k2].x}
+                  : cpx{f[k2].x + w[k2] * d[k2].x, f[k2].y + w[k2] * d[k2].y};
     buf ^= 1;
-  });
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
   col1_inverse<NX, TQ>(f, q, k1, Eb + buf * TILE, tx, pf + (long long)b * Nk, plane, q0);
 }
 
