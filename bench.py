@@ -72,9 +72,9 @@ def stage_bytes(info, S=1, M=1, has_vext=False, fused=False):
     pointwise = C * Br + S * Bio * (2 if has_vext else 1) + D * Br + S * Bio
     if fused:
         return {
-            "species_mean": S * Bio,
-            "plane_fwd_rho": S * Bio + S * Bc,
-            "col_fwd": S * Bc + M * 8 * Nk + C * Bc,
+            "-0": 0,
+            "plane_fwd_rho": S * Bio + S * Bc,  # the plane means re-read rho from L2
+            "col_fwd": S * Bc + M * 4 * Nk + C * Bc,  # (+ MF weight, FP32 real)
             "plane_inv_channels": C * (Bc + Br),
             "pointwise": pointwise,
             "plane_fwd_derivatives": D * (Br + Bc),

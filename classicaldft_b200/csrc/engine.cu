@@ -257,7 +257,7 @@ Engine::~Engine() {
   for (void* q : {rho_k_, chan_k_, chan_r_, deriv_r_, deriv_k_, force_k_, hs_r_, rho_lo_, (void*)mf_w_,
                   (void*)mean_, (void*)dbar_, (void*)err_, (void*)sync_, tan_chan_, (void*)tan_mean_, (void*)tan_dbar_,
                   (void*)tan_in_,
-                  (void*)partials_, fft_work_, tw_, (void*)wtab_, (void*)h_rho_, (void*)h_vext_, (void*)h_force_, (void*)h_scalars_})
+                  (void*)partials_, fft_work_, tw_, (void*)wtab_, (void*)pmean_, (void*)h_rho_, (void*)h_vext_, (void*)h_force_, (void*)h_scalars_})
     if (q) cudaFree(q);
   if (stream_) cudaStreamDestroy(stream_);
   for (cudaEvent_t e : stage_ev_)
@@ -327,6 +327,7 @@ void Engine::setup_fused() {
   const fft::cpx* t = static_cast<const fft::cpx*>(tw_);
   tables_ = FftTables{t, t + p.nx, t + p.nx + p.ny, t + p.nx + p.ny + p.nz / 2};
   CDFT_CUDA(cudaMalloc(&wtab_, sizeof(float) * fused_weight_table_floats(p)));
+  CDFT_CUDA(cudaMalloc(&pmean_, sizeof(double) * (size_t)p.batch * p.S * p.nx));
   fused_build_weights(p, mf_w_, wtab_, nullptr);
   CDFT_CUDA(cudaDeviceSynchronize());
   fusable_ = true;
@@ -492,18 +493,18 @@ void Engine::backward_stage(R* deriv, const double* dbar, double* out, const MuA
   mark(9, stream);
 }
 
-// Fused transform path, stages 1-3: species means, plane pass of rho, column
-// pass with the channel products, inverse plane pass of every channel.
+// Fused transform path, stages 1-3: plane pass of rho (split around the
+// plane means), column pass (species means, channel products), inverse
+// plane pass of every channel.
 void Engine::fused_forward(const double* rho, cudaStream_t stream) {
   const EvalParams& p = p_;
   const dim3 gs(grid_stream_, p.batch);
-  k_species_mean<<<dim3(grid_mean_, p.batch), 256, 0, stream>>>(rho, p.N, p.S, partials_, sync_, mean_);
-  mark(1, stream);
+  mark(1, stream);  // the species means come with the plane and column passes
   fft::cpx* prho = static_cast<fft::cpx*>(rho_k_);
   fft::cpx* q = static_cast<fft::cpx*>(chan_k_);
-  fused_plane_fwd_rho(plan_, p, rho, mean_, prho, err_, tables_, stream);
+  fused_plane_fwd_rho(plan_, p, rho, pmean_, prho, err_, tables_, stream);
   mark(2, stream);
-  fused_col_fwd(plan_, p, prho, wtab_, q, tables_, stream);
+  fused_col_fwd(plan_, p, prho, pmean_, mean_, wtab_, q, tables_, stream);
   mark(3, stream);
   fused_plane_inv(plan_, p, q, static_cast<float*>(chan_r_), err_, tables_, stream);
   mark(4, stream);

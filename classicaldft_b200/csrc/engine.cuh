@@ -163,7 +163,8 @@ class Engine {
   bool fusable_ = false, fused_ = false;
   FusedPlan plan_{};
   void* tw_ = nullptr;
-  float* wtab_ = nullptr;  // column-pass weight table ([1 + 5 S][Nk] floats)
+  float* wtab_ = nullptr;    // column-pass weight table ([5 S + M][Nk] floats)
+  double* pmean_ = nullptr;  // B * S * nx plane means of rho (fused path)
   FftTables tables_{};
 
   cufftHandle plan_rho_ = 0, plan_chan_ = 0, plan_deriv_ = 0, plan_force_ = 0;

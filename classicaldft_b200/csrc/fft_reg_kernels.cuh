@@ -58,6 +58,9 @@ struct RPlane {
   static constexpr int EZ = pad8(BZ * EZS);  // z exchange row stride
   static constexpr int BUF = cmax(NY * EY, cmax(NY * ER, NY * EZ));
   static constexpr int NT = NY * M >= 8192 ? 512 : (NY * M >= 2048 ? 256 : 128);
+  // the passes with one sequence per plane (rho in, force out) launch one
+  // CTA per x plane only: twice the threads per CTA
+  static constexpr int NT_WIDE = NT * 2;
   static constexpr size_t kSmem = sizeof(cpx) * ((size_t)BUF + NY + M + NZ);
   // tasks of each phase and the tasks a thread holds across a barrier
   static constexpr int T_Y_SPEC = M * AY, T_Y_NAT = M * BY, T_Z_SPEC = NY * AZ, T_Z_NAT = NY * BZ;
@@ -94,15 +97,18 @@ __device__ __forceinline__ bool bulk_load(void* dst, const void* src, uint32_t b
   return true;
 }
 
-// Forward plane pass of one real NY x NZ plane (IN = double: rho minus the
-// species mean, the mixed-precision split; IN = float: a derivative
-// channel) into its half spectrum (NY x (NZ/2 + 1), natural order).
-template <int NY, int NZ, typename IN>
-__global__ void __launch_bounds__(RPlane<NY, NZ>::NT)
-    k_rplane_fwd(EvalParams p, const IN* __restrict__ in, int nseq, const double* __restrict__ mean,
+// Forward plane pass of one real NY x NZ plane into its half spectrum
+// (NY x (NZ/2 + 1), natural order).  IN = float: a derivative channel.
+// IN = double: rho, split for mixed precision around the plane's own mean
+// m_x (FP64, written to pmean[(b S + s) nx + ix]): the plane transformed is
+// rho - m_x in FP32, and the column pass restores the plane means' profile
+// around the species mean (rk_dc_column).
+template <int NY, int NZ, typename IN, int NT = RPlane<NY, NZ>::NT>
+__global__ void __launch_bounds__(NT)
+    k_rplane_fwd(EvalParams p, const IN* __restrict__ in, int nseq, double* __restrict__ pmean,
                  cpx* __restrict__ out, int* err, FftTables T) {
   using P = RPlane<NY, NZ>;
-  constexpr int M = P::M, LD = P::LD, AY = P::AY, BY = P::BY, AZ = P::AZ, BZ = P::BZ, NT = P::NT;
+  constexpr int M = P::M, LD = P::LD, AY = P::AY, BY = P::BY, AZ = P::AZ, BZ = P::BZ;
   constexpr int EY = P::EY, ER = P::ER, EZS = P::EZS, EZ = P::EZ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cpx* E = reinterpret_cast<cpx*>(smem_raw);
@@ -114,26 +120,46 @@ __global__ void __launch_bounds__(RPlane<NY, NZ>::NT)
   __syncthreads();
   const IN* src = in + ((long long)b * nseq + sq) * p.N + (long long)ix * NY * NZ;
   if constexpr (sizeof(IN) == 8) {
-    // rho (FP64): task (y, n2) takes the pairs n = BZ n1 + n2 of row y
-    // straight from global memory, minus the species mean
-    const double c = mean ? mean[b * kMaxSpecies + sq] : 0.0;
-    for (int t = threadIdx.x; t < P::T_Z_NAT; t += NT) {
-      const int n2 = t % BZ, y = t / BZ;
-      cpx a[AZ];
+    // rho (FP64): one read of the plane into registers, its mean (a
+    // fixed-order block sum, recorded for the column pass), rho - mean in
+    // FP32 into shared memory as the real plane (pairs E[y * M + n])
+    constexpr int PER = NY * NZ / NT;
+    static_assert(PER * NT == NY * NZ, "plane samples per thread");
+    double v[PER];
+    double sum = 0.0;
 #pragma unroll
-      for (int n1 = 0; n1 < AZ; ++n1) {
-        const IN* q = src + (long long)y * NZ + 2 * (BZ * n1 + n2);  // the caller's buffer: scalar loads
-        a[n1] = {(float)(q[0] - c), (float)(q[1] - c)};
-      }
-      fft::nat_in<M, false>(a, n2, tz);
-#pragma unroll
-      for (int k1 = 0; k1 < AZ; ++k1) E[y * EZ + n2 * EZS + k1] = a[k1];
+    for (int j = 0; j < PER; ++j) {
+      v[j] = src[threadIdx.x + j * NT];  // the caller's buffer: scalar loads
+      sum += v[j];
     }
+    __shared__ double s_warp[NT / 32];
+    __shared__ double s_mean;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+    if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = 0.0;
+      for (int w = 0; w < NT / 32; ++w) m += s_warp[w];
+      m /= (double)(NY * NZ);
+      s_mean = m;
+      pmean[((long long)b * nseq + sq) * p.nx + ix] = m;
+    }
+    __syncthreads();
+    const double c = s_mean;
+    float* Ef = reinterpret_cast<float*>(E);
+#pragma unroll
+    for (int j = 0; j < PER; ++j) Ef[threadIdx.x + j * NT] = (float)(v[j] - c);
+    __syncthreads();
   } else {
     // a derivative channel (FP32, the engine's buffer): the plane arrives in
-    // shared memory by one bulk copy; its pairs are E[y * M + n]
+    // shared memory by one bulk copy
     __shared__ __align__(8) uint64_t bar;
     if (!bulk_load(E, src, sizeof(float) * NY * NZ, &bar, err)) return;
+  }
+  {
+    // z, first half from the real plane in shared memory: task (y, n2)
+    // takes the pairs E[y * M + BZ n1 + n2]
     constexpr int H0 = cdiv(P::T_Z_NAT, NT);
     cpx h0[H0][AZ];
 #pragma unroll
@@ -252,14 +278,14 @@ __global__ void __launch_bounds__(RPlane<NY, NZ>::NT)
 // (force_s += hs dV - mu_s dV + the DC split term); the CTA of plane 0,
 // species 0 of each problem also reduces the pointwise partials into the
 // scalars (the pointwise kernel completed before this launch).
-template <int NY, int NZ, bool EPI, bool MULTI, bool TENSOR>
-__global__ void __launch_bounds__(RPlane<NY, NZ>::NT)
+template <int NY, int NZ, bool EPI, bool MULTI, bool TENSOR, int NT = RPlane<NY, NZ>::NT>
+__global__ void __launch_bounds__(NT)
     k_rplane_inv(EvalParams p, const cpx* __restrict__ in, int nseq, float* __restrict__ out_f,
                  double* __restrict__ force, const double* __restrict__ dbar, const __grid_constant__ MuArgs mu,
                  FinalArgs fin, int* err, FftTables T) {
   using P = RPlane<NY, NZ>;
   using L = Lay<MULTI, TENSOR>;
-  constexpr int M = P::M, LD = P::LD, AY = P::AY, BY = P::BY, AZ = P::AZ, BZ = P::BZ, NT = P::NT;
+  constexpr int M = P::M, LD = P::LD, AY = P::AY, BY = P::BY, AZ = P::AZ, BZ = P::BZ;
   constexpr int EY = P::EY, ER = P::ER, EZS = P::EZS, EZ = P::EZ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cpx* E = reinterpret_cast<cpx*>(smem_raw);
@@ -519,10 +545,12 @@ __device__ __forceinline__ RColumn rk_column(const EvalParams& p, long long q, f
 }
 
 // Forward transform along x of one array's column tile: the natural-order
-// spectrum of tile column q, row kx, goes to spec[kx * TQ + q].
+// spectrum of tile column q, row kx, goes to spec[kx * TQ + q].  dc (or
+// null): real parts added to in-plane column 0 before the transform (the
+// plane-mean correction of the split rho, see rk_dc_column).
 template <int NX, int TQ>
 __device__ __forceinline__ void col_forward(const cpx* __restrict__ src, long long plane, long long q0, cpx* E,
-                                            cpx* spec, const cpx* tx) {
+                                            cpx* spec, const cpx* tx, const float* dc = nullptr) {
   using C = RCol<NX>;
   constexpr int AX = C::AX, BX = C::BX, NT = C::NT;
 #pragma unroll 1
@@ -532,6 +560,10 @@ __device__ __forceinline__ void col_forward(const cpx* __restrict__ src, long lo
     cpx a[AX];
 #pragma unroll
     for (int n1 = 0; n1 < AX; ++n1) a[n1] = ok ? src[(BX * n1 + n2) * plane + q0 + q] : cpx{0.0f, 0.0f};
+    if (dc && q0 + q == 0) {
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) a[n1].x += dc[BX * n1 + n2];
+    }
     fft::nat_in<NX, false>(a, n2, tx);
 #pragma unroll
     for (int k1 = 0; k1 < AX; ++k1) E[(n2 * AX + k1) * TQ + q] = a[k1];
@@ -582,14 +614,44 @@ __device__ __forceinline__ void col_inverse(V&& values, cpx* E, const cpx* tx, c
   }
 }
 
+// The species means and the plane-mean correction of the split rho.  The
+// plane pass transformed rho - m_x (m_x: plane x's mean, in pmean); the
+// channels are built on rho - m with m the species mean (the FP64 offset
+// the pointwise kernel adds back), so in-plane column (ky, kz) = (0, 0)
+// gets (m_x - m) NY NZ added before its x transform: small, the plane
+// means' own fluctuation.  Run by the CTA that holds column 0 (uniformly);
+// writes m to mean_out for the later stages.  dc: S x NX floats in shared
+// memory.
+template <int NX>
+__device__ __forceinline__ void rk_dc_column(const EvalParams& p, const double* __restrict__ pmean, int b,
+                                             double* __restrict__ mean_out, float* dc) {
+  __shared__ double s_m[kMaxSpecies];
+  const int S = p.S;
+  if (threadIdx.x < S) {
+    const double* pm = pmean + ((long long)b * S + threadIdx.x) * NX;
+    double m = 0.0;
+    for (int x = 0; x < NX; ++x) m += pm[x];
+    m /= (double)NX;
+    s_m[threadIdx.x] = m;
+    mean_out[b * kMaxSpecies + threadIdx.x] = m;
+  }
+  __syncthreads();
+  const double nyz = (double)p.ny * (double)p.nz;
+  for (int i = threadIdx.x; i < S * NX; i += blockDim.x) {
+    const int s = i / NX, x = i % NX;
+    dc[s * NX + x] = (float)((pmean[((long long)b * S + s) * NX + x] - s_m[s]) * nyz);
+  }
+  __syncthreads();
+}
+
 // Column pass of the forward stage: rho_k along x for every species, then
 // for every channel its k-space product and the inverse x transform.  Tile:
 // in-plane indices q0 .. q0 + TQ - 1 of all NX planes.  The two exchange
 // buffers alternate, so one barrier per transform suffices.
 template <int NX, int TQ, bool MULTI, bool TENSOR>
 __global__ void __launch_bounds__(256, 2)
-    k_rcol_fwd(EvalParams p, const cpx* __restrict__ prho, const float* __restrict__ wtab, cpx* __restrict__ q_out,
-               FftTables T) {
+    k_rcol_fwd(EvalParams p, const cpx* __restrict__ prho, const double* __restrict__ pmean,
+               double* __restrict__ mean_out, const float* __restrict__ wtab, cpx* __restrict__ q_out, FftTables T) {
   using L = Lay<MULTI, TENSOR>;
   constexpr int NT = RCol<NX>::NT, TILE = NX * TQ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -600,11 +662,14 @@ __global__ void __launch_bounds__(256, 2)
   const long long plane = (long long)p.ny * p.nzh, Nk = p.Nk;
   const int b = blockIdx.y;
   const long long q0 = (long long)blockIdx.x * TQ;
+  __shared__ float s_dc[kMaxSpecies * NX];
   for (int i = threadIdx.x; i < NX; i += NT) tx[i] = T.tx[i];
+  if (blockIdx.x == 0) rk_dc_column<NX>(p, pmean, b, mean_out, s_dc);
   __syncthreads();
   int buf = 0;
   for (int s = 0; s < S; ++s) {
-    col_forward<NX, TQ>(prho + ((long long)b * S + s) * Nk, plane, q0, Eb + buf * TILE, R + (size_t)s * TILE, tx);
+    col_forward<NX, TQ>(prho + ((long long)b * S + s) * Nk, plane, q0, Eb + buf * TILE, R + (size_t)s * TILE, tx,
+                        blockIdx.x == 0 ? s_dc + s * NX : nullptr);
     buf ^= 1;
   }
   const float dkx = (float)p.dkx, dky = (float)p.dky, dkz = (float)p.dkz;
@@ -869,7 +934,8 @@ __device__ __forceinline__ void col1_inverse(cpx (&bv)[RCol1<NX, TQ>::BX], int q
 // values (natural-order spectrum elements k1 + AX k2 of column q).
 template <int NX, int TQ>
 __device__ __forceinline__ void col1_forward(const cpx* __restrict__ src, long long plane, long long q0, int q, int k1,
-                                             cpx* E, const cpx* tx, cpx (&out)[RCol1<NX, TQ>::BX]) {
+                                             cpx* E, const cpx* tx, cpx (&out)[RCol1<NX, TQ>::BX],
+                                             const float* dc = nullptr) {
   using C = RCol1<NX, TQ>;
   constexpr int AX = C::AX, BX = C::BX;
   const int t = threadIdx.x;
@@ -879,6 +945,10 @@ __device__ __forceinline__ void col1_forward(const cpx* __restrict__ src, long l
     cpx a[AX];
 #pragma unroll
     for (int n1 = 0; n1 < AX; ++n1) a[n1] = ok ? src[(BX * n1 + n2) * plane + q0 + qn] : cpx{0.0f, 0.0f};
+    if (dc && q0 + qn == 0) {
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) a[n1].x += dc[BX * n1 + n2];
+    }
     fft::nat_in<NX, false>(a, n2, tx);
 #pragma unroll
     for (int kk = 0; kk < AX; ++kk) E[(n2 * AX + kk) * TQ + qn] = a[kk];
@@ -891,8 +961,8 @@ __device__ __forceinline__ void col1_forward(const cpx* __restrict__ src, long l
 
 template <int NX, int TQ, bool TENSOR>
 __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
-    k_rcol_fwd1(EvalParams p, const cpx* __restrict__ prho, const float* __restrict__ wtab, cpx* __restrict__ q_out,
-                FftTables T) {
+    k_rcol_fwd1(EvalParams p, const cpx* __restrict__ prho, const double* __restrict__ pmean,
+                double* __restrict__ mean_out, const float* __restrict__ wtab, cpx* __restrict__ q_out, FftTables T) {
   using L = Lay<false, TENSOR>;
   using C = RCol1<NX, TQ>;
   constexpr int AX = C::AX, BX = C::BX, NT = C::NT, TILE = C::TILE;
@@ -908,9 +978,11 @@ __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
   const RColumn col = rk_column(p, q0 + q, (float)p.dky, (float)p.dkz);
   const RTab<BX> tab = rk_task_table<NX, TQ>(wtab, Nk, plane, q0 + q, k1, col.valid);
   const float dkx = (float)p.dkx;
+  __shared__ float s_dc[NX];
+  if (blockIdx.x == 0) rk_dc_column<NX>(p, pmean, b, mean_out, s_dc);
   __syncthreads();
   cpx r[BX];
-  col1_forward<NX, TQ>(prho + (long long)b * Nk, plane, q0, q, k1, Eb, tx, r);
+  col1_forward<NX, TQ>(prho + (long long)b * Nk, plane, q0, q, k1, Eb, tx, r, blockIdx.x == 0 ? s_dc : nullptr);
   int buf = 1;
   cpx* out = q_out + (long long)b * NCH * Nk;
 #pragma unroll 1

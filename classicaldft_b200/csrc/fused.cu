@@ -90,12 +90,12 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan) {
   f.col_tiles = (int)(((long long)p.ny * p.nzh + f.tq - 1) / f.tq);
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
-    allow_smem(rk::k_rplane_fwd<NY, NZ, double>, f.plane_smem);
+    allow_smem(rk::k_rplane_fwd<NY, NZ, double, rk::RPlane<NY, NZ>::NT_WIDE>, f.plane_smem);
     allow_smem(rk::k_rplane_fwd<NY, NZ, float>, f.plane_smem);
     with_layout(p, [&](auto mc, auto tc) {
       constexpr bool MU = decltype(mc)::value, TE = decltype(tc)::value;
       allow_smem(rk::k_rplane_inv<NY, NZ, false, MU, TE>, f.plane_smem);
-      allow_smem(rk::k_rplane_inv<NY, NZ, true, MU, TE>, f.plane_smem);
+      allow_smem(rk::k_rplane_inv<NY, NZ, true, MU, TE, rk::RPlane<NY, NZ>::NT_WIDE>, f.plane_smem);
     });
   });
   with_len(p.nx, [&](auto xc) {
@@ -118,18 +118,19 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan) {
   return true;
 }
 
-void fused_plane_fwd_rho(const FusedPlan& f, const EvalParams& p, const double* rho, const double* mean,
+void fused_plane_fwd_rho(const FusedPlan& f, const EvalParams& p, const double* rho, double* pmean,
                          fft::cpx* prho, int* err, const FftTables& T, cudaStream_t st) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
-    rk::k_rplane_fwd<NY, NZ, double>
-        <<<dim3(p.nx, p.S, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(p, rho, p.S, mean, prho, err, T);
+    constexpr int NT = rk::RPlane<NY, NZ>::NT_WIDE;
+    rk::k_rplane_fwd<NY, NZ, double, NT>
+        <<<dim3(p.nx, p.S, p.batch), NT, f.plane_smem, st>>>(p, rho, p.S, pmean, prho, err, T);
   });
   CDFT_CUDA(cudaGetLastError());
 }
 
-void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho, const float* wtab, fft::cpx* q,
-                   const FftTables& T, cudaStream_t st) {
+void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho, const double* pmean, double* mean,
+                   const float* wtab, fft::cpx* q, const FftTables& T, cudaStream_t st) {
   with_len(p.nx, [&](auto xc) {
     with_tq(f.tq, [&](auto qc) {
       with_layout(p, [&](auto mc, auto tc) {
@@ -137,10 +138,11 @@ void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho
         constexpr bool MU = decltype(mc)::value, TE = decltype(tc)::value;
         if constexpr (MU)
           rk::k_rcol_fwd<NX, TQ, MU, TE>
-              <<<dim3(f.col_tiles, p.batch), rk::RCol<NX>::NT, f.colf_smem, st>>>(p, prho, wtab, q, T);
+              <<<dim3(f.col_tiles, p.batch), rk::RCol<NX>::NT, f.colf_smem, st>>>(p, prho, pmean, mean, wtab, q, T);
         else
           rk::k_rcol_fwd1<NX, TQ, TE>
-              <<<dim3(f.col_tiles, p.batch), rk::RCol1<NX, TQ>::NT, f.colf_smem, st>>>(p, prho, wtab, q, T);
+              <<<dim3(f.col_tiles, p.batch), rk::RCol1<NX, TQ>::NT, f.colf_smem, st>>>(p, prho, pmean, mean, wtab,
+                                                                                          q, T);
       });
     });
   });
@@ -195,9 +197,9 @@ void fused_plane_inv_epi(const FusedPlan& f, const EvalParams& p, const fft::cpx
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
     with_layout(p, [&](auto mc, auto tc) {
-      rk::k_rplane_inv<NY, NZ, true, decltype(mc)::value, decltype(tc)::value>
-          <<<dim3(p.nx, p.S, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(p, pf, p.S, nullptr, force, dbar,
-                                                                                   mu, fin, err, T);
+      constexpr int NT = rk::RPlane<NY, NZ>::NT_WIDE;
+      rk::k_rplane_inv<NY, NZ, true, decltype(mc)::value, decltype(tc)::value, NT>
+          <<<dim3(p.nx, p.S, p.batch), NT, f.plane_smem, st>>>(p, pf, p.S, nullptr, force, dbar, mu, fin, err, T);
     });
   });
   CDFT_CUDA(cudaGetLastError());

@@ -21,15 +21,18 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan);
 
 // err: the engine's error word, set when a bounded wait of a bulk copy
 // gives up (cdft_engine_status reports it).
-void fused_plane_fwd_rho(const FusedPlan& f, const EvalParams& p, const double* rho, const double* mean,
+// The rho plane pass writes each plane's mean (pmean, B * S * nx doubles);
+// the column pass turns them into the species means (mean, B * kMaxSpecies)
+// of the mixed-precision split.
+void fused_plane_fwd_rho(const FusedPlan& f, const EvalParams& p, const double* rho, double* pmean,
                          fft::cpx* prho, int* err, const FftTables& T, cudaStream_t st);
 // The column pass reads the FMT and mean-field weights from a table built
 // once per engine (after the mean-field weights).
 long long fused_weight_table_floats(const EvalParams& p);
 void fused_build_weights(const EvalParams& p, const double* mf_w, float* wtab, cudaStream_t st);
 
-void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho, const float* wtab, fft::cpx* q,
-                   const FftTables& T, cudaStream_t st);
+void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho, const double* pmean, double* mean,
+                   const float* wtab, fft::cpx* q, const FftTables& T, cudaStream_t st);
 void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q, float* chan_r, int* err,
                      const FftTables& T, cudaStream_t st);
 void fused_plane_fwd_deriv(const FusedPlan& f, const EvalParams& p, const float* deriv_r, fft::cpx* pd, int* err,

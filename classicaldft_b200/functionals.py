@@ -306,7 +306,7 @@ class Engine:
 
     STAGES = ("split", "r2c_rho", "k_forward", "c2r_channels", "pointwise", "r2c_derivatives", "k_backward",
               "c2r_force", "epilogue", "reduce")
-    STAGES_FUSED = ("species_mean", "plane_fwd_rho", "col_fwd", "plane_inv_channels", "pointwise",
+    STAGES_FUSED = ("-0", "plane_fwd_rho", "col_fwd", "plane_inv_channels", "pointwise",
                     "plane_fwd_derivatives", "col_bwd", "plane_inv_epilogue", "-8", "-9")
 
     @property

@@ -203,7 +203,7 @@ def test_stage_timing_hook_records_every_stage_and_changes_nothing(transforms):
     names = cd.Engine.STAGES if transforms == "cufft" else cd.Engine.STAGES_FUSED
     assert set(ms) == set(names)
     assert all(v >= 0.0 for v in ms.values())
-    assert all(ms[k] > 0.0 for k in names[:8])
+    assert all(ms[k] > 0.0 for k in names[:8] if not k.startswith("-"))  # "-n": an empty slot
     for t in timed:
         assert t.free_energy == plain.free_energy
         assert np.array_equal(t.forces[0], plain.forces[0])
