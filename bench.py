@@ -119,9 +119,10 @@ class L2Flush:
 
 
 # DRAM bytes per evaluation measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum over every launch of one evaluation, 128^3 mixed); the
-# launch list is summarised in profiles/eval_128cubed_mixed_launches.md.
-MEASURED_TRAFFIC = {"mixed": 1131.5e6}
+# dram__bytes_write.sum over the seven launches of one evaluation, 128^3
+# mixed, fused transforms); the launch list is summarised in
+# profiles/eval_128cubed_mixed_launches.md.
+MEASURED_TRAFFIC = {"mixed": 715.8e6}
 
 
 class ClockSampler:
@@ -435,7 +436,8 @@ def run_ours(args, ws, rank, local, dist):
     e2e_val = ws * n_e2e / el
 
     info = eng.info
-    nbytes = algorithmic_bytes(info, S=1, M=1, fused=eng.transforms == "fused")
+    fused = eng.transforms == "fused"
+    nbytes = algorithmic_bytes(info, S=1, M=1, fused=fused)
     peak, peak_kind = hbm_peak()
     achieved = nbytes / (ms_step * 1e-3) / 1e9
     names = {cd.MIXED: "mixed", cd.FP64: "fp64"}
@@ -454,8 +456,10 @@ def run_ours(args, ws, rank, local, dist):
                    "l2": "flushed between timed steps (256 MiB write + 256 MiB read, outside the events)",
                    "transforms": eng.transforms},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": MEASURED_TRAFFIC.get(names[precision]),
-                     "scope": "one full evaluation (cuFFT transforms + engine kernels)",
+                     "frac": achieved / peak,
+                     "traffic": MEASURED_TRAFFIC.get(names[precision]) if fused else None,
+                     "scope": ("one full evaluation (the seven fused-path kernels)" if fused
+                               else "one full evaluation (cuFFT transforms + engine kernels)"),
                      "algorithmic_bytes": nbytes, "peak_source": peak_kind,
                      "traffic_source": "ncu dram bytes over one evaluation's launches (profiles/)",
                      "dominant_engine_kernel": {"stage": top, **mine[top]}},
