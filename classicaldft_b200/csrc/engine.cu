@@ -229,7 +229,9 @@ Engine::Engine(const EngineSpec& spec) {
   // the species mean: four blocks per SM in all (its last block sums the
   // partials, so fewer blocks shorten that tail and the counter's contention)
   grid_mean_ = per_problem(std::max<long long>(1, std::min<long long>((long long)sms * 4, (p.N * B + 255) / 256)));
-  partials_ = dalloc<double>((size_t)B * std::max(std::max(grid_pw_, grid_tma_), grid_stream_) * p.n_terms, tot);
+  // (+8: the pointwise grid rounded up to whole chunks, see fused_middle)
+  partials_ =
+      dalloc<double>((size_t)B * (std::max(std::max(grid_pw_, grid_tma_), grid_stream_) + 8) * p.n_terms, tot);
   err_ = dalloc<int>(1, tot);
   CDFT_CUDA(cudaMemset(err_, 0, sizeof(int)));
   sync_ = dalloc<unsigned>((size_t)B, tot);
@@ -260,6 +262,9 @@ Engine::~Engine() {
                   (void*)partials_, fft_work_, tw_, (void*)wtab_, (void*)pmean_, (void*)h_rho_, (void*)h_vext_, (void*)h_force_, (void*)h_scalars_})
     if (q) cudaFree(q);
   if (stream_) cudaStreamDestroy(stream_);
+  for (cudaStream_t st : aux_) cudaStreamDestroy(st);
+  for (cudaEvent_t ev : join_ev_) cudaEventDestroy(ev);
+  if (fork_ev_) cudaEventDestroy(fork_ev_);
   for (cudaEvent_t e : stage_ev_)
     if (e) cudaEventDestroy(e);
 }
@@ -332,6 +337,16 @@ void Engine::setup_fused() {
   CDFT_CUDA(cudaDeviceSynchronize());
   fusable_ = true;
   fused_ = true;
+  chunks_ = (p.nx >= 64) ? 4 : 1;
+  for (int k = 1; k < chunks_; ++k) {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    CDFT_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CDFT_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    aux_.push_back(st);
+    join_ev_.push_back(ev);
+  }
+  if (chunks_ > 1) CDFT_CUDA(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
 }
 
 void Engine::set_fused(bool on) {
@@ -506,8 +521,61 @@ void Engine::fused_forward(const double* rho, cudaStream_t stream) {
   mark(2, stream);
   fused_col_fwd(plan_, p, prho, pmean_, mean_, wtab_, q, tables_, stream);
   mark(3, stream);
-  fused_plane_inv(plan_, p, q, static_cast<float*>(chan_r_), err_, tables_, stream);
-  mark(4, stream);
+}
+
+// Fused transform path, stages 4-6 on chunks of x planes: inverse plane pass
+// of the channels, the pointwise kernel on those planes' points, forward
+// plane pass of their derivatives.  Unchunked, the stage marks separate the
+// three (stage timing runs this way).
+template <typename R>
+void Engine::fused_middle(const double* rho, const double* vext, double* force, bool chunked, cudaStream_t stream) {
+  const EvalParams& p = p_;
+  const int K = chunked ? chunks_ : 1;
+  const int per = p.nx / K;
+  const int gk = (grid_tma_ + K - 1) / K;
+  const fft::cpx* q = static_cast<const fft::cpx*>(chan_k_);
+  fft::cpx* pd = static_cast<fft::cpx*>(deriv_k_);
+  float* chan_r = static_cast<float*>(chan_r_);
+  float* deriv_r = static_cast<float*>(deriv_r_);
+  PointwiseArgs a;
+  a.rho = rho;
+  a.vext = vext;
+  a.force = force;
+  a.partials = partials_;
+  a.mf_w = mf_w_;
+  a.mean = mean_;
+  a.dbar_out = dbar_;
+  if (K > 1) {
+    CDFT_CUDA(cudaEventRecord(fork_ev_, stream));
+    for (int k = 1; k < K; ++k) CDFT_CUDA(cudaStreamWaitEvent(aux_[k - 1], fork_ev_, 0));
+  }
+  for (int k = 0; k < K; ++k) {
+    cudaStream_t st = k == 0 ? stream : aux_[k - 1];
+    const int ix0 = k * per;
+    fused_plane_inv(plan_, p, q, chan_r, err_, ix0, per, tables_, st);
+    if (K == 1) mark(4, st);
+    const long long p0 = (long long)ix0 * p.ny * p.nz, pn = (long long)per * p.ny * p.nz;
+    with_kernels(true, [&](auto model_c, auto multi_c, auto r_c) {
+      constexpr int MD = decltype(model_c)::value;
+      constexpr bool MU = decltype(multi_c)::value;
+      using RT = typename decltype(r_c)::type;
+      if constexpr (std::is_same_v<RT, R>)
+        k_pointwise_tma<MD, MU, RT><<<dim3(gk, p.batch), kTmaTile, vext ? tma_smem_v_ : tma_smem_, st>>>(
+            p, chan_r, deriv_r, a, err_, p0, pn, k * gk, K * gk);
+    });
+    CDFT_CUDA(cudaGetLastError());
+    if (K == 1) mark(5, st);
+    fused_plane_fwd_deriv(plan_, p, deriv_r, pd, err_, ix0, per, tables_, st);
+  }
+  if (K > 1) {
+    for (int k = 1; k < K; ++k) {
+      CDFT_CUDA(cudaEventRecord(join_ev_[k - 1], aux_[k - 1]));
+      CDFT_CUDA(cudaStreamWaitEvent(stream, join_ev_[k - 1], 0));
+    }
+    mark(4, stream);
+    mark(5, stream);
+  }
+  mark(6, stream);
 }
 
 // Fused transform path, stages 5-8: plane pass of every derivative channel,
@@ -517,8 +585,6 @@ void Engine::fused_backward(double* force, const MuArgs& mu, const FinalArgs& fi
   const EvalParams& p = p_;
   fft::cpx* pd = static_cast<fft::cpx*>(deriv_k_);
   fft::cpx* pf = static_cast<fft::cpx*>(force_k_);
-  fused_plane_fwd_deriv(plan_, p, static_cast<const float*>(deriv_r_), pd, err_, tables_, stream);
-  mark(6, stream);
   fused_col_bwd(plan_, p, pd, wtab_, pf, tables_, stream);
   mark(7, stream);
   fused_plane_inv_epi(plan_, p, pf, dbar_, force, mu, fin, err_, tables_, stream);
@@ -545,10 +611,34 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   mark(0, stream);
   const bool fused = mixed && fused_;
   // 1-3. weighted densities
-  if (fused)
+  // TMA ring when every segment start is 16-byte aligned (N % 4 == 0 and
+  // aligned base pointers); otherwise the register-prefetch variant.
+  const bool tma = (p.N % 4 == 0) && ((uintptr_t)rho % 16 == 0) && ((uintptr_t)vext % 16 == 0);
+  MuArgs ma;
+  for (int b = 0; b < kMaxBatch; ++b)
+    for (int s = 0; s < kMaxSpecies; ++s) ma.mu[b][s] = (b < p.batch && s < p.S) ? mu[b * p.S + s] : 0.0;
+  if (fused && tma) {
+    // fused path: stages 4-6 in plane chunks (one chunk while stage timing)
     fused_forward(rho, stream);
-  else
+    if constexpr (sizeof(R) == sizeof(float)) fused_middle<R>(rho, vext, force, !timing_run_, stream);
+    const int K = timing_run_ ? 1 : chunks_;
+    FinalArgs fin{partials_, K * ((grid_tma_ + K - 1) / K), err_, scalars};
+    fused_backward(force, ma, fin, stream);
+    mark(10, stream);
+    if (timing_run_) {
+      timing_run_ = false;
+      ++ring_used_;
+    }
+    return;
+  }
+  if (fused) {
+    fused_forward(rho, stream);
+    fused_plane_inv(plan_, p, static_cast<const fft::cpx*>(chan_k_), static_cast<float*>(chan_r_), err_, 0, p.nx,
+                    tables_, stream);
+    mark(4, stream);
+  } else {
     forward_stage<R, C2>(rho, chan_r, mean_, stream);
+  }
   // 4. pointwise Phi / dPhi + local terms + reductions
   PointwiseArgs a;
   a.rho = rho;
@@ -558,9 +648,6 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   a.mf_w = mf_w_;
   a.mean = mean_;
   a.dbar_out = dbar_;
-  // TMA ring when every segment start is 16-byte aligned (N % 4 == 0 and
-  // aligned base pointers); otherwise the register-prefetch variant.
-  const bool tma = (p.N % 4 == 0) && ((uintptr_t)rho % 16 == 0) && ((uintptr_t)vext % 16 == 0);
   const int pw_blocks = tma ? grid_tma_ : grid_pw_;
   const dim3 gt(grid_tma_, p.batch), gp(grid_pw_, p.batch);
   with_kernels(mixed, [&](auto model_c, auto multi_c, auto r_c) {
@@ -569,8 +656,8 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
     using RT = typename decltype(r_c)::type;
     if constexpr (std::is_same_v<RT, R>) {
       if (tma)
-        k_pointwise_tma<MD, MU, RT><<<gt, kTmaTile, vext ? tma_smem_v_ : tma_smem_, stream>>>(p, chan_r, deriv_r,
-                                                                                             a, err_);
+        k_pointwise_tma<MD, MU, RT><<<gt, kTmaTile, vext ? tma_smem_v_ : tma_smem_, stream>>>(
+            p, chan_r, deriv_r, a, err_, 0, p.N, 0, grid_tma_);
       else
         k_pointwise<MD, MU, RT><<<gp, 256, 0, stream>>>(p, chan_r, deriv_r, a);
     }
@@ -578,9 +665,11 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   CDFT_CUDA(cudaGetLastError());
   mark(5, stream);
   // 5-7. back-convolution into the force
-  MuArgs ma;
-  for (int b = 0; b < kMaxBatch; ++b)
-    for (int s = 0; s < kMaxSpecies; ++s) ma.mu[b][s] = (b < p.batch && s < p.S) ? mu[b * p.S + s] : 0.0;
+  if (fused) {
+    fused_plane_fwd_deriv(plan_, p, static_cast<const float*>(deriv_r_), static_cast<fft::cpx*>(deriv_k_), err_, 0,
+                          p.nx, tables_, stream);
+    mark(6, stream);
+  }
   // 8. scalars: block 0 of each problem's epilogue reduces the partials
   FinalArgs fin{partials_, pw_blocks, err_, scalars};
   if (fused)

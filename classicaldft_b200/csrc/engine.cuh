@@ -113,6 +113,8 @@ class Engine {
   void upload_mean_field(const EngineSpec& spec);
   void setup_fused();
   void fused_forward(const double* rho, cudaStream_t stream);
+  template <typename R>
+  void fused_middle(const double* rho, const double* vext, double* force, bool chunked, cudaStream_t stream);
   void fused_backward(double* force, const MuArgs& mu, const FinalArgs& fin, cudaStream_t stream);
   template <typename R, typename C2>
   void run(const double* rho, const double* vext, const double* mu, double* force, double* scalars,
@@ -161,6 +163,15 @@ class Engine {
 
   // fused transform path
   bool fusable_ = false, fused_ = false;
+  // The fused path's middle stages (inverse plane pass, pointwise, forward
+  // plane pass of the derivatives) depend only on their own x planes: they
+  // run as chunks_ chunks of planes, chunk k > 0 on aux_[k - 1], forked from
+  // and joined back into the caller's stream, so the FP64 pointwise work of
+  // one chunk overlaps the FP32 transforms of another.
+  int chunks_ = 1;
+  std::vector<cudaStream_t> aux_;
+  cudaEvent_t fork_ev_ = nullptr;
+  std::vector<cudaEvent_t> join_ev_;
   FusedPlan plan_{};
   void* tw_ = nullptr;
   float* wtab_ = nullptr;    // column-pass weight table ([5 S + M][Nk] floats)

@@ -535,7 +535,7 @@ __device__ __forceinline__ void assemble(const EvalParams& p, const T* n, Measur
 // dbar (dPhi of the uniform fluid at the means).  Thread 0 fills shared memory.
 template <int MODEL, bool MULTI>
 __device__ __forceinline__ void split_prologue(const EvalParams& p, const PointwiseArgs& a, double* s_off,
-                                               double* s_dbar) {
+                                               double* s_dbar, bool write_dbar) {
   constexpr bool TENSOR = model_has_tensor(MODEL);
   using L = Lay<MULTI, TENSOR>;
   constexpr int NF = L::NFMT;
@@ -563,7 +563,7 @@ __device__ __forceinline__ void split_prologue(const EvalParams& p, const Pointw
 #pragma unroll
     for (int c = 0; c < NF; ++c) {
       s_dbar[c] = D0[c];
-      if (blockIdx.x == 0) a.dbar_out[c] = D0[c];
+      if (write_dbar) a.dbar_out[c] = D0[c];
     }
   }
   __syncthreads();
@@ -667,7 +667,7 @@ __global__ void __launch_bounds__(256) k_pointwise(EvalParams p, const RT* __res
   deriv += (long long)blockIdx.y * p.L.n_deriv * p.N;
   __shared__ double s_off[kMaxChannels];
   __shared__ double s_dbar[NF];
-  if (SPLIT) split_prologue<MODEL, MULTI>(p, a, s_off, s_dbar);
+  if (SPLIT) split_prologue<MODEL, MULTI>(p, a, s_off, s_dbar, blockIdx.x == 0);
   const long long N = p.N;
   double acc[NT];
 #pragma unroll
@@ -738,7 +738,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return false;
 }
 
-constexpr int kTmaTile = 256;
+constexpr int kTmaTile = 128;
 constexpr int kTmaStages = 3;
 constexpr long long kWaitLimit = 1ll << 26;
 
@@ -747,10 +747,14 @@ __host__ __device__ constexpr int tma_stage_bytes(int S, bool vext) {
   return (Lay<MULTI, TENSOR>::NFMT + 2) * kTmaTile * (int)sizeof(RT) + S * kTmaTile * 8 * (vext ? 2 : 1);
 }
 
+// Points p0 .. p0 + pn - 1 of every problem (p0 a multiple of 4); the
+// partial sums of block blockIdx.x go to slot blk0 + blockIdx.x of nblk per
+// problem, so launches over disjoint point ranges fill one partials array.
 template <int MODEL, bool MULTI, typename RT>
-__global__ void __launch_bounds__(kTmaTile) k_pointwise_tma(EvalParams p, const RT* __restrict__ chan,
+__global__ void __launch_bounds__(kTmaTile, 5) k_pointwise_tma(EvalParams p, const RT* __restrict__ chan,
                                                             RT* __restrict__ deriv, PointwiseArgs a_all,
-                                                            int* err) {
+                                                            int* err, long long p0, long long pn, int blk0,
+                                                            int nblk) {
   constexpr bool TENSOR = model_has_tensor(MODEL);
   using L = Lay<MULTI, TENSOR>;
   constexpr bool SPLIT = sizeof(RT) == sizeof(float);
@@ -764,7 +768,8 @@ __global__ void __launch_bounds__(kTmaTile) k_pointwise_tma(EvalParams p, const 
   __shared__ int s_fail;
   __shared__ int s_out[kTmaStages];             // warps done with the stage's current fill
   __shared__ long long s_issued[kTmaStages];    // last local tile issued into the stage
-  const PointwiseArgs a = batch_slice(p, a_all, blockIdx.y);
+  PointwiseArgs a = batch_slice(p, a_all, blockIdx.y);
+  a.partials = a_all.partials + ((long long)blockIdx.y * nblk + blk0) * p.n_terms;
   chan += (long long)blockIdx.y * p.n_chan * p.N;
   deriv += (long long)blockIdx.y * p.L.n_deriv * p.N;
   const bool has_v = a.vext != nullptr;
@@ -772,8 +777,8 @@ __global__ void __launch_bounds__(kTmaTile) k_pointwise_tma(EvalParams p, const 
   const int n_mf_pre = (p.n_chan - NF) < 2 ? (p.n_chan - NF) : 2;
   const int n_in = NF + n_mf_pre;  // channel segments per tile
   const int stage_bytes = NPRE * kTmaTile * (int)sizeof(RT) + S * kTmaTile * 8 * (has_v ? 2 : 1);
-  const long long N = p.N;
-  const long long ntiles = (N + kTmaTile - 1) / kTmaTile;
+  const long long N = p.N;  // the stride of the channel and species arrays
+  const long long ntiles = (pn + kTmaTile - 1) / kTmaTile;
   const long long mine = (blockIdx.x < ntiles) ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const int tid = threadIdx.x;
   if (tid == 0) {
@@ -785,15 +790,15 @@ __global__ void __launch_bounds__(kTmaTile) k_pointwise_tma(EvalParams p, const 
     s_fail = 0;
     fence_mbar_init();
   }
-  if (SPLIT) split_prologue<MODEL, MULTI>(p, a, s_off, s_dbar);
+  if (SPLIT) split_prologue<MODEL, MULTI>(p, a, s_off, s_dbar, blk0 + blockIdx.x == 0);
   __syncthreads();
 
   auto stage_ptr = [&](int st) { return smem + (size_t)st * stage_bytes; };
   auto issue = [&](long long i) {  // local tile i -> stage i % kTmaStages
     const int st = (int)(i % kTmaStages);
     const long long tile = blockIdx.x + i * gridDim.x;
-    const long long start = tile * kTmaTile;
-    const long long cnt = (N - start) < kTmaTile ? (N - start) : kTmaTile;
+    const long long start = p0 + tile * kTmaTile;
+    const long long cnt = (p0 + pn - start) < kTmaTile ? (p0 + pn - start) : kTmaTile;
     const uint32_t cb = (uint32_t)(cnt * sizeof(RT));
     const uint32_t db = (uint32_t)(cnt * 8);
     unsigned char* base = stage_ptr(st);
@@ -826,8 +831,8 @@ __global__ void __launch_bounds__(kTmaTile) k_pointwise_tma(EvalParams p, const 
       break;
     }
     const long long tile = blockIdx.x + i * gridDim.x;
-    const long long idx = tile * kTmaTile + tid;
-    if (idx < N) {
+    const long long idx = p0 + tile * kTmaTile + tid;
+    if (idx < p0 + pn) {
       const RT* cs = reinterpret_cast<const RT*>(stage_ptr(st));
       const double* rb = reinterpret_cast<const double*>(stage_ptr(st) + (size_t)NPRE * kTmaTile * sizeof(RT));
       double cur[NPRE], rs[kMaxSpecies], vs[kMaxSpecies];

@@ -106,7 +106,7 @@ __device__ __forceinline__ bool bulk_load(void* dst, const void* src, uint32_t b
 template <int NY, int NZ, typename IN, int NT = RPlane<NY, NZ>::NT>
 __global__ void __launch_bounds__(NT)
     k_rplane_fwd(EvalParams p, const IN* __restrict__ in, int nseq, double* __restrict__ pmean,
-                 cpx* __restrict__ out, int* err, FftTables T) {
+                 cpx* __restrict__ out, int* err, int ix0, FftTables T) {
   using P = RPlane<NY, NZ>;
   constexpr int M = P::M, LD = P::LD, AY = P::AY, BY = P::BY, AZ = P::AZ, BZ = P::BZ;
   constexpr int EY = P::EY, ER = P::ER, EZS = P::EZS, EZ = P::EZ;
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(NT)
   cpx* ty = E + P::BUF;
   cpx* tz = ty + NY;
   cpx* t2 = tz + M;
-  const int ix = blockIdx.x, sq = blockIdx.y, b = blockIdx.z;
+  const int ix = ix0 + blockIdx.x, sq = blockIdx.y, b = blockIdx.z;  // planes ix0 ..
   plane_tables<NY, NZ, NT>(ty, tz, t2, T);
   __syncthreads();
   const IN* src = in + ((long long)b * nseq + sq) * p.N + (long long)ix * NY * NZ;
@@ -282,7 +282,7 @@ template <int NY, int NZ, bool EPI, bool MULTI, bool TENSOR, int NT = RPlane<NY,
 __global__ void __launch_bounds__(NT)
     k_rplane_inv(EvalParams p, const cpx* __restrict__ in, int nseq, float* __restrict__ out_f,
                  double* __restrict__ force, const double* __restrict__ dbar, const __grid_constant__ MuArgs mu,
-                 FinalArgs fin, int* err, FftTables T) {
+                 FinalArgs fin, int* err, int ix0, FftTables T) {
   using P = RPlane<NY, NZ>;
   using L = Lay<MULTI, TENSOR>;
   constexpr int M = P::M, LD = P::LD, AY = P::AY, BY = P::BY, AZ = P::AZ, BZ = P::BZ;
@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(NT)
   cpx* ty = E + P::BUF;
   cpx* tz = ty + NY;
   cpx* t2 = tz + M;
-  const int ix = blockIdx.x, sq = blockIdx.y, b = blockIdx.z;
+  const int ix = ix0 + blockIdx.x, sq = blockIdx.y, b = blockIdx.z;  // planes ix0 ..
   __shared__ double s_const;
   if constexpr (EPI) {
     if (ix == 0 && sq == 0 && fin.scalars)

@@ -124,7 +124,7 @@ void fused_plane_fwd_rho(const FusedPlan& f, const EvalParams& p, const double* 
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
     constexpr int NT = rk::RPlane<NY, NZ>::NT_WIDE;
     rk::k_rplane_fwd<NY, NZ, double, NT>
-        <<<dim3(p.nx, p.S, p.batch), NT, f.plane_smem, st>>>(p, rho, p.S, pmean, prho, err, T);
+        <<<dim3(p.nx, p.S, p.batch), NT, f.plane_smem, st>>>(p, rho, p.S, pmean, prho, err, 0, T);
   });
   CDFT_CUDA(cudaGetLastError());
 }
@@ -149,25 +149,25 @@ void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho
   CDFT_CUDA(cudaGetLastError());
 }
 
-void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q, float* chan_r, int* err,
-                     const FftTables& T, cudaStream_t st) {
+void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q, float* chan_r, int* err, int ix0,
+                     int nplanes, const FftTables& T, cudaStream_t st) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
     with_layout(p, [&](auto mc, auto tc) {
       rk::k_rplane_inv<NY, NZ, false, decltype(mc)::value, decltype(tc)::value>
-          <<<dim3(p.nx, p.n_chan, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(
-              p, q, p.n_chan, chan_r, nullptr, nullptr, MuArgs{}, FinalArgs{nullptr, 0, nullptr, nullptr}, err, T);
+          <<<dim3(nplanes, p.n_chan, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(
+              p, q, p.n_chan, chan_r, nullptr, nullptr, MuArgs{}, FinalArgs{nullptr, 0, nullptr, nullptr}, err, ix0, T);
     });
   });
   CDFT_CUDA(cudaGetLastError());
 }
 
 void fused_plane_fwd_deriv(const FusedPlan& f, const EvalParams& p, const float* deriv_r, fft::cpx* pd, int* err,
-                           const FftTables& T, cudaStream_t st) {
+                           int ix0, int nplanes, const FftTables& T, cudaStream_t st) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
-    rk::k_rplane_fwd<NY, NZ, float><<<dim3(p.nx, p.L.n_deriv, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(
-        p, deriv_r, p.L.n_deriv, nullptr, pd, err, T);
+    rk::k_rplane_fwd<NY, NZ, float><<<dim3(nplanes, p.L.n_deriv, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(
+        p, deriv_r, p.L.n_deriv, nullptr, pd, err, ix0, T);
   });
   CDFT_CUDA(cudaGetLastError());
 }
@@ -199,7 +199,7 @@ void fused_plane_inv_epi(const FusedPlan& f, const EvalParams& p, const fft::cpx
     with_layout(p, [&](auto mc, auto tc) {
       constexpr int NT = rk::RPlane<NY, NZ>::NT_WIDE;
       rk::k_rplane_inv<NY, NZ, true, decltype(mc)::value, decltype(tc)::value, NT>
-          <<<dim3(p.nx, p.S, p.batch), NT, f.plane_smem, st>>>(p, pf, p.S, nullptr, force, dbar, mu, fin, err, T);
+          <<<dim3(p.nx, p.S, p.batch), NT, f.plane_smem, st>>>(p, pf, p.S, nullptr, force, dbar, mu, fin, err, 0, T);
     });
   });
   CDFT_CUDA(cudaGetLastError());

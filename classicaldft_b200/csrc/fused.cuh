@@ -33,10 +33,12 @@ void fused_build_weights(const EvalParams& p, const double* mf_w, float* wtab, c
 
 void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho, const double* pmean, double* mean,
                    const float* wtab, fft::cpx* q, const FftTables& T, cudaStream_t st);
-void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q, float* chan_r, int* err,
-                     const FftTables& T, cudaStream_t st);
+// The two middle plane passes take x planes ix0 .. ix0 + nplanes - 1 (the
+// engine may split them into concurrent chunks).
+void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q, float* chan_r, int* err, int ix0,
+                     int nplanes, const FftTables& T, cudaStream_t st);
 void fused_plane_fwd_deriv(const FusedPlan& f, const EvalParams& p, const float* deriv_r, fft::cpx* pd, int* err,
-                           const FftTables& T, cudaStream_t st);
+                           int ix0, int nplanes, const FftTables& T, cudaStream_t st);
 void fused_col_bwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* pd, const float* wtab, fft::cpx* pf,
                    const FftTables& T, cudaStream_t st);
 void fused_plane_inv_epi(const FusedPlan& f, const EvalParams& p, const fft::cpx* pf, const double* dbar,
