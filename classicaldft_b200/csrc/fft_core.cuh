@@ -37,44 +37,70 @@ CDFT_HD constexpr int ilog2(int n) {
   return l;
 }
 
-// exp(-/+ 2 pi i t / R) for R dividing 16, as constants: cos and sin of
-// 2 pi t / 16 for t = 0 .. 15.
-CDFT_HD constexpr float c16(int t) {
-  constexpr float c[16] = {1.0f, 0.92387953251128674f, 0.70710678118654752f, 0.38268343236508977f,
-                           0.0f, -0.38268343236508977f, -0.70710678118654752f, -0.92387953251128674f,
-                           -1.0f, -0.92387953251128674f, -0.70710678118654752f, -0.38268343236508977f,
-                           0.0f, 0.38268343236508977f, 0.70710678118654752f, 0.92387953251128674f};
-  return c[t & 15];
+// exp(-/+ 2 pi i t / R) for R dividing 48 (the radices 2, 3, 4, 6, 8, 12,
+// 16), as constants: cos(2 pi t / 48) from its first quadrant, cos(k 7.5
+// degrees) for k = 0 .. 12 rounded to FP32.
+CDFT_HD constexpr float c48(int t) {
+  constexpr float q[13] = {1.0f,
+                           0.99144486137381038f,
+                           0.96592582628906829f,
+                           0.92387953251128674f,
+                           0.86602540378443865f,
+                           0.79335334029123517f,
+                           0.70710678118654752f,
+                           0.60876142900872066f,
+                           0.5f,
+                           0.38268343236508977f,
+                           0.25881904510252076f,
+                           0.13052619222005159f,
+                           0.0f};
+  t = ((t % 48) + 48) % 48;
+  if (t <= 12) return q[t];
+  if (t <= 24) return -q[24 - t];
+  if (t <= 36) return -q[t - 24];
+  return q[48 - t];
 }
-CDFT_HD constexpr float s16(int t) { return c16(t + 12); }  // sin(x) = cos(x - pi/2)
+CDFT_HD constexpr float s48(int t) { return c48(t + 36); }  // sin(x) = cos(x - pi/2)
 
 // a * exp(-/+ 2 pi i t / R), exact for the trivial angles.
 template <int R, int T, bool INV>
 CDFT_HD cpx rot(cpx a) {
-  constexpr int t16 = (T * (16 / R)) & 15;
-  if constexpr (t16 == 0) {
+  static_assert(48 % R == 0, "rotation radix must divide 48");
+  constexpr int t48 = (T * (48 / R)) % 48;
+  if constexpr (t48 == 0) {
     return a;
-  } else if constexpr (t16 == 4) {
+  } else if constexpr (t48 == 12) {
     return INV ? mul_i(a) : mul_mi(a);
-  } else if constexpr (t16 == 8) {
+  } else if constexpr (t48 == 24) {
     return {-a.x, -a.y};
-  } else if constexpr (t16 == 12) {
+  } else if constexpr (t48 == 36) {
     return INV ? mul_mi(a) : mul_i(a);
   } else {
-    constexpr float c = c16(t16), sn = INV ? s16(t16) : -s16(t16);
+    constexpr float c = c48(t48), sn = INV ? s48(t48) : -s48(t48);
     return {a.x * c - a.y * sn, a.x * sn + a.y * c};
   }
 }
 
-// In-register DFT of a[0..R), natural order in and out (radix-2 decimation
-// in time, recursively), R in {1, 2, 4, 8, 16}.
+// In-register DFT of a[0..R), natural order in and out, R in {1, 2, 3, 4,
+// 6, 8, 12, 16}: radix-2 decimation in time recursively down to 2 or 3
+// points; the 3-point DFT is X0 = a0 + s, X1,2 = a0 - s/2 -/+ i (sqrt 3 / 2)
+// (a1 - a2) with s = a1 + a2 (signs swapped for the inverse).
 template <int R, bool INV>
 CDFT_HD void dft(cpx* a) {
   if constexpr (R == 2) {
     const cpx t = a[0];
     a[0] = t + a[1];
     a[1] = t - a[1];
-  } else if constexpr (R > 2) {
+  } else if constexpr (R == 3) {
+    constexpr float h = 0.86602540378443865f;
+    const cpx sum = a[1] + a[2];
+    const cpx d = scale(a[1] - a[2], h);
+    const cpx m = a[0] - scale(sum, 0.5f);
+    a[0] = a[0] + sum;
+    a[1] = INV ? m + mul_i(d) : m + mul_mi(d);
+    a[2] = INV ? m + mul_mi(d) : m + mul_i(d);
+  } else if constexpr (R > 3) {
+    static_assert(R % 2 == 0, "DFT length must be 3 times a power of two or a power of two");
     cpx e[R / 2], o[R / 2];
 CDFT_UNROLL
     for (int i = 0; i < R / 2; ++i) {

@@ -29,13 +29,28 @@
 namespace cdft {
 namespace fft {
 
+// N = A * B with A >= B: powers of two split as evenly as possible; the
+// lengths 3 * 2^k of the 48- and 96-point grids into in-register DFTs of at
+// most 12 points (3 = 3 x 1, 6 = 3 x 2, 12 = 4 x 3, 24 = 8 x 3, 48 = 8 x 6,
+// 96 = 12 x 8).
+CDFT_HD constexpr int split_a(int N) {
+  if ((N & (N - 1)) == 0) return 1 << ((ilog2(N) + 1) / 2);
+  switch (N) {
+    case 3: return 3;
+    case 6: return 3;
+    case 12: return 4;
+    case 24: return 8;
+    case 48: return 8;
+    case 96: return 12;
+    default: return 0;
+  }
+}
+
 template <int N>
 struct Split {
-  static constexpr int LN = ilog2(N);
-  static constexpr int LA = (LN + 1) / 2;
-  static constexpr int A = 1 << LA;
-  static constexpr int B = N >> LA;
-  static constexpr int LB = LN - LA;
+  static constexpr int A = split_a(N);
+  static constexpr int B = N / A;
+  static_assert(A > 0 && A * B == N, "unsupported transform length");
 };
 
 // tw[m] = exp(-2 pi i m / N), m < N; the inverse uses its conjugate.

@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(NT)
   // half-complex post-processing on the y-spectrum, stored in natural order
   cpx* dst = out + ((long long)b * nseq + sq) * p.Nk + (long long)ix * NY * LD;
   for (int t = threadIdx.x; t < NY * M; t += NT) {
-    const int kz = t % M, ky = t / M, km = (NY - ky) & (NY - 1);
+    const int kz = t % M, ky = t / M, km = (NY - ky) % NY;
     if (kz == 0) {
       cpx x0, xM;
       fft::r2c_post_2d_dc(E[ky * ER], E[km * ER], x0, xM);
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(NT)
       const int kz = t % M, k1 = t / M;
 #pragma unroll
       for (int k2 = 0; k2 < BY; ++k2) {
-        const int ky = k1 + AY * k2, km = (NY - ky) & (NY - 1);
+        const int ky = k1 + AY * k2, km = (NY - ky) % NY;
         if (kz == 0)
           h0[j][k2] = fft::c2r_pre_2d_dc(E[ky * LD], E[km * LD], E[ky * LD + M], E[km * LD + M]);
         else

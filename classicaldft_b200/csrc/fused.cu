@@ -22,7 +22,9 @@ bool with_len(int n, F&& f) {
   switch (n) {
     case 16: f(IC<16>{}); return true;
     case 32: f(IC<32>{}); return true;
+    case 48: f(IC<48>{}); return true;
     case 64: f(IC<64>{}); return true;
+    case 96: f(IC<96>{}); return true;
     case 128: f(IC<128>{}); return true;
     default: return false;
   }
@@ -107,7 +109,7 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan) {
         if constexpr (MU) {
           allow_smem(rk::k_rcol_fwd<NX, TQ, MU, TE>, f.colf_smem);
           allow_smem(rk::k_rcol_bwd<NX, TQ, MU, TE>, f.colb_smem);
-        } else {
+        } else if constexpr (TQ == 16) {  // one species: 16-column tiles only
           allow_smem(rk::k_rcol_fwd1<NX, TQ, TE>, f.colf_smem);
           allow_smem(rk::k_rcol_bwd1<NX, TQ, TE>, f.colb_smem);
         }
@@ -139,7 +141,7 @@ void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho
         if constexpr (MU)
           rk::k_rcol_fwd<NX, TQ, MU, TE>
               <<<dim3(f.col_tiles, p.batch), rk::RCol<NX>::NT, f.colf_smem, st>>>(p, prho, pmean, mean, wtab, q, T);
-        else
+        else if constexpr (TQ == 16)
           rk::k_rcol_fwd1<NX, TQ, TE>
               <<<dim3(f.col_tiles, p.batch), rk::RCol1<NX, TQ>::NT, f.colf_smem, st>>>(p, prho, pmean, mean, wtab,
                                                                                           q, T);
@@ -182,7 +184,7 @@ void fused_col_bwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* pd, 
         if constexpr (MU)
           rk::k_rcol_bwd<NX, TQ, MU, TE>
               <<<dim3(f.col_tiles, p.batch), rk::RCol<NX>::NT, f.colb_smem, st>>>(p, pd, wtab, pf, T);
-        else
+        else if constexpr (TQ == 16)
           rk::k_rcol_bwd1<NX, TQ, TE>
               <<<dim3(f.col_tiles, p.batch), rk::RCol1<NX, TQ>::NT, f.colb_smem, st>>>(p, pd, wtab, pf, T);
       });

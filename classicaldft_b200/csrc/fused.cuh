@@ -1,7 +1,7 @@
 // Launchers of the fused transform path (fused.cu, kernels in
-// fft_reg_kernels.cuh).  Specialisations exist for nx in {16, 32, 64, 128} and
-// (ny, nz) in {16, 32, 64, 128}^2; fused_plan reports whether an engine's grid
-// and channel count have one.
+// fft_reg_kernels.cuh).  Specialisations exist for nx in {16, 32, 48, 64, 96,
+// 128} and (ny, nz) in the same set squared; fused_plan reports whether an
+// engine's grid and channel count have one.
 #pragma once
 
 #include "cdft_common.cuh"

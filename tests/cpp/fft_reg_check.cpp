@@ -70,6 +70,12 @@ void transform_rt(int N, cpx* x, int stride, bool spectrum_in, const cpx* tw) {
     case 32: transform<32, INV>(x, stride, spectrum_in, tw); break;
     case 64: transform<64, INV>(x, stride, spectrum_in, tw); break;
     case 128: transform<128, INV>(x, stride, spectrum_in, tw); break;
+    case 3: transform<3, INV>(x, stride, spectrum_in, tw); break;
+    case 6: transform<6, INV>(x, stride, spectrum_in, tw); break;
+    case 12: transform<12, INV>(x, stride, spectrum_in, tw); break;
+    case 24: transform<24, INV>(x, stride, spectrum_in, tw); break;
+    case 48: transform<48, INV>(x, stride, spectrum_in, tw); break;
+    case 96: transform<96, INV>(x, stride, spectrum_in, tw); break;
     default: transform<256, INV>(x, stride, spectrum_in, tw); break;
   }
 }
@@ -78,18 +84,7 @@ void transform_rt(int N, cpx* x, int stride, bool spectrum_in, const cpx* tw) {
 
 extern "C" {
 
-int fr_split_a(int N) {
-  switch (N) {
-    case 2: return F::Split<2>::A;
-    case 4: return F::Split<4>::A;
-    case 8: return F::Split<8>::A;
-    case 16: return F::Split<16>::A;
-    case 32: return F::Split<32>::A;
-    case 64: return F::Split<64>::A;
-    case 128: return F::Split<128>::A;
-    default: return F::Split<256>::A;
-  }
-}
+int fr_split_a(int N) { return F::split_a(N); }
 
 // One complex transform: spectrum_in selects the ordering, inv the sign.
 void fr_transform(int N, int spectrum_in, int inv, double* re, double* im) {

@@ -1,6 +1,7 @@
 """The register-resident transform steps of the fused path
 (csrc/fft_reg.cuh), built for the host from the same header and checked
-against numpy: both orderings of the split transform in both signs, and the
+against numpy: both orderings of the split transform in both signs (power-of-two lengths
+and the 3 x 2^k lengths of the 48- and 96-point grids), and the
 plane R2C / C2R with the half-complex steps on the y-spectrum.  FP32
 arithmetic: tolerances are 2e-6 of the transform's max magnitude, as for the
 stage-by-stage building blocks.
@@ -38,7 +39,7 @@ def err(a, b):
     return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-30)
 
 
-@pytest.mark.parametrize("N", [2, 4, 8, 16, 32, 64, 128, 256])
+@pytest.mark.parametrize("N", [2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 256])
 def test_split_transform_both_orderings(lib, N):
     A = lib.fr_split_a(N)
     assert A * (N // A) == N and A >= N // A
@@ -53,7 +54,7 @@ def test_split_transform_both_orderings(lib, N):
 
 
 @pytest.mark.parametrize("ny,nz", [(2, 4), (16, 16), (32, 64), (64, 32), (128, 128), (16, 8), (128, 16),
-                                   (8, 256), (4, 2)])
+                                   (8, 256), (4, 2), (48, 48), (96, 96), (48, 128), (96, 16), (16, 96)])
 def test_plane_r2c_and_c2r_on_the_y_spectrum(lib, ny, nz):
     rng = np.random.default_rng(ny * 1000 + nz)
     x = rng.standard_normal((ny, nz))

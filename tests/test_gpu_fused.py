@@ -49,6 +49,9 @@ CASES = [
     ((64, 16, 16), 0.2, [1.0], "Rosenfeld", [(0, 0) + LJ]),
     ((32, 16, 32), 0.2, [1.0, 0.6], "esFMT", [(0, 0) + LJ, (0, 1, 1.0, 0.8, 2.5), (1, 1, 0.8, 0.5, 2.0)]),
     ((16, 16, 32), 0.2, [1.0, 0.7], "Rosenfeld", [(0, 1, 1.0, 0.8, 2.5)]),
+    ((48, 48, 48), 0.1, [1.0], "WhiteBearII", [(0, 0) + LJ]),
+    ((96, 48, 96), 0.1, [1.0], "esFMT", [(0, 0) + LJ]),
+    ((48, 96, 16), 0.2, [1.0, 0.6], "WhiteBearI", [(0, 1, 1.0, 0.8, 2.5)]),
 ]
 
 
