@@ -817,25 +817,32 @@ __global__ void __launch_bounds__(256, 2)
 
 // One species: the thread of spectrum task (q, k1) keeps its BX elements'
 // |k| factors and rho_k (forward) or force accumulators (backward) in
-// registers for the whole pass, and the FMT channel loop is unrolled at
-// compile time, so each k-space product is a few multiplies.  One spectrum
-// task per thread (NT = TQ * AX); the first TQ * BX threads also run the
-// natural-order half of each transform.
+// registers for the whole pass.  One spectrum task per thread (NT = TQ *
+// AX); the first TQ * BX threads also run the natural-order half of each
+// transform.  Natural-order task (q, n2) and spectrum task (q, k1) of a
+// thread share its column q = t % TQ.
 template <int NX, int TQ>
 struct RCol1 {
   using SX = fft::Split<NX>;
   static constexpr int AX = SX::A, BX = SX::B;
   static constexpr int NT = TQ * AX;
   static constexpr int TILE = NX * TQ;
+  static constexpr int KN = NX / 2;                   // the x Nyquist element
+  static constexpr int K1N = KN % AX, K2N = KN / AX;  // its spectrum task and slot
+  static_assert(NX % 2 == 0, "even column lengths only");
 };
 
-// tx, two exchange buffers and (backward) two load buffers of NX x TQ.
+// Forward: tx, two exchange buffers and two kept transforms of NX x TQ;
+// backward: tx, two exchange buffers and four load buffers.
 __host__ __device__ inline size_t rcol1_smem(int nx, int tq) { return sizeof(cpx) * ((size_t)nx + 4ull * nx * tq); }
+__host__ __device__ inline size_t rcol1_smem_bwd(int nx, int tq) {
+  return sizeof(cpx) * ((size_t)nx + 6ull * nx * tq);
+}
 
 // The |k| factors of a task's elements (zero for columns past the plane).
 template <int BX>
 struct RTab {
-  float w3[BX], w2[BX], fv[BX], a[BX], b[BX];
+  float w3[BX], w2[BX], fv[BX], a[BX];
 };
 
 template <int NX, int TQ>
@@ -851,7 +858,6 @@ __device__ __forceinline__ RTab<RCol1<NX, TQ>::BX> rk_task_table(const float* __
     t.w2[k2] = valid ? wtab[Nk + kidx] : 0.0f;
     t.fv[k2] = valid ? wtab[2 * Nk + kidx] : 0.0f;
     t.a[k2] = valid ? wtab[3 * Nk + kidx] : 0.0f;
-    t.b[k2] = valid ? wtab[4 * Nk + kidx] : 0.0f;
   }
   return t;
 }
@@ -862,54 +868,79 @@ __device__ __forceinline__ RKv rk_task_element(const EvalParams& p, int kx, floa
   return rk_element(dkx * (float)(kx <= p.nx / 2 ? kx : kx - p.nx), xnyq, col.ky, col.ynyq, col.kz, col.proj);
 }
 
-// Weights of FMT channel c (one species; c uniform across the block) at the
-// BX elements of a task, as rk_weight1; returns `odd` (the channel is
-// i w rho).  One switch per channel and task keeps a single copy of the
-// transform code in the channel loop.
-template <bool TENSOR, int NX, int TQ>
-__device__ __forceinline__ bool rk_task_weights(int c, const RTab<RCol1<NX, TQ>::BX>& t, const EvalParams& p,
-                                                int k1, float dkx, const RColumn& col,
-                                                float (&w)[RCol1<NX, TQ>::BX]) {
-  using L = Lay<false, TENSOR>;
+// Column bases.  Along one column (ky, kz fixed) every FMT weight of one
+// species (weights.hpp:163-179; channel = W rho) is a few kx-dependent
+// factors times column constants:
+//   W_vy = i fv ky o_y,  W_vz = i fv kz o_z,
+//   W_Txy = a kx ky c_xy,  W_Txz = a kx kz c_xz,  W_Tyz = a ky kz c_yz,
+// and, with the trace identity a k^2 + 3 b = w2 of the tensor weight
+// a k_i k_j + b delta_ij,
+//   W_Txx = (2/3) a kx^2 + w2 / 3 - (ky^2 + kz^2) / 3 a,
+//   W_Tyy = -(1/3) a kx^2 + w2 / 3 + (2 ky^2 - kz^2) / 3 a.
+// So one x transform per basis serves every channel of a column:
+//   w3, w2, i fv kx o_x, i fv, a kx c_xy, a, a kx^2
+// (the first four without the tensor): 7 transforms for 10 channels.  The
+// Hermitian-projection masks o_x and c_xy depend on kx only at the x
+// Nyquist element.  c_xz equals c_xy on every column with kz != 0 except
+// those of the kz = nz/2 plane with ky off Nyquist ("special" columns),
+// where c_xz keeps only the x Nyquist element, whose transform is the
+// single term c (-1)^x.
+enum : int { kBW3 = 0, kBW2 = 1, kBVX = 2, kBV = 3, kBTX = 4, kBTA = 5, kBTXX = 6 };
+
+// The real factors of basis j at the BX elements of a task; returns `odd`
+// (the basis is i w).
+template <int NX, int TQ>
+__device__ __forceinline__ bool rk_basis_weights(int j, const RTab<RCol1<NX, TQ>::BX>& t, const EvalParams& p,
+                                                 int k1, float dkx, const RColumn& col,
+                                                 float (&w)[RCol1<NX, TQ>::BX]) {
   constexpr int AX = RCol1<NX, TQ>::AX, BX = RCol1<NX, TQ>::BX;
-  if (c == L::ETA) {
-#pragma unroll
-    for (int k2 = 0; k2 < BX; ++k2) w[k2] = t.w3[k2];
-    return false;
-  }
-  if (c == L::N2) {
-#pragma unroll
-    for (int k2 = 0; k2 < BX; ++k2) w[k2] = t.w2[k2];
-    return false;
-  }
-  if (c < L::V1 + 3) {
-    const int a = c - L::V1;
-#pragma unroll
-    for (int k2 = 0; k2 < BX; ++k2) {
-      const RKv v = rk_task_element<NX>(p, k1 + AX * k2, dkx, col);
-      const float ka = a == 0 ? v.k[0] * v.o[0] : (a == 1 ? v.k[1] * v.o[1] : v.k[2] * v.o[2]);
-      w[k2] = t.fv[k2] * ka;
-    }
-    return true;
-  }
-  const int tt = c - L::T, i = tchan_i(tt), j = tchan_j(tt);
 #pragma unroll
   for (int k2 = 0; k2 < BX; ++k2) {
     const RKv v = rk_task_element<NX>(p, k1 + AX * k2, dkx, col);
-    const float ki = i == 0 ? v.k[0] : v.k[1];
-    const float kj = j == 0 ? v.k[0] : (j == 1 ? v.k[1] : v.k[2]);
-    const float m = (i == j) ? 1.0f : ((i + j == 1) ? v.cxy : ((i + j == 2) ? v.cxz : v.cyz));
-    w[k2] = t.a[k2] * (ki * kj * m) + ((i == j) ? t.b[k2] : 0.0f);
+    const float kx = v.k[0];
+    if (j == kBW3)
+      w[k2] = t.w3[k2];
+    else if (j == kBW2)
+      w[k2] = t.w2[k2];
+    else if (j == kBVX)
+      w[k2] = t.fv[k2] * (kx * v.o[0]);
+    else if (j == kBV)
+      w[k2] = t.fv[k2];
+    else if (j == kBTX)
+      w[k2] = t.a[k2] * (kx * v.cxy);
+    else if (j == kBTA)
+      w[k2] = t.a[k2];
+    else
+      w[k2] = t.a[k2] * (kx * kx);
   }
-  return false;
+  return j == kBVX || j == kBV;
+}
+
+// Column constants of the basis combinations (zero past the plane).
+struct RColK {
+  float ky, kz;
+  float vy, vz, yz;  // ky o_y, kz o_z, ky kz c_yz
+  bool special;      // kz = nz/2 plane, ky off Nyquist
+};
+
+__device__ __forceinline__ RColK rk_colk(const RColumn& c) {
+  RColK r;
+  r.ky = c.valid ? c.ky : 0.0f;
+  r.kz = c.valid ? c.kz : 0.0f;
+  r.vy = (!c.proj || !c.ynyq) ? r.ky : 0.0f;
+  r.vz = c.proj ? 0.0f : r.kz;
+  r.yz = (!c.proj || c.ynyq) ? r.ky * r.kz : 0.0f;
+  r.special = c.valid && c.proj && c.kz != 0.0f && !c.ynyq;
+  return r;
 }
 
 // Inverse x transform of the task values bv (this thread's spectrum task)
-// through exchange buffer E; the natural-order half stores column q0 + q of
-// dst.  The caller alternates E between two buffers.
-template <int NX, int TQ>
-__device__ __forceinline__ void col1_inverse(cpx (&bv)[RCol1<NX, TQ>::BX], int q, int k1, cpx* E, const cpx* tx,
-                                             cpx* __restrict__ dst, long long plane, long long q0) {
+// through exchange buffer E; the natural-order half hands its AX samples
+// x = BX n1 + n2 of column q to emit(a, n2).  The caller alternates E
+// between two buffers.
+template <int NX, int TQ, class Emit>
+__device__ __forceinline__ void col1_inverse_emit(cpx (&bv)[RCol1<NX, TQ>::BX], int q, int k1, cpx* E,
+                                                  const cpx* tx, Emit&& emit) {
   using C = RCol1<NX, TQ>;
   constexpr int AX = C::AX, BX = C::BX;
   fft::spec_in<NX, true>(bv, k1, tx);
@@ -918,16 +949,25 @@ __device__ __forceinline__ void col1_inverse(cpx (&bv)[RCol1<NX, TQ>::BX], int q
   __syncthreads();
   const int t = threadIdx.x;
   if (t < TQ * BX) {
-    const int qn = t % TQ, n2 = t / TQ;
+    const int n2 = t / TQ;
     cpx a[AX];
 #pragma unroll
-    for (int kk = 0; kk < AX; ++kk) a[kk] = E[(n2 * AX + kk) * TQ + qn];
+    for (int kk = 0; kk < AX; ++kk) a[kk] = E[(n2 * AX + kk) * TQ + q];
     fft::spec_out<NX, true>(a);
-    if (q0 + qn < plane) {
-#pragma unroll
-      for (int n1 = 0; n1 < AX; ++n1) dst[(BX * n1 + n2) * plane + q0 + qn] = a[n1];
-    }
+    emit(a, n2);
   }
+}
+
+template <int NX, int TQ>
+__device__ __forceinline__ void col1_inverse(cpx (&bv)[RCol1<NX, TQ>::BX], int q, int k1, cpx* E, const cpx* tx,
+                                             cpx* __restrict__ dst, long long plane, long long q0) {
+  constexpr int AX = RCol1<NX, TQ>::AX, BX = RCol1<NX, TQ>::BX;
+  col1_inverse_emit<NX, TQ>(bv, q, k1, E, tx, [&](const cpx(&a)[AX], int n2) {
+    if (q0 + q < plane) {
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) dst[(BX * n1 + n2) * plane + q0 + q] = a[n1];
+    }
+  });
 }
 
 // Forward x transform of one array's column tile into this thread's task
@@ -940,18 +980,18 @@ __device__ __forceinline__ void col1_forward(const cpx* __restrict__ src, long l
   constexpr int AX = C::AX, BX = C::BX;
   const int t = threadIdx.x;
   if (t < TQ * BX) {
-    const int qn = t % TQ, n2 = t / TQ;
-    const bool ok = q0 + qn < plane;
+    const int n2 = t / TQ;
+    const bool ok = q0 + q < plane;
     cpx a[AX];
 #pragma unroll
-    for (int n1 = 0; n1 < AX; ++n1) a[n1] = ok ? src[(BX * n1 + n2) * plane + q0 + qn] : cpx{0.0f, 0.0f};
-    if (dc && q0 + qn == 0) {
+    for (int n1 = 0; n1 < AX; ++n1) a[n1] = ok ? src[(BX * n1 + n2) * plane + q0 + q] : cpx{0.0f, 0.0f};
+    if (dc && q0 + q == 0) {
 #pragma unroll
       for (int n1 = 0; n1 < AX; ++n1) a[n1].x += dc[BX * n1 + n2];
     }
     fft::nat_in<NX, false>(a, n2, tx);
 #pragma unroll
-    for (int kk = 0; kk < AX; ++kk) E[(n2 * AX + kk) * TQ + qn] = a[kk];
+    for (int kk = 0; kk < AX; ++kk) E[(n2 * AX + kk) * TQ + q] = a[kk];
   }
   __syncthreads();
 #pragma unroll
@@ -959,6 +999,11 @@ __device__ __forceinline__ void col1_forward(const cpx* __restrict__ src, long l
   fft::nat_out<NX, false>(out);
 }
 
+// Forward column pass: rho along x, then one inverse x transform per basis
+// (and per mean-field channel), each written out as the channels it
+// serves.  The w2 and a transforms stay in shared memory (each thread
+// reads back only its own samples) until the a kx^2 basis combines them
+// into T_xx and T_yy.
 template <int NX, int TQ, bool TENSOR>
 __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
     k_rcol_fwd1(EvalParams p, const cpx* __restrict__ prho, const double* __restrict__ pmean,
@@ -966,46 +1011,101 @@ __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
   using L = Lay<false, TENSOR>;
   using C = RCol1<NX, TQ>;
   constexpr int AX = C::AX, BX = C::BX, NT = C::NT, TILE = C::TILE;
+  constexpr int NB = TENSOR ? 7 : 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cpx* tx = reinterpret_cast<cpx*>(smem_raw);
   cpx* Eb = tx + NX;
-  const int NCH = p.n_chan;
+  cpx* S1 = Eb + 2 * TILE;  // the w2 transform
+  cpx* S2 = S1 + TILE;      // the a transform
+  __shared__ cpx s_nyq[TQ];  // a kx rho at the x Nyquist element of each column
+  __shared__ float s_dc[NX];
   const long long plane = (long long)p.ny * p.nzh, Nk = p.Nk;
   const int b = blockIdx.y;
   const long long q0 = (long long)blockIdx.x * TQ;
-  const int q = threadIdx.x % TQ, k1 = threadIdx.x / TQ;
-  for (int i = threadIdx.x; i < NX; i += NT) tx[i] = T.tx[i];
+  const int t = threadIdx.x;
+  const int q = t % TQ, k1 = t / TQ;
+  for (int i = t; i < NX; i += NT) tx[i] = T.tx[i];
   const RColumn col = rk_column(p, q0 + q, (float)p.dky, (float)p.dkz);
+  const RColK ck = rk_colk(col);
   const RTab<BX> tab = rk_task_table<NX, TQ>(wtab, Nk, plane, q0 + q, k1, col.valid);
   const float dkx = (float)p.dkx;
-  __shared__ float s_dc[NX];
   if (blockIdx.x == 0) rk_dc_column<NX>(p, pmean, b, mean_out, s_dc);
   __syncthreads();
   cpx r[BX];
   col1_forward<NX, TQ>(prho + (long long)b * Nk, plane, q0, q, k1, Eb, tx, r, blockIdx.x == 0 ? s_dc : nullptr);
   int buf = 1;
-  cpx* out = q_out + (long long)b * NCH * Nk;
+  cpx* out = q_out + (long long)b * p.n_chan * Nk + q0 + q;
+  const float third = 1.0f / 3.0f;
 #pragma unroll 1
-  for (int ch = 0; ch < L::NFMT; ++ch) {
+  for (int j = 0; j < NB; ++j) {
     float w[BX];
-    const bool odd = rk_task_weights<TENSOR, NX, TQ>(ch, tab, p, k1, dkx, col, w);
+    const bool odd = rk_basis_weights<NX, TQ>(j, tab, p, k1, dkx, col, w);
     cpx bv[BX];
 #pragma unroll
-    for (int k2 = 0; k2 < BX; ++k2)
-      bv[k2] = odd ? cpx{-w[k2] * r[k2].y, w[k2] * r[k2].x} : cpx{w[k2] * r[k2].x, w[k2] * r[k2].y};
-    col1_inverse<NX, TQ>(bv, q, k1, Eb + buf * TILE, tx, out + (long long)ch * Nk, plane, q0);
+    for (int k2 = 0; k2 < BX; ++k2) bv[k2] = odd ? cpx{-w[k2] * r[k2].y, w[k2] * r[k2].x} : scale(r[k2], w[k2]);
+    if (TENSOR && j == kBTX && k1 == C::K1N) s_nyq[q] = scale(r[C::K2N], tab.a[C::K2N] * (dkx * (float)C::KN));
+    // the channels of basis j: c1 = f1 X_j (+ g1 S1 + h1 S2), c2 likewise;
+    // X_j kept in S1 or S2 for the a kx^2 basis
+    int c1 = 0, c2 = -1, keep = 0;
+    float f1 = 1.0f, g1 = 0.0f, h1 = 0.0f, f2 = 0.0f, g2 = 0.0f, h2 = 0.0f;
+    bool nyq2 = false;
+    if (j == kBW3) {
+      c1 = L::ETA;
+    } else if (j == kBW2) {
+      c1 = L::N2;
+      keep = TENSOR ? 1 : 0;
+    } else if (j == kBVX) {
+      c1 = L::V1;
+    } else if (j == kBV) {
+      c1 = L::V1 + 1, f1 = ck.vy;
+      c2 = L::V1 + 2, f2 = ck.vz;
+    } else if (j == kBTX) {
+      c1 = L::T + 1, f1 = ck.ky;
+      c2 = L::T + 2, f2 = ck.kz;
+      nyq2 = ck.special;
+    } else if (j == kBTA) {
+      c1 = L::T + 4, f1 = ck.yz;
+      keep = 2;
+    } else {  // kBTXX: T_xx and T_yy
+      c1 = L::T + 0, f1 = 2.0f * third, g1 = third, h1 = -(ck.ky * ck.ky + ck.kz * ck.kz) * third;
+      c2 = L::T + 3, f2 = -third, g2 = third, h2 = (2.0f * ck.ky * ck.ky - ck.kz * ck.kz) * third;
+    }
+    const bool mix = j == kBTXX;
+    col1_inverse_emit<NX, TQ>(bv, q, k1, Eb + buf * TILE, tx, [&](const cpx(&a)[AX], int n2) {
+      if (!col.valid) return;
+      cpx* o1 = out + (long long)c1 * Nk + (long long)n2 * plane;
+      cpx* o2 = out + (long long)(c2 < 0 ? 0 : c2) * Nk + (long long)n2 * plane;
+      const cpx c = scale(s_nyq[q], f2);
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) {
+        const int x = BX * n1 + n2;
+        const long long off = (long long)(BX * n1) * plane;
+        cpx v1 = scale(a[n1], f1), v2 = scale(a[n1], f2);
+        if (mix) {
+          const cpx s1 = S1[x * TQ + q], s2 = S2[x * TQ + q];
+          v1 = v1 + scale(s1, g1) + scale(s2, h1);
+          v2 = v2 + scale(s1, g2) + scale(s2, h2);
+        }
+        if (nyq2) v2 = (x & 1) ? cpx{-c.x, -c.y} : c;
+        o1[off] = v1;
+        if (c2 >= 0) o2[off] = v2;
+        if (keep == 1) S1[x * TQ + q] = a[n1];
+        if (keep == 2) S2[x * TQ + q] = a[n1];
+      }
+    });
     buf ^= 1;
   }
   // mean-field channels: w(k) rho_k with the real weight from the table
+  cpx* mf_out = q_out + (long long)b * p.n_chan * Nk;
   for (int m = 0; m < p.M; ++m) {
     cpx bv[BX];
 #pragma unroll
     for (int k2 = 0; k2 < BX; ++k2) {
       const long long kidx = (long long)(k1 + AX * k2) * plane + q0 + q;
       const float w = col.valid ? wtab[(5LL + m) * Nk + kidx] : 0.0f;
-      bv[k2] = cpx{w * r[k2].x, w * r[k2].y};
+      bv[k2] = scale(r[k2], w);
     }
-    col1_inverse<NX, TQ>(bv, q, k1, Eb + buf * TILE, tx, out + (long long)p.mf_chan_j[m] * Nk, plane, q0);
+    col1_inverse<NX, TQ>(bv, q, k1, Eb + buf * TILE, tx, mf_out + (long long)p.mf_chan_j[m] * Nk, plane, q0);
     buf ^= 1;
   }
 }
@@ -1016,12 +1116,23 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
-// Backward: each natural-order task's column values of the next derivative
-// channel stream into a second load buffer (cp.async; every thread reads
-// back only what it copied itself) while the current channel is
-// transformed.
+// Backward column pass: F = sum_c conj(W_c) D_c per element (the
+// back-convolution), with the bases above.  Each natural-order task
+// combines the derivative channels of its column with the column
+// constants before one forward x transform per basis:
+//   w3: D_eta            i fv kx o_x: D_vx      i fv: ky o_y D_vy + kz o_z D_vz
+//   w2: D_n2 + (D_xx + D_yy) / 3                a kx^2: (2 D_xx - D_yy) / 3
+//   a: ky^2 D_yy + ky kz c_yz D_yz - (ky^2 + kz^2) / 3 (D_xx + D_yy)
+//   a kx c_xy: ky D_xy + kz D_xz (special columns: ky D_xy, and the D_xz
+//   term a kx kz sum_x (-1)^x D_xz at the x Nyquist element alone).
+// The channel columns stream into four load buffers with cp.async; every
+// thread reads back only what it copied itself, and refills a buffer after
+// the barrier that follows its last read of it.
 template <int NX, int TQ, bool TENSOR>
 __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
     k_rcol_bwd1(EvalParams p, const cpx* __restrict__ pd, const float* __restrict__ wtab, cpx* __restrict__ pf,
@@ -1032,31 +1143,46 @@ __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cpx* tx = reinterpret_cast<cpx*>(smem_raw);
   cpx* Eb = tx + NX;
-  cpx* Lb = Eb + 2 * TILE;
+  cpx* Lt = Eb + 2 * TILE;
+  __shared__ cpx s_alt[BX * TQ];  // partial sums (-1)^x D_xz of each natural-order task
   const long long plane = (long long)p.ny * p.nzh, Nk = p.Nk;
   const int b = blockIdx.y;
   const long long q0 = (long long)blockIdx.x * TQ;
   const int t = threadIdx.x;
   const int q = t % TQ, k1 = t / TQ;
   const bool nat = t < TQ * BX;
-  const int qn = t % TQ, n2 = t / TQ;
-  const bool ok = q0 + qn < plane;
-  const cpx* src = pd + (long long)b * NF * Nk;
-  auto prefetch = [&](int ch) {
+  const int n2 = t / TQ;
+  const RColumn col = rk_column(p, q0 + q, (float)p.dky, (float)p.dkz);
+  const RColK ck = rk_colk(col);
+  const bool ok = col.valid;
+  const cpx* src = pd + (long long)b * NF * Nk + q0 + q;
+  // this task's samples of channel ch -> load buffer l
+  auto load = [&](int ch, int l) {
     if (nat && ok) {
-      cpx* dst = Lb + (ch & 1) * TILE;
-      const cpx* s0 = src + (long long)ch * Nk + q0 + qn;
 #pragma unroll
       for (int n1 = 0; n1 < AX; ++n1) {
         const int x = BX * n1 + n2;
-        cp_async8(dst + x * TQ + qn, s0 + (long long)x * plane);
+        cp_async8(Lt + l * TILE + x * TQ + q, src + (long long)ch * Nk + (long long)x * plane);
       }
     }
-    cp_async_commit();
   };
-  prefetch(0);
+  auto at = [&](int l, int n1) { return ok ? Lt[l * TILE + (BX * n1 + n2) * TQ + q] : cpx{0.0f, 0.0f}; };
+  if constexpr (TENSOR) {
+    load(L::N2, 0);
+    load(L::T + 0, 1);
+    load(L::T + 3, 2);
+    load(L::T + 4, 3);
+    cp_async_commit();
+  } else {
+    load(L::V1 + 1, 0);
+    load(L::V1 + 2, 1);
+    cp_async_commit();
+    load(L::V1, 2);
+    cp_async_commit();
+    load(L::N2, 3);
+    cp_async_commit();
+  }
   for (int i = t; i < NX; i += NT) tx[i] = T.tx[i];
-  const RColumn col = rk_column(p, q0 + q, (float)p.dky, (float)p.dkz);
   const RTab<BX> tab = rk_task_table<NX, TQ>(wtab, Nk, plane, q0 + q, k1, col.valid);
   const float dkx = (float)p.dkx;
   __syncthreads();
@@ -1064,36 +1190,123 @@ __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
 #pragma unroll
   for (int k2 = 0; k2 < BX; ++k2) f[k2] = cpx{0.0f, 0.0f};
   int buf = 0;
-#pragma unroll 1
-  for (int ch = 0; ch < NF; ++ch) {
-    if (ch + 1 < NF)
-      prefetch(ch + 1);
-    else
-      cp_async_commit();  // an empty group keeps the wait count uniform
+  // One basis: input(a) builds the natural-order samples (natural-order
+  // threads), after the barrier refill() issues the next loads, and every
+  // spectrum task accumulates conj(W) times the transform.
+  auto basis = [&](int j, auto&& input, auto&& refill) {
     cpx* E = Eb + buf * TILE;
     if (nat) {
-      cp_async_wait_one();  // channel ch has landed
-      const cpx* Lt = Lb + (ch & 1) * TILE;
       cpx a[AX];
-#pragma unroll
-      for (int n1 = 0; n1 < AX; ++n1) a[n1] = ok ? Lt[(BX * n1 + n2) * TQ + qn] : cpx{0.0f, 0.0f};
+      input(a);
       fft::nat_in<NX, false>(a, n2, tx);
 #pragma unroll
-      for (int kk = 0; kk < AX; ++kk) E[(n2 * AX + kk) * TQ + qn] = a[kk];
+      for (int kk = 0; kk < AX; ++kk) E[(n2 * AX + kk) * TQ + q] = a[kk];
     }
     __syncthreads();
+    refill();
     cpx d[BX];
 #pragma unroll
-    for (int j = 0; j < BX; ++j) d[j] = E[(j * AX + k1) * TQ + q];
+    for (int jj = 0; jj < BX; ++jj) d[jj] = E[(jj * AX + k1) * TQ + q];
     fft::nat_out<NX, false>(d);
     float w[BX];
-    const bool odd = rk_task_weights<TENSOR, NX, TQ>(ch, tab, p, k1, dkx, col, w);
-    // conj(i w) D = -i w D for an odd channel
+    const bool odd = rk_basis_weights<NX, TQ>(j, tab, p, k1, dkx, col, w);
+    // conj(i w) D = -i w D for an odd basis
 #pragma unroll
     for (int k2 = 0; k2 < BX; ++k2)
-      f[k2] = odd ? cpx{f[k2].x + w[k2] * d[k2].y, f[k2].y - w[k2] * d[k2].x}
-                  : cpx{f[k2].x + w[k2] * d[k2].x, f[k2].y + w[k2] * d[k2].y};
+      f[k2] = odd ? cpx{f[k2].x + w[k2] * d[k2].y, f[k2].y - w[k2] * d[k2].x} : f[k2] + scale(d[k2], w[k2]);
     buf ^= 1;
+  };
+  auto none = [] {};
+  if constexpr (TENSOR) {
+    // buffers: 0 n2, 1 xx, 2 yy, 3 yz
+    basis(kBTA, [&](cpx (&a)[AX]) {
+      cp_async_wait<0>();
+      const float c3 = (ck.ky * ck.ky + ck.kz * ck.kz) * (1.0f / 3.0f), cyy = ck.ky * ck.ky - c3;
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) a[n1] = scale(at(2, n1), cyy) + scale(at(3, n1), ck.yz) - scale(at(1, n1), c3);
+    }, [&] {
+      load(L::T + 1, 3);  // xy -> 3
+      cp_async_commit();
+    });
+    basis(kBW2, [&](cpx (&a)[AX]) {
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) a[n1] = at(0, n1) + scale(at(1, n1) + at(2, n1), 1.0f / 3.0f);
+    }, [&] {
+      load(L::T + 2, 0);  // xz -> 0
+      cp_async_commit();
+    });
+    basis(kBTXX, [&](cpx (&a)[AX]) {
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) a[n1] = scale(scale(at(1, n1), 2.0f) - at(2, n1), 1.0f / 3.0f);
+    }, [&] {
+      load(L::V1 + 1, 1);  // vy -> 1, vz -> 2
+      load(L::V1 + 2, 2);
+      cp_async_commit();
+    });
+    basis(kBTX, [&](cpx (&a)[AX]) {
+      cp_async_wait<1>();  // xy, xz
+      const float kz = ck.special ? 0.0f : ck.kz;
+      cpx alt{0.0f, 0.0f};
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) {
+        const cpx xz = at(0, n1);
+        a[n1] = scale(at(3, n1), ck.ky) + scale(xz, kz);
+        alt = ((BX * n1 + n2) & 1) ? alt - xz : alt + xz;
+      }
+      s_alt[n2 * TQ + q] = alt;
+    }, [&] {
+      load(L::V1, 3);  // vx -> 3
+      cp_async_commit();
+      load(L::ETA, 0);  // eta -> 0
+      cp_async_commit();
+      // the D_xz term of a special column at the x Nyquist element
+      if (ck.special && k1 == C::K1N) {
+        cpx s{0.0f, 0.0f};
+#pragma unroll
+        for (int jj = 0; jj < BX; ++jj) s = s + s_alt[jj * TQ + q];
+        f[C::K2N] = f[C::K2N] + scale(s, tab.a[C::K2N] * (dkx * (float)C::KN) * ck.kz);
+      }
+    });
+    basis(kBV, [&](cpx (&a)[AX]) {
+      cp_async_wait<2>();  // vy, vz
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) a[n1] = scale(at(1, n1), ck.vy) + scale(at(2, n1), ck.vz);
+    }, none);
+    basis(kBVX, [&](cpx (&a)[AX]) {
+      cp_async_wait<1>();
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) a[n1] = at(3, n1);
+    }, none);
+    basis(kBW3, [&](cpx (&a)[AX]) {
+      cp_async_wait<0>();
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) a[n1] = at(0, n1);
+    }, none);
+  } else {
+    // buffers: 0 vy, 1 vz, 2 vx, 3 n2
+    basis(kBV, [&](cpx (&a)[AX]) {
+      cp_async_wait<2>();
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) a[n1] = scale(at(0, n1), ck.vy) + scale(at(1, n1), ck.vz);
+    }, [&] {
+      load(L::ETA, 0);  // eta -> 0
+      cp_async_commit();
+    });
+    basis(kBVX, [&](cpx (&a)[AX]) {
+      cp_async_wait<2>();
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) a[n1] = at(2, n1);
+    }, none);
+    basis(kBW2, [&](cpx (&a)[AX]) {
+      cp_async_wait<1>();
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) a[n1] = at(3, n1);
+    }, none);
+    basis(kBW3, [&](cpx (&a)[AX]) {
+      cp_async_wait<0>();
+#pragma unroll
+      for (int n1 = 0; n1 < AX; ++n1) a[n1] = at(0, n1);
+    }, none);
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
   col1_inverse<NX, TQ>(f, q, k1, Eb + buf * TILE, tx, pf + (long long)b * Nk, plane, q0);

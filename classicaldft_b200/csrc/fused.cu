@@ -82,13 +82,14 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan) {
   if (p.S == 1) {
     f.tq = 16;
     f.colf_smem = rk::rcol1_smem(p.nx, f.tq);
+    f.colb_smem = rk::rcol1_smem_bwd(p.nx, f.tq);
   } else {
     f.tq = 32;
     if (rk::rcol_smem(p.nx, f.tq, p.S) > kSmemCap) f.tq = 16;
     f.colf_smem = rk::rcol_smem(p.nx, f.tq, p.S);
+    f.colb_smem = f.colf_smem;
   }
-  f.colb_smem = f.colf_smem;
-  if (f.colf_smem > kSmemCap) return false;
+  if (f.colf_smem > kSmemCap || f.colb_smem > kSmemCap) return false;
   f.col_tiles = (int)(((long long)p.ny * p.nzh + f.tq - 1) / f.tq);
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
