@@ -156,6 +156,23 @@ CDFT_UNROLL
   }
 }
 
+// Half of the outputs of a length-R DFT by one decimation-in-frequency
+// step: out[m] = X[2m + h] for m < R/2 is the length-R/2 DFT of
+// (a[k] + (-1)^h a[k + R/2]) w_R^(k h).
+template <int R, bool INV>
+CDFT_HD void dft_half(const cpx* a, int h, cpx* out) {
+  static_assert(R % 2 == 0, "even DFT lengths only");
+  if (h == 0) {
+CDFT_UNROLL
+    for (int k = 0; k < R / 2; ++k) out[k] = a[k] + a[k + R / 2];
+  } else {
+    [&]<int... T>(std::integer_sequence<int, T...>) {
+      ((out[T] = rot<R, T, INV>(a[T] - a[T + R / 2])), ...);
+    }(std::make_integer_sequence<int, R / 2>{});
+  }
+  dft<R / 2, INV>(out);
+}
+
 }  // namespace fft
 
 // Twiddle tables (exp(-2 pi i n / M), FP64-rounded to FP32) of the four

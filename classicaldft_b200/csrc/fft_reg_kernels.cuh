@@ -829,6 +829,9 @@ struct RCol1 {
   static constexpr int TILE = NX * TQ;
   static constexpr int KN = NX / 2;                   // the x Nyquist element
   static constexpr int K1N = KN % AX, K2N = KN / AX;  // its spectrum task and slot
+  // AX = 2 BX (128, 32): the second half of an inverse transform runs on
+  // every thread, two per natural-order task with half of its samples each
+  static constexpr bool SPLIT_OUT = AX == 2 * BX;
   static_assert(NX % 2 == 0, "even column lengths only");
 };
 
@@ -935,9 +938,12 @@ __device__ __forceinline__ RColK rk_colk(const RColumn& c) {
 }
 
 // Inverse x transform of the task values bv (this thread's spectrum task)
-// through exchange buffer E; the natural-order half hands its AX samples
-// x = BX n1 + n2 of column q to emit(a, n2).  The caller alternates E
-// between two buffers.
+// through exchange buffer E.  The second half hands the samples of
+// natural-order task (q, n2) to emit(v, n1_0, dn1, n2): v[i] is sample
+// x = BX (n1_0 + i dn1) + n2 of column q.  With SPLIT_OUT the two threads
+// t and t + TQ BX of a task compute its even and odd n1 (dft_half), else
+// the first TQ BX threads compute all AX.  The caller alternates E between
+// two buffers.
 template <int NX, int TQ, class Emit>
 __device__ __forceinline__ void col1_inverse_emit(cpx (&bv)[RCol1<NX, TQ>::BX], int q, int k1, cpx* E,
                                                   const cpx* tx, Emit&& emit) {
@@ -948,24 +954,33 @@ __device__ __forceinline__ void col1_inverse_emit(cpx (&bv)[RCol1<NX, TQ>::BX], 
   for (int n2 = 0; n2 < BX; ++n2) E[(n2 * AX + k1) * TQ + q] = bv[n2];
   __syncthreads();
   const int t = threadIdx.x;
-  if (t < TQ * BX) {
+  if constexpr (C::SPLIT_OUT) {
+    const int h = t / (TQ * BX), n2 = (t / TQ) % BX;
+    cpx a[AX];
+#pragma unroll
+    for (int kk = 0; kk < AX; ++kk) a[kk] = E[(n2 * AX + kk) * TQ + q];
+    cpx v[AX / 2];
+    fft::dft_half<AX, true>(a, h, v);
+    emit(v, h, 2, n2);
+  } else if (t < TQ * BX) {
     const int n2 = t / TQ;
     cpx a[AX];
 #pragma unroll
     for (int kk = 0; kk < AX; ++kk) a[kk] = E[(n2 * AX + kk) * TQ + q];
     fft::spec_out<NX, true>(a);
-    emit(a, n2);
+    emit(a, 0, 1, n2);
   }
 }
 
 template <int NX, int TQ>
 __device__ __forceinline__ void col1_inverse(cpx (&bv)[RCol1<NX, TQ>::BX], int q, int k1, cpx* E, const cpx* tx,
                                              cpx* __restrict__ dst, long long plane, long long q0) {
-  constexpr int AX = RCol1<NX, TQ>::AX, BX = RCol1<NX, TQ>::BX;
-  col1_inverse_emit<NX, TQ>(bv, q, k1, E, tx, [&](const cpx(&a)[AX], int n2) {
+  constexpr int BX = RCol1<NX, TQ>::BX;
+  col1_inverse_emit<NX, TQ>(bv, q, k1, E, tx, [&](const auto& v, int n1_0, int dn1, int n2) {
+    constexpr int K = std::extent_v<std::remove_reference_t<decltype(v)>>;
     if (q0 + q < plane) {
 #pragma unroll
-      for (int n1 = 0; n1 < AX; ++n1) dst[(BX * n1 + n2) * plane + q0 + q] = a[n1];
+      for (int i = 0; i < K; ++i) dst[(BX * (n1_0 + i * dn1) + n2) * plane + q0 + q] = v[i];
     }
   });
 }
@@ -1071,16 +1086,18 @@ __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
       c2 = L::T + 3, f2 = -third, g2 = third, h2 = (2.0f * ck.ky * ck.ky - ck.kz * ck.kz) * third;
     }
     const bool mix = j == kBTXX;
-    col1_inverse_emit<NX, TQ>(bv, q, k1, Eb + buf * TILE, tx, [&](const cpx(&a)[AX], int n2) {
+    col1_inverse_emit<NX, TQ>(bv, q, k1, Eb + buf * TILE, tx, [&](const auto& a, int n1_0, int dn1, int n2) {
+      constexpr int K = std::extent_v<std::remove_reference_t<decltype(a)>>;
       if (!col.valid) return;
       cpx* o1 = out + (long long)c1 * Nk + (long long)n2 * plane;
       cpx* o2 = out + (long long)(c2 < 0 ? 0 : c2) * Nk + (long long)n2 * plane;
       const cpx c = scale(s_nyq[q], f2);
 #pragma unroll
-      for (int n1 = 0; n1 < AX; ++n1) {
+      for (int i = 0; i < K; ++i) {
+        const int n1 = n1_0 + i * dn1;
         const int x = BX * n1 + n2;
         const long long off = (long long)(BX * n1) * plane;
-        cpx v1 = scale(a[n1], f1), v2 = scale(a[n1], f2);
+        cpx v1 = scale(a[i], f1), v2 = scale(a[i], f2);
         if (mix) {
           const cpx s1 = S1[x * TQ + q], s2 = S2[x * TQ + q];
           v1 = v1 + scale(s1, g1) + scale(s2, h1);
@@ -1089,8 +1106,8 @@ __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
         if (nyq2) v2 = (x & 1) ? cpx{-c.x, -c.y} : c;
         o1[off] = v1;
         if (c2 >= 0) o2[off] = v2;
-        if (keep == 1) S1[x * TQ + q] = a[n1];
-        if (keep == 2) S2[x * TQ + q] = a[n1];
+        if (keep == 1) S1[x * TQ + q] = a[i];
+        if (keep == 2) S2[x * TQ + q] = a[i];
       }
     });
     buf ^= 1;

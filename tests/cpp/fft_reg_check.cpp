@@ -86,6 +86,31 @@ extern "C" {
 
 int fr_split_a(int N) { return F::split_a(N); }
 
+// The outputs X[2m + h] of one length-R DFT (decimation in frequency).
+void fr_dft_half(int R, int inv, int h, const double* re, const double* im, double* out_re, double* out_im) {
+  cpx a[16], o[8];
+  for (int i = 0; i < R; ++i) a[i] = {(float)re[i], (float)im[i]};
+  auto run = [&](auto rc, auto ic) {
+    constexpr int RR = decltype(rc)::value;
+    F::dft_half<RR, decltype(ic)::value>(a, h, o);
+  };
+  using std::integral_constant;
+  switch (R * 2 + (inv ? 1 : 0)) {
+    case 8: run(integral_constant<int, 4>{}, std::false_type{}); break;
+    case 9: run(integral_constant<int, 4>{}, std::true_type{}); break;
+    case 16: run(integral_constant<int, 8>{}, std::false_type{}); break;
+    case 17: run(integral_constant<int, 8>{}, std::true_type{}); break;
+    case 24: run(integral_constant<int, 12>{}, std::false_type{}); break;
+    case 25: run(integral_constant<int, 12>{}, std::true_type{}); break;
+    case 32: run(integral_constant<int, 16>{}, std::false_type{}); break;
+    default: run(integral_constant<int, 16>{}, std::true_type{}); break;
+  }
+  for (int m = 0; m < R / 2; ++m) {
+    out_re[m] = o[m].x;
+    out_im[m] = o[m].y;
+  }
+}
+
 // One complex transform: spectrum_in selects the ordering, inv the sign.
 void fr_transform(int N, int spectrum_in, int inv, double* re, double* im) {
   std::vector<cpx> x(N);

@@ -1,8 +1,8 @@
 """The register-resident transform steps of the fused path
 (csrc/fft_reg.cuh), built for the host from the same header and checked
 against numpy: both orderings of the split transform in both signs (power-of-two lengths
-and the 3 x 2^k lengths of the 48- and 96-point grids), and the
-plane R2C / C2R with the half-complex steps on the y-spectrum.  FP32
+and the 3 x 2^k lengths of the 48- and 96-point grids), the half-output
+DFT of the column passes, and the plane R2C / C2R with the half-complex steps on the y-spectrum.  FP32
 arithmetic: tolerances are 2e-6 of the transform's max magnitude, as for the
 stage-by-stage building blocks.
 """
@@ -28,6 +28,7 @@ def lib(tmp_path_factory):
     L.fr_transform.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp]
     L.fr_plane_forward.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dp]
     L.fr_plane_inverse.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dp]
+    L.fr_dft_half.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp]
     return L
 
 
@@ -51,6 +52,21 @@ def test_split_transform_both_orderings(lib, N):
             lib.fr_transform(N, spectrum_in, inv, ptr(re), ptr(im))
             ref = np.fft.ifft(x) * N if inv else np.fft.fft(x)
             assert err(re + 1j * im, ref) <= TOL, (spectrum_in, inv)
+
+
+@pytest.mark.parametrize("R", [4, 8, 12, 16])
+def test_half_output_dft(lib, R):
+    """One decimation-in-frequency step: the even (h = 0) and odd (h = 1)
+    outputs of a length-R DFT, as two threads of the column passes split an
+    inverse transform's second half."""
+    rng = np.random.default_rng(R + 7)
+    x = rng.standard_normal(R) + 1j * rng.standard_normal(R)
+    for inv in (0, 1):
+        ref = np.fft.ifft(x) * R if inv else np.fft.fft(x)
+        for h in (0, 1):
+            ore, oim = np.zeros(R // 2), np.zeros(R // 2)
+            lib.fr_dft_half(R, inv, h, ptr(x.real.copy()), ptr(x.imag.copy()), ptr(ore), ptr(oim))
+            assert err(ore + 1j * oim, ref[h::2]) <= TOL, (inv, h)
 
 
 @pytest.mark.parametrize("ny,nz", [(2, 4), (16, 16), (32, 64), (64, 32), (128, 128), (16, 8), (128, 16),
