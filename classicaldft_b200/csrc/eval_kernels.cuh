@@ -601,54 +601,75 @@ __device__ __forceinline__ void point_body(const EvalParams& p, const PointwiseA
   acc[kTermHS] += phi;
 #pragma unroll
   for (int c = 0; c < NF; ++c) __stcs(deriv + c * N + idx, (RT)(SPLIT ? D[c] - s_dbar[c] : D[c]));
-  double f[kMaxSpecies];
-#pragma unroll
-  for (int s = 0; s < kMaxSpecies; ++s) {
-    if (s < p.S) {
-      const double r = rs[s];
-      const double v = vs[s];
-      const double lr = log(r < 1e-300 ? 1e-300 : r);
-      acc[kTermId] += r * (lr - 1.0);
-      acc[kTermExt] += r * v;
-      acc[kTermN0 + s] += r;
-      f[s] = lr * p.dv + v * p.dv;  // -mu dV is added by k_epilogue
+  if constexpr (!MULTI) {
+    // one species: every interaction is species 0 with itself, channel NF + q
+    const double r = rs[0], v = vs[0];
+    const double lr = log(r < 1e-300 ? 1e-300 : r);
+    acc[kTermId] += r * (lr - 1.0);
+    acc[kTermExt] += r * v;
+    acc[kTermN0] += r;
+    double f0 = lr + v;  // -mu dV is added by k_epilogue
+    for (int q = 0; q < p.M; ++q) {
+      double cj;
+      if (q < n_mf_pre)
+        cj = q == 0 ? cur[NF] : cur[NPRE - 1];
+      else
+        cj = (double)chan[(NF + q) * N + idx];
+      cj += SPLIT ? s_off[NF + q] : 0.0;
+      acc[kTermMF] += 0.5 * r * cj;
+      f0 += cj;
     }
-  }
-  for (int q = 0; q < p.M; ++q) {
-    const int i = p.mf_i[q], j = p.mf_j[q];
-    const int cjx = p.mf_chan_j[q];
-    const int cix = p.mf_chan_i[q];
-    double cj = 0.0, ci = 0.0;
-    bool hj = false, hi = false;
+    __stcs(a.force + idx, f0 * p.dv);
+  } else {
+    double f[kMaxSpecies];
 #pragma unroll
-    for (int c = NF; c < NPRE; ++c) {
-      if (c == cjx && c - NF < n_mf_pre) { cj = cur[c]; hj = true; }
-      if (c == cix && c - NF < n_mf_pre) { ci = cur[c]; hi = true; }
-    }
-    if (!hj) cj = (double)chan[cjx * N + idx];
-    cj += SPLIT ? s_off[cjx] : 0.0;
-    double ri = 0.0;
-#pragma unroll
-    for (int s = 0; s < kMaxSpecies; ++s)
-      if (s == i) ri = rs[s];
-    acc[kTermMF] += 0.5 * ri * cj;
-    if (i == j) {
-#pragma unroll
-      for (int s = 0; s < kMaxSpecies; ++s)
-        if (s == i) f[s] += cj * p.dv;
-    } else {
-      if (!hi) ci = (double)chan[cix * N + idx];
-      ci += SPLIT ? s_off[cix] : 0.0;
-#pragma unroll
-      for (int s = 0; s < kMaxSpecies; ++s) {
-        if (s == i) f[s] += 0.5 * cj * p.dv;
-        if (s == j) f[s] += 0.5 * ci * p.dv;
+    for (int s = 0; s < kMaxSpecies; ++s) {
+      if (s < p.S) {
+        const double r = rs[s];
+        const double v = vs[s];
+        const double lr = log(r < 1e-300 ? 1e-300 : r);
+        acc[kTermId] += r * (lr - 1.0);
+        acc[kTermExt] += r * v;
+        acc[kTermN0 + s] += r;
+        f[s] = lr * p.dv + v * p.dv;  // -mu dV is added by k_epilogue
       }
     }
-  }
+    for (int q = 0; q < p.M; ++q) {
+      const int i = p.mf_i[q], j = p.mf_j[q];
+      const int cjx = p.mf_chan_j[q];
+      const int cix = p.mf_chan_i[q];
+      double cj = 0.0, ci = 0.0;
+      bool hj = false, hi = false;
 #pragma unroll
-  for (int s = 0; s < kMaxSpecies; ++s)
-    if (s < p.S) __stcs(a.force + s * N + idx, f[s]);
+      for (int c = NF; c < NPRE; ++c) {
+        if (c == cjx && c - NF < n_mf_pre) { cj = cur[c]; hj = true; }
+        if (c == cix && c - NF < n_mf_pre) { ci = cur[c]; hi = true; }
+      }
+      if (!hj) cj = (double)chan[cjx * N + idx];
+      cj += SPLIT ? s_off[cjx] : 0.0;
+      double ri = 0.0;
+#pragma unroll
+      for (int s = 0; s < kMaxSpecies; ++s)
+        if (s == i) ri = rs[s];
+      acc[kTermMF] += 0.5 * ri * cj;
+      if (i == j) {
+#pragma unroll
+        for (int s = 0; s < kMaxSpecies; ++s)
+          if (s == i) f[s] += cj * p.dv;
+      } else {
+        if (!hi) ci = (double)chan[cix * N + idx];
+        ci += SPLIT ? s_off[cix] : 0.0;
+#pragma unroll
+        for (int s = 0; s < kMaxSpecies; ++s) {
+          if (s == i) f[s] += 0.5 * cj * p.dv;
+          if (s == j) f[s] += 0.5 * ci * p.dv;
+        }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < kMaxSpecies; ++s)
+      if (s < p.S) __stcs(a.force + s * N + idx, f[s]);
+  }
 }
 
 // Plain variant (any N): each thread loads the next point's inputs before
@@ -659,7 +680,7 @@ __global__ void __launch_bounds__(256) k_pointwise(EvalParams p, const RT* __res
   constexpr bool TENSOR = model_has_tensor(MODEL);
   using L = Lay<MULTI, TENSOR>;
   constexpr bool SPLIT = sizeof(RT) == sizeof(float);
-  constexpr int NT = 4 + kMaxSpecies;
+  constexpr int NT = 4 + (MULTI ? kMaxSpecies : 1);  // the partial sums (one species: 5)
   constexpr int NF = L::NFMT;
   constexpr int NPRE = NF + 2;
   const PointwiseArgs a = batch_slice(p, a_all, blockIdx.y);
@@ -680,7 +701,7 @@ __global__ void __launch_bounds__(256) k_pointwise(EvalParams p, const RT* __res
     for (int q = 0; q < NPRE; ++q)
       if (q < NF || q - NF < n_mf_pre) cur[q] = (double)__ldcs(chan + q * N + idx);
 #pragma unroll
-    for (int s = 0; s < kMaxSpecies; ++s) {
+    for (int s = 0; s < (MULTI ? kMaxSpecies : 1); ++s) {
       if (s < p.S) {
         rs[s] = __ldcs(a.rho + s * N + idx);
         vs[s] = a.vext ? __ldcs(a.vext + s * N + idx) : 0.0;
@@ -693,9 +714,9 @@ __global__ void __launch_bounds__(256) k_pointwise(EvalParams p, const RT* __res
 
 // ---- TMA-staged variant (N % 4 == 0) -----------------------------------
 //
-// Each CTA walks tiles of 256 points.  Every input segment of a tile
-// (channel values, rho, V_ext) streams from HBM into a 3-stage shared-memory
-// ring with cp.async.bulk (TMA bulk copies, no multicast), signalled by an
+// Each CTA walks tiles of kTmaTile points.  Every input segment of a tile
+// (channel values, rho, V_ext) streams from HBM into a kTmaStages-deep
+// shared-memory ring with cp.async.bulk (TMA bulk copies, no multicast), signalled by an
 // mbarrier with transaction counts; each thread then reads its point from
 // shared memory.  There is no block-wide barrier per tile: each warp counts
 // itself out of a stage when it has read it, and the last warp out issues
@@ -758,7 +779,7 @@ __global__ void __launch_bounds__(kTmaTile, 5) k_pointwise_tma(EvalParams p, con
   constexpr bool TENSOR = model_has_tensor(MODEL);
   using L = Lay<MULTI, TENSOR>;
   constexpr bool SPLIT = sizeof(RT) == sizeof(float);
-  constexpr int NT = 4 + kMaxSpecies;
+  constexpr int NT = 4 + (MULTI ? kMaxSpecies : 1);  // the partial sums (one species: 5)
   constexpr int NF = L::NFMT;
   constexpr int NPRE = NF + 2;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -822,17 +843,18 @@ __global__ void __launch_bounds__(kTmaTile, 5) k_pointwise_tma(EvalParams p, con
   constexpr int kWarps = kTmaTile / 32;
   const int lane = tid & 31;
   volatile int* fail = &s_fail;
-  for (long long i = 0; i < mine; ++i) {
-    const int st = (int)(i % kTmaStages);
-    const uint32_t par = (uint32_t)((i / kTmaStages) & 1);
+  // stage st = i % kTmaStages and its phase parity, advanced per tile
+  int st = 0;
+  uint32_t par = 0;
+  long long idx = p0 + (long long)blockIdx.x * kTmaTile + tid;
+  const long long idx_step = (long long)gridDim.x * kTmaTile, idx_end = p0 + pn;
+  for (long long i = 0; i < mine; ++i, idx += idx_step) {
     if (*fail) break;
     if (!mbar_wait_bounded(&bars[st], par, kWaitLimit)) {
       *fail = 1;
       break;
     }
-    const long long tile = blockIdx.x + i * gridDim.x;
-    const long long idx = p0 + tile * kTmaTile + tid;
-    if (idx < p0 + pn) {
+    if (idx < idx_end) {
       const RT* cs = reinterpret_cast<const RT*>(stage_ptr(st));
       const double* rb = reinterpret_cast<const double*>(stage_ptr(st) + (size_t)NPRE * kTmaTile * sizeof(RT));
       double cur[NPRE], rs[kMaxSpecies], vs[kMaxSpecies];
@@ -840,7 +862,7 @@ __global__ void __launch_bounds__(kTmaTile, 5) k_pointwise_tma(EvalParams p, con
       for (int q = 0; q < NPRE; ++q)
         if (q < NF || q - NF < n_mf_pre) cur[q] = (double)cs[q * kTmaTile + tid];
 #pragma unroll
-      for (int s = 0; s < kMaxSpecies; ++s) {
+      for (int s = 0; s < (MULTI ? kMaxSpecies : 1); ++s) {
         if (s < S) {
           rs[s] = rb[s * kTmaTile + tid];
           vs[s] = has_v ? rb[(S + s) * kTmaTile + tid] : 0.0;
@@ -859,6 +881,10 @@ __global__ void __launch_bounds__(kTmaTile, 5) k_pointwise_tma(EvalParams p, con
           issue(i + kTmaStages);
         }
       }
+    }
+    if (++st == kTmaStages) {
+      st = 0;
+      par ^= 1u;
     }
   }
   __syncthreads();

@@ -104,4 +104,9 @@ def test_fused_batch_and_unaligned_buffers():
     torch.cuda.synchronize()
     ref = pr.gpu([rho[0]], [mus[0]], [v])
     assert rel_err(float(sc[0]), ref.free_energy) <= 1e-13
-    assert force_err([buf[2 * N + 3:].cpu().numpy()], ref.forces) <= 1e-12
+    # misaligned rho / vext take the register-prefetch pointwise kernel
+    # instead of the TMA ring: the same FP64 formulas, but the compiler may
+    # contract them into FMAs differently, and a last-bit difference in a
+    # derivative can flip the FP32 rounding of its deviation from the mean
+    # (one FP32 ulp of a 5% deviation: ~3e-9 of the force scale)
+    assert force_err([buf[2 * N + 3:].cpu().numpy()], ref.forces) <= 1e-8
