@@ -120,13 +120,13 @@ class L2Flush:
 
 # DRAM bytes per evaluation measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum over the seven launches of one evaluation, 128^3
-# mixed, fused transforms); the launch list is summarised in
-# profiles/eval_128cubed_mixed_launches.md.
-MEASURED_TRAFFIC = {"mixed": 715.8e6}
+# mixed, fused transforms, middle stages in one plane chunk); the launch
+# list is summarised in profiles/eval_128cubed_mixed_launches.md.
+MEASURED_TRAFFIC = {"mixed": 618.5e6}
 # The same capture per launch of each fused-path stage (bytes).
-MEASURED_STAGE_TRAFFIC = {"plane_fwd_rho": 16.80e6, "col_fwd": 72.04e6, "plane_inv_channels": 137.64e6,
-                          "pointwise": 158.58e6, "plane_fwd_derivatives": 115.95e6, "col_bwd": 108.43e6,
-                          "plane_inv_epilogue": 25.34e6}
+MEASURED_STAGE_TRAFFIC = {"plane_fwd_rho": 16.79e6, "col_fwd": 64.78e6, "plane_inv_channels": 137.39e6,
+                          "pointwise": 156.50e6, "plane_fwd_derivatives": 115.17e6, "col_bwd": 102.54e6,
+                          "plane_inv_epilogue": 25.36e6}
 
 
 class ClockSampler:
@@ -373,6 +373,8 @@ def run_ours(args, ws, rank, local, dist):
     dev = torch.device("cuda", local)
     precision = cd.MIXED if args.precision == "mixed" else cd.FP64
     eng, d = _build_engine(cd, precision)
+    if args.plane_chunks:
+        eng.set_plane_chunks(args.plane_chunks)
     rho_h = workload_profile()
     rho = torch.tensor(rho_h, dtype=torch.float64, device=dev)
     force = torch.empty_like(rho)
@@ -458,7 +460,7 @@ def run_ours(args, ws, rank, local, dist):
                    "grid": list(SHAPE), "dx": DX, "kT": KT, "rho_bar": RHO_BAR, "noise": "1% uniform, seeded",
                    "hs_diameter": d, "precision": names[precision], "parallelism": f"replicas x{ws}",
                    "l2": "flushed between timed steps (256 MiB write + 256 MiB read, outside the events)",
-                   "transforms": eng.transforms},
+                   "transforms": eng.transforms, "plane_chunks": (info["kernels_per_eval"] - 4) // 3 if fused else None},
         # the dominant kernel (the longest stage of the evaluation): its
         # algorithmic bytes over its live duration; the whole evaluation beside it
         "roofline": {"bound": "hbm", "kernel": top, "achieved": mine[top]["achieved_gbs"], "peak": peak,
@@ -499,6 +501,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-sweep", action="store_true", help="skip the batched 48/64/96^3 sweep measurement")
+    ap.add_argument("--plane-chunks", type=int, default=0,
+                    help="plane chunks of the fused path's middle stages (0: the engine's default; 1 runs them "
+                         "back to back, as a profiler's serialised launch list sees them)")
     args = ap.parse_args()
     ws, rank, local, dist = setup_dist(args)
     try:

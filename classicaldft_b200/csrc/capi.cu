@@ -319,6 +319,14 @@ int cdft_engine_set_transforms(cdft_engine* engine, int transforms) {
   });
 }
 
+int cdft_engine_set_plane_chunks(cdft_engine* engine, int chunks) {
+  return guarded([&] {
+    if (!engine) throw std::invalid_argument("engine is NULL");
+    static_assert(CDFT_MAX_PLANE_CHUNKS == cdft::Engine::kMaxChunks, "chunk limit");
+    engine->impl->set_chunks(chunks);
+  });
+}
+
 int cdft_engine_transforms(const cdft_engine* engine, int* transforms, int* fused_available) {
   return guarded([&] {
     if (!engine) throw std::invalid_argument("engine is NULL");

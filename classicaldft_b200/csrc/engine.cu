@@ -338,7 +338,12 @@ void Engine::setup_fused() {
   fusable_ = true;
   fused_ = true;
   chunks_ = (p.nx >= 64) ? 4 : 1;
-  for (int k = 1; k < chunks_; ++k) {
+  ensure_chunk_streams(chunks_);
+}
+
+// Streams and events for k chunks (chunk 0 runs on the caller's stream).
+void Engine::ensure_chunk_streams(int k) {
+  while ((int)aux_.size() < k - 1) {
     cudaStream_t st = nullptr;
     cudaEvent_t ev = nullptr;
     CDFT_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -346,13 +351,21 @@ void Engine::setup_fused() {
     aux_.push_back(st);
     join_ev_.push_back(ev);
   }
-  if (chunks_ > 1) CDFT_CUDA(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
+  if (k > 1 && !fork_ev_) CDFT_CUDA(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
+}
+
+void Engine::set_chunks(int k) {
+  if (!fusable_) throw std::invalid_argument("plane chunks: the engine has no fused path");
+  if (k < 1 || k > kMaxChunks || p_.nx % k != 0)
+    throw std::invalid_argument("plane chunks: 1..8 dividing nx");
+  ensure_chunk_streams(k);
+  chunks_ = k;
 }
 
 void Engine::set_fused(bool on) {
   if (on && !fusable_)
-    throw Error(-1, "fused transforms need a mixed-precision engine on a power-of-two grid whose (y, z) plane "
-                    "fits in shared memory");
+    throw Error(-1, "fused transforms need a mixed-precision engine whose nx, ny, nz are each 16, 32, 48, 64, 96 or "
+                    "128 and whose (y, z) plane fits in shared memory");
   fused_ = on;
 }
 

@@ -78,7 +78,16 @@ class Engine {
   bool fused() const { return fused_; }
   void set_fused(bool on);
   double a_vdw(int m) const { return a_vdw_[m]; }
-  int kernels_per_eval() const { return precision_ == 1 ? (fused_ ? 8 : 6) : 4; }
+  // This library's kernel launches per evaluation (aligned buffers): fused
+  // path rho planes, column pass, chunks_ x (channel planes, pointwise,
+  // derivative planes), column pass, force planes; the cuFFT paths count
+  // their own kernels only.
+  // Plane chunks of the fused path's middle stages (1..kMaxChunks, dividing
+  // nx); std::invalid_argument otherwise or without the fused path.
+  static constexpr int kMaxChunks = 8;
+  void set_chunks(int k);
+  int chunks() const { return chunks_; }
+  int kernels_per_eval() const { return precision_ == 1 ? (fused_ ? 4 + 3 * chunks_ : 6) : 4; }
   // Reads and clears the device error word (synchronises the stream).
   int take_error(cudaStream_t stream);
 
@@ -169,6 +178,7 @@ class Engine {
   // and joined back into the caller's stream, so the FP64 pointwise work of
   // one chunk overlaps the FP32 transforms of another.
   int chunks_ = 1;
+  void ensure_chunk_streams(int k);
   std::vector<cudaStream_t> aux_;
   cudaEvent_t fork_ev_ = nullptr;
   std::vector<cudaEvent_t> join_ev_;

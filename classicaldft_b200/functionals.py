@@ -262,10 +262,13 @@ class Engine:
         b = ctypes.c_int()
         _lib.check(L.cdft_engine_batch(h, ctypes.byref(b)))
         self.batch = b.value
+        self.info = self._query_info()
+
+    def _query_info(self):
         info = (ctypes.c_longlong * 8)()
-        _lib.check(L.cdft_engine_info(h, info))
-        self.info = {"N": info[0], "Nk": info[1], "S": info[2], "channels": info[3], "deriv_channels": info[4],
-                     "precision": info[5], "kernels_per_eval": info[6], "scratch_bytes": info[7]}
+        _lib.check(_lib.lib().cdft_engine_info(self.handle, info))
+        return {"N": info[0], "Nk": info[1], "S": info[2], "channels": info[3], "deriv_channels": info[4],
+                "precision": info[5], "kernels_per_eval": info[6], "scratch_bytes": info[7]}
 
     def close(self):
         if getattr(self, "handle", None):
@@ -328,6 +331,16 @@ class Engine:
             raise ValueError("transforms: 'fused' or 'cufft'")
         _lib.check(_lib.lib().cdft_engine_set_transforms(
             self.handle, _lib.TRANSFORMS_FUSED if which == "fused" else _lib.TRANSFORMS_CUFFT))
+        self.info = self._query_info()
+
+    def set_plane_chunks(self, chunks: int):
+        """Run the fused path's middle stages (inverse plane pass, pointwise,
+        derivative plane pass) as `chunks` groups of x planes on forked
+        streams (1: back to back).  Forces are unchanged; the scalars only
+        by summation order.  ValueError without the fused path or for a
+        count outside 1..8 or not dividing nx."""
+        _lib.check(_lib.lib().cdft_engine_set_plane_chunks(self.handle, int(chunks)))
+        self.info = self._query_info()
 
     def stage_timing(self, on: bool = True):
         """Record CUDA events between the evaluation stages (synchronises each evaluation)."""

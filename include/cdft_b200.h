@@ -463,9 +463,9 @@ CDFT_API int cdft_engine_stage_times(cdft_engine* engine, double ms[CDFT_STAGE_C
 /* Transform implementation of an engine (no reference counterpart; the
  * reference uses FFTW).  CDFT_TRANSFORMS_FUSED: hand-written plane / column
  * FFT kernels with the k-space stages fused into the column pass, available
- * for mixed-precision engines whose nx, ny and nz are each one of 16, 32, 64
- * or 128 (and whose channel tiles fit in shared memory), and the default
- * there.
+ * for mixed-precision engines whose nx, ny and nz are each one of 16, 32,
+ * 48, 64, 96 or 128 (and whose channel tiles fit in shared memory), and the
+ * default there.
  * CDFT_TRANSFORMS_CUFFT: cuFFT plans with separate k-space kernels (every
  * other engine, and the exact HVP always).  Selecting FUSED where it is not
  * available is CDFT_ERR_INVALID. */
@@ -475,6 +475,18 @@ CDFT_API int cdft_engine_set_transforms(cdft_engine* engine, int transforms);
 
 /* The current transform implementation and whether FUSED is available. */
 CDFT_API int cdft_engine_transforms(const cdft_engine* engine, int* transforms, int* fused_available);
+
+/* Plane chunks of the fused path (no reference counterpart; execution
+ * tuning only, results unchanged but for the summation order of the
+ * scalars).  The inverse plane pass, the pointwise stage and the derivative
+ * plane pass run as `chunks` groups of nx / chunks x planes on
+ * engine-owned streams forked from the caller's stream, so one group's FP64
+ * pointwise work overlaps another's FP32 transforms; 1 runs them back to
+ * back.  chunks in 1..CDFT_MAX_PLANE_CHUNKS dividing nx; the default is 4
+ * from nx = 64 on, else 1.  CDFT_ERR_INVALID on an engine without the fused
+ * path or for another count. */
+#define CDFT_MAX_PLANE_CHUNKS 8
+CDFT_API int cdft_engine_set_plane_chunks(cdft_engine* engine, int chunks);
 
 /* Status of earlier asynchronous calls on `stream`: CDFT_ERR_RUNTIME if a
  * bounded device-side wait gave up (the scalars of that call are NaN), else

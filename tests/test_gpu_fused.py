@@ -39,7 +39,11 @@ def test_path_selection():
     assert not odd.weights.engine.fused_available and odd.weights.engine.transforms == "cufft"
     with pytest.raises(ValueError):
         odd.weights.engine.set_transforms("fused")
-    assert g32.weights.engine.info["kernels_per_eval"] == 8
+    # rho planes, column pass, (channel planes, pointwise, derivative planes)
+    # per chunk of x planes (four chunks from nx = 64), column pass, force planes
+    assert g32.weights.engine.info["kernels_per_eval"] == 7
+    g64m = Problem((64, 64, 64), 0.1, [1.0], "WhiteBearII", precision=cd.MIXED)
+    assert g64m.weights.engine.info["kernels_per_eval"] == 16
 
 
 CASES = [
@@ -110,3 +114,29 @@ def test_fused_batch_and_unaligned_buffers():
     # derivative can flip the FP32 rounding of its deviation from the mean
     # (one FP32 ulp of a 5% deviation: ~3e-9 of the force scale)
     assert force_err([buf[2 * N + 3:].cpu().numpy()], ref.forces) <= 1e-8
+
+
+def test_plane_chunks():
+    """The middle stages in 1, 2, 4 or 8 chunks of x planes on forked
+    streams: forces bitwise equal (each point is computed the same way),
+    scalars up to summation order; invalid counts are rejected."""
+    shape = (64, 32, 32)
+    pr = Problem(shape, 0.1, [1.0], "WhiteBearII", inters=[(0, 0) + LJ], kT=0.8, precision=cd.MIXED)
+    rng = np.random.default_rng(5)
+    rho = 0.35 * (1.0 + 0.05 * smooth_noise(shape, rng))
+    e = pr.weights.engine
+    assert e.info["kernels_per_eval"] == 16
+    ref = pr.gpu([rho], [0.2])
+    for k in (1, 2, 8, 4):
+        e.set_plane_chunks(k)
+        assert e.info["kernels_per_eval"] == 4 + 3 * k
+        r = pr.gpu([rho], [0.2])
+        assert np.array_equal(r.forces[0], ref.forces[0]), k
+        assert rel_err(r.free_energy, ref.free_energy) <= 1e-13
+    for bad in (0, 3, 16):
+        with pytest.raises(ValueError):
+            e.set_plane_chunks(bad)
+    cu = Problem((24, 24, 24), 0.2, [1.0], "WhiteBearII", precision=cd.MIXED)
+    with pytest.raises(ValueError):
+        cu.weights.engine.set_plane_chunks(2)
+
