@@ -340,6 +340,8 @@ def sweep_throughput(torch, cd, dev, precision, flush, stream, steps):
             eng = cd.Engine(cd.WhiteBearII(), model, precision, batch=B)
             f = torch.empty((B, N), dtype=torch.float64, device=dev)
             sc = torch.empty((B, 10), dtype=torch.float64, device=dev)
+            if eng.transforms == "fused":
+                eng.autotune(rho[0].data_ptr(), mu=mus[:B], stream=stream.cuda_stream, reps=5)
             calls = SWEEP_BATCH // B
 
             def step():
@@ -373,10 +375,15 @@ def run_ours(args, ws, rank, local, dist):
     dev = torch.device("cuda", local)
     precision = cd.MIXED if args.precision == "mixed" else cd.FP64
     eng, d = _build_engine(cd, precision)
-    if args.plane_chunks:
-        eng.set_plane_chunks(args.plane_chunks)
     rho_h = workload_profile()
     rho = torch.tensor(rho_h, dtype=torch.float64, device=dev)
+    tuned = None
+    if args.plane_chunks:
+        eng.set_plane_chunks(args.plane_chunks)
+    elif eng.transforms == "fused":
+        # the engine's autotuner picks the plane-chunk count on this state
+        k, ms = eng.autotune(rho.data_ptr(), mu=[0.0], reps=10)
+        tuned = {"chosen": k, "ms_per_eval": {str(c): round(t, 5) for c, t in ms.items()}}
     force = torch.empty_like(rho)
     scal = torch.zeros(10, dtype=torch.float64, device=dev)
     flush = L2Flush(torch, dev)
@@ -460,7 +467,8 @@ def run_ours(args, ws, rank, local, dist):
                    "grid": list(SHAPE), "dx": DX, "kT": KT, "rho_bar": RHO_BAR, "noise": "1% uniform, seeded",
                    "hs_diameter": d, "precision": names[precision], "parallelism": f"replicas x{ws}",
                    "l2": "flushed between timed steps (256 MiB write + 256 MiB read, outside the events)",
-                   "transforms": eng.transforms, "plane_chunks": (info["kernels_per_eval"] - 4) // 3 if fused else None},
+                   "transforms": eng.transforms, "plane_chunks": (info["kernels_per_eval"] - 4) // 3 if fused else None,
+                   "autotune": tuned},
         # the dominant kernel (the longest stage of the evaluation): its
         # algorithmic bytes over its live duration; the whole evaluation beside it
         "roofline": {"bound": "hbm", "kernel": top, "achieved": mine[top]["achieved_gbs"], "peak": peak,

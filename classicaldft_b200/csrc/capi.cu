@@ -327,6 +327,16 @@ int cdft_engine_set_plane_chunks(cdft_engine* engine, int chunks) {
   });
 }
 
+int cdft_engine_autotune(cdft_engine* engine, const double* rho, const double* vext, const double* mu,
+                         void* stream, int reps, int* chunks, double* ms) {
+  return guarded([&] {
+    if (!engine || !rho) throw std::invalid_argument("engine and rho are required");
+    if (reps < 1) throw std::invalid_argument("autotune: reps must be positive");
+    const int k = engine->impl->autotune(rho, vext, mu, static_cast<cudaStream_t>(stream), reps, ms);
+    if (chunks) *chunks = k;
+  });
+}
+
 int cdft_engine_transforms(const cdft_engine* engine, int* transforms, int* fused_available) {
   return guarded([&] {
     if (!engine) throw std::invalid_argument("engine is NULL");

@@ -8,9 +8,17 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <type_traits>
 
 namespace cdft {
+
+namespace {
+// The autotuner's choices per engine shape, for the lifetime of the process.
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune_chunks;
+}  // namespace
 
 namespace {
 
@@ -338,6 +346,16 @@ void Engine::setup_fused() {
   fusable_ = true;
   fused_ = true;
   chunks_ = (p.nx >= 64) ? 4 : 1;
+  // shape key of the autotuner's cache: grid, species and diameters, batch,
+  // model, interactions
+  tune_key_ = std::to_string(p.nx) + "x" + std::to_string(p.ny) + "x" + std::to_string(p.nz) + " S" +
+              std::to_string(p.S) + " B" + std::to_string(p.batch) + " m" + std::to_string(p.model) + " M" +
+              std::to_string(p.M);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    const auto it = g_tune_chunks.find(tune_key_);
+    if (it != g_tune_chunks.end()) chunks_ = it->second;
+  }
   ensure_chunk_streams(chunks_);
 }
 
@@ -352,6 +370,48 @@ void Engine::ensure_chunk_streams(int k) {
     join_ev_.push_back(ev);
   }
   if (k > 1 && !fork_ev_) CDFT_CUDA(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
+}
+
+int Engine::autotune(const double* rho, const double* vext, const double* mu, cudaStream_t stream, int reps,
+                     double* ms) {
+  if (ms)
+    for (int k = 0; k < kMaxChunks; ++k) ms[k] = 0.0;
+  if (!fusable_ || !fused_) return chunks_;
+  if (!rho) throw std::invalid_argument("autotune: rho is required");
+  reps = std::max(reps, 1);
+  std::vector<double> mu0((size_t)p_.batch * p_.S, 0.0);
+  if (!mu) mu = mu0.data();
+  const bool timing_was = timing_;
+  timing_ = false;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CDFT_CUDA(cudaEventCreate(&e0));
+  CDFT_CUDA(cudaEventCreate(&e1));
+  int best = chunks_;
+  double best_ms = 0.0;
+  for (int k = 1; k <= kMaxChunks; k *= 2) {
+    if (p_.nx % k != 0) continue;
+    set_chunks(k);
+    for (int w = 0; w < 2; ++w) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
+    CDFT_CUDA(cudaEventRecord(e0, stream));
+    for (int r = 0; r < reps; ++r) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
+    CDFT_CUDA(cudaEventRecord(e1, stream));
+    CDFT_CUDA(cudaEventSynchronize(e1));
+    float t = 0.0f;
+    CDFT_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    const double per = (double)t / reps;
+    if (ms) ms[k - 1] = per;
+    if (best_ms == 0.0 || per < best_ms) {
+      best_ms = per;
+      best = k;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  timing_ = timing_was;
+  set_chunks(best);
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune_chunks[tune_key_] = best;
+  return best;
 }
 
 void Engine::set_chunks(int k) {

@@ -86,6 +86,14 @@ class Engine {
   // nx); std::invalid_argument otherwise or without the fused path.
   static constexpr int kMaxChunks = 8;
   void set_chunks(int k);
+  // Autotuner: times every plane-chunk count (1, 2, 4, 8 dividing nx) on
+  // the caller's state, `reps` evaluations each after two untimed ones, and
+  // keeps the fastest, for this engine and for engines of the same shape
+  // created later in this process.  ms[k - 1]: time per evaluation of count
+  // k (0 where not tried).  Returns the count chosen (the current one when
+  // the engine has no fused path).  Synchronises the stream.
+  int autotune(const double* rho, const double* vext, const double* mu, cudaStream_t stream, int reps,
+               double* ms);
   int chunks() const { return chunks_; }
   int kernels_per_eval() const { return precision_ == 1 ? (fused_ ? 4 + 3 * chunks_ : 6) : 4; }
   // Reads and clears the device error word (synchronises the stream).
@@ -178,6 +186,7 @@ class Engine {
   // and joined back into the caller's stream, so the FP64 pointwise work of
   // one chunk overlaps the FP32 transforms of another.
   int chunks_ = 1;
+  std::string tune_key_;  // shape key of the autotuner's cache
   void ensure_chunk_streams(int k);
   std::vector<cudaStream_t> aux_;
   cudaEvent_t fork_ev_ = nullptr;

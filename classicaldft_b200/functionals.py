@@ -342,6 +342,23 @@ class Engine:
         _lib.check(_lib.lib().cdft_engine_set_plane_chunks(self.handle, int(chunks)))
         self.info = self._query_info()
 
+    def autotune(self, rho_ptr: int, vext_ptr: int = 0, mu=None, stream: int = 0, reps: int = 5):
+        """Time every plane-chunk count of the fused path on a device state
+        (rho_ptr / vext_ptr: device addresses as for total_device) and keep
+        the fastest, also for engines of the same shape created later.
+        Returns (chunks, {count: ms per evaluation})."""
+        chunks = ctypes.c_int()
+        ms = (ctypes.c_double * 8)()
+        mu_arr = None
+        if mu is not None:
+            mu_arr = (ctypes.c_double * (self.batch * self.S))(*[float(m) for m in mu])
+        _lib.check(_lib.lib().cdft_engine_autotune(self.handle, ctypes.c_void_p(rho_ptr),
+                                                   ctypes.c_void_p(vext_ptr or None), mu_arr,
+                                                   ctypes.c_void_p(stream or None), int(reps),
+                                                   ctypes.byref(chunks), ms))
+        self.info = self._query_info()
+        return chunks.value, {k + 1: ms[k] for k in range(8) if ms[k] > 0.0}
+
     def stage_timing(self, on: bool = True):
         """Record CUDA events between the evaluation stages (synchronises each evaluation)."""
         _lib.check(_lib.lib().cdft_engine_stage_timing(self.handle, 1 if on else 0))

@@ -488,6 +488,20 @@ CDFT_API int cdft_engine_transforms(const cdft_engine* engine, int* transforms, 
 #define CDFT_MAX_PLANE_CHUNKS 8
 CDFT_API int cdft_engine_set_plane_chunks(cdft_engine* engine, int chunks);
 
+/* Autotuner (no reference counterpart): times every plane-chunk count (1, 2,
+ * 4, 8 dividing nx) of the fused path on the caller's device state (rho and
+ * vext as for cdft_total_device, vext may be NULL; mu: B*S host values or
+ * NULL for zeros), `reps` evaluations each after two untimed ones, and keeps
+ * the fastest for this engine and for every engine created later in this
+ * process with the same grid, species count, batch, model and interaction
+ * count.  chunks (out, optional): the count chosen.  ms (out, optional,
+ * CDFT_MAX_PLANE_CHUNKS entries): ms[k - 1] is the time per evaluation of
+ * count k, 0 where not tried.  Synchronises the stream; the engine's scratch
+ * force and scalars are overwritten.  An engine without the fused path
+ * returns CDFT_OK, its current count and no timings. */
+CDFT_API int cdft_engine_autotune(cdft_engine* engine, const double* rho, const double* vext, const double* mu,
+                                  void* stream, int reps, int* chunks, double* ms);
+
 /* Status of earlier asynchronous calls on `stream`: CDFT_ERR_RUNTIME if a
  * bounded device-side wait gave up (the scalars of that call are NaN), else
  * CDFT_OK.  Synchronises the stream and clears the flag.  No reference

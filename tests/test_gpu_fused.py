@@ -140,3 +140,31 @@ def test_plane_chunks():
     with pytest.raises(ValueError):
         cu.weights.engine.set_plane_chunks(2)
 
+
+
+def test_autotune():
+    """The autotuner times every plane-chunk count on a device state, keeps
+    the fastest (forces unchanged), and later engines of the same shape start
+    from its choice."""
+    import torch
+    shape = (64, 32, 32)
+    pr = Problem(shape, 0.1, [1.0], "WhiteBearII", inters=[(0, 0) + LJ], kT=0.8, precision=cd.MIXED)
+    rng = np.random.default_rng(6)
+    rho = 0.35 * (1.0 + 0.05 * smooth_noise(shape, rng))
+    e = pr.weights.engine
+    before = pr.gpu([rho], [0.2])
+    rd = torch.tensor(rho.ravel(), device="cuda")
+    k, ms = e.autotune(rd.data_ptr(), mu=[0.2], reps=3)
+    assert sorted(ms) == [1, 2, 4, 8] and all(v > 0.0 for v in ms.values())
+    assert k == min(ms, key=ms.get)
+    assert e.info["kernels_per_eval"] == 4 + 3 * k
+    after = pr.gpu([rho], [0.2])
+    assert np.array_equal(after.forces[0], before.forces[0])
+    assert rel_err(after.free_energy, before.free_energy) <= 1e-13
+    again = cd.make_weights(pr.fmt, pr.model, cd.MIXED)
+    assert again.engine.info["kernels_per_eval"] == 4 + 3 * k
+    # an engine without the fused path: nothing to tune
+    cu = Problem((24, 24, 24), 0.2, [1.0], "WhiteBearII", precision=cd.MIXED)
+    r24 = torch.full((24 ** 3,), 0.3, dtype=torch.float64, device="cuda")
+    k24, ms24 = cu.weights.engine.autotune(r24.data_ptr())
+    assert k24 == 1 and ms24 == {}
