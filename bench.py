@@ -368,6 +368,43 @@ def sweep_throughput(torch, cd, dev, precision, flush, stream, steps):
     return out
 
 
+def fire_step_rates(torch, cd, precision, steps=200):
+    """FIRE minimisation steps per second (problem-steps: problems x steps),
+    each step replayed as a captured CUDA graph and launched kernel by
+    kernel: 16 problems at 48^3 on one batched engine, and one 16^3 problem
+    (launch-bound).  Host-driven loop, timed by the wall clock around it."""
+    import time
+    lj = cd.make_lennard_jones(1.0, 1.0, 2.5)
+    d = lj.hard_sphere_diameter(1.0, cd.WEEKS_CHANDLER_ANDERSEN)
+    rng = np.random.default_rng(SEED + 5)
+    out = {}
+    for n, B in ((48, SWEEP_BATCH), (16, 1)):
+        g = cd.Grid(dx=0.1, box_size=(0.1 * n,) * 3, shape=(n, n, n))
+        model = cd.Model(g, [cd.Species("LJ", d)], [cd.Interaction(0, 0, lj)], 1.0)
+        w = cd.make_weights(cd.FMTModel("WhiteBearII"), model, precision, batch=B)
+        rho0 = 0.6 * (1.0 + 0.01 * rng.uniform(-1.0, 1.0, (B, g.total_points)))
+        mus = list(np.linspace(-1.0, 2.0, B))
+        fire = cd.Fire(dt=0.01, dt_max=0.05, alpha_start=0.1, f_alpha=0.99, force_tolerance=1e-30, max_steps=steps)
+        rate = {}
+        try:
+            for on in (True, False, True, False):
+                cd.set_step_graphs(on)
+                mz = cd.Minimizer(fire=fire, check_interval=50)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                if B > 1:
+                    it = mz.grand_potential_batch(model, w, rho0, mus)[0].iterations
+                else:
+                    it = mz.grand_potential(model, w, rho0[0], mus[0]).iterations
+                torch.cuda.synchronize()
+                rate[on] = B * it / (time.perf_counter() - t0)  # the second run of each mode is kept
+        finally:
+            cd.set_step_graphs(True)
+        out[f"{n}^3 x{B}"] = {"graph_problem_steps_per_s": rate[True], "direct_problem_steps_per_s": rate[False],
+                              "speedup": rate[True] / rate[False]}
+    return out
+
+
 def run_ours(args, ws, rank, local, dist):
     import ctypes
     import torch
@@ -458,6 +495,7 @@ def run_ours(args, ws, rank, local, dist):
     mine = {k: v for k, v in stages.items() if v["kind"] == "engine kernel" and v["algorithmic_bytes"]}
     top = max(mine, key=lambda k: mine[k]["ms"])
     sweep = None if args.no_sweep else sweep_throughput(torch, cd, dev, precision, flush, stream, 20)
+    fire_rates = None if args.no_sweep else fire_step_rates(torch, cd, precision)
     line = {
         "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": ws, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -484,6 +522,7 @@ def run_ours(args, ws, rank, local, dist):
                                    else "one full evaluation (cuFFT transforms + engine kernels)")}},
         "stages": stages,
         "sweep": sweep,
+        "fire_steps": fire_rates,
         names[other]: {"value": ws * n2 / (t2 * 1e-3), "ms_per_step": t2 / n2},
         "mixed_vs_fp64": {"dF_over_F": dF, "max_dforce_over_max_force": dforce},
         "e2e": {"value": e2e_val, "unit": "evals/s", "h2d_bytes_per_step": 8 * info["N"],

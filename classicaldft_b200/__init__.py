@@ -12,6 +12,7 @@ from .functionals import (BARKER_HENDERSON, WEEKS_CHANDLER_ANDERSEN, Engine, EsF
                           make_ten_wolde_frenkel, make_wang_ramirez_dobnikar_frenkel, make_weights, total,
                           total_batch)
 
+from .algorithms import set_step_graphs, step_graphs  # noqa: F401
 from .algorithms import (Bounded, EigenvalueResult, EigenvalueSolver, Fire, FixedMassConstraint,  # noqa: F401
                          MinimizationResult, Minimizer, Picard, PicardResult, ReservoirBoundary, SaddleResult, Search,
                          Simulation, Snapshot, StepConfig, Unbounded, crank_nicholson_step, fixed_mass_constraint,

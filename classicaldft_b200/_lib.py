@@ -166,6 +166,8 @@ def lib():
         "cdft_engine_status": [vp, vp],
         "cdft_engine_set_transforms": [vp, ctypes.c_int],
         "cdft_engine_set_plane_chunks": [vp, ctypes.c_int],
+        "cdft_set_step_graphs": [ctypes.c_int],
+        "cdft_step_graphs": [ctypes.POINTER(ctypes.c_int)],
         "cdft_engine_autotune": [vp, vp, vp, ctypes.POINTER(ctypes.c_double), vp, ctypes.c_int,
                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)],
         "cdft_engine_transforms": [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],

@@ -87,6 +87,19 @@ class MinimizationResult:
     converged: bool
 
 
+def set_step_graphs(on: bool):
+    """Process-wide: the FIRE minimisers capture one step (FIRE update and
+    evaluation) as a CUDA graph and replay it every step (default on;
+    results are identical either way)."""
+    _lib.check(_lib.lib().cdft_set_step_graphs(1 if on else 0))
+
+
+def step_graphs() -> bool:
+    on = ctypes.c_int()
+    _lib.check(_lib.lib().cdft_step_graphs(ctypes.byref(on)))
+    return bool(on.value)
+
+
 @dataclass
 class Minimizer:
     """minimization.hpp:123-147 on the device.

@@ -327,6 +327,17 @@ int cdft_engine_set_plane_chunks(cdft_engine* engine, int chunks) {
   });
 }
 
+int cdft_set_step_graphs(int on) {
+  return guarded([&] { cdft::set_step_graphs(on != 0); });
+}
+
+int cdft_step_graphs(int* on) {
+  return guarded([&] {
+    if (!on) throw std::invalid_argument("on is NULL");
+    *on = cdft::step_graphs() ? 1 : 0;
+  });
+}
+
 int cdft_engine_autotune(cdft_engine* engine, const double* rho, const double* vext, const double* mu,
                          void* stream, int reps, int* chunks, double* ms) {
   return guarded([&] {

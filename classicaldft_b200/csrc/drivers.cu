@@ -3,6 +3,7 @@
 #include "drivers.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
@@ -798,6 +799,10 @@ Drivers::~Drivers() {
     if (snap_done_[i]) cudaEventDestroy(snap_done_[i]);
   }
   if (copy_stream_) cudaStreamDestroy(copy_stream_);
+  reset_step_graph();
+  if (graph_stream_) cudaStreamDestroy(graph_stream_);
+  for (cudaEvent_t e : graph_ev_)
+    if (e) cudaEventDestroy(e);
   if (host_pin_) cudaFreeHost(host_pin_);
   if (ddft_ready_) {
     cufftDestroy(plan_r2c_);
@@ -872,9 +877,52 @@ std::vector<FireResult> Drivers::fire_minimize_batch(const FireConfig& cfg, cons
 // FIRE2 for the B problems of the engine: each step is a fixed sequence of
 // launches over all problems; every control decision is taken per problem
 // on the device (fire.hpp:86-165, minimization.hpp:182-354).
+namespace {
+std::atomic<bool> g_step_graphs{true};
+}  // namespace
+
+void set_step_graphs(bool on) { g_step_graphs.store(on); }
+bool step_graphs() { return g_step_graphs.load(); }
+
+void Drivers::reset_step_graph() {
+  if (step_exec_) cudaGraphExecDestroy(step_exec_);
+  if (step_graph_) cudaGraphDestroy(step_graph_);
+  step_exec_ = nullptr;
+  step_graph_ = nullptr;
+  step_key_ = nullptr;
+}
+
+// The minimiser loop on the caller's stream, or (step graphs on, stage timing
+// off) on the driver's own stream joined to the caller's by events at entry
+// and exit: stream capture needs a stream other than the legacy default one.
 std::vector<FireResult> Drivers::fire_run(const FireConfig& cfg, const double* mu, const double* mass, double* rho,
                                           const double* direction, cudaStream_t stream, Engine* refine,
                                           double refine_switch) {
+  const bool graphs = step_graphs() && !eng_.stage_timing_on() && !(refine && refine->stage_timing_on());
+  if (!graphs) return fire_loop(cfg, mu, mass, rho, direction, stream, refine, refine_switch, false);
+  if (!graph_stream_) {
+    CDFT_CUDA(cudaStreamCreateWithFlags(&graph_stream_, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : graph_ev_) CDFT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  CDFT_CUDA(cudaEventRecord(graph_ev_[0], stream));
+  CDFT_CUDA(cudaStreamWaitEvent(graph_stream_, graph_ev_[0], 0));
+  std::vector<FireResult> out;
+  try {
+    out = fire_loop(cfg, mu, mass, rho, direction, graph_stream_, refine, refine_switch, true);
+  } catch (...) {
+    reset_step_graph();
+    cudaEventRecord(graph_ev_[1], graph_stream_);
+    cudaStreamWaitEvent(stream, graph_ev_[1], 0);
+    throw;
+  }
+  CDFT_CUDA(cudaEventRecord(graph_ev_[1], graph_stream_));
+  CDFT_CUDA(cudaStreamWaitEvent(stream, graph_ev_[1], 0));
+  return out;
+}
+
+std::vector<FireResult> Drivers::fire_loop(const FireConfig& cfg, const double* mu, const double* mass, double* rho,
+                                           const double* direction, cudaStream_t stream, Engine* refine,
+                                           double refine_switch, bool graphs) {
   const EvalParams& p = eng_.params();
   const int B = B_;
   Vec a;
@@ -912,6 +960,7 @@ std::vector<FireResult> Drivers::fire_run(const FireConfig& cfg, const double* m
   const int rt = 32 * kRedTerms;
 
   Engine* eng = &eng_;
+  reset_step_graph();  // a graph holds this call's arguments
   auto compute = [&](int initial) {
     // rescale (fixed mass / saddle), evaluate, post-process into f
     k_density_sums<<<gv, kBlock, 0, stream>>>(a, red_);
@@ -965,7 +1014,8 @@ std::vector<FireResult> Drivers::fire_run(const FireConfig& cfg, const double* m
       refining = true;
     }
     const int chunk = std::max(1, std::min(cfg.check_interval, fp.max_steps - steps));
-    for (int k = 0; k < chunk; ++k) {
+    // one FIRE step (fire.hpp:86-165): the v and x updates, then compute
+    auto step = [&] {
       k_power<<<gv, kBlock, 0, stream>>>(a, red_);
       k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
       k_fire_control1<<<B, 32, 0, stream>>>(st_, red_out_, fp);
@@ -974,6 +1024,29 @@ std::vector<FireResult> Drivers::fire_run(const FireConfig& cfg, const double* m
       k_fire_ratio<<<B, 32, 0, stream>>>(st_, red_out_);
       k_fire_xstep<<<gv, kBlock, 0, stream>>>(a, st_);
       compute(0);
+    };
+    if (graphs && step_key_ != eng) {
+      // (re)capture the step for the engine now evaluating; every kernel
+      // argument of a step is the same from one step to the next
+      reset_step_graph();
+      CDFT_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        step();
+      } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      CDFT_CUDA(cudaStreamEndCapture(stream, &step_graph_));
+      CDFT_CUDA(cudaGraphInstantiate(&step_exec_, step_graph_, 0));
+      step_key_ = eng;
+    }
+    for (int k = 0; k < chunk; ++k) {
+      if (graphs)
+        CDFT_CUDA(cudaGraphLaunch(step_exec_, stream));
+      else
+        step();
     }
     CDFT_CUDA(cudaGetLastError());
     steps += chunk;

@@ -69,6 +69,11 @@ struct FireResult {
   bool uphill_error = false;
 };
 
+// Process-wide switch: the minimisers replay each step as a captured CUDA
+// graph (default on; results are the same either way).
+void set_step_graphs(bool on);
+bool step_graphs();
+
 class Drivers {
  public:
   explicit Drivers(Engine& engine);
@@ -214,6 +219,17 @@ class Drivers {
   std::vector<FireResult> fire_run(const FireConfig& cfg, const double* mu, const double* mass, double* rho,
                                    const double* direction, cudaStream_t stream, Engine* refine,
                                    double refine_switch);
+  std::vector<FireResult> fire_loop(const FireConfig& cfg, const double* mu, const double* mass, double* rho,
+                                    const double* direction, cudaStream_t stream, Engine* refine,
+                                    double refine_switch, bool graphs);
+  // CUDA graph of one FIRE step (captured on graph_stream_, replayed per
+  // step; recaptured when the evaluating engine changes)
+  cudaStream_t graph_stream_ = nullptr;
+  cudaEvent_t graph_ev_[2] = {};
+  cudaGraph_t step_graph_ = nullptr;
+  cudaGraphExec_t step_exec_ = nullptr;
+  const void* step_key_ = nullptr;
+  void reset_step_graph();
 
   Engine& eng_;
   long long N_ = 0;

@@ -95,6 +95,7 @@ class Engine {
   int autotune(const double* rho, const double* vext, const double* mu, cudaStream_t stream, int reps,
                double* ms);
   int chunks() const { return chunks_; }
+  bool stage_timing_on() const { return timing_; }
   int kernels_per_eval() const { return precision_ == 1 ? (fused_ ? 4 + 3 * chunks_ : 6) : 4; }
   // Reads and clears the device error word (synchronises the stream).
   int take_error(cudaStream_t stream);

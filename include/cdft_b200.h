@@ -502,6 +502,15 @@ CDFT_API int cdft_engine_set_plane_chunks(cdft_engine* engine, int chunks);
 CDFT_API int cdft_engine_autotune(cdft_engine* engine, const double* rho, const double* vext, const double* mu,
                                   void* stream, int reps, int* chunks, double* ms);
 
+/* Step graphs (no reference counterpart; execution mode, process-wide): the
+ * FIRE minimisers (cdft_minimize, cdft_minimize_batch, the saddle search's
+ * FIRE) capture one step (the FIRE update and the evaluation) as a CUDA graph
+ * and replay it every step, on a driver-owned stream joined to the caller's
+ * stream by events.  On by default; results are identical either way.  Off
+ * while an engine records stage timings. */
+CDFT_API int cdft_set_step_graphs(int on);
+CDFT_API int cdft_step_graphs(int* on);
+
 /* Status of earlier asynchronous calls on `stream`: CDFT_ERR_RUNTIME if a
  * bounded device-side wait gave up (the scalars of that call are NaN), else
  * CDFT_OK.  Synchronises the stream and clears the flag.  No reference

@@ -177,3 +177,30 @@ def test_mixed_minimisation_with_fp64_refinement():
     assert a.converged and b.converged
     assert np.max(np.abs(a.densities[0] - b.densities[0])) <= 1e-8
     assert b.grand_potential == pytest.approx(a.grand_potential, rel=1e-10)
+
+
+@pytest.mark.parametrize("precision", [cd.FP64, cd.MIXED])
+def test_fire_step_graphs_match_direct_launches(precision):
+    """Each FIRE step replayed as a captured CUDA graph gives the same
+    minimisation, bit for bit, as launching its kernels one by one (the
+    mixed case includes the FP64 refinement engine, whose switch recaptures
+    the step, and the fused path's forked plane-chunk streams)."""
+    pr = problem(precision=precision)
+    pr64 = problem() if precision == cd.MIXED else None
+    rng = np.random.default_rng(9)
+    rho0 = 0.4 * (1.0 + 0.05 * smooth_noise(SHAPE, rng))
+    fire = dict(dt=0.05, dt_max=0.5, alpha_start=0.01, f_alpha=0.99, force_tolerance=1e-10, max_steps=3000)
+    kw = dict(refine=pr64.weights, refine_switch=1e3) if pr64 else {}
+    out = {}
+    assert cd.step_graphs()
+    try:
+        for on in (True, False):
+            cd.set_step_graphs(on)
+            out[on] = cd.Minimizer(fire=cd.Fire(**fire), **kw).grand_potential(pr.model, pr.weights, rho0, 1.5)
+    finally:
+        cd.set_step_graphs(True)
+    assert out[True].converged and out[False].converged
+    assert out[True].iterations == out[False].iterations
+    assert np.array_equal(out[True].densities[0], out[False].densities[0])
+    assert out[True].grand_potential == out[False].grand_potential
+
