@@ -800,6 +800,7 @@ Drivers::~Drivers() {
   }
   if (copy_stream_) cudaStreamDestroy(copy_stream_);
   reset_step_graph();
+  reset_fp_graph();
   if (graph_stream_) cudaStreamDestroy(graph_stream_);
   for (cudaEvent_t e : graph_ev_)
     if (e) cudaEventDestroy(e);
@@ -884,6 +885,19 @@ std::atomic<bool> g_step_graphs{true};
 void set_step_graphs(bool on) { g_step_graphs.store(on); }
 bool step_graphs() { return g_step_graphs.load(); }
 
+void Drivers::ensure_graph_stream() {
+  if (graph_stream_) return;
+  CDFT_CUDA(cudaStreamCreateWithFlags(&graph_stream_, cudaStreamNonBlocking));
+  for (cudaEvent_t& e : graph_ev_) CDFT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+}
+
+void Drivers::reset_fp_graph() {
+  if (fp_exec_) cudaGraphExecDestroy(fp_exec_);
+  if (fp_graph_) cudaGraphDestroy(fp_graph_);
+  fp_exec_ = nullptr;
+  fp_graph_ = nullptr;
+}
+
 void Drivers::reset_step_graph() {
   if (step_exec_) cudaGraphExecDestroy(step_exec_);
   if (step_graph_) cudaGraphDestroy(step_graph_);
@@ -900,10 +914,7 @@ std::vector<FireResult> Drivers::fire_run(const FireConfig& cfg, const double* m
                                           double refine_switch) {
   const bool graphs = step_graphs() && !eng_.stage_timing_on() && !(refine && refine->stage_timing_on());
   if (!graphs) return fire_loop(cfg, mu, mass, rho, direction, stream, refine, refine_switch, false);
-  if (!graph_stream_) {
-    CDFT_CUDA(cudaStreamCreateWithFlags(&graph_stream_, cudaStreamNonBlocking));
-    for (cudaEvent_t& e : graph_ev_) CDFT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  }
+  ensure_graph_stream();
   CDFT_CUDA(cudaEventRecord(graph_ev_[0], stream));
   CDFT_CUDA(cudaStreamWaitEvent(graph_stream_, graph_ev_[0], 0));
   std::vector<FireResult> out;
@@ -1093,7 +1104,30 @@ void Drivers::ensure_ddft() {
   ddft_ready_ = true;
 }
 
+// The step on the caller's stream, or (step graphs on) on the driver's
+// stream, joined to the caller's by events, with each fixed-point iteration
+// replayed as a captured CUDA graph.
 double Drivers::ddft_step(DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations) {
+  const bool graphs = step_graphs() && !eng_.stage_timing_on();
+  if (!graphs) return ddft_step_on(cfg, rho, stream, fp_iterations, false);
+  ensure_graph_stream();
+  CDFT_CUDA(cudaEventRecord(graph_ev_[0], stream));
+  CDFT_CUDA(cudaStreamWaitEvent(graph_stream_, graph_ev_[0], 0));
+  double e = 0.0;
+  try {
+    e = ddft_step_on(cfg, rho, graph_stream_, fp_iterations, true);
+  } catch (...) {
+    reset_fp_graph();
+    cudaEventRecord(graph_ev_[1], graph_stream_);
+    cudaStreamWaitEvent(stream, graph_ev_[1], 0);
+    throw;
+  }
+  CDFT_CUDA(cudaEventRecord(graph_ev_[1], graph_stream_));
+  CDFT_CUDA(cudaStreamWaitEvent(stream, graph_ev_[1], 0));
+  return e;
+}
+
+double Drivers::ddft_step_on(DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations, bool graphs) {
   ensure_ddft();
   const EvalParams& p = eng_.params();
   CDFT_CUFFT(cufftSetStream(plan_r2c_, stream));
@@ -1116,8 +1150,9 @@ double Drivers::ddft_step(DDFTConfig& cfg, double* rho, cudaStream_t stream, int
     const double dt = cfg.dt;
     CDFT_CUDA(cudaMemcpyAsync(d1, rho, sizeof(double) * N_, cudaMemcpyDeviceToDevice, stream));
     double deviation = 1e30;
-    for (int it = 0; it < cfg.fp_max_iterations; ++it) {
-      ++total_it;
+    // one fixed-point iteration (dynamics.hpp:362-389); its arguments are
+    // the driver's buffers, dt and mu
+    auto iteration = [&] {
       eng_.evaluate(d1, nullptr, &mu, f1, scalars_, stream);
       k_ddft_rhs<<<grid_, kBlock, 0, stream>>>(d1, f1, rhs, p.nx, p.ny, p.nz, p.dx, 1.0 / p.dv);
       CDFT_CUFFT(cufftExecD2Z(plan_r2c_, rhs, work));
@@ -1126,6 +1161,31 @@ double Drivers::ddft_step(DDFTConfig& cfg, double* rho, cudaStream_t stream, int
       k_ddft_update<<<grid_, kBlock, 0, stream>>>(tmp2_, d1, N_, 1.0 / (double)N_, red_);
       k_maxmin_finish<<<1, 32, 0, stream>>>(red_, grid_, red_out_);
       CDFT_CUDA(cudaMemcpyAsync(host_pin_, red_out_, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+    };
+    const int path = (eng_.fused() ? 16 : 0) + eng_.chunks();
+    if (graphs && !(fp_exec_ && fp_dt_ == dt && fp_mu_ == mu && fp_path_ == path)) {
+      reset_fp_graph();
+      CDFT_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        iteration();
+      } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      CDFT_CUDA(cudaStreamEndCapture(stream, &fp_graph_));
+      CDFT_CUDA(cudaGraphInstantiate(&fp_exec_, fp_graph_, 0));
+      fp_dt_ = dt;
+      fp_mu_ = mu;
+      fp_path_ = path;
+    }
+    for (int it = 0; it < cfg.fp_max_iterations; ++it) {
+      ++total_it;
+      if (graphs)
+        CDFT_CUDA(cudaGraphLaunch(fp_exec_, stream));
+      else
+        iteration();
       CDFT_CUDA(cudaStreamSynchronize(stream));
       const double old = deviation;
       deviation = host_pin_[0];

@@ -230,6 +230,14 @@ class Drivers {
   cudaGraphExec_t step_exec_ = nullptr;
   const void* step_key_ = nullptr;
   void reset_step_graph();
+  void ensure_graph_stream();
+  // CUDA graph of one DDFT fixed-point iteration (its arguments: dt, mu)
+  cudaGraph_t fp_graph_ = nullptr;
+  cudaGraphExec_t fp_exec_ = nullptr;
+  double fp_dt_ = 0.0, fp_mu_ = 0.0;
+  int fp_path_ = 0;  // the engine's transforms and plane chunks at capture
+  void reset_fp_graph();
+  double ddft_step_on(DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations, bool graphs);
 
   Engine& eng_;
   long long N_ = 0;

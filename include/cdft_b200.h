@@ -505,8 +505,9 @@ CDFT_API int cdft_engine_autotune(cdft_engine* engine, const double* rho, const 
 /* Step graphs (no reference counterpart; execution mode, process-wide): the
  * FIRE minimisers (cdft_minimize, cdft_minimize_batch, the saddle search's
  * FIRE) capture one step (the FIRE update and the evaluation) as a CUDA graph
- * and replay it every step, on a driver-owned stream joined to the caller's
- * stream by events.  On by default; results are identical either way.  Off
+ * and replay it every step, and the DDFT integrating-factor step
+ * (cdft_ddft_step, cdft_ddft_simulate) each fixed-point iteration, on a
+ * driver-owned stream joined to the caller's stream by events.  On by default; results are identical either way.  Off
  * while an engine records stage timings. */
 CDFT_API int cdft_set_step_graphs(int on);
 CDFT_API int cdft_step_graphs(int* on);
