@@ -123,14 +123,38 @@ __global__ void __launch_bounds__(NT)
     // rho (FP64): one read of the plane into registers, its mean (a
     // fixed-order block sum, recorded for the column pass), rho - mean in
     // FP32 into shared memory as the real plane (pairs E[y * M + n])
+    // each thread takes pairs of consecutive samples (PER even): one 16-byte
+    // load each where rho is 16-byte aligned, two 8-byte loads otherwise
+    // (the same samples and summation order either way)
     constexpr int PER = NY * NZ / NT;
     static_assert(PER * NT == NY * NZ, "plane samples per thread");
+    constexpr bool PAIRS = PER % 2 == 0;
     double v[PER];
     double sum = 0.0;
+    if constexpr (PAIRS) {
+      if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+        const double2* src2 = reinterpret_cast<const double2*>(src);
 #pragma unroll
-    for (int j = 0; j < PER; ++j) {
-      v[j] = src[threadIdx.x + j * NT];  // the caller's buffer: scalar loads
-      sum += v[j];
+        for (int j = 0; j < PER / 2; ++j) {
+          const double2 d = src2[threadIdx.x + j * NT];
+          v[2 * j] = d.x;
+          v[2 * j + 1] = d.y;
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < PER / 2; ++j) {
+          v[2 * j] = src[2 * (threadIdx.x + j * NT)];
+          v[2 * j + 1] = src[2 * (threadIdx.x + j * NT) + 1];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < PER / 2; ++j) sum += v[2 * j] + v[2 * j + 1];
+    } else {
+#pragma unroll
+      for (int j = 0; j < PER; ++j) {
+        v[j] = src[threadIdx.x + j * NT];
+        sum += v[j];
+      }
     }
     __shared__ double s_warp[NT / 32];
     __shared__ double s_mean;
@@ -147,9 +171,16 @@ __global__ void __launch_bounds__(NT)
     }
     __syncthreads();
     const double c = s_mean;
-    float* Ef = reinterpret_cast<float*>(E);
+    if constexpr (PAIRS) {
+      float2* Ef2 = reinterpret_cast<float2*>(E);
 #pragma unroll
-    for (int j = 0; j < PER; ++j) Ef[threadIdx.x + j * NT] = (float)(v[j] - c);
+      for (int j = 0; j < PER / 2; ++j)
+        Ef2[threadIdx.x + j * NT] = make_float2((float)(v[2 * j] - c), (float)(v[2 * j + 1] - c));
+    } else {
+      float* Ef = reinterpret_cast<float*>(E);
+#pragma unroll
+      for (int j = 0; j < PER; ++j) Ef[threadIdx.x + j * NT] = (float)(v[j] - c);
+    }
     __syncthreads();
   } else {
     // a derivative channel (FP32, the engine's buffer): the plane arrives in
@@ -400,6 +431,9 @@ __global__ void __launch_bounds__(NT)
   const long long plane_off = ((long long)b * (EPI ? p.S : nseq) + sq) * p.N + (long long)ix * NY * NZ;
   double cst = 0.0;
   if constexpr (EPI) cst = s_const;
+  // a 16-byte aligned force takes each sample pair in one load and one store
+  // (plane_off and 2 n are even)
+  const bool pairs = EPI && (reinterpret_cast<uintptr_t>(force) & 15) == 0;
   for (int t = threadIdx.x; t < P::T_Z_NAT; t += NT) {
     const int n2 = t % BZ, y = t / BZ;
     cpx a[AZ];
@@ -410,9 +444,16 @@ __global__ void __launch_bounds__(NT)
     for (int n1 = 0; n1 < AZ; ++n1) {
       const int n = BZ * n1 + n2;
       if constexpr (EPI) {
-        double* f = force + plane_off + (long long)y * NZ + 2 * n;  // the caller's buffer: 8-byte alignment
-        f[0] = f[0] + (double)(2.0f * a[n1].x) * p.dv + cst;
-        f[1] = f[1] + (double)(2.0f * a[n1].y) * p.dv + cst;
+        double* f = force + plane_off + (long long)y * NZ + 2 * n;
+        if (pairs) {
+          double2 fv = *reinterpret_cast<const double2*>(f);
+          fv.x = fv.x + (double)(2.0f * a[n1].x) * p.dv + cst;
+          fv.y = fv.y + (double)(2.0f * a[n1].y) * p.dv + cst;
+          *reinterpret_cast<double2*>(f) = fv;
+        } else {  // the caller's buffer, 8-byte aligned only
+          f[0] = f[0] + (double)(2.0f * a[n1].x) * p.dv + cst;
+          f[1] = f[1] + (double)(2.0f * a[n1].y) * p.dv + cst;
+        }
       } else {
         *reinterpret_cast<float2*>(out_f + plane_off + (long long)y * NZ + 2 * n) =
             make_float2(2.0f * a[n1].x, 2.0f * a[n1].y);
