@@ -116,6 +116,33 @@ CDFT_HD cpx c2r_pre_2d_dc(cpx x0, cpx x0m, cpx xM, cpx xMm) {
   return scale(p0 + pm, 0.5f) + mul_i(scale(p0 - pm, 0.5f));
 }
 
+// Mirror-pair units of a forward plane pass's y-spectrum tasks (kz, k1),
+// kz < M, k1 < AY, each task holding Z[k1 + AY k2][kz] for k2 < BY.  The
+// post-processing of element (ky, kz) needs its mirror (-ky, M - kz mod M),
+// which lies in task ((M - kz) mod M, (AY - k1) mod AY).  Unit u < M AY / 2
+// is a task A and the task B holding the mirrors of A's elements (and A
+// those of B's), or, for the four self-mirrored tasks (kz in {0, M/2}, k1
+// in {0, AY/2}), two of them side by side (self = true), so one thread
+// finishes a unit without an exchange.  M and AY even.
+struct MirrorUnit {
+  int kzA, k1A, kzB, k1B;
+  bool self;
+};
+CDFT_HD MirrorUnit mirror_unit(int u, int M, int AY) {
+  const int half = M / 2, c = u % half, r = u / half;
+  MirrorUnit m;
+  if (c != 0) {
+    m.kzA = c, m.k1A = r, m.kzB = M - c, m.k1B = (AY - r) % AY, m.self = false;
+  } else {
+    const int kz = r < AY / 2 ? 0 : half, rr = r < AY / 2 ? r : r - AY / 2;
+    m.kzA = kz, m.kzB = kz, m.k1A = rr, m.self = rr == 0;
+    m.k1B = rr == 0 ? AY / 2 : AY - rr;
+  }
+  return m;
+}
+// Index, in the task holding it, of the mirror of element k2 of a task k1.
+CDFT_HD int mirror_k2(int k1, int k2, int BY) { return k1 == 0 ? (BY - k2) % BY : BY - 1 - k2; }
+
 // Real-to-half-complex post-processing on the y-spectrum: Z[ky][kz] (kz <
 // M) is the forward y transform of the rows' forward length-M transforms of
 // z[n] = x[2n] + i x[2n+1]; X[ky][kz] for kz in 1..M-1 from Z[ky][kz] and

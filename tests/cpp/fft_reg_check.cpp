@@ -157,6 +157,54 @@ void fr_plane_forward(int ny, int nz, const double* real, double* out_re, double
   }
 }
 
+// The forward plane pass with the post-processing done per mirror unit
+// (F::mirror_unit) from the tasks' y-spectrum columns, as the kernel's
+// threads do; every output element written exactly once (count[] checks).
+int fr_plane_forward_units(int ny, int nz, const double* real, double* out_re, double* out_im) {
+  const int M = nz / 2, ld = M + 1;
+  const int AY = F::split_a(ny), BY = ny / AY;
+  std::vector<cpx> Z((size_t)ny * M);
+  for (int y = 0; y < ny; ++y)
+    for (int n = 0; n < M; ++n)
+      Z[(size_t)y * M + n] = {(float)real[(size_t)y * nz + 2 * n], (float)real[(size_t)y * nz + 2 * n + 1]};
+  const auto twz = table(M), tw2 = table(nz), twy = table(ny);
+  for (int y = 0; y < ny; ++y) transform_rt<false>(M, &Z[(size_t)y * M], 1, false, twz.data());
+  for (int kz = 0; kz < M; ++kz) transform_rt<false>(ny, &Z[kz], M, false, twy.data());
+  std::vector<int> count((size_t)ny * ld, 0);
+  auto task = [&](int kz, int k1, std::vector<cpx>& z) {
+    z.resize(BY);
+    for (int k2 = 0; k2 < BY; ++k2) z[k2] = Z[(size_t)(k1 + AY * k2) * M + kz];
+  };
+  auto post = [&](const std::vector<cpx>& zt, const std::vector<cpx>& zp, int k1, int kz) {
+    for (int k2 = 0; k2 < BY; ++k2) {
+      const int ky = k1 + AY * k2;
+      const cpx zm = zp[F::mirror_k2(k1, k2, BY)];
+      if (kz == 0) {
+        cpx x0, xM;
+        F::r2c_post_2d_dc(zt[k2], zm, x0, xM);
+        out_re[(size_t)ky * ld] = x0.x, out_im[(size_t)ky * ld] = x0.y;
+        out_re[(size_t)ky * ld + M] = xM.x, out_im[(size_t)ky * ld + M] = xM.y;
+        ++count[(size_t)ky * ld], ++count[(size_t)ky * ld + M];
+      } else {
+        const cpx v = F::r2c_post_2d(zt[k2], zm, tw2[kz]);
+        out_re[(size_t)ky * ld + kz] = v.x, out_im[(size_t)ky * ld + kz] = v.y;
+        ++count[(size_t)ky * ld + kz];
+      }
+    }
+  };
+  std::vector<cpx> za, zb;
+  for (int u = 0; u < M * AY / 2; ++u) {
+    const F::MirrorUnit m = F::mirror_unit(u, M, AY);
+    task(m.kzA, m.k1A, za);
+    task(m.kzB, m.k1B, zb);
+    post(za, m.self ? za : zb, m.k1A, m.kzA);
+    post(zb, m.self ? zb : za, m.k1B, m.kzB);
+  }
+  for (int c : count)
+    if (c != 1) return 0;
+  return 1;
+}
+
 // The inverse plane pass (unnormalised C2R of the Hermitian projection):
 // pre-processing on the y-spectrum, inverse y transforms of the M packed
 // columns, inverse z transforms of the rows, samples doubled.

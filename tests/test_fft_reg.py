@@ -29,6 +29,7 @@ def lib(tmp_path_factory):
     L.fr_plane_forward.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dp]
     L.fr_plane_inverse.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dp]
     L.fr_dft_half.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp]
+    L.fr_plane_forward_units.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dp]
     return L
 
 
@@ -84,3 +85,19 @@ def test_plane_r2c_and_c2r_on_the_y_spectrum(lib, ny, nz):
     lib.fr_plane_inverse(ny, nz, ptr(np.ascontiguousarray(Y.real.reshape(-1))),
                          ptr(np.ascontiguousarray(Y.imag.reshape(-1))), ptr(out))
     assert err(out.reshape(ny, nz), np.fft.irfft2(Y, s=(ny, nz)) * ny * nz) <= TOL
+
+
+@pytest.mark.parametrize("ny,nz", [(16, 16), (32, 64), (128, 128), (48, 48), (96, 96), (48, 128), (16, 96)])
+def test_plane_forward_mirror_units(lib, ny, nz):
+    """The forward plane pass's post-processing per mirror unit (a task and
+    the task holding its mirrors, or two self-mirrored tasks) writes every
+    output once and equals the element-by-element post-processing."""
+    rng = np.random.default_rng(ny * 7 + nz)
+    x = rng.standard_normal((ny, nz))
+    ld = nz // 2 + 1
+    a_re, a_im = np.zeros((ny, ld)), np.zeros((ny, ld))
+    lib.fr_plane_forward(ny, nz, ptr(x), ptr(a_re), ptr(a_im))
+    b_re, b_im = np.zeros((ny, ld)), np.zeros((ny, ld))
+    assert lib.fr_plane_forward_units(ny, nz, ptr(x), ptr(b_re), ptr(b_im)) == 1
+    assert np.array_equal(a_re, b_re) and np.array_equal(a_im, b_im)
+
