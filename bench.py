@@ -122,10 +122,10 @@ class L2Flush:
 # dram__bytes_write.sum over the seven launches of one evaluation, 128^3
 # mixed, fused transforms, middle stages in one plane chunk); the launch
 # list is summarised in profiles/eval_128cubed_mixed_launches.md.
-MEASURED_TRAFFIC = {"mixed": 618.5e6}
+MEASURED_TRAFFIC = {"mixed": 617.8e6}
 # The same capture per launch of each fused-path stage (bytes).
-MEASURED_STAGE_TRAFFIC = {"plane_fwd_rho": 16.79e6, "col_fwd": 64.78e6, "plane_inv_channels": 137.39e6,
-                          "pointwise": 156.50e6, "plane_fwd_derivatives": 115.17e6, "col_bwd": 102.54e6,
+MEASURED_STAGE_TRAFFIC = {"plane_fwd_rho": 16.79e6, "col_fwd": 64.87e6, "plane_inv_channels": 136.43e6,
+                          "pointwise": 156.49e6, "plane_fwd_derivatives": 114.92e6, "col_bwd": 102.91e6,
                           "plane_inv_epilogue": 25.36e6}
 
 
