@@ -1,8 +1,8 @@
 // Kernels of the fused transform path on register-resident transforms
 // (fft_reg.cuh).  A length-N transform is two in-register DFTs (A and B
 // points) with one shared-memory exchange between them; a plane pass is a
-// y transform and a z transform (four exchanges at most, with the
-// half-complex steps on the y-spectrum), a column pass one x transform per
+// y transform and a z transform (three exchanges, with the half-complex
+// steps on the y-spectrum), a column pass one x transform per
 // array.  The passes and their arrays are those of the stage-by-stage
 // kernels they replace:
 //
@@ -264,79 +264,39 @@ __global__ void __launch_bounds__(NT)
   }
   __syncthreads();
   cpx* dst = out + ((long long)b * nseq + sq) * p.Nk + (long long)ix * NY * LD;
-  if constexpr (NT == P::NT) {
-    // y, second half per mirror unit (fft::mirror_unit): the thread takes a
-    // task and the task holding its elements' mirrors and post-processes
-    // both from registers, with no further exchange
-    for (int u = threadIdx.x; u < P::T_Y_SPEC / 2; u += NT) {
-      const fft::MirrorUnit mu = fft::mirror_unit(u, M, AY);
-      cpx za[BY], zb[BY];
+  // y, second half per mirror unit (fft::mirror_unit): the thread takes a
+  // task and the task holding its elements' mirrors and post-processes
+  // both from registers, with no further exchange
+  for (int u = threadIdx.x; u < P::T_Y_SPEC / 2; u += NT) {
+    const fft::MirrorUnit mu = fft::mirror_unit(u, M, AY);
+    cpx za[BY], zb[BY];
 #pragma unroll
-      for (int n2 = 0; n2 < BY; ++n2) {
-        za[n2] = E[(n2 * AY + mu.k1A) * EY + mu.kzA];
-        zb[n2] = E[(n2 * AY + mu.k1B) * EY + mu.kzB];
-      }
-      fft::nat_out<NY, false>(za);
-      fft::nat_out<NY, false>(zb);
-      auto post = [&](const cpx(&zt)[BY], const cpx(&zo)[BY], int k1, int kz) {
+    for (int n2 = 0; n2 < BY; ++n2) {
+      za[n2] = E[(n2 * AY + mu.k1A) * EY + mu.kzA];
+      zb[n2] = E[(n2 * AY + mu.k1B) * EY + mu.kzB];
+    }
+    fft::nat_out<NY, false>(za);
+    fft::nat_out<NY, false>(zb);
+    auto post = [&](const cpx(&zt)[BY], const cpx(&zo)[BY], int k1, int kz) {
 #pragma unroll
-        for (int k2 = 0; k2 < BY; ++k2) {
-          const int ky = k1 + AY * k2;
-          // the mirror: element mirror_k2(k1, k2) of the partner task
-          const cpx m0 = mu.self ? zt[(BY - k2) % BY] : zo[(BY - k2) % BY];
-          const cpx m1 = mu.self ? zt[BY - 1 - k2] : zo[BY - 1 - k2];
-          const cpx zm = k1 == 0 ? m0 : m1;
-          if (kz == 0) {
-            cpx x0, xM;
-            fft::r2c_post_2d_dc(zt[k2], zm, x0, xM);
-            dst[ky * LD] = x0;
-            dst[ky * LD + M] = xM;
-          } else {
-            dst[ky * LD + kz] = fft::r2c_post_2d(zt[k2], zm, t2[kz]);
-          }
+      for (int k2 = 0; k2 < BY; ++k2) {
+        const int ky = k1 + AY * k2;
+        // the mirror: element mirror_k2(k1, k2) of the partner task
+        const cpx m0 = mu.self ? zt[(BY - k2) % BY] : zo[(BY - k2) % BY];
+        const cpx m1 = mu.self ? zt[BY - 1 - k2] : zo[BY - 1 - k2];
+        const cpx zm = k1 == 0 ? m0 : m1;
+        if (kz == 0) {
+          cpx x0, xM;
+          fft::r2c_post_2d_dc(zt[k2], zm, x0, xM);
+          dst[ky * LD] = x0;
+          dst[ky * LD + M] = xM;
+        } else {
+          dst[ky * LD + kz] = fft::r2c_post_2d(zt[k2], zm, t2[kz]);
         }
-      };
-      post(za, zb, mu.k1A, mu.kzA);
-      post(zb, za, mu.k1B, mu.kzB);
-    }
-  } else {
-    // the one-sequence (wide) pass: y second half per task, then the
-    // post-processing per element through one more exchange
-    constexpr int H3 = cdiv(P::T_Y_SPEC, NT);
-    cpx h3[H3][BY];
-#pragma unroll
-    for (int j = 0; j < H3; ++j) {
-      const int t = threadIdx.x + j * NT;
-      if (t < P::T_Y_SPEC) {
-        const int kz = t % M, k1 = t / M;
-#pragma unroll
-        for (int n2 = 0; n2 < BY; ++n2) h3[j][n2] = E[(n2 * AY + k1) * EY + kz];
-        fft::nat_out<NY, false>(h3[j]);
       }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < H3; ++j) {
-      const int t = threadIdx.x + j * NT;
-      if (t < P::T_Y_SPEC) {
-        const int kz = t % M, k1 = t / M;
-#pragma unroll
-        for (int k2 = 0; k2 < BY; ++k2) E[(k1 + AY * k2) * ER + kz] = h3[j][k2];
-      }
-    }
-    __syncthreads();
-    // half-complex post-processing on the y-spectrum, stored in natural order
-    for (int t = threadIdx.x; t < NY * M; t += NT) {
-      const int kz = t % M, ky = t / M, km = (NY - ky) % NY;
-      if (kz == 0) {
-        cpx x0, xM;
-        fft::r2c_post_2d_dc(E[ky * ER], E[km * ER], x0, xM);
-        dst[ky * LD] = x0;
-        dst[ky * LD + M] = xM;
-      } else {
-        dst[ky * LD + kz] = fft::r2c_post_2d(E[ky * ER + kz], E[km * ER + (M - kz)], t2[kz]);
-      }
-    }
+    };
+    post(za, zb, mu.k1A, mu.kzA);
+    post(zb, za, mu.k1B, mu.kzB);
   }
 }
 
