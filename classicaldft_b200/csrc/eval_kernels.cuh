@@ -587,13 +587,47 @@ __device__ __forceinline__ void point_body(const EvalParams& p, const PointwiseA
 #pragma unroll
   for (int c = 0; c < NF; ++c) n[c] = cur[c] + (SPLIT ? s_off[c] : 0.0);
   Measures<double> m;
-  assemble<MULTI, TENSOR>(p, n, m);
   double phi = 0.0;
   MeasureDerivs<double> dm;
   double D[NF];
-  if (fmt_phi_dphi<MODEL, double>(p.A, p.B, m, phi, dm)) {
-    fold_derivs<MULTI, TENSOR>(p, dm, D);
+  bool live;
+  if constexpr (MULTI) {
+    assemble<MULTI, TENSOR>(p, n, m);
+    live = fmt_phi_dphi<MODEL, double>(p.A, p.B, m, phi, dm);
+    if (live) fold_derivs<MULTI, TENSOR>(p, dm, D);
   } else {
+    // one species: n0, n1, v0 are multiples of n2, v1, folded into Phi
+    // and its derivatives directly
+    using L1 = Lay<false, TENSOR>;
+    m.eta = n[L1::ETA];
+    m.n2 = n[L1::N2];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) m.v1[c] = n[L1::V1 + c];
+    if constexpr (TENSOR) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) m.t[c] = n[L1::T + c];
+      m.t[5] = m.n2 - m.t[0] - m.t[3];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) m.t[c] = 0.0;
+    }
+    live = fmt_phi_dphi<MODEL, double, true>(p.A, p.B, m, phi, dm, p.inv4piR2[0], p.inv4piR[0]);
+    if (live) {
+      const double dzz = TENSOR ? dm.d_t[5] : 0.0;
+      D[L1::ETA] = dm.d_eta;
+      D[L1::N2] = dm.d_n2 + dzz;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) D[L1::V1 + c] = dm.d_v1[c];
+      if constexpr (TENSOR) {
+        D[L1::T + 0] = dm.d_t[0] - dzz;
+        D[L1::T + 1] = 2.0 * dm.d_t[1];
+        D[L1::T + 2] = 2.0 * dm.d_t[2];
+        D[L1::T + 3] = dm.d_t[3] - dzz;
+        D[L1::T + 4] = 2.0 * dm.d_t[4];
+      }
+    }
+  }
+  if (!live) {
     phi = 0.0;
 #pragma unroll
     for (int c = 0; c < NF; ++c) D[c] = 0.0;

@@ -139,8 +139,15 @@ __host__ __device__ __forceinline__ FVals<T> fmt_f(T eta) {
 // Phi and all partial derivatives at one point (models.hpp:22-81, 169-357).
 // Returns false (and leaves outputs untouched) where eta < 1e-30: the
 // reference skips those points (hard_sphere.hpp:199-200).
-template <int MODEL, class T>
-__host__ __device__ __forceinline__ bool fmt_phi_dphi(double A, double B, const Measures<T>& m, T& phi, MeasureDerivs<T>& dm) {
+// ONE: a single species of radius R, for which n0 = a0 n2, n1 = a1 n2 and
+// v0 = a1 v1 (a0 = 1/(4 pi R^2), a1 = 1/(4 pi R), hard_sphere.hpp:80-85);
+// m.n0, m.n1 and m.v0 are not read, and d_n2 and d_v1 come out with those
+// chains folded in (d_n0, d_n1, d_v0 zero):
+//   Phi = -a0 n2 f1 + a1 (n2^2 - v1.v1) f2 + Phi3 f3,
+//   d_n2 = -a0 f1 + 2 a1 n2 f2 + dPhi3/dn2 f3,  d_v1 = -2 a1 f2 v1 + dPhi3/dv1 f3.
+template <int MODEL, class T, bool ONE = false>
+__host__ __device__ __forceinline__ bool fmt_phi_dphi(double A, double B, const Measures<T>& m, T& phi,
+                                                      MeasureDerivs<T>& dm, double a0 = 0.0, double a1 = 0.0) {
   constexpr int model = MODEL;
   constexpr bool tensor = model_has_tensor(MODEL);
   if (val(m.eta) < 1e-30) return false;
@@ -151,7 +158,8 @@ __host__ __device__ __forceinline__ bool fmt_phi_dphi(double A, double B, const 
 
   // inner products (measures.hpp:34-44); T symmetric
   const T txx = m.t[0], txy = m.t[1], txz = m.t[2], tyy = m.t[3], tyz = m.t[4], tzz = m.t[5];
-  T dot01 = m.v0[0] * m.v1[0] + m.v0[1] * m.v1[1] + m.v0[2] * m.v1[2];
+  T dot01 = zero_like(m.eta);
+  if constexpr (!ONE) dot01 = m.v0[0] * m.v1[0] + m.v0[1] * m.v1[1] + m.v0[2] * m.v1[2];
   T dot11 = m.v1[0] * m.v1[0] + m.v1[1] * m.v1[1] + m.v1[2] * m.v1[2];
   T tt[6];   // TT = T*T (symmetric)
   T tv[3];   // T v1
@@ -209,16 +217,32 @@ __host__ __device__ __forceinline__ bool fmt_phi_dphi(double A, double B, const 
   }
 
   FVals<T> f = fmt_f<MODEL, T>(m.eta);
-  T c2 = m.n1 * n2 - dot01;
-  phi = -m.n0 * f.f1 + c2 * f.f2 + p3 * f.f3;
-  dm.d_eta = -m.n0 * f.df1 + c2 * f.df2 + p3 * f.df3;
-  dm.d_n0 = -f.f1;
-  dm.d_n1 = n2 * f.f2;
-  dm.d_n2 = m.n1 * f.f2 + dp3_n2 * f.f3;
+  if constexpr (ONE) {
+    const T c2 = a1 * (n2 * n2 - dot11);
+    const T n0 = a0 * n2;
+    phi = -n0 * f.f1 + c2 * f.f2 + p3 * f.f3;
+    dm.d_eta = -n0 * f.df1 + c2 * f.df2 + p3 * f.df3;
+    dm.d_n0 = zero_like(m.eta);
+    dm.d_n1 = zero_like(m.eta);
+    dm.d_n2 = -a0 * f.f1 + (2.0 * a1) * n2 * f.f2 + dp3_n2 * f.f3;
+    const T g = (-2.0 * a1) * f.f2;
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    dm.d_v0[a] = -m.v1[a] * f.f2;
-    dm.d_v1[a] = -m.v0[a] * f.f2 + dp3_v[a] * f.f3;
+    for (int a = 0; a < 3; ++a) {
+      dm.d_v0[a] = zero_like(m.eta);
+      dm.d_v1[a] = g * m.v1[a] + dp3_v[a] * f.f3;
+    }
+  } else {
+    T c2 = m.n1 * n2 - dot01;
+    phi = -m.n0 * f.f1 + c2 * f.f2 + p3 * f.f3;
+    dm.d_eta = -m.n0 * f.df1 + c2 * f.df2 + p3 * f.df3;
+    dm.d_n0 = -f.f1;
+    dm.d_n1 = n2 * f.f2;
+    dm.d_n2 = m.n1 * f.f2 + dp3_n2 * f.f3;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      dm.d_v0[a] = -m.v1[a] * f.f2;
+      dm.d_v1[a] = -m.v0[a] * f.f2 + dp3_v[a] * f.f3;
+    }
   }
   if constexpr (tensor) {
     // dPhi3/dT_ij (models.hpp:39-45, 348-357); T and TT symmetric
