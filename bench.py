@@ -14,7 +14,7 @@ bracketed by CUDA events on the engine's stream with an L2 flush between
 steps, outside the events: a write of a 256 MiB buffer, then a read of a
 second one, so that no dirty line of the flush is written back inside the
 timed region; barrier + synchronize on both sides; the max over ranks.  Each rank evaluates its own replica
-(one grid does not shard), so `value` = N * K / max time.
+(one grid does not shard: every transform of the evaluation is global), so `value` = N * K / max time.
 
 `e2e` repeats the metric through the public host API (cdft_total via
 classicaldft_b200.Engine.total_host) with pinned host buffers: H2D of rho,
@@ -118,15 +118,70 @@ class L2Flush:
         self.torch.sum(self.r, 0, out=self.acc)
 
 
-# DRAM bytes per evaluation measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum over the seven launches of one evaluation, 128^3
-# mixed, fused transforms, middle stages in one plane chunk); the launch
-# list is summarised in profiles/eval_128cubed_mixed_launches.md.
-MEASURED_TRAFFIC = {"mixed": 617.8e6}
-# The same capture per launch of each fused-path stage (bytes).
-MEASURED_STAGE_TRAFFIC = {"plane_fwd_rho": 16.79e6, "col_fwd": 64.87e6, "plane_inv_channels": 136.43e6,
-                          "pointwise": 156.49e6, "plane_fwd_derivatives": 114.92e6, "col_bwd": 102.91e6,
-                          "plane_inv_epilogue": 25.36e6}
+# DRAM bytes per launch of each fused-path stage, measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum, 128^3 mixed, middle stages
+# in one plane chunk).  The table is the text file below, written from the ncu
+# CSV by `python bench.py --traffic-table <ncu.csv>`; a stage missing from it
+# reports traffic null.
+TRAFFIC_TABLE = os.path.join(ROOT, "profiles", "traffic_128cubed_mixed.txt")
+FUSED_KERNELS = {  # kernel-name prefix in the ncu list -> stage
+    "k_rplane_fwd<128, 128, double": "plane_fwd_rho", "k_rcol_fwd1": "col_fwd",
+    "k_rplane_inv<128, 128, false": "plane_inv_channels", "k_pointwise_tma": "pointwise",
+    "k_rplane_fwd<128, 128, float": "plane_fwd_derivatives", "k_rcol_bwd1": "col_bwd",
+    "k_rplane_inv<128, 128, true": "plane_inv_epilogue"}
+
+
+def measured_traffic():
+    """{stage: DRAM bytes per launch} from the traffic table (empty if absent)."""
+    out = {}
+    try:
+        with open(TRAFFIC_TABLE) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 2 and not line.startswith("#"):
+                    out[parts[0]] = float(parts[1])
+    except OSError:
+        pass
+    return out
+
+
+def _short_kernel_name(name):
+    """ "void ns::k_x<1, 2>(args)" -> "k_x<1, 2>" """
+    name = name.split("(")[0].replace("void ", "").strip()
+    head, lt, tail = name.partition("<")
+    return head.rsplit("::", 1)[-1] + lt + tail
+
+
+def traffic_table(csv_path):
+    """Reduce an ncu --csv launch list with dram__bytes_read.sum and
+    dram__bytes_write.sum of the fused-path kernels to one line per stage:
+    `<stage> <mean DRAM bytes per launch> <launches>`."""
+    import csv
+    scale = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9}
+    with open(csv_path) as f:
+        rows = [r for r in csv.reader(f)]
+    head = next(i for i, r in enumerate(rows) if "Kernel Name" in r and "Metric Name" in r)
+    h = rows[head]
+    ki, mi, vi, ii = h.index("Kernel Name"), h.index("Metric Name"), h.index("Metric Value"), h.index("ID")
+    ui = h.index("Metric Unit") if "Metric Unit" in h else None
+    per = {}
+    for r in rows[head + 1:]:
+        if len(r) <= vi or r[mi] not in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            continue
+        name = _short_kernel_name(r[ki])
+        stage = next((st for pre, st in FUSED_KERNELS.items() if name.startswith(pre)), None)
+        if stage is None:
+            continue
+        unit = scale.get(r[ui], 1.0) if ui is not None else 1.0
+        per[(stage, r[ii])] = per.get((stage, r[ii]), 0.0) + float(r[vi].replace(",", "")) * unit
+    acc = {}
+    for (stage, _), b in per.items():
+        acc.setdefault(stage, []).append(b)
+    print("# stage  DRAM_bytes_per_launch  launches   (from " + os.path.basename(csv_path) + ")")
+    for stage in FUSED_KERNELS.values():
+        if stage in acc:
+            v = acc[stage]
+            print(f"{stage} {sum(v) / len(v):.4e} {len(v)}")
 
 
 class ClockSampler:
@@ -494,6 +549,7 @@ def run_ours(args, ws, rank, local, dist):
     stages = stage_breakdown(torch, eng, rho, force, scal, flush, stream, max(10, min(args.steps, 100)), peak)
     mine = {k: v for k, v in stages.items() if v["kind"] == "engine kernel" and v["algorithmic_bytes"]}
     top = max(mine, key=lambda k: mine[k]["ms"])
+    traffic = measured_traffic()
     sweep = None if args.no_sweep else sweep_throughput(torch, cd, dev, precision, flush, stream, 20)
     fire_rates = None if args.no_sweep else fire_step_rates(torch, cd, precision)
     line = {
@@ -511,13 +567,17 @@ def run_ours(args, ws, rank, local, dist):
         # algorithmic bytes over its live duration; the whole evaluation beside it
         "roofline": {"bound": "hbm", "kernel": top, "achieved": mine[top]["achieved_gbs"], "peak": peak,
                      "unit": "GB/s", "frac": mine[top]["frac"],
-                     "traffic": MEASURED_STAGE_TRAFFIC.get(top) if fused and precision == cd.MIXED else None,
+                     "traffic": traffic.get(top) if fused and precision == cd.MIXED else None,
                      "algorithmic_bytes": mine[top]["algorithmic_bytes"], "ms": mine[top]["ms"],
                      "peak_source": peak_kind,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch (profiles/)",
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
+                                       "profiles/traffic_128cubed_mixed.txt",
                      "evaluation": {
                          "achieved": achieved, "frac": achieved / peak, "algorithmic_bytes": nbytes,
-                         "traffic": MEASURED_TRAFFIC.get(names[precision]) if fused else None,
+                         "traffic": (sum(traffic[k] for k in FUSED_KERNELS.values())
+                                     if fused and precision == cd.MIXED and all(k in traffic for k in
+                                                                                 FUSED_KERNELS.values())
+                                     else None),
                          "scope": ("one full evaluation (the seven fused-path kernels)" if fused
                                    else "one full evaluation (cuFFT transforms + engine kernels)")}},
         "stages": stages,
@@ -531,8 +591,15 @@ def run_ours(args, ws, rank, local, dist):
         "gpu_launches": int(info["kernels_per_eval"]) * args.steps,
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cb, _ = cpu_baseline_sample(args.cpu_seconds)
+        cb, ref = cpu_baseline_sample(args.cpu_seconds)
         line["cpu_baseline"] = cb
+        # the timed runs' outputs against the oracle's evaluation of the same state
+        f_ref = ref.forces[0]
+        fmax = float(np.max(np.abs(f_ref)))
+        for key, f_dev, s_dev in (("oracle_vs_mixed", f32, s32), ("oracle_vs_fp64", f64, s64)):
+            line[key] = {"dF_over_F": abs(float(s_dev[0]) - ref.free_energy) / abs(ref.free_energy),
+                         "dOmega_over_Omega": abs(float(s_dev[1]) - ref.grand_potential) / abs(ref.grand_potential),
+                         "max_dforce_over_max_force": float(np.max(np.abs(f_dev.cpu().numpy() - f_ref))) / fmax}
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()
@@ -551,7 +618,12 @@ def main():
     ap.add_argument("--plane-chunks", type=int, default=0,
                     help="plane chunks of the fused path's middle stages (0: the engine's default; 1 runs them "
                          "back to back, as a profiler's serialised launch list sees them)")
+    ap.add_argument("--traffic-table", metavar="NCU_CSV",
+                    help="print the per-stage DRAM traffic table from an ncu --csv launch list and exit")
     args = ap.parse_args()
+    if args.traffic_table:
+        traffic_table(args.traffic_table)
+        return
     ws, rank, local, dist = setup_dist(args)
     try:
         if args.impl == "reference":

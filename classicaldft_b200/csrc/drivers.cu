@@ -1162,7 +1162,7 @@ double Drivers::ddft_step_on(DDFTConfig& cfg, double* rho, cudaStream_t stream, 
       k_maxmin_finish<<<1, 32, 0, stream>>>(red_, grid_, red_out_);
       CDFT_CUDA(cudaMemcpyAsync(host_pin_, red_out_, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
     };
-    const int path = (eng_.fused() ? 16 : 0) + eng_.chunks();
+    const unsigned long long path = eng_.generation();
     if (graphs && !(fp_exec_ && fp_dt_ == dt && fp_mu_ == mu && fp_path_ == path)) {
       reset_fp_graph();
       CDFT_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));

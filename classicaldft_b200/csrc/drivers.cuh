@@ -235,7 +235,7 @@ class Drivers {
   cudaGraph_t fp_graph_ = nullptr;
   cudaGraphExec_t fp_exec_ = nullptr;
   double fp_dt_ = 0.0, fp_mu_ = 0.0;
-  int fp_path_ = 0;  // the engine's transforms and plane chunks at capture
+  unsigned long long fp_path_ = 0;  // the engine's generation at capture
   void reset_fp_graph();
   double ddft_step_on(DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations, bool graphs);
 

@@ -283,6 +283,7 @@ void Engine::set_stage_timing(bool on) {
     for (cudaEvent_t& e : stage_ev_) CDFT_CUDA(cudaEventCreate(&e));
   }
   if (!on) harvest_stage_times();
+  if (on != timing_) ++generation_;
   timing_ = on;
 }
 
@@ -419,6 +420,7 @@ void Engine::set_chunks(int k) {
   if (k < 1 || k > kMaxChunks || p_.nx % k != 0)
     throw std::invalid_argument("plane chunks: 1..8 dividing nx");
   ensure_chunk_streams(k);
+  if (k != chunks_) ++generation_;
   chunks_ = k;
 }
 
@@ -426,6 +428,7 @@ void Engine::set_fused(bool on) {
   if (on && !fusable_)
     throw Error(-1, "fused transforms need a mixed-precision engine whose nx, ny, nz are each 16, 32, 48, 64, 96 or "
                     "128 and whose (y, z) plane fits in shared memory");
+  if (on != fused_) ++generation_;
   fused_ = on;
 }
 

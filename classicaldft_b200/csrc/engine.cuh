@@ -95,6 +95,10 @@ class Engine {
   int autotune(const double* rho, const double* vext, const double* mu, cudaStream_t stream, int reps,
                double* ms);
   int chunks() const { return chunks_; }
+  // Changes whenever a setter changes what an evaluation launches (transform
+  // path, plane chunks, stage timing): a captured graph of an evaluation is
+  // valid only for the generation it was captured at.
+  unsigned long long generation() const { return generation_; }
   bool stage_timing_on() const { return timing_; }
   int kernels_per_eval() const { return precision_ == 1 ? (fused_ ? 4 + 3 * chunks_ : 6) : 4; }
   // Reads and clears the device error word (synchronises the stream).
@@ -187,6 +191,7 @@ class Engine {
   // and joined back into the caller's stream, so the FP64 pointwise work of
   // one chunk overlaps the FP32 transforms of another.
   int chunks_ = 1;
+  unsigned long long generation_ = 0;
   std::string tune_key_;  // shape key of the autotuner's cache
   void ensure_chunk_streams(int k);
   std::vector<cudaStream_t> aux_;

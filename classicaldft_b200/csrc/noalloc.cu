@@ -16,7 +16,6 @@
 // threads on one device) race on it: serialise them.  The partial sums are
 // fully rewritten by every call before they are read, so nothing carries over
 // from the previous call.
-#include <mutex>
 #include <string>
 
 #include "../../include/cdft_b200.h"
@@ -27,7 +26,6 @@ namespace {
 constexpr int kNaBlocks = 592;                        // 4 CTAs per SM on 148 SMs
 constexpr int kNaTerms = 2 + cdft::kMaxSpecies;       // F_id, F_ext, N_0..N_3
 constexpr int kNaThreads = 256;
-constexpr int kMaxDevices = 64;
 
 // kNaBlocks x kNaTerms partial sums: 592 * 6 * 8 bytes = 28 KiB.
 static __device__ __align__(256) double g_noalloc_scratch[kNaBlocks * kNaTerms];
@@ -90,12 +88,11 @@ __global__ void k_local_finish(const double* __restrict__ partials, int nblocks,
   if (lane == 0) out[warp] = v * dv;
 }
 
-std::mutex g_setup_mutex;
-double* g_scratch_ptr[kMaxDevices] = {};
-
-// Once per device, with that device current: the device address of the
-// scratch array.  In host code `g_noalloc_scratch` names a host-side stand-in,
-// not device memory, so it is never passed to a kernel directly.
+// With the caller's device current: the device address of the scratch
+// array.  In host code `g_noalloc_scratch` names a host-side stand-in, not
+// device memory, so it is never passed to a kernel directly.  The address is
+// looked up on every call rather than cached: a device reset or a new primary
+// context reloads the module, and the array may then sit elsewhere.
 double* scratch_for_current_device(std::string& err) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -103,21 +100,14 @@ double* scratch_for_current_device(std::string& err) {
     err = std::string("cudaGetDevice failed: ") + cudaGetErrorString(e);
     return nullptr;
   }
-  if (dev < 0 || dev >= kMaxDevices) {
-    err = "device ordinal out of range for the allocation-free entry point";
+  void* p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) {
+    err = std::string("cudaGetSymbolAddress failed on device ") + std::to_string(dev) + ": " +
+          cudaGetErrorString(e);
     return nullptr;
   }
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) {
-      err = std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
-      return nullptr;
-    }
-    g_scratch_ptr[dev] = static_cast<double*>(p);
-  }
-  return g_scratch_ptr[dev];
+  return static_cast<double*>(p);
 }
 
 }  // namespace

@@ -439,8 +439,9 @@ CDFT_API int cdft_bulk_coexistence(const cdft_bulk_model* model, double rho_max,
  *   6.. of cdft_total's scalar block).
  * force = (ln max(rho, 1e-300) - mu + V) dV.  Scratch is a 28 KiB file-scope
  * device array (592 x 6 partial sums) held by every GPU that loads the
- * library; n_species is limited to 4 by it.  The first call on a device looks
- * the array's address up (cudaGetSymbolAddress): make that first call before
+ * library; n_species is limited to 4 by it.  Every call looks the array's
+ * address up (cudaGetSymbolAddress, so a device reset is harmless); the first
+ * call on a device also loads the module there: make that first call before
  * any stream capture.  All calls share the array: calls whose kernels overlap
  * on the GPU race, so serialise them.  Asynchronous on `stream`. */
 CDFT_API int cdft_local_terms_noalloc(const double* rho, const double* vext, const double* mu, int n_species,

@@ -56,6 +56,11 @@ CASES = [
     ((48, 48, 48), 0.1, [1.0], "WhiteBearII", [(0, 0) + LJ]),
     ((96, 48, 96), 0.1, [1.0], "esFMT", [(0, 0) + LJ]),
     ((48, 96, 16), 0.2, [1.0, 0.6], "WhiteBearI", [(0, 1, 1.0, 0.8, 2.5)]),
+    # the 128-point specialisations of every plane and column kernel
+    ((128, 128, 128), 0.125, [1.0], "WhiteBearII", [(0, 0) + LJ]),
+    ((128, 32, 64), 0.1, [1.0], "WhiteBearII", [(0, 0) + LJ]),
+    ((32, 128, 16), 0.1, [1.0], "esFMT", [(0, 0) + LJ]),
+    ((64, 64, 128), 0.1, [1.0, 0.6], "WhiteBearII", [(0, 0) + LJ, (0, 1, 1.0, 0.8, 2.5)]),
 ]
 
 

@@ -25,19 +25,23 @@ TOL = 1e-12
 
 
 def _noalloc(rho, vext, mu, dv):
+    """rho: (S, n) or (n,); vext the same shape or None; mu: S values."""
     import torch
     L = _lib.lib()
-    n = rho.size
+    rho = np.atleast_2d(rho)
+    S, n = rho.shape
+    mus = np.atleast_1d(mu)
     d_rho = torch.tensor(rho, dtype=torch.float64, device="cuda")
-    d_v = torch.tensor(vext, dtype=torch.float64, device="cuda")
-    d_f = torch.full((n,), np.nan, dtype=torch.float64, device="cuda")
-    d_sc = torch.full((3,), np.nan, dtype=torch.float64, device="cuda")
-    mu_c = (ctypes.c_double * 1)(mu)
-    st = L.cdft_local_terms_noalloc(d_rho.data_ptr(), d_v.data_ptr(), mu_c, 1, n, dv, d_f.data_ptr(),
-                                    d_sc.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    d_v = None if vext is None else torch.tensor(np.atleast_2d(vext), dtype=torch.float64, device="cuda")
+    d_f = torch.full((S, n), np.nan, dtype=torch.float64, device="cuda")
+    d_sc = torch.full((2 + S,), np.nan, dtype=torch.float64, device="cuda")
+    mu_c = (ctypes.c_double * S)(*mus)
+    st = L.cdft_local_terms_noalloc(d_rho.data_ptr(), None if d_v is None else d_v.data_ptr(), mu_c, S, n, dv,
+                                    d_f.data_ptr(), d_sc.data_ptr(), torch.cuda.current_stream().cuda_stream)
     assert st == _lib.CDFT_OK, L.cdft_last_error().decode()
     torch.cuda.synchronize()
-    return d_sc.cpu().numpy(), d_f.cpu().numpy()
+    f = d_f.cpu().numpy()
+    return d_sc.cpu().numpy(), (f[0] if S == 1 else f)
 
 
 def test_noalloc_local_terms_match_cdft_total_on_two_calls():
@@ -63,6 +67,32 @@ def test_noalloc_local_terms_match_cdft_total_on_two_calls():
             # rho = 0: every channel is exactly zero, the hard-sphere and
             # mean-field forces vanish, and cdft_total's force is the local force
             assert np.max(np.abs(f - f_ref[0])) <= TOL * np.max(np.abs(f_ref[0]))
+
+
+def test_noalloc_two_species_without_field_on_a_large_grid():
+    """64^3 points (more than the 592 x 256 threads of one pass of the
+    grid-stride loop), two species and no external field: F_id and N_s equal
+    cdft_total's, F_ext is zero and the force is (ln rho - mu) dV; two calls in
+    a row."""
+    shape, dx = (64, 64, 64), 0.1
+    g = cd.Grid(dx=dx, box_size=tuple(k * dx for k in shape), shape=shape)
+    model = cd.Model(g, [cd.Species("A", 1.0), cd.Species("B", 0.6)], [], 1.0)
+    w = cd.make_weights(cd.WhiteBearII(), model)
+    n = g.total_points
+    dv = g.cell_volume
+    rng = np.random.default_rng(8)
+    for call in range(2):
+        rho = np.stack([0.3 * (1.0 + 0.3 * rng.uniform(-1.0, 1.0, n)), 0.1 * rng.uniform(0.0, 1.0, n)])
+        rho[1, :: 97] = 0.0  # the clamp at 1e-300
+        mu = rng.uniform(-1.0, 1.0, 2)
+        sc_ref, _ = w.engine.total_host(rho, list(mu), None)
+        sc, f = _noalloc(rho, None, mu, dv)
+        assert abs(sc[0] - sc_ref[2]) <= TOL * abs(sc_ref[2]), (call, sc[0], sc_ref[2])
+        assert sc[1] == 0.0
+        for s in range(2):
+            assert abs(sc[2 + s] - sc_ref[6 + s]) <= TOL * abs(sc_ref[6 + s]), (call, s)
+            local = (np.log(np.maximum(rho[s], 1e-300)) - mu[s]) * dv
+            assert np.max(np.abs(f[s] - local)) <= TOL * np.max(np.abs(local)), (call, s)
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
