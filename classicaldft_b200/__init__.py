@@ -16,7 +16,8 @@ from .algorithms import set_step_graphs, step_graphs  # noqa: F401
 from .algorithms import (Bounded, EigenvalueResult, EigenvalueSolver, Fire, FixedMassConstraint,  # noqa: F401
                          MinimizationResult, Minimizer, Picard, PicardResult, ReservoirBoundary, SaddleResult, Search,
                          Simulation, Snapshot, StepConfig, Unbounded, crank_nicholson_step, fixed_mass_constraint,
-                         hessian_times_vector, integrating_factor_step, reservoir_boundary, split_operator_step)
+                         ddft_last_step, hessian_times_vector, integrating_factor_step, reservoir_boundary,
+                         split_operator_step)
 from .bulk import (BulkThermodynamics, Coexistence, PhaseSearch, Spinodal, density_from_chemical_potential,  # noqa: F401
                    densities_from_chemical_potentials, make_bulk_thermodynamics, make_bulk_weights)
 

@@ -87,9 +87,14 @@ class CPicardResult(ctypes.Structure):
 STOP_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_void_p)
 
 
+EIGEN_RAYLEIGH_RITZ = 0
+EIGEN_LANCZOS = 1
+
+
 class CEigenConfig(ctypes.Structure):
     _fields_ = [("tolerance", ctypes.c_double), ("max_iterations", ctypes.c_int), ("hessian_eps", ctypes.c_double),
-                ("exact_hvp", ctypes.c_int), ("seed", ctypes.c_ulonglong)]
+                ("exact_hvp", ctypes.c_int), ("seed", ctypes.c_ulonglong), ("method", ctypes.c_int),
+                ("block", ctypes.c_int), ("max_basis", ctypes.c_int), ("check_interval", ctypes.c_int)]
 
 
 class CBulkInteraction(ctypes.Structure):
@@ -204,6 +209,13 @@ def lib():
                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), vp],
         "cdft_saddle_find": [vp, ctypes.POINTER(CSaddleConfig), vp, ctypes.c_double, ctypes.c_double, vp,
                              c_double_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), vp],
+        "cdft_ddft_set_refine": [vp, vp, ctypes.c_int],
+        "cdft_ddft_last_step": [vp, ctypes.POINTER(ctypes.c_int), c_double_p],
+        "cdft_eigen_solve_ex": [vp, vp, ctypes.POINTER(CEigenConfig), vp, ctypes.c_double, vp, ctypes.c_int,
+                                c_double_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), vp],
+        "cdft_saddle_find_ex": [vp, vp, vp, ctypes.c_double, ctypes.POINTER(CSaddleConfig), vp, ctypes.c_double,
+                                ctypes.c_double, vp, c_double_p, ctypes.POINTER(ctypes.c_int),
+                                ctypes.POINTER(ctypes.c_int), vp],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)

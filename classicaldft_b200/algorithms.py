@@ -324,9 +324,19 @@ class StepConfig:
                                 self.fp_tolerance, self.fp_max_iterations)
 
 
-def integrating_factor_step(density, weights: Weights, config: StepConfig, chemical_potential=0.0):
+def _set_ddft_refine(weights: Weights, refine, refine_iterations):
+    _lib.check(_lib.lib().cdft_ddft_set_refine(weights.engine.handle,
+                                               refine.engine.handle if refine is not None else None,
+                                               int(refine_iterations) if refine is not None else 0))
+
+
+def integrating_factor_step(density, weights: Weights, config: StepConfig, chemical_potential=0.0, refine=None,
+                            refine_iterations=2):
     """dynamics.hpp:333-401: returns (density, energy, dt_used); config.dt is
-    divided by 10 on restarts, as in the reference."""
+    divided by 10 on restarts, as in the reference.  ``refine``: FP64 Weights
+    of the same model that run ``refine_iterations`` fixed-point iterations
+    after the step has converged with ``weights`` and give its final energy
+    (mixed-precision defect correction)."""
     torch = _torch()
     d, host = _dev(density)
     if not host:
@@ -334,11 +344,27 @@ def integrating_factor_step(density, weights: Weights, config: StepConfig, chemi
     c = config.c()
     e = ctypes.c_double()
     it = ctypes.c_int()
-    _lib.check(_lib.lib().cdft_ddft_step(weights.engine.handle, ctypes.byref(c), chemical_potential, d.data_ptr(),
-                                         ctypes.byref(e), ctypes.byref(it), _stream()))
+    _set_ddft_refine(weights, refine, refine_iterations)
+    try:
+        _lib.check(_lib.lib().cdft_ddft_step(weights.engine.handle, ctypes.byref(c), chemical_potential,
+                                             d.data_ptr(), ctypes.byref(e), ctypes.byref(it), _stream()))
+    finally:
+        _set_ddft_refine(weights, None, 0)
     torch.cuda.synchronize()
     config.dt = c.dt
     return (d.cpu().numpy() if host else d), e.value, c.dt
+
+
+def ddft_last_step(weights: Weights) -> dict:
+    """Facts of the last integrating-factor step of these weights' engine:
+    fixed-point iterations, restarts, status (1 converged, 2 gave up), whether
+    the loop ran on the device (a conditional graph node), and the deviation
+    of the last FP64 refinement iteration."""
+    info = (ctypes.c_int * 4)()
+    dev = ctypes.c_double()
+    _lib.check(_lib.lib().cdft_ddft_last_step(weights.engine.handle, info, ctypes.byref(dev)))
+    return {"fp_iterations": info[0], "restarts": info[1], "status": info[2], "device_loop": bool(info[3]),
+            "refine_deviation": dev.value}
 
 
 def _ddft_single(fn, density, weights: Weights, config: StepConfig, chemical_potential, with_iterations):
@@ -411,6 +437,9 @@ class Simulation:
     energy_offset: float = 0.0
     boundary: ReservoirBoundary = None
     stop_condition: object = None
+    # FP64 defect correction of a mixed-precision run (see integrating_factor_step)
+    refine: object = None
+    refine_iterations: int = 2
 
     def run(self, densities, weights: Weights, chemical_potential=0.0):
         torch = _torch()
@@ -450,12 +479,16 @@ class Simulation:
         if mask_dev is not None:
             d.masked_fill_(mask_dev.bool(), res_density)  # the driver applies it too; the initial mass needs it
         mass_initial = float(torch.sum(d).item()) * dv
-        _lib.check(_lib.lib().cdft_ddft_simulate(
-            weights.engine.handle, ctypes.byref(c), chemical_potential, self.n_steps, d.data_ptr(),
-            times.ctypes.data_as(_lib.c_double_p), energies.ctypes.data_as(_lib.c_double_p), self.snapshot_interval,
-            ctypes.cast(snaps.data_ptr(), _lib.c_double_p) if snaps is not None else None, snap_steps, cap,
-            ctypes.byref(count), mask_dev.data_ptr() if mask_dev is not None else None, res_density, cb, None,
-            ctypes.byref(done), _stream()))
+        _set_ddft_refine(weights, self.refine, self.refine_iterations)
+        try:
+            _lib.check(_lib.lib().cdft_ddft_simulate(
+                weights.engine.handle, ctypes.byref(c), chemical_potential, self.n_steps, d.data_ptr(),
+                times.ctypes.data_as(_lib.c_double_p), energies.ctypes.data_as(_lib.c_double_p),
+                self.snapshot_interval, ctypes.cast(snaps.data_ptr(), _lib.c_double_p) if snaps is not None else None,
+                snap_steps, cap, ctypes.byref(count), mask_dev.data_ptr() if mask_dev is not None else None,
+                res_density, cb, None, ctypes.byref(done), _stream()))
+        finally:
+            _set_ddft_refine(weights, None, 0)
         torch.cuda.synchronize()
         if err:
             raise err[0]
@@ -525,19 +558,34 @@ class EigenvalueResult:
 
 @dataclass
 class EigenvalueSolver:
-    """saddle_point.hpp:158-169 (``exact_hvp`` replaces the FD product)."""
+    """saddle_point.hpp:158-169 (``exact_hvp`` replaces the FD product).
+
+    ``method="lanczos"`` replaces the reference's 3-vector Rayleigh-Ritz
+    iteration by block Lanczos on exact products of the same operator (the
+    fixed-boundary Hessian, restricted to the interior): ``block`` directions
+    per batched product, ``max_basis`` blocks before a restart, the host
+    checking every ``check_interval`` products.  ``solve(..., hvp_weights=w)``
+    takes the products from ``w.engine`` (same model, batch = ``block``; e.g.
+    an FP64 engine under a mixed-precision one)."""
 
     tolerance: float = 1e-4
     max_iterations: int = 300
     hessian_eps: float = 1e-6
     exact_hvp: bool = False
     seed: int = 42
+    method: str = "rayleigh_ritz"
+    block: int = 1
+    max_basis: int = 32
+    check_interval: int = 4
 
     def c(self):
+        if self.method not in ("rayleigh_ritz", "lanczos"):
+            raise ValueError(f"unknown eigen method {self.method!r}")
+        m = _lib.EIGEN_LANCZOS if self.method == "lanczos" else _lib.EIGEN_RAYLEIGH_RITZ
         return _lib.CEigenConfig(self.tolerance, self.max_iterations, self.hessian_eps, 1 if self.exact_hvp else 0,
-                                 self.seed)
+                                 self.seed, m, self.block, self.max_basis, self.check_interval)
 
-    def solve(self, weights: Weights, rho, chemical_potential=0.0, initial_guess=None):
+    def solve(self, weights: Weights, rho, chemical_potential=0.0, initial_guess=None, hvp_weights=None):
         torch = _torch()
         r, host = _dev(rho)
         if initial_guess is not None:
@@ -549,10 +597,11 @@ class EigenvalueSolver:
         it = ctypes.c_int()
         cv = ctypes.c_int()
         c = self.c()
-        _lib.check(_lib.lib().cdft_eigen_solve(weights.engine.handle, ctypes.byref(c), r.data_ptr(),
-                                               chemical_potential, vec.data_ptr(), 1 if initial_guess is not None
-                                               else 0, ctypes.byref(ev), ctypes.byref(it), ctypes.byref(cv),
-                                               _stream()))
+        _lib.check(_lib.lib().cdft_eigen_solve_ex(weights.engine.handle,
+                                                  hvp_weights.engine.handle if hvp_weights is not None else None,
+                                                  ctypes.byref(c), r.data_ptr(), chemical_potential, vec.data_ptr(),
+                                                  1 if initial_guess is not None else 0, ctypes.byref(ev),
+                                                  ctypes.byref(it), ctypes.byref(cv), _stream()))
         torch.cuda.synchronize()
         return EigenvalueResult(vec.cpu().numpy() if host else vec, ev.value, it.value, bool(cv.value))
 
@@ -567,6 +616,8 @@ class SaddleResult:
     eigenvalue: float
     outer_iterations: int
     converged: bool
+    eigen_iterations: int = 0  # products of the eigen solves, summed over the outer iterations
+    fire_steps: int = 0        # projected FIRE steps, summed over the outer iterations
 
 
 @dataclass
@@ -583,6 +634,14 @@ class Search:
     max_outer_iterations: int = 20
     eigenvalue_clear_count: int = 2
 
+    # FP64 defect correction of a mixed-precision search: the FP64 `refine`
+    # weights take over each projected FIRE run once its rms force is below
+    # refine_switch times the run's tolerance
+    refine: object = None
+    refine_switch: float = 10.0
+    # product engine of a Lanczos eigen solve (batch = eigenvalue.block)
+    hvp_weights: object = None
+
     def find(self, model: Model, weights: Weights, initial_density, chemical_potential, target_mass):
         torch = _torch()
         r, host = _dev(initial_density)
@@ -592,11 +651,13 @@ class Search:
                                  self.tolerance_start, self.tolerance_factor, self.max_outer_iterations,
                                  self.eigenvalue_clear_count)
         out = (ctypes.c_double * 2)()
-        it = ctypes.c_int()
+        counts = (ctypes.c_int * 3)()
         cv = ctypes.c_int()
-        _lib.check(_lib.lib().cdft_saddle_find(weights.engine.handle, ctypes.byref(cfg), r.data_ptr(),
-                                               chemical_potential, target_mass, ev.data_ptr(), out,
-                                               ctypes.byref(it), ctypes.byref(cv), _stream()))
+        _lib.check(_lib.lib().cdft_saddle_find_ex(
+            weights.engine.handle, self.refine.engine.handle if self.refine is not None else None,
+            self.hvp_weights.engine.handle if self.hvp_weights is not None else None, self.refine_switch,
+            ctypes.byref(cfg), r.data_ptr(), chemical_potential, target_mass, ev.data_ptr(), out, counts,
+            ctypes.byref(cv), _stream()))
         torch.cuda.synchronize()
         conv = (lambda t: t.cpu().numpy()) if host else (lambda t: t)
-        return SaddleResult(conv(r), conv(ev), out[0], out[1], it.value, bool(cv.value))
+        return SaddleResult(conv(r), conv(ev), out[0], out[1], counts[0], bool(cv.value), counts[1], counts[2])

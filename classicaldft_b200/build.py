@@ -21,7 +21,8 @@ LIB = os.path.join(HERE, "libcdft_b200.so")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc") if os.path.exists(os.path.join(CUDA_HOME, "bin", "nvcc")) else "nvcc"
 
-SOURCES = ["engine.cu", "fused.cu", "drivers.cu", "capi.cu", "noalloc.cu", "bulk.cu", "lattice.cu", "physics.cpp"]
+SOURCES = ["engine.cu", "fused.cu", "drivers.cu", "lanczos.cu", "capi.cu", "noalloc.cu", "bulk.cu", "lattice.cu",
+           "physics.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++20", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I", CSRC, "-I", os.path.join(ROOT, "include")]
@@ -43,6 +44,21 @@ def _stale(obj, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _deps(src, obj, headers):
+    """The headers a source includes, from the dependency file nvcc / g++
+    wrote beside its object (-MD); every header when there is none yet."""
+    dfile = obj + ".d"
+    if not os.path.exists(dfile):
+        return headers
+    with open(dfile) as f:
+        text = f.read().replace("\\\n", " ")
+    out = []
+    for tok in text.split(":", 1)[-1].split():
+        if os.path.exists(tok) and os.path.abspath(tok).startswith(ROOT):
+            out.append(tok)
+    return out or headers
+
+
 def build(verbose: bool = False, extra=None) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = _headers()
@@ -51,12 +67,13 @@ def build(verbose: bool = False, extra=None) -> str:
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src + ".o")
         objs.append(obj)
-        if not _stale(obj, [path] + headers):
+        if not _stale(obj, [path] + _deps(path, obj, headers)):
             continue
-        cmd = [NVCC] + ARCH + FLAGS + (extra or []) + ["-c", path, "-o", obj]
+        cmd = [NVCC] + ARCH + FLAGS + (extra or []) + ["-MD", "-MF", obj + ".d", "-c", path, "-o", obj]
         if src.endswith(".cpp"):
             cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-I", CSRC, "-I",
-                   os.path.join(ROOT, "include"), "-I", os.path.join(CUDA_HOME, "include"), "-c", path, "-o", obj]
+                   os.path.join(ROOT, "include"), "-I", os.path.join(CUDA_HOME, "include"), "-MD", "-MF",
+                   obj + ".d", "-c", path, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         cmds.append(cmd)

@@ -397,6 +397,12 @@ cdft::Drivers::EigenConfig to_eigen(const cdft_eigen_config& c) {
   e.hessian_eps = c.hessian_eps;
   e.exact_hvp = c.exact_hvp;
   e.seed = c.seed;
+  e.method = c.method;
+  if (e.method != CDFT_EIGEN_RAYLEIGH_RITZ && e.method != CDFT_EIGEN_LANCZOS)
+    throw std::invalid_argument("eigen: unknown method");
+  e.block = c.block > 0 ? c.block : 1;
+  e.max_basis = c.max_basis > 0 ? c.max_basis : 32;
+  e.check_interval = c.check_interval > 0 ? c.check_interval : 4;
   return e;
 }
 
@@ -482,6 +488,25 @@ int cdft_ddft_step(cdft_engine* engine, cdft_ddft_config* cfg, double chemical_p
     const double e = d.ddft_step(dc, rho, static_cast<cudaStream_t>(stream), fp_iterations);
     cfg->dt = dc.dt;
     if (energy) *energy = e;
+  });
+}
+
+int cdft_ddft_set_refine(cdft_engine* engine, cdft_engine* refine, int iterations) {
+  return guarded([&] {
+    if (!engine) throw std::invalid_argument("engine is required");
+    drivers_of(engine).set_ddft_refine(refine ? refine->impl : nullptr, iterations);
+  });
+}
+
+int cdft_ddft_last_step(cdft_engine* engine, int info[4], double* refine_deviation) {
+  return guarded([&] {
+    if (!engine || !info) throw std::invalid_argument("engine and info are required");
+    const cdft::Drivers::DDFTStepInfo& i = drivers_of(engine).last_ddft_step();
+    info[0] = i.fp_iterations;
+    info[1] = i.restarts;
+    info[2] = i.status;
+    info[3] = i.device_loop;
+    if (refine_deviation) *refine_deviation = i.refine_deviation;
   });
 }
 
@@ -609,11 +634,38 @@ int cdft_eigen_solve(cdft_engine* engine, const cdft_eigen_config* cfg, const do
   });
 }
 
+int cdft_eigen_solve_ex(cdft_engine* engine, cdft_engine* hvp_engine, const cdft_eigen_config* cfg,
+                        const double* rho, double chemical_potential, double* vec, int use_guess, double* eigenvalue,
+                        int* iterations, int* converged, void* stream) {
+  return guarded([&] {
+    if (!cfg || !rho || !vec) throw std::invalid_argument("cfg, rho and vec are required");
+    cdft::Engine* he = hvp_engine ? hvp_engine->impl : nullptr;
+    cdft::Drivers::EigenResult r = drivers_of(engine).eigen_solve(to_eigen(*cfg), rho, chemical_potential, vec,
+                                                                  use_guess != 0, static_cast<cudaStream_t>(stream),
+                                                                  he);
+    if (eigenvalue) *eigenvalue = r.eigenvalue;
+    if (iterations) *iterations = r.iterations;
+    if (converged) *converged = r.converged ? 1 : 0;
+  });
+}
+
 int cdft_saddle_find(cdft_engine* engine, const cdft_saddle_config* cfg, double* rho, double chemical_potential,
                      double target_mass, double* eigvec, double out[2], int* outer_iterations, int* converged,
                      void* stream) {
+  int counts[3] = {0, 0, 0};
+  const int st = cdft_saddle_find_ex(engine, nullptr, nullptr, 10.0, cfg, rho, chemical_potential, target_mass, eigvec,
+                                     out, counts, converged, stream);
+  if (st == CDFT_OK && outer_iterations) *outer_iterations = counts[0];
+  return st;
+}
+
+int cdft_saddle_find_ex(cdft_engine* engine, cdft_engine* refine, cdft_engine* hvp_engine, double refine_switch,
+                        const cdft_saddle_config* cfg, double* rho, double chemical_potential, double target_mass,
+                        double* eigvec, double out[2], int counts[3], int* converged, void* stream) {
   return guarded([&] {
     if (!cfg || !rho || !eigvec) throw std::invalid_argument("cfg, rho and eigvec are required");
+    if (refine && refine->impl->precision() != cdft::kFP64)
+      throw std::invalid_argument("saddle: the refine engine must be FP64");
     cdft::Drivers::SaddleConfig sc;
     sc.fire = to_fire(cfg->fire);
     sc.eigen = to_eigen(cfg->eigen);
@@ -623,13 +675,18 @@ int cdft_saddle_find(cdft_engine* engine, const cdft_saddle_config* cfg, double*
     sc.tolerance_factor = cfg->tolerance_factor;
     sc.max_outer_iterations = cfg->max_outer_iterations;
     sc.eigenvalue_clear_count = cfg->eigenvalue_clear_count;
-    cdft::Drivers::SaddleResult r = drivers_of(engine).saddle_find(sc, rho, chemical_potential, target_mass, eigvec,
-                                                                   static_cast<cudaStream_t>(stream));
+    cdft::Drivers::SaddleResult r = drivers_of(engine).saddle_find(
+        sc, rho, chemical_potential, target_mass, eigvec, static_cast<cudaStream_t>(stream),
+        refine ? refine->impl : nullptr, hvp_engine ? hvp_engine->impl : nullptr, refine_switch);
     if (out) {
       out[0] = r.grand_potential;
       out[1] = r.eigenvalue;
     }
-    if (outer_iterations) *outer_iterations = r.outer_iterations;
+    if (counts) {
+      counts[0] = r.outer_iterations;
+      counts[1] = r.eigen_iterations;
+      counts[2] = r.fire_steps;
+    }
     if (converged) *converged = r.converged ? 1 : 0;
   });
 }

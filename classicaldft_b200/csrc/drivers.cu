@@ -1,6 +1,7 @@
 // Device-resident drivers: FIRE2 minimisation, DDFT integrating-factor steps,
 // Hessian-vector products.  See drivers.cuh.
 #include "drivers.cuh"
+#include "lanczos.cuh"
 
 #include <algorithm>
 #include <atomic>
@@ -367,6 +368,19 @@ __global__ void k_fire_finalize(FireDevState* st, const double* __restrict__ sum
   if (st->converged || st->iteration >= fp.max_steps) st->active = 0;
 }
 
+// The FP64 engine takes over a minimisation whose problems converged under
+// the mixed-precision forces: they continue until the FP64 forces meet the
+// tolerance too (problems stopped by an uphill error or the step limit stay
+// stopped).
+__global__ void k_fire_reactivate(FireDevState* st, int max_steps) {
+  st += blockIdx.x;
+  if (threadIdx.x != 0) return;
+  if (!st->active && st->converged && !st->uphill_error && st->iteration < max_steps) {
+    st->converged = 0;
+    st->active = 1;
+  }
+}
+
 // ---------------------------------------------------------------- DDFT
 
 // dynamics.hpp:135-206: R = div(rho grad(force/dV)) - lap(rho).
@@ -398,10 +412,26 @@ __global__ void k_ddft_rhs(const double* __restrict__ rho, const double* __restr
   }
 }
 
-// dynamics.hpp:247-287: work = U0 rho0_k + U1 R0_k + U2 (R1_k - R0_k).
+// Device-side control state of one integrating-factor step.
+struct DdftDevState {
+  double dt;               // the time step of the current attempt
+  double deviation;        // max |d1_new - d1| of the last iteration
+  double min_density;      // min d1_new of the last iteration
+  double refine_deviation; // deviation of the last FP64 refinement iteration
+  int it;                  // iterations of the current attempt
+  int total_it;            // iterations of the step
+  int restarts;
+  int status;              // 0 iterating, 1 converged, 2 gave up
+  int copy_back;           // the attempt restarts: d1 <- rho
+  int pad;
+};
+
+// dynamics.hpp:247-287: work = U0 rho0_k + U1 R0_k + U2 (R1_k - R0_k), at
+// the control state's dt.
 __global__ void k_ddft_propagate(const double2* __restrict__ rho0k, const double2* __restrict__ r0k,
                                  double2* __restrict__ r1k_work, const double* __restrict__ lam, int nx, int ny,
-                                 int nzh, double dt) {
+                                 int nzh, const DdftDevState* __restrict__ st) {
+  const double dt = st->dt;
   const long long Nk = (long long)nx * ny * nzh;
   for (long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x; pos < Nk;
        pos += (long long)gridDim.x * blockDim.x) {
@@ -461,6 +491,64 @@ __global__ void k_maxmin_finish(const double* __restrict__ partials, int nb, dou
   }
   out[0] = mx;
   out[1] = mn;
+}
+
+// Start of a step's fixed-point loop (dt is set by the host beforehand).
+__global__ void k_ddft_begin(DdftDevState* st) {
+  if (threadIdx.x != 0) return;
+  st->deviation = 1e30;
+  st->min_density = 0.0;
+  st->refine_deviation = 0.0;
+  st->it = st->total_it = st->restarts = st->status = st->copy_back = 0;
+}
+
+// One fixed-point iteration's decision (dynamics.hpp:362-389): a negative
+// density or a growing deviation restarts the attempt at dt / 10 from rho, as
+// does a deviation still above the tolerance after fp_max iterations; a
+// deviation below it ends the loop.  With use_cond the loop's conditional
+// node continues while the status is 0.  After max_restarts restarts the
+// step gives up (status 2) with the last iterate.
+__global__ void k_ddft_control(DdftDevState* st, const double* __restrict__ red, double tol, int fp_max,
+                               int max_restarts, cudaGraphConditionalHandle cond, int use_cond) {
+  if (threadIdx.x != 0) return;
+  const double old = st->deviation;
+  const double dev = red[0], mn = red[1];
+  st->it += 1;
+  st->total_it += 1;
+  st->deviation = dev;
+  st->min_density = mn;
+  st->copy_back = 0;
+  bool restart = false;
+  if (mn < 0.0 || (st->it > 1 && dev > old))
+    restart = true;
+  else if (dev < tol)
+    st->status = 1;
+  else if (st->it >= fp_max)
+    restart = true;
+  if (restart) {
+    st->restarts += 1;
+    if (st->restarts >= max_restarts) {
+      st->status = 2;
+    } else {
+      st->dt /= 10.0;
+      st->it = 0;
+      st->deviation = 1e30;
+      st->copy_back = 1;
+    }
+  }
+  if (use_cond) cudaGraphSetConditional(cond, st->status == 0 ? 1u : 0u);
+}
+
+// d1 <- rho when the attempt restarts.
+__global__ void k_ddft_copy_back(const DdftDevState* __restrict__ st, const double* __restrict__ rho,
+                                 double* __restrict__ d1, long long N) {
+  if (!st->copy_back) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+    d1[i] = rho[i];
+}
+
+__global__ void k_ddft_refine_record(DdftDevState* st, const double* __restrict__ red) {
+  if (threadIdx.x == 0) st->refine_deviation = red[0];
 }
 
 // ------------------------------------------------------------------- HVP
@@ -1017,13 +1105,22 @@ std::vector<FireResult> Drivers::fire_loop(const FireConfig& cfg, const double* 
       const FireDevState& h = st_host_[b];
       if (!h.active) continue;
       any_active = true;
-      if (!(h.iteration > 0 && h.monitor < refine_switch * fp.force_tolerance)) all_close = false;
+      const double metric = cfg.use_monitor ? h.monitor : h.rms_force;
+      if (!(h.iteration > 0 && metric < refine_switch * fp.force_tolerance)) all_close = false;
+    }
+    if (refine && !refining && all_close && steps < fp.max_steps) {
+      // FP64 defect correction from here on: once every running problem is
+      // within refine_switch of the tolerance, or once all of them have
+      // converged under the mixed-precision forces
+      eng = refine;
+      refining = true;
+      if (!any_active) {
+        k_fire_reactivate<<<B, 32, 0, stream>>>(st_, fp.max_steps);
+        CDFT_CUDA(cudaGetLastError());
+        any_active = true;
+      }
     }
     if (!any_active || steps >= fp.max_steps) break;
-    if (refine && !refining && cfg.use_monitor && all_close) {
-      eng = refine;  // FP64 defect correction from here on
-      refining = true;
-    }
     const int chunk = std::max(1, std::min(cfg.check_interval, fp.max_steps - steps));
     // one FIRE step (fire.hpp:86-165): the v and x updates, then compute
     auto step = [&] {
@@ -1101,110 +1198,212 @@ void Drivers::ensure_ddft() {
   CDFT_CUDA(cudaMemcpy(lam_, lam.data(), sizeof(double) * lam.size(), cudaMemcpyHostToDevice));
   CDFT_CUFFT(cufftPlan3d(&plan_r2c_, p.nx, p.ny, p.nz, CUFFT_D2Z));
   CDFT_CUFFT(cufftPlan3d(&plan_c2r_, p.nx, p.ny, p.nz, CUFFT_Z2D));
+  CDFT_CUDA(cudaMalloc(&ddft_st_, sizeof(DdftDevState)));
+  CDFT_CUDA(cudaMallocHost(&ddft_st_host_, sizeof(DdftDevState)));
+  std::memset(ddft_st_host_, 0, sizeof(DdftDevState));
   ddft_ready_ = true;
 }
 
-// The step on the caller's stream, or (step graphs on) on the driver's
-// stream, joined to the caller's by events, with each fixed-point iteration
-// replayed as a captured CUDA graph.
-double Drivers::ddft_step(DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations) {
-  const bool graphs = step_graphs() && !eng_.stage_timing_on();
-  if (!graphs) return ddft_step_on(cfg, rho, stream, fp_iterations, false);
-  ensure_graph_stream();
-  CDFT_CUDA(cudaEventRecord(graph_ev_[0], stream));
-  CDFT_CUDA(cudaStreamWaitEvent(graph_stream_, graph_ev_[0], 0));
-  double e = 0.0;
-  try {
-    e = ddft_step_on(cfg, rho, graph_stream_, fp_iterations, true);
-  } catch (...) {
-    reset_fp_graph();
-    cudaEventRecord(graph_ev_[1], graph_stream_);
-    cudaStreamWaitEvent(stream, graph_ev_[1], 0);
-    throw;
+void Drivers::set_ddft_refine(Engine* refine, int iterations) {
+  if (refine) {
+    if (refine->precision() != kFP64) throw Error(-1, "ddft: the refine engine must be FP64");
+    if (refine->points() != N_ || refine->species() != 1 || refine->batch() != 1)
+      throw Error(-1, "ddft: the refine engine must have the driver's grid, one species and batch 1");
+    if (iterations < 1) throw Error(-1, "ddft: refine iterations must be >= 1");
   }
-  CDFT_CUDA(cudaEventRecord(graph_ev_[1], graph_stream_));
-  CDFT_CUDA(cudaStreamWaitEvent(stream, graph_ev_[1], 0));
-  return e;
+  ddft_refine_ = refine;
+  ddft_refine_iterations_ = refine ? iterations : 0;
 }
 
-double Drivers::ddft_step_on(DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations, bool graphs) {
-  ensure_ddft();
+// compute(rho0), R0_k and rho0_k (dynamics.hpp:347-354) from the step's
+// copy of rho (v_), the iterate d1 (x_) <- rho, the control state reset.
+void Drivers::ddft_prologue(const DDFTConfig& cfg, cudaStream_t s) {
   const EvalParams& p = eng_.params();
-  CDFT_CUFFT(cufftSetStream(plan_r2c_, stream));
-  CDFT_CUFFT(cufftSetStream(plan_c2r_, stream));
+  CDFT_CUFFT(cufftSetStream(plan_r2c_, s));
+  double2* rho0k = static_cast<double2*>(ddft_k_);
+  double2* r0k = rho0k + p.Nk;
+  const double mu = cfg.mu;
+  eng_.evaluate(v_, nullptr, &mu, grad_, scalars_, s);
+  k_ddft_rhs<<<grid_, kBlock, 0, s>>>(v_, grad_, tmp_, p.nx, p.ny, p.nz, p.dx, 1.0 / p.dv);
+  CDFT_CUFFT(cufftExecD2Z(plan_r2c_, tmp_, r0k));
+  CDFT_CUFFT(cufftExecD2Z(plan_r2c_, v_, rho0k));
+  CDFT_CUDA(cudaMemcpyAsync(x_, v_, sizeof(double) * N_, cudaMemcpyDeviceToDevice, s));
+  k_ddft_begin<<<1, 32, 0, s>>>(static_cast<DdftDevState*>(ddft_st_));
+  CDFT_CUDA(cudaGetLastError());
+}
+
+// One fixed-point iteration (dynamics.hpp:362-389) and its decision.
+void Drivers::ddft_body(const DDFTConfig& cfg, cudaStream_t s, unsigned long long cond, int use_cond) {
+  const EvalParams& p = eng_.params();
+  CDFT_CUFFT(cufftSetStream(plan_r2c_, s));
+  CDFT_CUFFT(cufftSetStream(plan_c2r_, s));
   double2* rho0k = static_cast<double2*>(ddft_k_);
   double2* r0k = rho0k + p.Nk;
   double2* work = r0k + p.Nk;
-  double* d1 = x_;       // the iterate
-  double* f1 = grad_;    // forces
-  double* rhs = tmp_;    // R(rho) in real space
+  DdftDevState* st = static_cast<DdftDevState*>(ddft_st_);
   const double mu = cfg.mu;
-  // compute(rho0), R0_k, rho0_k (dynamics.hpp:347-354)
-  eng_.evaluate(rho, nullptr, &mu, f1, scalars_, stream);
-  k_ddft_rhs<<<grid_, kBlock, 0, stream>>>(rho, f1, rhs, p.nx, p.ny, p.nz, p.dx, 1.0 / p.dv);
-  CDFT_CUFFT(cufftExecD2Z(plan_r2c_, rhs, r0k));
-  CDFT_CUFFT(cufftExecD2Z(plan_r2c_, rho, rho0k));
-  int total_it = 0;
-  for (int restarts = 0; restarts < 64; ++restarts) {
-    bool restart = false;
-    const double dt = cfg.dt;
-    CDFT_CUDA(cudaMemcpyAsync(d1, rho, sizeof(double) * N_, cudaMemcpyDeviceToDevice, stream));
-    double deviation = 1e30;
-    // one fixed-point iteration (dynamics.hpp:362-389); its arguments are
-    // the driver's buffers, dt and mu
-    auto iteration = [&] {
-      eng_.evaluate(d1, nullptr, &mu, f1, scalars_, stream);
-      k_ddft_rhs<<<grid_, kBlock, 0, stream>>>(d1, f1, rhs, p.nx, p.ny, p.nz, p.dx, 1.0 / p.dv);
-      CDFT_CUFFT(cufftExecD2Z(plan_r2c_, rhs, work));
-      k_ddft_propagate<<<grid_, kBlock, 0, stream>>>(rho0k, r0k, work, lam_, p.nx, p.ny, p.nzh, dt);
-      CDFT_CUFFT(cufftExecZ2D(plan_c2r_, work, tmp2_));
-      k_ddft_update<<<grid_, kBlock, 0, stream>>>(tmp2_, d1, N_, 1.0 / (double)N_, red_);
-      k_maxmin_finish<<<1, 32, 0, stream>>>(red_, grid_, red_out_);
-      CDFT_CUDA(cudaMemcpyAsync(host_pin_, red_out_, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
-    };
-    const unsigned long long path = eng_.generation();
-    if (graphs && !(fp_exec_ && fp_dt_ == dt && fp_mu_ == mu && fp_path_ == path)) {
-      reset_fp_graph();
-      CDFT_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-      try {
-        iteration();
-      } catch (...) {
-        cudaGraph_t g = nullptr;
-        cudaStreamEndCapture(stream, &g);
-        if (g) cudaGraphDestroy(g);
-        throw;
-      }
-      CDFT_CUDA(cudaStreamEndCapture(stream, &fp_graph_));
-      CDFT_CUDA(cudaGraphInstantiate(&fp_exec_, fp_graph_, 0));
-      fp_dt_ = dt;
-      fp_mu_ = mu;
-      fp_path_ = path;
-    }
-    for (int it = 0; it < cfg.fp_max_iterations; ++it) {
-      ++total_it;
-      if (graphs)
-        CDFT_CUDA(cudaGraphLaunch(fp_exec_, stream));
-      else
-        iteration();
-      CDFT_CUDA(cudaStreamSynchronize(stream));
-      const double old = deviation;
-      deviation = host_pin_[0];
-      if (host_pin_[1] < 0.0 || (it > 0 && deviation > old)) {
-        restart = true;
-        break;
-      }
-      if (deviation < cfg.fp_tolerance) break;
-    }
-    if (!restart && deviation > cfg.fp_tolerance) restart = true;
-    if (!restart) break;
-    cfg.dt /= 10.0;
+  eng_.evaluate(x_, nullptr, &mu, grad_, scalars_, s);
+  k_ddft_rhs<<<grid_, kBlock, 0, s>>>(x_, grad_, tmp_, p.nx, p.ny, p.nz, p.dx, 1.0 / p.dv);
+  CDFT_CUFFT(cufftExecD2Z(plan_r2c_, tmp_, work));
+  k_ddft_propagate<<<grid_, kBlock, 0, s>>>(rho0k, r0k, work, lam_, p.nx, p.ny, p.nzh, st);
+  CDFT_CUFFT(cufftExecZ2D(plan_c2r_, work, tmp2_));
+  k_ddft_update<<<grid_, kBlock, 0, s>>>(tmp2_, x_, N_, 1.0 / (double)N_, red_);
+  k_maxmin_finish<<<1, 32, 0, s>>>(red_, grid_, red_out_);
+  k_ddft_control<<<1, 32, 0, s>>>(st, red_out_, cfg.fp_tolerance, cfg.fp_max_iterations, kMaxRestarts,
+                                  static_cast<cudaGraphConditionalHandle>(cond), use_cond);
+  k_ddft_copy_back<<<grid_, kBlock, 0, s>>>(st, v_, x_, N_);
+  CDFT_CUDA(cudaGetLastError());
+}
+
+// The FP64 refinement iterations (if any) and the final compute
+// (dynamics.hpp:394).
+void Drivers::ddft_epilogue(const DDFTConfig& cfg, cudaStream_t s) {
+  const EvalParams& p = eng_.params();
+  CDFT_CUFFT(cufftSetStream(plan_r2c_, s));
+  CDFT_CUFFT(cufftSetStream(plan_c2r_, s));
+  double2* rho0k = static_cast<double2*>(ddft_k_);
+  double2* r0k = rho0k + p.Nk;
+  double2* work = r0k + p.Nk;
+  DdftDevState* st = static_cast<DdftDevState*>(ddft_st_);
+  const double mu = cfg.mu;
+  Engine& fin = ddft_refine_ ? *ddft_refine_ : eng_;
+  for (int r = 0; r < ddft_refine_iterations_; ++r) {
+    ddft_refine_->evaluate(x_, nullptr, &mu, grad_, scalars_, s);
+    k_ddft_rhs<<<grid_, kBlock, 0, s>>>(x_, grad_, tmp_, p.nx, p.ny, p.nz, p.dx, 1.0 / p.dv);
+    CDFT_CUFFT(cufftExecD2Z(plan_r2c_, tmp_, work));
+    k_ddft_propagate<<<grid_, kBlock, 0, s>>>(rho0k, r0k, work, lam_, p.nx, p.ny, p.nzh, st);
+    CDFT_CUFFT(cufftExecZ2D(plan_c2r_, work, tmp2_));
+    k_ddft_update<<<grid_, kBlock, 0, s>>>(tmp2_, x_, N_, 1.0 / (double)N_, red_);
+    k_maxmin_finish<<<1, 32, 0, s>>>(red_, grid_, red_out_);
+    k_ddft_refine_record<<<1, 32, 0, s>>>(st, red_out_);
   }
-  if (fp_iterations) *fp_iterations = total_it;
-  // final compute (dynamics.hpp:394)
-  eng_.evaluate(d1, nullptr, &mu, f1, scalars_, stream);
-  CDFT_CUDA(cudaMemcpyAsync(rho, d1, sizeof(double) * N_, cudaMemcpyDeviceToDevice, stream));
-  CDFT_CUDA(cudaMemcpyAsync(host_pin_, scalars_, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
-  CDFT_CUDA(cudaStreamSynchronize(stream));
+  fin.evaluate(x_, nullptr, &mu, grad_, scalars_, s);
+  CDFT_CUDA(cudaGetLastError());
+}
+
+// Capture of the whole step on the driver stream: prologue, a conditional
+// WHILE node whose body (captured on a second stream into the node's body
+// graph) is one fixed-point iteration, then the epilogue.
+void Drivers::capture_ddft_step(const DDFTConfig& cfg) {
+  reset_fp_graph();
+  if (!body_stream_) CDFT_CUDA(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
+  cudaStream_t s = graph_stream_;
+  auto abort_capture = [&] {
+    for (cudaStream_t t : {body_stream_, s}) {
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      cudaStreamIsCapturing(t, &cs);
+      if (cs != cudaStreamCaptureStatusNone) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(t, &g);
+        if (g) cudaGraphDestroy(g);
+      }
+    }
+    cudaGetLastError();
+  };
+  CDFT_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  try {
+    ddft_prologue(cfg, s);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    CDFT_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd));
+    cudaGraphConditionalHandle h = 0;
+    CDFT_CUDA(cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault));
+    // zero-filled storage: the parameter union has no default constructor
+    alignas(cudaGraphNodeParams) unsigned char np_buf[sizeof(cudaGraphNodeParams)] = {};
+    cudaGraphNodeParams& np = *reinterpret_cast<cudaGraphNodeParams*>(np_buf);
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    CDFT_CUDA(cudaGraphAddNode(&node, cg, deps, nd, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    CDFT_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    CDFT_CUDA(cudaStreamBeginCaptureToGraph(body_stream_, body, nullptr, nullptr, 0,
+                                            cudaStreamCaptureModeThreadLocal));
+    ddft_body(cfg, body_stream_, h, 1);
+    cudaGraph_t body_out = nullptr;
+    CDFT_CUDA(cudaStreamEndCapture(body_stream_, &body_out));
+    ddft_epilogue(cfg, s);
+    CDFT_CUDA(cudaStreamEndCapture(s, &fp_graph_));
+  } catch (...) {
+    abort_capture();
+    reset_fp_graph();
+    throw;
+  }
+  CDFT_CUDA(cudaGraphInstantiate(&fp_exec_, fp_graph_, 0));
+}
+
+// integrating_factor_step (dynamics.hpp:333-401).  With step graphs on, the
+// step runs on the driver's stream, joined to the caller's by events, as one
+// graph launch; the host reads the control state and the energy once.
+double Drivers::ddft_step(DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations) {
+  ensure_ddft();
+  const bool graphs = step_graphs() && !eng_.stage_timing_on() && !(ddft_refine_ && ddft_refine_->stage_timing_on());
+  cudaStream_t s = stream;
+  if (graphs) {
+    ensure_graph_stream();
+    CDFT_CUDA(cudaEventRecord(graph_ev_[0], stream));
+    CDFT_CUDA(cudaStreamWaitEvent(graph_stream_, graph_ev_[0], 0));
+    s = graph_stream_;
+  }
+  DdftDevState* hst = static_cast<DdftDevState*>(ddft_st_host_);
+  try {
+    hst->dt = cfg.dt;
+    CDFT_CUDA(cudaMemcpyAsync(ddft_st_, hst, sizeof(double), cudaMemcpyHostToDevice, s));
+    CDFT_CUDA(cudaMemcpyAsync(v_, rho, sizeof(double) * N_, cudaMemcpyDeviceToDevice, s));
+    if (graphs) {
+      DDFTGraphKey key;
+      key.mu = cfg.mu;
+      key.tol = cfg.fp_tolerance;
+      key.min_density = cfg.min_density;
+      key.diffusion = cfg.diffusion;
+      key.fp_max = cfg.fp_max_iterations;
+      key.refine_iterations = ddft_refine_iterations_;
+      key.refine = ddft_refine_;
+      key.gen = eng_.generation();
+      key.refine_gen = ddft_refine_ ? ddft_refine_->generation() : 0;
+      if (!fp_exec_ || !(key == fp_key_)) {
+        capture_ddft_step(cfg);
+        fp_key_ = key;
+      }
+      CDFT_CUDA(cudaGraphLaunch(fp_exec_, s));
+    } else {
+      ddft_prologue(cfg, s);
+      // the same kernels, the host reading the decision after every iteration
+      for (int guard = 0; guard < (kMaxRestarts + 1) * std::max(cfg.fp_max_iterations, 1); ++guard) {
+        ddft_body(cfg, s, 0, 0);
+        CDFT_CUDA(cudaMemcpyAsync(hst, ddft_st_, sizeof(DdftDevState), cudaMemcpyDeviceToHost, s));
+        CDFT_CUDA(cudaStreamSynchronize(s));
+        if (hst->status != 0) break;
+      }
+      ddft_epilogue(cfg, s);
+    }
+    CDFT_CUDA(cudaMemcpyAsync(rho, x_, sizeof(double) * N_, cudaMemcpyDeviceToDevice, s));
+    CDFT_CUDA(cudaMemcpyAsync(hst, ddft_st_, sizeof(DdftDevState), cudaMemcpyDeviceToHost, s));
+    CDFT_CUDA(cudaMemcpyAsync(host_pin_, scalars_, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+    CDFT_CUDA(cudaStreamSynchronize(s));
+  } catch (...) {
+    if (graphs) {
+      reset_fp_graph();
+      cudaEventRecord(graph_ev_[1], graph_stream_);
+      cudaStreamWaitEvent(stream, graph_ev_[1], 0);
+    }
+    throw;
+  }
+  if (graphs) {
+    CDFT_CUDA(cudaEventRecord(graph_ev_[1], graph_stream_));
+    CDFT_CUDA(cudaStreamWaitEvent(stream, graph_ev_[1], 0));
+  }
+  cfg.dt = hst->dt;
+  ddft_info_.fp_iterations = hst->total_it;
+  ddft_info_.restarts = hst->restarts;
+  ddft_info_.status = hst->status;
+  ddft_info_.device_loop = graphs ? 1 : 0;
+  ddft_info_.refine_deviation = hst->refine_deviation;
+  if (fp_iterations) *fp_iterations = hst->total_it;
   return host_pin_[1];
 }
 
@@ -1213,7 +1412,28 @@ double Drivers::ddft_step_on(DDFTConfig& cfg, double* rho, cudaStream_t stream, 
 namespace cdft {
 
 Drivers::EigenResult Drivers::eigen_solve(const EigenConfig& cfg, const double* rho, double mu, double* vec,
-                                          bool use_guess, cudaStream_t stream) {
+                                          bool use_guess, cudaStream_t stream, Engine* hvp_engine) {
+  if (cfg.method == kLanczos) {
+    if (!cfg.exact_hvp) throw Error(-1, "eigen: the Lanczos solver needs exact products (exact_hvp = 1)");
+    Engine& he = hvp_engine ? *hvp_engine : eng_;
+    if (he.points() != N_ || he.species() != 1)
+      throw Error(-1, "eigen: the product engine must have the driver's grid and one species");
+    LanczosConfig lc;
+    lc.tolerance = cfg.tolerance;
+    lc.max_iterations = cfg.max_iterations;
+    lc.block = cfg.block;
+    lc.max_basis = cfg.max_basis;
+    lc.check_interval = cfg.check_interval;
+    lc.seed = cfg.seed;
+    const LanczosResult lr = lanczos_lowest(he, lc, rho, vec, use_guess, stream);
+    EigenResult r;
+    r.eigenvalue = lr.eigenvalue;
+    r.iterations = lr.iterations;
+    r.converged = lr.converged;
+    (void)mu;  // the Hessian does not depend on mu
+    return r;
+  }
+  if (cfg.method != kRayleighRitz) throw Error(-1, "eigen: unknown method");
   for (double*& p : ev_)
     if (!p) CDFT_CUDA(cudaMalloc(&p, sizeof(double) * N_));
   double* f0 = ev_[0];
@@ -1294,7 +1514,8 @@ Drivers::EigenResult Drivers::eigen_solve(const EigenConfig& cfg, const double* 
 }
 
 Drivers::SaddleResult Drivers::saddle_find(const SaddleConfig& cfg, double* rho, double mu, double target_mass,
-                                           double* eigvec, cudaStream_t stream) {
+                                           double* eigvec, cudaStream_t stream, Engine* refine, Engine* hvp_engine,
+                                           double refine_switch) {
   const EvalParams& p = eng_.params();
   double* dir = nullptr;
   CDFT_CUDA(cudaMalloc(&dir, sizeof(double) * N_));
@@ -1309,9 +1530,10 @@ Drivers::SaddleResult Drivers::saddle_find(const SaddleConfig& cfg, double* rho,
       const bool guess = have_vec && outer >= cfg.eigenvalue_clear_count;
       EigenConfig ec = cfg.eigen;
       ec.seed = cfg.eigen.seed + (unsigned long long)outer;
-      EigenResult er = eigen_solve(ec, rho, mu, eigvec, guess, stream);
+      EigenResult er = eigen_solve(ec, rho, mu, eigvec, guess, stream, hvp_engine);
       have_vec = true;
       res.eigenvalue = er.eigenvalue;
+      res.eigen_iterations += er.iterations;
       // direction in parameter space, normalised (saddle_point.hpp:424-430)
       k_dir_alias<<<grid_, kBlock, 0, stream>>>(eigvec, rho, dir, N_, cfg.rho_min);
       const double dn = std::sqrt(dot(dir, dir, N_, stream));
@@ -1336,9 +1558,10 @@ Drivers::SaddleResult Drivers::saddle_find(const SaddleConfig& cfg, double* rho,
       fc.target_mass = target_mass;
       fc.boundary_mass = avg * p.dv * n_face;
       fc.use_monitor = false;
-      FireResult fr = fire_minimize(fc, rho, dir, stream);
+      FireResult fr = fire_minimize(fc, rho, dir, stream, refine, refine_switch);
       if (fr.uphill_error) throw Error(-2, "fire::step: exceeded max uphill steps");
       omega = fr.grand_potential;
+      res.fire_steps += fr.iterations;
       if (outer > 0 && std::abs(omega - omega_old) < cfg.omega_tolerance) {
         res.converged = true;
         break;
@@ -1350,7 +1573,7 @@ Drivers::SaddleResult Drivers::saddle_find(const SaddleConfig& cfg, double* rho,
   }
   cudaFree(dir);
   res.grand_potential = omega;
-  res.outer_iterations = std::min(outer + 1, cfg.max_outer_iterations);
+  res.outer_iterations = outer + 1;  // as the reference reports it (saddle_point.hpp:584)
   return res;
 }
 

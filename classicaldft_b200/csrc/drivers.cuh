@@ -110,7 +110,30 @@ class Drivers {
     int fp_max_iterations = 100;
     double mu = 0.0;
   };
+  // The whole step runs on the device: with step graphs on (the default) it
+  // is one CUDA graph whose fixed-point loop is a conditional WHILE node, the
+  // restart decisions (negative density, growing deviation, no convergence
+  // in fp_max_iterations: dt /= 10 and start again) taken by a one-thread
+  // control kernel that also ends the loop; after kMaxRestarts restarts the
+  // step gives up with the last iterate, as the host loop did.  With graphs
+  // off the host launches the same kernels iteration by iteration.
+  static constexpr int kMaxRestarts = 64;
   double ddft_step(DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations = nullptr);
+  // FP64 defect correction of a mixed-precision IF step: after the fixed
+  // point has converged with this driver's engine, `iterations` more
+  // iterations use the FP64 `refine` engine (same model), which also gives
+  // the step's final forces and energy.  Null clears it.  Applies to
+  // ddft_step and ddft_run.
+  void set_ddft_refine(Engine* refine, int iterations);
+  // Facts of the last IF step: fixed-point iterations, restarts, status
+  // (1 converged, 2 gave up after kMaxRestarts), 1 if the loop ran as a
+  // device-side conditional node, and the deviation of the last FP64
+  // refinement iteration (0 without one).
+  struct DDFTStepInfo {
+    int fp_iterations = 0, restarts = 0, status = 0, device_loop = 0;
+    double refine_deviation = 0.0;
+  };
+  const DDFTStepInfo& last_ddft_step() const { return ddft_info_; }
 
   // split_operator_step (dynamics.hpp:410-465): half diffusion in k-space,
   // forward-Euler excess step, half diffusion; returns the energy after it.
@@ -180,20 +203,32 @@ class Drivers {
   // reference's 3-vector Rayleigh-Ritz iteration.  `vec` (device, N) holds
   // the initial guess if `use_guess`, else a seeded normal vector is drawn;
   // it receives the unit eigenvector.
+  // method kRayleighRitz is the reference's solver; kLanczos the block
+  // Lanczos of lanczos.cuh on exact products (block directions per batched
+  // product; the product engine's batch must equal `block`).
+  enum EigenMethod : int { kRayleighRitz = 0, kLanczos = 1 };
   struct EigenConfig {
     double tolerance = 1e-4;
     int max_iterations = 300;
     double hessian_eps = 1e-6;
     int exact_hvp = 0;
     unsigned long long seed = 42;
+    int method = kRayleighRitz;
+    int block = 1;
+    int max_basis = 32;
+    int check_interval = 4;
   };
   struct EigenResult {
     double eigenvalue = 0.0;
     int iterations = 0;
     bool converged = false;
   };
+  // `hvp_engine` (Lanczos only; null: this driver's engine, batch 1): an
+  // engine of the same model whose batch is the Lanczos block size, used for
+  // the batched exact products (an FP64 engine gives FP64 products under a
+  // mixed-precision driver).
   EigenResult eigen_solve(const EigenConfig& cfg, const double* rho, double mu, double* vec, bool use_guess,
-                          cudaStream_t stream);
+                          cudaStream_t stream, Engine* hvp_engine = nullptr);
 
   // Search::find (saddle_point.hpp:324-589): eigenvector following at fixed
   // mass.  rho (device, N) is replaced by the saddle density, eigvec (device,
@@ -209,9 +244,15 @@ class Drivers {
     double grand_potential = 0.0, eigenvalue = 0.0;
     int outer_iterations = 0;
     bool converged = false;
+    int eigen_iterations = 0;  // summed over the outer iterations
+    int fire_steps = 0;        // summed over the outer iterations
   };
+  // `refine`: an FP64 engine that finishes each projected FIRE run (mixed-
+  // precision defect correction, as fire_minimize); `hvp_engine`: the
+  // product engine of a Lanczos eigen solve (see eigen_solve).
   SaddleResult saddle_find(const SaddleConfig& cfg, double* rho, double mu, double target_mass, double* eigvec,
-                           cudaStream_t stream);
+                           cudaStream_t stream, Engine* refine = nullptr, Engine* hvp_engine = nullptr,
+                           double refine_switch = 10.0);
 
   Engine& engine() { return eng_; }
 
@@ -231,13 +272,32 @@ class Drivers {
   const void* step_key_ = nullptr;
   void reset_step_graph();
   void ensure_graph_stream();
-  // CUDA graph of one DDFT fixed-point iteration (its arguments: dt, mu)
+  // CUDA graph of one IF step, its device-side control state and its key
+  // (everything baked into its kernel arguments)
   cudaGraph_t fp_graph_ = nullptr;
   cudaGraphExec_t fp_exec_ = nullptr;
-  double fp_dt_ = 0.0, fp_mu_ = 0.0;
-  unsigned long long fp_path_ = 0;  // the engine's generation at capture
+  struct DDFTGraphKey {
+    double mu = 0.0, tol = 0.0, min_density = 0.0, diffusion = 0.0;
+    int fp_max = 0, refine_iterations = 0;
+    const Engine* refine = nullptr;
+    unsigned long long gen = 0, refine_gen = 0;
+    bool operator==(const DDFTGraphKey& o) const {
+      return mu == o.mu && tol == o.tol && min_density == o.min_density && diffusion == o.diffusion &&
+             fp_max == o.fp_max && refine_iterations == o.refine_iterations && refine == o.refine && gen == o.gen &&
+             refine_gen == o.refine_gen;
+    }
+  } fp_key_;
   void reset_fp_graph();
-  double ddft_step_on(DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations, bool graphs);
+  void ddft_prologue(const DDFTConfig& cfg, cudaStream_t s);
+  void ddft_body(const DDFTConfig& cfg, cudaStream_t s, unsigned long long cond, int use_cond);
+  void ddft_epilogue(const DDFTConfig& cfg, cudaStream_t s);
+  void capture_ddft_step(const DDFTConfig& cfg);
+  void* ddft_st_ = nullptr;       // device control state of the IF step
+  void* ddft_st_host_ = nullptr;  // pinned copy
+  cudaStream_t body_stream_ = nullptr;
+  Engine* ddft_refine_ = nullptr;
+  int ddft_refine_iterations_ = 0;
+  DDFTStepInfo ddft_info_;
 
   Engine& eng_;
   long long N_ = 0;

@@ -765,26 +765,38 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
 // kernel carries it through dPhi with dual numbers; the back-convolution is
 // linear.
 template <typename R, typename C2>
-void Engine::run_hvp(const double* rho, const double* v, const double* mu, double* hv, cudaStream_t stream) {
+void Engine::run_hvp_point(const double* rho, cudaStream_t stream) {
   const EvalParams& p = p_;
-  constexpr bool mixed = sizeof(R) == sizeof(float);
-  if (p.batch != 1) throw Error(-1, "hvp: needs an engine with batch 1");
+  const size_t SN = (size_t)p.S * p.N;
   for (cufftHandle h : {plan_rho_, plan_chan_, plan_deriv_, plan_force_}) CDFT_CUFFT(cufftSetStream(h, stream));
   if (!tan_chan_) {
-    const size_t rs = mixed ? sizeof(float) : sizeof(double);
-    CDFT_CUDA(cudaMalloc(&tan_chan_, rs * p.n_chan * p.N));
-    CDFT_CUDA(cudaMalloc(&tan_mean_, sizeof(double) * kMaxSpecies));
-    CDFT_CUDA(cudaMalloc(&tan_dbar_, sizeof(double) * kMaxChannels));
-    CDFT_CUDA(cudaMalloc(&tan_in_, sizeof(double) * 2 * p.S * p.N));
+    const size_t rs = sizeof(R);
+    CDFT_CUDA(cudaMalloc(&tan_chan_, rs * p.batch * p.n_chan * p.N));
+    CDFT_CUDA(cudaMalloc(&tan_mean_, sizeof(double) * p.batch * kMaxSpecies));
+    CDFT_CUDA(cudaMalloc(&tan_dbar_, sizeof(double) * p.batch * kMaxChannels));
+    CDFT_CUDA(cudaMalloc(&tan_in_, sizeof(double) * 2 * p.batch * SN));
   }
+  // every problem slot holds the same density: its channels and (mixed) its
+  // species means are computed once here for all the directions of later
+  // hvp_apply calls
+  for (int b = 0; b < p.batch; ++b)
+    CDFT_CUDA(cudaMemcpyAsync(tan_in_ + b * SN, rho, sizeof(double) * SN, cudaMemcpyDeviceToDevice, stream));
+  forward_stage<R, C2>(tan_in_, static_cast<R*>(chan_r_), mean_, stream);
+  hvp_ready_ = true;
+}
+
+template <typename R, typename C2>
+void Engine::run_hvp_apply(const double* v, double* hv, cudaStream_t stream) {
+  const EvalParams& p = p_;
+  constexpr bool mixed = sizeof(R) == sizeof(float);
+  const size_t SN = (size_t)p.S * p.N;
+  for (cufftHandle h : {plan_rho_, plan_chan_, plan_deriv_, plan_force_}) CDFT_CUFFT(cufftSetStream(h, stream));
   double* rho_al = tan_in_;
-  double* v_al = tan_in_ + p.S * p.N;
-  CDFT_CUDA(cudaMemcpyAsync(rho_al, rho, sizeof(double) * p.S * p.N, cudaMemcpyDeviceToDevice, stream));
-  CDFT_CUDA(cudaMemcpyAsync(v_al, v, sizeof(double) * p.S * p.N, cudaMemcpyDeviceToDevice, stream));
+  double* v_al = tan_in_ + p.batch * SN;
+  CDFT_CUDA(cudaMemcpyAsync(v_al, v, sizeof(double) * p.batch * SN, cudaMemcpyDeviceToDevice, stream));
   R* chan_r = static_cast<R*>(chan_r_);
   R* chan_t = static_cast<R*>(tan_chan_);
   R* deriv_r = static_cast<R*>(deriv_r_);
-  forward_stage<R, C2>(rho_al, chan_r, mean_, stream);
   forward_stage<R, C2>(v_al, chan_t, tan_mean_, stream);
   HvpArgs a;
   a.rho = rho_al;
@@ -799,20 +811,36 @@ void Engine::run_hvp(const double* rho, const double* v, const double* mu, doubl
     constexpr bool MU = decltype(multi_c)::value;
     using RT = typename decltype(r_c)::type;
     if constexpr (std::is_same_v<RT, R>)
-      k_pointwise_hvp<MD, MU, RT><<<grid_stream_, 128, 0, stream>>>(p, chan_r, chan_t, deriv_r, a);
+      k_pointwise_hvp<MD, MU, RT><<<dim3(grid_stream_, p.batch), 128, 0, stream>>>(p, chan_r, chan_t, deriv_r, a);
   });
   CDFT_CUDA(cudaGetLastError());
   MuArgs zero{};  // the Hessian does not depend on mu
   backward_stage<R, C2>(deriv_r, tan_dbar_, hv, zero, FinalArgs{nullptr, 0, nullptr, nullptr}, stream);
-  (void)mu;
+}
+
+void Engine::hvp_set_point(const double* rho, cudaStream_t stream) {
+  if (!rho) throw Error(-1, "hvp: rho is required");
+  if (precision_ == kMixed)
+    run_hvp_point<float, float2>(rho, stream);
+  else
+    run_hvp_point<double, double2>(rho, stream);
+}
+
+void Engine::hvp_apply(const double* v, double* hv, cudaStream_t stream) {
+  if (!v || !hv) throw Error(-1, "hvp: v and hv are required");
+  if (!hvp_ready_) throw Error(-1, "hvp: no point set since the last evaluation (hvp_set_point)");
+  if (precision_ == kMixed)
+    run_hvp_apply<float, float2>(v, hv, stream);
+  else
+    run_hvp_apply<double, double2>(v, hv, stream);
 }
 
 void Engine::hvp(const double* rho, const double* v, const double* mu, double* hv, cudaStream_t stream) {
   if (!rho || !v || !hv) throw Error(-1, "hvp: rho, v and hv are required");
-  if (precision_ == kMixed)
-    run_hvp<float, float2>(rho, v, mu, hv, stream);
-  else
-    run_hvp<double, double2>(rho, v, mu, hv, stream);
+  if (p_.batch != 1) throw Error(-1, "hvp: needs an engine with batch 1 (hvp_set_point / hvp_apply batch)");
+  (void)mu;
+  hvp_set_point(rho, stream);
+  hvp_apply(v, hv, stream);
 }
 
 int Engine::take_error(cudaStream_t stream) {
@@ -826,6 +854,7 @@ int Engine::take_error(cudaStream_t stream) {
 void Engine::evaluate(const double* rho, const double* vext, const double* mu, double* force, double* scalars,
                       cudaStream_t stream) {
   if (!rho || !force || !scalars || !mu) throw Error(-1, "evaluate: rho, mu, force and scalars are required");
+  hvp_ready_ = false;  // the channel buffers are the evaluation's
   if (precision_ == kMixed)
     run<float, float2>(rho, vext, mu, force, scalars, stream);
   else

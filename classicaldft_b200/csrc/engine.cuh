@@ -64,6 +64,14 @@ class Engine {
   // Hessian-vector product of Omega: hv = d(force)/d(rho) . v (S*N device
   // doubles each); exact, by forward-over-reverse differentiation.  Batch 1 only.
   void hvp(const double* rho, const double* v, const double* mu, double* hv, cudaStream_t stream);
+  // Products at one density for several directions (any batch B):
+  // hvp_set_point runs the forward pipeline of rho (S*N device doubles) once
+  // for every problem slot; hvp_apply then maps B directions v (B*S*N) to B
+  // products hv, each direction in its own problem slot of the batched
+  // launches.  An evaluate() in between invalidates the point (hvp_apply
+  // throws until it is set again).
+  void hvp_set_point(const double* rho, cudaStream_t stream);
+  void hvp_apply(const double* v, double* hv, cudaStream_t stream);
 
   const EvalParams& params() const { return p_; }
   int species() const { return p_.S; }
@@ -142,7 +150,10 @@ class Engine {
   void run(const double* rho, const double* vext, const double* mu, double* force, double* scalars,
            cudaStream_t stream);
   template <typename R, typename C2>
-  void run_hvp(const double* rho, const double* v, const double* mu, double* hv, cudaStream_t stream);
+  void run_hvp_point(const double* rho, cudaStream_t stream);
+  template <typename R, typename C2>
+  void run_hvp_apply(const double* v, double* hv, cudaStream_t stream);
+  bool hvp_ready_ = false;
   template <typename R, typename C2>
   void forward_stage(const double* in, R* chan_out, double* mean_out, cudaStream_t stream);
   template <typename R, typename C2>

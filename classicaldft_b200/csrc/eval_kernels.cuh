@@ -963,6 +963,20 @@ __global__ void __launch_bounds__(128) k_pointwise_hvp(EvalParams p, const RT* _
   __shared__ double s_off[kMaxChannels];
   __shared__ double s_toff[kMaxChannels];
   __shared__ double s_tdbar[NF];
+  {
+    // direction b of a batched product: its own problem slot of every array
+    const int b = blockIdx.y;
+    const long long cn = (long long)p.n_chan * p.N, sn = (long long)p.S * p.N;
+    chan += b * cn;
+    tchan += b * cn;
+    deriv += b * (long long)p.L.n_deriv * p.N;
+    a.rho += b * sn;
+    a.v += b * sn;
+    a.hv += b * sn;
+    a.mean += b * kMaxSpecies;
+    a.tmean += b * kMaxSpecies;
+    a.tdbar_out += b * kMaxChannels;
+  }
   if (SPLIT) {
     if (threadIdx.x == 0) {
       for (int c = 0; c < p.n_chan; ++c) s_off[c] = s_toff[c] = 0.0;

@@ -235,8 +235,11 @@ typedef struct {
  * and the projected FIRE of Search::find (saddle_point.hpp:445-530, mode
  * CDFT_MIN_SADDLE with `direction`).  rho: N doubles on the device, replaced
  * by the minimiser's final density.  `refine` (or NULL): an FP64 engine of
- * the same model that takes over once the monitor drops below
- * refine_switch * force_tolerance (mixed-precision defect correction).
+ * the same model that takes over once the convergence measure (the monitor,
+ * or the rms force when use_monitor is 0) drops below refine_switch *
+ * force_tolerance, or once the run has converged under the engine's own
+ * forces, and continues until the FP64 forces converge too (mixed-precision
+ * defect correction).
  * Returns CDFT_ERR_RUNTIME with "fire::step: exceeded max uphill steps" where
  * the reference throws (fire.hpp:106-108). */
 CDFT_API int cdft_minimize(cdft_engine* engine, const cdft_minimizer_config* cfg, double* rho,
@@ -268,6 +271,23 @@ typedef struct {
  * reference.  energy: Omega after the step. */
 CDFT_API int cdft_ddft_step(cdft_engine* engine, cdft_ddft_config* cfg, double chemical_potential, double* rho,
                             double* energy, int* fp_iterations, void* stream);
+
+/* FP64 defect correction of the integrating-factor steps of a mixed-
+ * precision engine (cdft_ddft_step, cdft_ddft_run, cdft_ddft_simulate): once
+ * a step's fixed point has converged with `engine`, `iterations` (>= 1) more
+ * fixed-point iterations run with the FP64 engine `refine` (same grid and
+ * model, batch 1), which also gives the step's final forces and energy.
+ * refine NULL clears it.  No reference counterpart (the reference has one
+ * precision). */
+CDFT_API int cdft_ddft_set_refine(cdft_engine* engine, cdft_engine* refine, int iterations);
+
+/* Facts of the engine's last integrating-factor step: info = {fixed-point
+ * iterations, restarts, status (1 converged, 2 gave up after 64 restarts with
+ * the last iterate), 1 if the fixed-point loop ran on the device as the
+ * conditional WHILE node of the step's CUDA graph (0: host-driven)};
+ * refine_deviation (or NULL): max |change| of the last FP64 refinement
+ * iteration (0 without refinement). */
+CDFT_API int cdft_ddft_last_step(cdft_engine* engine, int info[4], double* refine_deviation);
 
 /* Simulation::run (dynamics.hpp:583-693) without snapshots: n_steps steps
  * with the adaptive dt (x2 after 5 successes, capped at dt_max).
@@ -345,13 +365,23 @@ CDFT_API int cdft_hvp(cdft_engine* engine, const double* rho, const double* v, d
 CDFT_API int cdft_hvp_fd(cdft_engine* engine, const double* rho, const double* force_at_rho, const double* v,
                          double chemical_potential, double eps, int boundary, double* hv, void* stream);
 
-/* EigenvalueSolver (saddle_point.hpp:158-276). */
+/* EigenvalueSolver (saddle_point.hpp:158-276).  method
+ * CDFT_EIGEN_RAYLEIGH_RITZ is the reference's 3-vector iteration;
+ * CDFT_EIGEN_LANCZOS is block Lanczos on exact products (exact_hvp = 1) of
+ * the fixed-boundary Hessian restricted to the interior (the same operator,
+ * made symmetric): `block` directions per batched product (1..4), `max_basis`
+ * blocks before a restart, the host reading the projected matrix every
+ * `check_interval` products; zero fields take the defaults 1, 32 and 4. */
+#define CDFT_EIGEN_RAYLEIGH_RITZ 0
+#define CDFT_EIGEN_LANCZOS 1
 typedef struct {
   double tolerance;
   int max_iterations;
   double hessian_eps;
   int exact_hvp;            /* 1: cdft_hvp, 0: finite differences as the reference */
   unsigned long long seed;  /* random initial vector */
+  int method;               /* CDFT_EIGEN_* */
+  int block, max_basis, check_interval;
 } cdft_eigen_config;
 
 /* Smallest eigenpair of the Hessian at rho (fixed boundary).  vec (device,
@@ -359,6 +389,16 @@ typedef struct {
 CDFT_API int cdft_eigen_solve(cdft_engine* engine, const cdft_eigen_config* cfg, const double* rho,
                               double chemical_potential, double* vec, int use_guess, double* eigenvalue,
                               int* iterations, int* converged, void* stream);
+
+/* cdft_eigen_solve with a product engine for the Lanczos method: hvp_engine
+ * (or NULL: `engine`, which then needs batch 1) is an engine of the same grid
+ * and model whose batch equals cfg->block; its batched exact products at rho
+ * drive the block recurrence (an FP64 product engine keeps the products in
+ * FP64 under a mixed-precision `engine`).  Replaces EigenvalueSolver::solve
+ * (saddle_point.hpp:171-276) with the same operator and outputs. */
+CDFT_API int cdft_eigen_solve_ex(cdft_engine* engine, cdft_engine* hvp_engine, const cdft_eigen_config* cfg,
+                                 const double* rho, double chemical_potential, double* vec, int use_guess,
+                                 double* eigenvalue, int* iterations, int* converged, void* stream);
 
 /* Search (saddle_point.hpp:324-353). */
 typedef struct {
@@ -375,6 +415,17 @@ typedef struct {
 CDFT_API int cdft_saddle_find(cdft_engine* engine, const cdft_saddle_config* cfg, double* rho,
                               double chemical_potential, double target_mass, double* eigvec, double out[2],
                               int* outer_iterations, int* converged, void* stream);
+
+/* Search::find (saddle_point.hpp:367-589) with the mixed-precision and
+ * batched-product options: `refine` (or NULL) is an FP64 engine that finishes
+ * every projected FIRE run once its rms force is below refine_switch times
+ * the run's tolerance (FP64 defect correction); `hvp_engine` (or NULL) the
+ * product engine of a Lanczos eigen solve (cdft_eigen_solve_ex).
+ * counts = {outer iterations, eigen products, FIRE steps} (or NULL). */
+CDFT_API int cdft_saddle_find_ex(cdft_engine* engine, cdft_engine* refine, cdft_engine* hvp_engine,
+                                 double refine_switch, const cdft_saddle_config* cfg, double* rho,
+                                 double chemical_potential, double target_mass, double* eigvec, double out[2],
+                                 int counts[3], int* converged, void* stream);
 
 /* ---- bulk thermodynamics (host) ------------------------------------------ */
 

@@ -638,24 +638,33 @@ struct EigenvalueResult {
   bool converged = false;
 };
 
-// saddle_point.hpp:158-169 (exact_hvp replaces the finite difference)
+// saddle_point.hpp:158-169 (exact_hvp replaces the finite difference).
+// method CDFT_EIGEN_LANCZOS: block Lanczos on exact products of the same
+// operator, `block` directions per batched product taken from `hvp_weights`
+// (same model, batch = block) or from `w` itself (block 1).
 struct EigenvalueSolver {
   double tolerance = 1e-4;
   int max_iterations = 300;
   double hessian_eps = 1e-6;
   bool exact_hvp = false;
   unsigned long long seed = 42;
-  cdft_eigen_config c() const { return {tolerance, max_iterations, hessian_eps, exact_hvp ? 1 : 0, seed}; }
+  int method = CDFT_EIGEN_RAYLEIGH_RITZ;
+  int block = 1, max_basis = 32, check_interval = 4;
+  cdft_eigen_config c() const {
+    return {tolerance, max_iterations, hessian_eps, exact_hvp ? 1 : 0, seed, method, block, max_basis,
+            check_interval};
+  }
   EigenvalueResult solve(const functionals::Weights& w, const std::vector<double>& rho, double mu,
-                         const std::vector<double>& initial_guess = {}) const {
+                         const std::vector<double>& initial_guess = {},
+                         const functionals::Weights* hvp_weights = nullptr) const {
     DeviceVector d(rho);
     DeviceVector v(rho.size());
     if (initial_guess.size() == rho.size()) v.upload(initial_guess);
     cdft_eigen_config cfg = c();
     EigenvalueResult r;
     int it = 0, conv = 0;
-    check(cdft_eigen_solve(w.engine(), &cfg, d.get(), mu, v.get(), initial_guess.size() == rho.size() ? 1 : 0,
-                           &r.eigenvalue, &it, &conv, nullptr));
+    check(cdft_eigen_solve_ex(w.engine(), hvp_weights ? hvp_weights->engine() : nullptr, &cfg, d.get(), mu, v.get(),
+                              initial_guess.size() == rho.size() ? 1 : 0, &r.eigenvalue, &it, &conv, nullptr));
     r.eigenvector = v.download();
     r.iterations = it;
     r.converged = conv != 0;
@@ -668,6 +677,7 @@ struct Result {
   double grand_potential = 0.0, eigenvalue = 0.0;
   int outer_iterations = 0;
   bool converged = false;
+  int eigen_iterations = 0, fire_steps = 0;  // summed over the outer iterations
 };
 
 // saddle_point.hpp:324-353 (same defaults)
@@ -677,6 +687,11 @@ struct Search {
   minimization::Unbounded param{1e-18};
   double omega_tolerance = 1e-5, tolerance_start = 1e-3, tolerance_factor = 10.0;
   int max_outer_iterations = 20, eigenvalue_clear_count = 2;
+  // FP64 defect correction of a mixed-precision search (see cdft_saddle_find_ex)
+  const functionals::Weights* refine = nullptr;
+  double refine_switch = 10.0;
+  // product engine of a Lanczos eigen solve (batch = eigenvalue.block)
+  const functionals::Weights* hvp_weights = nullptr;
   Result find(const physics::Model&, const functionals::Weights& w, const std::vector<double>& rho0, double mu,
               double target_mass) const {
     cdft_saddle_config cfg{fire.c(),        eigenvalue.c(),   param.rho_min,        omega_tolerance,
@@ -684,14 +699,18 @@ struct Search {
     DeviceVector d(rho0);
     DeviceVector ev(rho0.size());
     double out[2] = {0.0, 0.0};
-    int it = 0, conv = 0;
-    check(cdft_saddle_find(w.engine(), &cfg, d.get(), mu, target_mass, ev.get(), out, &it, &conv, nullptr));
+    int counts[3] = {0, 0, 0}, conv = 0;
+    check(cdft_saddle_find_ex(w.engine(), refine ? refine->engine() : nullptr,
+                              hvp_weights ? hvp_weights->engine() : nullptr, refine_switch, &cfg, d.get(), mu,
+                              target_mass, ev.get(), out, counts, &conv, nullptr));
     Result r;
     r.density = d.download();
     r.eigenvector = ev.download();
     r.grand_potential = out[0];
     r.eigenvalue = out[1];
-    r.outer_iterations = it;
+    r.outer_iterations = counts[0];
+    r.eigen_iterations = counts[1];
+    r.fire_steps = counts[2];
     r.converged = conv != 0;
     return r;
   }

@@ -571,6 +571,126 @@ class EigenvalueSolver:
         return EigenvalueResult(v, lam, it, converged)
 
 
+@dataclass
+class SaddleResult:
+    """saddle_point.hpp:313-320."""
+
+    density: np.ndarray
+    eigenvector: np.ndarray
+    grand_potential: float
+    eigenvalue: float
+    outer_iterations: int
+    converged: bool
+    fire_steps: int = 0
+
+
+@dataclass
+class Search:
+    """saddle_point.hpp:324-589: eigenvector following at fixed mass.
+
+    ``total_fn(rho, mu) -> (free_energy, grand_potential, force)`` evaluates the
+    functional for a single-species profile.  Each outer iteration draws its
+    random eigen start from seed ``eigenvalue.seed + outer`` (the reference
+    draws from Armadillo's global generator)."""
+
+    fire: Fire = field(default_factory=lambda: Fire(dt=1e-3, dt_max=1.0, alpha_start=0.01, f_alpha=1.0,
+                                                    force_tolerance=1e-4, max_steps=100000))
+    eigenvalue: EigenvalueSolver = field(default_factory=lambda: EigenvalueSolver(1e-4, 300, 1e-6))
+    param: object = field(default_factory=lambda: Unbounded(1e-18))
+    omega_tolerance: float = 1e-5
+    tolerance_start: float = 1e-3
+    tolerance_factor: float = 10.0
+    max_outer_iterations: int = 20
+    eigenvalue_clear_count: int = 2
+
+    def find(self, grid: Grid, total_fn, initial_density, chemical_potential, target_mass):
+        dv = grid.cell_volume
+        bdry = boundary_mask(grid).astype(bool)
+        inner = ~bdry
+
+        def eig_force_fn(rho):  # saddle_point.hpp:377-384
+            _, omega, f = total_fn(rho, chemical_potential)
+            return omega, fixed_boundary(f, bdry)
+
+        rho = np.array(initial_density, dtype=np.float64)
+        eigvec = None
+        omega = 0.0
+        ev = 0.0
+        converged = False
+        ftol = self.tolerance_start
+        steps = 0
+        outer = 0
+        while outer < self.max_outer_iterations:
+            omega_old = omega
+            guess = eigvec if (outer >= self.eigenvalue_clear_count and eigvec is not None) else None
+            er = replace(self.eigenvalue, seed=self.eigenvalue.seed + outer).solve(eig_force_fn, rho, guess)
+            eigvec = er.eigenvector
+            ev = er.eigenvalue
+            # direction in parameter space (saddle_point.hpp:424-430)
+            x_cur = from_density(rho, self.param)
+            dir_alias = transform_force(eigvec, x_cur, self.param)
+            dn = float(np.linalg.norm(dir_alias))
+            if dn > 1e-30:
+                dir_alias = dir_alias / dn
+            # boundary mass (saddle_point.hpp:432-443)
+            nb = int(bdry.sum())
+            m_boundary = (float(rho[bdry].sum()) / nb if nb > 0 else 0.0) * dv * nb
+            m_t_int = target_mass - m_boundary
+
+            def compute(x_param):  # saddle_point.hpp:445-492
+                rho_l = to_density(x_param[0], self.param)
+                m_int = float(rho_l[inner].sum()) * dv
+                if m_int > 0.0 and m_t_int > 0.0:
+                    rho_l = rho_l.copy()
+                    rho_l[inner] *= m_t_int / m_int
+                _, om, grad = total_fn(rho_l, chemical_potential)
+                grad = fixed_boundary(grad, bdry)
+                mu_l = float(np.dot(grad[inner], rho_l[inner]))
+                if m_t_int > 0.0:
+                    mu_l /= m_t_int
+                grad = np.where(bdry, 0.0, grad - mu_l * dv)
+                f = transform_force(grad, x_param[0], self.param)
+                f = f - float(np.dot(dir_alias, f)) * dir_alias
+                return om, [-f]
+
+            # FIRE2 at fixed mass, projected (saddle_point.hpp:496-530)
+            fire_cfg = replace(self.fire, force_tolerance=max(ftol, self.fire.force_tolerance))
+            ftol /= self.tolerance_factor
+            st = fire_cfg.initialize([from_density(rho, self.param)], compute)
+            _, forces0 = compute(st.x)
+            for _ in range(fire_cfg.max_steps):
+                if st.converged:
+                    break
+                st, forces0 = fire_cfg.step(st, forces0, compute)
+            steps += st.iteration
+            # final density (saddle_point.hpp:533-549) and Omega (:551-554)
+            rho = to_density(st.x[0], self.param)
+            fm = float(rho[inner].sum()) * dv
+            if fm > 0.0 and m_t_int > 0.0:
+                rho = rho.copy()
+                rho[inner] *= m_t_int / fm
+            _, omega, _ = total_fn(rho, chemical_potential)
+            if outer > 0 and abs(omega - omega_old) < self.omega_tolerance:
+                converged = True
+                break
+            outer += 1
+        return SaddleResult(rho, eigvec, omega, ev, outer + 1, converged, steps)
+
+
+def dense_fixed_boundary_hessian(grid: Grid, force_fn, rho, h=1e-5):
+    """The interior block of the fixed-boundary Hessian by central
+    differences of the force (small grids only): H[:, j] =
+    (f(rho + h e_j) - f(rho - h e_j)) / 2h restricted to interior rows and
+    columns.  Returns (H, interior indices)."""
+    inner = np.nonzero(~boundary_mask(grid).astype(bool))[0]
+    H = np.empty((inner.size, inner.size))
+    for c, j in enumerate(inner):
+        e = np.zeros_like(rho)
+        e[j] = h
+        H[:, c] = ((force_fn(rho + e) - force_fn(rho - e)) / (2.0 * h))[inner]
+    return H, inner
+
+
 # ================================================================= Picard
 
 
