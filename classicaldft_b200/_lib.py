@@ -91,6 +91,12 @@ EIGEN_RAYLEIGH_RITZ = 0
 EIGEN_LANCZOS = 1
 
 
+class CGroupMember(ctypes.Structure):
+    _fields_ = [("engine", ctypes.c_void_p), ("refine", ctypes.c_void_p), ("refine_switch", ctypes.c_double),
+                ("mu", ctypes.POINTER(ctypes.c_double)), ("target_mass", ctypes.POINTER(ctypes.c_double)),
+                ("rho", ctypes.c_void_p), ("results", ctypes.POINTER(CMinimizerResult))]
+
+
 class CEigenConfig(ctypes.Structure):
     _fields_ = [("tolerance", ctypes.c_double), ("max_iterations", ctypes.c_int), ("hessian_eps", ctypes.c_double),
                 ("exact_hvp", ctypes.c_int), ("seed", ctypes.c_ulonglong), ("method", ctypes.c_int),
@@ -210,6 +216,7 @@ def lib():
         "cdft_saddle_find": [vp, ctypes.POINTER(CSaddleConfig), vp, ctypes.c_double, ctypes.c_double, vp,
                              c_double_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), vp],
         "cdft_ddft_set_refine": [vp, vp, ctypes.c_int],
+        "cdft_minimize_group": [ctypes.c_int, ctypes.POINTER(CGroupMember), ctypes.POINTER(CMinimizerConfig), vp],
         "cdft_ddft_last_step": [vp, ctypes.POINTER(ctypes.c_int), c_double_p],
         "cdft_eigen_solve_ex": [vp, vp, ctypes.POINTER(CEigenConfig), vp, ctypes.c_double, vp, ctypes.c_int,
                                 c_double_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), vp],

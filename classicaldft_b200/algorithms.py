@@ -198,6 +198,55 @@ class Minimizer:
             raise RuntimeError(f"fire::step: exceeded max uphill steps (problems {np.flatnonzero(uphill).tolist()})")
         return res
 
+    def minimize_group(self, members, mode="grand_potential"):
+        """Minimise the problems of several batched engines together -- an
+        uneven sweep with one engine per grid size.  ``members``: a list of
+        ``(weights, initial_densities (B, N), chemical_potentials (B,),
+        target_masses (B,) or None, refine_weights or None)``.  One FIRE step
+        of every running member is one graph launch; each problem stops at
+        its own convergence.  Returns one list of B results per member."""
+        torch = _torch()
+        if mode not in ("grand_potential", "fixed_mass"):
+            raise ValueError("minimize_group: mode is grand_potential or fixed_mass")
+        keep, cm = [], (_lib.CGroupMember * len(members))()
+        outs = []
+        for m, mem in enumerate(members):
+            w, rhos, mus, masses = mem[:4]
+            ref = mem[4] if len(mem) > 4 else None
+            e = w.engine
+            B, N = e.batch, e.N
+            if isinstance(rhos, np.ndarray) or not hasattr(rhos, "data_ptr"):
+                d = torch.tensor(np.asarray(rhos, dtype=np.float64).reshape(B, N), device="cuda")
+                host = True
+            else:
+                d = rhos.reshape(B, N).to(torch.float64).contiguous().clone()
+                host = False
+            mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mus, dtype=np.float64), (B,)))
+            mass = None if masses is None else np.ascontiguousarray(
+                np.broadcast_to(np.asarray(masses, dtype=np.float64), (B,)))
+            res = (_lib.CMinimizerResult * B)()
+            keep += [d, mu, mass, res]
+            cm[m].engine = e.handle
+            cm[m].refine = ref.engine.handle if ref is not None else None
+            cm[m].refine_switch = self.refine_switch
+            cm[m].mu = mu.ctypes.data_as(_lib.c_double_p)
+            cm[m].target_mass = None if mass is None else mass.ctypes.data_as(_lib.c_double_p)
+            cm[m].rho = d.data_ptr()
+            cm[m].results = ctypes.cast(res, ctypes.POINTER(_lib.CMinimizerResult))
+            outs.append((d, host, res))
+        cfg = self._config(0 if mode == "grand_potential" else 1, 0.0)
+        _lib.check(_lib.lib().cdft_minimize_group(len(members), cm, ctypes.byref(cfg), _stream()))
+        torch.cuda.synchronize()
+        results = []
+        for d, host, res in outs:
+            out = d.cpu().numpy() if host else d
+            results.append([MinimizationResult([out[b]], r.free_energy, r.grand_potential, r.rms_force,
+                                               r.iterations, bool(r.converged)) for b, r in enumerate(res)])
+            if any(r.uphill_error for r in res):
+                bad = [b for b, r in enumerate(res) if r.uphill_error]
+                raise RuntimeError(f"fire::step: exceeded max uphill steps (member problems {bad})")
+        return results
+
     def fixed_mass_batch(self, model: Model, weights: Weights, initial_densities, chemical_potentials,
                          target_masses):
         """``fixed_mass`` for every problem of a batched engine; target_masses (B,)."""

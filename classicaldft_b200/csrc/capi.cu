@@ -479,6 +479,38 @@ cdft::Drivers::DDFTConfig to_ddft(const cdft_ddft_config& c, double mu) {
 }
 }  // namespace
 
+int cdft_minimize_group(int n_members, const cdft_group_member* members, const cdft_minimizer_config* cfg,
+                        void* stream) {
+  return guarded([&] {
+    if (n_members < 1 || !members || !cfg) throw std::invalid_argument("members and cfg are required");
+    cdft::FireConfig fc = to_fire_config(cfg);
+    std::vector<cdft::GroupMember> g(n_members);
+    for (int m = 0; m < n_members; ++m) {
+      const cdft_group_member& c = members[m];
+      if (!c.engine || !c.results) throw std::invalid_argument("every member needs an engine and results");
+      g[m].drivers = &drivers_of(c.engine, true);
+      g[m].mu = c.mu;
+      g[m].mass = c.target_mass;
+      g[m].rho = c.rho;
+      g[m].refine = c.refine ? c.refine->impl : nullptr;
+      g[m].refine_switch = c.refine_switch > 0.0 ? c.refine_switch : 10.0;
+    }
+    const std::vector<std::vector<cdft::FireResult>> r =
+        cdft::fire_minimize_group(g, fc, static_cast<cudaStream_t>(stream));
+    for (int m = 0; m < n_members; ++m)
+      for (size_t b = 0; b < r[m].size(); ++b) {
+        cdft_minimizer_result& o = members[m].results[b];
+        o.free_energy = r[m][b].free_energy;
+        o.grand_potential = r[m][b].grand_potential;
+        o.rms_force = r[m][b].rms_force;
+        o.iterations = r[m][b].iterations;
+        o.converged = r[m][b].converged ? 1 : 0;
+        o.uphill_error = r[m][b].uphill_error ? 1 : 0;
+      }
+  });
+}
+
+
 int cdft_ddft_step(cdft_engine* engine, cdft_ddft_config* cfg, double chemical_potential, double* rho,
                    double* energy, int* fp_iterations, void* stream) {
   return guarded([&] {

@@ -1019,12 +1019,56 @@ std::vector<FireResult> Drivers::fire_run(const FireConfig& cfg, const double* m
   return out;
 }
 
-std::vector<FireResult> Drivers::fire_loop(const FireConfig& cfg, const double* mu, const double* mass, double* rho,
-                                           const double* direction, cudaStream_t stream, Engine* refine,
-                                           double refine_switch, bool graphs) {
+// State of one FIRE run of this driver (all problems of its engine): the
+// kernel arguments, the engine evaluating and the host's step count.
+struct FireRun {
+  FireConfig cfg;
+  Vec a;
+  ComputeCfg cc;
+  double volume = 0.0;
+  std::vector<double> mu_compute, mu_final;
+  Engine* eng = nullptr;
+  Engine* refine = nullptr;
+  double refine_switch = 10.0;
+  bool refining = false;
+  int steps = 0;
+  bool done = false;
+};
+
+// rescale (fixed mass / saddle), evaluate, post-process into f
+void Drivers::fire_compute(int initial, cudaStream_t stream) {
+  FireRun& r = *run_;
   const EvalParams& p = eng_.params();
   const int B = B_;
-  Vec a;
+  const dim3 gv(grid_, B);
+  const int rt = 32 * kRedTerms;
+  k_density_sums<<<gv, kBlock, 0, stream>>>(r.a, red_);
+  k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
+  k_scale_factor<<<B, 32, 0, stream>>>(st_, red_out_, r.cc, p.dv, initial);
+  k_rescale<<<gv, kBlock, 0, stream>>>(r.a, st_, r.cc, initial);
+  r.eng->evaluate(r.a.rho, nullptr, r.mu_compute.data(), grad_, scalars_, stream);
+  k_post_sums<<<gv, kBlock, 0, stream>>>(r.a, red_);
+  k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
+  k_post_control<<<B, 32, 0, stream>>>(st_, red_out_, r.cc);
+  k_post_apply<<<gv, kBlock, 0, stream>>>(r.a, st_, r.cc, red_);
+  k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_ + 4);
+  if (r.cfg.mode == kSaddle) {
+    k_project<<<gv, kBlock, 0, stream>>>(r.a, red_out_ + 4, red_);
+    k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_ + 4);
+  }
+  k_fire_finalize<<<B, 32, 0, stream>>>(st_, red_out_ + 4, scalars_, r.cfg.fire, (double)N_, r.volume,
+                                        r.cfg.use_monitor ? 1 : 0, initial);
+}
+
+void Drivers::fire_begin(const FireConfig& cfg, const double* mu, const double* mass, double* rho,
+                         const double* direction, cudaStream_t stream, Engine* refine, double refine_switch) {
+  const EvalParams& p = eng_.params();
+  const int B = B_;
+  if (!run_) run_.reset(new FireRun());
+  FireRun& r = *run_;
+  r = FireRun();
+  r.cfg = cfg;
+  Vec& a = r.a;
   a.x = x_;
   a.v = v_;
   a.f = f_;
@@ -1039,47 +1083,26 @@ std::vector<FireResult> Drivers::fire_loop(const FireConfig& cfg, const double* 
   a.param = cfg.param;
   a.rho_min = cfg.rho_min;
   a.range = cfg.rho_max - cfg.rho_min;
-  ComputeCfg cc;
-  cc.mode = cfg.mode;
-  cc.homogeneous = cfg.homogeneous_boundary ? 1 : 0;
-  cc.boundary_mass = cfg.boundary_mass;
+  r.cc.mode = cfg.mode;
+  r.cc.homogeneous = cfg.homogeneous_boundary ? 1 : 0;
+  r.cc.boundary_mass = cfg.boundary_mass;
   const long long inner = (long long)std::max(p.nx - 2, 0) * std::max(p.ny - 2, 0) * std::max(p.nz - 2, 0);
-  cc.n_face = (double)(N_ - inner);
-  const double volume = (double)N_ * p.dv;
+  r.cc.n_face = (double)(N_ - inner);
+  r.volume = (double)N_ * p.dv;
   // Minimizer::fixed_mass computes with mu = 0 (minimization.hpp:388); the
   // other modes with the given chemical potential.
-  std::vector<double> mu_compute(B), mu_final(B);
+  r.mu_compute.resize(B);
+  r.mu_final.resize(B);
   for (int b = 0; b < B; ++b) {
-    mu_final[b] = mu[b];
-    mu_compute[b] = (cfg.mode == kFixedMass) ? 0.0 : mu[b];
+    r.mu_final[b] = mu[b];
+    r.mu_compute[b] = (cfg.mode == kFixedMass) ? 0.0 : mu[b];
   }
-  const FireParams& fp = cfg.fire;
-  const int use_monitor = cfg.use_monitor ? 1 : 0;
-  const dim3 gv(grid_, B);
-  const int rt = 32 * kRedTerms;
-
-  Engine* eng = &eng_;
-  reset_step_graph();  // a graph holds this call's arguments
-  auto compute = [&](int initial) {
-    // rescale (fixed mass / saddle), evaluate, post-process into f
-    k_density_sums<<<gv, kBlock, 0, stream>>>(a, red_);
-    k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
-    k_scale_factor<<<B, 32, 0, stream>>>(st_, red_out_, cc, p.dv, initial);
-    k_rescale<<<gv, kBlock, 0, stream>>>(a, st_, cc, initial);
-    eng->evaluate(rho, nullptr, mu_compute.data(), grad_, scalars_, stream);
-    k_post_sums<<<gv, kBlock, 0, stream>>>(a, red_);
-    k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
-    k_post_control<<<B, 32, 0, stream>>>(st_, red_out_, cc);
-    k_post_apply<<<gv, kBlock, 0, stream>>>(a, st_, cc, red_);
-    k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_ + 4);
-    if (cfg.mode == kSaddle) {
-      k_project<<<gv, kBlock, 0, stream>>>(a, red_out_ + 4, red_);
-      k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_ + 4);
-    }
-    k_fire_finalize<<<B, 32, 0, stream>>>(st_, red_out_ + 4, scalars_, fp, (double)N_, volume, use_monitor, initial);
-  };
-
+  r.eng = &eng_;
+  r.refine = refine;
+  r.refine_switch = refine_switch;
+  reset_step_graph();  // a graph holds this run's arguments
   // initialise (fire.hpp:60-84)
+  const FireParams& fp = cfg.fire;
   for (int b = 0; b < B; ++b) {
     FireDevState& s0 = st_host_[b];
     std::memset(&s0, 0, sizeof(s0));
@@ -1091,90 +1114,87 @@ std::vector<FireResult> Drivers::fire_loop(const FireConfig& cfg, const double* 
     s0.target_mass = mass[b];
   }
   CDFT_CUDA(cudaMemcpyAsync(st_, st_host_, sizeof(FireDevState) * B, cudaMemcpyHostToDevice, stream));
-  k_from_density<<<gv, kBlock, 0, stream>>>(a, rho);
-  compute(1);
+  k_from_density<<<dim3(grid_, B), kBlock, 0, stream>>>(a, rho);
+  fire_compute(1, stream);
   CDFT_CUDA(cudaGetLastError());
+}
 
-  bool refining = false;
-  int steps = 0;
-  for (;;) {
-    CDFT_CUDA(cudaMemcpyAsync(st_host_, st_, sizeof(FireDevState) * B, cudaMemcpyDeviceToHost, stream));
-    CDFT_CUDA(cudaStreamSynchronize(stream));
-    bool any_active = false, all_close = true;
-    for (int b = 0; b < B; ++b) {
-      const FireDevState& h = st_host_[b];
-      if (!h.active) continue;
-      any_active = true;
-      const double metric = cfg.use_monitor ? h.monitor : h.rms_force;
-      if (!(h.iteration > 0 && metric < refine_switch * fp.force_tolerance)) all_close = false;
-    }
-    if (refine && !refining && all_close && steps < fp.max_steps) {
-      // FP64 defect correction from here on: once every running problem is
-      // within refine_switch of the tolerance, or once all of them have
-      // converged under the mixed-precision forces
-      eng = refine;
-      refining = true;
-      if (!any_active) {
-        k_fire_reactivate<<<B, 32, 0, stream>>>(st_, fp.max_steps);
-        CDFT_CUDA(cudaGetLastError());
-        any_active = true;
-      }
-    }
-    if (!any_active || steps >= fp.max_steps) break;
-    const int chunk = std::max(1, std::min(cfg.check_interval, fp.max_steps - steps));
-    // one FIRE step (fire.hpp:86-165): the v and x updates, then compute
-    auto step = [&] {
-      k_power<<<gv, kBlock, 0, stream>>>(a, red_);
-      k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
-      k_fire_control1<<<B, 32, 0, stream>>>(st_, red_out_, fp);
-      k_fire_vstep<<<gv, kBlock, 0, stream>>>(a, st_, red_);
-      k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
-      k_fire_ratio<<<B, 32, 0, stream>>>(st_, red_out_);
-      k_fire_xstep<<<gv, kBlock, 0, stream>>>(a, st_);
-      compute(0);
-    };
-    if (graphs && step_key_ != eng) {
-      // (re)capture the step for the engine now evaluating; every kernel
-      // argument of a step is the same from one step to the next
-      reset_step_graph();
-      CDFT_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-      try {
-        step();
-      } catch (...) {
-        cudaGraph_t g = nullptr;
-        cudaStreamEndCapture(stream, &g);
-        if (g) cudaGraphDestroy(g);
-        throw;
-      }
-      CDFT_CUDA(cudaStreamEndCapture(stream, &step_graph_));
-      CDFT_CUDA(cudaGraphInstantiate(&step_exec_, step_graph_, 0));
-      step_key_ = eng;
-    }
-    for (int k = 0; k < chunk; ++k) {
-      if (graphs)
-        CDFT_CUDA(cudaGraphLaunch(step_exec_, stream));
-      else
-        step();
-    }
-    CDFT_CUDA(cudaGetLastError());
-    steps += chunk;
+// one FIRE step (fire.hpp:86-165): the v and x updates, then compute
+void Drivers::fire_launch_step(cudaStream_t stream) {
+  FireRun& r = *run_;
+  const int B = B_;
+  const dim3 gv(grid_, B);
+  const int rt = 32 * kRedTerms;
+  k_power<<<gv, kBlock, 0, stream>>>(r.a, red_);
+  k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
+  k_fire_control1<<<B, 32, 0, stream>>>(st_, red_out_, r.cfg.fire);
+  k_fire_vstep<<<gv, kBlock, 0, stream>>>(r.a, st_, red_);
+  k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
+  k_fire_ratio<<<B, 32, 0, stream>>>(st_, red_out_);
+  k_fire_xstep<<<gv, kBlock, 0, stream>>>(r.a, st_);
+  fire_compute(0, stream);
+}
+
+void Drivers::fire_read_state(cudaStream_t stream) {
+  CDFT_CUDA(cudaMemcpyAsync(st_host_, st_, sizeof(FireDevState) * B_, cudaMemcpyDeviceToHost, stream));
+}
+
+int Drivers::fire_decide(cudaStream_t stream, bool* engine_changed) {
+  FireRun& r = *run_;
+  const FireParams& fp = r.cfg.fire;
+  if (engine_changed) *engine_changed = false;
+  if (r.done) return 0;
+  bool any_active = false, all_close = true;
+  for (int b = 0; b < B_; ++b) {
+    const FireDevState& h = st_host_[b];
+    if (!h.active) continue;
+    any_active = true;
+    const double metric = r.cfg.use_monitor ? h.monitor : h.rms_force;
+    if (!(h.iteration > 0 && metric < r.refine_switch * fp.force_tolerance)) all_close = false;
   }
+  if (r.refine && !r.refining && all_close && r.steps < fp.max_steps) {
+    // FP64 defect correction from here on: once every running problem is
+    // within refine_switch of the tolerance, or once all of them have
+    // converged under the mixed-precision forces
+    r.eng = r.refine;
+    r.refining = true;
+    if (engine_changed) *engine_changed = true;
+    if (!any_active) {
+      k_fire_reactivate<<<B_, 32, 0, stream>>>(st_, fp.max_steps);
+      CDFT_CUDA(cudaGetLastError());
+      any_active = true;
+    }
+  }
+  if (!any_active || r.steps >= fp.max_steps) {
+    r.done = true;
+    return 0;
+  }
+  return std::max(1, std::min(r.cfg.check_interval, fp.max_steps - r.steps));
+}
+
+void Drivers::fire_advance(int steps) { run_->steps += steps; }
+
+const Engine* Drivers::fire_engine() const { return run_ ? run_->eng : nullptr; }
+
+std::vector<FireResult> Drivers::fire_finish(cudaStream_t stream) {
+  FireRun& r = *run_;
+  const int B = B_;
   std::vector<FireResult> out(B);
   bool any_uphill = false;
   for (int b = 0; b < B; ++b) {
-    FireResult& r = out[b];
-    r.iterations = st_host_[b].iteration;
-    r.converged = st_host_[b].converged != 0;
-    r.rms_force = st_host_[b].rms_force;
-    r.uphill_error = st_host_[b].uphill_error != 0;
-    any_uphill = any_uphill || r.uphill_error;
+    FireResult& o = out[b];
+    o.iterations = st_host_[b].iteration;
+    o.converged = st_host_[b].converged != 0;
+    o.rms_force = st_host_[b].rms_force;
+    o.uphill_error = st_host_[b].uphill_error != 0;
+    any_uphill = any_uphill || o.uphill_error;
   }
   if (B == 1 && any_uphill) return out;
   // Final density (minimization.hpp:441-450, saddle_point.hpp:533-549): rho
   // already holds rho(x) with the mass rescale of the last compute, which is
   // exactly the reference's extraction from the final x.  The final total()
   // uses the caller's chemical potential (fixed mass iterates with mu = 0).
-  eng->evaluate(rho, nullptr, mu_final.data(), grad_, scalars_, stream);
+  r.eng->evaluate(r.a.rho, nullptr, r.mu_final.data(), grad_, scalars_, stream);
   std::vector<double> sc((size_t)B * kScalarCount);
   CDFT_CUDA(cudaMemcpyAsync(sc.data(), scalars_, sizeof(double) * sc.size(), cudaMemcpyDeviceToHost, stream));
   CDFT_CUDA(cudaStreamSynchronize(stream));
@@ -1182,6 +1202,157 @@ std::vector<FireResult> Drivers::fire_loop(const FireConfig& cfg, const double* 
     out[b].free_energy = sc[(size_t)b * kScalarCount + 0];
     out[b].grand_potential = sc[(size_t)b * kScalarCount + 1];
   }
+  return out;
+}
+
+void Drivers::capture_step(cudaStream_t stream) {
+  reset_step_graph();
+  CDFT_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    fire_launch_step(stream);
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(stream, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  CDFT_CUDA(cudaStreamEndCapture(stream, &step_graph_));
+  CDFT_CUDA(cudaGraphInstantiate(&step_exec_, step_graph_, 0));
+  step_key_ = run_->eng;
+}
+
+std::vector<FireResult> Drivers::fire_loop(const FireConfig& cfg, const double* mu, const double* mass, double* rho,
+                                           const double* direction, cudaStream_t stream, Engine* refine,
+                                           double refine_switch, bool graphs) {
+  fire_begin(cfg, mu, mass, rho, direction, stream, refine, refine_switch);
+  for (;;) {
+    fire_read_state(stream);
+    CDFT_CUDA(cudaStreamSynchronize(stream));
+    const int chunk = fire_decide(stream, nullptr);
+    if (chunk == 0) break;
+    // (re)capture the step for the engine now evaluating; every kernel
+    // argument of a step is the same from one step to the next
+    if (graphs && step_key_ != run_->eng) capture_step(stream);
+    for (int k = 0; k < chunk; ++k) {
+      if (graphs)
+        CDFT_CUDA(cudaGraphLaunch(step_exec_, stream));
+      else
+        fire_launch_step(stream);
+    }
+    CDFT_CUDA(cudaGetLastError());
+    fire_advance(chunk);
+  }
+  return fire_finish(stream);
+}
+
+std::vector<std::vector<FireResult>> fire_minimize_group(std::vector<GroupMember>& members, const FireConfig& cfg,
+                                                         cudaStream_t stream) {
+  if (members.empty()) return {};
+  if (cfg.mode == kSaddle) throw Error(-1, "fire_minimize_group: the saddle mode is single-problem");
+  const int M = (int)members.size();
+  std::vector<std::vector<double>> masses(M);
+  for (int m = 0; m < M; ++m) {
+    GroupMember& g = members[m];
+    if (!g.drivers || !g.mu || !g.rho) throw Error(-1, "fire_minimize_group: drivers, mu and rho are required");
+    for (int k = 0; k < m; ++k)
+      if (members[k].drivers == g.drivers) throw Error(-1, "fire_minimize_group: one member per engine");
+    const int B = g.drivers->batch();
+    masses[m].assign(B, 0.0);
+    if (cfg.mode == kFixedMass) {
+      if (!g.mass) throw Error(-1, "fire_minimize_group: fixed mass needs a target mass per problem");
+      for (int b = 0; b < B; ++b) {
+        if (!(g.mass[b] > 0.0)) throw Error(-1, "fire_minimize_group: target masses must be > 0");
+        masses[m][b] = g.mass[b];
+      }
+    }
+    if (g.refine && g.refine->batch() != B) throw Error(-1, "fire_minimize_group: refine engines need the same batch");
+  }
+  const bool graphs = step_graphs();
+  // the group runs on its own stream, joined to the caller's at entry and exit
+  cudaStream_t s0 = nullptr;
+  CDFT_CUDA(cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking));
+  std::vector<cudaEvent_t> ev(M + 1, nullptr);
+  for (cudaEvent_t& e : ev) CDFT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  auto release = [&] {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  };
+  std::vector<std::vector<FireResult>> out(M);
+  try {
+    CDFT_CUDA(cudaEventRecord(ev[M], stream));
+    CDFT_CUDA(cudaStreamWaitEvent(s0, ev[M], 0));
+    for (int m = 0; m < M; ++m)
+      members[m].drivers->fire_begin(cfg, members[m].mu, masses[m].data(), members[m].rho, nullptr, s0,
+                                     members[m].refine, members[m].refine_switch);
+    std::vector<std::pair<int, const Engine*>> key;
+    for (;;) {
+      for (int m = 0; m < M; ++m) members[m].drivers->fire_read_state(s0);
+      CDFT_CUDA(cudaStreamSynchronize(s0));
+      int chunk = 0;
+      std::vector<int> running;
+      for (int m = 0; m < M; ++m) {
+        const int c = members[m].drivers->fire_decide(s0, nullptr);
+        if (c > 0) {
+          running.push_back(m);
+          chunk = chunk ? std::min(chunk, c) : c;
+        }
+      }
+      if (running.empty()) break;
+      std::vector<std::pair<int, const Engine*>> now;
+      for (int m : running) now.emplace_back(m, members[m].drivers->fire_engine());
+      // one step of every running member on its own stream, forked from s0
+      auto step = [&] {
+        CDFT_CUDA(cudaEventRecord(ev[M], s0));
+        for (int m : running) {
+          cudaStream_t sm = members[m].drivers->graph_stream();
+          CDFT_CUDA(cudaStreamWaitEvent(sm, ev[M], 0));
+          members[m].drivers->fire_launch_step(sm);
+          CDFT_CUDA(cudaEventRecord(ev[m], sm));
+          CDFT_CUDA(cudaStreamWaitEvent(s0, ev[m], 0));
+        }
+      };
+      if (graphs && (!exec || now != key)) {
+        release();
+        CDFT_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+        try {
+          step();
+        } catch (...) {
+          cudaGraph_t g = nullptr;
+          cudaStreamEndCapture(s0, &g);
+          if (g) cudaGraphDestroy(g);
+          throw;
+        }
+        CDFT_CUDA(cudaStreamEndCapture(s0, &graph));
+        CDFT_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        key = now;
+      }
+      for (int k = 0; k < chunk; ++k) {
+        if (graphs)
+          CDFT_CUDA(cudaGraphLaunch(exec, s0));
+        else
+          step();
+      }
+      CDFT_CUDA(cudaGetLastError());
+      for (int m : running) members[m].drivers->fire_advance(chunk);
+    }
+    for (int m = 0; m < M; ++m) out[m] = members[m].drivers->fire_finish(s0);
+  } catch (...) {
+    cudaStreamSynchronize(s0);
+    release();
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    cudaStreamDestroy(s0);
+    throw;
+  }
+  CDFT_CUDA(cudaEventRecord(ev[M], s0));
+  CDFT_CUDA(cudaStreamWaitEvent(stream, ev[M], 0));
+  CDFT_CUDA(cudaStreamSynchronize(s0));
+  release();
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  cudaStreamDestroy(s0);
   return out;
 }
 
@@ -1685,7 +1856,17 @@ int Drivers::ddft_run(DDFTConfig& cfg, int n_steps, double* rho, double* times, 
   // Simulation::run (dynamics.hpp:597-649): initial energy, then steps with
   // the adaptive time step
   apply_boundary();
-  const double e0 = force(rho, tmp2_, cfg.mu, 0, stream);
+  // the initial energy from the FP64 refine engine when there is one, as
+  // every step's final energy
+  double e0 = 0.0;
+  if (ddft_refine_) {
+    ddft_refine_->evaluate(rho, nullptr, &cfg.mu, tmp2_, scalars_, stream);
+    CDFT_CUDA(cudaMemcpyAsync(host_pin_, scalars_, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+    CDFT_CUDA(cudaStreamSynchronize(stream));
+    e0 = host_pin_[1];
+  } else {
+    e0 = force(rho, tmp2_, cfg.mu, 0, stream);
+  }
   if (times) times[0] = 0.0;
   if (energies) energies[0] = e0;
   snapshot(0);

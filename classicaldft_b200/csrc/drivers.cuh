@@ -11,6 +11,7 @@
 
 #include <cufft.h>
 
+#include <memory>
 #include <vector>
 
 #include "cdft_common.cuh"
@@ -69,10 +70,36 @@ struct FireResult {
   bool uphill_error = false;
 };
 
+class Drivers;
+
+// One member of a group minimisation: the problems of one batched engine
+// (grand potential or fixed mass, as fire_minimize_batch).
+struct GroupMember {
+  Drivers* drivers = nullptr;
+  const double* mu = nullptr;    // B host values
+  const double* mass = nullptr;  // B host values (fixed mass) or null
+  double* rho = nullptr;         // B*N device doubles, replaced by the results
+  Engine* refine = nullptr;      // FP64 engine of the same batch, or null
+  double refine_switch = 10.0;
+};
+
+// Minimisations of several batched engines -- typically one per grid size of
+// an uneven parameter sweep -- advanced together: one step of every running
+// member is ONE launch (a CUDA graph whose branches run each member's step
+// on its own stream, so small grids fill the SMs beside large ones), the
+// host checks every member's control blocks every check_interval steps, and
+// a member leaves the graph when all its problems have stopped (the graph is
+// captured again then, and when a member switches to its FP64 engine).
+// Returns each member's results in member order.
+std::vector<std::vector<FireResult>> fire_minimize_group(std::vector<GroupMember>& members, const FireConfig& cfg,
+                                                         cudaStream_t stream);
+
 // Process-wide switch: the minimisers replay each step as a captured CUDA
 // graph (default on; results are the same either way).
 void set_step_graphs(bool on);
 bool step_graphs();
+
+struct FireRun;
 
 class Drivers {
  public:
@@ -256,7 +283,35 @@ class Drivers {
 
   Engine& engine() { return eng_; }
 
+  // The FIRE loop in pieces, for driving several drivers together (a group
+  // minimisation whose steps are one graph over every member):
+  //   fire_begin      initial compute (fire.hpp:60-84) of a run
+  //   fire_launch_step one step of every problem with the engine now evaluating
+  //   fire_read_state  async D2H of the control blocks (the caller syncs)
+  //   fire_decide      the host's check after that sync: the FP64 switch of
+  //                    the refine engine (engine_changed), and the steps to
+  //                    launch before the next check (0: the run is over)
+  //   fire_advance     count launched steps
+  //   fire_finish      final compute and results (synchronises the stream)
+  void fire_begin(const FireConfig& cfg, const double* mu, const double* mass, double* rho, const double* direction,
+                  cudaStream_t stream, Engine* refine, double refine_switch);
+  void fire_launch_step(cudaStream_t stream);
+  void fire_read_state(cudaStream_t stream);
+  int fire_decide(cudaStream_t stream, bool* engine_changed);
+  void fire_advance(int steps);
+  const Engine* fire_engine() const;
+  std::vector<FireResult> fire_finish(cudaStream_t stream);
+  int batch() const { return B_; }
+  // this driver's own stream for graph capture (created on first use)
+  cudaStream_t graph_stream() {
+    ensure_graph_stream();
+    return graph_stream_;
+  }
+
  private:
+  void fire_compute(int initial, cudaStream_t stream);
+  void capture_step(cudaStream_t stream);
+  std::unique_ptr<FireRun> run_;
   std::vector<FireResult> fire_run(const FireConfig& cfg, const double* mu, const double* mass, double* rho,
                                    const double* direction, cudaStream_t stream, Engine* refine,
                                    double refine_switch);

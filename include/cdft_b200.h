@@ -260,6 +260,31 @@ CDFT_API int cdft_minimize_batch(cdft_engine* engine, const cdft_minimizer_confi
                                  const double* target_mass, double* rho, cdft_engine* refine, double refine_switch,
                                  cdft_minimizer_result* results, void* stream);
 
+/* One member of a group minimisation: the problems of one batched engine. */
+typedef struct {
+  cdft_engine* engine;          /* batch B (cdft_create_batch / cdft_create_model) */
+  cdft_engine* refine;          /* FP64 engine of the same batch, or NULL */
+  double refine_switch;
+  const double* mu;             /* B host values (beta mu) */
+  const double* target_mass;    /* B host values (fixed mass), or NULL */
+  double* rho;                  /* B * N device doubles, replaced by the results */
+  cdft_minimizer_result* results;  /* B entries */
+} cdft_group_member;
+
+/* Minimizer::grand_potential / fixed_mass for the problems of several
+ * batched engines at once -- an uneven parameter sweep with one engine per
+ * grid size (48^3, 64^3, 96^3 ...).  One FIRE step of every running member is
+ * one launch of a CUDA graph whose branches run each member's step on its
+ * own stream, so the grids share the GPU; every control decision is per
+ * problem on the device and the host reads all control blocks every
+ * cfg->check_interval steps.  A member leaves the graph when all its
+ * problems have stopped.  cfg as cdft_minimize_batch (mode grand potential
+ * or fixed mass; chemical_potential and target_mass unused).  Uphill errors
+ * are reported per problem.  No reference counterpart: the reference
+ * minimises one state per call (minimization.hpp:280-354). */
+CDFT_API int cdft_minimize_group(int n_members, const cdft_group_member* members, const cdft_minimizer_config* cfg,
+                                 void* stream);
+
 /* DDFT step configuration, dynamics.hpp:26-33. */
 typedef struct {
   double dt, diffusion_coefficient, min_density, dt_max, fp_tolerance;

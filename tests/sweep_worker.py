@@ -35,3 +35,49 @@ def run(rank, world, port, n, batch, gather_profiles, out_dir):
                  prof=res.profiles if res.profiles is not None else np.zeros(0), seen=np.array(seen))
     finally:
         dist.destroy_process_group()
+
+
+UNEVEN_SHAPES = [(2, 2, 2), (4, 4, 4), (2, 2, 4), (4, 4, 4), (2, 2, 2), (3, 3, 3), (4, 4, 2)]
+
+
+def fake_uneven_solve(problems):
+    def solve(idx):
+        sc = np.array([[10.0 * i, -1.0 * i, 1e-3 * i, 7 + i, float(i % 2 == 0)] for i in idx])
+        prof = [np.full(problems[i].model.grid.total_points, 0.1 * i) for i in idx]
+        return sc, prof
+    return solve
+
+
+def uneven_problems(n):
+    from classicaldft_b200 import Grid, Model, Species
+    from classicaldft_b200.sweep import SweepProblem
+    out = []
+    for i in range(n):
+        shape = UNEVEN_SHAPES[i % len(UNEVEN_SHAPES)]
+        m = Model(Grid(0.5, tuple(0.5 * s for s in shape), shape), [Species("A", 1.0)], [], 1.0)
+        out.append(SweepProblem(m, 0.1 * i, np.zeros(int(np.prod(shape)))))
+    return out
+
+
+def run_uneven(rank, world, port, n, out_dir):
+    import torch.distributed as dist
+
+    from classicaldft_b200 import WhiteBearII
+    from classicaldft_b200.sweep import run_uneven_sweep
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        problems = uneven_problems(n)
+        seen = []
+        base = fake_uneven_solve(problems)
+
+        def solve(idx):
+            seen.extend(list(idx))
+            return base(idx)
+        res = run_uneven_sweep(problems, WhiteBearII(), None, gather_profiles=True, solve=solve)
+        np.savez(os.path.join(out_dir, f"uneven{rank}.npz"), F=res.free_energy, it=res.iterations,
+                 conv=res.converged, rank=res.rank, seen=np.array(seen),
+                 prof=np.concatenate(res.profiles), lens=np.array([len(p) for p in res.profiles]))
+    finally:
+        dist.destroy_process_group()

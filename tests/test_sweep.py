@@ -6,8 +6,8 @@ import socket
 import numpy as np
 import pytest
 
-from classicaldft_b200.sweep import chunks, shard
-from tests.sweep_worker import fake_solve
+from classicaldft_b200.sweep import chunks, partition_by_cost, problem_cost, shard
+from tests.sweep_worker import fake_solve, fake_uneven_solve, uneven_problems
 
 
 def test_shard_is_a_balanced_contiguous_partition():
@@ -46,6 +46,46 @@ def test_two_rank_gloo_sweep_gathers_every_problem_in_order(tmp_path, n, batch, 
         np.testing.assert_array_equal(d["conv"], sc[:, 4] > 0.5)
         if profiles:
             np.testing.assert_array_equal(d["prof"], prof)
+
+
+def test_cost_partition_is_deterministic_and_balanced():
+    """Longest-processing-time split of an uneven sweep (16 each of 48^3,
+    64^3 and 96^3 problems): every problem once, the same split on every
+    call, and no rank above 4/3 of the optimum bound (the LPT guarantee)."""
+    sizes = [48 ** 3] * 16 + [64 ** 3] * 16 + [96 ** 3] * 16
+    costs = [problem_cost(n) for n in sizes]
+    for world in (1, 2, 3, 4, 8):
+        parts = partition_by_cost(costs, world)
+        assert sorted(i for p in parts for i in p) == list(range(len(sizes)))
+        assert parts == partition_by_cost(costs, world)
+        loads = [sum(costs[i] for i in p) for p in parts]
+        bound = max(sum(costs) / world, max(costs))
+        assert max(loads) <= (4.0 / 3.0) * bound
+    # by count the 96^3 problems would all sit on the last ranks
+    by_count = [sum(costs[i] for i in shard(48, r, 4)) for r in range(4)]
+    lpt = [sum(costs[i] for i in p) for p in partition_by_cost(costs, 4)]
+    assert max(lpt) / min(lpt) < max(by_count) / min(by_count)
+
+
+def test_two_rank_gloo_uneven_sweep_gathers_every_problem_in_order(tmp_path):
+    import torch.multiprocessing as mp
+
+    from tests import sweep_worker
+    n = 9
+    mp.spawn(sweep_worker.run_uneven, args=(2, _port(), n, str(tmp_path)), nprocs=2, join=True)
+    problems = uneven_problems(n)
+    sc, prof = fake_uneven_solve(problems)(list(range(n)))
+    parts = partition_by_cost([problem_cost(p.model.grid.total_points) for p in problems], 2)
+    for r in range(2):
+        d = np.load(tmp_path / f"uneven{r}.npz")
+        np.testing.assert_array_equal(d["F"], sc[:, 0])
+        np.testing.assert_array_equal(d["it"], sc[:, 3].astype(int))
+        np.testing.assert_array_equal(d["conv"], sc[:, 4] > 0.5)
+        np.testing.assert_array_equal(d["seen"], parts[r])
+        np.testing.assert_array_equal(d["lens"], [len(p) for p in prof])
+        np.testing.assert_array_equal(d["prof"], np.concatenate(prof))
+        for i in range(n):
+            assert d["rank"][i] == (0 if i in parts[0] else 1)
 
 
 @pytest.mark.gpu
