@@ -460,6 +460,213 @@ def fire_step_rates(torch, cd, precision, steps=200):
     return out
 
 
+# ------------------------------------------------------------- config runs
+#
+# The other configurations of the workload family, each run once at N = 1 and
+# reported beside the headline: the drivers at their stated sizes, mixed
+# precision with FP64 refinement against FP64.
+
+
+def _lj_model(cd, n, dx, kT, diameter=None, rc=2.5, batch_shape=None):
+    lj = cd.make_lennard_jones(1.0, 1.0, rc)
+    d = diameter if diameter is not None else lj.hard_sphere_diameter(kT, cd.WEEKS_CHANDLER_ANDERSEN)
+    shape = batch_shape or (n, n, n)
+    g = cd.Grid(dx=dx, box_size=tuple(k * dx for k in shape), shape=shape)
+    return cd.Model(g, [cd.Species("LJ", d)], [cd.Interaction(0, 0, lj)], kT)
+
+
+def _smoothed_gaussian_noise(shape, dx, width, rng):
+    """Unit-normal white noise convolved with a normalised Gaussian of the
+    given width (sigma units), rescaled to unit variance."""
+    w = rng.standard_normal(shape)
+    k = [2.0 * np.pi * np.fft.fftfreq(n, d=dx) for n in shape]
+    K2 = k[0][:, None, None] ** 2 + k[1][None, :, None] ** 2 + k[2][None, None, :] ** 2
+    f = np.real(np.fft.ifftn(np.fft.fftn(w) * np.exp(-0.5 * width * width * K2)))
+    return (f / f.std()).reshape(-1)
+
+
+def config_wall(cd, torch):
+    """64^3, dx = 0.1, kT = 1, WBII (d = 1) + cut LJ (WCA, QF): rho = 0.5 (1 +
+    0.05 G) with G seeded unit-normal noise smoothed over 0.5 sigma; a hard
+    wall at x = 0 as rho = 0 and V_ext = 50 kT on the planes x < d/2.  FIRE
+    grand-potential minimisation at the bulk mu of rho = 0.5 to tolerance
+    1e-10 in FP64, and in mixed precision with the FP64 refine engine."""
+    n, dx = 64, 0.1
+    model = _lj_model(cd, n, dx, 1.0, diameter=1.0)
+    rng = np.random.default_rng(SEED + 1)
+    rho0 = 0.5 * (1.0 + 0.05 * _smoothed_gaussian_noise((n, n, n), dx, 0.5, rng))
+    ix = np.repeat(np.arange(n), n * n)
+    wall = ix * dx < 0.5
+    rho0[wall] = 0.0
+    vext = np.where(wall, 50.0, 0.0)
+    w64 = cd.make_weights(cd.WhiteBearII(), model, cd.FP64)
+    wmx = cd.make_weights(cd.WhiteBearII(), model, cd.MIXED)
+    mu = cd.make_bulk_thermodynamics(model.species, w64).chemical_potential([0.5], 0)
+    fire = cd.Fire(dt=0.1, dt_max=1.0, alpha_start=0.01, f_alpha=0.99, force_tolerance=1e-10, max_steps=50000)
+    out = {"workload": "64^3 WBII + cut LJ, hard wall at x = 0, grand potential at the mu of rho = 0.5",
+           "tolerance": 1e-10}
+    res = {}
+    for label, w, ref in (("fp64", w64, None), ("mixed_refined", wmx, w64)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = cd.Minimizer(fire=fire, refine=ref, refine_switch=1e3).grand_potential(model, w, rho0, mu,
+                                                                                 external_field=vext)
+        torch.cuda.synchronize()
+        res[label] = r
+        # the converged residual: max |dOmega/drho| over the fluid
+        chk = cd.total(model, [r.densities[0]], w64, [mu], [vext])
+        resid = float(np.max(np.abs(chk.forces[0][~wall]))) / model.grid.cell_volume
+        out[label] = {"iterations": r.iterations, "converged": r.converged, "wall_s": time.perf_counter() - t0,
+                      "grand_potential": r.grand_potential, "max_dOmega_drho_fluid": resid}
+    a, b = res["fp64"], res["mixed_refined"]
+    out["mixed_vs_fp64"] = {"max_drho": float(np.max(np.abs(a.densities[0] - b.densities[0]))),
+                            "dOmega_over_Omega": abs(a.grand_potential - b.grand_potential) / abs(a.grand_potential)}
+    for w in (w64, wmx):
+        w.engine.close()
+    return out
+
+
+def config_ddft(cd, torch, n_steps=2000):
+    """The headline state (128^3, dx = 0.125, kT = 0.8, rho = 0.35 (1 + 0.01 U))
+    relaxed by 2000 integrating-factor DDFT steps at dt = 1e-4 (dt_max = dt),
+    fixed-point tolerance 1e-8: FP64, and mixed precision with two FP64
+    refinement iterations per step; the difference every 100 steps."""
+    model = _lj_model(cd, 128, DX, KT)
+    rho0 = workload_profile()
+    w64 = cd.make_weights(cd.WhiteBearII(), model, cd.FP64)
+    wmx = cd.make_weights(cd.WhiteBearII(), model, cd.MIXED)
+    runs, times = {}, {}
+    for label, w, ref in (("fp64", w64, None), ("mixed_refined", wmx, w64)):
+        sim = cd.Simulation(step=cd.StepConfig(dt=1e-4, dt_max=1e-4, fp_tolerance=1e-8), n_steps=n_steps,
+                            snapshot_interval=100, log_interval=100, refine=ref)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        runs[label] = sim.run([rho0], w, 0.0)
+        torch.cuda.synchronize()
+        times[label] = time.perf_counter() - t0
+    per = []
+    for a, b in zip(runs["fp64"]["snapshots"], runs["mixed_refined"]["snapshots"]):
+        per.append([a.step, float(np.max(np.abs(a.densities[0] - b.densities[0]))),
+                    abs(a.energy - b.energy) / abs(a.energy)])
+    for w in (w64, wmx):
+        w.engine.close()
+    return {"workload": f"128^3 LJ fluid, {n_steps} IF steps at dt = 1e-4, fp_tolerance 1e-8",
+            "fp64_s": times["fp64"], "mixed_refined_s": times["mixed_refined"],
+            "fp64_steps_per_s": n_steps / times["fp64"], "mixed_refined_steps_per_s": n_steps / times["mixed_refined"],
+            "per_100_steps": {"columns": ["step", "max_drho", "dF_over_F"], "rows": per},
+            "max_drho": max(r[1] for r in per), "max_dF_over_F": max(r[2] for r in per)}
+
+
+def config_nucleus(cd, torch):
+    """Critical vapour-liquid nucleus: 128^3, dx = 0.1 (L = 12.8), LJ (rc = 3)
+    at kT = 0.7, WBII; vapour at S = 1.5 times the coexisting vapour density,
+    a tanh droplet of radius 3 sigma and width 0.5 of the coexisting liquid;
+    the fixed-mass FP64 FIRE cluster, then the saddle search (eigenvector
+    following at fixed mass, the lowest mode by block Lanczos, block 2, on
+    batched FP64 Hessian-vector products) in FP64 and in mixed precision with
+    the FP64 refine engine, both from that cluster.  The barrier is Omega at
+    the saddle minus Omega of the uniform background at its chemical
+    potential."""
+    n, dx, kT = 128, 0.1, 0.7
+    model = _lj_model(cd, n, dx, kT, rc=3.0)
+    w64 = cd.make_weights(cd.WhiteBearII(), model, cd.FP64)
+    wmx = cd.make_weights(cd.WhiteBearII(), model, cd.MIXED)
+    hw = cd.make_weights(cd.WhiteBearII(), model, cd.FP64, batch=2)
+    eos = cd.make_bulk_thermodynamics(model.species, w64)
+    co = cd.PhaseSearch(rho_max=1.0, rho_scan_step=0.005).find_coexistence(eos)
+    rout = 1.5 * co.rho_vapor
+    mu = eos.chemical_potential([rout], 0)
+    x = np.arange(n) * dx - n * dx / 2
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    r = np.sqrt(X ** 2 + Y ** 2 + Z ** 2).ravel()
+    rho0 = rout + (co.rho_liquid - rout) * 0.5 * (1.0 - np.tanh((r - 3.0) / 0.5))
+    dv = model.grid.cell_volume
+    tm = float(rho0.sum()) * dv
+    out = {"workload": "128^3 LJ nucleus at kT = 0.7, S = 1.5, tanh R = 3 sigma (WBII)",
+           "rho_vapor": co.rho_vapor, "rho_liquid": co.rho_liquid}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    cl = cd.Minimizer(fire=cd.Fire(dt=0.1, dt_max=1.0, alpha_start=0.01, f_alpha=0.99, force_tolerance=1e-9,
+                                   max_steps=50000), param=cd.Unbounded(1e-99)).fixed_mass(model, w64, rho0, mu, tm)
+    torch.cuda.synchronize()
+    rc = np.asarray(cl.densities[0])
+    faces = model.grid.boundary_mask().astype(bool)
+    bg = float(rc[faces].mean())
+    mubg = eos.chemical_potential([bg], 0)
+    omega_bg = cd.total(model, [np.full(rc.size, bg)], w64, [mubg]).grand_potential
+    out["cluster"] = {"iterations": cl.iterations, "converged": cl.converged, "s": time.perf_counter() - t0,
+                      "background": bg, "max_density": float(rc.max())}
+    res = {}
+    for label, w, kw in (("fp64", w64, {}), ("mixed_refined", wmx, {"refine": w64})):
+        se = cd.Search(fire=cd.Fire(dt=1e-3, dt_max=1.0, alpha_start=0.01, f_alpha=1.0, force_tolerance=1e-10,
+                                    max_steps=20000),
+                       eigenvalue=cd.EigenvalueSolver(1e-6, 300, exact_hvp=True, method="lanczos", block=2),
+                       omega_tolerance=1e-9, tolerance_start=1e-6, max_outer_iterations=12, hvp_weights=hw, **kw)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s_ = se.find(model, w, rc, mubg, tm)
+        torch.cuda.synchronize()
+        res[label] = s_
+        out[label] = {"barrier": s_.grand_potential - omega_bg, "grand_potential": s_.grand_potential,
+                      "eigenvalue": s_.eigenvalue, "converged": s_.converged,
+                      "outer_iterations": s_.outer_iterations, "fire_steps": s_.fire_steps,
+                      "lanczos_products": s_.eigen_iterations, "s": time.perf_counter() - t0}
+    a, b = out["fp64"], out["mixed_refined"]
+    out["mixed_vs_fp64"] = {"barrier_rel": abs(a["barrier"] - b["barrier"]) / abs(a["barrier"]),
+                            "eigenvalue_rel": abs(a["eigenvalue"] - b["eigenvalue"]) / abs(a["eigenvalue"]),
+                            "max_drho": float(np.max(np.abs(res["fp64"].density - res["mixed_refined"].density)))}
+    for w in (w64, wmx, hw):
+        w.engine.close()
+    return out
+
+
+def config_sweep(cd, torch):
+    """16 state points each on 48^3, 64^3 and 96^3 grids (dx = 0.1, kT = 1,
+    WBII + cut LJ), mu evenly spaced over the liquid branch (from the bulk
+    coexistence to 1.5 above it), seeded 1% noise around the bulk liquid
+    density: FIRE grand-potential minimisations as one group minimisation
+    (one graph launch per step for all 48), against the three per-size
+    batched minimisations one after another."""
+    per = 16
+    lj = cd.make_lennard_jones(1.0, 1.0, 2.5)
+    rng = np.random.default_rng(SEED + 4)
+    fire = cd.Fire(dt=0.05, dt_max=0.5, alpha_start=0.01, f_alpha=0.99, force_tolerance=1e-10, max_steps=4000)
+    members, ws = [], []
+    eos = None
+    for n in SWEEP_SHAPES:
+        model = _lj_model(cd, n, 0.1, 1.0)
+        w = cd.make_weights(cd.WhiteBearII(), model, cd.FP64, batch=per)
+        if eos is None:
+            eos = cd.make_bulk_thermodynamics(model.species, w)
+            co = cd.PhaseSearch(rho_max=1.0, rho_scan_step=0.005).find_coexistence(eos)
+            mu_coex = eos.chemical_potential([co.rho_liquid], 0)
+            mus = np.linspace(mu_coex, mu_coex + 1.5, per)
+            rl = [cd.density_from_chemical_potential(m, co.rho_liquid, eos) for m in mus]
+        N = model.grid.total_points
+        rhos = np.stack([rl[b] * (1.0 + 0.01 * rng.uniform(-1.0, 1.0, N)) for b in range(per)])
+        members.append((w, rhos, mus, None))
+        ws.append(w)
+    mz = cd.Minimizer(fire=fire)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = mz.minimize_group(members)
+    torch.cuda.synchronize()
+    t_group = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    seq = [mz.grand_potential_batch(None, w, rhos, mus) for (w, rhos, mus, _) in members]
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    steps = sum(r.iterations for rs in res for r in rs)
+    same = all(np.array_equal(a.densities[0], b.densities[0]) for ra, rb in zip(res, seq) for a, b in zip(ra, rb))
+    for w in ws:
+        w.engine.close()
+    return {"workload": "16 each of 48^3 / 64^3 / 96^3 grand-potential minimisations (WBII + cut LJ, kT = 1)",
+            "converged": int(sum(r.converged for rs in res for r in rs)), "problems": 3 * per,
+            "problem_steps": steps, "group_s": t_group, "per_size_batches_s": t_seq,
+            "group_problem_steps_per_s": steps / t_group, "per_size_problem_steps_per_s": steps / t_seq,
+            "speedup": t_seq / t_group, "identical_to_per_size_runs": bool(same)}
+
+
 def run_ours(args, ws, rank, local, dist):
     import ctypes
     import torch
@@ -590,6 +797,14 @@ def run_ours(args, ws, rank, local, dist):
         "clocks": clocks,
         "gpu_launches": int(info["kernels_per_eval"]) * args.steps,
     }
+    if ws == 1 and not args.no_configs:
+        # the other configurations at their own sizes (N = 1 only)
+        for key, fn in (("config_wall_64", config_wall), ("config_ddft_128", config_ddft),
+                        ("config_nucleus_128", config_nucleus), ("config_sweep_48_64_96", config_sweep)):
+            try:
+                line[key] = fn(cd, torch)
+            except Exception as exc:  # reported, not hidden
+                line[key] = {"error": f"{type(exc).__name__}: {exc}"}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cb, ref = cpu_baseline_sample(args.cpu_seconds)
         line["cpu_baseline"] = cb
@@ -618,6 +833,8 @@ def main():
     ap.add_argument("--plane-chunks", type=int, default=0,
                     help="plane chunks of the fused path's middle stages (0: the engine's default; 1 runs them "
                          "back to back, as a profiler's serialised launch list sees them)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the runs of the other configurations (wall, DDFT, nucleus, uneven sweep)")
     ap.add_argument("--traffic-table", metavar="NCU_CSV",
                     help="print the per-stage DRAM traffic table from an ncu --csv launch list and exit")
     args = ap.parse_args()

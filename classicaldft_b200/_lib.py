@@ -58,7 +58,8 @@ class CMinimizerConfig(ctypes.Structure):
     _fields_ = [("fire", CFireParams), ("mode", ctypes.c_int), ("parametrization", ctypes.c_int),
                 ("rho_min", ctypes.c_double), ("rho_max", ctypes.c_double), ("homogeneous_boundary", ctypes.c_int),
                 ("chemical_potential", ctypes.c_double), ("target_mass", ctypes.c_double),
-                ("boundary_mass", ctypes.c_double), ("use_monitor", ctypes.c_int), ("check_interval", ctypes.c_int)]
+                ("boundary_mass", ctypes.c_double), ("use_monitor", ctypes.c_int), ("check_interval", ctypes.c_int),
+                ("external_field", ctypes.c_void_p)]
 
 
 class CMinimizerResult(ctypes.Structure):

@@ -133,12 +133,18 @@ class Minimizer:
         return cfg
 
     def _run(self, weights: Weights, rho, mode, mu, target_mass=0.0, boundary_mass=0.0, direction=None,
-             use_monitor=True):
+             use_monitor=True, external_field=None):
         torch = _torch()
         d, host = _dev(rho)
         if not host:
             d = d.clone()
         cfg = self._config(mode, mu, target_mass, boundary_mass, use_monitor)
+        vx = None
+        if external_field is not None:
+            vx, _ = _dev(np.asarray(external_field, dtype=np.float64).reshape(-1)
+                         if not hasattr(external_field, "data_ptr") else external_field)
+            vx = vx.to(torch.float64).contiguous()
+            cfg.external_field = vx.data_ptr()
         res = _lib.CMinimizerResult()
         dirp = None
         if direction is not None:
@@ -157,13 +163,18 @@ class Minimizer:
         return MinimizationResult([out], res.free_energy, res.grand_potential, res.rms_force, res.iterations,
                                   bool(res.converged))
 
-    def grand_potential(self, model: Model, weights: Weights, initial_density, chemical_potential):
-        """minimization.hpp:280-354."""
-        return self._run(weights, initial_density, 0, chemical_potential)
+    def grand_potential(self, model: Model, weights: Weights, initial_density, chemical_potential,
+                        external_field=None):
+        """minimization.hpp:280-354.  ``external_field`` (N values, or None):
+        V_ext / kT of every evaluation (a wall; the reference's Minimizer has
+        no field, its profile states drop V_ext)."""
+        return self._run(weights, initial_density, 0, chemical_potential, external_field=external_field)
 
-    def fixed_mass(self, model: Model, weights: Weights, initial_density, chemical_potential, target_mass):
-        """minimization.hpp:182-278."""
-        return self._run(weights, initial_density, 1, chemical_potential, target_mass=target_mass)
+    def fixed_mass(self, model: Model, weights: Weights, initial_density, chemical_potential, target_mass,
+                   external_field=None):
+        """minimization.hpp:182-278 (``external_field`` as grand_potential)."""
+        return self._run(weights, initial_density, 1, chemical_potential, target_mass=target_mass,
+                         external_field=external_field)
 
     def _run_batch(self, weights: Weights, rhos, mode, mus, masses=None):
         torch = _torch()

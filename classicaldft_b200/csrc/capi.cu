@@ -423,6 +423,7 @@ cdft::FireConfig to_fire_config(const cdft_minimizer_config* cfg) {
   fc.boundary_mass = cfg->boundary_mass;
   fc.use_monitor = cfg->use_monitor != 0;
   fc.check_interval = cfg->check_interval > 0 ? cfg->check_interval : 25;
+  fc.vext = cfg->external_field;
   return fc;
 }
 

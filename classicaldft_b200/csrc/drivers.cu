@@ -68,6 +68,7 @@ struct Vec {
   double* rho;
   double* grad;
   const double* dir;
+  const double* vext;  // external field of the evaluations (B*N) or null
   long long N;
   int nx, ny, nz;
   double dv;
@@ -1033,7 +1034,16 @@ struct FireRun {
   bool refining = false;
   int steps = 0;
   bool done = false;
+  // stagnation of the mixed-precision run: the best convergence measure seen
+  // at a check and the checks since it last improved by 10%
+  double best_metric = 0.0;
+  int stalled_checks = 0;
 };
+
+// Checks without a 10% improvement after which the FP64 engine takes over:
+// mixed-precision forces have a noise floor, and a tolerance below it is
+// reached only with FP64 forces.
+constexpr int kStallChecks = 8;
 
 // rescale (fixed mass / saddle), evaluate, post-process into f
 void Drivers::fire_compute(int initial, cudaStream_t stream) {
@@ -1046,7 +1056,7 @@ void Drivers::fire_compute(int initial, cudaStream_t stream) {
   k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
   k_scale_factor<<<B, 32, 0, stream>>>(st_, red_out_, r.cc, p.dv, initial);
   k_rescale<<<gv, kBlock, 0, stream>>>(r.a, st_, r.cc, initial);
-  r.eng->evaluate(r.a.rho, nullptr, r.mu_compute.data(), grad_, scalars_, stream);
+  r.eng->evaluate(r.a.rho, r.a.vext, r.mu_compute.data(), grad_, scalars_, stream);
   k_post_sums<<<gv, kBlock, 0, stream>>>(r.a, red_);
   k_finish_sums<<<B, rt, 0, stream>>>(red_, grid_, red_out_);
   k_post_control<<<B, 32, 0, stream>>>(st_, red_out_, r.cc);
@@ -1075,6 +1085,7 @@ void Drivers::fire_begin(const FireConfig& cfg, const double* mu, const double* 
   a.rho = rho;
   a.grad = grad_;
   a.dir = direction;
+  a.vext = cfg.vext;
   a.N = N_;
   a.nx = p.nx;
   a.ny = p.ny;
@@ -1145,16 +1156,27 @@ int Drivers::fire_decide(cudaStream_t stream, bool* engine_changed) {
   if (engine_changed) *engine_changed = false;
   if (r.done) return 0;
   bool any_active = false, all_close = true;
+  double worst = 0.0;
   for (int b = 0; b < B_; ++b) {
     const FireDevState& h = st_host_[b];
     if (!h.active) continue;
     any_active = true;
     const double metric = r.cfg.use_monitor ? h.monitor : h.rms_force;
+    worst = std::max(worst, metric);
     if (!(h.iteration > 0 && metric < r.refine_switch * fp.force_tolerance)) all_close = false;
+  }
+  if (r.refine && !r.refining && any_active && r.steps > 0) {
+    if (r.best_metric == 0.0 || worst < 0.9 * r.best_metric) {
+      r.best_metric = worst;
+      r.stalled_checks = 0;
+    } else if (++r.stalled_checks >= kStallChecks) {
+      all_close = true;
+    }
   }
   if (r.refine && !r.refining && all_close && r.steps < fp.max_steps) {
     // FP64 defect correction from here on: once every running problem is
-    // within refine_switch of the tolerance, or once all of them have
+    // within refine_switch of the tolerance, once the mixed-precision run
+    // has stopped improving (its noise floor), or once all problems have
     // converged under the mixed-precision forces
     r.eng = r.refine;
     r.refining = true;
@@ -1194,7 +1216,7 @@ std::vector<FireResult> Drivers::fire_finish(cudaStream_t stream) {
   // already holds rho(x) with the mass rescale of the last compute, which is
   // exactly the reference's extraction from the final x.  The final total()
   // uses the caller's chemical potential (fixed mass iterates with mu = 0).
-  r.eng->evaluate(r.a.rho, nullptr, r.mu_final.data(), grad_, scalars_, stream);
+  r.eng->evaluate(r.a.rho, r.a.vext, r.mu_final.data(), grad_, scalars_, stream);
   std::vector<double> sc((size_t)B * kScalarCount);
   CDFT_CUDA(cudaMemcpyAsync(sc.data(), scalars_, sizeof(double) * sc.size(), cudaMemcpyDeviceToHost, stream));
   CDFT_CUDA(cudaStreamSynchronize(stream));

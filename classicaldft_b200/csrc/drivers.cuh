@@ -61,6 +61,10 @@ struct FireConfig {
   double boundary_mass = 0.0;   // saddle: mass held by the boundary shell
   int check_interval = 25;
   bool use_monitor = true;      // Minimizer convergence (minimization.hpp:431-434) vs rms (fire.hpp:162)
+  // External field of every evaluation (device, B*N, or null).  The
+  // reference's Minimizer evaluates without one (init::from_profile drops
+  // V_ext, init.hpp:28-58); a wall or a trap needs it.
+  const double* vext = nullptr;
 };
 
 struct FireResult {

@@ -224,6 +224,10 @@ typedef struct {
   double boundary_mass;     /* saddle: mass of the boundary shell */
   int use_monitor;          /* 1: the minimiser's energy monitor; 0: rms force (Fire::step) */
   int check_interval;       /* device steps between host checks */
+  /* external field of every evaluation: device, B * N doubles (the engine's
+   * batch), or NULL.  The reference's Minimizer has none (init.hpp:28-58
+   * drops V_ext); a hard wall or a trap needs it. */
+  const double* external_field;
 } cdft_minimizer_config;
 
 typedef struct {
@@ -237,9 +241,10 @@ typedef struct {
  * by the minimiser's final density.  `refine` (or NULL): an FP64 engine of
  * the same model that takes over once the convergence measure (the monitor,
  * or the rms force when use_monitor is 0) drops below refine_switch *
- * force_tolerance, or once the run has converged under the engine's own
- * forces, and continues until the FP64 forces converge too (mixed-precision
- * defect correction).
+ * force_tolerance, once it has not improved by 10% over 8 host checks (the
+ * noise floor of mixed-precision forces), or once the run has converged
+ * under the engine's own forces, and continues until the FP64 forces
+ * converge too (mixed-precision defect correction).
  * Returns CDFT_ERR_RUNTIME with "fire::step: exceeded max uphill steps" where
  * the reference throws (fire.hpp:106-108). */
 CDFT_API int cdft_minimize(cdft_engine* engine, const cdft_minimizer_config* cfg, double* rho,

@@ -80,9 +80,9 @@ def test_group_graphs_and_members_alone_are_bitwise_equal():
 def test_mixed_group_with_refinement_matches_fp64():
     probs = setup()
     probs_m = setup(cd.MIXED)
-    f64 = group(cd.Minimizer(fire=cd.Fire(**dict(FIRE, force_tolerance=1e-11))), probs)
-    mix = group(cd.Minimizer(fire=cd.Fire(**dict(FIRE, force_tolerance=1e-11)), refine_switch=1e3), probs_m,
-                precision=cd.MIXED, refine=True)
+    tight = dict(FIRE, force_tolerance=1e-13, max_steps=12000)
+    f64 = group(cd.Minimizer(fire=cd.Fire(**tight)), probs)
+    mix = group(cd.Minimizer(fire=cd.Fire(**tight), refine_switch=1e3), probs_m, precision=cd.MIXED, refine=True)
     for a, b in zip(f64, mix):
         for k in range(PER):
             assert a[k].converged and b[k].converged
