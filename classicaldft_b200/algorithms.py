@@ -115,8 +115,14 @@ class Minimizer:
     check_interval: int = 25
     refine: Weights = None
     refine_switch: float = 10.0
+    # convergence test: the reference Minimizer's energy monitor
+    # (minimization.hpp:431-434), or with False the rms force of Fire::step
+    # (fire.hpp:162) against fire.force_tolerance
+    use_monitor: bool = True
 
-    def _config(self, mode, mu, target_mass=0.0, boundary_mass=0.0, use_monitor=True):
+    def _config(self, mode, mu, target_mass=0.0, boundary_mass=0.0, use_monitor=None):
+        if use_monitor is None:
+            use_monitor = self.use_monitor
         cfg = _lib.CMinimizerConfig()
         cfg.fire = self.fire.c()
         cfg.mode = mode
@@ -133,7 +139,7 @@ class Minimizer:
         return cfg
 
     def _run(self, weights: Weights, rho, mode, mu, target_mass=0.0, boundary_mass=0.0, direction=None,
-             use_monitor=True, external_field=None):
+             use_monitor=None, external_field=None):
         torch = _torch()
         d, host = _dev(rho)
         if not host:

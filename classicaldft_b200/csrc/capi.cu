@@ -343,8 +343,41 @@ int cdft_engine_autotune(cdft_engine* engine, const double* rho, const double* v
   return guarded([&] {
     if (!engine || !rho) throw std::invalid_argument("engine and rho are required");
     if (reps < 1) throw std::invalid_argument("autotune: reps must be positive");
-    const int k = engine->impl->autotune(rho, vext, mu, static_cast<cudaStream_t>(stream), reps, ms);
+    double all[cdft::Engine::kPointwiseVariants * cdft::Engine::kMaxChunks];
+    int v = 0;
+    const int k = engine->impl->autotune(rho, vext, mu, static_cast<cudaStream_t>(stream), reps, all, &v);
     if (chunks) *chunks = k;
+    if (ms)
+      for (int c = 0; c < cdft::Engine::kMaxChunks; ++c) ms[c] = all[v * cdft::Engine::kMaxChunks + c];
+  });
+}
+
+int cdft_engine_autotune_ex(cdft_engine* engine, const double* rho, const double* vext, const double* mu,
+                            void* stream, int reps, int choice[2], double* ms) {
+  return guarded([&] {
+    if (!engine || !rho) throw std::invalid_argument("engine and rho are required");
+    if (reps < 1) throw std::invalid_argument("autotune: reps must be positive");
+    int v = 0;
+    const int k = engine->impl->autotune(rho, vext, mu, static_cast<cudaStream_t>(stream), reps, ms, &v);
+    if (choice) {
+      choice[0] = k;
+      choice[1] = v;
+    }
+  });
+}
+
+int cdft_engine_set_pointwise(cdft_engine* engine, int variant) {
+  return guarded([&] {
+    if (!engine) throw std::invalid_argument("engine is NULL");
+    engine->impl->set_pointwise(variant);
+  });
+}
+
+int cdft_engine_pointwise(const cdft_engine* engine, int* variant, int* available) {
+  return guarded([&] {
+    if (!engine) throw std::invalid_argument("engine is NULL");
+    if (variant) *variant = engine->impl->pointwise();
+    if (available) *available = engine->impl->pointwise_one_species() ? 1 : 0;
   });
 }
 

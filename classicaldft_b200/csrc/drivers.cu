@@ -1474,35 +1474,41 @@ void Drivers::ddft_epilogue(const DDFTConfig& cfg, cudaStream_t s) {
   CDFT_CUDA(cudaGetLastError());
 }
 
-// Capture of the whole step on the driver stream: prologue, a conditional
-// WHILE node whose body (captured on a second stream into the node's body
-// graph) is one fixed-point iteration, then the epilogue.
+// The whole step as one graph: the prologue, a conditional WHILE node whose
+// body is one fixed-point iteration, the epilogue.  Each part is captured as
+// an ordinary graph on the driver stream (the evaluation may fork its plane
+// chunks onto other streams, which a capture straight into a conditional
+// body does not support) and embedded as a child-graph node.
 void Drivers::capture_ddft_step(const DDFTConfig& cfg) {
   reset_fp_graph();
-  if (!body_stream_) CDFT_CUDA(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
   cudaStream_t s = graph_stream_;
-  auto abort_capture = [&] {
-    for (cudaStream_t t : {body_stream_, s}) {
-      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-      cudaStreamIsCapturing(t, &cs);
-      if (cs != cudaStreamCaptureStatusNone) {
-        cudaGraph_t g = nullptr;
-        cudaStreamEndCapture(t, &g);
-        if (g) cudaGraphDestroy(g);
-      }
-    }
-    cudaGetLastError();
+  cudaGraph_t parts[3] = {nullptr, nullptr, nullptr};
+  auto release_parts = [&] {
+    for (cudaGraph_t& g : parts)
+      if (g) cudaGraphDestroy(g);
   };
-  CDFT_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  auto capture = [&](int k, auto&& launches) {
+    CDFT_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+      launches();
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(s, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      throw;
+    }
+    CDFT_CUDA(cudaStreamEndCapture(s, &parts[k]));
+  };
   try {
-    ddft_prologue(cfg, s);
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    cudaGraph_t cg = nullptr;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t nd = 0;
-    CDFT_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd));
+    CDFT_CUDA(cudaGraphCreate(&fp_graph_, 0));
     cudaGraphConditionalHandle h = 0;
-    CDFT_CUDA(cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault));
+    CDFT_CUDA(cudaGraphConditionalHandleCreate(&h, fp_graph_, 1, cudaGraphCondAssignDefault));
+    capture(0, [&] { ddft_prologue(cfg, s); });
+    capture(1, [&] { ddft_body(cfg, s, h, 1); });
+    capture(2, [&] { ddft_epilogue(cfg, s); });
+    cudaGraphNode_t pro = nullptr, loop = nullptr, epi = nullptr, it = nullptr;
+    CDFT_CUDA(cudaGraphAddChildGraphNode(&pro, fp_graph_, nullptr, 0, parts[0]));
     // zero-filled storage: the parameter union has no default constructor
     alignas(cudaGraphNodeParams) unsigned char np_buf[sizeof(cudaGraphNodeParams)] = {};
     cudaGraphNodeParams& np = *reinterpret_cast<cudaGraphNodeParams*>(np_buf);
@@ -1510,23 +1516,17 @@ void Drivers::capture_ddft_step(const DDFTConfig& cfg) {
     np.conditional.handle = h;
     np.conditional.type = cudaGraphCondTypeWhile;
     np.conditional.size = 1;
-    cudaGraphNode_t node = nullptr;
-    CDFT_CUDA(cudaGraphAddNode(&node, cg, deps, nd, &np));
+    CDFT_CUDA(cudaGraphAddNode(&loop, fp_graph_, &pro, 1, &np));
     cudaGraph_t body = np.conditional.phGraph_out[0];
-    CDFT_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
-    CDFT_CUDA(cudaStreamBeginCaptureToGraph(body_stream_, body, nullptr, nullptr, 0,
-                                            cudaStreamCaptureModeThreadLocal));
-    ddft_body(cfg, body_stream_, h, 1);
-    cudaGraph_t body_out = nullptr;
-    CDFT_CUDA(cudaStreamEndCapture(body_stream_, &body_out));
-    ddft_epilogue(cfg, s);
-    CDFT_CUDA(cudaStreamEndCapture(s, &fp_graph_));
+    CDFT_CUDA(cudaGraphAddChildGraphNode(&it, body, nullptr, 0, parts[1]));
+    CDFT_CUDA(cudaGraphAddChildGraphNode(&epi, fp_graph_, &loop, 1, parts[2]));
+    CDFT_CUDA(cudaGraphInstantiate(&fp_exec_, fp_graph_, 0));
   } catch (...) {
-    abort_capture();
+    release_parts();
     reset_fp_graph();
     throw;
   }
-  CDFT_CUDA(cudaGraphInstantiate(&fp_exec_, fp_graph_, 0));
+  release_parts();  // the child nodes hold copies
 }
 
 // integrating_factor_step (dynamics.hpp:333-401).  With step graphs on, the

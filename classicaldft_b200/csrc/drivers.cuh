@@ -353,7 +353,6 @@ class Drivers {
   void capture_ddft_step(const DDFTConfig& cfg);
   void* ddft_st_ = nullptr;       // device control state of the IF step
   void* ddft_st_host_ = nullptr;  // pinned copy
-  cudaStream_t body_stream_ = nullptr;
   Engine* ddft_refine_ = nullptr;
   int ddft_refine_iterations_ = 0;
   DDFTStepInfo ddft_info_;

@@ -18,6 +18,7 @@ namespace {
 // The autotuner's choices per engine shape, for the lifetime of the process.
 std::mutex g_tune_mu;
 std::map<std::string, int> g_tune_chunks;
+std::map<std::string, int> g_tune_variant;
 }  // namespace
 
 namespace {
@@ -118,6 +119,64 @@ void Engine::with_kernels(bool mixed, F&& f) const {
     by_multi(std::type_identity<float>{});
   else
     by_multi(std::type_identity<double>{});
+}
+
+namespace {
+// f(IC<m>) for a mean-field channel count m in 0..2 of the one-species kernel.
+template <class F>
+void with_nmf(int m, F&& f) {
+  if (m == 0)
+    f(std::integral_constant<int, 0>{});
+  else if (m == 1)
+    f(std::integral_constant<int, 1>{});
+  else
+    f(std::integral_constant<int, 2>{});
+}
+}  // namespace
+
+// The TMA-staged pointwise kernel over points p0 .. p0 + pn of every problem:
+// the one-species specialisation where it applies, else the generic kernel.
+template <typename R>
+void Engine::launch_pointwise_tma(const R* chan, R* deriv, const PointwiseArgs& a, long long p0, long long pn,
+                                  int blk0, int nblk, int grid, cudaStream_t st) {
+  const EvalParams& p = p_;
+  const bool vext = a.vext != nullptr;
+  const dim3 g(grid, p.batch);
+  if constexpr (std::is_same_v<R, float>) {
+    if (pw1_ && pw_variant_ > 0) {
+      with_kernels(true, [&](auto model_c, auto, auto) {
+        constexpr int MD = decltype(model_c)::value;
+        with_nmf(p.M, [&](auto nc) {
+          constexpr int NMF = decltype(nc)::value;
+          auto go = [&](auto kern, size_t smem) {
+            kern<<<g, kTmaTile, smem, st>>>(p, chan, deriv, a, err_, p0, pn, blk0, nblk);
+          };
+          if (pw_variant_ == 1) {
+            if (vext)
+              go(k_pointwise1_tma<MD, NMF, true, 5>, tma1_smem_v_);
+            else
+              go(k_pointwise1_tma<MD, NMF, false, 5>, tma1_smem_);
+          } else {
+            if (vext)
+              go(k_pointwise1_tma<MD, NMF, true, 6>, tma1_smem_v_);
+            else
+              go(k_pointwise1_tma<MD, NMF, false, 6>, tma1_smem_);
+          }
+        });
+      });
+      CDFT_CUDA(cudaGetLastError());
+      return;
+    }
+  }
+  with_kernels(sizeof(R) == sizeof(float), [&](auto model_c, auto multi_c, auto r_c) {
+    constexpr int MD = decltype(model_c)::value;
+    constexpr bool MU = decltype(multi_c)::value;
+    using RT = typename decltype(r_c)::type;
+    if constexpr (std::is_same_v<RT, R>)
+      k_pointwise_tma<MD, MU, RT><<<g, kTmaTile, vext ? tma_smem_v_ : tma_smem_, st>>>(p, chan, deriv, a, err_, p0,
+                                                                                       pn, blk0, nblk);
+  });
+  CDFT_CUDA(cudaGetLastError());
 }
 
 Engine::Engine(const EngineSpec& spec) {
@@ -233,13 +292,46 @@ Engine::Engine(const EngineSpec& spec) {
                                                             tma_smem_v_));
     grid_tma_ = per_problem((long long)sms * std::max(per_sm, 1));
   });
+  // the one-species mixed-precision specialisation (k_pointwise1_tma)
+  pw1_ = mixed && p.S == 1 && p.M <= 2;
+  if (pw1_) {
+    with_kernels(true, [&](auto model_c, auto, auto) {
+      constexpr int MD = decltype(model_c)::value;
+      constexpr bool TE = model_has_tensor(MD);
+      with_nmf(p.M, [&](auto nc) {
+        constexpr int NMF = decltype(nc)::value;
+        const int sb = kTmaStages * tma1_stage_bytes<NMF, false, TE>();
+        const int sv = kTmaStages * tma1_stage_bytes<NMF, true, TE>();
+        CDFT_CUDA(cudaFuncSetAttribute(k_pointwise1_tma<MD, NMF, false, 5>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, sb));
+        CDFT_CUDA(cudaFuncSetAttribute(k_pointwise1_tma<MD, NMF, true, 5>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, sv));
+        CDFT_CUDA(cudaFuncSetAttribute(k_pointwise1_tma<MD, NMF, false, 6>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, sb));
+        CDFT_CUDA(cudaFuncSetAttribute(k_pointwise1_tma<MD, NMF, true, 6>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, sv));
+        int per5 = 0, per6 = 0;
+        CDFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per5, k_pointwise1_tma<MD, NMF, true, 5>, kTmaTile,
+                                                                sv));
+        CDFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per6, k_pointwise1_tma<MD, NMF, true, 6>, kTmaTile,
+                                                                sv));
+        grid_pw1_[0] = per_problem((long long)sms * std::max(per5, 1));
+        grid_pw1_[1] = per_problem((long long)sms * std::max(per6, 1));
+        tma1_smem_ = (size_t)kTmaStages * tma1_stage_bytes<NMF, false, TE>();
+        tma1_smem_v_ = (size_t)kTmaStages * tma1_stage_bytes<NMF, true, TE>();
+      });
+    });
+    pw_variant_ = 1;
+  }
   grid_stream_ = per_problem(std::max<long long>(1, std::min<long long>((long long)sms * 8, (p.N * B + 255) / 256)));
   // the species mean: four blocks per SM in all (its last block sums the
   // partials, so fewer blocks shorten that tail and the counter's contention)
   grid_mean_ = per_problem(std::max<long long>(1, std::min<long long>((long long)sms * 4, (p.N * B + 255) / 256)));
   // (+8: the pointwise grid rounded up to whole chunks, see fused_middle)
   partials_ =
-      dalloc<double>((size_t)B * (std::max(std::max(grid_pw_, grid_tma_), grid_stream_) + 8) * p.n_terms, tot);
+      dalloc<double>((size_t)B *
+                         (std::max({grid_pw_, grid_tma_, grid_stream_, grid_pw1_[0], grid_pw1_[1]}) + 8) * p.n_terms,
+                     tot);
   err_ = dalloc<int>(1, tot);
   CDFT_CUDA(cudaMemset(err_, 0, sizeof(int)));
   sync_ = dalloc<unsigned>((size_t)B, tot);
@@ -322,6 +414,16 @@ long long Engine::take_stage_times(double* ms) {
 // cuFFT plans.
 void Engine::setup_fused() {
   const EvalParams& p = p_;
+  // shape key of the autotuner's cache: grid, species, batch, model,
+  // interactions, precision (and the pointwise variant kept for it)
+  tune_key_ = std::to_string(p.nx) + "x" + std::to_string(p.ny) + "x" + std::to_string(p.nz) + " S" +
+              std::to_string(p.S) + " B" + std::to_string(p.batch) + " m" + std::to_string(p.model) + " M" +
+              std::to_string(p.M) + " P" + std::to_string(precision_);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    const auto iv = g_tune_variant.find(tune_key_);
+    if (iv != g_tune_variant.end() && (iv->second == 0 || pw1_)) pw_variant_ = iv->second;
+  }
   fusable_ = false;
   if (precision_ != kMixed || !fused_plan(p, &plan_)) return;
   // twiddle tables, FP64-rounded
@@ -347,11 +449,6 @@ void Engine::setup_fused() {
   fusable_ = true;
   fused_ = true;
   chunks_ = (p.nx >= 64) ? 4 : 1;
-  // shape key of the autotuner's cache: grid, species and diameters, batch,
-  // model, interactions
-  tune_key_ = std::to_string(p.nx) + "x" + std::to_string(p.ny) + "x" + std::to_string(p.nz) + " S" +
-              std::to_string(p.S) + " B" + std::to_string(p.batch) + " m" + std::to_string(p.model) + " M" +
-              std::to_string(p.M);
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     const auto it = g_tune_chunks.find(tune_key_);
@@ -373,11 +470,15 @@ void Engine::ensure_chunk_streams(int k) {
   if (k > 1 && !fork_ev_) CDFT_CUDA(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
 }
 
+// Every (plane-chunk count, pointwise variant) pair the engine has, timed on
+// the caller's state; the fastest is kept and cached for the shape.
 int Engine::autotune(const double* rho, const double* vext, const double* mu, cudaStream_t stream, int reps,
-                     double* ms) {
+                     double* ms, int* variant) {
   if (ms)
-    for (int k = 0; k < kMaxChunks; ++k) ms[k] = 0.0;
-  if (!fusable_ || !fused_) return chunks_;
+    for (int k = 0; k < kPointwiseVariants * kMaxChunks; ++k) ms[k] = 0.0;
+  if (variant) *variant = pw_variant_;
+  const bool tune_chunks = fusable_ && fused_;
+  if (!tune_chunks && !pw1_) return chunks_;
   if (!rho) throw std::invalid_argument("autotune: rho is required");
   reps = std::max(reps, 1);
   std::vector<double> mu0((size_t)p_.batch * p_.S, 0.0);
@@ -387,33 +488,56 @@ int Engine::autotune(const double* rho, const double* vext, const double* mu, cu
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   CDFT_CUDA(cudaEventCreate(&e0));
   CDFT_CUDA(cudaEventCreate(&e1));
-  int best = chunks_;
+  int best = chunks_, best_v = pw_variant_;
   double best_ms = 0.0;
-  for (int k = 1; k <= kMaxChunks; k *= 2) {
-    if (p_.nx % k != 0) continue;
-    set_chunks(k);
-    for (int w = 0; w < 2; ++w) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
-    CDFT_CUDA(cudaEventRecord(e0, stream));
-    for (int r = 0; r < reps; ++r) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
-    CDFT_CUDA(cudaEventRecord(e1, stream));
-    CDFT_CUDA(cudaEventSynchronize(e1));
-    float t = 0.0f;
-    CDFT_CUDA(cudaEventElapsedTime(&t, e0, e1));
-    const double per = (double)t / reps;
-    if (ms) ms[k - 1] = per;
-    if (best_ms == 0.0 || per < best_ms) {
-      best_ms = per;
-      best = k;
+  for (int v = 0; v < kPointwiseVariants; ++v) {
+    if (v > 0 && !pw1_) break;
+    set_pointwise(v);
+    for (int k = 1; k <= kMaxChunks; k *= 2) {
+      if (tune_chunks) {
+        if (p_.nx % k != 0) continue;
+        set_chunks(k);
+      } else if (k != chunks_) {
+        continue;
+      }
+      for (int w = 0; w < 2; ++w) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
+      CDFT_CUDA(cudaEventRecord(e0, stream));
+      for (int r = 0; r < reps; ++r) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
+      CDFT_CUDA(cudaEventRecord(e1, stream));
+      CDFT_CUDA(cudaEventSynchronize(e1));
+      float t = 0.0f;
+      CDFT_CUDA(cudaEventElapsedTime(&t, e0, e1));
+      const double per = (double)t / reps;
+      if (ms) ms[v * kMaxChunks + k - 1] = per;
+      if (best_ms == 0.0 || per < best_ms) {
+        best_ms = per;
+        best = k;
+        best_v = v;
+      }
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   timing_ = timing_was;
-  set_chunks(best);
+  if (tune_chunks) set_chunks(best);
+  set_pointwise(best_v);
+  if (variant) *variant = best_v;
   std::lock_guard<std::mutex> lock(g_tune_mu);
-  g_tune_chunks[tune_key_] = best;
-  return best;
+  if (tune_chunks) g_tune_chunks[tune_key_] = best;
+  g_tune_variant[tune_key_] = best_v;
+  return chunks_;
 }
+
+void Engine::set_pointwise(int v) {
+  if (v < 0 || v >= kPointwiseVariants) throw std::invalid_argument("pointwise variant: 0, 1 or 2");
+  if (v > 0 && !pw1_)
+    throw std::invalid_argument("pointwise variant: the one-species kernel needs a mixed-precision engine with one "
+                                "species and at most two interactions");
+  if (v != pw_variant_) ++generation_;
+  pw_variant_ = v;
+}
+
+int Engine::pw_grid() const { return (pw1_ && pw_variant_ > 0) ? grid_pw1_[pw_variant_ - 1] : grid_tma_; }
 
 void Engine::set_chunks(int k) {
   if (!fusable_) throw std::invalid_argument("plane chunks: the engine has no fused path");
@@ -608,7 +732,7 @@ void Engine::fused_middle(const double* rho, const double* vext, double* force, 
   const EvalParams& p = p_;
   const int K = chunked ? chunks_ : 1;
   const int per = p.nx / K;
-  const int gk = (grid_tma_ + K - 1) / K;
+  const int gk = (pw_grid() + K - 1) / K;
   const fft::cpx* q = static_cast<const fft::cpx*>(chan_k_);
   fft::cpx* pd = static_cast<fft::cpx*>(deriv_k_);
   float* chan_r = static_cast<float*>(chan_r_);
@@ -631,15 +755,7 @@ void Engine::fused_middle(const double* rho, const double* vext, double* force, 
     fused_plane_inv(plan_, p, q, chan_r, err_, ix0, per, tables_, st);
     if (K == 1) mark(4, st);
     const long long p0 = (long long)ix0 * p.ny * p.nz, pn = (long long)per * p.ny * p.nz;
-    with_kernels(true, [&](auto model_c, auto multi_c, auto r_c) {
-      constexpr int MD = decltype(model_c)::value;
-      constexpr bool MU = decltype(multi_c)::value;
-      using RT = typename decltype(r_c)::type;
-      if constexpr (std::is_same_v<RT, R>)
-        k_pointwise_tma<MD, MU, RT><<<dim3(gk, p.batch), kTmaTile, vext ? tma_smem_v_ : tma_smem_, st>>>(
-            p, chan_r, deriv_r, a, err_, p0, pn, k * gk, K * gk);
-    });
-    CDFT_CUDA(cudaGetLastError());
+    launch_pointwise_tma<float>(chan_r, deriv_r, a, p0, pn, k * gk, K * gk, gk, st);
     if (K == 1) mark(5, st);
     fused_plane_fwd_deriv(plan_, p, deriv_r, pd, err_, ix0, per, tables_, st);
   }
@@ -698,7 +814,7 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
     fused_forward(rho, stream);
     if constexpr (sizeof(R) == sizeof(float)) fused_middle<R>(rho, vext, force, !timing_run_, stream);
     const int K = timing_run_ ? 1 : chunks_;
-    FinalArgs fin{partials_, K * ((grid_tma_ + K - 1) / K), err_, scalars};
+    FinalArgs fin{partials_, K * ((pw_grid() + K - 1) / K), err_, scalars};
     fused_backward(force, ma, fin, stream);
     mark(10, stream);
     if (timing_run_) {
@@ -724,21 +840,19 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   a.mf_w = mf_w_;
   a.mean = mean_;
   a.dbar_out = dbar_;
-  const int pw_blocks = tma ? grid_tma_ : grid_pw_;
-  const dim3 gt(grid_tma_, p.batch), gp(grid_pw_, p.batch);
-  with_kernels(mixed, [&](auto model_c, auto multi_c, auto r_c) {
-    constexpr int MD = decltype(model_c)::value;
-    constexpr bool MU = decltype(multi_c)::value;
-    using RT = typename decltype(r_c)::type;
-    if constexpr (std::is_same_v<RT, R>) {
-      if (tma)
-        k_pointwise_tma<MD, MU, RT><<<gt, kTmaTile, vext ? tma_smem_v_ : tma_smem_, stream>>>(
-            p, chan_r, deriv_r, a, err_, 0, p.N, 0, grid_tma_);
-      else
-        k_pointwise<MD, MU, RT><<<gp, 256, 0, stream>>>(p, chan_r, deriv_r, a);
-    }
-  });
-  CDFT_CUDA(cudaGetLastError());
+  const int pw_blocks = tma ? pw_grid() : grid_pw_;
+  const dim3 gp(grid_pw_, p.batch);
+  if (tma) {
+    launch_pointwise_tma<R>(chan_r, deriv_r, a, 0, p.N, 0, pw_blocks, pw_blocks, stream);
+  } else {
+    with_kernels(mixed, [&](auto model_c, auto multi_c, auto r_c) {
+      constexpr int MD = decltype(model_c)::value;
+      constexpr bool MU = decltype(multi_c)::value;
+      using RT = typename decltype(r_c)::type;
+      if constexpr (std::is_same_v<RT, R>) k_pointwise<MD, MU, RT><<<gp, 256, 0, stream>>>(p, chan_r, deriv_r, a);
+    });
+    CDFT_CUDA(cudaGetLastError());
+  }
   mark(5, stream);
   // 5-7. back-convolution into the force
   if (fused) {

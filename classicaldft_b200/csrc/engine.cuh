@@ -21,6 +21,8 @@ namespace cdft {
 
 enum Precision : int { kFP64 = 0, kMixed = 1 };
 
+struct PointwiseArgs;
+
 struct InteractionSpec {
   int species_i = 0, species_j = 0;
   std::vector<double> weight_real;  // N doubles: cell weight * dV / N (mean_field.hpp:188)
@@ -100,8 +102,17 @@ class Engine {
   // created later in this process.  ms[k - 1]: time per evaluation of count
   // k (0 where not tried).  Returns the count chosen (the current one when
   // the engine has no fused path).  Synchronises the stream.
+  // The pointwise kernel variants (see pw_variant_) are tuned with the chunk
+  // counts: ms[v * kMaxChunks + k - 1]; *variant receives the variant kept.
+  static constexpr int kPointwiseVariants = 3;
   int autotune(const double* rho, const double* vext, const double* mu, cudaStream_t stream, int reps,
-               double* ms);
+               double* ms, int* variant);
+  // Pointwise kernel of the TMA path: 0 generic, 1 / 2 one-species (5 / 6
+  // CTAs per SM); std::invalid_argument where the variant does not exist.
+  void set_pointwise(int v);
+  int pointwise() const { return pw_variant_; }
+  bool pointwise_one_species() const { return pw1_; }
+  int pw_grid() const;
   int chunks() const { return chunks_; }
   // Changes whenever a setter changes what an evaluation launches (transform
   // path, plane chunks, stage timing): a captured graph of an evaluation is
@@ -191,6 +202,15 @@ class Engine {
   int grid_mean_ = 0;         // k_species_mean
   // grid_* are CTAs per problem: a launch has grid_* x B CTAs
   size_t tma_smem_ = 0, tma_smem_v_ = 0;
+  bool pw1_ = false;  // one species, <= 2 mean-field channels, mixed: k_pointwise1_tma exists
+  // pointwise kernel of the TMA path: 0 generic (k_pointwise_tma), 1 / 2 the
+  // one-species kernel sized for 5 / 6 CTAs per SM (grid grid_pw1_[v - 1])
+  int pw_variant_ = 0;
+  int grid_pw1_[2] = {0, 0};
+  size_t tma1_smem_ = 0, tma1_smem_v_ = 0;
+  template <typename R>
+  void launch_pointwise_tma(const R* chan, R* deriv, const PointwiseArgs& a, long long p0, long long pn, int blk0,
+                            int nblk, int grid, cudaStream_t st);
   void* fft_work_ = nullptr;
   size_t scratch_bytes_ = 0;
 

@@ -935,6 +935,181 @@ __global__ void __launch_bounds__(kTmaTile, 5) k_pointwise_tma(EvalParams p, con
   block_reduce_store<NT>(acc, p.n_terms, a.partials);
 }
 
+// One species with NMF (0..2) mean-field channels, mixed precision: the TMA
+// ring of k_pointwise_tma with every layout size a compile-time constant, no
+// species or interaction loops and no runtime channel selection (the common
+// case of every benchmark workload).  Same arithmetic as point_body's
+// one-species branch, so the results equal the generic kernel's.
+template <int NMF, bool HAS_V, bool TENSOR>
+__host__ __device__ constexpr int tma1_stage_bytes() {
+  return (Lay<false, TENSOR>::NFMT + NMF) * kTmaTile * 4 + kTmaTile * 8 * (HAS_V ? 2 : 1);
+}
+
+// MINB: the CTAs per SM the register allocation is sized for (5: 96
+// registers, no spills; 6: 80 registers with a few spills) -- the
+// autotuner picks one per engine shape.
+template <int MODEL, int NMF, bool HAS_V, int MINB>
+__global__ void __launch_bounds__(kTmaTile, MINB) k_pointwise1_tma(EvalParams p, const float* __restrict__ chan,
+                                                             float* __restrict__ deriv, PointwiseArgs a_all,
+                                                             int* err, long long p0, long long pn, int blk0,
+                                                             int nblk) {
+  constexpr bool TENSOR = model_has_tensor(MODEL);
+  using L = Lay<false, TENSOR>;
+  constexpr int NF = L::NFMT;
+  constexpr int NIN = NF + NMF;                      // float segments per tile
+  constexpr int RHO_OFF = NIN * kTmaTile * 4;
+  constexpr int V_OFF = RHO_OFF + kTmaTile * 8;
+  constexpr int STAGE = tma1_stage_bytes<NMF, HAS_V, TENSOR>();
+  constexpr int NT = 5;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bars[kTmaStages];
+  __shared__ double s_off[kMaxChannels];
+  __shared__ double s_dbar[NF];
+  __shared__ int s_fail;
+  __shared__ int s_out[kTmaStages];
+  __shared__ long long s_issued[kTmaStages];
+  PointwiseArgs a = batch_slice(p, a_all, blockIdx.y);
+  a.partials = a_all.partials + ((long long)blockIdx.y * nblk + blk0) * p.n_terms;
+  chan += (long long)blockIdx.y * p.n_chan * p.N;
+  deriv += (long long)blockIdx.y * NF * p.N;
+  const long long N = p.N;
+  const long long ntiles = (pn + kTmaTile - 1) / kTmaTile;
+  const long long mine = (blockIdx.x < ntiles) ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int st = 0; st < kTmaStages; ++st) {
+      mbar_init(&bars[st], 1);
+      s_out[st] = 0;
+      s_issued[st] = -1;
+    }
+    s_fail = 0;
+    fence_mbar_init();
+  }
+  split_prologue<MODEL, false>(p, a, s_off, s_dbar, blk0 + blockIdx.x == 0);
+  __syncthreads();
+
+  auto issue = [&](long long i) {  // local tile i -> stage i % kTmaStages
+    const int st = (int)(i % kTmaStages);
+    const long long start = p0 + (blockIdx.x + i * gridDim.x) * kTmaTile;
+    const long long cnt = (p0 + pn - start) < kTmaTile ? (p0 + pn - start) : kTmaTile;
+    const uint32_t cb = (uint32_t)(cnt * 4), db = (uint32_t)(cnt * 8);
+    unsigned char* base = smem + (size_t)st * STAGE;
+    s_issued[st] = i;
+    mbar_arrive_expect_tx(&bars[st], cb * NIN + db * (HAS_V ? 2 : 1));
+#pragma unroll
+    for (int q = 0; q < NIN; ++q) bulk_copy_g2s(base + q * kTmaTile * 4, chan + q * N + start, cb, &bars[st]);
+    bulk_copy_g2s(base + RHO_OFF, a.rho + start, db, &bars[st]);
+    if constexpr (HAS_V) bulk_copy_g2s(base + V_OFF, a.vext + start, db, &bars[st]);
+  };
+  if (tid == 0)
+    for (long long i = 0; i < mine && i < kTmaStages; ++i) issue(i);
+
+  // the split offsets stay in shared memory and the model constants in the
+  // parameter bank: held in registers they would spill
+  const double* off = s_off;
+  const double* dbar = s_dbar;
+  double acc[NT];
+#pragma unroll
+  for (int t = 0; t < NT; ++t) acc[t] = 0.0;
+  constexpr int kWarps = kTmaTile / 32;
+  const int lane = tid & 31;
+  volatile int* fail = &s_fail;
+  int st = 0;
+  uint32_t par = 0;
+  long long idx = p0 + (long long)blockIdx.x * kTmaTile + tid;
+  const long long idx_step = (long long)gridDim.x * kTmaTile, idx_end = p0 + pn;
+  for (long long i = 0; i < mine; ++i, idx += idx_step) {
+    if (*fail) break;
+    if (!mbar_wait_bounded(&bars[st], par, kWaitLimit)) {
+      *fail = 1;
+      break;
+    }
+    if (idx < idx_end) {
+      const unsigned char* base = smem + (size_t)st * STAGE;
+      const float* cs = reinterpret_cast<const float*>(base) + tid;
+      double n[NIN];
+#pragma unroll
+      for (int c = 0; c < NIN; ++c) n[c] = (double)cs[c * kTmaTile] + off[c];
+      const double r = reinterpret_cast<const double*>(base + RHO_OFF)[tid];
+      const double v = HAS_V ? reinterpret_cast<const double*>(base + V_OFF)[tid] : 0.0;
+      Measures<double> m;
+      m.eta = n[L::ETA];
+      m.n2 = n[L::N2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) m.v1[c] = n[L::V1 + c];
+      if constexpr (TENSOR) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) m.t[c] = n[L::T + c];
+        m.t[5] = m.n2 - m.t[0] - m.t[3];
+      } else {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) m.t[c] = 0.0;
+      }
+      double phi = 0.0;
+      MeasureDerivs<double> dm;
+      double D[NF];
+      if (fmt_phi_dphi<MODEL, double, true>(p.A, p.B, m, phi, dm, p.inv4piR2[0], p.inv4piR[0])) {
+        const double dzz = TENSOR ? dm.d_t[5] : 0.0;
+        D[L::ETA] = dm.d_eta;
+        D[L::N2] = dm.d_n2 + dzz;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) D[L::V1 + c] = dm.d_v1[c];
+        if constexpr (TENSOR) {
+          D[L::T + 0] = dm.d_t[0] - dzz;
+          D[L::T + 1] = 2.0 * dm.d_t[1];
+          D[L::T + 2] = 2.0 * dm.d_t[2];
+          D[L::T + 3] = dm.d_t[3] - dzz;
+          D[L::T + 4] = 2.0 * dm.d_t[4];
+        }
+      } else {
+        phi = 0.0;
+#pragma unroll
+        for (int c = 0; c < NF; ++c) D[c] = 0.0;
+      }
+      acc[kTermHS] += phi;
+#pragma unroll
+      for (int c = 0; c < NF; ++c) __stcs(deriv + c * N + idx, (float)(D[c] - dbar[c]));
+      const double lr = log(r < 1e-300 ? 1e-300 : r);
+      acc[kTermId] += r * (lr - 1.0);
+      acc[kTermExt] += r * v;
+      acc[kTermN0] += r;
+      double f0 = lr + v;  // -mu dV is added by k_epilogue
+#pragma unroll
+      for (int q = 0; q < NMF; ++q) {
+        acc[kTermMF] += 0.5 * r * n[NF + q];
+        f0 += n[NF + q];
+      }
+      __stcs(a.force + idx, f0 * p.dv);
+    }
+    // this warp is done reading stage st; the last warp out refills it
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence_block();
+      if (atomicAdd(&s_out[st], 1) == kWarps - 1) {
+        s_out[st] = 0;
+        if (i + kTmaStages < mine) {
+          fence_proxy_async();
+          issue(i + kTmaStages);
+        }
+      }
+    }
+    if (++st == kTmaStages) {
+      st = 0;
+      par ^= 1u;
+    }
+  }
+  __syncthreads();
+  if (s_fail) {
+    if (tid == 0) {
+      *err = 1;
+      for (int q = 0; q < kTmaStages; ++q)
+        if (s_issued[q] >= 0) mbar_wait_bounded(&bars[q], (uint32_t)((s_issued[q] / kTmaStages) & 1), kWaitLimit);
+    }
+    __syncthreads();
+  }
+  block_reduce_store<NT>(acc, p.n_terms, a.partials);
+}
+
 // ---- exact Hessian-vector product ---------------------------------------
 
 struct HvpArgs {

@@ -359,6 +359,37 @@ class Engine:
         self.info = self._query_info()
         return chunks.value, {k + 1: ms[k] for k in range(8) if ms[k] > 0.0}
 
+    def autotune_ex(self, rho_ptr: int, vext_ptr: int = 0, mu=None, stream: int = 0, reps: int = 5):
+        """Time every (plane-chunk count, pointwise variant) pair and keep the
+        fastest.  Returns ((chunks, variant), {(variant, count): ms})."""
+        choice = (ctypes.c_int * 2)()
+        ms = (ctypes.c_double * (3 * 8))()
+        mu_arr = None
+        if mu is not None:
+            mu_arr = (ctypes.c_double * (self.batch * self.S))(*[float(m) for m in mu])
+        _lib.check(_lib.lib().cdft_engine_autotune_ex(self.handle, ctypes.c_void_p(rho_ptr),
+                                                      ctypes.c_void_p(vext_ptr or None), mu_arr,
+                                                      ctypes.c_void_p(stream or None), int(reps), choice, ms))
+        self.info = self._query_info()
+        return (choice[0], choice[1]), {(v, k + 1): ms[v * 8 + k] for v in range(3) for k in range(8)
+                                        if ms[v * 8 + k] > 0.0}
+
+    @property
+    def pointwise(self) -> int:
+        """Pointwise kernel variant: 0 generic, 1 / 2 one-species (5 / 6 CTAs per SM)."""
+        v, a = ctypes.c_int(), ctypes.c_int()
+        _lib.check(_lib.lib().cdft_engine_pointwise(self.handle, ctypes.byref(v), ctypes.byref(a)))
+        return v.value
+
+    @property
+    def pointwise_variants(self) -> list:
+        v, a = ctypes.c_int(), ctypes.c_int()
+        _lib.check(_lib.lib().cdft_engine_pointwise(self.handle, ctypes.byref(v), ctypes.byref(a)))
+        return [0, 1, 2] if a.value else [0]
+
+    def set_pointwise(self, variant: int):
+        _lib.check(_lib.lib().cdft_engine_set_pointwise(self.handle, int(variant)))
+
     def stage_timing(self, on: bool = True):
         """Record CUDA events between the evaluation stages (synchronises each evaluation)."""
         _lib.check(_lib.lib().cdft_engine_stage_timing(self.handle, 1 if on else 0))

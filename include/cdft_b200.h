@@ -584,6 +584,21 @@ CDFT_API int cdft_engine_set_plane_chunks(cdft_engine* engine, int chunks);
 CDFT_API int cdft_engine_autotune(cdft_engine* engine, const double* rho, const double* vext, const double* mu,
                                   void* stream, int reps, int* chunks, double* ms);
 
+/* The pointwise kernel of the TMA-staged path (no reference counterpart):
+ * 0 the generic kernel; 1 and 2 the kernel specialised for one species and
+ * at most two interactions (mixed precision), with its registers sized for
+ * 5 or 6 CTAs per SM.  Every variant gives the same results up to the
+ * rounding of the pointwise FP64 arithmetic.  available (out): 1 where 1 and
+ * 2 exist.  cdft_engine_autotune times every variant with every plane-chunk
+ * count and keeps the fastest pair; cdft_engine_autotune_ex also returns the
+ * whole table: ms[v * CDFT_MAX_PLANE_CHUNKS + k - 1] for variant v and k
+ * chunks (0 where not tried), choice = {chunks, variant}. */
+#define CDFT_POINTWISE_VARIANTS 3
+CDFT_API int cdft_engine_set_pointwise(cdft_engine* engine, int variant);
+CDFT_API int cdft_engine_pointwise(const cdft_engine* engine, int* variant, int* available);
+CDFT_API int cdft_engine_autotune_ex(cdft_engine* engine, const double* rho, const double* vext, const double* mu,
+                                     void* stream, int reps, int choice[2], double* ms);
+
 /* Step graphs (no reference counterpart; execution mode, process-wide): the
  * FIRE minimisers (cdft_minimize, cdft_minimize_batch, the saddle search's
  * FIRE) capture one step (the FIRE update and the evaluation) as a CUDA graph

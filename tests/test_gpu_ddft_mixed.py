@@ -56,6 +56,34 @@ def test_device_loop_matches_the_host_loop():
     assert out[True][1] == out[False][1]
 
 
+@pytest.mark.parametrize("shape", [(64, 64, 64), (128, 64, 64)])
+def test_device_loop_with_forked_plane_chunks(shape):
+    """A mixed-precision engine whose evaluation forks its middle stages onto
+    four plane-chunk streams: the step graph (each part captured on its own
+    and embedded as a child graph of the conditional loop) matches the host
+    loop bit for bit, with refinement by an FP64 engine."""
+    kw = dict(inters=[(0, 0, 1.0, 1.0, 2.5)], kT=0.8)
+    prm = Problem(shape, 0.125, [1.0], "WhiteBearII", precision=cd.MIXED, **kw)
+    pr64 = Problem(shape, 0.125, [1.0], "WhiteBearII", precision=cd.FP64, **kw)
+    assert prm.weights.engine.info["kernels_per_eval"] == 16  # four chunks
+    rng = np.random.default_rng(3)
+    rho0 = 0.35 * (1.0 + 0.01 * rng.uniform(-1.0, 1.0, int(np.prod(shape))))
+    out = {}
+    try:
+        for on in (True, False):
+            cd.set_step_graphs(on)
+            cfg = cd.StepConfig(dt=1e-4, fp_tolerance=1e-8)
+            r = rho0.copy()
+            for _ in range(3):
+                r, e, dt = cd.integrating_factor_step(r, prm.weights, cfg, 0.0, refine=pr64.weights)
+                assert cd.ddft_last_step(prm.weights)["device_loop"] == on
+            out[on] = (r, e, dt)
+    finally:
+        cd.set_step_graphs(True)
+    assert np.array_equal(out[True][0], out[False][0])
+    assert out[True][1:] == out[False][1:]
+
+
 def test_mixed_with_fp64_refinement_tracks_fp64():
     pr64, prm = problems()
     rho0 = start_density()

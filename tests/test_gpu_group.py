@@ -80,9 +80,12 @@ def test_group_graphs_and_members_alone_are_bitwise_equal():
 def test_mixed_group_with_refinement_matches_fp64():
     probs = setup()
     probs_m = setup(cd.MIXED)
-    tight = dict(FIRE, force_tolerance=1e-13, max_steps=12000)
-    f64 = group(cd.Minimizer(fire=cd.Fire(**tight)), probs)
-    mix = group(cd.Minimizer(fire=cd.Fire(**tight), refine_switch=1e3), probs_m, precision=cd.MIXED, refine=True)
+    # the rms-force convergence test (the energy monitor leaves soft modes
+    # unresolved at the 1e-8 level)
+    tight = dict(FIRE, force_tolerance=1e-12, max_steps=20000)
+    f64 = group(cd.Minimizer(fire=cd.Fire(**tight), use_monitor=False), probs)
+    mix = group(cd.Minimizer(fire=cd.Fire(**tight), refine_switch=1e3, use_monitor=False), probs_m,
+                precision=cd.MIXED, refine=True)
     for a, b in zip(f64, mix):
         for k in range(PER):
             assert a[k].converged and b[k].converged
