@@ -536,25 +536,30 @@ def config_ddft(cd, torch, n_steps=2000):
     w64 = cd.make_weights(cd.WhiteBearII(), model, cd.FP64)
     wmx = cd.make_weights(cd.WhiteBearII(), model, cd.MIXED)
     runs, times = {}, {}
-    for label, w, ref in (("fp64", w64, None), ("mixed_refined", wmx, w64)):
+    # mixed: FP32 transforms, FP64 Phi and sums; mixed_fp64_energy: the same
+    # steps with each step's final compute (its energy and forces) in FP64
+    for label, w, ref in (("fp64", w64, None), ("mixed", wmx, None), ("mixed_fp64_energy", wmx, w64)):
         sim = cd.Simulation(step=cd.StepConfig(dt=1e-4, dt_max=1e-4, fp_tolerance=1e-8), n_steps=n_steps,
-                            snapshot_interval=100, log_interval=100, refine=ref)
+                            snapshot_interval=100, log_interval=100, refine=ref, refine_iterations=0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         runs[label] = sim.run([rho0], w, 0.0)
         torch.cuda.synchronize()
         times[label] = time.perf_counter() - t0
-    per = []
-    for a, b in zip(runs["fp64"]["snapshots"], runs["mixed_refined"]["snapshots"]):
-        per.append([a.step, float(np.max(np.abs(a.densities[0] - b.densities[0]))),
-                    abs(a.energy - b.energy) / abs(a.energy)])
+    out = {"workload": f"128^3 LJ fluid, {n_steps} IF steps at dt = 1e-4, fp_tolerance 1e-8"}
+    for label in ("fp64", "mixed", "mixed_fp64_energy"):
+        out[label] = {"s": times[label], "steps_per_s": n_steps / times[label]}
+    for label in ("mixed", "mixed_fp64_energy"):
+        per = []
+        for a, b in zip(runs["fp64"]["snapshots"], runs[label]["snapshots"]):
+            per.append([a.step, float(np.max(np.abs(a.densities[0] - b.densities[0]))),
+                        abs(a.energy - b.energy) / abs(a.energy)])
+        out[label].update({"vs_fp64_per_100_steps": {"columns": ["step", "max_drho", "dF_over_F"], "rows": per},
+                           "max_drho": max(r[1] for r in per), "max_dF_over_F": max(r[2] for r in per),
+                           "speedup_vs_fp64": times["fp64"] / times[label]})
     for w in (w64, wmx):
         w.engine.close()
-    return {"workload": f"128^3 LJ fluid, {n_steps} IF steps at dt = 1e-4, fp_tolerance 1e-8",
-            "fp64_s": times["fp64"], "mixed_refined_s": times["mixed_refined"],
-            "fp64_steps_per_s": n_steps / times["fp64"], "mixed_refined_steps_per_s": n_steps / times["mixed_refined"],
-            "per_100_steps": {"columns": ["step", "max_drho", "dF_over_F"], "rows": per},
-            "max_drho": max(r[1] for r in per), "max_dF_over_F": max(r[2] for r in per)}
+    return out
 
 
 def config_nucleus(cd, torch):
@@ -680,9 +685,11 @@ def run_ours(args, ws, rank, local, dist):
     if args.plane_chunks:
         eng.set_plane_chunks(args.plane_chunks)
     elif eng.transforms == "fused":
-        # the engine's autotuner picks the plane-chunk count on this state
-        k, ms = eng.autotune(rho.data_ptr(), mu=[0.0], reps=10)
-        tuned = {"chosen": k, "ms_per_eval": {str(c): round(t, 5) for c, t in ms.items()}}
+        # the engine's autotuner picks the plane-chunk count and the pointwise
+        # kernel variant on this state
+        (k, v), ms = eng.autotune_ex(rho.data_ptr(), mu=[0.0], reps=10)
+        tuned = {"chosen": {"plane_chunks": k, "pointwise_variant": v},
+                 "ms_per_eval": {f"v{vv}_k{c}": round(t, 5) for (vv, c), t in ms.items()}}
     force = torch.empty_like(rho)
     scal = torch.zeros(10, dtype=torch.float64, device=dev)
     flush = L2Flush(torch, dev)

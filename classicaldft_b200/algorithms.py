@@ -397,12 +397,12 @@ def _set_ddft_refine(weights: Weights, refine, refine_iterations):
 
 
 def integrating_factor_step(density, weights: Weights, config: StepConfig, chemical_potential=0.0, refine=None,
-                            refine_iterations=2):
+                            refine_iterations=1):
     """dynamics.hpp:333-401: returns (density, energy, dt_used); config.dt is
     divided by 10 on restarts, as in the reference.  ``refine``: FP64 Weights
-    of the same model that run ``refine_iterations`` fixed-point iterations
-    after the step has converged with ``weights`` and give its final energy
-    (mixed-precision defect correction)."""
+    of the same model that run ``refine_iterations`` (>= 0) fixed-point
+    iterations after the step has converged with ``weights`` and give its
+    final energy (mixed-precision defect correction)."""
     torch = _torch()
     d, host = _dev(density)
     if not host:
@@ -505,7 +505,7 @@ class Simulation:
     stop_condition: object = None
     # FP64 defect correction of a mixed-precision run (see integrating_factor_step)
     refine: object = None
-    refine_iterations: int = 2
+    refine_iterations: int = 1
 
     def run(self, densities, weights: Weights, chemical_potential=0.0):
         torch = _torch()

@@ -1402,7 +1402,7 @@ void Drivers::set_ddft_refine(Engine* refine, int iterations) {
     if (refine->precision() != kFP64) throw Error(-1, "ddft: the refine engine must be FP64");
     if (refine->points() != N_ || refine->species() != 1 || refine->batch() != 1)
       throw Error(-1, "ddft: the refine engine must have the driver's grid, one species and batch 1");
-    if (iterations < 1) throw Error(-1, "ddft: refine iterations must be >= 1");
+    if (iterations < 0) throw Error(-1, "ddft: refine iterations must be >= 0");
   }
   ddft_refine_ = refine;
   ddft_refine_iterations_ = refine ? iterations : 0;

@@ -151,10 +151,10 @@ class Drivers {
   static constexpr int kMaxRestarts = 64;
   double ddft_step(DDFTConfig& cfg, double* rho, cudaStream_t stream, int* fp_iterations = nullptr);
   // FP64 defect correction of a mixed-precision IF step: after the fixed
-  // point has converged with this driver's engine, `iterations` more
+  // point has converged with this driver's engine, `iterations` (>= 0) more
   // iterations use the FP64 `refine` engine (same model), which also gives
-  // the step's final forces and energy.  Null clears it.  Applies to
-  // ddft_step and ddft_run.
+  // the step's final forces and energy (0: only that).  Null clears it.
+  // Applies to ddft_step and ddft_run.
   void set_ddft_refine(Engine* refine, int iterations);
   // Facts of the last IF step: fixed-point iterations, restarts, status
   // (1 converged, 2 gave up after kMaxRestarts), 1 if the loop ran as a

@@ -304,9 +304,10 @@ CDFT_API int cdft_ddft_step(cdft_engine* engine, cdft_ddft_config* cfg, double c
 
 /* FP64 defect correction of the integrating-factor steps of a mixed-
  * precision engine (cdft_ddft_step, cdft_ddft_run, cdft_ddft_simulate): once
- * a step's fixed point has converged with `engine`, `iterations` (>= 1) more
+ * a step's fixed point has converged with `engine`, `iterations` (>= 0) more
  * fixed-point iterations run with the FP64 engine `refine` (same grid and
- * model, batch 1), which also gives the step's final forces and energy.
+ * model, batch 1), which also gives the step's final forces and energy (with
+ * 0 iterations only those).
  * refine NULL clears it.  No reference counterpart (the reference has one
  * precision). */
 CDFT_API int cdft_ddft_set_refine(cdft_engine* engine, cdft_engine* refine, int iterations);

@@ -348,6 +348,11 @@ struct Minimizer {
   int check_interval = 25;
   const functionals::Weights* refine = nullptr;  // optional FP64 defect correction
   double refine_switch = 10.0;
+  // true: the energy monitor (minimization.hpp:431-434); false: the rms force (fire.hpp:162)
+  bool use_monitor = true;
+  // V_ext of every evaluation (N values), or empty; the reference's
+  // Minimizer has none (init.hpp:28-58 drops it), a wall needs it
+  std::vector<double> external_field;
 
   Result run(const functionals::Weights& w, const std::vector<double>& rho0, int mode, double mu, double mass) const {
     cdft_minimizer_config cfg{};
@@ -359,9 +364,11 @@ struct Minimizer {
     cfg.homogeneous_boundary = use_homogeneous_boundary ? 1 : 0;
     cfg.chemical_potential = mu;
     cfg.target_mass = mass;
-    cfg.use_monitor = 1;
+    cfg.use_monitor = use_monitor ? 1 : 0;
     cfg.check_interval = check_interval;
     DeviceVector d(rho0);
+    DeviceVector vx(external_field.empty() ? std::vector<double>(1, 0.0) : external_field);
+    cfg.external_field = external_field.empty() ? nullptr : vx.get();
     cdft_minimizer_result res{};
     check(cdft_minimize(w.engine(), &cfg, d.get(), nullptr, refine ? refine->engine() : nullptr, refine_switch, &res,
                         nullptr));
