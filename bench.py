@@ -687,9 +687,9 @@ def run_ours(args, ws, rank, local, dist):
     elif eng.transforms == "fused":
         # the engine's autotuner picks the plane-chunk count and the pointwise
         # kernel variant on this state
-        (k, v), ms = eng.autotune_ex(rho.data_ptr(), mu=[0.0], reps=10)
-        tuned = {"chosen": {"plane_chunks": k, "pointwise_variant": v},
-                 "ms_per_eval": {f"v{vv}_k{c}": round(t, 5) for (vv, c), t in ms.items()}}
+        (k, v, tq), ms = eng.autotune_ex(rho.data_ptr(), mu=[0.0], reps=10)
+        tuned = {"chosen": {"plane_chunks": k, "pointwise_variant": v, "column_tile": tq},
+                 "ms_per_eval": {f"t{tt}_v{vv}_k{c}": round(t, 5) for (tt, vv, c), t in ms.items()}}
     force = torch.empty_like(rho)
     scal = torch.zeros(10, dtype=torch.float64, device=dev)
     flush = L2Flush(torch, dev)

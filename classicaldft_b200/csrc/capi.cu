@@ -343,26 +343,43 @@ int cdft_engine_autotune(cdft_engine* engine, const double* rho, const double* v
   return guarded([&] {
     if (!engine || !rho) throw std::invalid_argument("engine and rho are required");
     if (reps < 1) throw std::invalid_argument("autotune: reps must be positive");
-    double all[cdft::Engine::kPointwiseVariants * cdft::Engine::kMaxChunks];
-    int v = 0;
-    const int k = engine->impl->autotune(rho, vext, mu, static_cast<cudaStream_t>(stream), reps, all, &v);
+    double all[2 * cdft::Engine::kPointwiseVariants * cdft::Engine::kMaxChunks];
+    int v = 0, tq = 16;
+    const int k = engine->impl->autotune(rho, vext, mu, static_cast<cudaStream_t>(stream), reps, all, &v, &tq);
     if (chunks) *chunks = k;
+    const int ti = tq == 32 ? 1 : 0;
     if (ms)
-      for (int c = 0; c < cdft::Engine::kMaxChunks; ++c) ms[c] = all[v * cdft::Engine::kMaxChunks + c];
+      for (int c = 0; c < cdft::Engine::kMaxChunks; ++c)
+        ms[c] = all[(ti * cdft::Engine::kPointwiseVariants + v) * cdft::Engine::kMaxChunks + c];
   });
 }
 
 int cdft_engine_autotune_ex(cdft_engine* engine, const double* rho, const double* vext, const double* mu,
-                            void* stream, int reps, int choice[2], double* ms) {
+                            void* stream, int reps, int choice[3], double* ms) {
   return guarded([&] {
     if (!engine || !rho) throw std::invalid_argument("engine and rho are required");
     if (reps < 1) throw std::invalid_argument("autotune: reps must be positive");
-    int v = 0;
-    const int k = engine->impl->autotune(rho, vext, mu, static_cast<cudaStream_t>(stream), reps, ms, &v);
+    int v = 0, tq = 0;
+    const int k = engine->impl->autotune(rho, vext, mu, static_cast<cudaStream_t>(stream), reps, ms, &v, &tq);
     if (choice) {
       choice[0] = k;
       choice[1] = v;
+      choice[2] = tq;
     }
+  });
+}
+
+int cdft_engine_set_column_tile(cdft_engine* engine, int tile) {
+  return guarded([&] {
+    if (!engine) throw std::invalid_argument("engine is NULL");
+    engine->impl->set_col_tile(tile);
+  });
+}
+
+int cdft_engine_column_tile(const cdft_engine* engine, int* tile) {
+  return guarded([&] {
+    if (!engine || !tile) throw std::invalid_argument("engine and tile are required");
+    *tile = engine->impl->col_tile();
   });
 }
 

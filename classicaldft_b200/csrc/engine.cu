@@ -19,6 +19,7 @@ namespace {
 std::mutex g_tune_mu;
 std::map<std::string, int> g_tune_chunks;
 std::map<std::string, int> g_tune_variant;
+std::map<std::string, int> g_tune_tile;
 }  // namespace
 
 namespace {
@@ -453,6 +454,8 @@ void Engine::setup_fused() {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     const auto it = g_tune_chunks.find(tune_key_);
     if (it != g_tune_chunks.end()) chunks_ = it->second;
+    const auto tt = g_tune_tile.find(tune_key_);
+    if (tt != g_tune_tile.end()) fused_plan_set_tile(p, &plan_, tt->second);
   }
   ensure_chunk_streams(chunks_);
 }
@@ -473,11 +476,14 @@ void Engine::ensure_chunk_streams(int k) {
 // Every (plane-chunk count, pointwise variant) pair the engine has, timed on
 // the caller's state; the fastest is kept and cached for the shape.
 int Engine::autotune(const double* rho, const double* vext, const double* mu, cudaStream_t stream, int reps,
-                     double* ms, int* variant) {
+                     double* ms, int* variant, int* tile) {
+  constexpr int kTiles = 2;  // column tile widths 16, 32
   if (ms)
-    for (int k = 0; k < kPointwiseVariants * kMaxChunks; ++k) ms[k] = 0.0;
+    for (int k = 0; k < kPointwiseVariants * kMaxChunks * kTiles; ++k) ms[k] = 0.0;
   if (variant) *variant = pw_variant_;
+  if (tile) *tile = col_tile();
   const bool tune_chunks = fusable_ && fused_;
+  const bool tune_tiles = tune_chunks && p_.S > 1;
   if (!tune_chunks && !pw1_) return chunks_;
   if (!rho) throw std::invalid_argument("autotune: rho is required");
   reps = std::max(reps, 1);
@@ -488,45 +494,68 @@ int Engine::autotune(const double* rho, const double* vext, const double* mu, cu
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   CDFT_CUDA(cudaEventCreate(&e0));
   CDFT_CUDA(cudaEventCreate(&e1));
-  int best = chunks_, best_v = pw_variant_;
+  int best = chunks_, best_v = pw_variant_, best_t = col_tile();
   double best_ms = 0.0;
-  for (int v = 0; v < kPointwiseVariants; ++v) {
-    if (v > 0 && !pw1_) break;
-    set_pointwise(v);
-    for (int k = 1; k <= kMaxChunks; k *= 2) {
-      if (tune_chunks) {
-        if (p_.nx % k != 0) continue;
-        set_chunks(k);
-      } else if (k != chunks_) {
-        continue;
-      }
-      for (int w = 0; w < 2; ++w) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
-      CDFT_CUDA(cudaEventRecord(e0, stream));
-      for (int r = 0; r < reps; ++r) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
-      CDFT_CUDA(cudaEventRecord(e1, stream));
-      CDFT_CUDA(cudaEventSynchronize(e1));
-      float t = 0.0f;
-      CDFT_CUDA(cudaEventElapsedTime(&t, e0, e1));
-      const double per = (double)t / reps;
-      if (ms) ms[v * kMaxChunks + k - 1] = per;
-      if (best_ms == 0.0 || per < best_ms) {
-        best_ms = per;
-        best = k;
-        best_v = v;
+  for (int ti = 0; ti < kTiles; ++ti) {
+    const int tq = 16 << ti;
+    if (tune_tiles) {
+      if (!fused_plan_set_tile(p_, &plan_, tq)) continue;
+      ++generation_;
+    } else if (tq != best_t) {
+      continue;
+    }
+    for (int v = 0; v < kPointwiseVariants; ++v) {
+      if (v > 0 && !pw1_) break;
+      set_pointwise(v);
+      for (int k = 1; k <= kMaxChunks; k *= 2) {
+        if (tune_chunks) {
+          if (p_.nx % k != 0) continue;
+          set_chunks(k);
+        } else if (k != chunks_) {
+          continue;
+        }
+        for (int w = 0; w < 2; ++w) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
+        CDFT_CUDA(cudaEventRecord(e0, stream));
+        for (int r = 0; r < reps; ++r) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
+        CDFT_CUDA(cudaEventRecord(e1, stream));
+        CDFT_CUDA(cudaEventSynchronize(e1));
+        float t = 0.0f;
+        CDFT_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        const double per = (double)t / reps;
+        if (ms) ms[(ti * kPointwiseVariants + v) * kMaxChunks + k - 1] = per;
+        if (best_ms == 0.0 || per < best_ms) {
+          best_ms = per;
+          best = k;
+          best_v = v;
+          best_t = tq;
+        }
       }
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   timing_ = timing_was;
+  if (tune_tiles) set_col_tile(best_t);
   if (tune_chunks) set_chunks(best);
   set_pointwise(best_v);
   if (variant) *variant = best_v;
+  if (tile) *tile = col_tile();
   std::lock_guard<std::mutex> lock(g_tune_mu);
   if (tune_chunks) g_tune_chunks[tune_key_] = best;
+  if (tune_tiles) g_tune_tile[tune_key_] = best_t;
   g_tune_variant[tune_key_] = best_v;
   return chunks_;
 }
+
+void Engine::set_col_tile(int tq) {
+  if (!fusable_) throw std::invalid_argument("column tile: the engine has no fused path");
+  const int old = plan_.tq;
+  if (!fused_plan_set_tile(p_, &plan_, tq))
+    throw std::invalid_argument("column tile: 16 (any engine) or 32 (several species, where the spectra fit)");
+  if (plan_.tq != old) ++generation_;
+}
+
+int Engine::col_tile() const { return fusable_ ? plan_.tq : 0; }
 
 void Engine::set_pointwise(int v) {
   if (v < 0 || v >= kPointwiseVariants) throw std::invalid_argument("pointwise variant: 0, 1 or 2");

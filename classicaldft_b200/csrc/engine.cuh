@@ -104,9 +104,15 @@ class Engine {
   // the engine has no fused path).  Synchronises the stream.
   // The pointwise kernel variants (see pw_variant_) are tuned with the chunk
   // counts: ms[v * kMaxChunks + k - 1]; *variant receives the variant kept.
+  // Several species also tune the column tile width (16, 32):
+  // ms[(tile_index * kPointwiseVariants + v) * kMaxChunks + k - 1].
   static constexpr int kPointwiseVariants = 3;
   int autotune(const double* rho, const double* vext, const double* mu, cudaStream_t stream, int reps,
-               double* ms, int* variant);
+               double* ms, int* variant, int* tile = nullptr);
+  // Column tile width of the fused path's column passes (16, or 32 for
+  // several species where their spectra fit); std::invalid_argument otherwise.
+  void set_col_tile(int tq);
+  int col_tile() const;
   // Pointwise kernel of the TMA path: 0 generic, 1 / 2 one-species (5 / 6
   // CTAs per SM); std::invalid_argument where the variant does not exist.
   void set_pointwise(int v);

@@ -84,8 +84,8 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan) {
     f.colf_smem = rk::rcol1_smem(p.nx, f.tq);
     f.colb_smem = rk::rcol1_smem_bwd(p.nx, f.tq);
   } else {
-    f.tq = 32;
-    if (rk::rcol_smem(p.nx, f.tq, p.S) > kSmemCap) f.tq = 16;
+    f.tq32 = rk::rcol_smem(p.nx, 32, p.S) <= kSmemCap;
+    f.tq = f.tq32 ? 32 : 16;
     f.colf_smem = rk::rcol_smem(p.nx, f.tq, p.S);
     f.colb_smem = f.colf_smem;
   }
@@ -103,21 +103,37 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan) {
   });
   with_len(p.nx, [&](auto xc) {
     constexpr int NX = decltype(xc)::value;
-    with_tq(f.tq, [&](auto qc) {
-      constexpr int TQ = decltype(qc)::value;
-      with_layout(p, [&](auto mc, auto tc) {
-        constexpr bool MU = decltype(mc)::value, TE = decltype(tc)::value;
-        if constexpr (MU) {
-          allow_smem(rk::k_rcol_fwd<NX, TQ, MU, TE>, f.colf_smem);
-          allow_smem(rk::k_rcol_bwd<NX, TQ, MU, TE>, f.colb_smem);
-        } else if constexpr (TQ == 16) {  // one species: 16-column tiles only
-          allow_smem(rk::k_rcol_fwd1<NX, TQ, TE>, f.colf_smem);
-          allow_smem(rk::k_rcol_bwd1<NX, TQ, TE>, f.colb_smem);
-        }
+    // every tile width the plan may switch to (several species: 16 and,
+    // where it fits, 32)
+    for (int tq : {16, 32}) {
+      if (tq != f.tq && !(p.S > 1 && tq == 16) && !(tq == 32 && f.tq32)) continue;
+      const size_t sm = p.S > 1 ? rk::rcol_smem(p.nx, tq, p.S) : 0;
+      with_tq(tq, [&](auto qc) {
+        constexpr int TQ = decltype(qc)::value;
+        with_layout(p, [&](auto mc, auto tc) {
+          constexpr bool MU = decltype(mc)::value, TE = decltype(tc)::value;
+          if constexpr (MU) {
+            allow_smem(rk::k_rcol_fwd<NX, TQ, MU, TE>, sm);
+            allow_smem(rk::k_rcol_bwd<NX, TQ, MU, TE>, sm);
+          } else if constexpr (TQ == 16) {  // one species: 16-column tiles only
+            allow_smem(rk::k_rcol_fwd1<NX, TQ, TE>, f.colf_smem);
+            allow_smem(rk::k_rcol_bwd1<NX, TQ, TE>, f.colb_smem);
+          }
+        });
       });
-    });
+    }
   });
   *plan = f;
+  return true;
+}
+
+bool fused_plan_set_tile(const EvalParams& p, FusedPlan* f, int tq) {
+  if (p.S == 1) return tq == 16;  // one species: 16-column tiles only
+  if (tq != 16 && !(tq == 32 && f->tq32)) return false;
+  f->tq = tq;
+  f->colf_smem = rk::rcol_smem(p.nx, tq, p.S);
+  f->colb_smem = f->colf_smem;
+  f->col_tiles = (int)(((long long)p.ny * p.nzh + tq - 1) / tq);
   return true;
 }
 

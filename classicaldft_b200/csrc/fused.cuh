@@ -13,7 +13,12 @@ struct FusedPlan {
   size_t plane_smem = 0, colf_smem = 0, colb_smem = 0;
   int tq = 0;         // columns per column-pass tile
   int col_tiles = 0;  // column-pass CTAs per problem
+  bool tq32 = false;  // several species: 32-column tiles fit (16 always do)
 };
+
+// Column tile width of the plan (16, or 32 where tq32): false, plan
+// unchanged, for a width it does not have.
+bool fused_plan_set_tile(const EvalParams& p, FusedPlan* plan, int tq);
 
 // True (and `plan` filled, the kernels' shared-memory limits raised) when the
 // fused path serves this engine.

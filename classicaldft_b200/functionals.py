@@ -360,10 +360,11 @@ class Engine:
         return chunks.value, {k + 1: ms[k] for k in range(8) if ms[k] > 0.0}
 
     def autotune_ex(self, rho_ptr: int, vext_ptr: int = 0, mu=None, stream: int = 0, reps: int = 5):
-        """Time every (plane-chunk count, pointwise variant) pair and keep the
-        fastest.  Returns ((chunks, variant), {(variant, count): ms})."""
-        choice = (ctypes.c_int * 2)()
-        ms = (ctypes.c_double * (3 * 8))()
+        """Time every (plane-chunk count, pointwise variant, column tile)
+        combination the engine has and keep the fastest.  Returns
+        ((chunks, variant, tile), {(tile, variant, count): ms})."""
+        choice = (ctypes.c_int * 3)()
+        ms = (ctypes.c_double * (2 * 3 * 8))()
         mu_arr = None
         if mu is not None:
             mu_arr = (ctypes.c_double * (self.batch * self.S))(*[float(m) for m in mu])
@@ -371,8 +372,18 @@ class Engine:
                                                       ctypes.c_void_p(vext_ptr or None), mu_arr,
                                                       ctypes.c_void_p(stream or None), int(reps), choice, ms))
         self.info = self._query_info()
-        return (choice[0], choice[1]), {(v, k + 1): ms[v * 8 + k] for v in range(3) for k in range(8)
-                                        if ms[v * 8 + k] > 0.0}
+        return (choice[0], choice[1], choice[2]), {(16 << t, v, k + 1): ms[(t * 3 + v) * 8 + k] for t in range(2)
+                                                   for v in range(3) for k in range(8) if ms[(t * 3 + v) * 8 + k] > 0.0}
+
+    @property
+    def column_tile(self) -> int:
+        """Columns per tile of the fused column passes (0 without the fused path)."""
+        t = ctypes.c_int()
+        _lib.check(_lib.lib().cdft_engine_column_tile(self.handle, ctypes.byref(t)))
+        return t.value
+
+    def set_column_tile(self, tile: int):
+        _lib.check(_lib.lib().cdft_engine_set_column_tile(self.handle, int(tile)))
 
     @property
     def pointwise(self) -> int:

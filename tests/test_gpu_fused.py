@@ -173,3 +173,36 @@ def test_autotune():
     r24 = torch.full((24 ** 3,), 0.3, dtype=torch.float64, device="cuda")
     k24, ms24 = cu.weights.engine.autotune(r24.data_ptr())
     assert k24 == 1 and ms24 == {}
+
+
+def test_column_tile_widths_and_autotune_table():
+    """Two species: the column passes in tiles of 16 or 32 columns give the
+    same forces bitwise (each column is transformed alone); the autotuner's
+    table covers both widths and every chunk count and its choice is kept."""
+    import torch
+    shape = (64, 32, 32)
+    inters = [(0, 0) + LJ, (0, 1, 1.0, 0.8, 2.5)]
+    pr = Problem(shape, 0.1, [1.0, 0.6], "WhiteBearII", inters=inters, kT=0.9, precision=cd.MIXED)
+    rng = np.random.default_rng(8)
+    rhos = [0.3 * (1.0 + 0.05 * smooth_noise(shape, rng)), 0.1 * (1.0 + 0.05 * smooth_noise(shape, rng))]
+    e = pr.weights.engine
+    assert e.column_tile == 32
+    base = pr.gpu(rhos, [0.2, -0.1])
+    e.set_column_tile(16)
+    assert e.column_tile == 16
+    r16 = pr.gpu(rhos, [0.2, -0.1])
+    for s in range(2):
+        assert np.array_equal(r16.forces[s], base.forces[s]), s
+    assert rel_err(r16.free_energy, base.free_energy) <= 1e-13
+    for bad in (0, 8, 64):
+        with pytest.raises(ValueError):
+            e.set_column_tile(bad)
+    rd = torch.tensor(np.concatenate([r.ravel() for r in rhos]), device="cuda")
+    (k, v, tq), ms = e.autotune_ex(rd.data_ptr(), mu=[0.2, -0.1], reps=2)
+    assert v == 0 and tq in (16, 32)
+    assert sorted(ms) == sorted((t, 0, c) for t in (16, 32) for c in (1, 2, 4, 8))
+    assert (tq, v, k) == min(ms, key=ms.get)
+    assert e.column_tile == tq and e.info["kernels_per_eval"] == 4 + 3 * k
+    after = pr.gpu(rhos, [0.2, -0.1])
+    for s in range(2):
+        assert np.array_equal(after.forces[s], base.forces[s]), s

@@ -74,3 +74,27 @@ def test_headline_state_every_chunk_count(headline):
             base = res.forces[0]
         assert np.array_equal(res.forces[0], base), k
     w.engine.close()
+
+
+def test_headline_state_every_pointwise_variant(headline):
+    """The generic and the one-species pointwise kernels (5 and 6 CTAs per
+    SM) compute each point the same way: identical forces, the oracle's F."""
+    model, rho, mu, ref = headline
+    w = cd.make_weights(cd.WhiteBearII(), model, cd.MIXED)
+    assert w.engine.pointwise_variants == [0, 1, 2]
+    base = None
+    for v in (0, 1, 2):
+        w.engine.set_pointwise(v)
+        assert w.engine.pointwise == v
+        res = cd.total(model, [rho], w, mu)
+        assert rel_err(res.free_energy, ref.free_energy) <= 1e-9
+        assert force_err(res.forces, ref.forces) <= 1e-6
+        if base is None:
+            base = res.forces[0]
+        assert np.array_equal(res.forces[0], base), v
+    with pytest.raises(ValueError):
+        w.engine.set_pointwise(3)
+    assert w.engine.column_tile == 16
+    with pytest.raises(ValueError):  # one species: 16-column tiles only
+        w.engine.set_column_tile(32)
+    w.engine.close()
