@@ -10,7 +10,7 @@ from .functionals import (BARKER_HENDERSON, WEEKS_CHANDLER_ANDERSEN, Engine, EsF
                           Grid, Interaction, Model, Potential, Result, Rosenfeld, RSLT, Species, Weights,
                           WhiteBearI, WhiteBearII, interaction_weight, make_grid, make_lennard_jones,
                           make_ten_wolde_frenkel, make_wang_ramirez_dobnikar_frenkel, make_weights, total,
-                          total_batch)
+                          total_batch, total_stream)
 
 from .algorithms import set_step_graphs, step_graphs  # noqa: F401
 from .algorithms import (Bounded, EigenvalueResult, EigenvalueSolver, Fire, FixedMassConstraint,  # noqa: F401

@@ -174,6 +174,8 @@ def lib():
         "cdft_engine_info": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "cdft_engine_a_vdw": [vp, ctypes.c_int, c_double_p],
         "cdft_total": [vp, vp, vp, c_double_p, vp, c_double_p],
+        "cdft_total_stream": [vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.POINTER(vp), c_double_p,
+                              ctypes.POINTER(vp), c_double_p],
         "cdft_total_device": [vp, vp, vp, c_double_p, vp, vp, vp],
         "cdft_engine_status": [vp, vp],
         "cdft_engine_set_transforms": [vp, ctypes.c_int],

@@ -21,8 +21,8 @@ LIB = os.path.join(HERE, "libcdft_b200.so")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc") if os.path.exists(os.path.join(CUDA_HOME, "bin", "nvcc")) else "nvcc"
 
-SOURCES = ["engine.cu", "fused.cu", "drivers.cu", "lanczos.cu", "capi.cu", "noalloc.cu", "bulk.cu", "lattice.cu",
-           "physics.cpp"]
+SOURCES = ["engine.cu", "fused.cu", "drivers.cu", "lanczos.cu", "host_stream.cu", "capi.cu", "noalloc.cu", "bulk.cu",
+           "lattice.cu", "physics.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++20", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I", CSRC, "-I", os.path.join(ROOT, "include")]

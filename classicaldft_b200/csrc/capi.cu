@@ -8,11 +8,13 @@
 #include "../../include/cdft_b200.h"
 #include "drivers.cuh"
 #include "engine.cuh"
+#include "host_stream.cuh"
 #include "physics.hpp"
 
 struct cdft_engine {
   cdft::Engine* impl;
-  cdft::Drivers* drivers;  // created on first driver call
+  cdft::Drivers* drivers;         // created on first driver call
+  cdft::HostStream* host_stream;  // created on first cdft_total_stream call
 };
 
 namespace {
@@ -141,7 +143,7 @@ cdft::EngineSpec base_spec(const long shape[3], double dx, int n_species, const 
 }
 
 void make_engine(cdft_engine** out, const cdft::EngineSpec& spec) {
-  auto* e = new cdft_engine{nullptr, nullptr};
+  auto* e = new cdft_engine{nullptr, nullptr, nullptr};
   try {
     e->impl = new cdft::Engine(spec);
   } catch (...) {
@@ -237,6 +239,7 @@ int cdft_engine_bulk_model(const cdft_engine* engine, cdft_bulk_model* out) {
 int cdft_destroy(cdft_engine* engine) {
   return guarded([&] {
     if (!engine) return;
+    delete engine->host_stream;
     delete engine->drivers;
     delete engine->impl;
     delete engine;
@@ -282,6 +285,15 @@ int cdft_total(cdft_engine* engine, const double* rho, const double* vext, const
     CDFT_CUDA(cudaStreamSynchronize(st));
     if (e.take_error(st)) throw cdft::Error(CDFT_ERR_RUNTIME, "evaluation aborted: a bounded device wait timed out");
     if (scalars) std::memcpy(scalars, tmp.data(), sizeof(double) * tmp.size());
+  });
+}
+
+int cdft_total_stream(cdft_engine* engine, int count, const double* const* rho, const double* const* vext,
+                      const double* mu, double* const* force, double* scalars) {
+  return guarded([&] {
+    if (!engine) throw std::invalid_argument("engine is NULL");
+    if (!engine->host_stream) engine->host_stream = new cdft::HostStream(*engine->impl);
+    engine->host_stream->run(count, rho, vext, mu, force, scalars);
   });
 }
 

@@ -494,6 +494,9 @@ int Engine::autotune(const double* rho, const double* vext, const double* mu, cu
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   CDFT_CUDA(cudaEventCreate(&e0));
   CDFT_CUDA(cudaEventCreate(&e1));
+  // engines without a tile choice time their current tile (row 0 of the
+  // table where they have no fused path)
+  const int tile_now = col_tile() == 32 ? 32 : 16;
   int best = chunks_, best_v = pw_variant_, best_t = col_tile();
   double best_ms = 0.0;
   for (int ti = 0; ti < kTiles; ++ti) {
@@ -501,7 +504,7 @@ int Engine::autotune(const double* rho, const double* vext, const double* mu, cu
     if (tune_tiles) {
       if (!fused_plan_set_tile(p_, &plan_, tq)) continue;
       ++generation_;
-    } else if (tq != best_t) {
+    } else if (tq != tile_now) {
       continue;
     }
     for (int v = 0; v < kPointwiseVariants; ++v) {
@@ -527,7 +530,7 @@ int Engine::autotune(const double* rho, const double* vext, const double* mu, cu
           best_ms = per;
           best = k;
           best_v = v;
-          best_t = tq;
+          if (tune_tiles) best_t = tq;
         }
       }
     }

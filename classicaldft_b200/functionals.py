@@ -307,6 +307,39 @@ class Engine:
                                          sc.ctypes.data_as(_lib.c_double_p)))
         return sc, force
 
+    def total_stream_ptrs(self, rho_ptrs, mu, force_ptrs=None, vext_ptrs=None):
+        """cdft_total_stream on host addresses (one per state; page-locked
+        memory lets the copies overlap the evaluations).  ``mu``: (count, S)
+        or (count, B, S) values.  Returns the scalars, (count, 10) or
+        (count, B, 10)."""
+        count = len(rho_ptrs)
+        lead = (self.S,) if self.batch == 1 else (self.batch, self.S)
+        m = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), (count, *lead)))
+        arr = ctypes.c_void_p * max(count, 1)
+        rp = arr(*rho_ptrs)
+        fp = None if force_ptrs is None else arr(*force_ptrs)
+        vp = None if vext_ptrs is None else arr(*vext_ptrs)
+        sc = np.empty((count, _lib.SCALAR_COUNT) if self.batch == 1 else (count, self.batch, _lib.SCALAR_COUNT))
+        _lib.check(_lib.lib().cdft_total_stream(self.handle, count, rp, vp, m.ctypes.data_as(_lib.c_double_p), fp,
+                                                sc.ctypes.data_as(_lib.c_double_p)))
+        return sc
+
+    def total_stream(self, rhos, mus, vexts=None, want_force=True):
+        """cdft_total_stream on a list of host states, each shaped as for
+        total_host.  Returns (scalars per state, forces per state or None)."""
+        lead = (self.S,) if self.batch == 1 else (self.batch, self.S)
+        rs = [np.ascontiguousarray(r, dtype=np.float64).reshape(*lead, self.N) for r in rhos]
+        vs = None
+        if vexts is not None:
+            vs = [None if v is None else np.ascontiguousarray(v, dtype=np.float64).reshape(*lead, self.N)
+                  for v in vexts]
+        fs = [np.empty((*lead, self.N)) for _ in rs] if want_force else None
+        mu = np.stack([self._mu(m) for m in mus]) if len(rs) else np.zeros((0, *lead))
+        sc = self.total_stream_ptrs([r.ctypes.data for r in rs], mu,
+                                    None if fs is None else [f.ctypes.data for f in fs],
+                                    None if vs is None else [None if v is None else v.ctypes.data for v in vs])
+        return sc, fs
+
     STAGES = ("split", "r2c_rho", "k_forward", "c2r_channels", "pointwise", "r2c_derivatives", "k_backward",
               "c2r_force", "epilogue", "reduce")
     STAGES_FUSED = ("-0", "plane_fwd_rho", "col_fwd", "plane_inv_channels", "pointwise",
@@ -471,6 +504,32 @@ def total(model: Model, rhos, weights: Weights, mus=None, vexts=None) -> Result:
              "N": [sc[6 + s] for s in range(S)]}
     return Result(free_energy=float(sc[0]), grand_potential=float(sc[1]), forces=[force[s] for s in range(S)],
                   parts=parts)
+
+
+def total_stream(model: Model, states, weights: Weights, mus=None, vexts=None) -> list:
+    """``total`` for a sequence of states (each one profile per species or an
+    (S, N) array) through cdft_total_stream: the copies of one state overlap
+    the evaluation of the next.  ``mus``: one beta*mu set per state (default
+    0); ``vexts``: None or one list of fields (or None) per state.  Returns
+    one Result per state, equal to ``total`` on each."""
+    S = len(model.species)
+    N = model.grid.total_points
+    rhos = [np.stack([np.asarray(r, dtype=np.float64).reshape(-1) for r in st]) if not isinstance(st, np.ndarray)
+            else np.asarray(st, dtype=np.float64).reshape(S, N) for st in states]
+    mus = [np.zeros(S)] * len(rhos) if mus is None else [np.asarray(m, dtype=np.float64) for m in mus]
+    vs = None
+    if vexts is not None:
+        vs = [None if v is None or all(x is None for x in v) else
+              np.stack([np.zeros(N) if x is None else np.asarray(x, dtype=np.float64).reshape(-1) for x in v])
+              for v in vexts]
+    sc, forces = weights.engine.total_stream(rhos, mus, vs)
+    out = []
+    for i in range(len(rhos)):
+        parts = {"ideal": sc[i, 2], "external": sc[i, 3], "hard_sphere": sc[i, 4], "mean_field": sc[i, 5],
+                 "N": [sc[i, 6 + s] for s in range(S)]}
+        out.append(Result(free_energy=float(sc[i, 0]), grand_potential=float(sc[i, 1]),
+                          forces=[forces[i][s] for s in range(S)], parts=parts))
+    return out
 
 
 def total_batch(model: Model, rhos, weights: Weights, mus=None, vexts=None) -> list:

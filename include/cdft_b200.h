@@ -189,6 +189,22 @@ CDFT_API int cdft_engine_a_vdw(const cdft_engine* engine, int m, double* a_vdw);
 CDFT_API int cdft_total(cdft_engine* engine, const double* rho, const double* vext, const double* mu, double* force,
                double* scalars);
 
+/* functionals::total for `count` states held in HOST memory, one after the
+ * other, with the copies overlapped: the host->device copy of state i+1 and
+ * the device->host copy of state i-1 run on their own streams while state i
+ * is evaluated (two device slots alternate).  The same evaluation as count
+ * cdft_total calls, the same results; returns when every result is in host
+ * memory.  Page-locked host buffers let the copies overlap.
+ *   rho    : count pointers to B*S*N doubles
+ *   vext   : NULL (no field) or count pointers (entries may be NULL)
+ *   mu     : count * B*S values (state i at mu + i*B*S)
+ *   force  : NULL or count pointers (entries may be NULL: no force copy)
+ *   scalars: NULL or count * B*CDFT_SCALAR_COUNT doubles
+ * No reference counterpart: the reference evaluates one state per call
+ * (functionals.hpp:64-95); this is that call for a stream of states. */
+CDFT_API int cdft_total_stream(cdft_engine* engine, int count, const double* const* rho, const double* const* vext,
+                               const double* mu, double* const* force, double* scalars);
+
 /* functionals::total on DEVICE buffers, asynchronous on `stream`
  * (cudaStream_t; NULL = the legacy default stream).  rho, vext, force and
  * scalars are device pointers; mu is a host array read at call time. */

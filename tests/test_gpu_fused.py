@@ -168,11 +168,18 @@ def test_autotune():
     assert rel_err(after.free_energy, before.free_energy) <= 1e-13
     again = cd.make_weights(pr.fmt, pr.model, cd.MIXED)
     assert again.engine.info["kernels_per_eval"] == 4 + 3 * k
-    # an engine without the fused path: nothing to tune
+    # an engine without the fused path keeps one chunk; with one species it
+    # still times its pointwise variants (the table holds the one count)
     cu = Problem((24, 24, 24), 0.2, [1.0], "WhiteBearII", precision=cd.MIXED)
     r24 = torch.full((24 ** 3,), 0.3, dtype=torch.float64, device="cuda")
     k24, ms24 = cu.weights.engine.autotune(r24.data_ptr())
-    assert k24 == 1 and ms24 == {}
+    assert k24 == 1 and sorted(ms24) == [1]
+    assert cu.weights.engine.column_tile == 0
+    # two species without the fused path: nothing to tune
+    cu2 = Problem((24, 24, 24), 0.2, [1.0, 0.6], "WhiteBearII", precision=cd.MIXED)
+    r2 = torch.full((2 * 24 ** 3,), 0.2, dtype=torch.float64, device="cuda")
+    k2, ms2 = cu2.weights.engine.autotune(r2.data_ptr())
+    assert k2 == 1 and ms2 == {}
 
 
 def test_column_tile_widths_and_autotune_table():

@@ -78,7 +78,13 @@ def test_headline_state_every_chunk_count(headline):
 
 def test_headline_state_every_pointwise_variant(headline):
     """The generic and the one-species pointwise kernels (5 and 6 CTAs per
-    SM) compute each point the same way: identical forces, the oracle's F."""
+    SM) evaluate the same expressions: each meets the oracle's tolerances;
+    the generic and the 5-CTA kernel agree bitwise.  The 6-CTA kernel is
+    compiled for 80 registers, and its FP64 results may differ from the
+    others' in the last bit (contraction of products into fused multiply-
+    adds is the compiler's choice per kernel), which can flip the FP32
+    rounding of a derivative channel: its forces agree to 1e-8 of the
+    largest force, its F to 1e-13."""
     model, rho, mu, ref = headline
     w = cd.make_weights(cd.WhiteBearII(), model, cd.MIXED)
     assert w.engine.pointwise_variants == [0, 1, 2]
@@ -90,8 +96,12 @@ def test_headline_state_every_pointwise_variant(headline):
         assert rel_err(res.free_energy, ref.free_energy) <= 1e-9
         assert force_err(res.forces, ref.forces) <= 1e-6
         if base is None:
-            base = res.forces[0]
-        assert np.array_equal(res.forces[0], base), v
+            base = res
+        if v < 2:
+            assert np.array_equal(res.forces[0], base.forces[0]), v
+        else:
+            assert force_err(res.forces, base.forces) <= 1e-8
+            assert rel_err(res.free_energy, base.free_energy) <= 1e-13
     with pytest.raises(ValueError):
         w.engine.set_pointwise(3)
     assert w.engine.column_tile == 16
