@@ -689,12 +689,16 @@ def run_ours(args, ws, rank, local, dist):
     tuned = None
     if args.plane_chunks:
         eng.set_plane_chunks(args.plane_chunks)
+        if args.pointwise >= 0:
+            eng.set_pointwise(args.pointwise)
+        if args.pointwise_spread >= 0:
+            eng.set_pointwise_spread(args.pointwise_spread)
     elif eng.transforms == "fused":
         # the engine's autotuner picks the plane-chunk count and the pointwise
         # kernel variant on this state
-        (k, v, tq), ms = eng.autotune_ex(rho.data_ptr(), mu=[0.0], reps=10)
-        tuned = {"chosen": {"plane_chunks": k, "pointwise_variant": v, "column_tile": tq},
-                 "ms_per_eval": {f"t{tt}_v{vv}_k{c}": round(t, 5) for (tt, vv, c), t in ms.items()}}
+        (k, v, tq, sp), ms = eng.autotune_ex(rho.data_ptr(), mu=[0.0], reps=10)
+        tuned = {"chosen": {"plane_chunks": k, "pointwise_variant": v, "column_tile": tq, "pointwise_spread": sp},
+                 "ms_per_eval": {f"t{tt}_v{vv}_k{c}_d{dd}": round(t, 5) for (tt, vv, c, dd), t in ms.items()}}
     force = torch.empty_like(rho)
     scal = torch.zeros(10, dtype=torch.float64, device=dev)
     flush = L2Flush(torch, dev)
@@ -863,6 +867,11 @@ def main():
     ap.add_argument("--plane-chunks", type=int, default=0,
                     help="plane chunks of the fused path's middle stages (0: the engine's default; 1 runs them "
                          "back to back, as a profiler's serialised launch list sees them)")
+    ap.add_argument("--pointwise", type=int, default=-1,
+                    help="with --plane-chunks: the pointwise kernel variant (0 generic, 1 / 2 one species at 5 / 6 "
+                         "CTAs per SM; -1: the engine's default)")
+    ap.add_argument("--pointwise-spread", type=int, default=-1,
+                    help="with --plane-chunks: divisor of the pointwise grid per chunk (0: the chunk count)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the runs of the other configurations (wall, DDFT, nucleus, uneven sweep)")
     ap.add_argument("--traffic-table", metavar="NCU_CSV",

@@ -355,29 +355,51 @@ int cdft_engine_autotune(cdft_engine* engine, const double* rho, const double* v
   return guarded([&] {
     if (!engine || !rho) throw std::invalid_argument("engine and rho are required");
     if (reps < 1) throw std::invalid_argument("autotune: reps must be positive");
-    double all[2 * cdft::Engine::kPointwiseVariants * cdft::Engine::kMaxChunks];
-    int v = 0, tq = 16;
-    const int k = engine->impl->autotune(rho, vext, mu, static_cast<cudaStream_t>(stream), reps, all, &v, &tq);
+    using E = cdft::Engine;
+    double all[2 * E::kPointwiseVariants * E::kMaxChunks * E::kSpreads];
+    int v = 0, tq = 16, d = 0;
+    const int k = engine->impl->autotune(rho, vext, mu, static_cast<cudaStream_t>(stream), reps, all, &v, &tq, &d);
     if (chunks) *chunks = k;
     const int ti = tq == 32 ? 1 : 0;
-    if (ms)
-      for (int c = 0; c < cdft::Engine::kMaxChunks; ++c)
-        ms[c] = all[(ti * cdft::Engine::kPointwiseVariants + v) * cdft::Engine::kMaxChunks + c];
+    if (ms)  // per chunk count: the best spread at the kept tile and variant
+      for (int c = 0; c < E::kMaxChunks; ++c) {
+        double best = 0.0;
+        for (int di = 0; di < E::kSpreads; ++di) {
+          const double t = all[((ti * E::kPointwiseVariants + v) * E::kMaxChunks + c) * E::kSpreads + di];
+          if (t > 0.0 && (best == 0.0 || t < best)) best = t;
+        }
+        ms[c] = best;
+      }
   });
 }
 
 int cdft_engine_autotune_ex(cdft_engine* engine, const double* rho, const double* vext, const double* mu,
-                            void* stream, int reps, int choice[3], double* ms) {
+                            void* stream, int reps, int choice[4], double* ms) {
   return guarded([&] {
     if (!engine || !rho) throw std::invalid_argument("engine and rho are required");
     if (reps < 1) throw std::invalid_argument("autotune: reps must be positive");
-    int v = 0, tq = 0;
-    const int k = engine->impl->autotune(rho, vext, mu, static_cast<cudaStream_t>(stream), reps, ms, &v, &tq);
+    int v = 0, tq = 0, d = 0;
+    const int k = engine->impl->autotune(rho, vext, mu, static_cast<cudaStream_t>(stream), reps, ms, &v, &tq, &d);
     if (choice) {
       choice[0] = k;
       choice[1] = v;
       choice[2] = tq;
+      choice[3] = d;
     }
+  });
+}
+
+int cdft_engine_set_pointwise_spread(cdft_engine* engine, int spread) {
+  return guarded([&] {
+    if (!engine) throw std::invalid_argument("engine is NULL");
+    engine->impl->set_pw_spread(spread);
+  });
+}
+
+int cdft_engine_pointwise_spread(const cdft_engine* engine, int* spread) {
+  return guarded([&] {
+    if (!engine || !spread) throw std::invalid_argument("engine and spread are required");
+    *spread = engine->impl->pw_spread();
   });
 }
 

@@ -20,6 +20,7 @@ std::mutex g_tune_mu;
 std::map<std::string, int> g_tune_chunks;
 std::map<std::string, int> g_tune_variant;
 std::map<std::string, int> g_tune_tile;
+std::map<std::string, int> g_tune_spread;
 }  // namespace
 
 namespace {
@@ -329,10 +330,12 @@ Engine::Engine(const EngineSpec& spec) {
   // partials, so fewer blocks shorten that tail and the counter's contention)
   grid_mean_ = per_problem(std::max<long long>(1, std::min<long long>((long long)sms * 4, (p.N * B + 255) / 256)));
   // (+8: the pointwise grid rounded up to whole chunks, see fused_middle)
-  partials_ =
-      dalloc<double>((size_t)B *
-                         (std::max({grid_pw_, grid_tma_, grid_stream_, grid_pw1_[0], grid_pw1_[1]}) + 8) * p.n_terms,
-                     tot);
+  // (a plane chunk may take the whole pointwise grid: kMaxChunks grids)
+  partials_ = dalloc<double>(
+      (size_t)B *
+          ((size_t)std::max({grid_pw_, grid_tma_, grid_stream_, grid_pw1_[0], grid_pw1_[1]}) * kMaxChunks + 8) *
+          p.n_terms,
+      tot);
   err_ = dalloc<int>(1, tot);
   CDFT_CUDA(cudaMemset(err_, 0, sizeof(int)));
   sync_ = dalloc<unsigned>((size_t)B, tot);
@@ -424,6 +427,8 @@ void Engine::setup_fused() {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     const auto iv = g_tune_variant.find(tune_key_);
     if (iv != g_tune_variant.end() && (iv->second == 0 || pw1_)) pw_variant_ = iv->second;
+    const auto is = g_tune_spread.find(tune_key_);
+    if (is != g_tune_spread.end()) pw_div_ = is->second;
   }
   fusable_ = false;
   if (precision_ != kMixed || !fused_plan(p, &plan_)) return;
@@ -476,12 +481,13 @@ void Engine::ensure_chunk_streams(int k) {
 // Every (plane-chunk count, pointwise variant) pair the engine has, timed on
 // the caller's state; the fastest is kept and cached for the shape.
 int Engine::autotune(const double* rho, const double* vext, const double* mu, cudaStream_t stream, int reps,
-                     double* ms, int* variant, int* tile) {
+                     double* ms, int* variant, int* tile, int* spread) {
   constexpr int kTiles = 2;  // column tile widths 16, 32
   if (ms)
-    for (int k = 0; k < kPointwiseVariants * kMaxChunks * kTiles; ++k) ms[k] = 0.0;
+    for (int k = 0; k < kPointwiseVariants * kMaxChunks * kTiles * kSpreads; ++k) ms[k] = 0.0;
   if (variant) *variant = pw_variant_;
   if (tile) *tile = col_tile();
+  if (spread) *spread = pw_div_;
   const bool tune_chunks = fusable_ && fused_;
   const bool tune_tiles = tune_chunks && p_.S > 1;
   if (!tune_chunks && !pw1_) return chunks_;
@@ -497,7 +503,7 @@ int Engine::autotune(const double* rho, const double* vext, const double* mu, cu
   // engines without a tile choice time their current tile (row 0 of the
   // table where they have no fused path)
   const int tile_now = col_tile() == 32 ? 32 : 16;
-  int best = chunks_, best_v = pw_variant_, best_t = col_tile();
+  int best = chunks_, best_v = pw_variant_, best_t = col_tile(), best_d = pw_div_;
   double best_ms = 0.0;
   for (int ti = 0; ti < kTiles; ++ti) {
     const int tq = 16 << ti;
@@ -517,20 +523,26 @@ int Engine::autotune(const double* rho, const double* vext, const double* mu, cu
         } else if (k != chunks_) {
           continue;
         }
-        for (int w = 0; w < 2; ++w) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
-        CDFT_CUDA(cudaEventRecord(e0, stream));
-        for (int r = 0; r < reps; ++r) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
-        CDFT_CUDA(cudaEventRecord(e1, stream));
-        CDFT_CUDA(cudaEventSynchronize(e1));
-        float t = 0.0f;
-        CDFT_CUDA(cudaEventElapsedTime(&t, e0, e1));
-        const double per = (double)t / reps;
-        if (ms) ms[(ti * kPointwiseVariants + v) * kMaxChunks + k - 1] = per;
-        if (best_ms == 0.0 || per < best_ms) {
-          best_ms = per;
-          best = k;
-          best_v = v;
-          if (tune_tiles) best_t = tq;
+        for (int di = 0; di < kSpreads; ++di) {
+          const int d = 1 << di;
+          if (d > k || (!tune_chunks && d > 1)) break;
+          set_pw_spread(d);
+          for (int w = 0; w < 2; ++w) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
+          CDFT_CUDA(cudaEventRecord(e0, stream));
+          for (int r = 0; r < reps; ++r) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
+          CDFT_CUDA(cudaEventRecord(e1, stream));
+          CDFT_CUDA(cudaEventSynchronize(e1));
+          float t = 0.0f;
+          CDFT_CUDA(cudaEventElapsedTime(&t, e0, e1));
+          const double per = (double)t / reps;
+          if (ms) ms[((ti * kPointwiseVariants + v) * kMaxChunks + k - 1) * kSpreads + di] = per;
+          if (best_ms == 0.0 || per < best_ms) {
+            best_ms = per;
+            best = k;
+            best_v = v;
+            best_d = d;
+            if (tune_tiles) best_t = tq;
+          }
         }
       }
     }
@@ -541,12 +553,15 @@ int Engine::autotune(const double* rho, const double* vext, const double* mu, cu
   if (tune_tiles) set_col_tile(best_t);
   if (tune_chunks) set_chunks(best);
   set_pointwise(best_v);
+  set_pw_spread(best_d);
   if (variant) *variant = best_v;
   if (tile) *tile = col_tile();
+  if (spread) *spread = pw_div_;
   std::lock_guard<std::mutex> lock(g_tune_mu);
   if (tune_chunks) g_tune_chunks[tune_key_] = best;
   if (tune_tiles) g_tune_tile[tune_key_] = best_t;
   g_tune_variant[tune_key_] = best_v;
+  g_tune_spread[tune_key_] = best_d;
   return chunks_;
 }
 
@@ -570,6 +585,18 @@ void Engine::set_pointwise(int v) {
 }
 
 int Engine::pw_grid() const { return (pw1_ && pw_variant_ > 0) ? grid_pw1_[pw_variant_ - 1] : grid_tma_; }
+
+int Engine::pw_chunk_grid(int K) const {
+  const int d = pw_div_ == 0 ? K : std::min(pw_div_, K);
+  return (pw_grid() + d - 1) / d;
+}
+
+void Engine::set_pw_spread(int d) {
+  if (d != 0 && d != 1 && d != 2 && d != 4 && d != 8)
+    throw std::invalid_argument("pointwise spread: 1, 2, 4, 8 or 0 (the chunk count)");
+  if (d != pw_div_) ++generation_;
+  pw_div_ = d;
+}
 
 void Engine::set_chunks(int k) {
   if (!fusable_) throw std::invalid_argument("plane chunks: the engine has no fused path");
@@ -764,7 +791,7 @@ void Engine::fused_middle(const double* rho, const double* vext, double* force, 
   const EvalParams& p = p_;
   const int K = chunked ? chunks_ : 1;
   const int per = p.nx / K;
-  const int gk = (pw_grid() + K - 1) / K;
+  const int gk = pw_chunk_grid(K);
   const fft::cpx* q = static_cast<const fft::cpx*>(chan_k_);
   fft::cpx* pd = static_cast<fft::cpx*>(deriv_k_);
   float* chan_r = static_cast<float*>(chan_r_);
@@ -846,7 +873,7 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
     fused_forward(rho, stream);
     if constexpr (sizeof(R) == sizeof(float)) fused_middle<R>(rho, vext, force, !timing_run_, stream);
     const int K = timing_run_ ? 1 : chunks_;
-    FinalArgs fin{partials_, K * ((pw_grid() + K - 1) / K), err_, scalars};
+    FinalArgs fin{partials_, K * pw_chunk_grid(K), err_, scalars};
     fused_backward(force, ma, fin, stream);
     mark(10, stream);
     if (timing_run_) {

@@ -104,11 +104,21 @@ class Engine {
   // the engine has no fused path).  Synchronises the stream.
   // The pointwise kernel variants (see pw_variant_) are tuned with the chunk
   // counts: ms[v * kMaxChunks + k - 1]; *variant receives the variant kept.
-  // Several species also tune the column tile width (16, 32):
-  // ms[(tile_index * kPointwiseVariants + v) * kMaxChunks + k - 1].
+  // Several species also tune the column tile width (16, 32), and every
+  // chunk count k its pointwise spread d (1, 2, 4, 8 up to k):
+  // ms[((tile_index * kPointwiseVariants + v) * kMaxChunks + k - 1) * kSpreads + log2 d].
   static constexpr int kPointwiseVariants = 3;
+  static constexpr int kSpreads = 4;
   int autotune(const double* rho, const double* vext, const double* mu, cudaStream_t stream, int reps,
-               double* ms, int* variant, int* tile = nullptr);
+               double* ms, int* variant, int* tile = nullptr, int* spread = nullptr);
+  // Pointwise grid of one plane chunk: the full pointwise grid (pw_grid)
+  // divided by d = min(spread, chunks), 0 = the chunk count (each chunk one
+  // share).  Larger shares put more warps on one chunk's FP64 work (a
+  // chunk's pointwise launch often runs alone); smaller ones leave SM room
+  // for the transforms of the other chunks.  1, 2, 4, 8 or 0.
+  void set_pw_spread(int d);
+  int pw_spread() const { return pw_div_; }
+  int pw_chunk_grid(int K) const;
   // Column tile width of the fused path's column passes (16, or 32 for
   // several species where their spectra fit); std::invalid_argument otherwise.
   void set_col_tile(int tq);
@@ -212,6 +222,7 @@ class Engine {
   // pointwise kernel of the TMA path: 0 generic (k_pointwise_tma), 1 / 2 the
   // one-species kernel sized for 5 / 6 CTAs per SM (grid grid_pw1_[v - 1])
   int pw_variant_ = 0;
+  int pw_div_ = 0;  // pointwise grid divisor of a plane chunk (0: the chunk count)
   int grid_pw1_[2] = {0, 0};
   size_t tma1_smem_ = 0, tma1_smem_v_ = 0;
   template <typename R>

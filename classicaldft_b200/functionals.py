@@ -393,11 +393,12 @@ class Engine:
         return chunks.value, {k + 1: ms[k] for k in range(8) if ms[k] > 0.0}
 
     def autotune_ex(self, rho_ptr: int, vext_ptr: int = 0, mu=None, stream: int = 0, reps: int = 5):
-        """Time every (plane-chunk count, pointwise variant, column tile)
-        combination the engine has and keep the fastest.  Returns
-        ((chunks, variant, tile), {(tile, variant, count): ms})."""
-        choice = (ctypes.c_int * 3)()
-        ms = (ctypes.c_double * (2 * 3 * 8))()
+        """Time every (plane-chunk count, pointwise variant, column tile,
+        pointwise spread) combination the engine has and keep the fastest.
+        Returns ((chunks, variant, tile, spread),
+        {(tile, variant, count, spread): ms})."""
+        choice = (ctypes.c_int * 4)()
+        ms = (ctypes.c_double * (2 * 3 * 8 * 4))()
         mu_arr = None
         if mu is not None:
             mu_arr = (ctypes.c_double * (self.batch * self.S))(*[float(m) for m in mu])
@@ -405,8 +406,19 @@ class Engine:
                                                       ctypes.c_void_p(vext_ptr or None), mu_arr,
                                                       ctypes.c_void_p(stream or None), int(reps), choice, ms))
         self.info = self._query_info()
-        return (choice[0], choice[1], choice[2]), {(16 << t, v, k + 1): ms[(t * 3 + v) * 8 + k] for t in range(2)
-                                                   for v in range(3) for k in range(8) if ms[(t * 3 + v) * 8 + k] > 0.0}
+        idx = {(16 << t, v, k + 1, 1 << d): ((t * 3 + v) * 8 + k) * 4 + d
+               for t in range(2) for v in range(3) for k in range(8) for d in range(4)}
+        return (choice[0], choice[1], choice[2], choice[3]), {key: ms[i] for key, i in idx.items() if ms[i] > 0.0}
+
+    @property
+    def pointwise_spread(self) -> int:
+        """Divisor of the pointwise grid per plane chunk (0: the chunk count)."""
+        d = ctypes.c_int()
+        _lib.check(_lib.lib().cdft_engine_pointwise_spread(self.handle, ctypes.byref(d)))
+        return d.value
+
+    def set_pointwise_spread(self, spread: int):
+        _lib.check(_lib.lib().cdft_engine_set_pointwise_spread(self.handle, int(spread)))
 
     @property
     def column_tile(self) -> int:

@@ -609,20 +609,28 @@ CDFT_API int cdft_engine_autotune(cdft_engine* engine, const double* rho, const 
  * 2 exist.  The column passes of an engine with several species run tiles of
  * 16 or (where the spectra fit in shared memory) 32 in-plane columns; one
  * species always 16 (cdft_engine_set_column_tile / cdft_engine_column_tile;
- * 0 without the fused path).  cdft_engine_autotune times every pointwise
- * variant and column tile width with every plane-chunk count and keeps the
- * fastest combination; cdft_engine_autotune_ex also returns the whole table:
- * ms[(t * CDFT_POINTWISE_VARIANTS + v) * CDFT_MAX_PLANE_CHUNKS + k - 1] for
- * tile index t (0: 16, 1: 32), variant v and k chunks (0 where not tried;
- * 2 * CDFT_POINTWISE_VARIANTS * CDFT_MAX_PLANE_CHUNKS entries),
- * choice = {chunks, variant, tile}. */
+ * 0 without the fused path).  Each plane chunk's pointwise launch takes the
+ * full pointwise grid divided by d = min(spread, chunks); spread 0 (the
+ * default) divides it by the chunk count, 1, 2, 4, 8 give a chunk a larger
+ * share (cdft_engine_set_pointwise_spread / cdft_engine_pointwise_spread).
+ * cdft_engine_autotune times every pointwise variant, column tile width and
+ * spread with every plane-chunk count and keeps the fastest combination;
+ * cdft_engine_autotune_ex also returns the whole table:
+ * ms[((t * CDFT_POINTWISE_VARIANTS + v) * CDFT_MAX_PLANE_CHUNKS + k - 1)
+ *    * CDFT_POINTWISE_SPREADS + log2 d]
+ * for tile index t (0: 16, 1: 32), variant v, k chunks and spread d (0
+ * where not tried; 2 * CDFT_POINTWISE_VARIANTS * CDFT_MAX_PLANE_CHUNKS *
+ * CDFT_POINTWISE_SPREADS entries), choice = {chunks, variant, tile, spread}. */
 #define CDFT_POINTWISE_VARIANTS 3
+#define CDFT_POINTWISE_SPREADS 4
 CDFT_API int cdft_engine_set_pointwise(cdft_engine* engine, int variant);
 CDFT_API int cdft_engine_pointwise(const cdft_engine* engine, int* variant, int* available);
 CDFT_API int cdft_engine_set_column_tile(cdft_engine* engine, int tile);
 CDFT_API int cdft_engine_column_tile(const cdft_engine* engine, int* tile);
+CDFT_API int cdft_engine_set_pointwise_spread(cdft_engine* engine, int spread);
+CDFT_API int cdft_engine_pointwise_spread(const cdft_engine* engine, int* spread);
 CDFT_API int cdft_engine_autotune_ex(cdft_engine* engine, const double* rho, const double* vext, const double* mu,
-                                     void* stream, int reps, int choice[3], double* ms);
+                                     void* stream, int reps, int choice[4], double* ms);
 
 /* Step graphs (no reference counterpart; execution mode, process-wide): the
  * FIRE minimisers (cdft_minimize, cdft_minimize_batch, the saddle search's

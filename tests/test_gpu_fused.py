@@ -205,11 +205,39 @@ def test_column_tile_widths_and_autotune_table():
         with pytest.raises(ValueError):
             e.set_column_tile(bad)
     rd = torch.tensor(np.concatenate([r.ravel() for r in rhos]), device="cuda")
-    (k, v, tq), ms = e.autotune_ex(rd.data_ptr(), mu=[0.2, -0.1], reps=2)
+    (k, v, tq, sp), ms = e.autotune_ex(rd.data_ptr(), mu=[0.2, -0.1], reps=2)
     assert v == 0 and tq in (16, 32)
-    assert sorted(ms) == sorted((t, 0, c) for t in (16, 32) for c in (1, 2, 4, 8))
-    assert (tq, v, k) == min(ms, key=ms.get)
+    assert sorted(ms) == sorted((t, 0, c, d) for t in (16, 32) for c in (1, 2, 4, 8) for d in (1, 2, 4, 8) if d <= c)
+    assert (tq, v, k, sp) == min(ms, key=ms.get)
+    assert e.pointwise_spread == sp
     assert e.column_tile == tq and e.info["kernels_per_eval"] == 4 + 3 * k
     after = pr.gpu(rhos, [0.2, -0.1])
     for s in range(2):
         assert np.array_equal(after.forces[s], base.forces[s]), s
+
+
+def test_pointwise_spread():
+    """Each plane chunk's pointwise launch may take 1/8 .. all of the
+    pointwise grid: forces bitwise equal (each point is computed the same
+    way), F up to the summation order of the block partials."""
+    shape = (64, 32, 32)
+    pr = Problem(shape, 0.1, [1.0], "WhiteBearII", inters=[(0, 0) + LJ], kT=0.8, precision=cd.MIXED)
+    rng = np.random.default_rng(9)
+    rho = 0.35 * (1.0 + 0.05 * smooth_noise(shape, rng))
+    e = pr.weights.engine
+    e.set_plane_chunks(8)
+    e.set_pointwise_spread(0)  # (an earlier autotune of this shape may have set another)
+    assert e.pointwise_spread == 0
+    ref = pr.gpu([rho], [0.2])
+    for v in e.pointwise_variants:
+        e.set_pointwise(v)
+        base = pr.gpu([rho], [0.2])
+        for d in (1, 2, 4, 8, 0):
+            e.set_pointwise_spread(d)
+            assert e.pointwise_spread == d
+            r = pr.gpu([rho], [0.2])
+            assert np.array_equal(r.forces[0], base.forces[0]), (v, d)
+            assert rel_err(r.free_energy, ref.free_energy) <= 1e-13
+    for bad in (-1, 3, 16):
+        with pytest.raises(ValueError):
+            e.set_pointwise_spread(bad)
