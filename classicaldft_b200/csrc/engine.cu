@@ -150,19 +150,19 @@ void Engine::launch_pointwise_tma(const R* chan, R* deriv, const PointwiseArgs& 
         constexpr int MD = decltype(model_c)::value;
         with_nmf(p.M, [&](auto nc) {
           constexpr int NMF = decltype(nc)::value;
-          auto go = [&](auto kern, size_t smem) {
-            kern<<<g, kTmaTile, smem, st>>>(p, chan, deriv, a, err_, p0, pn, blk0, nblk);
-          };
-          if (pw_variant_ == 1) {
-            if (vext)
-              go(k_pointwise1_tma<MD, NMF, true, 5>, tma1_smem_v_);
-            else
-              go(k_pointwise1_tma<MD, NMF, false, 5>, tma1_smem_);
+          const int v = pw_variant_;
+          const size_t smem = v == 4 ? (vext ? tma1_smem2_v_ : tma1_smem2_) : (vext ? tma1_smem_v_ : tma1_smem_);
+          auto go = [&](auto kern) { kern<<<g, kTmaTile, smem, st>>>(p, chan, deriv, a, err_, p0, pn, blk0, nblk); };
+          if (vext) {
+            if (v == 1) go(k_pointwise1_tma<MD, NMF, true, 5>);
+            else if (v == 2) go(k_pointwise1_tma<MD, NMF, true, 6>);
+            else if (v == 3) go(k_pointwise1_tma<MD, NMF, true, 5, 1, true>);
+            else go(k_pointwise1_tma<MD, NMF, true, 3, 2, true>);
           } else {
-            if (vext)
-              go(k_pointwise1_tma<MD, NMF, true, 6>, tma1_smem_v_);
-            else
-              go(k_pointwise1_tma<MD, NMF, false, 6>, tma1_smem_);
+            if (v == 1) go(k_pointwise1_tma<MD, NMF, false, 5>);
+            else if (v == 2) go(k_pointwise1_tma<MD, NMF, false, 6>);
+            else if (v == 3) go(k_pointwise1_tma<MD, NMF, false, 5, 1, true>);
+            else go(k_pointwise1_tma<MD, NMF, false, 3, 2, true>);
           }
         });
       });
@@ -304,23 +304,26 @@ Engine::Engine(const EngineSpec& spec) {
         constexpr int NMF = decltype(nc)::value;
         const int sb = kTmaStages * tma1_stage_bytes<NMF, false, TE>();
         const int sv = kTmaStages * tma1_stage_bytes<NMF, true, TE>();
-        CDFT_CUDA(cudaFuncSetAttribute(k_pointwise1_tma<MD, NMF, false, 5>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, sb));
-        CDFT_CUDA(cudaFuncSetAttribute(k_pointwise1_tma<MD, NMF, true, 5>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, sv));
-        CDFT_CUDA(cudaFuncSetAttribute(k_pointwise1_tma<MD, NMF, false, 6>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, sb));
-        CDFT_CUDA(cudaFuncSetAttribute(k_pointwise1_tma<MD, NMF, true, 6>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, sv));
-        int per5 = 0, per6 = 0;
-        CDFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per5, k_pointwise1_tma<MD, NMF, true, 5>, kTmaTile,
-                                                                sv));
-        CDFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per6, k_pointwise1_tma<MD, NMF, true, 6>, kTmaTile,
-                                                                sv));
-        grid_pw1_[0] = per_problem((long long)sms * std::max(per5, 1));
-        grid_pw1_[1] = per_problem((long long)sms * std::max(per6, 1));
-        tma1_smem_ = (size_t)kTmaStages * tma1_stage_bytes<NMF, false, TE>();
-        tma1_smem_v_ = (size_t)kTmaStages * tma1_stage_bytes<NMF, true, TE>();
+        const int sb2 = kTmaStages * tma1_stage_bytes<NMF, false, TE, 2>();
+        const int sv2 = kTmaStages * tma1_stage_bytes<NMF, true, TE, 2>();
+        // the occupancy of the vext form (the larger stages) sizes both forms' grids
+        int per[4] = {0, 0, 0, 0};
+        auto prep = [&](auto kb, auto kv, int b, int v, int* out) {
+          CDFT_CUDA(cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+          CDFT_CUDA(cudaFuncSetAttribute(kv, cudaFuncAttributeMaxDynamicSharedMemorySize, v));
+          CDFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, kv, kTmaTile, v));
+        };
+        prep(k_pointwise1_tma<MD, NMF, false, 5>, k_pointwise1_tma<MD, NMF, true, 5>, sb, sv, &per[0]);
+        prep(k_pointwise1_tma<MD, NMF, false, 6>, k_pointwise1_tma<MD, NMF, true, 6>, sb, sv, &per[1]);
+        prep(k_pointwise1_tma<MD, NMF, false, 5, 1, true>, k_pointwise1_tma<MD, NMF, true, 5, 1, true>, sb, sv,
+             &per[2]);
+        prep(k_pointwise1_tma<MD, NMF, false, 3, 2, true>, k_pointwise1_tma<MD, NMF, true, 3, 2, true>, sb2, sv2,
+             &per[3]);
+        for (int v = 0; v < 4; ++v) grid_pw1_[v] = per_problem((long long)sms * std::max(per[v], 1));
+        tma1_smem_ = (size_t)sb;
+        tma1_smem_v_ = (size_t)sv;
+        tma1_smem2_ = (size_t)sb2;
+        tma1_smem2_v_ = (size_t)sv2;
       });
     });
     pw_variant_ = 1;
@@ -333,7 +336,8 @@ Engine::Engine(const EngineSpec& spec) {
   // (a plane chunk may take the whole pointwise grid: kMaxChunks grids)
   partials_ = dalloc<double>(
       (size_t)B *
-          ((size_t)std::max({grid_pw_, grid_tma_, grid_stream_, grid_pw1_[0], grid_pw1_[1]}) * kMaxChunks + 8) *
+          ((size_t)std::max({grid_pw_, grid_tma_, grid_stream_, grid_pw1_[0], grid_pw1_[1], grid_pw1_[2],
+                             grid_pw1_[3]}) * kMaxChunks + 8) *
           p.n_terms,
       tot);
   err_ = dalloc<int>(1, tot);
@@ -576,7 +580,7 @@ void Engine::set_col_tile(int tq) {
 int Engine::col_tile() const { return fusable_ ? plan_.tq : 0; }
 
 void Engine::set_pointwise(int v) {
-  if (v < 0 || v >= kPointwiseVariants) throw std::invalid_argument("pointwise variant: 0, 1 or 2");
+  if (v < 0 || v >= kPointwiseVariants) throw std::invalid_argument("pointwise variant: 0 .. 4");
   if (v > 0 && !pw1_)
     throw std::invalid_argument("pointwise variant: the one-species kernel needs a mixed-precision engine with one "
                                 "species and at most two interactions");

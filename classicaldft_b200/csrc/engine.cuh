@@ -107,7 +107,7 @@ class Engine {
   // Several species also tune the column tile width (16, 32), and every
   // chunk count k its pointwise spread d (1, 2, 4, 8 up to k):
   // ms[((tile_index * kPointwiseVariants + v) * kMaxChunks + k - 1) * kSpreads + log2 d].
-  static constexpr int kPointwiseVariants = 3;
+  static constexpr int kPointwiseVariants = 5;
   static constexpr int kSpreads = 4;
   int autotune(const double* rho, const double* vext, const double* mu, cudaStream_t stream, int reps,
                double* ms, int* variant, int* tile = nullptr, int* spread = nullptr);
@@ -123,8 +123,10 @@ class Engine {
   // several species where their spectra fit); std::invalid_argument otherwise.
   void set_col_tile(int tq);
   int col_tile() const;
-  // Pointwise kernel of the TMA path: 0 generic, 1 / 2 one-species (5 / 6
-  // CTAs per SM); std::invalid_argument where the variant does not exist.
+  // Pointwise kernel of the TMA path: 0 generic; one species: 1 / 2 sized
+  // for 5 / 6 CTAs per SM, 3 the branch-free FP64 path for warps with eta >=
+  // 1e-6 everywhere (5 CTAs per SM), 4 the same with two points per thread
+  // (3 CTAs per SM); std::invalid_argument where the variant does not exist.
   void set_pointwise(int v);
   int pointwise() const { return pw_variant_; }
   bool pointwise_one_species() const { return pw1_; }
@@ -219,12 +221,13 @@ class Engine {
   // grid_* are CTAs per problem: a launch has grid_* x B CTAs
   size_t tma_smem_ = 0, tma_smem_v_ = 0;
   bool pw1_ = false;  // one species, <= 2 mean-field channels, mixed: k_pointwise1_tma exists
-  // pointwise kernel of the TMA path: 0 generic (k_pointwise_tma), 1 / 2 the
-  // one-species kernel sized for 5 / 6 CTAs per SM (grid grid_pw1_[v - 1])
+  // pointwise kernel of the TMA path: 0 generic (k_pointwise_tma), 1 .. 4
+  // the one-species kernel k_pointwise1_tma (grid grid_pw1_[v - 1])
   int pw_variant_ = 0;
   int pw_div_ = 0;  // pointwise grid divisor of a plane chunk (0: the chunk count)
-  int grid_pw1_[2] = {0, 0};
-  size_t tma1_smem_ = 0, tma1_smem_v_ = 0;
+  int grid_pw1_[4] = {0, 0, 0, 0};
+  size_t tma1_smem_ = 0, tma1_smem_v_ = 0;    // one point per thread
+  size_t tma1_smem2_ = 0, tma1_smem2_v_ = 0;  // two points per thread
   template <typename R>
   void launch_pointwise_tma(const R* chan, R* deriv, const PointwiseArgs& a, long long p0, long long pn, int blk0,
                             int nblk, int grid, cudaStream_t st);

@@ -940,15 +940,82 @@ __global__ void __launch_bounds__(kTmaTile, 5) k_pointwise_tma(EvalParams p, con
 // species or interaction loops and no runtime channel selection (the common
 // case of every benchmark workload).  Same arithmetic as point_body's
 // one-species branch, so the results equal the generic kernel's.
-template <int NMF, bool HAS_V, bool TENSOR>
+//
+// PTS points per thread (a tile of PTS * kTmaTile points): the FP64 chains
+// of the points are independent, so the scheduler can interleave them.
+// FAST: a warp whose points all have eta >= 1e-6 takes the branch-free
+// path of fmt_phi_dphi (no Taylor branch, no skip, one reciprocal for
+// 1/eta and 1/(1 - eta)); other warps take the exact path.  FAST results
+// may differ from the exact path's in the last bit of the FP64 values.
+template <int NMF, bool HAS_V, bool TENSOR, int PTS = 1>
 __host__ __device__ constexpr int tma1_stage_bytes() {
-  return (Lay<false, TENSOR>::NFMT + NMF) * kTmaTile * 4 + kTmaTile * 8 * (HAS_V ? 2 : 1);
+  return ((Lay<false, TENSOR>::NFMT + NMF) * kTmaTile * 4 + kTmaTile * 8 * (HAS_V ? 2 : 1)) * PTS;
 }
 
-// MINB: the CTAs per SM the register allocation is sized for (5: 96
-// registers, no spills; 6: 80 registers with a few spills) -- the
-// autotuner picks one per engine shape.
-template <int MODEL, int NMF, bool HAS_V, int MINB>
+// Phi/dPhi and the local terms at one point of the one-species kernel:
+// derivative channels minus their split constants out (FP32), the local
+// force terms out (FP64), the five partial sums accumulated where `live`.
+template <int MODEL, int NMF, bool HAS_V, bool FAST>
+__device__ __forceinline__ void pw1_point(const EvalParams& p, const double* n, double r, double v, bool live,
+                                          const double* dbar, float* __restrict__ deriv, double* __restrict__ force,
+                                          long long idx, long long N, double (&acc)[5]) {
+  constexpr bool TENSOR = model_has_tensor(MODEL);
+  using L = Lay<false, TENSOR>;
+  constexpr int NF = L::NFMT;
+  Measures<double> m;
+  m.eta = n[L::ETA];
+  m.n2 = n[L::N2];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) m.v1[c] = n[L::V1 + c];
+  if constexpr (TENSOR) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) m.t[c] = n[L::T + c];
+    m.t[5] = m.n2 - m.t[0] - m.t[3];
+  } else {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) m.t[c] = 0.0;
+  }
+  double phi = 0.0;
+  MeasureDerivs<double> dm;
+  double D[NF];
+  if (fmt_phi_dphi<MODEL, double, true, FAST>(p.A, p.B, m, phi, dm, p.inv4piR2[0], p.inv4piR[0])) {
+    const double dzz = TENSOR ? dm.d_t[5] : 0.0;
+    D[L::ETA] = dm.d_eta;
+    D[L::N2] = dm.d_n2 + dzz;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) D[L::V1 + c] = dm.d_v1[c];
+    if constexpr (TENSOR) {
+      D[L::T + 0] = dm.d_t[0] - dzz;
+      D[L::T + 1] = 2.0 * dm.d_t[1];
+      D[L::T + 2] = 2.0 * dm.d_t[2];
+      D[L::T + 3] = dm.d_t[3] - dzz;
+      D[L::T + 4] = 2.0 * dm.d_t[4];
+    }
+  } else {
+    phi = 0.0;
+#pragma unroll
+    for (int c = 0; c < NF; ++c) D[c] = 0.0;
+  }
+  const double lr = log(r < 1e-300 ? 1e-300 : r);
+  double f0 = lr + v;  // -mu dV is added by k_epilogue
+#pragma unroll
+  for (int q = 0; q < NMF; ++q) f0 += n[NF + q];
+  if (live) {
+    acc[kTermHS] += phi;
+#pragma unroll
+    for (int c = 0; c < NF; ++c) __stcs(deriv + c * N + idx, (float)(D[c] - dbar[c]));
+    acc[kTermId] += r * (lr - 1.0);
+    acc[kTermExt] += r * v;
+    acc[kTermN0] += r;
+#pragma unroll
+    for (int q = 0; q < NMF; ++q) acc[kTermMF] += 0.5 * r * n[NF + q];
+    __stcs(force + idx, f0 * p.dv);
+  }
+}
+
+// MINB: the CTAs per SM the register allocation is sized for; the variants
+// (PTS, FAST, MINB) are chosen per engine shape by the autotuner.
+template <int MODEL, int NMF, bool HAS_V, int MINB, int PTS = 1, bool FAST = false>
 __global__ void __launch_bounds__(kTmaTile, MINB) k_pointwise1_tma(EvalParams p, const float* __restrict__ chan,
                                                              float* __restrict__ deriv, PointwiseArgs a_all,
                                                              int* err, long long p0, long long pn, int blk0,
@@ -956,10 +1023,11 @@ __global__ void __launch_bounds__(kTmaTile, MINB) k_pointwise1_tma(EvalParams p,
   constexpr bool TENSOR = model_has_tensor(MODEL);
   using L = Lay<false, TENSOR>;
   constexpr int NF = L::NFMT;
-  constexpr int NIN = NF + NMF;                      // float segments per tile
-  constexpr int RHO_OFF = NIN * kTmaTile * 4;
-  constexpr int V_OFF = RHO_OFF + kTmaTile * 8;
-  constexpr int STAGE = tma1_stage_bytes<NMF, HAS_V, TENSOR>();
+  constexpr int NIN = NF + NMF;  // float segments per tile
+  constexpr int TP = kTmaTile * PTS;  // points per tile
+  constexpr int RHO_OFF = NIN * TP * 4;
+  constexpr int V_OFF = RHO_OFF + TP * 8;
+  constexpr int STAGE = tma1_stage_bytes<NMF, HAS_V, TENSOR, PTS>();
   constexpr int NT = 5;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bars[kTmaStages];
@@ -973,7 +1041,7 @@ __global__ void __launch_bounds__(kTmaTile, MINB) k_pointwise1_tma(EvalParams p,
   chan += (long long)blockIdx.y * p.n_chan * p.N;
   deriv += (long long)blockIdx.y * NF * p.N;
   const long long N = p.N;
-  const long long ntiles = (pn + kTmaTile - 1) / kTmaTile;
+  const long long ntiles = (pn + TP - 1) / TP;
   const long long mine = (blockIdx.x < ntiles) ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const int tid = threadIdx.x;
   if (tid == 0) {
@@ -990,14 +1058,14 @@ __global__ void __launch_bounds__(kTmaTile, MINB) k_pointwise1_tma(EvalParams p,
 
   auto issue = [&](long long i) {  // local tile i -> stage i % kTmaStages
     const int st = (int)(i % kTmaStages);
-    const long long start = p0 + (blockIdx.x + i * gridDim.x) * kTmaTile;
-    const long long cnt = (p0 + pn - start) < kTmaTile ? (p0 + pn - start) : kTmaTile;
+    const long long start = p0 + (blockIdx.x + i * gridDim.x) * TP;
+    const long long cnt = (p0 + pn - start) < TP ? (p0 + pn - start) : TP;
     const uint32_t cb = (uint32_t)(cnt * 4), db = (uint32_t)(cnt * 8);
     unsigned char* base = smem + (size_t)st * STAGE;
     s_issued[st] = i;
     mbar_arrive_expect_tx(&bars[st], cb * NIN + db * (HAS_V ? 2 : 1));
 #pragma unroll
-    for (int q = 0; q < NIN; ++q) bulk_copy_g2s(base + q * kTmaTile * 4, chan + q * N + start, cb, &bars[st]);
+    for (int q = 0; q < NIN; ++q) bulk_copy_g2s(base + q * TP * 4, chan + q * N + start, cb, &bars[st]);
     bulk_copy_g2s(base + RHO_OFF, a.rho + start, db, &bars[st]);
     if constexpr (HAS_V) bulk_copy_g2s(base + V_OFF, a.vext + start, db, &bars[st]);
   };
@@ -1016,70 +1084,42 @@ __global__ void __launch_bounds__(kTmaTile, MINB) k_pointwise1_tma(EvalParams p,
   volatile int* fail = &s_fail;
   int st = 0;
   uint32_t par = 0;
-  long long idx = p0 + (long long)blockIdx.x * kTmaTile + tid;
-  const long long idx_step = (long long)gridDim.x * kTmaTile, idx_end = p0 + pn;
+  long long idx = p0 + (long long)blockIdx.x * TP + tid;
+  const long long idx_step = (long long)gridDim.x * TP, idx_end = p0 + pn;
   for (long long i = 0; i < mine; ++i, idx += idx_step) {
-    if (*fail) break;
-    if (!mbar_wait_bounded(&bars[st], par, kWaitLimit)) {
+    // every exit decision is warp-uniform, so the warp stays converged for
+    // the vote and the warp barrier below
+    if (__any_sync(0xffffffffu, *fail != 0)) break;
+    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bars[st], par, kWaitLimit))) {
       *fail = 1;
       break;
     }
-    if (idx < idx_end) {
-      const unsigned char* base = smem + (size_t)st * STAGE;
-      const float* cs = reinterpret_cast<const float*>(base) + tid;
-      double n[NIN];
+    const unsigned char* base = smem + (size_t)st * STAGE;
+    double n[PTS][NIN], r[PTS], v[PTS];
+    bool live[PTS];
+    bool lane_fast = true;
 #pragma unroll
-      for (int c = 0; c < NIN; ++c) n[c] = (double)cs[c * kTmaTile] + off[c];
-      const double r = reinterpret_cast<const double*>(base + RHO_OFF)[tid];
-      const double v = HAS_V ? reinterpret_cast<const double*>(base + V_OFF)[tid] : 0.0;
-      Measures<double> m;
-      m.eta = n[L::ETA];
-      m.n2 = n[L::N2];
+    for (int j = 0; j < PTS; ++j) {
+      const int o = tid + j * kTmaTile;
+      live[j] = idx + j * kTmaTile < idx_end;
+      const float* cs = reinterpret_cast<const float*>(base) + o;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) m.v1[c] = n[L::V1 + c];
-      if constexpr (TENSOR) {
+      for (int c = 0; c < NIN; ++c) n[j][c] = (double)cs[c * TP] + off[c];
+      r[j] = reinterpret_cast<const double*>(base + RHO_OFF)[o];
+      v[j] = HAS_V ? reinterpret_cast<const double*>(base + V_OFF)[o] : 0.0;
+      lane_fast = lane_fast && (!live[j] || n[j][L::ETA] >= 1e-6);
+    }
+    if (FAST && __all_sync(0xffffffffu, lane_fast)) {
 #pragma unroll
-        for (int c = 0; c < 5; ++c) m.t[c] = n[L::T + c];
-        m.t[5] = m.n2 - m.t[0] - m.t[3];
-      } else {
+      for (int j = 0; j < PTS; ++j)
+        pw1_point<MODEL, NMF, HAS_V, true>(p, n[j], r[j], v[j], live[j], dbar, deriv, a.force,
+                                           idx + j * kTmaTile, N, acc);
+    } else {
 #pragma unroll
-        for (int c = 0; c < 6; ++c) m.t[c] = 0.0;
-      }
-      double phi = 0.0;
-      MeasureDerivs<double> dm;
-      double D[NF];
-      if (fmt_phi_dphi<MODEL, double, true>(p.A, p.B, m, phi, dm, p.inv4piR2[0], p.inv4piR[0])) {
-        const double dzz = TENSOR ? dm.d_t[5] : 0.0;
-        D[L::ETA] = dm.d_eta;
-        D[L::N2] = dm.d_n2 + dzz;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) D[L::V1 + c] = dm.d_v1[c];
-        if constexpr (TENSOR) {
-          D[L::T + 0] = dm.d_t[0] - dzz;
-          D[L::T + 1] = 2.0 * dm.d_t[1];
-          D[L::T + 2] = 2.0 * dm.d_t[2];
-          D[L::T + 3] = dm.d_t[3] - dzz;
-          D[L::T + 4] = 2.0 * dm.d_t[4];
-        }
-      } else {
-        phi = 0.0;
-#pragma unroll
-        for (int c = 0; c < NF; ++c) D[c] = 0.0;
-      }
-      acc[kTermHS] += phi;
-#pragma unroll
-      for (int c = 0; c < NF; ++c) __stcs(deriv + c * N + idx, (float)(D[c] - dbar[c]));
-      const double lr = log(r < 1e-300 ? 1e-300 : r);
-      acc[kTermId] += r * (lr - 1.0);
-      acc[kTermExt] += r * v;
-      acc[kTermN0] += r;
-      double f0 = lr + v;  // -mu dV is added by k_epilogue
-#pragma unroll
-      for (int q = 0; q < NMF; ++q) {
-        acc[kTermMF] += 0.5 * r * n[NF + q];
-        f0 += n[NF + q];
-      }
-      __stcs(a.force + idx, f0 * p.dv);
+      for (int j = 0; j < PTS; ++j)
+        if (live[j])
+          pw1_point<MODEL, NMF, HAS_V, false>(p, n[j], r[j], v[j], true, dbar, deriv, a.force,
+                                              idx + j * kTmaTile, N, acc);
     }
     // this warp is done reading stage st; the last warp out refills it
     __syncwarp();

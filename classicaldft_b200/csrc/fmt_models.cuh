@@ -75,23 +75,33 @@ struct FVals {
 // log(1 - eta), 1/(1 - eta) and 1/eta are formed once; every other quotient
 // of the reference's expressions is rewritten with these reciprocals, which
 // keeps the FP64 division count at two per point.
-template <int MODEL, class T>
+// FAST: the caller guarantees eta >= 1e-6 (no Taylor branch), and the two
+// reciprocals come from one: 1/(eta e) times e or eta.
+template <int MODEL, class T, bool FAST = false>
 __host__ __device__ __forceinline__ FVals<T> fmt_f(T eta) {
   constexpr int model = MODEL;
+  constexpr bool needs_ih = model != kRosenfeld && model != kEsFMT;
   FVals<T> r;
   const double ev = val(eta);
   const T e = 1.0 - eta;
-  const T ie = 1.0 / e;
+  T ie, ih = cst<T>(0.0), ih2 = cst<T>(0.0);
+  const bool taylor = FAST ? false : ev < 1e-6;
+  if constexpr (FAST && needs_ih) {
+    const T rr = 1.0 / (eta * e);
+    ie = eta * rr;
+    ih = e * rr;
+    ih2 = ih * ih;
+  } else {
+    ie = 1.0 / e;
+    if (!taylor && needs_ih) {  // 1/eta only where it is used
+      ih = 1.0 / eta;
+      ih2 = ih * ih;
+    }
+  }
   const T ie2 = ie * ie;
   const T lg = dlog(e);
   r.f1 = lg;
   r.df1 = -ie;
-  const bool taylor = ev < 1e-6;
-  T ih = cst<T>(0.0), ih2 = cst<T>(0.0);
-  if (!taylor && model != kRosenfeld && model != kEsFMT) {  // 1/eta only where it is used
-    ih = 1.0 / eta;
-    ih2 = ih * ih;
-  }
   if constexpr (model == kWhiteBearII) {
     if (taylor) {
       r.f2 = 1.0 + eta * (1.0 + eta * (10.0 / 9.0 + (7.0 / 6.0) * eta));
@@ -145,12 +155,13 @@ __host__ __device__ __forceinline__ FVals<T> fmt_f(T eta) {
 // chains folded in (d_n0, d_n1, d_v0 zero):
 //   Phi = -a0 n2 f1 + a1 (n2^2 - v1.v1) f2 + Phi3 f3,
 //   d_n2 = -a0 f1 + 2 a1 n2 f2 + dPhi3/dn2 f3,  d_v1 = -2 a1 f2 v1 + dPhi3/dv1 f3.
-template <int MODEL, class T, bool ONE = false>
+// FAST: the caller guarantees eta >= 1e-6 (see fmt_f); always returns true.
+template <int MODEL, class T, bool ONE = false, bool FAST = false>
 __host__ __device__ __forceinline__ bool fmt_phi_dphi(double A, double B, const Measures<T>& m, T& phi,
                                                       MeasureDerivs<T>& dm, double a0 = 0.0, double a1 = 0.0) {
   constexpr int model = MODEL;
   constexpr bool tensor = model_has_tensor(MODEL);
-  if (val(m.eta) < 1e-30) return false;
+  if (!FAST && val(m.eta) < 1e-30) return false;
   constexpr double INV_24PI = 1.0 / (24.0 * kPi);
   constexpr double INV_8PI = 1.0 / (8.0 * kPi);
   constexpr double INV_4PI = 1.0 / (4.0 * kPi);
@@ -216,7 +227,7 @@ __host__ __device__ __forceinline__ bool fmt_phi_dphi(double A, double B, const 
     for (int a = 0; a < 3; ++a) dp3_v[a] = INV_24PI * A * (-6.0 * n2 * m.v1[a] + 6.0 * tv[a]);
   }
 
-  FVals<T> f = fmt_f<MODEL, T>(m.eta);
+  FVals<T> f = fmt_f<MODEL, T, FAST>(m.eta);
   if constexpr (ONE) {
     const T c2 = a1 * (n2 * n2 - dot11);
     const T n0 = a0 * n2;
