@@ -738,8 +738,10 @@ __global__ void __launch_bounds__(256, 2)
             const cpx r = R[(size_t)mf_sp * TILE + kx * TQ + q];
             acc = cpx{w * r.x, w * r.y};
           } else {
-            const bool xnyq = (p.nx % 2 == 0) && kx == p.nx / 2;
-            const RKv v = rk_element(dkx * (float)(kx <= p.nx / 2 ? kx : kx - p.nx), xnyq, col.ky, col.ynyq, col.kz,
+            // (NX equals p.nx here; the constant lets the compiler fold the
+            // element's sign and Nyquist tests)
+            const bool xnyq = (NX % 2 == 0) && kx == NX / 2;
+            const RKv v = rk_element(dkx * (float)(kx <= NX / 2 ? kx : kx - NX), xnyq, col.ky, col.ynyq, col.kz,
                                      col.proj);
 #pragma unroll
             for (int s = 0; s < (MULTI ? kMaxSpecies : 1); ++s) {
@@ -821,9 +823,8 @@ __global__ void __launch_bounds__(256, 2)
       for (int k2 = 0; k2 < BX; ++k2) {
         const int kx = k1 + AX * k2;
         const long long kidx = (long long)kx * plane + q0 + q;
-        const bool xnyq = (p.nx % 2 == 0) && kx == p.nx / 2;
-        const RKv v =
-            rk_element(dkx * (float)(kx <= p.nx / 2 ? kx : kx - p.nx), xnyq, col.ky, col.ynyq, col.kz, col.proj);
+        const bool xnyq = (NX % 2 == 0) && kx == NX / 2;
+        const RKv v = rk_element(dkx * (float)(kx <= NX / 2 ? kx : kx - NX), xnyq, col.ky, col.ynyq, col.kz, col.proj);
 #pragma unroll
         for (int s = 0; s < (MULTI ? kMaxSpecies : 1); ++s) {
           if (s < S) {
@@ -904,10 +905,12 @@ __device__ __forceinline__ RTab<RCol1<NX, TQ>::BX> rk_task_table(const float* __
   return t;
 }
 
+// Element kx of a column (NX = p.nx: the compile-time length folds the sign
+// and Nyquist tests of the unrolled elements).
 template <int NX>
-__device__ __forceinline__ RKv rk_task_element(const EvalParams& p, int kx, float dkx, const RColumn& col) {
-  const bool xnyq = (p.nx % 2 == 0) && kx == p.nx / 2;
-  return rk_element(dkx * (float)(kx <= p.nx / 2 ? kx : kx - p.nx), xnyq, col.ky, col.ynyq, col.kz, col.proj);
+__device__ __forceinline__ RKv rk_task_element(const EvalParams&, int kx, float dkx, const RColumn& col) {
+  const bool xnyq = (NX % 2 == 0) && kx == NX / 2;
+  return rk_element(dkx * (float)(kx <= NX / 2 ? kx : kx - NX), xnyq, col.ky, col.ynyq, col.kz, col.proj);
 }
 
 // Column bases.  Along one column (ky, kz fixed) every FMT weight of one
