@@ -264,6 +264,50 @@ inline Result total(const physics::Model& model, const State& state, const Weigh
   return r;
 }
 
+// `total` for a sequence of states (cdft_total_stream): the copies of one
+// state overlap the evaluation of the next; one Result per state, equal to
+// `total` on each.
+inline std::vector<Result> total_stream(const physics::Model& model, const std::vector<State>& states,
+                                        const Weights& weights) {
+  const std::size_t S = model.species.size();
+  const std::size_t N = static_cast<std::size_t>(model.grid.total_points());
+  const std::size_t K = states.size();
+  std::vector<std::vector<double>> rho(K), vext(K), force(K, std::vector<double>(S * N));
+  std::vector<const double*> rp(K), vp(K, nullptr);
+  std::vector<double*> fp(K);
+  std::vector<double> mu(K * S), sc(K * CDFT_SCALAR_COUNT);
+  for (std::size_t i = 0; i < K; ++i) {
+    const State& st = states[i];
+    if (st.species.size() != S) throw std::invalid_argument("total_stream: one SpeciesState per species");
+    rho[i].resize(S * N);
+    for (std::size_t s = 0; s < S; ++s) {
+      const auto& sp = st.species[s];
+      if (sp.values.size() != N) throw std::invalid_argument("total_stream: density has the wrong size");
+      std::memcpy(rho[i].data() + s * N, sp.values.data(), sizeof(double) * N);
+      if (!sp.external_field.empty()) {
+        if (sp.external_field.size() != N)
+          throw std::invalid_argument("total_stream: external field has the wrong size");
+        if (vext[i].empty()) vext[i].assign(S * N, 0.0);
+        std::memcpy(vext[i].data() + s * N, sp.external_field.data(), sizeof(double) * N);
+      }
+      mu[i * S + s] = sp.chemical_potential;
+    }
+    rp[i] = rho[i].data();
+    vp[i] = vext[i].empty() ? nullptr : vext[i].data();
+    fp[i] = force[i].data();
+  }
+  check(cdft_total_stream(weights.engine(), static_cast<int>(K), rp.data(), vp.data(), mu.data(), fp.data(),
+                          sc.data()));
+  std::vector<Result> out(K);
+  for (std::size_t i = 0; i < K; ++i) {
+    out[i].free_energy = sc[i * CDFT_SCALAR_COUNT];
+    out[i].grand_potential = sc[i * CDFT_SCALAR_COUNT + 1];
+    for (std::size_t s = 0; s < S; ++s)
+      out[i].forces.emplace_back(force[i].begin() + s * N, force[i].begin() + (s + 1) * N);
+  }
+  return out;
+}
+
 using ForceCallback = std::function<std::pair<double, std::vector<std::vector<double>>>(
     const std::vector<std::vector<double>>&)>;
 

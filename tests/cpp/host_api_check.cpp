@@ -70,6 +70,22 @@ int main(int argc, char** argv) {
     const auto cb = func.grand_potential_callback(0.7);
     std::printf("callback_omega=%.17g\n", cb({rho}).first);
 
+    // 1b. total_stream: three states (with, without the field, scaled) equal to total on each
+    {
+      std::vector<d::functionals::State> states(3, st);
+      states[1].species[0].external_field.clear();
+      for (double& v : states[2].species[0].values) v *= 1.01;
+      states[2].species[0].chemical_potential = 0.2;
+      const auto rs = d::functionals::total_stream(model, states, *func.weights);
+      int equal = rs.size() == 3;
+      for (std::size_t i = 0; i < rs.size(); ++i) {
+        const auto one = d::functionals::total(model, states[i], *func.weights);
+        equal = equal && one.free_energy == rs[i].free_energy && one.grand_potential == rs[i].grand_potential &&
+                one.forces == rs[i].forces;
+      }
+      std::printf("stream_equal=%d\n", equal);
+    }
+
     // 2. FIRE2 grand-potential minimisation
     d::algorithms::minimization::Minimizer mz;
     mz.fire.dt = 0.05;
