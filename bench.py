@@ -526,6 +526,17 @@ def config_wall(cd, torch):
     a, b = res["fp64"], res["mixed_refined"]
     out["mixed_vs_fp64"] = {"max_drho": float(np.max(np.abs(a.densities[0] - b.densities[0]))),
                             "dOmega_over_Omega": abs(a.grand_potential - b.grand_potential) / abs(a.grand_potential)}
+    # two profiles that both meet rms 1e-10 differ by up to ~1e-8 (the
+    # criterion's tolerance ball); both converged to 1e-11 they agree closer
+    tight = cd.Fire(dt=0.1, dt_max=1.0, alpha_start=0.01, f_alpha=0.99, force_tolerance=1e-11, max_steps=50000)
+    tr = {}
+    for label, w, ref in (("fp64", w64, None), ("mixed_refined", wmx, w64)):
+        tr[label] = cd.Minimizer(fire=tight, refine=ref, refine_switch=1e3, use_homogeneous_boundary=False,
+                                 use_monitor=False).grand_potential(model, w, rho0, mu, external_field=vext)
+    out["mixed_vs_fp64_at_1e-11"] = {
+        "iterations": [tr["fp64"].iterations, tr["mixed_refined"].iterations],
+        "converged": tr["fp64"].converged and tr["mixed_refined"].converged,
+        "max_drho": float(np.max(np.abs(tr["fp64"].densities[0] - tr["mixed_refined"].densities[0])))}
     for w in (w64, wmx):
         w.engine.close()
     return out

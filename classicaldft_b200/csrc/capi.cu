@@ -389,6 +389,28 @@ int cdft_engine_autotune_ex(cdft_engine* engine, const double* rho, const double
   });
 }
 
+int cdft_engine_set_anchor(cdft_engine* engine, cdft_engine* fp64_engine, const double* rho_anchor, void* stream) {
+  return guarded([&] {
+    if (!engine || !fp64_engine || !rho_anchor)
+      throw std::invalid_argument("anchor: engine, the FP64 engine and rho_anchor are required");
+    engine->impl->set_anchor(*fp64_engine->impl, rho_anchor, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int cdft_engine_clear_anchor(cdft_engine* engine) {
+  return guarded([&] {
+    if (!engine) throw std::invalid_argument("engine is NULL");
+    engine->impl->clear_anchor();
+  });
+}
+
+int cdft_engine_anchored(const cdft_engine* engine, int* anchored) {
+  return guarded([&] {
+    if (!engine || !anchored) throw std::invalid_argument("engine and anchored are required");
+    *anchored = engine->impl->anchored() ? 1 : 0;
+  });
+}
+
 int cdft_engine_set_pointwise_spread(cdft_engine* engine, int spread) {
   return guarded([&] {
     if (!engine) throw std::invalid_argument("engine is NULL");

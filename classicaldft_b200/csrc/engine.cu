@@ -145,7 +145,7 @@ void Engine::launch_pointwise_tma(const R* chan, R* deriv, const PointwiseArgs& 
   const bool vext = a.vext != nullptr;
   const dim3 g(grid, p.batch);
   if constexpr (std::is_same_v<R, float>) {
-    if (pw1_ && pw_variant_ > 0) {
+    if (pw1_ && pw_variant_ > 0 && !a.n_anc) {
       with_kernels(true, [&](auto model_c, auto, auto) {
         constexpr int MD = decltype(model_c)::value;
         with_nmf(p.M, [&](auto nc) {
@@ -367,7 +367,8 @@ Engine::~Engine() {
   for (void* q : {rho_k_, chan_k_, chan_r_, deriv_r_, deriv_k_, force_k_, hs_r_, rho_lo_, (void*)mf_w_,
                   (void*)mean_, (void*)dbar_, (void*)err_, (void*)sync_, tan_chan_, (void*)tan_mean_, (void*)tan_dbar_,
                   (void*)tan_in_,
-                  (void*)partials_, fft_work_, tw_, (void*)wtab_, (void*)pmean_, (void*)h_rho_, (void*)h_vext_, (void*)h_force_, (void*)h_scalars_})
+                  (void*)partials_, fft_work_, tw_, (void*)wtab_, (void*)pmean_, (void*)h_rho_, (void*)h_vext_, (void*)h_force_, (void*)h_scalars_,
+                  (void*)anc_rho_, (void*)anc_n_, (void*)anc_d_, (void*)anc_hs_})
     if (q) cudaFree(q);
   if (stream_) cudaStreamDestroy(stream_);
   for (cudaStream_t st : aux_) cudaStreamDestroy(st);
@@ -701,7 +702,8 @@ void Engine::upload_mean_field(const EngineSpec& spec) {
 // doubles) in real space.  Mixed precision transforms in - mean in FP32 and
 // stores the species means in `mean_out`.
 template <typename R, typename C2>
-void Engine::forward_stage(const double* in, R* chan_out, double* mean_out, cudaStream_t stream) {
+void Engine::forward_stage(const double* in, R* chan_out, double* mean_out, cudaStream_t stream,
+                           const double* anchor) {
   const EvalParams& p = p_;
   constexpr bool mixed = sizeof(R) == sizeof(float);
   C2* rho_k = static_cast<C2*>(rho_k_);
@@ -709,7 +711,7 @@ void Engine::forward_stage(const double* in, R* chan_out, double* mean_out, cuda
   if constexpr (mixed) {
     const dim3 gs(grid_stream_, p.batch);
     k_species_mean<<<dim3(grid_mean_, p.batch), 256, 0, stream>>>(in, p.N, p.S, partials_, sync_, mean_out);
-    k_split_convert<<<gs, 256, 0, stream>>>(in, p.N, p.S, static_cast<float*>(rho_lo_), mean_out);
+    k_split_convert<<<gs, 256, 0, stream>>>(in, p.N, p.S, static_cast<float*>(rho_lo_), mean_out, anchor);
     mark(1, stream);
     CDFT_CUFFT(cufftExecR2C(plan_rho_, static_cast<float*>(rho_lo_), reinterpret_cast<cufftComplex*>(rho_k)));
   } else {
@@ -737,7 +739,7 @@ void Engine::forward_stage(const double* in, R* chan_out, double* mean_out, cuda
 // FP64 constants of the split derivative channels, `dbar`).
 template <typename R, typename C2>
 void Engine::backward_stage(R* deriv, const double* dbar, double* out, const MuArgs& mu, const FinalArgs& fin,
-                            cudaStream_t stream) {
+                            cudaStream_t stream, const double* hs_anc) {
   const EvalParams& p = p_;
   constexpr bool mixed = sizeof(R) == sizeof(float);
   C2* deriv_k = static_cast<C2*>(deriv_k_);
@@ -763,10 +765,10 @@ void Engine::backward_stage(R* deriv, const double* dbar, double* out, const MuA
     CDFT_CUFFT(cufftExecZ2D(plan_force_, reinterpret_cast<cufftDoubleComplex*>(force_k),
                             reinterpret_cast<double*>(hs_r)));
   mark(8, stream);
-  if (!multi && !tensor) k_epilogue<false, false, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu, fin);
-  if (!multi && tensor) k_epilogue<false, true, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu, fin);
-  if (multi && !tensor) k_epilogue<true, false, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu, fin);
-  if (multi && tensor) k_epilogue<true, true, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu, fin);
+  if (!multi && !tensor) k_epilogue<false, false, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu, fin, hs_anc);
+  if (!multi && tensor) k_epilogue<false, true, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu, fin, hs_anc);
+  if (multi && !tensor) k_epilogue<true, false, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu, fin, hs_anc);
+  if (multi && tensor) k_epilogue<true, true, R><<<gs, 256, 0, stream>>>(p, hs_r, dbar, out, mu, fin, hs_anc);
   CDFT_CUDA(cudaGetLastError());
   mark(9, stream);
 }
@@ -864,7 +866,10 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   timing_run_ = timing_;
   if (timing_run_ && ring_used_ == kTimingRing) harvest_stage_times();
   mark(0, stream);
-  const bool fused = mixed && fused_;
+  // an anchored split runs the cuFFT transforms (the fused passes split
+  // around the plane means)
+  const bool anc = mixed && anchored_;
+  const bool fused = mixed && fused_ && !anc;
   // 1-3. weighted densities
   // TMA ring when every segment start is 16-byte aligned (N % 4 == 0 and
   // aligned base pointers); otherwise the register-prefetch variant.
@@ -892,7 +897,7 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
                     tables_, stream);
     mark(4, stream);
   } else {
-    forward_stage<R, C2>(rho, chan_r, mean_, stream);
+    forward_stage<R, C2>(rho, chan_r, mean_, stream, anc ? anc_rho_ : nullptr);
   }
   // 4. pointwise Phi / dPhi + local terms + reductions
   PointwiseArgs a;
@@ -903,7 +908,12 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   a.mf_w = mf_w_;
   a.mean = mean_;
   a.dbar_out = dbar_;
-  const int pw_blocks = tma ? pw_grid() : grid_pw_;
+  if (anc) {
+    a.n_anc = anc_n_;
+    a.d_anc = anc_d_;
+  }
+  // (the one-species kernels have no anchored split: the generic grid)
+  const int pw_blocks = tma ? (anc ? grid_tma_ : pw_grid()) : grid_pw_;
   const dim3 gp(grid_pw_, p.batch);
   if (tma) {
     launch_pointwise_tma<R>(chan_r, deriv_r, a, 0, p.N, 0, pw_blocks, pw_blocks, stream);
@@ -928,7 +938,7 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   if (fused)
     fused_backward(force, ma, fin, stream);
   else
-    backward_stage<R, C2>(deriv_r, dbar_, force, ma, fin, stream);
+    backward_stage<R, C2>(deriv_r, dbar_, force, ma, fin, stream, anc ? anc_hs_ : nullptr);
   mark(10, stream);
   if (timing_run_) {
     timing_run_ = false;
@@ -1018,6 +1028,44 @@ void Engine::hvp(const double* rho, const double* v, const double* mu, double* h
   (void)mu;
   hvp_set_point(rho, stream);
   hvp_apply(v, hv, stream);
+}
+
+void Engine::export_fields(double* chan, double* deriv, double* hs, cudaStream_t stream) const {
+  if (precision_ == kMixed) throw Error(-1, "export_fields: needs an FP64 engine");
+  const EvalParams& p = p_;
+  const size_t B = (size_t)p.batch, N = (size_t)p.N;
+  CDFT_CUDA(cudaMemcpyAsync(chan, chan_r_, sizeof(double) * B * p.n_chan * N, cudaMemcpyDeviceToDevice, stream));
+  CDFT_CUDA(cudaMemcpyAsync(deriv, deriv_r_, sizeof(double) * B * p.L.n_deriv * N, cudaMemcpyDeviceToDevice, stream));
+  CDFT_CUDA(cudaMemcpyAsync(hs, hs_r_, sizeof(double) * B * p.S * N, cudaMemcpyDeviceToDevice, stream));
+}
+
+void Engine::set_anchor(Engine& fp64, const double* rho_a, cudaStream_t stream) {
+  if (precision_ != kMixed) throw Error(-1, "anchor: needs a mixed-precision engine");
+  if (fp64.precision_ == kMixed) throw Error(-1, "anchor: the anchor engine must be FP64");
+  if (!rho_a) throw Error(-1, "anchor: rho_a is required");
+  const EvalParams &p = p_, &q = fp64.p_;
+  if (p.nx != q.nx || p.ny != q.ny || p.nz != q.nz || p.S != q.S || p.batch != q.batch || p.model != q.model ||
+      p.M != q.M || p.n_chan != q.n_chan || p.L.n_deriv != q.L.n_deriv || p.dx != q.dx)
+    throw Error(-1, "anchor: the FP64 engine must have the same grid, species, model, interactions and batch");
+  const size_t B = (size_t)p.batch, N = (size_t)p.N;
+  if (!anc_rho_) {
+    CDFT_CUDA(cudaMalloc(&anc_rho_, sizeof(double) * B * p.S * N));
+    CDFT_CUDA(cudaMalloc(&anc_n_, sizeof(double) * B * p.n_chan * N));
+    CDFT_CUDA(cudaMalloc(&anc_d_, sizeof(double) * B * p.L.n_deriv * N));
+    CDFT_CUDA(cudaMalloc(&anc_hs_, sizeof(double) * B * p.S * N));
+  }
+  CDFT_CUDA(cudaMemcpyAsync(anc_rho_, rho_a, sizeof(double) * B * p.S * N, cudaMemcpyDeviceToDevice, stream));
+  std::vector<double> mu0(B * p.S, 0.0);
+  fp64.evaluate(anc_rho_, nullptr, mu0.data(), fp64.h_force_, fp64.h_scalars_, stream);
+  fp64.export_fields(anc_n_, anc_d_, anc_hs_, stream);
+  if (fp64.take_error(stream)) throw Error(-2, "anchor: the FP64 evaluation of the anchor state failed");
+  if (!anchored_) ++generation_;
+  anchored_ = true;
+}
+
+void Engine::clear_anchor() {
+  if (anchored_) ++generation_;
+  anchored_ = false;
 }
 
 int Engine::take_error(cudaStream_t stream) {

@@ -140,6 +140,21 @@ class Engine {
   int kernels_per_eval() const { return precision_ == 1 ? (fused_ ? 4 + 3 * chunks_ : 6) : 4; }
   // Reads and clears the device error word (synchronises the stream).
   int take_error(cudaStream_t stream);
+  // Anchored split (mixed precision): from set_anchor on, every evaluation
+  // transforms rho - rho_a in FP32 instead of rho minus the species means,
+  // and adds the FP64 channels, derivative channels and back-convolution of
+  // the anchor state rho_a point by point (the FP32 round-off then scales
+  // with |rho - rho_a| instead of the density's own swing: a solid near a
+  // reference state).  `fp64` is an FP64 engine of the same grid, species,
+  // model, interactions and batch; rho_a (device, B*S*N) is evaluated by it
+  // once here.  Anchored evaluations run the cuFFT transforms and the
+  // generic pointwise kernel.  clear_anchor returns to the mean split.
+  void set_anchor(Engine& fp64, const double* rho_a, cudaStream_t stream);
+  void clear_anchor();
+  bool anchored() const { return anchored_; }
+  // FP64 engines: after evaluate(), the real-space channels, derivative
+  // channels and back-convolution (before dV) of the evaluated state.
+  void export_fields(double* chan, double* deriv, double* hs, cudaStream_t stream) const;
 
   // Stage timing: when on, every evaluate() records CUDA events between its
   // stages on its stream (one set of a ring of kTimingRing sets per
@@ -184,10 +199,11 @@ class Engine {
   void run_hvp_apply(const double* v, double* hv, cudaStream_t stream);
   bool hvp_ready_ = false;
   template <typename R, typename C2>
-  void forward_stage(const double* in, R* chan_out, double* mean_out, cudaStream_t stream);
+  void forward_stage(const double* in, R* chan_out, double* mean_out, cudaStream_t stream,
+                     const double* anchor = nullptr);
   template <typename R, typename C2>
   void backward_stage(R* deriv, const double* dbar, double* out, const MuArgs& mu, const FinalArgs& fin,
-                      cudaStream_t stream);
+                      cudaStream_t stream, const double* hs_anc = nullptr);
 
   EvalParams p_{};
   int precision_ = kFP64;
@@ -265,6 +281,11 @@ class Engine {
   double stage_ms_[kStages] = {};
   long long stage_count_ = 0;
 
+  bool anchored_ = false;
+  double* anc_rho_ = nullptr;  // B*S*N
+  double* anc_n_ = nullptr;    // B*n_chan*N
+  double* anc_d_ = nullptr;    // B*n_deriv*N
+  double* anc_hs_ = nullptr;   // B*S*N
   double* h_rho_ = nullptr;   // device staging for host API
   double* h_vext_ = nullptr;
   double* h_force_ = nullptr;

@@ -432,12 +432,21 @@ static __global__ void __launch_bounds__(256) k_species_mean(const double* __res
   }
 }
 
-// Mixed precision, step 2: delta_rho = rho - mean in FP32.
+// Mixed precision, step 2: delta_rho = rho - mean in FP32, or with an
+// anchor state rho_a (B*S*N, FP64) delta_rho = rho - rho_a.
 static __global__ void __launch_bounds__(256) k_split_convert(const double* __restrict__ rho, long long N, int S,
-                                                       float* __restrict__ out, const double* __restrict__ mean) {
+                                                       float* __restrict__ out, const double* __restrict__ mean,
+                                                       const double* __restrict__ anchor = nullptr) {
   rho += (long long)blockIdx.y * S * N;
   out += (long long)blockIdx.y * S * N;
   mean += blockIdx.y * kMaxSpecies;
+  if (anchor) {
+    anchor += (long long)blockIdx.y * S * N;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x)
+      for (int s = 0; s < S; ++s) out[s * N + i] = (float)(rho[s * N + i] - anchor[s * N + i]);
+    return;
+  }
   __shared__ double sm[kMaxSpecies];
   if (threadIdx.x < S) sm[threadIdx.x] = mean[threadIdx.x];
   __syncthreads();
@@ -457,6 +466,11 @@ struct PointwiseArgs {
   const double* mf_w;     // M*Nk (k = 0 entries give the mean-field DC weights)
   const double* mean;     // B*kMaxSpecies species means (mixed precision) or null
   double* dbar_out;       // B*kMaxChannels derivative-channel constants (mixed precision) or null
+  // anchored split (mixed precision, generic kernels): the FP64 channels
+  // (B*n_chan*N) and derivative channels (B*n_deriv*N) of the anchor state
+  // replace the constant offsets and dbar point by point; null otherwise
+  const double* n_anc = nullptr;
+  const double* d_anc = nullptr;
 };
 
 // The arguments of problem b of a batch.
@@ -468,6 +482,8 @@ __device__ __forceinline__ PointwiseArgs batch_slice(const EvalParams& p, Pointw
   a.partials += (long long)b * gridDim.x * p.n_terms;
   if (a.mean) a.mean += b * kMaxSpecies;
   if (a.dbar_out) a.dbar_out += b * kMaxChannels;
+  if (a.n_anc) a.n_anc += (long long)b * p.n_chan * p.N;
+  if (a.d_anc) a.d_anc += (long long)b * p.L.n_deriv * p.N;
   return a;
 }
 
@@ -583,9 +599,14 @@ __device__ __forceinline__ void point_body(const EvalParams& p, const PointwiseA
   constexpr bool SPLIT = sizeof(RT) == sizeof(float);
   constexpr int NF = L::NFMT;
   const long long N = p.N;
+  // the split offsets of channel c at this point: the constants of the
+  // species means, or the anchor state's FP64 channels
+  const double* na = (SPLIT && a.n_anc) ? a.n_anc + idx : nullptr;
+  const double* da = (SPLIT && a.d_anc) ? a.d_anc + idx : nullptr;
+  auto off = [&](int c) { return SPLIT ? (na ? na[(long long)c * N] : s_off[c]) : 0.0; };
   double n[NF];
 #pragma unroll
-  for (int c = 0; c < NF; ++c) n[c] = cur[c] + (SPLIT ? s_off[c] : 0.0);
+  for (int c = 0; c < NF; ++c) n[c] = cur[c] + off(c);
   Measures<double> m;
   double phi = 0.0;
   MeasureDerivs<double> dm;
@@ -634,7 +655,8 @@ __device__ __forceinline__ void point_body(const EvalParams& p, const PointwiseA
   }
   acc[kTermHS] += phi;
 #pragma unroll
-  for (int c = 0; c < NF; ++c) __stcs(deriv + c * N + idx, (RT)(SPLIT ? D[c] - s_dbar[c] : D[c]));
+  for (int c = 0; c < NF; ++c)
+    __stcs(deriv + c * N + idx, (RT)(SPLIT ? D[c] - (da ? da[(long long)c * N] : s_dbar[c]) : D[c]));
   if constexpr (!MULTI) {
     // one species: every interaction is species 0 with itself, channel NF + q
     const double r = rs[0], v = vs[0];
@@ -649,7 +671,7 @@ __device__ __forceinline__ void point_body(const EvalParams& p, const PointwiseA
         cj = q == 0 ? cur[NF] : cur[NPRE - 1];
       else
         cj = (double)chan[(NF + q) * N + idx];
-      cj += SPLIT ? s_off[NF + q] : 0.0;
+      cj += off(NF + q);
       acc[kTermMF] += 0.5 * r * cj;
       f0 += cj;
     }
@@ -680,7 +702,7 @@ __device__ __forceinline__ void point_body(const EvalParams& p, const PointwiseA
         if (c == cix && c - NF < n_mf_pre) { ci = cur[c]; hi = true; }
       }
       if (!hj) cj = (double)chan[cjx * N + idx];
-      cj += SPLIT ? s_off[cjx] : 0.0;
+      cj += off(cjx);
       double ri = 0.0;
 #pragma unroll
       for (int s = 0; s < kMaxSpecies; ++s)
@@ -692,7 +714,7 @@ __device__ __forceinline__ void point_body(const EvalParams& p, const PointwiseA
           if (s == i) f[s] += cj * p.dv;
       } else {
         if (!hi) ci = (double)chan[cix * N + idx];
-        ci += SPLIT ? s_off[cix] : 0.0;
+        ci += off(cix);
 #pragma unroll
         for (int s = 0; s < kMaxSpecies; ++s) {
           if (s == i) f[s] += 0.5 * cj * p.dv;
@@ -1318,6 +1340,7 @@ __device__ __forceinline__ void reduce_final(const double* __restrict__ partials
     out[4] = f_hs;
     out[5] = f_mf;
     for (int s = 0; s < p.S; ++s) out[6 + s] = sh[kTermN0 + s] * dv;
+    for (int s = p.S; s < kMaxSpecies; ++s) out[6 + s] = 0.0;  // unused species slots
   }
 }
 
@@ -1328,7 +1351,7 @@ __device__ __forceinline__ void reduce_final(const double* __restrict__ partials
 template <bool MULTI, bool TENSOR, typename RT>
 __global__ void __launch_bounds__(256) k_epilogue(EvalParams p, const RT* __restrict__ hs, const double* __restrict__ dbar,
                                                   double* __restrict__ force, const __grid_constant__ MuArgs mu,
-                                                  FinalArgs fin) {
+                                                  FinalArgs fin, const double* __restrict__ hs_anc = nullptr) {
   using L = Lay<MULTI, TENSOR>;
   constexpr bool SPLIT = sizeof(RT) == sizeof(float);
   const int b = blockIdx.y;
@@ -1339,6 +1362,16 @@ __global__ void __launch_bounds__(256) k_epilogue(EvalParams p, const RT* __rest
   hs += (long long)b * p.S * N;
   force += (long long)b * p.S * N;
   dbar += b * kMaxChannels;
+  if (hs_anc) {
+    // anchored split: the anchor's FP64 back-convolution replaces the
+    // constants of the split derivative channels
+    hs_anc += (long long)b * p.S * N;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x)
+      for (int s = 0; s < p.S; ++s)
+        force[s * N + i] = force[s * N + i] + ((double)hs[s * N + i] + hs_anc[s * N + i]) * p.dv - mu.mu[b][s] * p.dv;
+    return;
+  }
   __shared__ double s_const[kMaxSpecies];
   if (threadIdx.x < p.S) {
     const int s = threadIdx.x;

@@ -410,6 +410,30 @@ class Engine:
                for t in range(2) for v in range(5) for k in range(8) for d in range(4)}
         return (choice[0], choice[1], choice[2], choice[3]), {key: ms[i] for key, i in idx.items() if ms[i] > 0.0}
 
+    def set_anchor(self, fp64_engine: "Engine", rho_anchor, stream: int = 0):
+        """Anchored split (cdft_engine_set_anchor): ``rho_anchor`` a device
+        tensor (B*S*N doubles) or a host array; ``fp64_engine`` an FP64 engine
+        of the same model and batch."""
+        torch = None
+        if hasattr(rho_anchor, "data_ptr"):
+            ptr = rho_anchor.data_ptr()
+            keep = rho_anchor
+        else:
+            import torch
+            keep = torch.tensor(np.ascontiguousarray(rho_anchor, dtype=np.float64).reshape(-1), device="cuda")
+            ptr = keep.data_ptr()
+        _lib.check(_lib.lib().cdft_engine_set_anchor(self.handle, fp64_engine.handle, ptr, stream))
+        del keep, torch
+
+    def clear_anchor(self):
+        _lib.check(_lib.lib().cdft_engine_clear_anchor(self.handle))
+
+    @property
+    def anchored(self) -> bool:
+        a = ctypes.c_int()
+        _lib.check(_lib.lib().cdft_engine_anchored(self.handle, ctypes.byref(a)))
+        return bool(a.value)
+
     @property
     def pointwise_spread(self) -> int:
         """Divisor of the pointwise grid per plane chunk (0: the chunk count)."""

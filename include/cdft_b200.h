@@ -630,6 +630,23 @@ CDFT_API int cdft_engine_pointwise(const cdft_engine* engine, int* variant, int*
 CDFT_API int cdft_engine_set_column_tile(cdft_engine* engine, int tile);
 CDFT_API int cdft_engine_column_tile(const cdft_engine* engine, int* tile);
 CDFT_API int cdft_engine_set_pointwise_spread(cdft_engine* engine, int spread);
+
+/* Anchored split (no reference counterpart; mixed-precision engines): the
+ * mixed path transforms rho - mean in FP32, so its round-off scales with the
+ * density's own swing, which for a solid is the peak height.  From
+ * cdft_engine_set_anchor on, an evaluation instead transforms rho - rho_a in
+ * FP32 and adds, point by point, the FP64 weighted densities, derivative
+ * channels and back-convolution of the anchor state rho_a, evaluated once
+ * here by fp64_engine (an FP64 engine of the same grid, species, model,
+ * interactions and batch): near the anchor the error scales with
+ * |rho - rho_a|.  rho_anchor: device, B*S*N doubles (copied).  Anchored
+ * evaluations run the cuFFT transforms and the generic pointwise kernel;
+ * the HVP keeps the mean split.  Synchronises `stream`.
+ * cdft_engine_clear_anchor returns to the mean split. */
+CDFT_API int cdft_engine_set_anchor(cdft_engine* engine, cdft_engine* fp64_engine, const double* rho_anchor,
+                                    void* stream);
+CDFT_API int cdft_engine_clear_anchor(cdft_engine* engine);
+CDFT_API int cdft_engine_anchored(const cdft_engine* engine, int* anchored);
 CDFT_API int cdft_engine_pointwise_spread(const cdft_engine* engine, int* spread);
 CDFT_API int cdft_engine_autotune_ex(cdft_engine* engine, const double* rho, const double* vext, const double* mu,
                                      void* stream, int reps, int choice[4], double* ms);

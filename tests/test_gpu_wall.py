@@ -9,11 +9,12 @@ x < d/2), FIRE grand-potential minimisation at the bulk mu of rho = 0.5.
   functional of the reference, include/dft/functionals/functionals.hpp:64-95,
   with V_ext): the rms of its forces in the minimiser's variable x
   (rho = rho_min + x^2, dOmega/dx = 2 x dOmega/drho) is the convergence
-  criterion's, below 1e-10, and max |dOmega/drho| / dV over the fluid is
+  criterion's, below 1e-11, and max |dOmega/drho| / dV over the fluid is
   below 1e-4 (the largest forces sit in the dilute first layer at the wall,
   where x is small).
 The box is periodic (no boundary treatment) and convergence is the rms
-force of Fire::step (fire.hpp:162) below 1e-10.
+force of Fire::step (fire.hpp:162) below 1e-11 (at 1e-10 the two converged
+profiles agree only to ~1.5e-8: the tolerance ball of the criterion).
 """
 import numpy as np
 import pytest
@@ -39,7 +40,7 @@ def test_hard_wall_mixed_refined_matches_fp64_and_the_oracle():
     vext = np.where(wall, 50.0, 0.0)
     mu = cd.make_bulk_thermodynamics(pr.model.species, pr.weights).chemical_potential([0.5], 0)
     # periodic box: no boundary treatment; convergence on the rms force
-    fire = cd.Fire(dt=0.1, dt_max=1.0, alpha_start=0.01, f_alpha=0.99, force_tolerance=1e-10, max_steps=50000)
+    fire = cd.Fire(dt=0.1, dt_max=1.0, alpha_start=0.01, f_alpha=0.99, force_tolerance=1e-11, max_steps=50000)
     kw = dict(use_homogeneous_boundary=False, use_monitor=False)
     a = cd.Minimizer(fire=fire, **kw).grand_potential(pr.model, pr.weights, rho0, mu, external_field=vext)
     b = cd.Minimizer(fire=fire, refine=pr.weights, refine_switch=1e3, **kw).grand_potential(
@@ -51,6 +52,6 @@ def test_hard_wall_mixed_refined_matches_fp64_and_the_oracle():
     assert np.max(a.densities[0][wall]) < 1e-12
     ref = pr.ref([a.densities[0]], [mu], [vext])
     x = np.sqrt(np.maximum(a.densities[0] - 1e-18, 0.0))
-    assert float(np.sqrt(np.mean((2.0 * x * ref.forces[0]) ** 2))) <= 1.001e-10
+    assert float(np.sqrt(np.mean((2.0 * x * ref.forces[0]) ** 2))) <= 1.001e-11
     assert np.max(np.abs(ref.forces[0][~wall])) / pr.grid.cell_volume <= 1e-4
     assert ref.grand_potential == pytest.approx(a.grand_potential, rel=1e-12)
