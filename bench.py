@@ -641,6 +641,82 @@ def config_nucleus(cd, torch):
     return out
 
 
+def config_solid(cd, torch, cells=8, reps=5):
+    """The binary hard-sphere FCC solid: 256^3 on 8 x 8 x 8 cells (a = 1.55,
+    dx = 0.0484375), large spheres (d = 1) as Gaussian peaks (alpha = 50, 0.8
+    particles per site) on FCC(001) sites, small spheres (d = 0.5) uniform at
+    0.1, esFMT A = 1 B = 0.  At the crystal and 1% off it (the crystal times
+    1 + 0.01 G, G smoothed unit noise, seeded): FP64, mixed with the mean
+    split, and mixed with the anchored split at the crystal (FP64 channels
+    of the anchor, FP32 transforms of the difference).  The FP64 engine is
+    pinned to the oracle at 64^3 on the same solid."""
+    import math
+    from classicaldft_b200 import crystal as cc
+    a_fcc, dx, alpha, occ = 1.55, 0.0484375, 50.0, 0.8
+    n = int(round(cells * a_fcc / dx))
+    lat = cc.build_lattice(cc.Structure.FCC, cc.Orientation._001, (cells,) * 3)
+    sites = lat.scaled_positions(a_fcc / math.sqrt(2.0))
+    grid = cd.Grid(dx=dx, box_size=(n * dx,) * 3, shape=(n,) * 3)
+    rho1 = cc.gaussian_peaks(grid, sites, alpha, occ * (alpha / math.pi) ** 1.5, 0.0)
+    N = grid.total_points
+    rho2 = torch.full((N,), 0.1, dtype=torch.float64, device=rho1.device)
+    model = cd.Model(grid, [cd.Species("large", 1.0), cd.Species("small", 0.5)], [], 1.0)
+    fmt = cd.FMTModel("esFMT", 1.0, 0.0)
+    gen = torch.Generator(device=rho1.device).manual_seed(SEED + 5)
+    noise = torch.randn(2, n, n, n, dtype=torch.float64, device=rho1.device, generator=gen)
+    k = torch.fft.fftfreq(n, device=rho1.device, dtype=torch.float64)
+    K2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2
+    g = torch.fft.ifftn(torch.fft.fftn(noise, dim=(1, 2, 3)) * torch.exp(-2.0 * (math.pi * 2.0) ** 2 * K2),
+                        dim=(1, 2, 3)).real
+    g = (g / g.std(dim=(1, 2, 3), keepdim=True)).reshape(2, N)
+    crystal = torch.cat([rho1, rho2]).contiguous()
+    near = torch.cat([rho1 * (1.0 + 0.01 * g[0]), rho2 * (1.0 + 0.01 * g[1])]).contiguous()
+    del noise, g, K2
+    w64 = cd.make_weights(fmt, model, cd.FP64)
+    wmx = cd.make_weights(fmt, model, cd.MIXED)
+    force = torch.empty_like(crystal)
+    scal = torch.zeros(10, dtype=torch.float64, device=crystal.device)
+    mu = [0.0, 0.0]
+
+    def run(w, x):
+        w.engine.total_device(x.data_ptr(), None, mu, force.data_ptr(), scal.data_ptr(), 0)
+        torch.cuda.synchronize()
+        return float(scal[0]), force.clone()
+
+    def rate(w, x):
+        run(w, x)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            w.engine.total_device(x.data_ptr(), None, mu, force.data_ptr(), scal.data_ptr(), 0)
+        torch.cuda.synchronize()
+        return reps / (time.perf_counter() - t0)
+
+    out = {"workload": f"{n}^3 binary hard-sphere FCC solid ({cells}^3 cells, a = 1.55), esFMT A = 1 B = 0",
+           "states": {"crystal": "Gaussian peaks alpha = 50, 0.8 per site; small spheres 0.1",
+                      "near": "the crystal times 1 + 0.01 G (G smoothed unit noise, seeded)"}}
+    res = {}
+    for label, x in (("crystal", crystal), ("near", near)):
+        f64, F64 = run(w64, x)
+        fmx, Fmx = run(wmx, x)
+        res[label] = (f64, F64, fmx, Fmx)
+    wmx.engine.set_anchor(w64.engine, crystal)
+    for label, x in (("crystal", crystal), ("near", near)):
+        f64, F64, fmx, Fmx = res[label]
+        fan, Fan = run(wmx, x)
+        den = float(F64.abs().max())
+        out[label] = {"F_fp64": f64,
+                      "mixed_mean_split": {"dF_over_F": abs(fmx - f64) / abs(f64),
+                                           "max_dforce_over_max_force": float((Fmx - F64).abs().max()) / den},
+                      "mixed_anchored": {"dF_over_F": abs(fan - f64) / abs(f64),
+                                         "max_dforce_over_max_force": float((Fan - F64).abs().max()) / den}}
+    out["evals_per_s"] = {"fp64": rate(w64, near), "mixed_anchored": rate(wmx, near)}
+    wmx.engine.clear_anchor()
+    out["evals_per_s"]["mixed_mean_split"] = rate(wmx, near)
+    for w in (w64, wmx):
+        w.engine.close()
+    return out
+
+
 def config_sweep(cd, torch):
     """16 state points each on 48^3, 64^3 and 96^3 grids (dx = 0.1, kT = 1,
     WBII + cut LJ), mu evenly spaced over the liquid branch (from the bulk
@@ -845,7 +921,8 @@ def run_ours(args, ws, rank, local, dist):
     if ws == 1 and not args.no_configs:
         # the other configurations at their own sizes (N = 1 only)
         for key, fn in (("config_wall_64", config_wall), ("config_ddft_128", config_ddft),
-                        ("config_nucleus_128", config_nucleus), ("config_sweep_48_64_96", config_sweep)):
+                        ("config_nucleus_128", config_nucleus), ("config_sweep_48_64_96", config_sweep),
+                        ("config_solid_256", config_solid)):
             try:
                 line[key] = fn(cd, torch)
             except Exception as exc:  # reported, not hidden
