@@ -381,6 +381,42 @@ SWEEP_SHAPES = (48, 64, 96)
 SWEEP_BATCH = 16
 
 
+def batched_headline(torch, cd, dev, precision, rho, flush, stream, steps):
+    """The headline state (128^3) as B = 2 and 4 problems of one batched
+    engine per launch (independent states sharing the launches: the
+    throughput of evaluating many states, not the latency of one), in
+    problem evaluations per second, L2 flushed between steps."""
+    lj = cd.make_lennard_jones(1.0, 1.0, 2.5)
+    d = lj.hard_sphere_diameter(KT, cd.WEEKS_CHANDLER_ANDERSEN)
+    g = cd.Grid(dx=DX, box_size=tuple(n * DX for n in SHAPE), shape=SHAPE)
+    model = cd.Model(g, [cd.Species("LJ", d)], [cd.Interaction(0, 0, lj)], KT)
+    out = {}
+    for B in (2, 4):
+        eng = cd.Engine(cd.WhiteBearII(), model, precision, batch=B)
+        rb = rho.repeat(B).contiguous()
+        f = torch.empty_like(rb)
+        sc = torch.empty((B, 10), dtype=torch.float64, device=dev)
+        mus = [0.0] * B
+        if eng.transforms == "fused":
+            eng.autotune_ex(rb.data_ptr(), mu=mus, stream=stream.cuda_stream, reps=5)
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                eng.total_device(rb.data_ptr(), None, mus, f.data_ptr(), sc.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        with torch.cuda.stream(stream):
+            for i in range(steps):
+                flush(i)
+                evs[i][0].record(stream)
+                eng.total_device(rb.data_ptr(), None, mus, f.data_ptr(), sc.data_ptr(), stream.cuda_stream)
+                evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        t = sum(a.elapsed_time(b) for a, b in evs) / steps
+        out[f"B{B}"] = {"problem_evals_per_s": B / (t * 1e-3), "ms_per_launch": t}
+        eng.close()
+    return out
+
+
 def sweep_throughput(torch, cd, dev, precision, flush, stream, steps):
     """Batched evaluation of 16 problems of each grid of the parameter sweep
     (48^3, 64^3, 96^3 at dx = 0.1, kT = 1, WhiteBearII + cut LJ), as problem
@@ -876,6 +912,7 @@ def run_ours(args, ws, rank, local, dist):
     top = max(mine, key=lambda k: mine[k]["ms"])
     traffic = measured_traffic()
     sweep = None if args.no_sweep else sweep_throughput(torch, cd, dev, precision, flush, stream, 20)
+    batched = None if args.no_sweep else batched_headline(torch, cd, dev, precision, rho, flush, stream, 20)
     fire_rates = None if args.no_sweep else fire_step_rates(torch, cd, precision)
     line = {
         "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": ws, "steps": args.steps,
@@ -907,6 +944,7 @@ def run_ours(args, ws, rank, local, dist):
                                    else "one full evaluation (cuFFT transforms + engine kernels)")}},
         "stages": stages,
         "sweep": sweep,
+        "batched_128": batched,
         "fire_steps": fire_rates,
         names[other]: {"value": ws * n2 / (t2 * 1e-3), "ms_per_step": t2 / n2},
         "mixed_vs_fp64": {"dF_over_F": dF, "max_dforce_over_max_force": dforce},

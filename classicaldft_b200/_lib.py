@@ -225,6 +225,7 @@ def lib():
         "cdft_engine_set_column_tile": [vp, ctypes.c_int],
         "cdft_engine_set_pointwise_spread": [vp, ctypes.c_int],
         "cdft_engine_set_anchor": [vp, vp, vp, vp],
+        "cdft_engine_set_anchor_host": [vp, vp, vp],
         "cdft_engine_clear_anchor": [vp],
         "cdft_engine_anchored": [vp, ctypes.POINTER(ctypes.c_int)],
         "cdft_engine_pointwise_spread": [vp, ctypes.POINTER(ctypes.c_int)],

@@ -397,6 +397,18 @@ int cdft_engine_set_anchor(cdft_engine* engine, cdft_engine* fp64_engine, const 
   });
 }
 
+int cdft_engine_set_anchor_host(cdft_engine* engine, cdft_engine* fp64_engine, const double* rho_anchor) {
+  return guarded([&] {
+    if (!engine || !fp64_engine || !rho_anchor)
+      throw std::invalid_argument("anchor: engine, the FP64 engine and rho_anchor are required");
+    cdft::Engine& e = *engine->impl;
+    const size_t bytes = sizeof(double) * e.batch() * e.species() * e.points();
+    cudaStream_t st = e.stream();
+    CDFT_CUDA(cudaMemcpyAsync(e.host_rho(), rho_anchor, bytes, cudaMemcpyHostToDevice, st));
+    e.set_anchor(*fp64_engine->impl, e.host_rho(), st);
+  });
+}
+
 int cdft_engine_clear_anchor(cdft_engine* engine) {
   return guarded([&] {
     if (!engine) throw std::invalid_argument("engine is NULL");

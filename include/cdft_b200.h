@@ -645,6 +645,8 @@ CDFT_API int cdft_engine_set_pointwise_spread(cdft_engine* engine, int spread);
  * cdft_engine_clear_anchor returns to the mean split. */
 CDFT_API int cdft_engine_set_anchor(cdft_engine* engine, cdft_engine* fp64_engine, const double* rho_anchor,
                                     void* stream);
+/* The same with rho_anchor in HOST memory (B*S*N doubles). */
+CDFT_API int cdft_engine_set_anchor_host(cdft_engine* engine, cdft_engine* fp64_engine, const double* rho_anchor);
 CDFT_API int cdft_engine_clear_anchor(cdft_engine* engine);
 CDFT_API int cdft_engine_anchored(const cdft_engine* engine, int* anchored);
 CDFT_API int cdft_engine_pointwise_spread(const cdft_engine* engine, int* spread);

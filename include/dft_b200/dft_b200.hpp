@@ -204,6 +204,14 @@ class Weights {
   }
   cdft_engine* engine() const { return engine_.get(); }
   const std::vector<double>& a_vdw() const { return a_vdw_; }
+  // Anchored split of a mixed-precision Weights (cdft_engine_set_anchor_host):
+  // later evaluations transform rho - rho_anchor in FP32 around the FP64
+  // fields of rho_anchor, evaluated once by `fp64` (an FP64 Weights of the
+  // same model).  rho_anchor: S*N values, species after species.
+  void set_anchor(const Weights& fp64, const std::vector<double>& rho_anchor) {
+    check(cdft_engine_set_anchor_host(engine(), fp64.engine(), rho_anchor.data()));
+  }
+  void clear_anchor() { check(cdft_engine_clear_anchor(engine())); }
   const FMTModel& fmt_model() const { return fmt_; }
 
  private:

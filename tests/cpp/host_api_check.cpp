@@ -86,6 +86,18 @@ int main(int argc, char** argv) {
       std::printf("stream_equal=%d\n", equal);
     }
 
+    // 1c. a mixed Weights anchored at rho, evaluated 1% off it
+    {
+      d::functionals::Weights wm(d::functionals::FMTModel::WhiteBearII(), model, CDFT_MIXED);
+      wm.set_anchor(*func.weights, rho);
+      d::functionals::State s1 = st;
+      for (double& v : s1.species[0].values) v *= 1.01;
+      const auto am = d::functionals::total(model, s1, wm);
+      const auto a64 = d::functionals::total(model, s1, *func.weights);
+      std::printf("anchor_dF=%.17g\n", std::abs(am.free_energy - a64.free_energy) / std::abs(a64.free_energy));
+      wm.clear_anchor();
+    }
+
     // 2. FIRE2 grand-potential minimisation
     d::algorithms::minimization::Minimizer mz;
     mz.fire.dt = 0.05;
