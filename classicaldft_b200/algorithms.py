@@ -494,6 +494,15 @@ class Simulation:
     the entries the reference records (step 0, every log_interval-th step
     and the last one); ``all_times`` / ``all_energies`` hold every step.
     ``stop_condition(step, time, energy) -> bool`` ends the run early.
+
+    ``anchor`` (FP64 Weights of the same model) with ``anchor_interval`` k > 0
+    runs a mixed-precision engine in segments of k steps, each with the
+    engine's split anchored at the state the segment starts from (one FP64
+    evaluation per segment, cdft_engine_set_anchor): the FP32 round-off then
+    scales with how far the density moved within the segment instead of its
+    own swing (solids).  The adaptive dt carries over the segments; the
+    anchor is cleared after the run.  Snapshots are then taken between
+    segments: snapshot_interval must be a multiple of anchor_interval.
     """
 
     step: StepConfig = field(default_factory=StepConfig)
@@ -506,6 +515,9 @@ class Simulation:
     # FP64 defect correction of a mixed-precision run (see integrating_factor_step)
     refine: object = None
     refine_iterations: int = 1
+    # anchored split of a mixed-precision run, re-anchored every anchor_interval steps
+    anchor: object = None
+    anchor_interval: int = 0
 
     def run(self, densities, weights: Weights, chemical_potential=0.0):
         torch = _torch()
@@ -533,10 +545,11 @@ class Simulation:
             mask_dev = torch.tensor(m.astype(np.uint8), device="cuda")
             res_density = self.boundary.reservoir_density
         err = []
+        offset = [0, 0.0]  # steps and time before the current segment
 
         def _stop(step, time, energy, _user):
             try:
-                return 1 if self.stop_condition(step, time, energy) else 0
+                return 1 if self.stop_condition(step + offset[0], time + offset[1], energy) else 0
             except Exception as exc:  # surfaced after the run
                 err.append(exc)
                 return 1
@@ -545,25 +558,61 @@ class Simulation:
         if mask_dev is not None:
             d.masked_fill_(mask_dev.bool(), res_density)  # the driver applies it too; the initial mass needs it
         mass_initial = float(torch.sum(d).item()) * dv
+        anchored = self.anchor is not None and self.anchor_interval > 0
+        if anchored and self.snapshot_interval > 0 and self.snapshot_interval % self.anchor_interval:
+            raise ValueError("anchored DDFT: snapshot_interval must be a multiple of anchor_interval")
+        seg_len = self.anchor_interval if anchored else self.n_steps
+        snapshots = []
+        steps = 0
+
+        def take(step, x):  # a snapshot between anchored segments
+            rho_k = x.cpu().numpy().copy() if host else x.clone()
+            snapshots.append(Snapshot(step, float(times[step]), float(energies[step]), [rho_k]))
+
+        initial = d.clone() if anchored and self.snapshot_interval > 0 else None
+
         _set_ddft_refine(weights, self.refine, self.refine_iterations)
         try:
-            _lib.check(_lib.lib().cdft_ddft_simulate(
-                weights.engine.handle, ctypes.byref(c), chemical_potential, self.n_steps, d.data_ptr(),
-                times.ctypes.data_as(_lib.c_double_p), energies.ctypes.data_as(_lib.c_double_p),
-                self.snapshot_interval, ctypes.cast(snaps.data_ptr(), _lib.c_double_p) if snaps is not None else None,
-                snap_steps, cap, ctypes.byref(count), mask_dev.data_ptr() if mask_dev is not None else None,
-                res_density, cb, None, ctypes.byref(done), _stream()))
+            while True:
+                k = min(seg_len, self.n_steps - steps)
+                if anchored:
+                    weights.engine.set_anchor(self.anchor.engine, d)
+                ts = np.zeros(k + 1)
+                es = np.zeros(k + 1)
+                scap = 1 + k // self.snapshot_interval if self.snapshot_interval > 0 and not anchored else 0
+                _lib.check(_lib.lib().cdft_ddft_simulate(
+                    weights.engine.handle, ctypes.byref(c), chemical_potential, k, d.data_ptr(),
+                    ts.ctypes.data_as(_lib.c_double_p), es.ctypes.data_as(_lib.c_double_p),
+                    self.snapshot_interval if scap else 0,
+                    ctypes.cast(snaps.data_ptr(), _lib.c_double_p) if snaps is not None else None,
+                    snap_steps, scap, ctypes.byref(count), mask_dev.data_ptr() if mask_dev is not None else None,
+                    res_density, cb, None, ctypes.byref(done), _stream()))
+                torch.cuda.synchronize()
+                got = done.value
+                first = steps == 0
+                times[steps:steps + got + 1] = ts[:got + 1] + offset[1]
+                if first:
+                    energies[:got + 1] = es[:got + 1]
+                else:  # step 0 of a segment repeats the previous segment's last
+                    energies[steps + 1:steps + got + 1] = es[1:got + 1]
+                for q in range(count.value if scap else 0):
+                    st = snap_steps[q]
+                    rho_k = snaps[q].numpy().copy() if host else snaps[q].to(d.device)
+                    snapshots.append(Snapshot(st, float(times[st]), float(energies[st]), [rho_k]))
+                if initial is not None and first:
+                    take(0, initial)
+                steps += got
+                if anchored and self.snapshot_interval > 0 and got and steps % self.snapshot_interval == 0:
+                    take(steps, d)
+                offset[0], offset[1] = steps, float(times[steps])
+                if got < k or steps >= self.n_steps or err:
+                    break
         finally:
             _set_ddft_refine(weights, None, 0)
-        torch.cuda.synchronize()
+            if anchored:
+                weights.engine.clear_anchor()
         if err:
             raise err[0]
-        steps = done.value
-        snapshots = []
-        for k in range(count.value):
-            st = snap_steps[k]
-            rho_k = snaps[k].numpy().copy() if host else snaps[k].to(d.device)
-            snapshots.append(Snapshot(st, float(times[st]), float(energies[st]), [rho_k]))
         idx = [0]
         if self.log_interval > 0:
             idx += [s for s in range(1, steps + 1) if s % self.log_interval == 0 or s == self.n_steps]
