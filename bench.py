@@ -822,6 +822,23 @@ def run_ours(args, ws, rank, local, dist):
         (k, v, tq, sp), ms = eng.autotune_ex(rho.data_ptr(), mu=[0.0], reps=10)
         tuned = {"chosen": {"plane_chunks": k, "pointwise_variant": v, "column_tile": tq, "pointwise_spread": sp},
                  "ms_per_eval": {f"t{tt}_v{vv}_k{c}_d{dd}": round(t, 5) for (tt, vv, c, dd), t in ms.items()}}
+        # programmatic dependent launch between the passes, off against on
+        # (back-to-back evaluations, CUDA events; the timed run uses on)
+        f_tmp = torch.empty_like(rho)
+        s_tmp = torch.zeros(10, dtype=torch.float64, device=dev)
+        dl = {}
+        for on in (False, True, False, True):
+            eng.set_dependent_launch(on)
+            for _ in range(3):
+                eng.total_device(rho.data_ptr(), None, [0.0], f_tmp.data_ptr(), s_tmp.data_ptr(), 0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(50):
+                eng.total_device(rho.data_ptr(), None, [0.0], f_tmp.data_ptr(), s_tmp.data_ptr(), 0)
+            e1.record()
+            torch.cuda.synchronize()
+            dl.setdefault("on_ms" if on else "off_ms", []).append(round(e0.elapsed_time(e1) / 50, 5))
+        tuned["dependent_launch"] = dl
     force = torch.empty_like(rho)
     scal = torch.zeros(10, dtype=torch.float64, device=dev)
     flush = L2Flush(torch, dev)

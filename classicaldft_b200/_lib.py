@@ -224,6 +224,7 @@ def lib():
         "cdft_engine_autotune_ex": [vp, vp, vp, c_double_p, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), c_double_p],
         "cdft_engine_set_column_tile": [vp, ctypes.c_int],
         "cdft_engine_set_pointwise_spread": [vp, ctypes.c_int],
+        "cdft_engine_set_dependent_launch": [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
         "cdft_engine_set_anchor": [vp, vp, vp, vp],
         "cdft_engine_set_anchor_host": [vp, vp, vp],
         "cdft_engine_clear_anchor": [vp],

@@ -409,6 +409,14 @@ int cdft_engine_set_anchor_host(cdft_engine* engine, cdft_engine* fp64_engine, c
   });
 }
 
+int cdft_engine_set_dependent_launch(cdft_engine* engine, int on, int* was) {
+  return guarded([&] {
+    if (!engine) throw std::invalid_argument("engine is NULL");
+    if (was) *was = engine->impl->dependent_launch() ? 1 : 0;
+    if (on >= 0) engine->impl->set_dependent_launch(on != 0);
+  });
+}
+
 int cdft_engine_clear_anchor(cdft_engine* engine) {
   return guarded([&] {
     if (!engine) throw std::invalid_argument("engine is NULL");

@@ -9,6 +9,8 @@
 // fully coalesced warps and cuFFT runs one batched plan over all channels.
 #pragma once
 
+#include <utility>
+
 #include <cuda_runtime.h>
 #include <cufft.h>
 
@@ -132,6 +134,32 @@ class Error : public std::runtime_error {
       throw ::cdft::Error(-3, std::string("CUDA error ") + cudaGetErrorString(e_) + " at " + \
                                   __FILE__ + ":" + std::to_string(__LINE__));               \
   } while (0)
+
+// Programmatic dependent launch.  A kernel launched with the attribute
+// (launch_k with pdl) may be scheduled while its stream predecessor still
+// runs; pdl_wait() blocks until that predecessor has completed and its
+// writes are visible (a no-op in a launch without the attribute).
+// pdl_trigger() lets this grid's dependent be scheduled once every CTA of
+// this grid has started (so the dependent's waiting CTAs never keep this
+// grid's later CTAs from starting).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <class... Exp, class... Act>
+inline void launch_k(void (*kern)(Exp...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, bool pdl,
+                     Act&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  CDFT_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<Act>(args)...));
+}
 
 #define CDFT_CUFFT(call)                                                                   \
   do {                                                                                     \

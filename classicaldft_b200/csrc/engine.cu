@@ -152,7 +152,10 @@ void Engine::launch_pointwise_tma(const R* chan, R* deriv, const PointwiseArgs& 
           constexpr int NMF = decltype(nc)::value;
           const int v = pw_variant_;
           const size_t smem = v == 4 ? (vext ? tma1_smem2_v_ : tma1_smem2_) : (vext ? tma1_smem_v_ : tma1_smem_);
-          auto go = [&](auto kern) { kern<<<g, kTmaTile, smem, st>>>(p, chan, deriv, a, err_, p0, pn, blk0, nblk); };
+          // (stream predecessor: the chunk's channel plane pass)
+          auto go = [&](auto kern) {
+            launch_k(kern, g, dim3(kTmaTile), smem, st, plan_.pdl, p, chan, deriv, a, err_, p0, pn, blk0, nblk);
+          };
           if (vext) {
             if (v == 1) go(k_pointwise1_tma<MD, NMF, true, 5>);
             else if (v == 2) go(k_pointwise1_tma<MD, NMF, true, 6>);
@@ -865,6 +868,7 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   }
   timing_run_ = timing_;
   if (timing_run_ && ring_used_ == kTimingRing) harvest_stage_times();
+  plan_.pdl = false;  // set below for the chunked fused path only
   mark(0, stream);
   // an anchored split runs the cuFFT transforms (the fused passes split
   // around the plane means)
@@ -878,6 +882,12 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
   for (int b = 0; b < kMaxBatch; ++b)
     for (int s = 0; s < kMaxSpecies; ++s) ma.mu[b][s] = (b < p.batch && s < p.S) ? mu[b * p.S + s] : 0.0;
   if (fused && tma) {
+    // programmatic dependent launches between consecutive passes of one
+    // stream, except while stage events sit between them or a graph is
+    // being captured
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CDFT_CUDA(cudaStreamIsCapturing(stream, &cap));
+    plan_.pdl = pdl_on_ && !timing_run_ && cap == cudaStreamCaptureStatusNone;
     // fused path: stages 4-6 in plane chunks (one chunk while stage timing)
     fused_forward(rho, stream);
     if constexpr (sizeof(R) == sizeof(float)) fused_middle<R>(rho, vext, force, !timing_run_, stream);
@@ -1061,6 +1071,11 @@ void Engine::set_anchor(Engine& fp64, const double* rho_a, cudaStream_t stream) 
   if (fp64.take_error(stream)) throw Error(-2, "anchor: the FP64 evaluation of the anchor state failed");
   if (!anchored_) ++generation_;
   anchored_ = true;
+}
+
+void Engine::set_dependent_launch(bool on) {
+  if (on != pdl_on_) ++generation_;
+  pdl_on_ = on;
 }
 
 void Engine::clear_anchor() {

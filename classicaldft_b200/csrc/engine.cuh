@@ -152,6 +152,10 @@ class Engine {
   void set_anchor(Engine& fp64, const double* rho_a, cudaStream_t stream);
   void clear_anchor();
   bool anchored() const { return anchored_; }
+  // Programmatic dependent launch between consecutive passes of the fused
+  // path (on by default; results are the same either way).
+  void set_dependent_launch(bool on);
+  bool dependent_launch() const { return pdl_on_; }
   // FP64 engines: after evaluate(), the real-space channels, derivative
   // channels and back-convolution (before dV) of the evaluated state.
   void export_fields(double* chan, double* deriv, double* hs, cudaStream_t stream) const;
@@ -282,6 +286,7 @@ class Engine {
   long long stage_count_ = 0;
 
   bool anchored_ = false;
+  bool pdl_on_ = true;
   double* anc_rho_ = nullptr;  // B*S*N
   double* anc_n_ = nullptr;    // B*n_chan*N
   double* anc_d_ = nullptr;    // B*n_deriv*N

@@ -832,6 +832,8 @@ __global__ void __launch_bounds__(kTmaTile, 5) k_pointwise_tma(EvalParams p, con
                                                             RT* __restrict__ deriv, PointwiseArgs a_all,
                                                             int* err, long long p0, long long pn, int blk0,
                                                             int nblk) {
+  pdl_trigger();
+  pdl_wait();
   constexpr bool TENSOR = model_has_tensor(MODEL);
   using L = Lay<MULTI, TENSOR>;
   constexpr bool SPLIT = sizeof(RT) == sizeof(float);
@@ -1042,6 +1044,8 @@ __global__ void __launch_bounds__(kTmaTile, MINB) k_pointwise1_tma(EvalParams p,
                                                              float* __restrict__ deriv, PointwiseArgs a_all,
                                                              int* err, long long p0, long long pn, int blk0,
                                                              int nblk) {
+  pdl_trigger();
+  pdl_wait();
   constexpr bool TENSOR = model_has_tensor(MODEL);
   using L = Lay<false, TENSOR>;
   constexpr int NF = L::NFMT;

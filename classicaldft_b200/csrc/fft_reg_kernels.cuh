@@ -107,6 +107,8 @@ template <int NY, int NZ, typename IN, int NT = RPlane<NY, NZ>::NT>
 __global__ void __launch_bounds__(NT)
     k_rplane_fwd(EvalParams p, const IN* __restrict__ in, int nseq, double* __restrict__ pmean,
                  cpx* __restrict__ out, int* err, int ix0, FftTables T) {
+  pdl_trigger();
+  pdl_wait();
   using P = RPlane<NY, NZ>;
   constexpr int M = P::M, LD = P::LD, AY = P::AY, BY = P::BY, AZ = P::AZ, BZ = P::BZ;
   constexpr int EY = P::EY, ER = P::ER, EZS = P::EZS, EZ = P::EZ;
@@ -312,6 +314,8 @@ __global__ void __launch_bounds__(NT)
     k_rplane_inv(EvalParams p, const cpx* __restrict__ in, int nseq, float* __restrict__ out_f,
                  double* __restrict__ force, const double* __restrict__ dbar, const __grid_constant__ MuArgs mu,
                  FinalArgs fin, int* err, int ix0, FftTables T) {
+  pdl_trigger();
+  pdl_wait();
   using P = RPlane<NY, NZ>;
   using L = Lay<MULTI, TENSOR>;
   constexpr int M = P::M, LD = P::LD, AY = P::AY, BY = P::BY, AZ = P::AZ, BZ = P::BZ;
@@ -691,6 +695,8 @@ template <int NX, int TQ, bool MULTI, bool TENSOR>
 __global__ void __launch_bounds__(256, 2)
     k_rcol_fwd(EvalParams p, const cpx* __restrict__ prho, const double* __restrict__ pmean,
                double* __restrict__ mean_out, const float* __restrict__ wtab, cpx* __restrict__ q_out, FftTables T) {
+  pdl_trigger();
+  pdl_wait();
   using L = Lay<MULTI, TENSOR>;
   constexpr int NT = RCol<NX>::NT, TILE = NX * TQ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -775,6 +781,8 @@ template <int NX, int TQ, bool MULTI, bool TENSOR>
 __global__ void __launch_bounds__(256, 2)
     k_rcol_bwd(EvalParams p, const cpx* __restrict__ pd, const float* __restrict__ wtab, cpx* __restrict__ pf,
                FftTables T) {
+  pdl_trigger();
+  pdl_wait();
   using L = Lay<MULTI, TENSOR>;
   constexpr int NF = L::NFMT, NT = RCol<NX>::NT, TILE = NX * TQ;
   constexpr int AX = RCol<NX>::AX, BX = RCol<NX>::BX;
@@ -1065,6 +1073,8 @@ template <int NX, int TQ, bool TENSOR>
 __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
     k_rcol_fwd1(EvalParams p, const cpx* __restrict__ prho, const double* __restrict__ pmean,
                 double* __restrict__ mean_out, const float* __restrict__ wtab, cpx* __restrict__ q_out, FftTables T) {
+  pdl_trigger();
+  pdl_wait();
   using L = Lay<false, TENSOR>;
   using C = RCol1<NX, TQ>;
   constexpr int AX = C::AX, BX = C::BX, NT = C::NT, TILE = C::TILE;
@@ -1196,6 +1206,8 @@ template <int NX, int TQ, bool TENSOR>
 __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
     k_rcol_bwd1(EvalParams p, const cpx* __restrict__ pd, const float* __restrict__ wtab, cpx* __restrict__ pf,
                 FftTables T) {
+  pdl_trigger();
+  pdl_wait();
   using L = Lay<false, TENSOR>;
   using C = RCol1<NX, TQ>;
   constexpr int AX = C::AX, BX = C::BX, NT = C::NT, TILE = C::TILE, NF = L::NFMT;

@@ -155,13 +155,13 @@ void fused_col_fwd(const FusedPlan& f, const EvalParams& p, const fft::cpx* prho
       with_layout(p, [&](auto mc, auto tc) {
         constexpr int NX = decltype(xc)::value, TQ = decltype(qc)::value;
         constexpr bool MU = decltype(mc)::value, TE = decltype(tc)::value;
+        // (stream predecessor: the rho plane pass)
         if constexpr (MU)
-          rk::k_rcol_fwd<NX, TQ, MU, TE>
-              <<<dim3(f.col_tiles, p.batch), rk::RCol<NX>::NT, f.colf_smem, st>>>(p, prho, pmean, mean, wtab, q, T);
+          launch_k(rk::k_rcol_fwd<NX, TQ, MU, TE>, dim3(f.col_tiles, p.batch), dim3(rk::RCol<NX>::NT), f.colf_smem,
+                   st, f.pdl, p, prho, pmean, mean, wtab, q, T);
         else if constexpr (TQ == 16)
-          rk::k_rcol_fwd1<NX, TQ, TE>
-              <<<dim3(f.col_tiles, p.batch), rk::RCol1<NX, TQ>::NT, f.colf_smem, st>>>(p, prho, pmean, mean, wtab,
-                                                                                          q, T);
+          launch_k(rk::k_rcol_fwd1<NX, TQ, TE>, dim3(f.col_tiles, p.batch), dim3(rk::RCol1<NX, TQ>::NT),
+                   f.colf_smem, st, f.pdl, p, prho, pmean, mean, wtab, q, T);
       });
     });
   });
@@ -185,8 +185,9 @@ void fused_plane_fwd_deriv(const FusedPlan& f, const EvalParams& p, const float*
                            int ix0, int nplanes, const FftTables& T, cudaStream_t st) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
-    rk::k_rplane_fwd<NY, NZ, float><<<dim3(nplanes, p.L.n_deriv, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(
-        p, deriv_r, p.L.n_deriv, nullptr, pd, err, ix0, T);
+    // (stream predecessor: the chunk's pointwise kernel)
+    launch_k(rk::k_rplane_fwd<NY, NZ, float>, dim3(nplanes, p.L.n_deriv, p.batch), dim3(rk::RPlane<NY, NZ>::NT),
+             f.plane_smem, st, f.pdl, p, deriv_r, p.L.n_deriv, (double*)nullptr, pd, err, ix0, T);
   });
   CDFT_CUDA(cudaGetLastError());
 }
@@ -217,8 +218,9 @@ void fused_plane_inv_epi(const FusedPlan& f, const EvalParams& p, const fft::cpx
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
     with_layout(p, [&](auto mc, auto tc) {
       constexpr int NT = rk::RPlane<NY, NZ>::NT_WIDE;
-      rk::k_rplane_inv<NY, NZ, true, decltype(mc)::value, decltype(tc)::value, NT>
-          <<<dim3(p.nx, p.S, p.batch), NT, f.plane_smem, st>>>(p, pf, p.S, nullptr, force, dbar, mu, fin, err, 0, T);
+      // (stream predecessor: the backward column pass)
+      launch_k(rk::k_rplane_inv<NY, NZ, true, decltype(mc)::value, decltype(tc)::value, NT>, dim3(p.nx, p.S, p.batch),
+               dim3(NT), f.plane_smem, st, f.pdl, p, pf, p.S, (float*)nullptr, force, dbar, mu, fin, err, 0, T);
     });
   });
   CDFT_CUDA(cudaGetLastError());

@@ -14,6 +14,10 @@ struct FusedPlan {
   int tq = 0;         // columns per column-pass tile
   int col_tiles = 0;  // column-pass CTAs per problem
   bool tq32 = false;  // several species: 32-column tiles fit (16 always do)
+  // programmatic dependent launch of the passes whose stream predecessor is
+  // the previous pass (set per evaluation: off while timing stages or
+  // capturing a graph)
+  bool pdl = false;
 };
 
 // Column tile width of the plan (16, or 32 where tq32): false, plan

@@ -435,6 +435,16 @@ class Engine:
         return bool(a.value)
 
     @property
+    def dependent_launch(self) -> bool:
+        """Programmatic dependent launch between the fused path's passes."""
+        w = ctypes.c_int()
+        _lib.check(_lib.lib().cdft_engine_set_dependent_launch(self.handle, -1, ctypes.byref(w)))
+        return bool(w.value)
+
+    def set_dependent_launch(self, on: bool):
+        _lib.check(_lib.lib().cdft_engine_set_dependent_launch(self.handle, 1 if on else 0, None))
+
+    @property
     def pointwise_spread(self) -> int:
         """Divisor of the pointwise grid per plane chunk (0: the chunk count)."""
         d = ctypes.c_int()

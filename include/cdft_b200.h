@@ -631,6 +631,14 @@ CDFT_API int cdft_engine_set_column_tile(cdft_engine* engine, int tile);
 CDFT_API int cdft_engine_column_tile(const cdft_engine* engine, int* tile);
 CDFT_API int cdft_engine_set_pointwise_spread(cdft_engine* engine, int spread);
 
+/* Programmatic dependent launch between consecutive passes of the fused path
+ * (a pass may be scheduled while its predecessor in the stream finishes and
+ * waits in the kernel for its completion): on = 1 (default) or 0, -1 leaves
+ * it; was (optional) receives the setting before the call.  Results are
+ * the same either way; it is off while stage timing runs or a graph is
+ * being captured. */
+CDFT_API int cdft_engine_set_dependent_launch(cdft_engine* engine, int on, int* was);
+
 /* Anchored split (no reference counterpart; mixed-precision engines): the
  * mixed path transforms rho - mean in FP32, so its round-off scales with the
  * density's own swing, which for a solid is the peak height.  From

@@ -104,3 +104,21 @@ def test_headline_state_every_pointwise_variant(headline):
     with pytest.raises(ValueError):  # one species: 16-column tiles only
         w.engine.set_column_tile(32)
     w.engine.close()
+
+
+def test_headline_state_dependent_launch_same_results(headline):
+    """Programmatic dependent launch between the passes changes when a pass
+    is scheduled, not what it computes: F and forces bitwise equal on and
+    off (four plane chunks, the launch order the bench uses)."""
+    model, rho, mu, ref = headline
+    w = cd.make_weights(cd.WhiteBearII(), model, cd.MIXED)
+    w.engine.set_plane_chunks(4)
+    assert w.engine.dependent_launch
+    on = cd.total(model, [rho], w, mu)
+    w.engine.set_dependent_launch(False)
+    assert not w.engine.dependent_launch
+    off = cd.total(model, [rho], w, mu)
+    assert on.free_energy == off.free_energy
+    assert np.array_equal(on.forces[0], off.forces[0])
+    assert rel_err(on.free_energy, ref.free_energy) <= 1e-9
+    w.engine.close()
