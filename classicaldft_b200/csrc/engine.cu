@@ -883,11 +883,9 @@ void Engine::run(const double* rho, const double* vext, const double* mu, double
     for (int s = 0; s < kMaxSpecies; ++s) ma.mu[b][s] = (b < p.batch && s < p.S) ? mu[b * p.S + s] : 0.0;
   if (fused && tma) {
     // programmatic dependent launches between consecutive passes of one
-    // stream, except while stage events sit between them or a graph is
-    // being captured
-    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    CDFT_CUDA(cudaStreamIsCapturing(stream, &cap));
-    plan_.pdl = pdl_on_ && !timing_run_ && cap == cudaStreamCaptureStatusNone;
+    // stream (captured graphs keep them as programmatic edges), except
+    // while stage events sit between them
+    plan_.pdl = pdl_on_ && !timing_run_;
     // fused path: stages 4-6 in plane chunks (one chunk while stage timing)
     fused_forward(rho, stream);
     if constexpr (sizeof(R) == sizeof(float)) fused_middle<R>(rho, vext, force, !timing_run_, stream);

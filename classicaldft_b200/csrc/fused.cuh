@@ -15,8 +15,7 @@ struct FusedPlan {
   int col_tiles = 0;  // column-pass CTAs per problem
   bool tq32 = false;  // several species: 32-column tiles fit (16 always do)
   // programmatic dependent launch of the passes whose stream predecessor is
-  // the previous pass (set per evaluation: off while timing stages or
-  // capturing a graph)
+  // the previous pass (set per evaluation: off while timing stages)
   bool pdl = false;
 };
 

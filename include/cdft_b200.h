@@ -635,8 +635,8 @@ CDFT_API int cdft_engine_set_pointwise_spread(cdft_engine* engine, int spread);
  * (a pass may be scheduled while its predecessor in the stream finishes and
  * waits in the kernel for its completion): on = 1 (default) or 0, -1 leaves
  * it; was (optional) receives the setting before the call.  Results are
- * the same either way; it is off while stage timing runs or a graph is
- * being captured. */
+ * the same either way; it is off while stage timing runs (captured graphs
+ * keep the launches as programmatic edges). */
 CDFT_API int cdft_engine_set_dependent_launch(cdft_engine* engine, int on, int* was);
 
 /* Anchored split (no reference counterpart; mixed-precision engines): the
