@@ -127,11 +127,12 @@ class L2Flush:
 # CSV by `python bench.py --traffic-table <ncu.csv>`; a stage missing from it
 # reports traffic null.
 TRAFFIC_TABLE = os.path.join(ROOT, "profiles", "traffic_128cubed_mixed.txt")
-FUSED_KERNELS = {  # kernel-name prefix in the ncu list -> stage
+FUSED_KERNELS = {  # kernel-name prefix in the ncu list -> stage (bool arguments print as 0 / 1)
     "k_rplane_fwd<128, 128, double": "plane_fwd_rho", "k_rcol_fwd1": "col_fwd",
-    "k_rplane_inv<128, 128, false": "plane_inv_channels", "k_pointwise_tma": "pointwise",
+    "k_rplane_inv<128, 128, 0": "plane_inv_channels", "k_rplane_inv<128, 128, false": "plane_inv_channels",
+    "k_pointwise1_tma": "pointwise", "k_pointwise_tma": "pointwise",
     "k_rplane_fwd<128, 128, float": "plane_fwd_derivatives", "k_rcol_bwd1": "col_bwd",
-    "k_rplane_inv<128, 128, true": "plane_inv_epilogue"}
+    "k_rplane_inv<128, 128, 1": "plane_inv_epilogue", "k_rplane_inv<128, 128, true": "plane_inv_epilogue"}
 
 
 def measured_traffic():
@@ -181,7 +182,7 @@ def traffic_table(csv_path):
     for (stage, _), b in per.items():
         acc.setdefault(stage, []).append(b)
     print("# stage  DRAM_bytes_per_launch  launches   (from " + os.path.basename(csv_path) + ")")
-    for stage in FUSED_KERNELS.values():
+    for stage in dict.fromkeys(FUSED_KERNELS.values()):
         if stage in acc:
             v = acc[stage]
             print(f"{stage} {sum(v) / len(v):.4e} {len(v)}")
