@@ -1143,6 +1143,21 @@ __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
       if (!col.valid) return;
       cpx* o1 = out + (long long)c1 * Nk + (long long)n2 * plane;
       cpx* o2 = out + (long long)(c2 < 0 ? 0 : c2) * Nk + (long long)n2 * plane;
+      if (mix) {  // (uniform per basis: the a kx^2 basis alone reads the kept transforms)
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+          const int n1 = n1_0 + i * dn1;
+          const int x = BX * n1 + n2;
+          const long long off = (long long)(BX * n1) * plane;
+          cpx v1 = scale(a[i], f1), v2 = scale(a[i], f2);
+          const cpx s1 = S1[x * TQ + q], s2 = S2[x * TQ + q];
+          v1 = v1 + scale(s1, g1) + scale(s2, h1);
+          v2 = v2 + scale(s1, g2) + scale(s2, h2);
+          o1[off] = v1;
+          o2[off] = v2;
+        }
+        return;
+      }
       const cpx c = scale(s_nyq[q], f2);
 #pragma unroll
       for (int i = 0; i < K; ++i) {
@@ -1150,11 +1165,6 @@ __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
         const int x = BX * n1 + n2;
         const long long off = (long long)(BX * n1) * plane;
         cpx v1 = scale(a[i], f1), v2 = scale(a[i], f2);
-        if (mix) {
-          const cpx s1 = S1[x * TQ + q], s2 = S2[x * TQ + q];
-          v1 = v1 + scale(s1, g1) + scale(s2, h1);
-          v2 = v2 + scale(s1, g2) + scale(s2, h2);
-        }
         if (nyq2) v2 = (x & 1) ? cpx{-c.x, -c.y} : c;
         o1[off] = v1;
         if (c2 >= 0) o2[off] = v2;
