@@ -1158,18 +1158,29 @@ __global__ void __launch_bounds__(RCol1<NX, TQ>::NT, 2)
         }
         return;
       }
-      const cpx c = scale(s_nyq[q], f2);
+      if (c2 >= 0) {  // (uniform per basis) two channels, no kept transform
+        const cpx c = scale(s_nyq[q], f2);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+          const int n1 = n1_0 + i * dn1;
+          const int x = BX * n1 + n2;
+          const long long off = (long long)(BX * n1) * plane;
+          cpx v1 = scale(a[i], f1), v2 = scale(a[i], f2);
+          if (nyq2) v2 = (x & 1) ? cpx{-c.x, -c.y} : c;
+          o1[off] = v1;
+          o2[off] = v2;
+        }
+        return;
+      }
+      // one channel, and the transform kept in S1 or S2 for the a kx^2 basis
+      cpx* S = keep == 1 ? S1 : S2;
 #pragma unroll
       for (int i = 0; i < K; ++i) {
         const int n1 = n1_0 + i * dn1;
         const int x = BX * n1 + n2;
         const long long off = (long long)(BX * n1) * plane;
-        cpx v1 = scale(a[i], f1), v2 = scale(a[i], f2);
-        if (nyq2) v2 = (x & 1) ? cpx{-c.x, -c.y} : c;
-        o1[off] = v1;
-        if (c2 >= 0) o2[off] = v2;
-        if (keep == 1) S1[x * TQ + q] = a[i];
-        if (keep == 2) S2[x * TQ + q] = a[i];
+        o1[off] = scale(a[i], f1);
+        if (keep) S[x * TQ + q] = a[i];
       }
     });
     buf ^= 1;
