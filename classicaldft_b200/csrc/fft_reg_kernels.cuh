@@ -947,24 +947,23 @@ __device__ __forceinline__ bool rk_basis_weights(int j, const RTab<RCol1<NX, TQ>
                                                  int k1, float dkx, const RColumn& col,
                                                  float (&w)[RCol1<NX, TQ>::BX]) {
   constexpr int AX = RCol1<NX, TQ>::AX, BX = RCol1<NX, TQ>::BX;
+  // (j is uniform: one branch per basis; only the kx bases form kx)
+  if (j == kBW3 || j == kBW2 || j == kBV || j == kBTA) {
 #pragma unroll
-  for (int k2 = 0; k2 < BX; ++k2) {
-    const RKv v = rk_task_element<NX>(p, k1 + AX * k2, dkx, col);
-    const float kx = v.k[0];
-    if (j == kBW3)
-      w[k2] = t.w3[k2];
-    else if (j == kBW2)
-      w[k2] = t.w2[k2];
-    else if (j == kBVX)
-      w[k2] = t.fv[k2] * (kx * v.o[0]);
-    else if (j == kBV)
-      w[k2] = t.fv[k2];
-    else if (j == kBTX)
-      w[k2] = t.a[k2] * (kx * v.cxy);
-    else if (j == kBTA)
-      w[k2] = t.a[k2];
-    else
-      w[k2] = t.a[k2] * (kx * kx);
+    for (int k2 = 0; k2 < BX; ++k2)
+      w[k2] = j == kBW3 ? t.w3[k2] : j == kBW2 ? t.w2[k2] : j == kBV ? t.fv[k2] : t.a[k2];
+  } else {
+#pragma unroll
+    for (int k2 = 0; k2 < BX; ++k2) {
+      const RKv v = rk_task_element<NX>(p, k1 + AX * k2, dkx, col);
+      const float kx = v.k[0];
+      if (j == kBVX)
+        w[k2] = t.fv[k2] * (kx * v.o[0]);
+      else if (j == kBTX)
+        w[k2] = t.a[k2] * (kx * v.cxy);
+      else
+        w[k2] = t.a[k2] * (kx * kx);
+    }
   }
   return j == kBVX || j == kBV;
 }
