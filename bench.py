@@ -1013,6 +1013,7 @@ def main():
                          "back to back, as a profiler's serialised launch list sees them)")
     ap.add_argument("--pointwise", type=int, default=-1,
                     help="with --plane-chunks: the pointwise kernel variant (0 generic, 1 / 2 one species at 5 / 6 "
+                         "CTAs per SM, 3 branch-free, 4 / 5 branch-free with two points per thread at 3 / 4 "
                          "CTAs per SM; -1: the engine's default)")
     ap.add_argument("--pointwise-spread", type=int, default=-1,
                     help="with --plane-chunks: divisor of the pointwise grid per chunk (0: the chunk count)")

@@ -151,7 +151,7 @@ void Engine::launch_pointwise_tma(const R* chan, R* deriv, const PointwiseArgs& 
         with_nmf(p.M, [&](auto nc) {
           constexpr int NMF = decltype(nc)::value;
           const int v = pw_variant_;
-          const size_t smem = v == 4 ? (vext ? tma1_smem2_v_ : tma1_smem2_) : (vext ? tma1_smem_v_ : tma1_smem_);
+          const size_t smem = v >= 4 ? (vext ? tma1_smem2_v_ : tma1_smem2_) : (vext ? tma1_smem_v_ : tma1_smem_);
           // (stream predecessor: the chunk's channel plane pass)
           auto go = [&](auto kern) {
             launch_k(kern, g, dim3(kTmaTile), smem, st, plan_.pdl, p, chan, deriv, a, err_, p0, pn, blk0, nblk);
@@ -160,12 +160,14 @@ void Engine::launch_pointwise_tma(const R* chan, R* deriv, const PointwiseArgs& 
             if (v == 1) go(k_pointwise1_tma<MD, NMF, true, 5>);
             else if (v == 2) go(k_pointwise1_tma<MD, NMF, true, 6>);
             else if (v == 3) go(k_pointwise1_tma<MD, NMF, true, 5, 1, true>);
-            else go(k_pointwise1_tma<MD, NMF, true, 3, 2, true>);
+            else if (v == 4) go(k_pointwise1_tma<MD, NMF, true, 3, 2, true>);
+            else go(k_pointwise1_tma<MD, NMF, true, 4, 2, true>);
           } else {
             if (v == 1) go(k_pointwise1_tma<MD, NMF, false, 5>);
             else if (v == 2) go(k_pointwise1_tma<MD, NMF, false, 6>);
             else if (v == 3) go(k_pointwise1_tma<MD, NMF, false, 5, 1, true>);
-            else go(k_pointwise1_tma<MD, NMF, false, 3, 2, true>);
+            else if (v == 4) go(k_pointwise1_tma<MD, NMF, false, 3, 2, true>);
+            else go(k_pointwise1_tma<MD, NMF, false, 4, 2, true>);
           }
         });
       });
@@ -310,7 +312,7 @@ Engine::Engine(const EngineSpec& spec) {
         const int sb2 = kTmaStages * tma1_stage_bytes<NMF, false, TE, 2>();
         const int sv2 = kTmaStages * tma1_stage_bytes<NMF, true, TE, 2>();
         // the occupancy of the vext form (the larger stages) sizes both forms' grids
-        int per[4] = {0, 0, 0, 0};
+        int per[5] = {0, 0, 0, 0, 0};
         auto prep = [&](auto kb, auto kv, int b, int v, int* out) {
           CDFT_CUDA(cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
           CDFT_CUDA(cudaFuncSetAttribute(kv, cudaFuncAttributeMaxDynamicSharedMemorySize, v));
@@ -322,7 +324,9 @@ Engine::Engine(const EngineSpec& spec) {
              &per[2]);
         prep(k_pointwise1_tma<MD, NMF, false, 3, 2, true>, k_pointwise1_tma<MD, NMF, true, 3, 2, true>, sb2, sv2,
              &per[3]);
-        for (int v = 0; v < 4; ++v) grid_pw1_[v] = per_problem((long long)sms * std::max(per[v], 1));
+        prep(k_pointwise1_tma<MD, NMF, false, 4, 2, true>, k_pointwise1_tma<MD, NMF, true, 4, 2, true>, sb2, sv2,
+             &per[4]);
+        for (int v = 0; v < 5; ++v) grid_pw1_[v] = per_problem((long long)sms * std::max(per[v], 1));
         tma1_smem_ = (size_t)sb;
         tma1_smem_v_ = (size_t)sv;
         tma1_smem2_ = (size_t)sb2;
@@ -340,7 +344,7 @@ Engine::Engine(const EngineSpec& spec) {
   partials_ = dalloc<double>(
       (size_t)B *
           ((size_t)std::max({grid_pw_, grid_tma_, grid_stream_, grid_pw1_[0], grid_pw1_[1], grid_pw1_[2],
-                             grid_pw1_[3]}) * kMaxChunks + 8) *
+                             grid_pw1_[3], grid_pw1_[4]}) * kMaxChunks + 8) *
           p.n_terms,
       tot);
   err_ = dalloc<int>(1, tot);
@@ -584,7 +588,7 @@ void Engine::set_col_tile(int tq) {
 int Engine::col_tile() const { return fusable_ ? plan_.tq : 0; }
 
 void Engine::set_pointwise(int v) {
-  if (v < 0 || v >= kPointwiseVariants) throw std::invalid_argument("pointwise variant: 0 .. 4");
+  if (v < 0 || v >= kPointwiseVariants) throw std::invalid_argument("pointwise variant: 0 .. 5");
   if (v > 0 && !pw1_)
     throw std::invalid_argument("pointwise variant: the one-species kernel needs a mixed-precision engine with one "
                                 "species and at most two interactions");

@@ -107,7 +107,7 @@ class Engine {
   // Several species also tune the column tile width (16, 32), and every
   // chunk count k its pointwise spread d (1, 2, 4, 8 up to k):
   // ms[((tile_index * kPointwiseVariants + v) * kMaxChunks + k - 1) * kSpreads + log2 d].
-  static constexpr int kPointwiseVariants = 5;
+  static constexpr int kPointwiseVariants = 6;
   static constexpr int kSpreads = 4;
   int autotune(const double* rho, const double* vext, const double* mu, cudaStream_t stream, int reps,
                double* ms, int* variant, int* tile = nullptr, int* spread = nullptr);
@@ -241,11 +241,11 @@ class Engine {
   // grid_* are CTAs per problem: a launch has grid_* x B CTAs
   size_t tma_smem_ = 0, tma_smem_v_ = 0;
   bool pw1_ = false;  // one species, <= 2 mean-field channels, mixed: k_pointwise1_tma exists
-  // pointwise kernel of the TMA path: 0 generic (k_pointwise_tma), 1 .. 4
+  // pointwise kernel of the TMA path: 0 generic (k_pointwise_tma), 1 .. 5
   // the one-species kernel k_pointwise1_tma (grid grid_pw1_[v - 1])
   int pw_variant_ = 0;
   int pw_div_ = 0;  // pointwise grid divisor of a plane chunk (0: the chunk count)
-  int grid_pw1_[4] = {0, 0, 0, 0};
+  int grid_pw1_[5] = {0, 0, 0, 0, 0};
   size_t tma1_smem_ = 0, tma1_smem_v_ = 0;    // one point per thread
   size_t tma1_smem2_ = 0, tma1_smem2_v_ = 0;  // two points per thread
   template <typename R>

@@ -68,6 +68,8 @@ def make_grid(dx: float, box) -> Grid:
 WEEKS_CHANDLER_ANDERSEN = "WeeksChandlerAndersen"
 BARKER_HENDERSON = "BarkerHenderson"
 _SPLIT = {WEEKS_CHANDLER_ANDERSEN: _lib.SPLIT_WCA, BARKER_HENDERSON: _lib.SPLIT_BH}
+# pointwise kernel variants of the TMA path (CDFT_POINTWISE_VARIANTS)
+POINTWISE_VARIANTS = 6
 
 
 @dataclass
@@ -398,7 +400,7 @@ class Engine:
         Returns ((chunks, variant, tile, spread),
         {(tile, variant, count, spread): ms})."""
         choice = (ctypes.c_int * 4)()
-        ms = (ctypes.c_double * (2 * 5 * 8 * 4))()
+        ms = (ctypes.c_double * (2 * POINTWISE_VARIANTS * 8 * 4))()
         mu_arr = None
         if mu is not None:
             mu_arr = (ctypes.c_double * (self.batch * self.S))(*[float(m) for m in mu])
@@ -406,8 +408,8 @@ class Engine:
                                                       ctypes.c_void_p(vext_ptr or None), mu_arr,
                                                       ctypes.c_void_p(stream or None), int(reps), choice, ms))
         self.info = self._query_info()
-        idx = {(16 << t, v, k + 1, 1 << d): ((t * 5 + v) * 8 + k) * 4 + d
-               for t in range(2) for v in range(5) for k in range(8) for d in range(4)}
+        idx = {(16 << t, v, k + 1, 1 << d): ((t * POINTWISE_VARIANTS + v) * 8 + k) * 4 + d
+               for t in range(2) for v in range(POINTWISE_VARIANTS) for k in range(8) for d in range(4)}
         return (choice[0], choice[1], choice[2], choice[3]), {key: ms[i] for key, i in idx.items() if ms[i] > 0.0}
 
     def set_anchor(self, fp64_engine: "Engine", rho_anchor, stream: int = 0):
@@ -467,7 +469,7 @@ class Engine:
     @property
     def pointwise(self) -> int:
         """Pointwise kernel variant: 0 generic; one species: 1 / 2 (5 / 6 CTAs per SM), 3 the branch-free
-        FP64 path, 4 the same with two points per thread."""
+        FP64 path, 4 / 5 the same with two points per thread (3 / 4 CTAs per SM)."""
         v, a = ctypes.c_int(), ctypes.c_int()
         _lib.check(_lib.lib().cdft_engine_pointwise(self.handle, ctypes.byref(v), ctypes.byref(a)))
         return v.value
@@ -476,7 +478,7 @@ class Engine:
     def pointwise_variants(self) -> list:
         v, a = ctypes.c_int(), ctypes.c_int()
         _lib.check(_lib.lib().cdft_engine_pointwise(self.handle, ctypes.byref(v), ctypes.byref(a)))
-        return [0, 1, 2, 3, 4] if a.value else [0]
+        return list(range(POINTWISE_VARIANTS)) if a.value else [0]
 
     def set_pointwise(self, variant: int):
         _lib.check(_lib.lib().cdft_engine_set_pointwise(self.handle, int(variant)))

@@ -602,13 +602,13 @@ CDFT_API int cdft_engine_autotune(cdft_engine* engine, const double* rho, const 
                                   void* stream, int reps, int* chunks, double* ms);
 
 /* The pointwise kernel of the TMA-staged path (no reference counterpart):
- * 0 the generic kernel; 1 .. 4 the kernel specialised for one species and
+ * 0 the generic kernel; 1 .. 5 the kernel specialised for one species and
  * at most two interactions (mixed precision): 1 and 2 with its registers
- * sized for 5 or 6 CTAs per SM; 3 (5 CTAs per SM) and 4 (two points per
- * thread, 3 CTAs per SM) take a branch-free FP64 path in warps whose points
- * all have eta >= 1e-6 (one reciprocal for 1/eta and 1/(1 - eta)).  Every
- * variant gives the same results up to the rounding of the pointwise FP64
- * arithmetic.  available (out): 1 where 1 .. 4 exist.  The column passes of an engine with several species run tiles of
+ * sized for 5 or 6 CTAs per SM; 3 (5 CTAs per SM), 4 and 5 (two points per
+ * thread, 3 or 4 CTAs per SM) take a branch-free FP64 path in warps whose
+ * points all have eta >= 1e-6 (one reciprocal for 1/eta and 1/(1 - eta)).
+ * Every variant gives the same results up to the rounding of the pointwise
+ * FP64 arithmetic.  available (out): 1 where 1 .. 5 exist.  The column passes of an engine with several species run tiles of
  * 16 or (where the spectra fit in shared memory) 32 in-plane columns; one
  * species always 16 (cdft_engine_set_column_tile / cdft_engine_column_tile;
  * 0 without the fused path).  Each plane chunk's pointwise launch takes the
@@ -623,7 +623,7 @@ CDFT_API int cdft_engine_autotune(cdft_engine* engine, const double* rho, const 
  * for tile index t (0: 16, 1: 32), variant v, k chunks and spread d (0
  * where not tried; 2 * CDFT_POINTWISE_VARIANTS * CDFT_MAX_PLANE_CHUNKS *
  * CDFT_POINTWISE_SPREADS entries), choice = {chunks, variant, tile, spread}. */
-#define CDFT_POINTWISE_VARIANTS 5
+#define CDFT_POINTWISE_VARIANTS 6
 #define CDFT_POINTWISE_SPREADS 4
 CDFT_API int cdft_engine_set_pointwise(cdft_engine* engine, int variant);
 CDFT_API int cdft_engine_pointwise(const cdft_engine* engine, int* variant, int* available);

@@ -80,15 +80,15 @@ def test_headline_state_every_pointwise_variant(headline):
     """The generic and the one-species pointwise kernels evaluate the same
     expressions, and each meets the oracle's tolerances.  Their FP64 results
     may differ in the last bit (contraction of products into fused multiply-
-    adds is the compiler's choice per kernel, and the branch-free kernels 3
-    and 4 form 1/eta and 1/(1-eta) from one reciprocal), which can flip the
+    adds is the compiler's choice per kernel, and the branch-free kernels 3,
+    4 and 5 form 1/eta and 1/(1-eta) from one reciprocal), which can flip the
     FP32 rounding of a derivative channel: against the generic kernel the
     forces agree to 1e-8 of the largest force and F to 1e-13."""
     model, rho, mu, ref = headline
     w = cd.make_weights(cd.WhiteBearII(), model, cd.MIXED)
-    assert w.engine.pointwise_variants == [0, 1, 2, 3, 4]
+    assert w.engine.pointwise_variants == [0, 1, 2, 3, 4, 5]
     base = None
-    for v in (0, 1, 2, 3, 4):
+    for v in (0, 1, 2, 3, 4, 5):
         w.engine.set_pointwise(v)
         assert w.engine.pointwise == v
         res = cd.total(model, [rho], w, mu)
@@ -99,7 +99,7 @@ def test_headline_state_every_pointwise_variant(headline):
         assert force_err(res.forces, base.forces) <= 1e-8, v
         assert rel_err(res.free_energy, base.free_energy) <= 1e-13, v
     with pytest.raises(ValueError):
-        w.engine.set_pointwise(5)
+        w.engine.set_pointwise(6)
     assert w.engine.column_tile == 16
     with pytest.raises(ValueError):  # one species: 16-column tiles only
         w.engine.set_column_tile(32)
