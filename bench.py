@@ -105,6 +105,19 @@ def algorithmic_bytes(info, S=1, M=1, has_vext=False, fused=False):
     return sum(stage_bytes(info, S, M, has_vext, fused).values())
 
 
+def unfused_bytes(N, Nk, s, S=1, C=11, M=1):
+    """Compulsory HBM bytes of the unfused 25-transform decomposition of one
+    evaluation (the reference's own pass structure: hard_sphere.hpp:50-136,
+    mean_field.hpp:234-281, functionals.hpp:64-95): one read and one write per
+    FFT pass and per pointwise pass, C FMT channels per species (eta, n2, v2
+    and the six tensor components), M mean-field interactions, transforms in
+    s-byte reals, rho and the force FP64.  128^3 mixed (s = 4): 0.934 GB."""
+    Br, Bc, Bio = N * s, 2 * Nk * s, 8 * N
+    SC = S * C
+    return (S * Bio + 2 * S * Bc + M * Bc / 2 + 2 * (SC + M) * Bc + (SC + M) * Br + SC * Br + M * Br
+            + 2 * S * Bio + SC * Br + S * Bio + SC * Br + 2 * SC * Bc + 2 * S * Bc + 2 * S * Br + 2 * S * Bio)
+
+
 class L2Flush:
     """Between timed steps: write a 256 MiB buffer (more than the 126 MB L2),
     then read another, leaving L2 clean and cold."""
@@ -922,6 +935,7 @@ def run_ours(args, ws, rank, local, dist):
     info = eng.info
     fused = eng.transforms == "fused"
     nbytes = algorithmic_bytes(info, S=1, M=1, fused=fused)
+    ub = unfused_bytes(info["N"], info["Nk"], 4 if precision == cd.MIXED else 8)
     peak, peak_kind = hbm_peak()
     achieved = nbytes / (ms_step * 1e-3) / 1e9
     names = {cd.MIXED: "mixed", cd.FP64: "fp64"}
@@ -959,7 +973,11 @@ def run_ours(args, ws, rank, local, dist):
                                                                                  FUSED_KERNELS.values())
                                      else None),
                          "scope": ("one full evaluation (the seven fused-path kernels)" if fused
-                                   else "one full evaluation (cuFFT transforms + engine kernels)")}},
+                                   else "one full evaluation (cuFFT transforms + engine kernels)"),
+                         # the same time against the bytes of the unfused 25-transform
+                         # decomposition (what a pass-per-transform evaluation must move)
+                         "unfused_count": {"algorithmic_bytes": ub, "achieved": ub / (ms_step * 1e-3) / 1e9,
+                                           "frac": ub / (ms_step * 1e-3) / 1e9 / peak}}},
         "stages": stages,
         "sweep": sweep,
         "batched_128": batched,
