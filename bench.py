@@ -834,15 +834,17 @@ def run_ours(args, ws, rank, local, dist):
         # the engine's autotuner picks the plane-chunk count and the pointwise
         # kernel variant on this state
         (k, v, tq, sp), ms = eng.autotune_ex(rho.data_ptr(), mu=[0.0], reps=10)
-        tuned = {"chosen": {"plane_chunks": k, "pointwise_variant": v, "column_tile": tq, "pointwise_spread": sp},
+        pw_kept = eng.plane_width
+        tuned = {"chosen": {"plane_chunks": k, "pointwise_variant": v, "column_tile": tq, "pointwise_spread": sp,
+                            "plane_width": pw_kept},
                  "ms_per_eval": {f"t{tt}_v{vv}_k{c}_d{dd}": round(t, 5) for (tt, vv, c, dd), t in ms.items()}}
-        # programmatic dependent launch between the passes, off against on
-        # (back-to-back evaluations, CUDA events; the timed run uses on)
+        # back-to-back evaluations, CUDA events: programmatic dependent launch
+        # between the passes off against on (the timed run uses on), and the
+        # two middle plane widths at the chosen configuration
         f_tmp = torch.empty_like(rho)
         s_tmp = torch.zeros(10, dtype=torch.float64, device=dev)
-        dl = {}
-        for on in (False, True, False, True):
-            eng.set_dependent_launch(on)
+
+        def per_eval():
             for _ in range(3):
                 eng.total_device(rho.data_ptr(), None, [0.0], f_tmp.data_ptr(), s_tmp.data_ptr(), 0)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -851,8 +853,18 @@ def run_ours(args, ws, rank, local, dist):
                 eng.total_device(rho.data_ptr(), None, [0.0], f_tmp.data_ptr(), s_tmp.data_ptr(), 0)
             e1.record()
             torch.cuda.synchronize()
-            dl.setdefault("on_ms" if on else "off_ms", []).append(round(e0.elapsed_time(e1) / 50, 5))
+            return round(e0.elapsed_time(e1) / 50, 5)
+
+        dl, pw = {}, {}
+        for on in (False, True, False, True):
+            eng.set_dependent_launch(on)
+            dl.setdefault("on_ms" if on else "off_ms", []).append(per_eval())
+        for wide in (0, 1, 0, 1):
+            eng.set_plane_width(wide)
+            pw.setdefault(f"width{wide}_ms", []).append(per_eval())
+        eng.set_plane_width(pw_kept)
         tuned["dependent_launch"] = dl
+        tuned["plane_width"] = pw
     force = torch.empty_like(rho)
     scal = torch.zeros(10, dtype=torch.float64, device=dev)
     flush = L2Flush(torch, dev)

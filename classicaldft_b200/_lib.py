@@ -231,6 +231,8 @@ def lib():
         "cdft_engine_anchored": [vp, ctypes.POINTER(ctypes.c_int)],
         "cdft_engine_pointwise_spread": [vp, ctypes.POINTER(ctypes.c_int)],
         "cdft_engine_column_tile": [vp, ctypes.POINTER(ctypes.c_int)],
+        "cdft_engine_set_plane_width": [vp, ctypes.c_int],
+        "cdft_engine_plane_width": [vp, ctypes.POINTER(ctypes.c_int)],
         "cdft_minimize_group": [ctypes.c_int, ctypes.POINTER(CGroupMember), ctypes.POINTER(CMinimizerConfig), vp],
         "cdft_ddft_last_step": [vp, ctypes.POINTER(ctypes.c_int), c_double_p],
         "cdft_eigen_solve_ex": [vp, vp, ctypes.POINTER(CEigenConfig), vp, ctypes.c_double, vp, ctypes.c_int,

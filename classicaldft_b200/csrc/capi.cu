@@ -445,6 +445,20 @@ int cdft_engine_pointwise_spread(const cdft_engine* engine, int* spread) {
   });
 }
 
+int cdft_engine_set_plane_width(cdft_engine* engine, int wide) {
+  return guarded([&] {
+    if (!engine) throw std::invalid_argument("engine is NULL");
+    engine->impl->set_plane_width(wide);
+  });
+}
+
+int cdft_engine_plane_width(const cdft_engine* engine, int* wide) {
+  return guarded([&] {
+    if (!engine || !wide) throw std::invalid_argument("engine and wide are required");
+    *wide = engine->impl->plane_width();
+  });
+}
+
 int cdft_engine_set_column_tile(cdft_engine* engine, int tile) {
   return guarded([&] {
     if (!engine) throw std::invalid_argument("engine is NULL");

@@ -21,6 +21,7 @@ std::map<std::string, int> g_tune_chunks;
 std::map<std::string, int> g_tune_variant;
 std::map<std::string, int> g_tune_tile;
 std::map<std::string, int> g_tune_spread;
+std::map<std::string, int> g_tune_plane;
 }  // namespace
 
 namespace {
@@ -473,6 +474,8 @@ void Engine::setup_fused() {
     if (it != g_tune_chunks.end()) chunks_ = it->second;
     const auto tt = g_tune_tile.find(tune_key_);
     if (tt != g_tune_tile.end()) fused_plan_set_tile(p, &plan_, tt->second);
+    const auto tp = g_tune_plane.find(tune_key_);
+    if (tp != g_tune_plane.end()) plan_.plane_wide = tp->second != 0;
   }
   ensure_chunk_streams(chunks_);
 }
@@ -493,13 +496,14 @@ void Engine::ensure_chunk_streams(int k) {
 // Every (plane-chunk count, pointwise variant) pair the engine has, timed on
 // the caller's state; the fastest is kept and cached for the shape.
 int Engine::autotune(const double* rho, const double* vext, const double* mu, cudaStream_t stream, int reps,
-                     double* ms, int* variant, int* tile, int* spread) {
+                     double* ms, int* variant, int* tile, int* spread, int* plane) {
   constexpr int kTiles = 2;  // column tile widths 16, 32
   if (ms)
     for (int k = 0; k < kPointwiseVariants * kMaxChunks * kTiles * kSpreads; ++k) ms[k] = 0.0;
   if (variant) *variant = pw_variant_;
   if (tile) *tile = col_tile();
   if (spread) *spread = pw_div_;
+  if (plane) *plane = plane_width();
   const bool tune_chunks = fusable_ && fused_;
   const bool tune_tiles = tune_chunks && p_.S > 1;
   if (!tune_chunks && !pw1_) return chunks_;
@@ -515,45 +519,52 @@ int Engine::autotune(const double* rho, const double* vext, const double* mu, cu
   // engines without a tile choice time their current tile (row 0 of the
   // table where they have no fused path)
   const int tile_now = col_tile() == 32 ? 32 : 16;
-  int best = chunks_, best_v = pw_variant_, best_t = col_tile(), best_d = pw_div_;
+  int best = chunks_, best_v = pw_variant_, best_t = col_tile(), best_d = pw_div_, best_w = plane_width();
   double best_ms = 0.0;
-  for (int ti = 0; ti < kTiles; ++ti) {
-    const int tq = 16 << ti;
-    if (tune_tiles) {
-      if (!fused_plan_set_tile(p_, &plan_, tq)) continue;
-      ++generation_;
-    } else if (tq != tile_now) {
-      continue;
-    }
-    for (int v = 0; v < kPointwiseVariants; ++v) {
-      if (v > 0 && !pw1_) break;
-      set_pointwise(v);
-      for (int k = 1; k <= kMaxChunks; k *= 2) {
-        if (tune_chunks) {
-          if (p_.nx % k != 0) continue;
-          set_chunks(k);
-        } else if (k != chunks_) {
-          continue;
-        }
-        for (int di = 0; di < kSpreads; ++di) {
-          const int d = 1 << di;
-          if (d > k || (!tune_chunks && d > 1)) break;
-          set_pw_spread(d);
-          for (int w = 0; w < 2; ++w) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
-          CDFT_CUDA(cudaEventRecord(e0, stream));
-          for (int r = 0; r < reps; ++r) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
-          CDFT_CUDA(cudaEventRecord(e1, stream));
-          CDFT_CUDA(cudaEventSynchronize(e1));
-          float t = 0.0f;
-          CDFT_CUDA(cudaEventElapsedTime(&t, e0, e1));
-          const double per = (double)t / reps;
-          if (ms) ms[((ti * kPointwiseVariants + v) * kMaxChunks + k - 1) * kSpreads + di] = per;
-          if (best_ms == 0.0 || per < best_ms) {
-            best_ms = per;
-            best = k;
-            best_v = v;
-            best_d = d;
-            if (tune_tiles) best_t = tq;
+  for (int wi = 0; wi < (tune_chunks ? 2 : 1); ++wi) {
+    if (tune_chunks) set_plane_width(wi);
+    for (int ti = 0; ti < kTiles; ++ti) {
+      const int tq = 16 << ti;
+      if (tune_tiles) {
+        if (!fused_plan_set_tile(p_, &plan_, tq)) continue;
+        ++generation_;
+      } else if (tq != tile_now) {
+        continue;
+      }
+      for (int v = 0; v < kPointwiseVariants; ++v) {
+        if (v > 0 && !pw1_) break;
+        set_pointwise(v);
+        for (int k = 1; k <= kMaxChunks; k *= 2) {
+          if (tune_chunks) {
+            if (p_.nx % k != 0) continue;
+            set_chunks(k);
+          } else if (k != chunks_) {
+            continue;
+          }
+          for (int di = 0; di < kSpreads; ++di) {
+            const int d = 1 << di;
+            if (d > k || (!tune_chunks && d > 1)) break;
+            set_pw_spread(d);
+            for (int w = 0; w < 2; ++w) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
+            CDFT_CUDA(cudaEventRecord(e0, stream));
+            for (int r = 0; r < reps; ++r) evaluate(rho, vext, mu, h_force_, h_scalars_, stream);
+            CDFT_CUDA(cudaEventRecord(e1, stream));
+            CDFT_CUDA(cudaEventSynchronize(e1));
+            float t = 0.0f;
+            CDFT_CUDA(cudaEventElapsedTime(&t, e0, e1));
+            const double per = (double)t / reps;
+            if (ms) {
+              double& slot = ms[((ti * kPointwiseVariants + v) * kMaxChunks + k - 1) * kSpreads + di];
+              if (slot == 0.0 || per < slot) slot = per;
+            }
+            if (best_ms == 0.0 || per < best_ms) {
+              best_ms = per;
+              best = k;
+              best_v = v;
+              best_d = d;
+              if (tune_tiles) best_t = tq;
+              if (tune_chunks) best_w = wi;
+            }
           }
         }
       }
@@ -563,14 +574,17 @@ int Engine::autotune(const double* rho, const double* vext, const double* mu, cu
   cudaEventDestroy(e1);
   timing_ = timing_was;
   if (tune_tiles) set_col_tile(best_t);
+  if (tune_chunks) set_plane_width(best_w);
   if (tune_chunks) set_chunks(best);
   set_pointwise(best_v);
   set_pw_spread(best_d);
   if (variant) *variant = best_v;
   if (tile) *tile = col_tile();
   if (spread) *spread = pw_div_;
+  if (plane) *plane = plane_width();
   std::lock_guard<std::mutex> lock(g_tune_mu);
   if (tune_chunks) g_tune_chunks[tune_key_] = best;
+  if (tune_chunks) g_tune_plane[tune_key_] = best_w;
   if (tune_tiles) g_tune_tile[tune_key_] = best_t;
   g_tune_variant[tune_key_] = best_v;
   g_tune_spread[tune_key_] = best_d;
@@ -586,6 +600,15 @@ void Engine::set_col_tile(int tq) {
 }
 
 int Engine::col_tile() const { return fusable_ ? plan_.tq : 0; }
+
+void Engine::set_plane_width(int wide) {
+  if (!fusable_) throw std::invalid_argument("plane width: the engine has no fused path");
+  if (wide != 0 && wide != 1) throw std::invalid_argument("plane width: 0 (RPlane::NT threads) or 1 (twice that)");
+  if (plan_.plane_wide != (wide == 1)) ++generation_;
+  plan_.plane_wide = wide == 1;
+}
+
+int Engine::plane_width() const { return fusable_ ? (plan_.plane_wide ? 1 : 0) : -1; }
 
 void Engine::set_pointwise(int v) {
   if (v < 0 || v >= kPointwiseVariants) throw std::invalid_argument("pointwise variant: 0 .. 5");

@@ -106,11 +106,13 @@ class Engine {
   // counts: ms[v * kMaxChunks + k - 1]; *variant receives the variant kept.
   // Several species also tune the column tile width (16, 32), and every
   // chunk count k its pointwise spread d (1, 2, 4, 8 up to k):
-  // ms[((tile_index * kPointwiseVariants + v) * kMaxChunks + k - 1) * kSpreads + log2 d].
+  // ms[((tile_index * kPointwiseVariants + v) * kMaxChunks + k - 1) * kSpreads + log2 d]
+  // (the faster of the two middle plane-pass widths, which is also tuned).
+  // *plane (optional) receives the plane width kept.
   static constexpr int kPointwiseVariants = 6;
   static constexpr int kSpreads = 4;
   int autotune(const double* rho, const double* vext, const double* mu, cudaStream_t stream, int reps,
-               double* ms, int* variant, int* tile = nullptr, int* spread = nullptr);
+               double* ms, int* variant, int* tile = nullptr, int* spread = nullptr, int* plane = nullptr);
   // Pointwise grid of one plane chunk: the full pointwise grid (pw_grid)
   // divided by d = min(spread, chunks), 0 = the chunk count (each chunk one
   // share).  Larger shares put more warps on one chunk's FP64 work (a
@@ -123,10 +125,17 @@ class Engine {
   // several species where their spectra fit); std::invalid_argument otherwise.
   void set_col_tile(int tq);
   int col_tile() const;
+  // Threads per plane CTA of the fused path's two middle plane passes
+  // (channels inverse, derivatives forward): 0 RPlane::NT, 1 twice that
+  // (RPlane::NT_WIDE, the width of the one-sequence passes).  The autotuner
+  // times both.  plane_width() is -1 without the fused path.
+  void set_plane_width(int wide);
+  int plane_width() const;
   // Pointwise kernel of the TMA path: 0 generic; one species: 1 / 2 sized
   // for 5 / 6 CTAs per SM, 3 the branch-free FP64 path for warps with eta >=
   // 1e-6 everywhere (5 CTAs per SM), 4 the same with two points per thread
-  // (3 CTAs per SM); std::invalid_argument where the variant does not exist.
+  // (3 CTAs per SM), 5 as 4 at 4 CTAs per SM; std::invalid_argument where the
+  // variant does not exist.
   void set_pointwise(int v);
   int pointwise() const { return pw_variant_; }
   bool pointwise_one_species() const { return pw1_; }

@@ -94,11 +94,14 @@ bool fused_plan(const EvalParams& p, FusedPlan* plan) {
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
     allow_smem(rk::k_rplane_fwd<NY, NZ, double, rk::RPlane<NY, NZ>::NT_WIDE>, f.plane_smem);
+    constexpr int NTW = rk::RPlane<NY, NZ>::NT_WIDE;
     allow_smem(rk::k_rplane_fwd<NY, NZ, float>, f.plane_smem);
+    allow_smem(rk::k_rplane_fwd<NY, NZ, float, NTW>, f.plane_smem);
     with_layout(p, [&](auto mc, auto tc) {
       constexpr bool MU = decltype(mc)::value, TE = decltype(tc)::value;
       allow_smem(rk::k_rplane_inv<NY, NZ, false, MU, TE>, f.plane_smem);
-      allow_smem(rk::k_rplane_inv<NY, NZ, true, MU, TE, rk::RPlane<NY, NZ>::NT_WIDE>, f.plane_smem);
+      allow_smem(rk::k_rplane_inv<NY, NZ, false, MU, TE, NTW>, f.plane_smem);
+      allow_smem(rk::k_rplane_inv<NY, NZ, true, MU, TE, NTW>, f.plane_smem);
     });
   });
   with_len(p.nx, [&](auto xc) {
@@ -173,9 +176,16 @@ void fused_plane_inv(const FusedPlan& f, const EvalParams& p, const fft::cpx* q,
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
     with_layout(p, [&](auto mc, auto tc) {
-      rk::k_rplane_inv<NY, NZ, false, decltype(mc)::value, decltype(tc)::value>
-          <<<dim3(nplanes, p.n_chan, p.batch), rk::RPlane<NY, NZ>::NT, f.plane_smem, st>>>(
-              p, q, p.n_chan, chan_r, nullptr, nullptr, MuArgs{}, FinalArgs{nullptr, 0, nullptr, nullptr}, err, ix0, T);
+      constexpr bool MU = decltype(mc)::value, TE = decltype(tc)::value;
+      auto go = [&](auto nc) {
+        constexpr int NT = decltype(nc)::value;
+        rk::k_rplane_inv<NY, NZ, false, MU, TE, NT><<<dim3(nplanes, p.n_chan, p.batch), NT, f.plane_smem, st>>>(
+            p, q, p.n_chan, chan_r, nullptr, nullptr, MuArgs{}, FinalArgs{nullptr, 0, nullptr, nullptr}, err, ix0, T);
+      };
+      if (f.plane_wide)
+        go(IC<rk::RPlane<NY, NZ>::NT_WIDE>{});
+      else
+        go(IC<rk::RPlane<NY, NZ>::NT>{});
     });
   });
   CDFT_CUDA(cudaGetLastError());
@@ -186,8 +196,15 @@ void fused_plane_fwd_deriv(const FusedPlan& f, const EvalParams& p, const float*
   with_plane(p.ny, p.nz, [&](auto yc, auto zc) {
     constexpr int NY = decltype(yc)::value, NZ = decltype(zc)::value;
     // (stream predecessor: the chunk's pointwise kernel)
-    launch_k(rk::k_rplane_fwd<NY, NZ, float>, dim3(nplanes, p.L.n_deriv, p.batch), dim3(rk::RPlane<NY, NZ>::NT),
-             f.plane_smem, st, f.pdl, p, deriv_r, p.L.n_deriv, (double*)nullptr, pd, err, ix0, T);
+    auto go = [&](auto nc) {
+      constexpr int NT = decltype(nc)::value;
+      launch_k(rk::k_rplane_fwd<NY, NZ, float, NT>, dim3(nplanes, p.L.n_deriv, p.batch), dim3(NT), f.plane_smem, st,
+               f.pdl, p, deriv_r, p.L.n_deriv, (double*)nullptr, pd, err, ix0, T);
+    };
+    if (f.plane_wide)
+      go(IC<rk::RPlane<NY, NZ>::NT_WIDE>{});
+    else
+      go(IC<rk::RPlane<NY, NZ>::NT>{});
   });
   CDFT_CUDA(cudaGetLastError());
 }

@@ -14,6 +14,9 @@ struct FusedPlan {
   int tq = 0;         // columns per column-pass tile
   int col_tiles = 0;  // column-pass CTAs per problem
   bool tq32 = false;  // several species: 32-column tiles fit (16 always do)
+  // the two middle plane passes (channels inverse, derivatives forward) with
+  // twice the threads per plane CTA (RPlane::NT_WIDE instead of NT)
+  bool plane_wide = false;
   // programmatic dependent launch of the passes whose stream predecessor is
   // the previous pass (set per evaluation: off while timing stages)
   bool pdl = false;

@@ -396,9 +396,10 @@ class Engine:
 
     def autotune_ex(self, rho_ptr: int, vext_ptr: int = 0, mu=None, stream: int = 0, reps: int = 5):
         """Time every (plane-chunk count, pointwise variant, column tile,
-        pointwise spread) combination the engine has and keep the fastest.
-        Returns ((chunks, variant, tile, spread),
-        {(tile, variant, count, spread): ms})."""
+        pointwise spread, middle plane width) combination the engine has and
+        keep the fastest.  Returns ((chunks, variant, tile, spread),
+        {(tile, variant, count, spread): ms}), each entry the faster of the
+        two plane widths (``plane_width`` gives the one kept)."""
         choice = (ctypes.c_int * 4)()
         ms = (ctypes.c_double * (2 * POINTWISE_VARIANTS * 8 * 4))()
         mu_arr = None
@@ -465,6 +466,17 @@ class Engine:
 
     def set_column_tile(self, tile: int):
         _lib.check(_lib.lib().cdft_engine_set_column_tile(self.handle, int(tile)))
+
+    @property
+    def plane_width(self) -> int:
+        """Threads per CTA of the fused path's middle plane passes: 0 the base width, 1 twice it
+        (-1 without the fused path)."""
+        w = ctypes.c_int()
+        _lib.check(_lib.lib().cdft_engine_plane_width(self.handle, ctypes.byref(w)))
+        return w.value
+
+    def set_plane_width(self, wide: int):
+        _lib.check(_lib.lib().cdft_engine_set_plane_width(self.handle, int(wide)))
 
     @property
     def pointwise(self) -> int:

@@ -622,13 +622,23 @@ CDFT_API int cdft_engine_autotune(cdft_engine* engine, const double* rho, const 
  *    * CDFT_POINTWISE_SPREADS + log2 d]
  * for tile index t (0: 16, 1: 32), variant v, k chunks and spread d (0
  * where not tried; 2 * CDFT_POINTWISE_VARIANTS * CDFT_MAX_PLANE_CHUNKS *
- * CDFT_POINTWISE_SPREADS entries), choice = {chunks, variant, tile, spread}. */
+ * CDFT_POINTWISE_SPREADS entries), choice = {chunks, variant, tile, spread};
+ * the middle plane width kept is read with cdft_engine_plane_width. */
 #define CDFT_POINTWISE_VARIANTS 6
 #define CDFT_POINTWISE_SPREADS 4
 CDFT_API int cdft_engine_set_pointwise(cdft_engine* engine, int variant);
 CDFT_API int cdft_engine_pointwise(const cdft_engine* engine, int* variant, int* available);
 CDFT_API int cdft_engine_set_column_tile(cdft_engine* engine, int tile);
 CDFT_API int cdft_engine_column_tile(const cdft_engine* engine, int* tile);
+/* Threads per plane CTA of the fused path's two middle plane passes (the
+ * inverse transforms of the weighted-density channels and the forward
+ * transforms of the derivative channels, one CTA per x plane and channel):
+ * wide = 0 the base width (512 threads at 128 x 128 planes), 1 twice that.
+ * Results are bitwise the same.  cdft_engine_autotune times both; its table
+ * holds the faster one per entry.  cdft_engine_plane_width gives -1 without
+ * the fused path. */
+CDFT_API int cdft_engine_set_plane_width(cdft_engine* engine, int wide);
+CDFT_API int cdft_engine_plane_width(const cdft_engine* engine, int* wide);
 CDFT_API int cdft_engine_set_pointwise_spread(cdft_engine* engine, int spread);
 
 /* Programmatic dependent launch between consecutive passes of the fused path

@@ -216,6 +216,42 @@ def test_column_tile_widths_and_autotune_table():
         assert np.array_equal(after.forces[s], base.forces[s]), s
 
 
+@pytest.mark.parametrize("shape,diams", [((64, 32, 32), [1.0, 0.6]), ((128, 32, 64), [1.0]),
+                                         ((32, 128, 128), [1.0]), ((48, 96, 48), [1.0])])
+def test_middle_plane_widths(shape, diams):
+    """The middle plane passes at the base width and at twice the threads
+    per plane CTA compute every sample the same way: forces and F bitwise
+    equal.  The autotuner keeps one of the two; an engine without the fused
+    path has none."""
+    import torch
+    S = len(diams)
+    inters = [(0, 0) + LJ] + ([(0, 1, 1.0, 0.8, 2.5)] if S > 1 else [])
+    pr = Problem(shape, 0.1, diams, "WhiteBearII", inters=inters, kT=0.9, precision=cd.MIXED)
+    rng = np.random.default_rng(10)
+    rhos = [0.3 / (s + 1) * (1.0 + 0.05 * smooth_noise(shape, rng)) for s in range(S)]
+    mu = [0.2, -0.1][:S]
+    e = pr.weights.engine
+    e.set_plane_width(0)
+    assert e.plane_width == 0
+    base = pr.gpu(rhos, mu)
+    e.set_plane_width(1)
+    assert e.plane_width == 1
+    wide = pr.gpu(rhos, mu)
+    for s in range(S):
+        assert np.array_equal(wide.forces[s], base.forces[s]), s
+    assert wide.free_energy == base.free_energy
+    assert rel_err(base.free_energy, pr.ref(rhos, mu).free_energy) <= 1e-9
+    with pytest.raises(ValueError):
+        e.set_plane_width(2)
+    rd = torch.tensor(np.concatenate([r.ravel() for r in rhos]), device="cuda")
+    e.autotune_ex(rd.data_ptr(), mu=mu, reps=1)
+    assert e.plane_width in (0, 1)
+    cu = Problem((24, 24, 24), 0.2, [1.0], "WhiteBearII", precision=cd.MIXED)
+    assert cu.weights.engine.plane_width == -1
+    with pytest.raises(ValueError):
+        cu.weights.engine.set_plane_width(1)
+
+
 def test_pointwise_spread():
     """Each plane chunk's pointwise launch may take 1/8 .. all of the
     pointwise grid: forces bitwise equal (each point is computed the same
