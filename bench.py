@@ -396,17 +396,20 @@ SWEEP_BATCH = 16
 
 
 def batched_headline(torch, cd, dev, precision, rho, flush, stream, steps):
-    """The headline state (128^3) as B = 2 and 4 problems of one batched
+    """The headline state (128^3) as B = 2, 4 and 8 problems of one batched
     engine per launch (independent states sharing the launches: the
     throughput of evaluating many states, not the latency of one), in
-    problem evaluations per second, L2 flushed between steps."""
+    problem evaluations per second, L2 flushed between steps; and the FP64
+    path batched the same way at B = 4 (fp64_B4), its like-for-like
+    reference."""
     lj = cd.make_lennard_jones(1.0, 1.0, 2.5)
     d = lj.hard_sphere_diameter(KT, cd.WEEKS_CHANDLER_ANDERSEN)
     g = cd.Grid(dx=DX, box_size=tuple(n * DX for n in SHAPE), shape=SHAPE)
     model = cd.Model(g, [cd.Species("LJ", d)], [cd.Interaction(0, 0, lj)], KT)
     out = {}
-    for B in (2, 4):
-        eng = cd.Engine(cd.WhiteBearII(), model, precision, batch=B)
+    other = cd.FP64 if precision == cd.MIXED else cd.MIXED
+    for B, prec in ((2, precision), (4, precision), (8, precision), (4, other)):
+        eng = cd.Engine(cd.WhiteBearII(), model, prec, batch=B)
         rb = rho.repeat(B).contiguous()
         f = torch.empty_like(rb)
         sc = torch.empty((B, 10), dtype=torch.float64, device=dev)
@@ -426,8 +429,11 @@ def batched_headline(torch, cd, dev, precision, rho, flush, stream, steps):
                 evs[i][1].record(stream)
         torch.cuda.synchronize()
         t = sum(a.elapsed_time(b) for a, b in evs) / steps
-        out[f"B{B}"] = {"problem_evals_per_s": B / (t * 1e-3), "ms_per_launch": t}
+        key = f"B{B}" if prec == precision else ("fp64" if other == cd.FP64 else "mixed") + f"_B{B}"
+        out[key] = {"problem_evals_per_s": B / (t * 1e-3), "ms_per_launch": t}
         eng.close()
+    if "fp64_B4" in out:
+        out["B4_vs_fp64_B4"] = out["B4"]["problem_evals_per_s"] / out["fp64_B4"]["problem_evals_per_s"]
     return out
 
 
