@@ -21,7 +21,8 @@ buffers, H2D of every state's rho and D2H of its force and scalars inside the
 timed region: `value` through cdft_total_stream (a sequence of states per
 call, the copies of one state overlapping the evaluation of the next),
 `per_call` through cdft_total (one state per call, copies and evaluation in
-series).
+series), and `copy_bound` the same page-locked copies alone (the PCIe rate
+the streamed number is measured against).
 """
 from __future__ import annotations
 
