@@ -56,6 +56,14 @@ struct Lay {
   static constexpr int V0 = MULTI ? 7 : -1;
   static constexpr int T = MULTI ? 10 : 5;  // xx, xy, xz, yy, yz
   static constexpr int NFMT = MULTI ? (TENSOR ? 15 : 10) : (TENSOR ? 10 : 5);
+  // Channels whose weight vanishes at k = 0 (the vectors and the off-diagonal
+  // tensor components): their split offset and their derivative constant at
+  // the mean state are exactly zero (chan_dc; dPhi/dv and dPhi/dT_ij, i != j,
+  // vanish where v = 0 and T is diagonal).
+  static constexpr bool zero_dc(int c) {
+    return (c >= V1 && c < V1 + 3) || (MULTI && c >= V0 && c < V0 + 3) ||
+           (TENSOR && (c == T + 1 || c == T + 2 || c == T + 4));
+  }
 };
 
 // |k|-only factors of the FMT weights of one species at one wavevector.
@@ -1026,8 +1034,9 @@ __device__ __forceinline__ void pw1_point(const EvalParams& p, const double* n, 
   for (int q = 0; q < NMF; ++q) f0 += n[NF + q];
   if (live) {
     acc[kTermHS] += phi;
+    // (no subtraction where the constant is zero: fewer shared loads and FP64 adds)
 #pragma unroll
-    for (int c = 0; c < NF; ++c) __stcs(deriv + c * N + idx, (float)(D[c] - dbar[c]));
+    for (int c = 0; c < NF; ++c) __stcs(deriv + c * N + idx, L::zero_dc(c) ? (float)D[c] : (float)(D[c] - dbar[c]));
     acc[kTermId] += r * (lr - 1.0);
     acc[kTermExt] += r * v;
     acc[kTermN0] += r;
@@ -1130,7 +1139,10 @@ __global__ void __launch_bounds__(kTmaTile, MINB) k_pointwise1_tma(EvalParams p,
       live[j] = idx + j * kTmaTile < idx_end;
       const float* cs = reinterpret_cast<const float*>(base) + o;
 #pragma unroll
-      for (int c = 0; c < NIN; ++c) n[j][c] = (double)cs[c * TP] + off[c];
+      for (int c = 0; c < NIN; ++c) {
+        const double x = (double)cs[c * TP];
+        n[j][c] = (c < NF && L::zero_dc(c)) ? x : x + off[c];
+      }
       r[j] = reinterpret_cast<const double*>(base + RHO_OFF)[o];
       v[j] = HAS_V ? reinterpret_cast<const double*>(base + V_OFF)[o] : 0.0;
       lane_fast = lane_fast && (!live[j] || n[j][L::ETA] >= 1e-6);
