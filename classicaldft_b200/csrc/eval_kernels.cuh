@@ -1029,7 +1029,7 @@ __device__ __forceinline__ void pw1_point(const EvalParams& p, const double* n, 
     for (int c = 0; c < NF; ++c) D[c] = 0.0;
   }
   const double lr = log(r < 1e-300 ? 1e-300 : r);
-  double f0 = lr + v;  // -mu dV is added by k_epilogue
+  double f0 = HAS_V ? lr + v : lr;  // -mu dV is added by k_epilogue
 #pragma unroll
   for (int q = 0; q < NMF; ++q) f0 += n[NF + q];
   if (live) {
@@ -1038,7 +1038,7 @@ __device__ __forceinline__ void pw1_point(const EvalParams& p, const double* n, 
 #pragma unroll
     for (int c = 0; c < NF; ++c) __stcs(deriv + c * N + idx, L::zero_dc(c) ? (float)D[c] : (float)(D[c] - dbar[c]));
     acc[kTermId] += r * (lr - 1.0);
-    acc[kTermExt] += r * v;
+    if constexpr (HAS_V) acc[kTermExt] += r * v;
     acc[kTermN0] += r;
 #pragma unroll
     for (int q = 0; q < NMF; ++q) acc[kTermMF] += 0.5 * r * n[NF + q];
